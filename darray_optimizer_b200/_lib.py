@@ -1,0 +1,124 @@
+"""ctypes binding of libdarray_b200.so (the C ABI declared in include/darray_b200.h).
+
+The library is the product: there is no CPU fallback.  If the shared object is missing, loading raises
+instead of degrading silently.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "lib" / "libdarray_b200.so"
+HEADER = PKG.parent / "include" / "darray_b200.h"
+
+_c_int, _c_float, _c_double = ctypes.c_int, ctypes.c_float, ctypes.c_double
+_vp = ctypes.c_void_p
+_i64 = ctypes.c_int64
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "db200_create": (_c_int, [ctypes.POINTER(_vp), _c_int, _vp]),
+    "db200_destroy": (_c_int, [_vp]),
+    "db200_last_error": (ctypes.c_char_p, [_vp]),
+    "db200_synchronize": (_c_int, [_vp]),
+    "db200_stream": (_vp, [_vp]),
+    "db200_launch_count": (_i64, [_vp]),
+    "db200_rbf_sketch": (_c_int, [_vp, _c_int, _c_int, _c_int, _c_int, _vp, _c_int, _vp, _c_int, _c_int, _vp, _vp,
+                                  _vp, _c_int, _vp, _c_int, _c_float]),
+    "db200_rbf_block": (_c_int, [_vp, _c_int, _c_int, _c_int, _vp, _c_int, _vp, _c_int, _c_int, _vp, _vp, _vp,
+                                 _c_int, _c_float]),
+}
+
+STATUS = {
+    0: "DB200_OK", -1: "DB200_ERR_INVALID", -2: "DB200_ERR_CUDA", -3: "DB200_ERR_NOT_SPD",
+    -4: "DB200_ERR_MAXITER", -5: "DB200_ERR_INFEASIBLE", -6: "DB200_ERR_TIMEOUT", -7: "DB200_ERR_NOMEM",
+    -8: "DB200_ERR_UNSUPPORTED",
+}
+POINT_MAJOR, FEATURE_MAJOR = 0, 1
+
+_lib = None
+
+
+class DB200Error(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+def header_functions() -> list[str]:
+    """Names of every function declared in include/darray_b200.h."""
+    text = HEADER.read_text()
+    return sorted(set(re.findall(r"^\s*(?:DB200_API\s+)?(?:int|void|const char\s*\*|void\s*\*|int64_t)\s*\*?\s*(db200_\w+)\s*\(",
+                                 text, flags=re.M)))
+
+
+def load() -> ctypes.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m darray_optimizer_b200.build`")
+    lib = ctypes.CDLL(str(LIB_PATH), mode=os.RTLD_NOW | os.RTLD_GLOBAL)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+class Context:
+    """Owns a db200_context on one device; `stream` is a raw cudaStream_t (int) or None."""
+
+    def __init__(self, device: int = 0, stream: int | None = None):
+        self.lib = load()
+        h = _vp()
+        st = self.lib.db200_create(ctypes.byref(h), device, stream)
+        if st != 0:
+            raise DB200Error(st, f"db200_create(device={device}) failed")
+        self.h = h
+
+    def check(self, st: int):
+        if st != 0:
+            msg = self.lib.db200_last_error(self.h)
+            raise DB200Error(st, msg.decode() if msg else "")
+        return st
+
+    def sync(self):
+        return self.check(self.lib.db200_synchronize(self.h))
+
+    @property
+    def stream(self) -> int:
+        return self.lib.db200_stream(self.h) or 0
+
+    def launches(self) -> int:
+        return int(self.lib.db200_launch_count(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.db200_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -------------------------------------------------------------- thin wrappers (device pointers as ints)
+    def rbf_sketch(self, m, n, d, l, Xi, ldxi, Xj, ldxj, layout, yi, yj, Om, ldo, Y, ldy, gamma):
+        return self.check(self.lib.db200_rbf_sketch(self.h, m, n, d, l, Xi, ldxi, Xj, ldxj, layout, yi, yj, Om,
+                                                    ldo, Y, ldy, gamma))
+
+    def rbf_block(self, m, n, d, Xi, ldxi, Xj, ldxj, layout, yi, yj, K, ldk, gamma):
+        return self.check(self.lib.db200_rbf_block(self.h, m, n, d, Xi, ldxi, Xj, ldxj, layout, yi, yj, K, ldk,
+                                                   gamma))

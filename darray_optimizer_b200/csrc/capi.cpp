@@ -1,0 +1,219 @@
+// C ABI of libdarray_b200: context management and the RBF kernel / sketch entry points.
+#include <cstdio>
+#include <cstring>
+#include <atomic>
+#include <string>
+
+#include "internal.h"
+
+namespace db200 {
+
+static std::atomic<long long> g_tile_launches{0};
+
+int fail(db200_context* ctx, int status, const std::string& msg) {
+  if (ctx) ctx->last_error = msg;
+  return status;
+}
+
+int cuda_fail(db200_context* ctx, cudaError_t err, const char* what) {
+  std::string m = std::string(what) + ": " + cudaGetErrorString(err);
+  return fail(ctx, err == cudaErrorMemoryAllocation ? DB200_ERR_NOMEM : DB200_ERR_CUDA, m);
+}
+
+void* workspace(db200_context* ctx, size_t bytes) {
+  if (bytes <= ctx->ws_size) return ctx->ws;
+  // Growing: queued work may still read the old buffer.
+  cudaStreamSynchronize(ctx->stream);
+  if (ctx->ws) cudaFree(ctx->ws);
+  ctx->ws = nullptr;
+  ctx->ws_size = 0;
+  size_t want = align_up(bytes + bytes / 8, 1 << 20);
+  cudaError_t e = cudaMalloc(&ctx->ws, want);
+  if (e != cudaSuccess) {
+    ctx->ws = nullptr;
+    cuda_fail(ctx, e, "cudaMalloc(workspace)");
+    return nullptr;
+  }
+  ctx->ws_size = want;
+  return ctx->ws;
+}
+
+void count_tile_launch() { g_tile_launches.fetch_add(1); }
+
+}  // namespace db200
+
+using namespace db200;
+
+extern "C" {
+
+int db200_create(db200_context** out, int device, void* stream) {
+  if (!out) return DB200_ERR_INVALID;
+  *out = nullptr;
+  auto* ctx = new db200_context();
+  ctx->device = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) {
+    delete ctx;
+    return DB200_ERR_CUDA;
+  }
+  cudaDeviceProp prop;
+  e = cudaGetDeviceProperties(&prop, device);
+  if (e != cudaSuccess) {
+    delete ctx;
+    return DB200_ERR_CUDA;
+  }
+  if (prop.major != 10) {
+    std::fprintf(stderr, "darray_b200: device %d is sm_%d%d; this library is built for sm_100a only\n", device,
+                 prop.major, prop.minor);
+    delete ctx;
+    return DB200_ERR_UNSUPPORTED;
+  }
+  ctx->num_sms = prop.multiProcessorCount;
+  if (stream) {
+    ctx->stream = static_cast<cudaStream_t>(stream);
+  } else {
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      delete ctx;
+      return DB200_ERR_CUDA;
+    }
+    ctx->own_stream = true;
+  }
+  if (cudaMalloc(&ctx->d_status, sizeof(int)) != cudaSuccess ||
+      cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream) != cudaSuccess ||
+      cudaMallocHost(&ctx->h_pinned, 4096) != cudaSuccess) {
+    db200_destroy(ctx);
+    return DB200_ERR_CUDA;
+  }
+  *out = ctx;
+  return DB200_OK;
+}
+
+int db200_destroy(db200_context* ctx) {
+  if (!ctx) return DB200_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->ws) cudaFree(ctx->ws);
+  if (ctx->d_status) cudaFree(ctx->d_status);
+  if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
+  if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return DB200_OK;
+}
+
+const char* db200_last_error(const db200_context* ctx) { return ctx ? ctx->last_error.c_str() : "no context"; }
+
+void* db200_stream(const db200_context* ctx) { return ctx ? static_cast<void*>(ctx->stream) : nullptr; }
+
+int64_t db200_launch_count(const db200_context*) { return (int64_t)g_tile_launches.load(); }
+
+int db200_synchronize(db200_context* ctx) {
+  if (!ctx) return DB200_ERR_INVALID;
+  DB200_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  int st = 0;
+  DB200_CUDA(ctx, cudaMemcpy(&st, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+  if (st != 0) {
+    cudaMemset(ctx->d_status, 0, sizeof(int));
+    return fail(ctx, st, "a device-side bounded wait gave up (kernel pipeline stalled)");
+  }
+  return DB200_OK;
+}
+
+static int check_points(db200_context* ctx, int m, int d, const float* X, int ldx, int layout) {
+  if (!X) return fail(ctx, DB200_ERR_INVALID, "null point matrix");
+  if (layout == DB200_POINT_MAJOR) {
+    if (ldx < d) return fail(ctx, DB200_ERR_INVALID, "point-major ldx < d");
+  } else if (layout == DB200_FEATURE_MAJOR) {
+    if (ldx < m) return fail(ctx, DB200_ERR_INVALID, "feature-major ldx < m");
+  } else {
+    return fail(ctx, DB200_ERR_INVALID, "unknown point layout");
+  }
+  return DB200_OK;
+}
+
+// Packs Xi (and Xj unless it is the same matrix) into the workspace.
+static int pack_pair(db200_context* ctx, int m, int n, int d, const float* Xi, int ldxi, const float* Xj, int ldxj,
+                     int layout, size_t extra_bytes, PackedPoints& pi, PackedPoints& pj, Carve& carve) {
+  const int dp = feature_pad(d);
+  const int mpad = round_up(m, 128), npad = round_up(n, 128);
+  const bool same = (Xi == Xj && ldxi == ldxj && m == n);
+  size_t bytes = 4096 + (size_t)mpad * (2 * dp * 2 + 4) + extra_bytes + 4 * 256;
+  if (!same) bytes += (size_t)npad * (2 * dp * 2 + 4);
+  void* ws = workspace(ctx, bytes);
+  if (!ws) return DB200_ERR_NOMEM;
+  carve = Carve{static_cast<char*>(ws)};
+  void* xpi = carve.take<uint16_t>((size_t)mpad * 2 * dp);
+  float* ni = carve.take<float>(mpad);
+  int st = pack_points(ctx, Xi, ldxi, layout, m, d, dp, mpad, xpi, ni);
+  if (st) return st;
+  pi.xp = xpi;
+  pi.norms = ni;
+  pi.n = m;
+  pi.npad = mpad;
+  pi.dp = dp;
+  if (same) {
+    pj = pi;
+  } else {
+    void* xpj = carve.take<uint16_t>((size_t)npad * 2 * dp);
+    float* nj = carve.take<float>(npad);
+    st = pack_points(ctx, Xj, ldxj, layout, n, d, dp, npad, xpj, nj);
+    if (st) return st;
+    pj.xp = xpj;
+    pj.norms = nj;
+    pj.n = n;
+    pj.npad = npad;
+    pj.dp = dp;
+  }
+  return DB200_OK;
+}
+
+int db200_rbf_sketch(db200_context* ctx, int m, int n, int d, int l, const float* Xi, int ldxi, const float* Xj,
+                     int ldxj, int x_layout, const float* yi, const float* yj, const float* Omega, int ldo, float* Y,
+                     int ldy, float gamma) {
+  if (!ctx) return DB200_ERR_INVALID;
+  if (m < 0 || n < 0 || d < 1 || l < 0) return fail(ctx, DB200_ERR_INVALID, "rbf_sketch: negative size");
+  if (m == 0 || l == 0) return DB200_OK;
+  if (d > 128) return fail(ctx, DB200_ERR_UNSUPPORTED, "rbf_sketch: d > 128 not supported");
+  if (!Y || ldy < m) return fail(ctx, DB200_ERR_INVALID, "rbf_sketch: bad Y / ldy");
+  if (n == 0) {
+    for (int c = 0; c < l; ++c) DB200_CUDA(ctx, cudaMemsetAsync(Y + (size_t)c * ldy, 0, sizeof(float) * m, ctx->stream));
+    return DB200_OK;
+  }
+  if (!Omega || ldo < n) return fail(ctx, DB200_ERR_INVALID, "rbf_sketch: bad Omega / ldo");
+  int st = check_points(ctx, m, d, Xi, ldxi, x_layout);
+  if (!st) st = check_points(ctx, n, d, Xj, ldxj, x_layout);
+  if (st) return st;
+  const SketchPlan plan = plan_sketch(l);
+  const int npad = round_up(n, 128);
+  PackedPoints pi, pj;
+  Carve carve{nullptr};
+  st = pack_pair(ctx, m, n, d, Xi, ldxi, Xj, ldxj, x_layout, (size_t)plan.lrows * npad * 2 + 256, pi, pj, carve);
+  if (st) return st;
+  void* op = carve.take<uint16_t>((size_t)plan.lrows * npad);
+  st = pack_sketch(ctx, Omega, ldo, yj, n, l, npad, plan.lrows, op);
+  if (st) return st;
+  st = launch_rbf_tiles(ctx, RBF_MODE_SKETCH, pi, pj, yi, nullptr, op, plan, l, gamma, Y, ldy);
+  if (!st) count_tile_launch();
+  return st;
+}
+
+int db200_rbf_block(db200_context* ctx, int m, int n, int d, const float* Xi, int ldxi, const float* Xj, int ldxj,
+                    int x_layout, const float* yi, const float* yj, float* K, int ldk, float gamma) {
+  if (!ctx) return DB200_ERR_INVALID;
+  if (m < 0 || n < 0 || d < 1) return fail(ctx, DB200_ERR_INVALID, "rbf_block: negative size");
+  if (m == 0 || n == 0) return DB200_OK;
+  if (d > 128) return fail(ctx, DB200_ERR_UNSUPPORTED, "rbf_block: d > 128 not supported");
+  if (!K || ldk < m) return fail(ctx, DB200_ERR_INVALID, "rbf_block: bad K / ldk");
+  int st = check_points(ctx, m, d, Xi, ldxi, x_layout);
+  if (!st) st = check_points(ctx, n, d, Xj, ldxj, x_layout);
+  if (st) return st;
+  PackedPoints pi, pj;
+  Carve carve{nullptr};
+  st = pack_pair(ctx, m, n, d, Xi, ldxi, Xj, ldxj, x_layout, 0, pi, pj, carve);
+  if (st) return st;
+  SketchPlan plan;
+  st = launch_rbf_tiles(ctx, RBF_MODE_KBLOCK, pi, pj, yi, yj, nullptr, plan, 0, gamma, K, ldk);
+  if (!st) count_tile_launch();
+  return st;
+}
+
+}  // extern "C"

@@ -1,0 +1,83 @@
+// Internal host-side interfaces shared by the .cu translation units of libdarray_b200.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <cuda_runtime.h>
+
+#include "../../include/darray_b200.h"
+
+struct db200_context {
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int* d_status = nullptr;       // device status word written by kernels whose bounded waits give up
+  void* ws = nullptr;            // device workspace (packed operands, small factors)
+  size_t ws_size = 0;
+  double* h_pinned = nullptr;    // small pinned host staging area for scalar readbacks
+  std::string last_error;
+};
+
+namespace db200 {
+
+// Error helpers: set ctx->last_error and return the status.
+int fail(db200_context* ctx, int status, const std::string& msg);
+int cuda_fail(db200_context* ctx, cudaError_t err, const char* what);
+
+#define DB200_CUDA(ctx, call)                                   \
+  do {                                                          \
+    cudaError_t e_ = (call);                                    \
+    if (e_ != cudaSuccess) return ::db200::cuda_fail((ctx), e_, #call); \
+  } while (0)
+
+// Grow-only workspace; returns nullptr on failure (ctx->last_error set).
+void* workspace(db200_context* ctx, size_t bytes);
+
+inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+inline int round_up(int x, int a) { return (x + a - 1) / a * a; }
+
+// Bump allocator over one workspace request.
+struct Carve {
+  char* base;
+  size_t off = 0;
+  template <class T>
+  T* take(size_t count) {
+    off = align_up(off, 256);
+    T* p = reinterpret_cast<T*>(base + off);
+    off += count * sizeof(T);
+    return p;
+  }
+};
+
+// ------------------------------------------------------------------ RBF tile engine (rbf_tile.cu)
+enum RbfMode { RBF_MODE_SKETCH = 0, RBF_MODE_KBLOCK = 1 };
+
+struct PackedPoints {
+  const void* xp = nullptr;   // bf16 [npad][2*dp]: [hi | lo] split of each point
+  const float* norms = nullptr;  // fp32 [npad], ||x||^2 (zero on padding rows)
+  int n = 0, npad = 0, dp = 0;
+};
+
+// Pack points into the split-bf16 operand layout plus squared norms.
+// layout: DB200_POINT_MAJOR (x_ik = X[k + i*ldx]) or DB200_FEATURE_MAJOR (x_ik = X[i + k*ldx]).
+int pack_points(db200_context* ctx, const float* X, int ldx, int layout, int n, int d, int dp, int npad, void* xp,
+                float* norms);
+
+// Omega^T (bf16, [lrows][njpad]) with the column labels folded in: Op[c][j] = y_j * Omega[j + c*ldo].
+int pack_sketch(db200_context* ctx, const float* Omega, int ldo, const float* yj, int n, int l, int njpad, int lrows,
+                void* op);
+
+struct SketchPlan {
+  int n_panels = 1, panel = 16, lrows = 16;
+};
+SketchPlan plan_sketch(int l);
+int feature_pad(int d);  // dp: padded feature count of the split operand
+
+// Launch the fused tile kernel.  For RBF_MODE_SKETCH, `op` is the packed Omega^T and `out` is Y (m x l, column
+// major, leading dimension ldo); for RBF_MODE_KBLOCK, `out` is the kernel block K (m x n, column major).
+int launch_rbf_tiles(db200_context* ctx, int mode, const PackedPoints& pi, const PackedPoints& pj, const float* yi,
+                     const float* yj, const void* op, const SketchPlan& plan, int l, float gamma, float* out,
+                     int ldo);
+
+}  // namespace db200

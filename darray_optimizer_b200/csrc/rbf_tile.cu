@@ -1,0 +1,521 @@
+// Fused RBF-kernel tile engine for sm_100a (tcgen05 + TMEM + TMA).
+//
+// One CTA owns a 128-row block of points i and one panel of sketch columns.  It streams every 128-column
+// block of points j and, per tile:
+//   MMA1  G   = Xi . Xj^T  in TMEM (fp32), from split-bf16 operands: hi.hi + hi.lo + lo.hi
+//   epi   P   = exp2(min(a_i + b_j + c*G, 0)),  a = -gamma*log2(e)*||x||^2,  c = 2*gamma*log2(e)
+//   MMA2  Y  += P . Omega~_j   (SKETCH mode; P is written to shared memory as the bf16 A operand)
+//         or  K[i, j] = y_i y_j P   stored as fp32 (KBLOCK mode)
+// so the kernel matrix is never written to HBM in SKETCH mode.  Algorithm restated from
+// include/dkernel.cu:102-129 (vecnorm, rbf) and :151-178 / :194-231 (distance GEMM, rbf, sketch GEMM).
+//
+// Warp roles (320 threads): warp 0 = TMA producer, warp 1 = TMEM allocator + MMA issuer,
+// warps 2..9 = epilogue (two warps per TMEM lane quadrant, each owning 64 of the 128 tile columns).
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cstdio>
+#include <mutex>
+
+#include "internal.h"
+#include "ptx.cuh"
+
+namespace db200 {
+
+namespace {
+
+constexpr int BM = 128;          // rows of i per CTA (UMMA M)
+constexpr int BN = 128;          // columns of j per tile
+constexpr int KC = 64;           // bf16 elements per 128-byte swizzled row chunk
+constexpr int CHUNK_BYTES = BM * KC * 2;  // one 128 x 64 bf16 chunk = 16 KB
+constexpr int NUM_THREADS = 320;
+constexpr int NUM_EPI_WARPS = 8;
+constexpr int TMEM_COLS = 512;
+constexpr int TMEM_G0 = 0;       // two G buffers of 128 columns
+constexpr int TMEM_Y = 256;      // sketch accumulator, up to 256 columns
+constexpr float LOG2E = 1.4426950408889634f;
+
+struct TileArgs {
+  int m, n;            // valid rows / columns
+  int dp;              // padded feature count; packed row = [hi(dp) | lo(dp)]
+  int n_itiles, n_jtiles, n_panels, panel, l;
+  float c_row, c_dot;  // -gamma*log2e, 2*gamma*log2e
+  const float* si;
+  const float* sj;
+  const float* yi;
+  const float* yj;
+  float* out;
+  int ldo;
+  int* status;
+};
+
+struct SmemLayout {
+  int nkc;       // chunks per packed row
+  int nsx;       // Xj ring stages
+  int nso;       // Omega ring stages
+  int om_stage;  // bytes per Omega stage
+  size_t off_xi, off_xj, off_om, off_p, off_bar, total;
+};
+
+__host__ __device__ inline SmemLayout make_layout(int dp, int panel, int mode) {
+  SmemLayout L;
+  L.nkc = (2 * dp) / KC;
+  L.nsx = (mode == RBF_MODE_SKETCH) ? 4 : 8;
+  L.nso = (mode == RBF_MODE_SKETCH) ? 2 : 0;
+  L.om_stage = panel * 128;
+  L.off_xi = 0;
+  L.off_xj = L.off_xi + (size_t)L.nkc * CHUNK_BYTES;
+  L.off_om = L.off_xj + (size_t)L.nsx * CHUNK_BYTES;
+  L.off_p = L.off_om + (size_t)L.nso * L.om_stage;
+  L.off_bar = L.off_p + ((mode == RBF_MODE_SKETCH) ? 2 * CHUNK_BYTES : 0);
+  L.total = L.off_bar + 512;  // barriers, TMEM slot, abort flag
+  return L;
+}
+
+// Barrier slots (8 bytes each) after off_bar.
+enum {
+  B_XI_FULL = 0,
+  B_XI_EMPTY,
+  B_G_FULL0,
+  B_G_FULL1,
+  B_G_EMPTY0,
+  B_G_EMPTY1,
+  B_P_FULL,
+  B_P_EMPTY,
+  B_Y_FULL,
+  B_Y_EMPTY,
+  B_DRAIN,
+  B_XJ_FULL0,  // nsx full, then nsx empty, then nso full, nso empty
+};
+
+template <int MODE>
+__global__ void __launch_bounds__(NUM_THREADS, 1)
+    rbf_tile_kernel(const __grid_constant__ CUtensorMap tm_xi, const __grid_constant__ CUtensorMap tm_xj,
+                    const __grid_constant__ CUtensorMap tm_om, TileArgs args) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const SmemLayout L = make_layout(args.dp, args.panel, MODE);
+  const uint32_t s_xi = smem_u32(smem + L.off_xi);
+  const uint32_t s_xj = smem_u32(smem + L.off_xj);
+  const uint32_t s_om = smem_u32(smem + L.off_om);
+  const uint32_t s_p = smem_u32(smem + L.off_p);
+  const uint32_t s_bar = smem_u32(smem + L.off_bar);
+  auto bar = [&](int idx) -> uint32_t { return s_bar + 8u * (uint32_t)idx; };
+  const int XJ_FULL = B_XJ_FULL0, XJ_EMPTY = B_XJ_FULL0 + L.nsx, OM_FULL = XJ_EMPTY + L.nsx,
+            OM_EMPTY = OM_FULL + L.nso;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + L.off_bar + 400);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + L.off_bar + 408);
+
+  const int warp = threadIdx.x / 32;
+  const int lane = threadIdx.x % 32;
+  const int n_items = args.n_itiles * args.n_panels;
+
+  if (threadIdx.x == 0) {
+    *abort_flag = 0;
+    mbar_init(bar(B_XI_FULL), 1);
+    mbar_init(bar(B_XI_EMPTY), 1);
+    mbar_init(bar(B_G_FULL0), 1);
+    mbar_init(bar(B_G_FULL1), 1);
+    mbar_init(bar(B_G_EMPTY0), NUM_EPI_WARPS);
+    mbar_init(bar(B_G_EMPTY1), NUM_EPI_WARPS);
+    mbar_init(bar(B_P_FULL), NUM_EPI_WARPS);
+    mbar_init(bar(B_P_EMPTY), 1);
+    mbar_init(bar(B_Y_FULL), 1);
+    mbar_init(bar(B_Y_EMPTY), NUM_EPI_WARPS);
+    mbar_init(bar(B_DRAIN), 1);
+    for (int s = 0; s < L.nsx; ++s) {
+      mbar_init(bar(XJ_FULL + s), 1);
+      mbar_init(bar(XJ_EMPTY + s), 1);
+    }
+    for (int s = 0; s < L.nso; ++s) {
+      mbar_init(bar(OM_FULL + s), 1);
+      mbar_init(bar(OM_EMPTY + s), 1);
+    }
+    fence_mbarrier_init();
+  }
+  if (warp == 0 && lane == 0) {
+    prefetch_tmap(&tm_xi);
+    prefetch_tmap(&tm_xj);
+    if (MODE == RBF_MODE_SKETCH) prefetch_tmap(&tm_om);
+  }
+  if (warp == 1) {
+    tmem_alloc(smem_u32(tmem_slot), TMEM_COLS);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  if (warp == 0) {
+    // ------------------------------------------------------------ TMA producer
+    if (lane == 0) {
+      uint32_t kx = 0, ko = 0, items_done = 0, xi_loads = 0;
+      bool ok = true;
+      for (int item = blockIdx.x; item < n_items && ok; item += gridDim.x, ++items_done) {
+        const int it = item % args.n_itiles, pn = item / args.n_itiles;
+        if (!mbar_wait(bar(B_XI_EMPTY), (items_done & 1) ^ 1, abort_flag)) { ok = false; break; }
+        mbar_arrive_expect_tx(bar(B_XI_FULL), L.nkc * CHUNK_BYTES);
+        ++xi_loads;
+        for (int c = 0; c < L.nkc; ++c)
+          tma_load_2d(s_xi + c * CHUNK_BYTES, &tm_xi, bar(B_XI_FULL), c * KC, it * BM);
+        for (int jt = 0; jt < args.n_jtiles && ok; ++jt) {
+          for (int c = 0; c < L.nkc; ++c, ++kx) {
+            const uint32_t s = kx % L.nsx, ph = (kx / L.nsx) & 1;
+            if (!mbar_wait(bar(XJ_EMPTY + s), ph ^ 1, abort_flag)) { ok = false; break; }
+            mbar_arrive_expect_tx(bar(XJ_FULL + s), CHUNK_BYTES);
+            tma_load_2d(s_xj + s * CHUNK_BYTES, &tm_xj, bar(XJ_FULL + s), c * KC, jt * BN);
+          }
+          if (MODE == RBF_MODE_SKETCH) {
+            for (int c = 0; c < 2 && ok; ++c, ++ko) {
+              const uint32_t s = ko % L.nso, ph = (ko / L.nso) & 1;
+              if (!mbar_wait(bar(OM_EMPTY + s), ph ^ 1, abort_flag)) { ok = false; break; }
+              mbar_arrive_expect_tx(bar(OM_FULL + s), L.om_stage);
+              tma_load_2d(s_om + s * L.om_stage, &tm_om, bar(OM_FULL + s), jt * BN + c * KC, pn * args.panel);
+            }
+          }
+        }
+      }
+      if (!ok) {
+        // Drain: wait (time-bounded, ignoring the abort flag) for the loads this thread issued.
+        volatile int never = 0;
+        for (uint32_t k = (kx > (uint32_t)L.nsx ? kx - L.nsx : 0); k < kx; ++k)
+          mbar_wait(bar(XJ_FULL + k % L.nsx), (k / L.nsx) & 1, &never);
+        for (uint32_t k = (ko > (uint32_t)L.nso ? ko - L.nso : 0); k < ko; ++k)
+          mbar_wait(bar(OM_FULL + k % L.nso), (k / L.nso) & 1, &never);
+        if (xi_loads > 0) mbar_wait(bar(B_XI_FULL), (xi_loads - 1) & 1, &never);
+      }
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    // ------------------------------------------------------------ MMA issuer
+    if (lane == 0) {
+      const uint32_t idesc_g = idesc_f16(BM, BN, true);
+      const uint32_t idesc_y = idesc_f16(BM, args.panel, true);
+      const int dp = args.dp;
+      uint32_t kx = 0, ko = 0, kg = 0, kp = 0, items_done = 0;
+      bool ok = true;
+
+      auto issue_mma1 = [&]() -> bool {
+        const uint32_t b = kg & 1, ph = (kg >> 1) & 1;
+        if (!mbar_wait(bar(B_G_EMPTY0 + b), ph ^ 1, abort_flag)) return false;
+        tc_fence_after();
+        const uint32_t d_tmem = tmem_base + TMEM_G0 + b * BN;
+        bool first = true;
+        for (int c = 0; c < L.nkc; ++c, ++kx) {
+          const uint32_t s = kx % L.nsx, sph = (kx / L.nsx) & 1;
+          if (!mbar_wait(bar(XJ_FULL + s), sph, abort_flag)) return false;
+          tc_fence_after();
+          for (int ks = 0; ks < KC / 16; ++ks) {
+            const int o = c * KC + ks * 16;  // K offset of this slice inside the packed row
+            const uint64_t bdesc = sdesc_k_sw128(s_xj + s * CHUNK_BYTES + ks * 32);
+            if (o < dp) {  // B slice is hi_j: pair with hi_i and lo_i
+              const int oh = o, ol = dp + o;
+              umma_f16(d_tmem, sdesc_k_sw128(s_xi + (oh / KC) * CHUNK_BYTES + (oh % KC) * 2), bdesc, idesc_g,
+                       first ? 0u : 1u);
+              first = false;
+              umma_f16(d_tmem, sdesc_k_sw128(s_xi + (ol / KC) * CHUNK_BYTES + (ol % KC) * 2), bdesc, idesc_g, 1u);
+            } else {  // B slice is lo_j: pair with hi_i
+              const int oh = o - dp;
+              umma_f16(d_tmem, sdesc_k_sw128(s_xi + (oh / KC) * CHUNK_BYTES + (oh % KC) * 2), bdesc, idesc_g, 1u);
+            }
+          }
+          umma_commit(bar(XJ_EMPTY + s));
+        }
+        umma_commit(bar(B_G_FULL0 + b));
+        ++kg;
+        return true;
+      };
+
+      for (int item = blockIdx.x; item < n_items && ok; item += gridDim.x, ++items_done) {
+        if (!mbar_wait(bar(B_XI_FULL), items_done & 1, abort_flag)) { ok = false; break; }
+        tc_fence_after();
+        if (MODE == RBF_MODE_SKETCH && items_done > 0) {
+          if (!mbar_wait(bar(B_Y_EMPTY), (items_done - 1) & 1, abort_flag)) { ok = false; break; }
+          tc_fence_after();
+        }
+        if (!issue_mma1()) { ok = false; break; }
+        for (int jt = 0; jt < args.n_jtiles; ++jt) {
+          if (jt + 1 < args.n_jtiles && !issue_mma1()) { ok = false; break; }
+          if (MODE == RBF_MODE_SKETCH) {
+            if (!mbar_wait(bar(B_P_FULL), kp & 1, abort_flag)) { ok = false; break; }
+            tc_fence_after();
+            for (int c = 0; c < 2 && ok; ++c, ++ko) {
+              const uint32_t s = ko % L.nso, sph = (ko / L.nso) & 1;
+              if (!mbar_wait(bar(OM_FULL + s), sph, abort_flag)) { ok = false; break; }
+              tc_fence_after();
+              for (int ks = 0; ks < KC / 16; ++ks) {
+                umma_f16(tmem_base + TMEM_Y, sdesc_k_sw128(s_p + c * CHUNK_BYTES + ks * 32),
+                         sdesc_k_sw128(s_om + s * L.om_stage + ks * 32), idesc_y, (jt | c | ks) ? 1u : 0u);
+              }
+              umma_commit(bar(OM_EMPTY + s));
+            }
+            if (!ok) break;
+            umma_commit(bar(B_P_EMPTY));
+            ++kp;
+          }
+        }
+        if (!ok) break;
+        umma_commit(bar(B_XI_EMPTY));
+        if (MODE == RBF_MODE_SKETCH) umma_commit(bar(B_Y_FULL));
+      }
+      // All MMAs issued by this thread must be complete before TMEM is released.
+      umma_commit(bar(B_DRAIN));
+      volatile int never = 0;
+      mbar_wait(bar(B_DRAIN), 0, &never);
+    }
+    __syncwarp();
+  } else {
+    // ------------------------------------------------------------ epilogue
+    const int ew = warp - 2;              // 0..7
+    const int q = warp & 3;               // TMEM lane quadrant this warp may access
+    const int h = ew >> 2;                // column half of the tile
+    const int row = 32 * q + lane;        // row inside the 128-row block
+    const uint32_t t_lane = (uint32_t)(32 * q) << 16;
+    uint32_t kg = 0, kp = 0, items_done = 0;
+    bool ok = true;
+    for (int item = blockIdx.x; item < n_items && ok; item += gridDim.x, ++items_done) {
+      const int it = item % args.n_itiles, pn = item / args.n_itiles;
+      const int i = it * BM + row;
+      const float a_i = args.c_row * args.si[i];  // si is padded to n_itiles*BM
+      const float y_i = (i < args.m && args.yi) ? args.yi[i] : 1.0f;
+      for (int jt = 0; jt < args.n_jtiles; ++jt) {
+        const uint32_t b = kg & 1, ph = (kg >> 1) & 1;
+        if (!__all_sync(0xffffffffu, mbar_wait(bar(B_G_FULL0 + b), ph, abort_flag))) { ok = false; break; }
+        tc_fence_after();
+        float v[64];
+        const uint32_t tcol = tmem_base + t_lane + TMEM_G0 + b * BN + h * 64;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) tmem_ld16(tcol + c * 16, v + c * 16);
+        tmem_wait_ld();
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(bar(B_G_EMPTY0 + b));
+        ++kg;
+
+        const int j0 = jt * BN + h * 64;
+        const float4* sj4 = reinterpret_cast<const float4*>(args.sj + j0);
+#pragma unroll
+        for (int c = 0; c < 16; ++c) {
+          const float4 s4 = __ldg(sj4 + c);
+          v[4 * c + 0] = fast_exp2(fminf(fmaf(args.c_dot, v[4 * c + 0], fmaf(args.c_row, s4.x, a_i)), 0.0f));
+          v[4 * c + 1] = fast_exp2(fminf(fmaf(args.c_dot, v[4 * c + 1], fmaf(args.c_row, s4.y, a_i)), 0.0f));
+          v[4 * c + 2] = fast_exp2(fminf(fmaf(args.c_dot, v[4 * c + 2], fmaf(args.c_row, s4.z, a_i)), 0.0f));
+          v[4 * c + 3] = fast_exp2(fminf(fmaf(args.c_dot, v[4 * c + 3], fmaf(args.c_row, s4.w, a_i)), 0.0f));
+        }
+
+        if (MODE == RBF_MODE_SKETCH) {
+          if (!__all_sync(0xffffffffu, mbar_wait(bar(B_P_EMPTY), (kp & 1) ^ 1, abort_flag))) { ok = false; break; }
+          const uint32_t base = s_p + h * CHUNK_BYTES + (row >> 3) * 1024 + (row & 7) * 128;
+#pragma unroll
+          for (int g = 0; g < 8; ++g) {
+            const uint32_t addr = base + ((uint32_t)(g ^ (row & 7)) << 4);
+            st_shared_v4(addr, pack_bf16x2(v[8 * g + 0], v[8 * g + 1]), pack_bf16x2(v[8 * g + 2], v[8 * g + 3]),
+                         pack_bf16x2(v[8 * g + 4], v[8 * g + 5]), pack_bf16x2(v[8 * g + 6], v[8 * g + 7]));
+          }
+          fence_proxy_async_smem();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(bar(B_P_FULL));
+          ++kp;
+        } else {
+          if (i < args.m) {
+            float* out = args.out + i;
+#pragma unroll
+            for (int c = 0; c < 64; ++c) {
+              const int j = j0 + c;
+              if (j < args.n) {
+                const float yj = args.yj ? __ldg(args.yj + j) : 1.0f;
+                out[(size_t)j * args.ldo] = y_i * yj * v[c];
+              }
+            }
+          }
+        }
+      }
+      if (!ok) break;
+      if (MODE == RBF_MODE_SKETCH) {
+        if (!__all_sync(0xffffffffu, mbar_wait(bar(B_Y_FULL), items_done & 1, abort_flag))) { ok = false; break; }
+        tc_fence_after();
+        const int half = args.panel / 2;
+        for (int cc = 0; cc < half; cc += 8) {
+          float yv[8];
+          tmem_ld8(tmem_base + t_lane + TMEM_Y + h * half + cc, yv);
+          tmem_wait_ld();
+          if (i < args.m) {
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+              const int col = pn * args.panel + h * half + cc + e;
+              if (col < args.l) args.out[i + (size_t)col * args.ldo] = y_i * yv[e];
+            }
+          }
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(bar(B_Y_EMPTY));
+      }
+    }
+    __syncwarp();
+  }
+
+  __syncthreads();
+  if (threadIdx.x == 0 && *abort_flag) atomicExch(args.status, DB200_ERR_TIMEOUT);
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem_base, TMEM_COLS);
+  }
+}
+
+// ------------------------------------------------------------------ packing kernels
+__global__ void pack_points_kernel(const float* __restrict__ X, long long sp, long long sf, int n, int d, int dp,
+                                   int npad, __nv_bfloat16* __restrict__ Xp, float* __restrict__ norms) {
+  const int lane = threadIdx.x & 31;
+  const long long warps = (long long)gridDim.x * (blockDim.x / 32);
+  for (long long i = (long long)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32; i < npad; i += warps) {
+    float acc = 0.f;
+    __nv_bfloat16* row = Xp + i * (2 * dp);
+    for (int k = lane; k < dp; k += 32) {
+      const float x = (i < n && k < d) ? X[i * sp + (long long)k * sf] : 0.f;
+      const __nv_bfloat16 hi = __float2bfloat16_rn(x);
+      const __nv_bfloat16 lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+      row[k] = hi;
+      row[dp + k] = lo;
+      acc = fmaf(x, x, acc);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) norms[i] = acc;
+  }
+}
+
+__global__ void pack_sketch_kernel(const float* __restrict__ Om, long long ldo, const float* __restrict__ yj, int n,
+                                   int l, int njpad, int lrows, __nv_bfloat16* __restrict__ Op) {
+  const long long total = (long long)njpad * lrows;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int j = (int)(e % njpad);
+    const int c = (int)(e / njpad);
+    float v = 0.f;
+    if (j < n && c < l) v = Om[j + (long long)c * ldo] * (yj ? yj[j] : 1.0f);
+    Op[e] = __float2bfloat16_rn(v);
+  }
+}
+
+// ------------------------------------------------------------------ host helpers
+PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, []() {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+// 2-D bf16 tensor map: inner dimension `inner` (elements, contiguous), `outer` rows of pitch `pitch_elems`,
+// box 64 x box_rows, 128-byte swizzle.
+bool make_tmap(CUtensorMap* tm, const void* base, uint64_t inner, uint64_t outer, uint64_t pitch_elems,
+               uint32_t box_rows) {
+  auto enc = get_encode();
+  if (!enc) return false;
+  cuuint64_t dims[2] = {inner, outer};
+  cuuint64_t strides[1] = {pitch_elems * 2};
+  cuuint32_t box[2] = {64, box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = enc(tm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+}  // namespace
+
+int feature_pad(int d) { return round_up(d < 1 ? 1 : d, 32); }
+
+SketchPlan plan_sketch(int l) {
+  SketchPlan p;
+  const int lpad = round_up(l, 16);
+  p.n_panels = (lpad + 255) / 256;
+  p.panel = round_up((lpad + p.n_panels - 1) / p.n_panels, 16);
+  p.lrows = p.n_panels * p.panel;
+  return p;
+}
+
+int pack_points(db200_context* ctx, const float* X, int ldx, int layout, int n, int d, int dp, int npad, void* xp,
+                float* norms) {
+  const long long sp = (layout == DB200_POINT_MAJOR) ? ldx : 1;
+  const long long sf = (layout == DB200_POINT_MAJOR) ? 1 : ldx;
+  const int threads = 256;
+  long long blocks = ((long long)npad * 32 + threads - 1) / threads;
+  if (blocks > 65535LL * 4) blocks = 65535LL * 4;
+  pack_points_kernel<<<(unsigned)blocks, threads, 0, ctx->stream>>>(X, sp, sf, n, d, dp, npad,
+                                                                    static_cast<__nv_bfloat16*>(xp), norms);
+  DB200_CUDA(ctx, cudaGetLastError());
+  return DB200_OK;
+}
+
+int pack_sketch(db200_context* ctx, const float* Omega, int ldo, const float* yj, int n, int l, int njpad, int lrows,
+                void* op) {
+  const long long total = (long long)njpad * lrows;
+  long long blocks = (total + 255) / 256;
+  if (blocks > (long long)ctx->num_sms * 32) blocks = (long long)ctx->num_sms * 32;
+  pack_sketch_kernel<<<(unsigned)blocks, 256, 0, ctx->stream>>>(Omega, ldo, yj, n, l, njpad, lrows,
+                                                                static_cast<__nv_bfloat16*>(op));
+  DB200_CUDA(ctx, cudaGetLastError());
+  return DB200_OK;
+}
+
+int launch_rbf_tiles(db200_context* ctx, int mode, const PackedPoints& pi, const PackedPoints& pj, const float* yi,
+                     const float* yj, const void* op, const SketchPlan& plan, int l, float gamma, float* out,
+                     int ldo) {
+  if (pi.dp != pj.dp || pi.dp > 128) return fail(ctx, DB200_ERR_UNSUPPORTED, "rbf tiles: feature count > 128");
+  if (pi.npad % BM || pj.npad % BN) return fail(ctx, DB200_ERR_INVALID, "rbf tiles: unpadded operands");
+  if (mode == RBF_MODE_SKETCH && (plan.panel % 16 || plan.panel > 256 || plan.panel < 16))
+    return fail(ctx, DB200_ERR_INVALID, "rbf tiles: bad sketch panel");
+  CUtensorMap tm_xi, tm_xj, tm_om;
+  const int kp = 2 * pi.dp;
+  if (!make_tmap(&tm_xi, pi.xp, kp, pi.npad, kp, BM) || !make_tmap(&tm_xj, pj.xp, kp, pj.npad, kp, BN))
+    return fail(ctx, DB200_ERR_CUDA, "cuTensorMapEncodeTiled failed for the point operands");
+  if (mode == RBF_MODE_SKETCH) {
+    if (!make_tmap(&tm_om, op, pj.npad, plan.lrows, pj.npad, plan.panel))
+      return fail(ctx, DB200_ERR_CUDA, "cuTensorMapEncodeTiled failed for the sketch operand");
+  } else {
+    tm_om = tm_xj;  // unused
+  }
+  TileArgs a;
+  a.m = pi.n;
+  a.n = pj.n;
+  a.dp = pi.dp;
+  a.n_itiles = pi.npad / BM;
+  a.n_jtiles = pj.npad / BN;
+  a.n_panels = (mode == RBF_MODE_SKETCH) ? plan.n_panels : 1;
+  a.panel = (mode == RBF_MODE_SKETCH) ? plan.panel : 16;
+  a.l = l;
+  a.c_row = -gamma * LOG2E;
+  a.c_dot = 2.0f * gamma * LOG2E;
+  a.si = pi.norms;
+  a.sj = pj.norms;
+  a.yi = yi;
+  a.yj = yj;
+  a.out = out;
+  a.ldo = ldo;
+  a.status = ctx->d_status;
+  const SmemLayout L = make_layout(a.dp, a.panel, mode);
+  const size_t smem = L.total + 1024;
+  const int n_items = a.n_itiles * a.n_panels;
+  const int grid = n_items < ctx->num_sms ? n_items : ctx->num_sms;
+  if (mode == RBF_MODE_SKETCH) {
+    DB200_CUDA(ctx, cudaFuncSetAttribute(rbf_tile_kernel<RBF_MODE_SKETCH>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    rbf_tile_kernel<RBF_MODE_SKETCH><<<grid, NUM_THREADS, smem, ctx->stream>>>(tm_xi, tm_xj, tm_om, a);
+  } else {
+    DB200_CUDA(ctx, cudaFuncSetAttribute(rbf_tile_kernel<RBF_MODE_KBLOCK>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    rbf_tile_kernel<RBF_MODE_KBLOCK><<<grid, NUM_THREADS, smem, ctx->stream>>>(tm_xi, tm_xj, tm_om, a);
+  }
+  DB200_CUDA(ctx, cudaGetLastError());
+  return DB200_OK;
+}
+
+}  // namespace db200

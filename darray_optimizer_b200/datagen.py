@@ -1,0 +1,95 @@
+"""Seeded synthetic workloads (Philox counter-based generator) standing in for the LIBSVM datasets the
+reference's run scripts use (covtype, ijcnn1, SUSY, HIGGS; tests/README.md:31-143), which are not available.
+
+Points are returned point-major (n x d float32, row i = point i), which is the byte layout of the reference's
+DMatrix X (d x n column major, tests/testsvm.cpp:76).  Labels are +-1 float32 (read_input.h:20-22 maps every
+label to +-1).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+
+def rng(seed: int) -> np.random.Generator:
+    return np.random.Generator(np.random.Philox(seed))
+
+
+@dataclass
+class Workload:
+    name: str
+    X: np.ndarray            # n x d float32, point-major
+    y: np.ndarray            # n float32 in {-1, +1}
+    gamma: float
+    rank: int                # target rank r
+    oversample: int          # p; sketch width l = r + p
+    power_iters: int         # q
+    C: float                 # box constraint
+    seed: int
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def n(self) -> int:
+        return self.X.shape[0]
+
+    @property
+    def d(self) -> int:
+        return self.X.shape[1]
+
+    @property
+    def l(self) -> int:
+        return self.rank + self.oversample
+
+    def omega(self, seed_offset: int = 7919) -> np.ndarray:
+        """Gaussian test matrix Omega (n x l, float32, Fortran/column-major order like DMatrix O)."""
+        g = rng(self.seed + seed_offset)
+        return np.asfortranarray(g.standard_normal((self.n, self.l), dtype=np.float32))
+
+
+def two_gaussians(n: int = 4096, d: int = 32, seed: int = 1) -> Workload:
+    """Config 1: two isotropic Gaussians N(+-0.5*1, I), labels by component; gamma = 1/d, r = 128 + 10, q = 1,
+    C = 1."""
+    g = rng(seed)
+    y = np.where(g.random(n) < 0.5, 1.0, -1.0).astype(np.float32)
+    X = (g.standard_normal((n, d)) + 0.5 * y[:, None]).astype(np.float32)
+    return Workload("two_gaussians", X, y, 1.0 / d, 128, 10, 1, 1.0, seed)
+
+
+def uniform_hyperplane(n: int = 131072, d: int = 128, seed: int = 2, flip: float = 0.05) -> Workload:
+    """Config 2: x ~ U[0,1)^d float32; y = sign(w.(x - mean)) for a seeded w, 5% of labels flipped;
+    gamma = 0.5/d, r = 512 + 16, q = 1, C = 10."""
+    g = rng(seed)
+    X = g.random((n, d), dtype=np.float32)
+    w = g.standard_normal(d)
+    s = (X.astype(np.float64) - X.mean(axis=0, dtype=np.float64)) @ w
+    y = np.where(s >= 0, 1.0, -1.0)
+    flips = g.random(n) < flip
+    y[flips] = -y[flips]
+    return Workload("uniform_hyperplane", X, y.astype(np.float32), 0.5 / d, 512, 16, 1, 10.0, seed)
+
+
+def sparse_binary(n: int = 262144, d: int = 123, seed: int = 3, p: float = 0.11) -> Workload:
+    """Config 3: x_k ~ Bernoulli(0.11) in {0,1}; y = sign(w.x + b + eps), w ~ N(0,1) on a random 20% of the
+    coordinates (0 elsewhere), eps ~ N(0, 0.5), b = -mean(w.x) so both classes appear; gamma = 0.05,
+    r = 1024 + 16, C = 1."""
+    g = rng(seed)
+    X = (g.random((n, d)) < p).astype(np.float32)
+    w = np.zeros(d)
+    idx = g.choice(d, size=max(1, int(round(0.2 * d))), replace=False)
+    w[idx] = g.standard_normal(idx.size)
+    s = X.astype(np.float64) @ w
+    b = -s.mean()
+    y = np.where(s + b + g.normal(0.0, 0.5, n) >= 0, 1.0, -1.0).astype(np.float32)
+    return Workload("sparse_binary", X, y, 0.05, 1024, 16, 1, 1.0, seed, meta={"b": b})
+
+
+CONFIGS = {
+    "c1": two_gaussians,
+    "c2": uniform_hyperplane,
+    "c3": sparse_binary,
+}
+
+
+def make(name: str, **kw) -> Workload:
+    return CONFIGS[name](**kw)

@@ -1,0 +1,93 @@
+/*
+ * darray_b200.h -- C ABI of libdarray_b200.so, the B200 (sm_100a) implementation of DArray's
+ * kernel-SVM hot path (rushah05/DArray_Optimizer).
+ *
+ * Conventions
+ *   - Every function returns an int status (DB200_OK == 0, negative on error); the message of the last
+ *     error is available from db200_last_error().
+ *   - Matrices are column-major with an explicit leading dimension, as in the reference's LMatrix/DMatrix.
+ *   - "Device" entry points take device pointers and are stream-ordered on the context's stream; they do
+ *     not synchronize.  db200_synchronize() waits and also reports errors raised inside kernels (a bounded
+ *     device-side wait that gave up reports DB200_ERR_TIMEOUT).
+ *   - No torch or C++ types cross this boundary.
+ */
+#ifndef DARRAY_B200_H
+#define DARRAY_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define DB200_API __attribute__((visibility("default")))
+#else
+#define DB200_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DB200_OK 0
+#define DB200_ERR_INVALID (-1)     /* bad argument (size, pointer, leading dimension) */
+#define DB200_ERR_CUDA (-2)        /* CUDA runtime/driver error */
+#define DB200_ERR_NOT_SPD (-3)     /* Cholesky met a non-positive pivot */
+#define DB200_ERR_MAXITER (-4)     /* an iteration cap was reached */
+#define DB200_ERR_INFEASIBLE (-5)  /* barrier iterate left the box 0 < a < C */
+#define DB200_ERR_TIMEOUT (-6)     /* a bounded device-side wait gave up */
+#define DB200_ERR_NOMEM (-7)       /* device allocation failed */
+#define DB200_ERR_UNSUPPORTED (-8) /* shape outside what the kernels implement */
+
+/* Layout of a point matrix X holding n points of d features. */
+#define DB200_POINT_MAJOR 0   /* x(i,k) = X[k + i*ldx]  (the reference's DMatrix X, d x n column major) */
+#define DB200_FEATURE_MAJOR 1 /* x(i,k) = X[i + k*ldx]  (rbf_kernel's Xi/Xj, m x d column major) */
+
+typedef struct db200_context db200_context;
+
+/* Create a context on `device`.  `stream` is a cudaStream_t (NULL: the context creates its own stream).
+ * Replaces cuda_init() (include/dkernel.cu:28), whose handles were process globals. */
+DB200_API int db200_create(db200_context** ctx, int device, void* stream);
+
+/* Release the context and its device workspace.  Replaces cuda_finalize() (include/dkernel.cu:38). */
+DB200_API int db200_destroy(db200_context* ctx);
+
+/* Message of the last error on this context ("" if none). */
+DB200_API const char* db200_last_error(const db200_context* ctx);
+
+/* Wait for all work queued on the context's stream; returns the first device-side error if any. */
+DB200_API int db200_synchronize(db200_context* ctx);
+
+/* The context's stream as a cudaStream_t. */
+DB200_API void* db200_stream(const db200_context* ctx);
+
+/* Number of tcgen05 tile kernels launched on this context since creation (for launch accounting). */
+DB200_API int64_t db200_launch_count(const db200_context* ctx);
+
+/*
+ * Fused RBF kernel x sketch (device pointers):
+ *     Y(m x l) = diag(yi) * K(Xi, Xj) * diag(yj) * Omega,   K(a,b) = exp(-gamma * ||x_a - x_b||^2)
+ * The kernel block K is never stored: squared distances come from split-bf16 tensor-core products
+ * (||x||^2 + ||y||^2 - 2 x.y), exp is applied in the epilogue and the bf16 tile feeds the sketch product,
+ * accumulated in fp32.  Replaces rbf_kernel (include/dkernel.cu:132) followed by tc_gemm
+ * (include/dkernel.cu:194) inside DArray::LRA (include/dkernel.h:13-46), for the whole n x n matrix.
+ *   Xi, Xj : points in `x_layout` (DB200_POINT_MAJOR or DB200_FEATURE_MAJOR) with leading dims ldxi/ldxj
+ *   yi, yj : labels of length m and n (NULL means all ones)
+ *   Omega  : n x l column major (ldo >= n);  Y : m x l column major (ldy >= m)
+ * Supports d <= 128.
+ */
+DB200_API int db200_rbf_sketch(db200_context* ctx, int m, int n, int d, int l, const float* Xi, int ldxi, const float* Xj,
+                     int ldxj, int x_layout, const float* yi, const float* yj, const float* Omega, int ldo, float* Y,
+                     int ldy, float gamma);
+
+/*
+ * Materialised RBF block (device pointers):  K(m x n) = diag(yi) * exp(-gamma * D2(Xi, Xj)) * diag(yj),
+ * column major with leading dimension ldk.  Same arithmetic as db200_rbf_sketch's epilogue, in fp32.
+ * Replaces rbf_kernel (include/dkernel.cu:132-190, kernels vecnorm :102 and rbf :116) on device memory.
+ */
+DB200_API int db200_rbf_block(db200_context* ctx, int m, int n, int d, const float* Xi, int ldxi, const float* Xj, int ldxj,
+                    int x_layout, const float* yi, const float* yj, float* K, int ldk, float gamma);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DARRAY_B200_H */

@@ -1,0 +1,113 @@
+"""Parity of the tcgen05 RBF tile engine (through the C ABI) against the FP64 oracle.
+
+Tolerances (stated here, checked below):
+  * db200_rbf_block: |K_gpu - K_oracle| <= 2e-5 elementwise.  Distances come from split-bf16 products
+    (relative error ~2^-16 of |x||y|), exp2 and norms in fp32.
+  * db200_rbf_sketch: ||Y_gpu - Y_oracle||_F <= 1e-2 ||Y_oracle||_F.  The kernel tile P and Omega enter the
+    sketch product as bf16 (relative rounding 2^-9 each) with fp32 accumulation.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from util import colmajor_empty, colmajor_host, dev, ptr, rel_fro
+
+pytestmark = pytest.mark.gpu
+
+POINT_MAJOR, FEATURE_MAJOR = 0, 1
+
+
+def _points(n, d, seed, scale=1.0):
+    g = np.random.default_rng(seed)
+    return (scale * g.standard_normal((n, d))).astype(np.float32)
+
+
+def _labels(n, seed):
+    g = np.random.default_rng(seed + 100)
+    return np.where(g.random(n) < 0.5, 1.0, -1.0).astype(np.float32)
+
+
+@pytest.mark.parametrize("m,n,d,layout", [
+    (128, 128, 32, POINT_MAJOR),
+    (300, 257, 20, POINT_MAJOR),
+    (1000, 1000, 128, POINT_MAJOR),
+    (77, 390, 64, FEATURE_MAJOR),
+    (1, 5, 3, POINT_MAJOR),
+])
+def test_rbf_block_matches_oracle(gpu_ctx, m, n, d, layout):
+    Xi, Xj = _points(m, d, 1), _points(n, d, 2)
+    yi, yj = _labels(m, 1), _labels(n, 2)
+    gamma = 0.7 / d
+    Kref = O.rbf_block(Xi, Xj, yi, yj, gamma)
+    if layout == POINT_MAJOR:
+        dXi, dXj, ldxi, ldxj = dev(Xi), dev(Xj), d, d
+    else:  # m x d column major: store X^T row-major
+        dXi, dXj, ldxi, ldxj = dev(np.asfortranarray(Xi)), dev(np.asfortranarray(Xj)), m, n
+    ldk = m + 3
+    K = colmajor_empty(m, n, ldk)
+    gpu_ctx.rbf_block(m, n, d, ptr(dXi), ldxi, ptr(dXj), ldxj, layout, ptr(dev(yi)), ptr(dev(yj)), ptr(K), ldk,
+                      gamma)
+    gpu_ctx.sync()
+    Kg = colmajor_host(K, m)
+    assert np.max(np.abs(Kg - Kref)) <= 2e-5
+
+
+def test_rbf_block_symmetric_unit_diagonal(gpu_ctx):
+    n, d = 512, 48
+    X = _points(n, d, 5, scale=0.3)
+    dX = dev(X)
+    K = colmajor_empty(n, n)
+    gpu_ctx.rbf_block(n, n, d, ptr(dX), d, ptr(dX), d, POINT_MAJOR, 0, 0, ptr(K), n, 1.0 / d)
+    gpu_ctx.sync()
+    Kg = colmajor_host(K, n)
+    assert np.allclose(np.diag(Kg), 1.0, atol=1e-5)
+    assert np.max(np.abs(Kg - Kg.T)) <= 1e-5
+    assert Kg.min() > 0 and Kg.max() <= 1.0 + 1e-6
+
+
+@pytest.mark.parametrize("m,n,d,l", [
+    (256, 256, 32, 16),
+    (1000, 1000, 20, 40),
+    (300, 777, 128, 200),
+    (512, 512, 64, 528),
+    (130, 4096, 32, 138),
+])
+def test_rbf_sketch_matches_oracle(gpu_ctx, m, n, d, l):
+    Xi = _points(m, d, 11, 0.5)
+    Xj = Xi if m == n else _points(n, d, 12, 0.5)
+    yi = _labels(m, 3)
+    yj = yi if m == n else _labels(n, 4)
+    g = np.random.default_rng(9)
+    Om = np.asfortranarray(g.standard_normal((n, l)).astype(np.float32))
+    gamma = 1.0 / d
+    Yref = O.sketch(Xi, Xj, yi, yj, Om, gamma)
+    dXi = dev(Xi)
+    dXj = dXi if Xj is Xi else dev(Xj)
+    dyi = dev(yi)
+    dyj = dyi if yj is yi else dev(yj)
+    ldy = m + 1
+    Y = colmajor_empty(m, l, ldy)
+    gpu_ctx.rbf_sketch(m, n, d, l, ptr(dXi), d, ptr(dXj), d, POINT_MAJOR, ptr(dyi), ptr(dyj), ptr(dev(Om)), n,
+                       ptr(Y), ldy, gamma)
+    gpu_ctx.sync()
+    Yg = colmajor_host(Y, m)
+    assert rel_fro(Yg, Yref) <= 1e-2
+    # every column individually, so a dropped panel cannot hide behind the global norm
+    col_err = np.linalg.norm(Yg - Yref, axis=0) / np.maximum(np.linalg.norm(Yref, axis=0), 1e-30)
+    assert col_err.max() <= 3e-2
+
+
+def test_rbf_sketch_two_calls_reuse_workspace(gpu_ctx):
+    n, d, l = 640, 16, 24
+    X = _points(n, d, 21)
+    y = _labels(n, 21)
+    Om = np.asfortranarray(np.random.default_rng(3).standard_normal((n, l)).astype(np.float32))
+    dX, dy, dO = dev(X), dev(y), dev(Om)
+    outs = []
+    for _ in range(2):
+        Y = colmajor_empty(n, l)
+        gpu_ctx.rbf_sketch(n, n, d, l, ptr(dX), d, ptr(dX), d, POINT_MAJOR, ptr(dy), ptr(dy), ptr(dO), n, ptr(Y), n,
+                           0.1)
+        gpu_ctx.sync()
+        outs.append(colmajor_host(Y, n))
+    assert np.array_equal(outs[0], outs[1])  # deterministic: same tiles, same order
