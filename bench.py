@@ -1,0 +1,317 @@
+#!/usr/bin/env python
+"""Benchmark of the kernel-SVM hot path on B200: one step = one fused RBF-kernel x sketch pass Y = K.Omega
+(DArray::LRA, include/dkernel.h:13-46) over the whole n x n kernel at the precision-form workload
+(n = 131072 points, d = 128 features, sketch width l = 512 + 16, gamma = 0.5/d).
+
+Metric: K.Omega throughput in TFLOP/s with the algorithmic count F = 2 n^2 (d + l) per pass (distance Gram plus
+sketch product; the split-bf16 extra products are not counted).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs N independent replicas (one per GPU, launched by torchrun); the path has no exchange step, so the
+whole-job value is the sum of the replicas' work over the slowest replica's time ("scaling": "weak").
+--impl reference times the FP64 CPU restatement of the same pass (the reference has no CPU implementation of
+K.Omega; its rbf_kernel/tc_gemm run on the GPU with host round trips) on a bounded row sample on all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "K.Omega sketch TFLOP/s (F = 2 n^2 (d+l) per pass), SVM hot path"
+UNIT = "TFLOP/s"
+N_POINTS, D_FEAT, RANK, OVERSAMPLE = 131072, 128, 512, 16
+L_SKETCH = RANK + OVERSAMPLE
+
+
+def flops(n, d, l):
+    return 2.0 * n * n * (d + l)
+
+
+def config(extra=None):
+    c = {"workload": f"C2 fused RBF x sketch pass (uniform [0,1)^{D_FEAT}, hyperplane labels, 5% flipped)",
+         "n": N_POINTS, "d": D_FEAT, "l": L_SKETCH, "gamma": 0.5 / D_FEAT,
+         "l2": "inputs larger than L2 (X 67 MB + Omega 277 MB fp32, packed 67 + 138 MB bf16, Y 277 MB)"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+# ------------------------------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["active", "hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for name, val in zip(names[1:], parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------------------------------ distributed plumbing
+def dist_init(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def all_max(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ------------------------------------------------------------------------------------------ CPU baseline
+def cpu_sample(w, Om, rows: int, seconds: float):
+    """FP64 oracle (tests-only restatement of the reference's pass) on `rows` rows of Y = K Omega, repeated
+    until `seconds` elapsed; returns (TFLOP/s, sample description, threads)."""
+    from oracle import oracle as O
+    g = np.random.default_rng(5)
+    n = w.n
+    t0 = time.perf_counter()
+    done = 0
+    reps = 0
+    while True:
+        r0 = int(g.integers(0, n - rows))
+        O.sketch(w.X[r0:r0 + rows], w.X, w.y[r0:r0 + rows], w.y, Om, w.gamma, block=rows)
+        done += rows
+        reps += 1
+        el = time.perf_counter() - t0
+        if el >= seconds:
+            break
+    tf = flops(n, w.d, w.l) * done / n / el / 1e12
+    try:
+        from threadpoolctl import threadpool_info
+        threads = max((i.get("num_threads", 1) for i in threadpool_info()), default=os.cpu_count())
+    except Exception:
+        threads = os.cpu_count()
+    desc = (f"{reps} x {rows} rows of Y = K.Omega against all {n} points (FP64 numpy/OpenBLAS oracle), "
+            f"{el:.1f} s; throughput scaled by the algorithmic flop count")
+    return tf, desc, threads
+
+
+def run_reference(args):
+    world, rank, _ = dist_init(args.gpus)
+    if rank != 0:
+        return 0
+    from darray_optimizer_b200 import datagen
+    w = datagen.uniform_hyperplane(n=N_POINTS, d=D_FEAT)
+    Om = w.omega()
+    rows = 256
+    vals = []
+    cpu_sample(w, Om, 64, 0.5)  # warm-up (thread pool, page-in)
+    for _ in range(max(args.warmup - 1, 0)):
+        cpu_sample(w, Om, rows, 0.1)
+    t0 = time.perf_counter()
+    desc = threads = None
+    for _ in range(args.steps):
+        v, desc, threads = cpu_sample(w, Om, rows, 2.0)
+        vals.append(v)
+    el = time.perf_counter() - t0
+    value = statistics.median(vals)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded Philox)", "config": config(),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------------------------------ our arm
+def run_ours(args):
+    import torch
+    world, rank, local = dist_init(args.gpus)
+    torch.cuda.set_device(local)
+    from darray_optimizer_b200 import datagen
+    from darray_optimizer_b200._lib import Context
+
+    w = datagen.uniform_hyperplane(n=N_POINTS, d=D_FEAT, seed=2 + rank)
+    n, d, l = w.n, w.d, w.l
+    Om = w.omega()
+    stream = torch.cuda.current_stream()
+    ctx = Context(local, stream.cuda_stream)
+    X = torch.from_numpy(w.X).cuda()
+    y = torch.from_numpy(w.y).cuda()
+    O = torch.from_numpy(np.ascontiguousarray(Om.T)).cuda()   # n x l column major
+    Y = torch.empty((l, n), dtype=torch.float32, device="cuda")
+
+    def step():
+        ctx.rbf_sketch(n, n, d, l, X.data_ptr(), d, X.data_ptr(), d, 0, y.data_ptr(), y.data_ptr(), O.data_ptr(), n,
+                       Y.data_ptr(), n, w.gamma)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    ctx.sync()
+
+    # device-resident timed region
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    barrier(world)
+    torch.cuda.synchronize()
+    launches0 = ctx.launches()
+    ctx.profile(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    ctx.sync()
+    torch.cuda.synchronize()
+    kernel_ms, kernel_count = ctx.profile_read()
+    ctx.profile(False)
+    barrier(world)
+    clocks = sampler.stop()
+    launches = ctx.launches() - launches0
+    ms = e0.elapsed_time(e1)
+    ms_max = all_max(ms, world)
+    F = flops(n, d, l)
+    value = world * F * args.steps / (ms_max / 1e3) / 1e12
+
+    # end to end through the host-pointer LRA entry point (pinned host buffers, copies inside the timed region)
+    Xh = torch.from_numpy(w.X).pin_memory()
+    yh = torch.from_numpy(w.y).pin_memory()
+    Oh = torch.from_numpy(np.ascontiguousarray(Om.T)).pin_memory()
+    Ah = torch.empty((l, n), dtype=torch.float32).pin_memory()
+
+    def e2e_step():
+        ctx.lra_host(n, d, l, Xh.data_ptr(), d, yh.data_ptr(), Oh.data_ptr(), n, Ah.data_ptr(), n, w.gamma)
+
+    e2e_step()
+    barrier(world)
+    t0 = time.perf_counter()
+    k2 = max(1, args.steps)
+    for _ in range(k2):
+        e2e_step()
+    e2e_s = all_max(time.perf_counter() - t0, world)
+    e2e_val = world * F * k2 / e2e_s / 1e12
+    h2d = Xh.numel() * 4 + yh.numel() * 4 + Oh.numel() * 4
+    d2h = Ah.numel() * 4
+
+    # roofline of the dominant kernel (tcgen05 tile kernel), timed live with events on its stream
+    peaks = {}
+    pk = ROOT / "MEASURED_PEAKS.json"
+    if pk.exists():
+        peaks = json.loads(pk.read_text())
+    peak = float(peaks.get("bf16_tflops", 1590.0))
+    per_launch_ms = kernel_ms / max(kernel_count, 1)
+    achieved = F / (per_launch_ms / 1e3) / 1e12
+    roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+            "traffic": None, "kernel": "rbf_tile_kernel<SKETCH>", "kernel_ms": per_launch_ms,
+            "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)" if pk.exists() else "fallback 1590"}
+    traffic_file = ROOT / "profiles" / "rbf_sketch_traffic.json"
+    if traffic_file.exists():
+        try:
+            roof["traffic"] = json.loads(traffic_file.read_text()).get("bytes_per_launch")
+        except Exception:
+            pass
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "bf16", "data": "synthetic (seeded Philox)",
+            "config": config({"parallelism": f"replicas x{world}"}), "clocks": clocks,
+            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches, "roofline": roof}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, desc, threads = cpu_sample(w, Om, 256, args.cpu_seconds)
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

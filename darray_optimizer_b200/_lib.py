@@ -30,6 +30,9 @@ SIGNATURES = {
                                   _vp, _c_int, _vp, _c_int, _c_float]),
     "db200_rbf_block": (_c_int, [_vp, _c_int, _c_int, _c_int, _vp, _c_int, _vp, _c_int, _c_int, _vp, _vp, _vp,
                                  _c_int, _c_float]),
+    "db200_profile": (_c_int, [_vp, _c_int]),
+    "db200_profile_read": (_c_int, [_vp, ctypes.POINTER(_c_double), ctypes.POINTER(_i64)]),
+    "db200_lra_host": (_c_int, [_vp, _c_int, _c_int, _c_int, _vp, _c_int, _vp, _vp, _c_int, _vp, _c_int, _c_float]),
 }
 
 STATUS = {
@@ -118,6 +121,17 @@ class Context:
     def rbf_sketch(self, m, n, d, l, Xi, ldxi, Xj, ldxj, layout, yi, yj, Om, ldo, Y, ldy, gamma):
         return self.check(self.lib.db200_rbf_sketch(self.h, m, n, d, l, Xi, ldxi, Xj, ldxj, layout, yi, yj, Om,
                                                     ldo, Y, ldy, gamma))
+
+    def profile(self, enable: bool):
+        return self.check(self.lib.db200_profile(self.h, 1 if enable else 0))
+
+    def profile_read(self):
+        ms, cnt = _c_double(), _i64()
+        self.check(self.lib.db200_profile_read(self.h, ctypes.byref(ms), ctypes.byref(cnt)))
+        return ms.value, cnt.value
+
+    def lra_host(self, n, d, k, X, ldx, Y, O, ldo, A, lda, gamma):
+        return self.check(self.lib.db200_lra_host(self.h, n, d, k, X, ldx, Y, O, ldo, A, lda, gamma))
 
     def rbf_block(self, m, n, d, Xi, ldxi, Xj, ldxj, layout, yi, yj, K, ldk, gamma):
         return self.check(self.lib.db200_rbf_block(self.h, m, n, d, Xi, ldxi, Xj, ldxj, layout, yi, yj, K, ldk,

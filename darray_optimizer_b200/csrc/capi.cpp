@@ -8,8 +8,6 @@
 
 namespace db200 {
 
-static std::atomic<long long> g_tile_launches{0};
-
 int fail(db200_context* ctx, int status, const std::string& msg) {
   if (ctx) ctx->last_error = msg;
   return status;
@@ -38,7 +36,44 @@ void* workspace(db200_context* ctx, size_t bytes) {
   return ctx->ws;
 }
 
-void count_tile_launch() { g_tile_launches.fetch_add(1); }
+void prof_begin(db200_context* ctx, cudaEvent_t* e0) {
+  *e0 = nullptr;
+  if (!ctx->profiling) return;
+  if (cudaEventCreate(e0) != cudaSuccess || cudaEventRecord(*e0, ctx->stream) != cudaSuccess) *e0 = nullptr;
+}
+
+void prof_end(db200_context* ctx, cudaEvent_t e0) {
+  if (!ctx->profiling || !e0) return;
+  cudaEvent_t e1;
+  if (cudaEventCreate(&e1) != cudaSuccess) return;
+  cudaEventRecord(e1, ctx->stream);
+  ctx->prof_events.emplace_back(e0, e1);
+}
+
+static void prof_clear(db200_context* ctx) {
+  for (auto& p : ctx->prof_events) {
+    cudaEventDestroy(p.first);
+    cudaEventDestroy(p.second);
+  }
+  ctx->prof_events.clear();
+}
+
+void* io_buffer(db200_context* ctx, size_t bytes) {
+  if (bytes <= ctx->io_size) return ctx->io;
+  cudaStreamSynchronize(ctx->stream);
+  if (ctx->io) cudaFree(ctx->io);
+  ctx->io = nullptr;
+  ctx->io_size = 0;
+  size_t want = align_up(bytes, 1 << 20);
+  cudaError_t e = cudaMalloc(&ctx->io, want);
+  if (e != cudaSuccess) {
+    ctx->io = nullptr;
+    cuda_fail(ctx, e, "cudaMalloc(io buffer)");
+    return nullptr;
+  }
+  ctx->io_size = want;
+  return ctx->io;
+}
 
 }  // namespace db200
 
@@ -69,14 +104,14 @@ int db200_create(db200_context** out, int device, void* stream) {
     return DB200_ERR_UNSUPPORTED;
   }
   ctx->num_sms = prop.multiProcessorCount;
-  if (stream) {
-    ctx->stream = static_cast<cudaStream_t>(stream);
-  } else {
+  if (stream == DB200_OWN_STREAM) {
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
       delete ctx;
       return DB200_ERR_CUDA;
     }
     ctx->own_stream = true;
+  } else {
+    ctx->stream = static_cast<cudaStream_t>(stream);  // NULL: the CUDA default stream
   }
   if (cudaMalloc(&ctx->d_status, sizeof(int)) != cudaSuccess ||
       cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream) != cudaSuccess ||
@@ -92,7 +127,9 @@ int db200_destroy(db200_context* ctx) {
   if (!ctx) return DB200_OK;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  prof_clear(ctx);
   if (ctx->ws) cudaFree(ctx->ws);
+  if (ctx->io) cudaFree(ctx->io);
   if (ctx->d_status) cudaFree(ctx->d_status);
   if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -104,7 +141,30 @@ const char* db200_last_error(const db200_context* ctx) { return ctx ? ctx->last_
 
 void* db200_stream(const db200_context* ctx) { return ctx ? static_cast<void*>(ctx->stream) : nullptr; }
 
-int64_t db200_launch_count(const db200_context*) { return (int64_t)g_tile_launches.load(); }
+int64_t db200_launch_count(const db200_context* ctx) { return ctx ? (int64_t)ctx->launches : 0; }
+
+int db200_profile(db200_context* ctx, int enable) {
+  if (!ctx) return DB200_ERR_INVALID;
+  DB200_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  prof_clear(ctx);
+  ctx->profiling = enable != 0;
+  return DB200_OK;
+}
+
+int db200_profile_read(db200_context* ctx, double* total_ms, int64_t* count) {
+  if (!ctx || !total_ms || !count) return DB200_ERR_INVALID;
+  DB200_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  double t = 0;
+  for (auto& p : ctx->prof_events) {
+    float ms = 0;
+    DB200_CUDA(ctx, cudaEventElapsedTime(&ms, p.first, p.second));
+    t += ms;
+  }
+  *total_ms = t;
+  *count = (int64_t)ctx->prof_events.size();
+  prof_clear(ctx);
+  return DB200_OK;
+}
 
 int db200_synchronize(db200_context* ctx) {
   if (!ctx) return DB200_ERR_INVALID;
@@ -191,9 +251,7 @@ int db200_rbf_sketch(db200_context* ctx, int m, int n, int d, int l, const float
   void* op = carve.take<uint16_t>((size_t)plan.lrows * npad);
   st = pack_sketch(ctx, Omega, ldo, yj, n, l, npad, plan.lrows, op);
   if (st) return st;
-  st = launch_rbf_tiles(ctx, RBF_MODE_SKETCH, pi, pj, yi, nullptr, op, plan, l, gamma, Y, ldy);
-  if (!st) count_tile_launch();
-  return st;
+  return launch_rbf_tiles(ctx, RBF_MODE_SKETCH, pi, pj, yi, nullptr, op, plan, l, gamma, Y, ldy);
 }
 
 int db200_rbf_block(db200_context* ctx, int m, int n, int d, const float* Xi, int ldxi, const float* Xj, int ldxj,
@@ -211,9 +269,33 @@ int db200_rbf_block(db200_context* ctx, int m, int n, int d, const float* Xi, in
   st = pack_pair(ctx, m, n, d, Xi, ldxi, Xj, ldxj, x_layout, 0, pi, pj, carve);
   if (st) return st;
   SketchPlan plan;
-  st = launch_rbf_tiles(ctx, RBF_MODE_KBLOCK, pi, pj, yi, yj, nullptr, plan, 0, gamma, K, ldk);
-  if (!st) count_tile_launch();
-  return st;
+  return launch_rbf_tiles(ctx, RBF_MODE_KBLOCK, pi, pj, yi, yj, nullptr, plan, 0, gamma, K, ldk);
+}
+
+int db200_lra_host(db200_context* ctx, int n, int d, int k, const float* X, int ldx, const float* Y,
+                   const float* O, int ldo, float* A, int lda, float gamma) {
+  if (!ctx) return DB200_ERR_INVALID;
+  if (n < 0 || d < 1 || k < 0 || !X || !Y || !O || !A || ldx < d || ldo < n || lda < n)
+    return fail(ctx, DB200_ERR_INVALID, "lra_host: bad arguments");
+  if (n == 0 || k == 0) return DB200_OK;
+  const size_t bx = align_up(sizeof(float) * (size_t)n * d, 256), by = align_up(sizeof(float) * (size_t)n, 256),
+               bo = align_up(sizeof(float) * (size_t)n * k, 256);
+  char* io = static_cast<char*>(io_buffer(ctx, bx + by + 2 * bo));
+  if (!io) return DB200_ERR_NOMEM;
+  float* dX = reinterpret_cast<float*>(io);
+  float* dY = reinterpret_cast<float*>(io + bx);
+  float* dO = reinterpret_cast<float*>(io + bx + by);
+  float* dA = reinterpret_cast<float*>(io + bx + by + bo);
+  DB200_CUDA(ctx, cudaMemcpy2DAsync(dX, sizeof(float) * d, X, sizeof(float) * ldx, sizeof(float) * d, n,
+                                    cudaMemcpyHostToDevice, ctx->stream));
+  DB200_CUDA(ctx, cudaMemcpyAsync(dY, Y, sizeof(float) * n, cudaMemcpyHostToDevice, ctx->stream));
+  DB200_CUDA(ctx, cudaMemcpy2DAsync(dO, sizeof(float) * n, O, sizeof(float) * ldo, sizeof(float) * n, k,
+                                    cudaMemcpyHostToDevice, ctx->stream));
+  int st = db200_rbf_sketch(ctx, n, n, d, k, dX, d, dX, d, DB200_POINT_MAJOR, dY, dY, dO, n, dA, n, gamma);
+  if (st) return st;
+  DB200_CUDA(ctx, cudaMemcpy2DAsync(A, sizeof(float) * lda, dA, sizeof(float) * n, sizeof(float) * n, k,
+                                    cudaMemcpyDeviceToHost, ctx->stream));
+  return db200_synchronize(ctx);
 }
 
 }  // extern "C"

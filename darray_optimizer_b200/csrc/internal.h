@@ -3,6 +3,8 @@
 #include <cstddef>
 #include <cstdint>
 #include <string>
+#include <utility>
+#include <vector>
 #include <cuda_runtime.h>
 
 #include "../../include/darray_b200.h"
@@ -15,8 +17,14 @@ struct db200_context {
   int* d_status = nullptr;       // device status word written by kernels whose bounded waits give up
   void* ws = nullptr;            // device workspace (packed operands, small factors)
   size_t ws_size = 0;
+  void* io = nullptr;            // device staging for the host-pointer entry points
+  size_t io_size = 0;
   double* h_pinned = nullptr;    // small pinned host staging area for scalar readbacks
   std::string last_error;
+  long long launches = 0;        // kernels launched through this context
+  // Optional per-launch timing of the tcgen05 tile kernels (CUDA events on the launching stream).
+  bool profiling = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
 };
 
 namespace db200 {
@@ -31,8 +39,14 @@ int cuda_fail(db200_context* ctx, cudaError_t err, const char* what);
     if (e_ != cudaSuccess) return ::db200::cuda_fail((ctx), e_, #call); \
   } while (0)
 
+// Launch accounting and optional event timing around the dominant (tile) kernels.
+inline void count_launch(db200_context* ctx, int k = 1) { ctx->launches += k; }
+void prof_begin(db200_context* ctx, cudaEvent_t* e0);
+void prof_end(db200_context* ctx, cudaEvent_t e0);
+
 // Grow-only workspace; returns nullptr on failure (ctx->last_error set).
 void* workspace(db200_context* ctx, size_t bytes);
+void* io_buffer(db200_context* ctx, size_t bytes);
 
 inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 inline int round_up(int x, int a) { return (x + a - 1) / a * a; }

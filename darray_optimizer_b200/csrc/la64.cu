@@ -1,0 +1,510 @@
+// FP64 dense linear algebra for the 1 x 1 DMatrix path: tall-skinny Gram (matrix_multiply T,N), tall GEMM,
+// blocked Cholesky (cholesky_factorize 'U'), triangular inverse / solves (triangular_solve), GEMV pairs.
+//
+// Restated from include/lapack_like.h:10-56 (blocked right-looking Cholesky: potrf on the diagonal block, trsm on
+// the panel, syrk on the trailing matrix), include/blas_like.h:63-127 (matrix_multiply T,N; triangular_solve
+// L,U,T,N) and include/cblas_like.h:40-69, in FP64 on the GPU.  All matrices are column major.
+#include <cstdio>
+
+#include "internal.h"
+#include "la64.h"
+
+namespace db200 {
+
+namespace {
+
+constexpr int TB = 64;  // output tile
+constexpr int TK = 16;  // k step
+
+template <typename T>
+__device__ __forceinline__ double ld64(const T* p) { return (double)__ldg(p); }
+
+// C[p x q] (+)= alpha * A^T diag(w) B over rows [r0, r1) of A (n x p) and B (n x q); FP64 accumulation.
+// grid.z splits the rows; partial tiles are added with FP64 atomics when grid.z > 1.
+template <typename TA, typename TBt>
+__global__ void __launch_bounds__(256) gram_kernel(int n, int p, int q, const TA* __restrict__ A, long long lda,
+                                                   const TBt* __restrict__ B, long long ldb,
+                                                   const double* __restrict__ w, double alpha, double* C, int ldc,
+                                                   int rows_per_split, int upper_only, int atomic) {
+  const int bi = blockIdx.x, bj = blockIdx.y;
+  if (upper_only && bi > bj) return;
+  const int i0 = bi * TB, j0 = bj * TB;
+  const int r0 = blockIdx.z * rows_per_split;
+  const int r1 = min(n, r0 + rows_per_split);
+  __shared__ double sA[TK][TB + 1];
+  __shared__ double sB[TK][TB + 1];
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+  for (int k0 = r0; k0 < r1; k0 += TK) {
+    // 256 threads load 16 x 64 of A and of B: thread -> (kk = t % 16, col = t / 16 + 16 * s)
+    const int kk = threadIdx.x % TK;
+    const int k = k0 + kk;
+    const double wk = (w && k < r1) ? w[k] : 1.0;
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      const int c = threadIdx.x / TK + 16 * s;
+      const int ia = i0 + c, jb = j0 + c;
+      sA[kk][c] = (k < r1 && ia < p) ? wk * ld64(A + (long long)ia * lda + k) : 0.0;
+      sB[kk][c] = (k < r1 && jb < q) ? ld64(B + (long long)jb * ldb + k) : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int t = 0; t < TK; ++t) {
+      double av[4], bv[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) av[a] = sA[t][ty * 4 + a];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) bv[b] = sB[t][tx * 4 + b];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const int i = i0 + ty * 4 + a;
+    if (i >= p) continue;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int j = j0 + tx * 4 + b;
+      if (j >= q) continue;
+      if (upper_only && i > j) continue;
+      double* dst = C + (long long)j * ldc + i;
+      if (atomic)
+        atomicAdd(dst, alpha * acc[a][b]);
+      else
+        *dst += alpha * acc[a][b];
+    }
+  }
+}
+
+// C[n x q] = A[n x p] * op(B) (+ beta * C);  op(B) = B (p x q) or B^T (B is q x p) when transB.
+template <typename TA, typename TC>
+__global__ void __launch_bounds__(256) gemm_nn_kernel(int n, int p, int q, const TA* __restrict__ A, long long lda,
+                                                      const double* __restrict__ B, int ldb, int transB,
+                                                      double beta, TC* C, long long ldc) {
+  const int i0 = blockIdx.x * TB, j0 = blockIdx.y * TB;
+  __shared__ double sA[TK][TB + 1];
+  __shared__ double sB[TK][TB + 1];
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+  for (int k0 = 0; k0 < p; k0 += TK) {
+    // A tile 64 rows x 16 k: consecutive threads -> consecutive rows (coalesced)
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      const int e = threadIdx.x + 256 * s;
+      const int r = e % TB, kk = e / TB;
+      const int i = i0 + r, k = k0 + kk;
+      sA[kk][r] = (i < n && k < p) ? ld64(A + (long long)k * lda + i) : 0.0;
+      const int jc = e % TB;
+      const int j = j0 + jc;
+      double bv = 0.0;
+      if (j < q && k < p) bv = transB ? B[(long long)k * ldb + j] : B[(long long)j * ldb + k];
+      sB[kk][jc] = bv;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int t = 0; t < TK; ++t) {
+      double av[4], bv[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) av[a] = sA[t][ty + 16 * a];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) bv[b] = sB[t][tx * 4 + b];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const int i = i0 + ty + 16 * a;
+    if (i >= n) continue;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int j = j0 + tx * 4 + b;
+      if (j >= q) continue;
+      TC* dst = C + (long long)j * ldc + i;
+      double v = acc[a][b];
+      if (beta != 0.0) v += beta * (double)*dst;
+      *dst = (TC)v;
+    }
+  }
+}
+
+// Unblocked upper Cholesky of one diagonal block (kb <= 64) held in shared memory.  status <- DB200_ERR_NOT_SPD
+// and *bad <- global pivot index on a non-positive (or NaN) pivot.
+__global__ void __launch_bounds__(256) potrf_diag_kernel(double* A, int lda, int k0, int kb, int* status,
+                                                         int* bad) {
+  __shared__ double s[64][65];
+  __shared__ int fail;
+  if (threadIdx.x == 0) fail = 0;
+  for (int e = threadIdx.x; e < kb * kb; e += blockDim.x) {
+    const int i = e % kb, j = e / kb;
+    s[i][j] = A[(long long)(k0 + j) * lda + k0 + i];
+  }
+  __syncthreads();
+  for (int k = 0; k < kb; ++k) {
+    if (threadIdx.x == 0) {
+      const double piv = s[k][k];
+      if (!(piv > 0.0)) {
+        fail = 1;
+      } else {
+        s[k][k] = sqrt(piv);
+      }
+    }
+    __syncthreads();
+    if (fail) break;
+    const double rkk = s[k][k];
+    for (int j = k + 1 + threadIdx.x; j < kb; j += blockDim.x) s[k][j] /= rkk;
+    __syncthreads();
+    // trailing update of the upper triangle: s[i][j] -= s[k][i] * s[k][j], k < i <= j
+    const int m = kb - k - 1;
+    for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
+      const int i = k + 1 + e % m, j = k + 1 + e / m;
+      if (i <= j) s[i][j] -= s[k][i] * s[k][j];
+    }
+    __syncthreads();
+  }
+  if (fail) {
+    if (threadIdx.x == 0) {
+      if (atomicCAS(status, 0, DB200_ERR_NOT_SPD) == 0) *bad = k0;
+    }
+    return;
+  }
+  for (int e = threadIdx.x; e < kb * kb; e += blockDim.x) {
+    const int i = e % kb, j = e / kb;
+    A[(long long)(k0 + j) * lda + k0 + i] = (i <= j) ? s[i][j] : 0.0;
+  }
+}
+
+// Panel solve A12 <- R11^-T A12 for the kb x (l - k0 - kb) panel right of the diagonal block: one thread per
+// column, forward substitution with R11^T (lower).
+__global__ void __launch_bounds__(128) potrf_panel_kernel(double* A, int lda, int k0, int kb, int l, const int* status) {
+  if (*status) return;
+  __shared__ double r[64][65];
+  for (int e = threadIdx.x; e < kb * kb; e += blockDim.x) {
+    const int i = e % kb, j = e / kb;
+    r[i][j] = A[(long long)(k0 + j) * lda + k0 + i];
+  }
+  __syncthreads();
+  const int col = k0 + kb + blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= l) return;
+  double* c = A + (long long)col * lda + k0;
+  double x[64];
+#pragma unroll 4
+  for (int i = 0; i < kb; ++i) {
+    double v = c[i];
+    for (int k = 0; k < i; ++k) v -= r[k][i] * x[k];
+    x[i] = v / r[i][i];
+  }
+  for (int i = 0; i < kb; ++i) c[i] = x[i];
+}
+
+// Zero the strictly lower triangle of an l x l matrix.
+__global__ void zero_lower_kernel(double* A, int lda, int l) {
+  const long long total = (long long)l * l;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e % l), j = (int)(e / l);
+    if (i > j) A[(long long)j * lda + i] = 0.0;
+  }
+}
+
+// X = R^-1 for upper triangular R (l x l): one warp per column j solves R x = e_j by column-oriented
+// back substitution.
+__global__ void trinv_upper_kernel(const double* R, int ldr, int l, double* X, int ldx) {
+  const int warps = blockDim.x / 32;
+  const int j = blockIdx.x * warps + threadIdx.x / 32;
+  const int lane = threadIdx.x % 32;
+  if (j >= l) return;
+  double* x = X + (long long)j * ldx;
+  for (int i = lane; i < l; i += 32) x[i] = (i == j) ? 1.0 : 0.0;
+  __syncwarp();
+  for (int i = j; i >= 0; --i) {
+    const double xi = x[i] / R[(long long)i * ldr + i];
+    __syncwarp();
+    if (lane == 0) x[i] = xi;
+    const double* ri = R + (long long)i * ldr;
+    for (int k = lane; k < i; k += 32) x[k] -= ri[k] * xi;
+    __syncwarp();
+  }
+}
+
+// Single-CTA triangular solves with an upper factor R (and its transpose L = R^T stored separately so every
+// inner product reads a contiguous column):
+//   mode 0: solve R^T y = b   (forward; row i of R^T = column i of R)
+//   mode 1: solve R x = y     (backward; row i of R = column i of L)
+// x/b in place, FP64.  Blocks of 32 rows: all warps form the off-block inner products, warp 0 solves the
+// 32 x 32 triangle.
+__global__ void __launch_bounds__(1024) trsv_kernel(const double* R, const double* L, int ld, int l, double* x,
+                                                    int mode) {
+  __shared__ double part[32];
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const int nb = (l + 31) / 32;
+  for (int bb = 0; bb < nb; ++bb) {
+    const int blk = (mode == 0) ? bb : nb - 1 - bb;
+    const int i0 = blk * 32;
+    const int i = i0 + warp;
+    // off-block contribution for row i
+    double s = 0.0;
+    if (i < l) {
+      if (mode == 0) {  // sum_{k < i0} R[k, i] x_k
+        const double* col = R + (long long)i * ld;
+        for (int k = lane; k < i0; k += 32) s += col[k] * x[k];
+      } else {  // sum_{k >= i0 + 32} R[i, k] x_k = sum L[k, i] x_k
+        const double* col = L + (long long)i * ld;
+        for (int k = i0 + 32 + lane; k < l; k += 32) s += col[k] * x[k];
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) part[warp] = s;
+    __syncthreads();
+    if (warp == 0) {
+      const int bl = min(32, l - i0);
+      double v = (lane < bl) ? x[i0 + lane] - part[lane] : 0.0;
+      // solve the bl x bl triangle, one row per step
+      if (mode == 0) {
+        for (int r = 0; r < bl; ++r) {
+          const double rr = R[(long long)(i0 + r) * ld + i0 + r];
+          const double xr = __shfl_sync(0xffffffffu, v, r) / rr;
+          if (lane == r) v = xr;
+          if (lane > r && lane < bl) v -= R[(long long)(i0 + lane) * ld + i0 + r] * xr;
+        }
+      } else {
+        for (int r = bl - 1; r >= 0; --r) {
+          const double rr = R[(long long)(i0 + r) * ld + i0 + r];
+          const double xr = __shfl_sync(0xffffffffu, v, r) / rr;
+          if (lane == r) v = xr;
+          if (lane < r) v -= R[(long long)(i0 + r) * ld + i0 + lane] * xr;
+        }
+      }
+      if (lane < bl) x[i0 + lane] = v;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void transpose_kernel(const double* A, int lda, int m, int n, double* B, int ldb) {
+  __shared__ double t[32][33];
+  const int bi = blockIdx.x * 32, bj = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int i = bi + threadIdx.x, j = bj + r;
+    if (i < m && j < n) t[r][threadIdx.x] = A[(long long)j * lda + i];
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int j = bj + threadIdx.x, i = bi + r;
+    if (i < m && j < n) B[(long long)i * ldb + j] = t[threadIdx.x][r];
+  }
+}
+
+__global__ void scale_kernel(double* C, int ldc, int m, int n, double beta, int upper_only) {
+  const long long total = (long long)m * n;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e % m), j = (int)(e / m);
+    if (upper_only && i > j) continue;
+    double* p = C + (long long)j * ldc + i;
+    *p = (beta == 0.0) ? 0.0 : beta * *p;
+  }
+}
+
+__global__ void symmetrize_kernel(double* C, int ldc, int l, double shift) {
+  // C <- (C + C^T)/2 + shift I, full matrix
+  const long long total = (long long)l * l;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e % l), j = (int)(e / l);
+    if (i > j) continue;
+    double* a = C + (long long)j * ldc + i;
+    double* b = C + (long long)i * ldc + j;
+    double v = 0.5 * (*a + *b);
+    if (i == j) v += shift;
+    *a = v;
+    *b = v;
+  }
+}
+
+__global__ void fill_upper_from_lower_kernel(double* C, int ldc, int l) {
+  const long long total = (long long)l * l;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e % l), j = (int)(e / l);
+    if (i > j) C[(long long)j * ldc + i] = C[(long long)i * ldc + j];
+  }
+}
+
+template <typename TS, typename TD>
+__global__ void convert_kernel(const TS* src, long long lds, TD* dst, long long ldd, int m, int n) {
+  const long long total = (long long)m * n;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e % m), j = (int)(e / m);
+    dst[j * ldd + i] = (TD)src[j * lds + i];
+  }
+}
+
+__global__ void trace_kernel(const double* C, int ldc, int l, double* out) {
+  double s = 0.0;
+  for (int i = threadIdx.x; i < l; i += blockDim.x) s += C[(long long)i * ldc + i];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  __shared__ double w[32];
+  if (threadIdx.x % 32 == 0) w[threadIdx.x / 32] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int k = 0; k < (int)(blockDim.x / 32); ++k) t += w[k];
+    *out = t;
+  }
+}
+
+inline unsigned grid_for(long long total, int threads, int cap) {
+  long long b = (total + threads - 1) / threads;
+  if (b < 1) b = 1;
+  if (b > cap) b = cap;
+  return (unsigned)b;
+}
+
+}  // namespace
+
+template <typename TA, typename TBt>
+int gram(db200_context* ctx, int n, int p, int q, const TA* A, long long lda, const TBt* B, long long ldb,
+         const double* w, double alpha, double beta, double* C, int ldc, bool upper_only) {
+  if (p <= 0 || q <= 0) return DB200_OK;
+  scale_kernel<<<grid_for((long long)p * q, 256, 4096), 256, 0, ctx->stream>>>(C, ldc, p, q, beta, upper_only ? 1 : 0);
+  count_launch(ctx);
+  if (n <= 0) return DB200_OK;
+  const int tp = (p + TB - 1) / TB, tq = (q + TB - 1) / TB;
+  const int tiles = upper_only ? (tp * (tp + 1)) / 2 : tp * tq;
+  int splits = (4 * ctx->num_sms + tiles - 1) / tiles;
+  int rows = (n + splits - 1) / splits;
+  rows = round_up(rows < TK ? TK : rows, TK);
+  splits = (n + rows - 1) / rows;
+  if (splits > 65535) return fail(ctx, DB200_ERR_UNSUPPORTED, "gram: too many row splits");
+  dim3 grid(tp, tq, splits);
+  gram_kernel<TA, TBt><<<grid, 256, 0, ctx->stream>>>(n, p, q, A, lda, B, ldb, w, alpha, C, ldc, rows,
+                                                     upper_only ? 1 : 0, splits > 1 ? 1 : 0);
+  DB200_CUDA(ctx, cudaGetLastError());
+  count_launch(ctx);
+  return DB200_OK;
+}
+
+template int gram<float, float>(db200_context*, int, int, int, const float*, long long, const float*, long long,
+                                const double*, double, double, double*, int, bool);
+template int gram<double, double>(db200_context*, int, int, int, const double*, long long, const double*, long long,
+                                  const double*, double, double, double*, int, bool);
+template int gram<double, float>(db200_context*, int, int, int, const double*, long long, const float*, long long,
+                                 const double*, double, double, double*, int, bool);
+
+template <typename TA, typename TC>
+int gemm_tall(db200_context* ctx, int n, int p, int q, const TA* A, long long lda, const double* B, int ldb,
+              bool transB, double beta, TC* C, long long ldc) {
+  if (n <= 0 || q <= 0) return DB200_OK;
+  dim3 grid((n + TB - 1) / TB, (q + TB - 1) / TB);
+  if (grid.y > 65535) return fail(ctx, DB200_ERR_UNSUPPORTED, "gemm_tall: q too large");
+  gemm_nn_kernel<TA, TC><<<grid, 256, 0, ctx->stream>>>(n, p, q, A, lda, B, ldb, transB ? 1 : 0, beta, C, ldc);
+  DB200_CUDA(ctx, cudaGetLastError());
+  count_launch(ctx);
+  return DB200_OK;
+}
+
+template int gemm_tall<float, double>(db200_context*, int, int, int, const float*, long long, const double*, int,
+                                      bool, double, double*, long long);
+template int gemm_tall<double, double>(db200_context*, int, int, int, const double*, long long, const double*, int,
+                                       bool, double, double*, long long);
+template int gemm_tall<double, float>(db200_context*, int, int, int, const double*, long long, const double*, int,
+                                      bool, double, float*, long long);
+template int gemm_tall<float, float>(db200_context*, int, int, int, const float*, long long, const double*, int,
+                                     bool, double, float*, long long);
+
+int potrf_upper(db200_context* ctx, double* A, int lda, int l, int* d_status, int* d_bad, int nb) {
+  if (nb < 1 || nb > 64) nb = 64;
+  for (int k0 = 0; k0 < l; k0 += nb) {
+    const int kb = (l - k0 < nb) ? l - k0 : nb;
+    potrf_diag_kernel<<<1, 256, 0, ctx->stream>>>(A, lda, k0, kb, d_status, d_bad);
+    count_launch(ctx);
+    const int rest = l - k0 - kb;
+    if (rest > 0) {
+      potrf_panel_kernel<<<(rest + 127) / 128, 128, 0, ctx->stream>>>(A, lda, k0, kb, l, d_status);
+      count_launch(ctx);
+      // trailing update A22 -= A12^T A12 (upper triangle only)
+      const int tp = (rest + TB - 1) / TB;
+      dim3 grid(tp, tp, 1);
+      gram_kernel<double, double><<<grid, 256, 0, ctx->stream>>>(kb, rest, rest, A + (long long)(k0 + kb) * lda + k0,
+                                                                 lda, A + (long long)(k0 + kb) * lda + k0, lda, nullptr,
+                                                                 -1.0, A + (long long)(k0 + kb) * lda + k0 + kb, lda,
+                                                                 kb, 1, 0);
+      count_launch(ctx);
+    }
+  }
+  zero_lower_kernel<<<grid_for((long long)l * l, 256, 1024), 256, 0, ctx->stream>>>(A, lda, l);
+  count_launch(ctx);
+  DB200_CUDA(ctx, cudaGetLastError());
+  return DB200_OK;
+}
+
+int trinv_upper(db200_context* ctx, const double* R, int ldr, int l, double* X, int ldx) {
+  trinv_upper_kernel<<<(l + 7) / 8, 256, 0, ctx->stream>>>(R, ldr, l, X, ldx);
+  DB200_CUDA(ctx, cudaGetLastError());
+  count_launch(ctx);
+  return DB200_OK;
+}
+
+int trsv_upper(db200_context* ctx, const double* R, const double* L, int ld, int l, double* x, bool transposed) {
+  trsv_kernel<<<1, 1024, 0, ctx->stream>>>(R, L, ld, l, x, transposed ? 0 : 1);
+  DB200_CUDA(ctx, cudaGetLastError());
+  count_launch(ctx);
+  return DB200_OK;
+}
+
+int transpose64(db200_context* ctx, const double* A, int lda, int m, int n, double* B, int ldb) {
+  dim3 grid((m + 31) / 32, (n + 31) / 32), block(32, 8);
+  transpose_kernel<<<grid, block, 0, ctx->stream>>>(A, lda, m, n, B, ldb);
+  DB200_CUDA(ctx, cudaGetLastError());
+  count_launch(ctx);
+  return DB200_OK;
+}
+
+int symmetrize(db200_context* ctx, double* C, int ldc, int l, double shift) {
+  symmetrize_kernel<<<grid_for((long long)l * l, 256, 1024), 256, 0, ctx->stream>>>(C, ldc, l, shift);
+  DB200_CUDA(ctx, cudaGetLastError());
+  count_launch(ctx);
+  return DB200_OK;
+}
+
+int mirror_upper(db200_context* ctx, double* C, int ldc, int l) {
+  fill_upper_from_lower_kernel<<<grid_for((long long)l * l, 256, 1024), 256, 0, ctx->stream>>>(C, ldc, l);
+  DB200_CUDA(ctx, cudaGetLastError());
+  count_launch(ctx);
+  return DB200_OK;
+}
+
+template <typename TS, typename TD>
+int convert(db200_context* ctx, const TS* src, long long lds, TD* dst, long long ldd, int m, int n) {
+  convert_kernel<TS, TD><<<grid_for((long long)m * n, 256, 8 * ctx->num_sms), 256, 0, ctx->stream>>>(src, lds, dst,
+                                                                                                     ldd, m, n);
+  DB200_CUDA(ctx, cudaGetLastError());
+  count_launch(ctx);
+  return DB200_OK;
+}
+template int convert<double, float>(db200_context*, const double*, long long, float*, long long, int, int);
+template int convert<float, double>(db200_context*, const float*, long long, double*, long long, int, int);
+template int convert<double, double>(db200_context*, const double*, long long, double*, long long, int, int);
+template int convert<float, float>(db200_context*, const float*, long long, float*, long long, int, int);
+
+int trace(db200_context* ctx, const double* C, int ldc, int l, double* d_out) {
+  trace_kernel<<<1, 1024, 0, ctx->stream>>>(C, ldc, l, d_out);
+  DB200_CUDA(ctx, cudaGetLastError());
+  count_launch(ctx);
+  return DB200_OK;
+}
+
+}  // namespace db200

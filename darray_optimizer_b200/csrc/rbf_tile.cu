@@ -452,6 +452,7 @@ int pack_points(db200_context* ctx, const float* X, int ldx, int layout, int n, 
   pack_points_kernel<<<(unsigned)blocks, threads, 0, ctx->stream>>>(X, sp, sf, n, d, dp, npad,
                                                                     static_cast<__nv_bfloat16*>(xp), norms);
   DB200_CUDA(ctx, cudaGetLastError());
+  count_launch(ctx);
   return DB200_OK;
 }
 
@@ -463,6 +464,7 @@ int pack_sketch(db200_context* ctx, const float* Omega, int ldo, const float* yj
   pack_sketch_kernel<<<(unsigned)blocks, 256, 0, ctx->stream>>>(Omega, ldo, yj, n, l, njpad, lrows,
                                                                 static_cast<__nv_bfloat16*>(op));
   DB200_CUDA(ctx, cudaGetLastError());
+  count_launch(ctx);
   return DB200_OK;
 }
 
@@ -505,6 +507,8 @@ int launch_rbf_tiles(db200_context* ctx, int mode, const PackedPoints& pi, const
   const size_t smem = L.total + 1024;
   const int n_items = a.n_itiles * a.n_panels;
   const int grid = n_items < ctx->num_sms ? n_items : ctx->num_sms;
+  cudaEvent_t e0 = nullptr;
+  prof_begin(ctx, &e0);
   if (mode == RBF_MODE_SKETCH) {
     DB200_CUDA(ctx, cudaFuncSetAttribute(rbf_tile_kernel<RBF_MODE_SKETCH>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -515,6 +519,8 @@ int launch_rbf_tiles(db200_context* ctx, int mode, const PackedPoints& pi, const
     rbf_tile_kernel<RBF_MODE_KBLOCK><<<grid, NUM_THREADS, smem, ctx->stream>>>(tm_xi, tm_xj, tm_om, a);
   }
   DB200_CUDA(ctx, cudaGetLastError());
+  prof_end(ctx, e0);
+  count_launch(ctx);
   return DB200_OK;
 }
 

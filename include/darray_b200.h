@@ -43,7 +43,11 @@ extern "C" {
 
 typedef struct db200_context db200_context;
 
-/* Create a context on `device`.  `stream` is a cudaStream_t (NULL: the context creates its own stream).
+/* Pass as `stream` to db200_create() to have the context create (and later destroy) its own stream. */
+#define DB200_OWN_STREAM ((void*)(intptr_t)-1)
+
+/* Create a context on `device`.  `stream` is the cudaStream_t all work is queued on (NULL: the CUDA default
+ * stream; DB200_OWN_STREAM: a new non-blocking stream owned by the context).
  * Replaces cuda_init() (include/dkernel.cu:28), whose handles were process globals. */
 DB200_API int db200_create(db200_context** ctx, int device, void* stream);
 
@@ -59,8 +63,14 @@ DB200_API int db200_synchronize(db200_context* ctx);
 /* The context's stream as a cudaStream_t. */
 DB200_API void* db200_stream(const db200_context* ctx);
 
-/* Number of tcgen05 tile kernels launched on this context since creation (for launch accounting). */
+/* Number of kernels this library has launched on this context since creation (launch accounting). */
 DB200_API int64_t db200_launch_count(const db200_context* ctx);
+
+/* Enable (1) or disable (0) CUDA-event timing of every tcgen05 tile-kernel launch on the context's stream;
+ * db200_profile_read() returns the summed kernel time (ms) and the number of timed launches since the last
+ * read, then clears them.  Both synchronize the stream. */
+DB200_API int db200_profile(db200_context* ctx, int enable);
+DB200_API int db200_profile_read(db200_context* ctx, double* total_ms, int64_t* count);
 
 /*
  * Fused RBF kernel x sketch (device pointers):
@@ -85,6 +95,17 @@ DB200_API int db200_rbf_sketch(db200_context* ctx, int m, int n, int d, int l, c
  */
 DB200_API int db200_rbf_block(db200_context* ctx, int m, int n, int d, const float* Xi, int ldxi, const float* Xj, int ldxj,
                     int x_layout, const float* yi, const float* yj, float* K, int ldk, float gamma);
+
+/*
+ * Host-pointer sketch with the calling convention of DArray::LRA (include/dkernel.h:13) on a 1 x 1 grid:
+ *     A(n x k) = diag(Y) K(X, X) diag(Y) O
+ * X is the d x n feature matrix (column major, ldx >= d: the reference's DMatrix X of tests/testsvm.cpp:76),
+ * Y the n labels, O the n x k test matrix (ldo >= n), A the n x k result (lda >= n).  Copies in, runs the fused
+ * kernel over every block (the reference stops after the first, include/dkernel.h:43) and copies out;
+ * synchronous.  Stands in for the rbf_kernel + tc_gemm host round trips of include/dkernel.cu:132-231.
+ */
+DB200_API int db200_lra_host(db200_context* ctx, int n, int d, int k, const float* X, int ldx, const float* Y,
+                             const float* O, int ldo, float* A, int lda, float gamma);
 
 #ifdef __cplusplus
 }

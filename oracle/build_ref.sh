@@ -1,0 +1,27 @@
+#!/usr/bin/env bash
+# Compile the reference's own C++ headers (read in place under the reference checkout) together with
+# oracle/ref_driver.cpp and the single-rank MPI stub into oracle/_ref/libdarray_ref.so, linked against the
+# OpenBLAS 0.3.15 that ships inside the image's opencv wheel (the reference needs Fortran BLAS/LAPACK symbols
+# with 32-bit integers).  Outputs go to oracle/_ref/ only.  Test infrastructure: the product never links it.
+set -euo pipefail
+HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
+REF="${DARRAY_REFERENCE:-/root/reference}"
+if [ ! -d "$REF/include" ]; then
+  echo "reference sources not found at $REF; nothing to build" >&2
+  exit 0
+fi
+BLAS_DIR="$(python -c 'import os, cv2; print(os.path.join(os.path.dirname(os.path.dirname(cv2.__file__)), "opencv_python_headless.libs"))' 2>/dev/null || true)"
+if [ -z "$BLAS_DIR" ] || [ ! -d "$BLAS_DIR" ]; then
+  BLAS_DIR="$(python -c 'import site; print(site.getsitepackages()[0])')/opencv_python_headless.libs"
+fi
+BLAS_LIB="$(ls "$BLAS_DIR"/libopenblasp-*.so 2>/dev/null | head -1)"
+if [ -z "$BLAS_LIB" ]; then
+  echo "no OpenBLAS with Fortran symbols found; reference build skipped" >&2
+  exit 0
+fi
+mkdir -p "$HERE/_ref"
+g++ -O2 -std=c++17 -shared -fPIC -w \
+    -I "$HERE/mpi_stub" -I "$REF/include" \
+    "$HERE/ref_driver.cpp" -o "$HERE/_ref/libdarray_ref.so" \
+    "$BLAS_LIB" -Wl,--disable-new-dtags -Wl,-rpath,"$BLAS_DIR"
+echo "$HERE/_ref/libdarray_ref.so"

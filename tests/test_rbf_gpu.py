@@ -45,8 +45,8 @@ def test_rbf_block_matches_oracle(gpu_ctx, m, n, d, layout):
         dXi, dXj, ldxi, ldxj = dev(np.asfortranarray(Xi)), dev(np.asfortranarray(Xj)), m, n
     ldk = m + 3
     K = colmajor_empty(m, n, ldk)
-    gpu_ctx.rbf_block(m, n, d, ptr(dXi), ldxi, ptr(dXj), ldxj, layout, ptr(dev(yi)), ptr(dev(yj)), ptr(K), ldk,
-                      gamma)
+    dyi, dyj = dev(yi), dev(yj)  # keep the device buffers alive across the call
+    gpu_ctx.rbf_block(m, n, d, ptr(dXi), ldxi, ptr(dXj), ldxj, layout, ptr(dyi), ptr(dyj), ptr(K), ldk, gamma)
     gpu_ctx.sync()
     Kg = colmajor_host(K, m)
     assert np.max(np.abs(Kg - Kref)) <= 2e-5
@@ -87,14 +87,16 @@ def test_rbf_sketch_matches_oracle(gpu_ctx, m, n, d, l):
     dyj = dyi if yj is yi else dev(yj)
     ldy = m + 1
     Y = colmajor_empty(m, l, ldy)
-    gpu_ctx.rbf_sketch(m, n, d, l, ptr(dXi), d, ptr(dXj), d, POINT_MAJOR, ptr(dyi), ptr(dyj), ptr(dev(Om)), n,
-                       ptr(Y), ldy, gamma)
+    dOm = dev(Om)
+    gpu_ctx.rbf_sketch(m, n, d, l, ptr(dXi), d, ptr(dXj), d, POINT_MAJOR, ptr(dyi), ptr(dyj), ptr(dOm), n, ptr(Y),
+                       ldy, gamma)
     gpu_ctx.sync()
     Yg = colmajor_host(Y, m)
     assert rel_fro(Yg, Yref) <= 1e-2
-    # every column individually, so a dropped panel cannot hide behind the global norm
-    col_err = np.linalg.norm(Yg - Yref, axis=0) / np.maximum(np.linalg.norm(Yref, axis=0), 1e-30)
-    assert col_err.max() <= 3e-2
+    # every column against the RMS column norm, so a dropped panel cannot hide behind the global norm
+    # (single columns can nearly cancel when K has a dominant constant mode, so not per-column relative)
+    rms_col = np.linalg.norm(Yref) / np.sqrt(l)
+    assert (np.linalg.norm(Yg - Yref, axis=0) / rms_col).max() <= 3e-2
 
 
 def test_rbf_sketch_two_calls_reuse_workspace(gpu_ctx):
