@@ -1,0 +1,36 @@
+// FP64 dense linear-algebra building blocks (la64.cu).  All stream-ordered on ctx->stream, column major.
+#pragma once
+#include "internal.h"
+
+namespace db200 {
+
+// C[p x q] = alpha * A^T diag(w) B + beta * C over n rows (w may be null); FP64 accumulation.  With upper_only
+// only the upper triangle of C (p == q) is formed.  Restates matrix_multiply("T","N") of include/blas_like.h:63.
+template <typename TA, typename TBt>
+int gram(db200_context* ctx, int n, int p, int q, const TA* A, long long lda, const TBt* B, long long ldb,
+         const double* w, double alpha, double beta, double* C, int ldc, bool upper_only);
+
+// C[n x q] = A[n x p] * op(B) + beta * C,  op(B) = B (p x q, ldb) or B^T (B stored q x p) when transB.
+template <typename TA, typename TC>
+int gemm_tall(db200_context* ctx, int n, int p, int q, const TA* A, long long lda, const double* B, int ldb,
+              bool transB, double beta, TC* C, long long ldc);
+
+// In-place upper Cholesky (A = R^T R) with block size nb <= 64; the strictly lower part is zeroed.  A
+// non-positive pivot sets *d_status = DB200_ERR_NOT_SPD and *d_bad = first row of the failing block.
+// Restates cholesky_factorize(A, 'U', n, 0, bs) of include/lapack_like.h:10-56.
+int potrf_upper(db200_context* ctx, double* A, int lda, int l, int* d_status, int* d_bad, int nb = 64);
+
+// X = R^-1 for upper triangular R.
+int trinv_upper(db200_context* ctx, const double* R, int ldr, int l, double* X, int ldx);
+
+// In-place triangular solve with upper R and its stored transpose L: transposed -> R^T x = b, else R x = b.
+int trsv_upper(db200_context* ctx, const double* R, const double* L, int ld, int l, double* x, bool transposed);
+
+int transpose64(db200_context* ctx, const double* A, int lda, int m, int n, double* B, int ldb);
+int symmetrize(db200_context* ctx, double* C, int ldc, int l, double shift);
+int mirror_upper(db200_context* ctx, double* C, int ldc, int l);
+template <typename TS, typename TD>
+int convert(db200_context* ctx, const TS* src, long long lds, TD* dst, long long ldd, int m, int n);
+int trace(db200_context* ctx, const double* C, int ldc, int l, double* d_out);
+
+}  // namespace db200
