@@ -33,13 +33,16 @@ SIGNATURES = {
     "db200_profile": (_c_int, [_vp, _c_int]),
     "db200_profile_read": (_c_int, [_vp, ctypes.POINTER(_c_double), ctypes.POINTER(_i64)]),
     "db200_lra_host": (_c_int, [_vp, _c_int, _c_int, _c_int, _vp, _c_int, _vp, _vp, _c_int, _vp, _c_int, _c_float]),
+    "db200_rbf_sketch_noalloc": (_c_int, [_vp, _c_int, _c_int, _c_int, _c_int, _vp, _c_int, _vp, _c_int, _c_int, _vp,
+                                          _vp, _vp, _c_int, _vp, _c_int, _c_float]),
 }
 
 STATUS = {
     0: "DB200_OK", -1: "DB200_ERR_INVALID", -2: "DB200_ERR_CUDA", -3: "DB200_ERR_NOT_SPD",
     -4: "DB200_ERR_MAXITER", -5: "DB200_ERR_INFEASIBLE", -6: "DB200_ERR_TIMEOUT", -7: "DB200_ERR_NOMEM",
-    -8: "DB200_ERR_UNSUPPORTED",
+    -8: "DB200_ERR_UNSUPPORTED", -9: "DB200_ERR_TOO_LARGE",
 }
+NOALLOC_SCRATCH_BYTES = 32 << 20
 POINT_MAJOR, FEATURE_MAJOR = 0, 1
 
 _lib = None

@@ -1,0 +1,131 @@
+// Allocation-free variant of the fused RBF x sketch entry point.
+//
+// Some callers cannot allocate device memory: plugin hosts that hand out a stream but own every allocation
+// (the library must not call cudaMalloc/cudaFree behind their allocator), code running under a strict
+// memory budget, or a process that must not touch the allocator between set-up and a latency-critical phase.
+// This entry point serves them.  Its scratch (packed split-bf16 points, norms, packed Omega^T and the device
+// status word) lives in one file-scope __device__ array of DB200_NOALLOC_SCRATCH_BYTES, which every GPU that
+// loads the library holds until the process exits.  Nothing here calls cudaMalloc, cudaFree or any allocating
+// library routine.
+#include <cstdio>
+#include <mutex>
+
+#include "internal.h"
+
+namespace db200 {
+namespace {
+
+// The scratch array.  In host code this name is only a host-side stand-in for the symbol; its device address
+// must be obtained with cudaGetSymbolAddress on each device before a kernel may use it.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[DB200_NOALLOC_SCRATCH_BYTES];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_setup_mutex;
+void* g_scratch_addr[kMaxDevices] = {};
+
+// Resolve the scratch array's device address on the current device (once per device).
+int scratch_address(int device, void** out) {
+  if (device < 0 || device >= kMaxDevices) return DB200_ERR_UNSUPPORTED;
+  std::lock_guard<std::mutex> lock(g_setup_mutex);
+  if (!g_scratch_addr[device]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      std::fprintf(stderr, "db200_rbf_sketch_noalloc: cudaGetSymbolAddress failed on device %d: %s\n", device,
+                   cudaGetErrorString(e));
+      return DB200_ERR_CUDA;
+    }
+    g_scratch_addr[device] = p;
+  }
+  *out = g_scratch_addr[device];
+  return DB200_OK;
+}
+
+}  // namespace
+}  // namespace db200
+
+using namespace db200;
+
+extern "C" int db200_rbf_sketch_noalloc(void* stream, int m, int n, int d, int l, const float* Xi, int ldxi,
+                                        const float* Xj, int ldxj, int x_layout, const float* yi, const float* yj,
+                                        const float* Omega, int ldo, float* Y, int ldy, float gamma) {
+  if (m < 0 || n < 0 || d < 1 || l < 0) return DB200_ERR_INVALID;
+  if (m == 0 || l == 0) return DB200_OK;
+  if (n < 1 || d > 128) return DB200_ERR_UNSUPPORTED;
+  if (!Xi || !Xj || !Omega || !Y || ldo < n || ldy < m) return DB200_ERR_INVALID;
+  if (x_layout == DB200_POINT_MAJOR) {
+    if (ldxi < d || ldxj < d) return DB200_ERR_INVALID;
+  } else if (x_layout == DB200_FEATURE_MAJOR) {
+    if (ldxi < m || ldxj < n) return DB200_ERR_INVALID;
+  } else {
+    return DB200_ERR_INVALID;
+  }
+
+  // Scratch layout: [status | Xi packed | Xi norms | Xj packed | Xj norms | Omega^T packed], 256-byte aligned.
+  const int dp = feature_pad(d);
+  const int mpad = round_up(m, 128), npad = round_up(n, 128);
+  const bool same = (Xi == Xj && ldxi == ldxj && m == n);
+  const SketchPlan plan = plan_sketch(l);
+  size_t need = 256;
+  need = align_up(need + (size_t)mpad * 2 * dp * 2, 256);
+  need = align_up(need + (size_t)mpad * 4, 256);
+  if (!same) {
+    need = align_up(need + (size_t)npad * 2 * dp * 2, 256);
+    need = align_up(need + (size_t)npad * 4, 256);
+  }
+  need = align_up(need + (size_t)plan.lrows * npad * 2, 256);
+  if (need > (size_t)DB200_NOALLOC_SCRATCH_BYTES) {
+    std::fprintf(stderr,
+                 "db200_rbf_sketch_noalloc: m=%d n=%d d=%d l=%d needs %zu bytes of scratch, more than the fixed "
+                 "%zu-byte array; use db200_rbf_sketch for this size\n",
+                 m, n, d, l, need, (size_t)DB200_NOALLOC_SCRATCH_BYTES);
+    return DB200_ERR_TOO_LARGE;
+  }
+
+  int device = 0;
+  if (cudaGetDevice(&device) != cudaSuccess) return DB200_ERR_CUDA;
+  void* base = nullptr;
+  int st = scratch_address(device, &base);
+  if (st) return st;
+
+  // A context on the stack: it owns nothing and allocates nothing.
+  db200_context ctx;
+  ctx.device = device;
+  ctx.stream = static_cast<cudaStream_t>(stream);
+  if (cudaDeviceGetAttribute(&ctx.num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+    return DB200_ERR_CUDA;
+  Carve carve{static_cast<char*>(base)};
+  ctx.d_status = carve.take<int>(64);
+  if (cudaMemsetAsync(ctx.d_status, 0, sizeof(int), ctx.stream) != cudaSuccess) return DB200_ERR_CUDA;
+
+  PackedPoints pi, pj;
+  void* xpi = carve.take<uint16_t>((size_t)mpad * 2 * dp);
+  float* ni = carve.take<float>(mpad);
+  if ((st = pack_points(&ctx, Xi, ldxi, x_layout, m, d, dp, mpad, xpi, ni))) return st;
+  pi.xp = xpi;
+  pi.norms = ni;
+  pi.n = m;
+  pi.npad = mpad;
+  pi.dp = dp;
+  if (same) {
+    pj = pi;
+  } else {
+    void* xpj = carve.take<uint16_t>((size_t)npad * 2 * dp);
+    float* nj = carve.take<float>(npad);
+    if ((st = pack_points(&ctx, Xj, ldxj, x_layout, n, d, dp, npad, xpj, nj))) return st;
+    pj.xp = xpj;
+    pj.norms = nj;
+    pj.n = n;
+    pj.npad = npad;
+    pj.dp = dp;
+  }
+  void* op = carve.take<uint16_t>((size_t)plan.lrows * npad);
+  if ((st = pack_sketch(&ctx, Omega, ldo, yj, n, l, npad, plan.lrows, op))) return st;
+  if ((st = launch_rbf_tiles(&ctx, RBF_MODE_SKETCH, pi, pj, yi, nullptr, op, plan, l, gamma, Y, ldy))) return st;
+
+  // Synchronous: wait, then report a device-side wait that gave up.
+  if (cudaStreamSynchronize(ctx.stream) != cudaSuccess) return DB200_ERR_CUDA;
+  int dev_status = 0;
+  if (cudaMemcpy(&dev_status, ctx.d_status, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return DB200_ERR_CUDA;
+  return dev_status;
+}

@@ -36,6 +36,7 @@ extern "C" {
 #define DB200_ERR_TIMEOUT (-6)     /* a bounded device-side wait gave up */
 #define DB200_ERR_NOMEM (-7)       /* device allocation failed */
 #define DB200_ERR_UNSUPPORTED (-8) /* shape outside what the kernels implement */
+#define DB200_ERR_TOO_LARGE (-9)   /* request exceeds the fixed scratch of db200_rbf_sketch_noalloc */
 
 /* Layout of a point matrix X holding n points of d features. */
 #define DB200_POINT_MAJOR 0   /* x(i,k) = X[k + i*ldx]  (the reference's DMatrix X, d x n column major) */
@@ -106,6 +107,28 @@ DB200_API int db200_rbf_block(db200_context* ctx, int m, int n, int d, const flo
  */
 DB200_API int db200_lra_host(db200_context* ctx, int n, int d, int k, const float* X, int ldx, const float* Y,
                              const float* O, int ldo, float* A, int lda, float gamma);
+
+/*
+ * Allocation-free fused RBF x sketch.  No counterpart in the reference: it exists for callers that cannot call
+ * cudaMalloc -- plugin hosts that own every device allocation and only lend a stream, processes under a hard
+ * memory budget, or latency-critical phases that must not enter the allocator.
+ *
+ * Same arguments, arithmetic and result as db200_rbf_sketch, but no context: work is queued on `stream`
+ * (a cudaStream_t; NULL = the default stream) and the call waits for it before returning.  Its scratch
+ * (packed operands and a status word) is one static device array of DB200_NOALLOC_SCRATCH_BYTES that every GPU
+ * loading this library holds until the process exits; the function calls no cudaMalloc, cudaFree or other
+ * allocating routine.  Requests whose scratch would exceed the array return DB200_ERR_TOO_LARGE (with a message
+ * on stderr naming the bytes needed).  The scratch need is about
+ *     (m + n) * (4 * roundup(d, 32) + 4) + 2 * n * roundup(l, 16)   bytes   (the n term once when Xi == Xj).
+ * The first call on each device resolves the array's device address (cudaGetSymbolAddress, with that device
+ * current); make that first call before any stream capture.  All calls share the one array and it keeps the
+ * previous call's contents (every byte a call reads is written by that call first); calls that overlap on the
+ * GPU -- from two host threads, or on two streams -- race on it and must be serialised by the caller.
+ */
+#define DB200_NOALLOC_SCRATCH_BYTES (32u << 20)
+DB200_API int db200_rbf_sketch_noalloc(void* stream, int m, int n, int d, int l, const float* Xi, int ldxi,
+                                       const float* Xj, int ldxj, int x_layout, const float* yi, const float* yj,
+                                       const float* Omega, int ldo, float* Y, int ldy, float gamma);
 
 #ifdef __cplusplus
 }
