@@ -200,7 +200,7 @@ def run_ours(args):
     from darray_optimizer_b200 import datagen
     from darray_optimizer_b200._lib import Context
 
-    w = datagen.uniform_hyperplane(n=N_POINTS, d=D_FEAT, seed=2 + rank)
+    w = datagen.uniform_hyperplane(n=args.n, d=D_FEAT, seed=2 + rank)
     n, d, l = w.n, w.d, w.l
     Om = w.omega()
     stream = torch.cuda.current_stream()
@@ -244,6 +244,17 @@ def run_ours(args):
     value = world * F * args.steps / (ms_max / 1e3) / 1e12
 
     # end to end through the host-pointer LRA entry point (pinned host buffers, copies inside the timed region)
+    e2e_val = h2d = d2h = None
+    if not args.no_e2e:
+        e2e_val, h2d, d2h = e2e_run(ctx, w, Om, world, args.steps)
+    return finish(args, ctx, w, world, rank, ms_max, kernel_ms, kernel_count, launches, clocks, e2e_val, h2d, d2h,
+                  Om)
+
+
+def e2e_run(ctx, w, Om, world, steps):
+    import torch
+    n, d, l = w.n, w.d, w.l
+    F = flops(n, d, l)
     Xh = torch.from_numpy(w.X).pin_memory()
     yh = torch.from_numpy(w.y).pin_memory()
     Oh = torch.from_numpy(np.ascontiguousarray(Om.T)).pin_memory()
@@ -255,13 +266,20 @@ def run_ours(args):
     e2e_step()
     barrier(world)
     t0 = time.perf_counter()
-    k2 = max(1, args.steps)
+    k2 = max(1, steps)
     for _ in range(k2):
         e2e_step()
     e2e_s = all_max(time.perf_counter() - t0, world)
     e2e_val = world * F * k2 / e2e_s / 1e12
     h2d = Xh.numel() * 4 + yh.numel() * 4 + Oh.numel() * 4
     d2h = Ah.numel() * 4
+    return e2e_val, h2d, d2h
+
+
+def finish(args, ctx, w, world, rank, ms_max, kernel_ms, kernel_count, launches, clocks, e2e_val, h2d, d2h, Om):
+    n, d, l = w.n, w.d, w.l
+    F = flops(n, d, l)
+    value = world * F * args.steps / (ms_max / 1e3) / 1e12
 
     # roofline of the dominant kernel (tcgen05 tile kernel), timed live with events on its stream
     peaks = {}
@@ -284,7 +302,7 @@ def run_ours(args):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "bf16", "data": "synthetic (seeded Philox)",
-            "config": config({"parallelism": f"replicas x{world}"}), "clocks": clocks,
+            "config": config({"parallelism": f"replicas x{world}", "n": n}), "clocks": clocks,
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches, "roofline": roof}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -307,6 +325,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg (profiling runs)")
+    ap.add_argument("--n", type=int, default=N_POINTS, help="points (default: the C2 workload, 131072)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

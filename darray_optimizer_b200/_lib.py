@@ -18,6 +18,22 @@ _c_int, _c_float, _c_double = ctypes.c_int, ctypes.c_float, ctypes.c_double
 _vp = ctypes.c_void_p
 _i64 = ctypes.c_int64
 
+
+class BarrierParams(ctypes.Structure):
+    _fields_ = [("t0", ctypes.c_double), ("mu", ctypes.c_double), ("alpha", ctypes.c_double),
+                ("beta", ctypes.c_double), ("gap_tol", ctypes.c_double), ("newton_tol", ctypes.c_double),
+                ("max_outer", ctypes.c_int), ("max_newton", ctypes.c_int)]
+
+
+class SvmReport(ctypes.Structure):
+    _fields_ = [("f", ctypes.c_double), ("gap_barrier", ctypes.c_double), ("gap_primal_dual", ctypes.c_double),
+                ("t", ctypes.c_double), ("nu", ctypes.c_double), ("outer", ctypes.c_int), ("newton", ctypes.c_int),
+                ("status", ctypes.c_int), ("ms_sketch", ctypes.c_double), ("ms_orth", ctypes.c_double),
+                ("ms_core", ctypes.c_double), ("ms_barrier", ctypes.c_double), ("ms_total", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     "db200_create": (_c_int, [ctypes.POINTER(_vp), _c_int, _vp]),
@@ -33,6 +49,19 @@ SIGNATURES = {
     "db200_profile": (_c_int, [_vp, _c_int]),
     "db200_profile_read": (_c_int, [_vp, ctypes.POINTER(_c_double), ctypes.POINTER(_i64)]),
     "db200_lra_host": (_c_int, [_vp, _c_int, _c_int, _c_int, _vp, _c_int, _vp, _vp, _c_int, _vp, _c_int, _c_float]),
+    "db200_potrf": (_c_int, [_vp, _c_int, _vp, _c_int, _c_int]),
+    "db200_cholqr2": (_c_int, [_vp, _c_int, _c_int, _vp, _c_int, _vp, _c_int]),
+    "db200_gemm_tn": (_c_int, [_vp, _c_int, _c_int, _c_int, _c_double, _vp, _c_int, _vp, _c_int, _c_double, _vp,
+                               _c_int]),
+    "db200_trsm_lutn": (_c_int, [_vp, _c_int, _c_int, _vp, _c_int, _vp, _c_int]),
+    "db200_barrier_defaults": (None, [ctypes.POINTER(BarrierParams)]),
+    "db200_svm_barrier": (_c_int, [_vp, _c_int, _c_int, _vp, _c_int, _vp, _c_double, ctypes.POINTER(BarrierParams),
+                                   _vp, ctypes.POINTER(SvmReport)]),
+    "db200_lowrank": (_c_int, [_vp, _c_int, _c_int, _c_int, _c_int, _vp, _c_int, _vp, _vp, _c_int, _c_float, _vp,
+                               _c_int, ctypes.POINTER(SvmReport)]),
+    "db200_svm_solve": (_c_int, [_vp, _c_int, _c_int, _c_int, _c_int, _vp, _c_int, _vp, _vp, _c_int, _c_float,
+                                 _c_double, ctypes.POINTER(BarrierParams), _vp, _vp, _c_int,
+                                 ctypes.POINTER(SvmReport)]),
     "db200_rbf_sketch_noalloc": (_c_int, [_vp, _c_int, _c_int, _c_int, _c_int, _vp, _c_int, _vp, _c_int, _c_int, _vp,
                                           _vp, _vp, _c_int, _vp, _c_int, _c_float]),
 }
@@ -135,6 +164,46 @@ class Context:
 
     def lra_host(self, n, d, k, X, ldx, Y, O, ldo, A, lda, gamma):
         return self.check(self.lib.db200_lra_host(self.h, n, d, k, X, ldx, Y, O, ldo, A, lda, gamma))
+
+    def potrf(self, n, A, lda, nb=64):
+        return self.check(self.lib.db200_potrf(self.h, n, A, lda, nb))
+
+    def cholqr2(self, n, l, Y, ldy, R, ldr):
+        return self.check(self.lib.db200_cholqr2(self.h, n, l, Y, ldy, R, ldr))
+
+    def gemm_tn(self, k, m, n, alpha, A, lda, B, ldb, beta, C, ldc):
+        return self.check(self.lib.db200_gemm_tn(self.h, k, m, n, alpha, A, lda, B, ldb, beta, C, ldc))
+
+    def trsm_lutn(self, m, n, R, ldr, B, ldb):
+        return self.check(self.lib.db200_trsm_lutn(self.h, m, n, R, ldr, B, ldb))
+
+    @staticmethod
+    def barrier_params(**kw) -> BarrierParams:
+        p = BarrierParams()
+        load().db200_barrier_defaults(ctypes.byref(p))
+        for k, v in kw.items():
+            setattr(p, k, v)
+        return p
+
+    def svm_barrier(self, n, r, Z, ldz, y, C, a, params=None, allow_maxiter=False):
+        rep = SvmReport()
+        p = params or self.barrier_params()
+        st = self.lib.db200_svm_barrier(self.h, n, r, Z, ldz, y, C, ctypes.byref(p), a, ctypes.byref(rep))
+        if not (allow_maxiter and st == -4):
+            self.check(st)
+        return rep
+
+    def lowrank(self, n, d, l, q, X, ldx, y, Om, ldo, gamma, Z, ldz):
+        rep = SvmReport()
+        self.check(self.lib.db200_lowrank(self.h, n, d, l, q, X, ldx, y, Om, ldo, gamma, Z, ldz, ctypes.byref(rep)))
+        return rep
+
+    def svm_solve(self, n, d, l, q, X, ldx, y, Om, ldo, gamma, C, a, Z, ldz, params=None):
+        rep = SvmReport()
+        p = params or self.barrier_params()
+        self.check(self.lib.db200_svm_solve(self.h, n, d, l, q, X, ldx, y, Om, ldo, gamma, C, ctypes.byref(p), a, Z,
+                                            ldz, ctypes.byref(rep)))
+        return rep
 
     def rbf_block(self, m, n, d, Xi, ldxi, Xj, ldxj, layout, yi, yj, K, ldk, gamma):
         return self.check(self.lib.db200_rbf_block(self.h, m, n, d, Xi, ldxi, Xj, ldxj, layout, yi, yj, K, ldk,

@@ -1,0 +1,28 @@
+// Device building blocks of the barrier solver (barrier.cu); FP64, column-major Z (n x r, leading dim ld).
+#pragma once
+#include "internal.h"
+
+namespace db200 {
+
+// red[0..nsum) = 0, next nmax = 0 (for maxima of non-negative values), next nmin = DBL_MAX.
+int bar_init_red(db200_context* ctx, double* red, int nsum, int nmax, int nmin);
+// g = Z w - 1 + (-1/a + 1/(C-a))/t,  dinv = 1/D,  D = (1/a^2 + 1/(C-a)^2)/t  (include/dbarrier.h:48-81);
+// red: [0] += sum a, [1] += sum(log a + log(C-a)), [2] max D, [3] min D.
+int bar_grad_hess(db200_context* ctx, int n, int r, const double* Z, long long ld, const double* w, const double* a,
+                  double C, double t, double* g, double* dinv, double* red);
+// s = -dinv (g + Z u);  red: [0] += g.s, [1] += sum s, [2] min feasible step (init DBL_MAX).
+int bar_direction(db200_context* ctx, int n, int r, const double* Z, long long ld, const double* u, const double* g,
+                  const double* dinv, const double* a, double C, double* s, double* red);
+// out = sign * Z^T (scale .* v)  (scale may be null); out is zeroed first.
+int bar_gemv_t(db200_context* ctx, int n, int r, const double* Z, long long ld, const double* v, const double* scale,
+               double sign, double* out);
+// out[k] = sum log(a + tau_k s) + log(C - a - tau_k s), out[16 + k] = count of coordinates leaving the box.
+int bar_linesearch16(db200_context* ctx, int n, const double* a, const double* s, double C, const double* taus,
+                     double* out);
+int bar_axpy(db200_context* ctx, int n, double alpha, const double* x, double* y);
+// red[0] = sum max(0, 1 - (Z w)_i)
+int bar_hinge(db200_context* ctx, int n, int r, const double* Z, long long ld, const double* w, double* red);
+int bar_add_identity(db200_context* ctx, double* M, int ldm, int r);
+int bar_dot(db200_context* ctx, int r, const double* x, const double* y, double* out);
+
+}  // namespace db200

@@ -75,6 +75,23 @@ void* io_buffer(db200_context* ctx, size_t bytes) {
   return ctx->io;
 }
 
+void* slot_buffer(db200_context* ctx, int slot, size_t bytes) {
+  if (bytes <= ctx->slot_size[slot]) return ctx->slot[slot];
+  cudaStreamSynchronize(ctx->stream);
+  if (ctx->slot[slot]) cudaFree(ctx->slot[slot]);
+  ctx->slot[slot] = nullptr;
+  ctx->slot_size[slot] = 0;
+  size_t want = align_up(bytes, 1 << 20);
+  cudaError_t e = cudaMalloc(&ctx->slot[slot], want);
+  if (e != cudaSuccess) {
+    ctx->slot[slot] = nullptr;
+    cuda_fail(ctx, e, "cudaMalloc(slot buffer)");
+    return nullptr;
+  }
+  ctx->slot_size[slot] = want;
+  return ctx->slot[slot];
+}
+
 }  // namespace db200
 
 using namespace db200;
@@ -130,6 +147,8 @@ int db200_destroy(db200_context* ctx) {
   prof_clear(ctx);
   if (ctx->ws) cudaFree(ctx->ws);
   if (ctx->io) cudaFree(ctx->io);
+  for (void* p : ctx->slot)
+    if (p) cudaFree(p);
   if (ctx->d_status) cudaFree(ctx->d_status);
   if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);

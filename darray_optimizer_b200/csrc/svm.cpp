@@ -1,0 +1,476 @@
+// Host orchestration of the kernel-SVM path (C++ over the device kernels): dense FP64 LA entry points,
+// CholeskyQR2, the Nystrom low-rank factor and the barrier / Newton loop.
+//
+// Restated from tests/testsvm.cpp:86-321 (the SVM driver), include/lapack_like.h:10-90,283-379 and
+// include/dbarrier.h:14-139, with the corrections listed in oracle/oracle.py's header (every block of K, the
+// Q C Q^T core, the Woodbury Newton system, a line search that keeps 0 < a < C, barrier stop at 1e-6).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "barrier.h"
+#include "internal.h"
+#include "la64.h"
+
+namespace db200 {
+namespace {
+
+struct EventTimer {
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaStream_t s;
+  explicit EventTimer(cudaStream_t st) : s(st) {
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, s);
+  }
+  double stop_ms() {
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    return ms;
+  }
+  ~EventTimer() {
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+};
+
+// Device status pair [status, bad index] used by potrf; lives at the start of the LA slot.
+struct LaStatus {
+  int* d = nullptr;
+};
+
+int read_status(db200_context* ctx, int* d_pair, int* st, int* bad) {
+  int h[2] = {0, 0};
+  DB200_CUDA(ctx, cudaMemcpyAsync(h, d_pair, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+  DB200_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  *st = h[0];
+  *bad = h[1];
+  return DB200_OK;
+}
+
+// One CholeskyQR pass Yout = Yin R^-1 with R = chol(Yin^T Yin + shift I); returns NOT_SPD without touching Yout
+// when the Gram is not positive definite.  W, Rinv: l x l scratch; R (l x l) receives the factor.
+int cholqr_pass(db200_context* ctx, int n, int l, const double* Yin, int ldin, double* Yout, int ldout, double* R,
+                double* Rinv, double shift_rel, int* d_pair, double* d_scalar) {
+  int st = gram<double, double>(ctx, n, l, l, Yin, ldin, Yin, ldin, nullptr, 1.0, 0.0, R, l, true);
+  if (st) return st;
+  if (shift_rel > 0.0) {
+    // shift = shift_rel * trace(W)
+    if ((st = trace(ctx, R, l, l, d_scalar))) return st;
+    double tr = 0;
+    DB200_CUDA(ctx, cudaMemcpyAsync(&tr, d_scalar, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    DB200_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if ((st = mirror_upper(ctx, R, l, l))) return st;  // the Gram kernel formed the upper triangle only
+    if ((st = symmetrize(ctx, R, l, l, shift_rel * tr))) return st;
+  }
+  DB200_CUDA(ctx, cudaMemsetAsync(d_pair, 0, 2 * sizeof(int), ctx->stream));
+  if ((st = potrf_upper(ctx, R, l, l, d_pair, d_pair + 1))) return st;
+  int pst = 0, bad = 0;
+  if ((st = read_status(ctx, d_pair, &pst, &bad))) return st;
+  if (pst) return fail(ctx, DB200_ERR_NOT_SPD, "CholeskyQR: Gram matrix not positive definite at row " +
+                                                   std::to_string(bad));
+  if ((st = trinv_upper(ctx, R, l, l, Rinv, l))) return st;
+  return gemm_tall<double, double>(ctx, n, l, l, Yin, ldin, Rinv, l, false, 0.0, Yout, ldout);
+}
+
+}  // namespace
+
+int cholqr2_impl(db200_context* ctx, int n, int l, double* Y, int ldy, double* Rout, int ldr) {
+  // slot layout: [pair | scalar | T (n x l) | R1 | R2 | R3 | Rinv | Racc]
+  const size_t ll = (size_t)l * l;
+  const size_t bytes = 1024 + align_up((size_t)n * l * 8, 256) + 5 * align_up(ll * 8, 256) + 1024;
+  char* base = static_cast<char*>(slot_buffer(ctx, SLOT_LA, bytes));
+  if (!base) return DB200_ERR_NOMEM;
+  Carve cv{base};
+  int* d_pair = cv.take<int>(4);
+  double* d_scalar = cv.take<double>(4);
+  double* T = cv.take<double>((size_t)n * l);
+  double* R1 = cv.take<double>(ll);
+  double* R2 = cv.take<double>(ll);
+  double* R3 = cv.take<double>(ll);
+  double* Rinv = cv.take<double>(ll);
+  double* Racc = cv.take<double>(ll);
+  int st = cholqr_pass(ctx, n, l, Y, ldy, T, n, R1, Rinv, 0.0, d_pair, d_scalar);
+  bool shifted = false;
+  if (st == DB200_ERR_NOT_SPD) {
+    // shifted CholeskyQR3 (Fukaya, Kannan, Nakatsukasa, Yamamoto, Yanagisawa 2020): first pass with
+    // shift 11 (n l + l (l + 1)) u ||Y||^2, ||Y||_2^2 <= trace(Y^T Y)
+    const double u = 1.1102230246251565e-16;
+    const double rel = 11.0 * ((double)n * l + (double)l * (l + 1)) * u;
+    st = cholqr_pass(ctx, n, l, Y, ldy, T, n, R1, Rinv, rel, d_pair, d_scalar);
+    shifted = true;
+  }
+  if (st) return st;
+  // second pass T -> Y
+  if ((st = cholqr_pass(ctx, n, l, T, n, Y, ldy, R2, Rinv, 0.0, d_pair, d_scalar))) return st;
+  // R = R2 R1 (upper * upper)
+  if ((st = gemm_tall<double, double>(ctx, l, l, l, R2, l, R1, l, false, 0.0, Racc, l))) return st;
+  if (shifted) {
+    // third pass Y -> T, then copy back; R = R3 (R2 R1)
+    if ((st = cholqr_pass(ctx, n, l, Y, ldy, T, n, R3, Rinv, 0.0, d_pair, d_scalar))) return st;
+    DB200_CUDA(ctx, cudaMemcpy2DAsync(Y, sizeof(double) * ldy, T, sizeof(double) * n, sizeof(double) * n, l,
+                                      cudaMemcpyDeviceToDevice, ctx->stream));
+    if ((st = gemm_tall<double, double>(ctx, l, l, l, R3, l, Racc, l, false, 0.0, R1, l))) return st;
+    Racc = R1;
+  }
+  if (Rout) {
+    DB200_CUDA(ctx, cudaMemcpy2DAsync(Rout, sizeof(double) * ldr, Racc, sizeof(double) * l, sizeof(double) * l, l,
+                                      cudaMemcpyDeviceToDevice, ctx->stream));
+  }
+  return DB200_OK;
+}
+
+// ---------------------------------------------------------------------------------------------- barrier
+namespace {
+
+__attribute__((unused)) void set_a0_host(const std::vector<float>& y, double C, double* pval, double* mval) {
+  long plus = 0, minus = 0;
+  for (float v : y) {
+    if (v == 1.0f) ++plus;
+    else ++minus;
+  }
+  if (plus > minus) {
+    *mval = 0.9 * C;
+    *pval = minus > 0 ? *mval * minus / plus : *mval;
+  } else {
+    *pval = 0.9 * C;
+    *mval = plus > 0 ? *pval * plus / minus : *pval;
+  }
+}
+
+}  // namespace
+
+int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz, const float* y, double C,
+                     const db200_barrier_params& P, double* a, db200_svm_report* rep) {
+  if (r > 4096) return fail(ctx, DB200_ERR_UNSUPPORTED, "svm_barrier: r > 4096");
+  EventTimer timer(ctx->stream);
+  const size_t rr = (size_t)r * r;
+  const size_t bytes = 4096 + 3 * align_up((size_t)n * 8, 256) + 6 * align_up((size_t)r * 8, 256) +
+                       2 * align_up(rr * 8, 256) + 4096;
+  char* base = static_cast<char*>(slot_buffer(ctx, SLOT_BAR, bytes));
+  if (!base) return DB200_ERR_NOMEM;
+  Carve cv{base};
+  double* red = cv.take<double>(64);
+  double* taus = cv.take<double>(16);
+  double* ls = cv.take<double>(32);
+  double* sc = cv.take<double>(8);  // scalars: [0] w.w, [1] w.v, [2] v.v, [3] hinge
+  int* d_pair = cv.take<int>(4);
+  double* g = cv.take<double>(n);
+  double* dinv = cv.take<double>(n);
+  double* s = cv.take<double>(n);
+  double* w = cv.take<double>(r);
+  double* v = cv.take<double>(r);
+  double* u = cv.take<double>(r);
+  double* M = cv.take<double>(rr);
+  double* L = cv.take<double>(rr);
+
+  // class-balanced start (tests/testsvm.cpp:192-212)
+  std::vector<float> hy(n);
+  DB200_CUDA(ctx, cudaMemcpyAsync(hy.data(), y, sizeof(float) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  DB200_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  double pval = 0, mval = 0;
+  set_a0_host(hy, C, &pval, &mval);
+  {
+    std::vector<double> ha(n);
+    for (int i = 0; i < n; ++i) ha[i] = (hy[i] == 1.0f) ? pval : mval;
+    DB200_CUDA(ctx, cudaMemcpyAsync(a, ha.data(), sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+    DB200_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+
+  double t = P.t0;
+  int total_newton = 0, outer = 0, status = DB200_OK;
+  double h[64];
+  int st;
+  auto fetch = [&](const double* d_src, int count) -> int {
+    DB200_CUDA(ctx, cudaMemcpyAsync(h, d_src, sizeof(double) * count, cudaMemcpyDeviceToHost, ctx->stream));
+    DB200_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return DB200_OK;
+  };
+  double fa = 0.0, suma_now = 0.0;
+  for (outer = 1; outer <= P.max_outer; ++outer) {
+    int ni = 0;
+    while (true) {
+      ++ni;
+      ++total_newton;
+      // gradient / Hessian diagonal at a
+      if ((st = bar_gemv_t(ctx, n, r, Z, ldz, a, nullptr, 1.0, w))) return st;
+      if ((st = bar_init_red(ctx, red, 2, 1, 1))) return st;
+      if ((st = bar_grad_hess(ctx, n, r, Z, ldz, w, a, C, t, g, dinv, red))) return st;
+      if ((st = bar_dot(ctx, r, w, w, sc))) return st;
+      DB200_CUDA(ctx, cudaMemcpyAsync(red + 8, sc, sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+      if ((st = fetch(red, 9))) return st;
+      const double suma = h[0], sumlog = h[1], dmax = h[2], dmin = h[3], ww = h[8];
+      if (dmax / dmin > 1e18) break;  // tests/testsvm.cpp:258-263
+      const double lastg = 0.5 * ww - suma - sumlog / t;
+      // capacity matrix M = I + Z^T D^-1 Z and right-hand side u = -Z^T D^-1 g
+      if ((st = gram<double, double>(ctx, n, r, r, Z, ldz, Z, ldz, dinv, 1.0, 0.0, M, r, true))) return st;
+      if ((st = bar_add_identity(ctx, M, r, r))) return st;
+      if ((st = bar_gemv_t(ctx, n, r, Z, ldz, g, dinv, -1.0, u))) return st;
+      DB200_CUDA(ctx, cudaMemsetAsync(d_pair, 0, 2 * sizeof(int), ctx->stream));
+      if ((st = potrf_upper(ctx, M, r, r, d_pair, d_pair + 1))) return st;
+      if ((st = transpose64(ctx, M, r, r, r, L, r))) return st;
+      if ((st = trsv_upper(ctx, M, L, r, r, u, true))) return st;   // R^T z = rhs
+      if ((st = trsv_upper(ctx, M, L, r, r, u, false))) return st;  // R u = z
+      if ((st = bar_init_red(ctx, red, 2, 0, 1))) return st;
+      if ((st = bar_direction(ctx, n, r, Z, ldz, u, g, dinv, a, C, s, red))) return st;
+      if ((st = bar_gemv_t(ctx, n, r, Z, ldz, s, nullptr, 1.0, v))) return st;
+      if ((st = bar_dot(ctx, r, w, v, sc + 1))) return st;
+      if ((st = bar_dot(ctx, r, v, v, sc + 2))) return st;
+      DB200_CUDA(ctx, cudaMemcpyAsync(red + 8, sc + 1, 2 * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+      DB200_CUDA(ctx, cudaMemcpyAsync(red + 12, d_pair, 2 * sizeof(int), cudaMemcpyDeviceToDevice, ctx->stream));
+      if ((st = fetch(red, 13))) return st;
+      int pst;
+      std::memcpy(&pst, &h[12], sizeof(int));
+      if (pst) return fail(ctx, DB200_ERR_NOT_SPD, "svm_barrier: Woodbury capacity matrix not positive definite");
+      const double gs = h[0], sums = h[1], tmax = h[2], wv = h[8], vv = h[9];
+      const double lam2 = -gs;
+      // backtracking line search inside the box, 16 candidates per device pass
+      double tau = std::min(1.0, 0.99 * tmax);
+      double accepted = -1.0, newg = lastg;
+      for (int round = 0; round < 4 && accepted < 0; ++round) {
+        double ht[16];
+        for (int k = 0; k < 16; ++k) ht[k] = tau * std::pow(P.beta, k);
+        DB200_CUDA(ctx, cudaMemcpyAsync(taus, ht, sizeof(ht), cudaMemcpyHostToDevice, ctx->stream));
+        if ((st = bar_linesearch16(ctx, n, a, s, C, taus, ls))) return st;
+        if ((st = fetch(ls, 32))) return st;
+        for (int k = 0; k < 16; ++k) {
+          if (h[16 + k] != 0.0) continue;  // leaves the box
+          const double tk = ht[k];
+          const double fk = 0.5 * (ww + 2.0 * tk * wv + tk * tk * vv) - (suma + tk * sums) - h[k] / t;
+          if (fk <= lastg + P.alpha * tk * gs) {
+            accepted = tk;
+            newg = fk;
+            break;
+          }
+        }
+        tau = ht[15] * P.beta;
+      }
+      if (accepted < 0) accepted = 0.0;  // no decrease found: stop this Newton loop below
+      if (accepted > 0 && (st = bar_axpy(ctx, n, accepted, s, a))) return st;
+      if (lam2 / 2 < P.newton_tol) break;
+      if (accepted == 0.0) break;
+      if (ni > 1 && (lastg - newg) < 1e-9 * std::fabs(newg)) break;
+      if (ni >= P.max_newton) {
+        status = DB200_ERR_MAXITER;
+        break;
+      }
+    }
+    // f(a) for the barrier stop
+    if ((st = bar_gemv_t(ctx, n, r, Z, ldz, a, nullptr, 1.0, w))) return st;
+    if ((st = bar_init_red(ctx, red, 2, 1, 1))) return st;
+    if ((st = bar_grad_hess(ctx, n, r, Z, ldz, w, a, C, t, g, dinv, red))) return st;
+    if ((st = bar_dot(ctx, r, w, w, sc))) return st;
+    DB200_CUDA(ctx, cudaMemcpyAsync(red + 8, sc, sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    if ((st = fetch(red, 9))) return st;
+    suma_now = h[0];
+    fa = 0.5 * h[8] - suma_now;
+    if (2.0 * n / t < P.gap_tol * std::fabs(fa)) break;
+    t *= P.mu;
+  }
+  if (outer > P.max_outer) {
+    outer = P.max_outer;
+    status = DB200_ERR_MAXITER;
+  }
+  // primal-dual gap at w = Z^T a (w is current)
+  if ((st = bar_hinge(ctx, n, r, Z, ldz, w, sc + 3))) return st;
+  if ((st = fetch(sc, 4))) return st;
+  const double primal = 0.5 * h[0] + C * h[3];
+  if (rep) {
+    rep->f = fa;
+    rep->t = t;
+    rep->outer = outer;
+    rep->newton = total_newton;
+    rep->gap_barrier = 2.0 * n / t / std::fabs(fa);
+    rep->gap_primal_dual = (primal + fa) / std::fabs(fa);
+    rep->status = status;
+    rep->ms_barrier = timer.stop_ms();
+  }
+  return status == DB200_ERR_MAXITER ? DB200_ERR_MAXITER : DB200_OK;
+}
+
+// ---------------------------------------------------------------------------------------------- low rank
+int lowrank_impl(db200_context* ctx, int n, int d, int l, int q, const float* X, int ldx, const float* y,
+                 const float* Omega, int ldo, float gamma, double* Z, int ldz, db200_svm_report* rep) {
+  if (l > n) return fail(ctx, DB200_ERR_INVALID, "lowrank: l > n");
+  const size_t nl = (size_t)n * l, ll = (size_t)l * l;
+  const size_t bytes = 4096 + 2 * align_up(nl * 4, 256) + align_up(nl * 8, 256) + 3 * align_up(ll * 8, 256) + 4096;
+  char* base = static_cast<char*>(slot_buffer(ctx, SLOT_PIPE, bytes));
+  if (!base) return DB200_ERR_NOMEM;
+  Carve cv{base};
+  int* d_pair = cv.take<int>(4);
+  double* d_scalar = cv.take<double>(4);
+  float* Y32 = cv.take<float>(nl);
+  float* Qf = cv.take<float>(nl);
+  double* Q = cv.take<double>(nl);
+  double* Cm = cv.take<double>(ll);
+  double* R = cv.take<double>(ll);
+  double ms_sketch = 0, ms_orth = 0, ms_core = 0;
+  int st;
+
+  auto sketch = [&](const float* Om, int ldom) -> int {
+    EventTimer tm(ctx->stream);
+    int s2 = db200_rbf_sketch(ctx, n, n, d, l, X, ldx, X, ldx, DB200_POINT_MAJOR, y, y, Om, ldom, Y32, n, gamma);
+    ms_sketch += tm.stop_ms();
+    return s2;
+  };
+  auto orth = [&]() -> int {
+    EventTimer tm(ctx->stream);
+    int s2 = convert<float, double>(ctx, Y32, n, Q, n, n, l);
+    if (!s2) s2 = cholqr2_impl(ctx, n, l, Q, n, nullptr, 0);
+    if (!s2) s2 = convert<double, float>(ctx, Q, n, Qf, n, n, l);
+    ms_orth += tm.stop_ms();
+    return s2;
+  };
+  if ((st = sketch(Omega, ldo))) return st;
+  if ((st = orth())) return st;
+  for (int it = 0; it < q; ++it) {
+    if ((st = sketch(Qf, n))) return st;
+    if ((st = orth())) return st;
+  }
+  if ((st = sketch(Qf, n))) return st;  // Y32 = K Q
+  EventTimer tcore(ctx->stream);
+  // C = Q^T (K Q), symmetrised; R^T R = C + nu I with nu = 1e-7 trace(C)/l, x10 until positive definite
+  if ((st = gram<double, float>(ctx, n, l, l, Q, n, Y32, n, nullptr, 1.0, 0.0, Cm, l, false))) return st;
+  if ((st = symmetrize(ctx, Cm, l, l, 0.0))) return st;
+  if ((st = trace(ctx, Cm, l, l, d_scalar))) return st;
+  double tr = 0;
+  DB200_CUDA(ctx, cudaMemcpyAsync(&tr, d_scalar, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  DB200_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  double nu = 1e-7 * std::max(tr, 1e-300) / l;
+  bool ok = false;
+  for (int tries = 0; tries < 12 && !ok; ++tries) {
+    DB200_CUDA(ctx, cudaMemcpyAsync(R, Cm, sizeof(double) * ll, cudaMemcpyDeviceToDevice, ctx->stream));
+    if ((st = symmetrize(ctx, R, l, l, nu))) return st;
+    DB200_CUDA(ctx, cudaMemsetAsync(d_pair, 0, 2 * sizeof(int), ctx->stream));
+    if ((st = potrf_upper(ctx, R, l, l, d_pair, d_pair + 1))) return st;
+    int pst = 0, bad = 0;
+    if ((st = read_status(ctx, d_pair, &pst, &bad))) return st;
+    if (pst == 0) ok = true;
+    else nu *= 10.0;
+  }
+  if (!ok) return fail(ctx, DB200_ERR_NOT_SPD, "lowrank: Q^T K Q + nu I not positive definite after 12 shifts");
+  // Z = Q R^T
+  if ((st = gemm_tall<double, double>(ctx, n, l, l, Q, n, R, l, true, 0.0, Z, ldz))) return st;
+  ms_core = tcore.stop_ms();
+  if (rep) {
+    rep->nu = nu;
+    rep->ms_sketch = ms_sketch;
+    rep->ms_orth = ms_orth;
+    rep->ms_core = ms_core;
+  }
+  return DB200_OK;
+}
+
+}  // namespace db200
+
+using namespace db200;
+
+extern "C" {
+
+void db200_barrier_defaults(db200_barrier_params* p) {
+  if (!p) return;
+  p->t0 = 1.0;
+  p->mu = 20.0;
+  p->alpha = 0.1;
+  p->beta = 0.5;
+  p->gap_tol = 1e-6;
+  p->newton_tol = 1e-6;
+  p->max_outer = 60;
+  p->max_newton = 200;
+}
+
+int db200_potrf(db200_context* ctx, int n, double* A, int lda, int nb) {
+  if (!ctx) return DB200_ERR_INVALID;
+  if (n < 0 || !A || lda < n) return fail(ctx, DB200_ERR_INVALID, "potrf: bad arguments");
+  if (n == 0) return DB200_OK;
+  int* pair = static_cast<int*>(slot_buffer(ctx, SLOT_SPARE, 256));
+  if (!pair) return DB200_ERR_NOMEM;
+  DB200_CUDA(ctx, cudaMemsetAsync(pair, 0, 2 * sizeof(int), ctx->stream));
+  int st = potrf_upper(ctx, A, lda, n, pair, pair + 1, nb <= 0 ? 64 : nb);
+  if (st) return st;
+  int pst = 0, bad = 0;
+  if ((st = read_status(ctx, pair, &pst, &bad))) return st;
+  if (pst) return fail(ctx, DB200_ERR_NOT_SPD, "potrf: non-positive pivot in the block starting at row " +
+                                                   std::to_string(bad));
+  return DB200_OK;
+}
+
+int db200_cholqr2(db200_context* ctx, int n, int l, double* Y, int ldy, double* R, int ldr) {
+  if (!ctx) return DB200_ERR_INVALID;
+  if (n < l || l < 1 || !Y || ldy < n || (R && ldr < l)) return fail(ctx, DB200_ERR_INVALID, "cholqr2: bad arguments");
+  int st = cholqr2_impl(ctx, n, l, Y, ldy, R, ldr);
+  if (st) return st;
+  return db200_synchronize(ctx);
+}
+
+int db200_gemm_tn(db200_context* ctx, int k, int m, int n, double alpha, const double* A, int lda, const double* B,
+                  int ldb, double beta, double* C, int ldc) {
+  if (!ctx) return DB200_ERR_INVALID;
+  if (k < 0 || m < 0 || n < 0 || !A || !B || !C || lda < k || ldb < k || ldc < m)
+    return fail(ctx, DB200_ERR_INVALID, "gemm_tn: bad arguments");
+  return gram<double, double>(ctx, k, m, n, A, lda, B, ldb, nullptr, alpha, beta, C, ldc, false);
+}
+
+int db200_trsm_lutn(db200_context* ctx, int m, int n, const double* R, int ldr, double* B, int ldb) {
+  if (!ctx) return DB200_ERR_INVALID;
+  if (m < 0 || n < 0 || !R || !B || ldr < m || ldb < m) return fail(ctx, DB200_ERR_INVALID, "trsm: bad arguments");
+  if (m == 0 || n == 0) return DB200_OK;
+  // B <- (R^-1)^T B:  X = R^-1 (triangular inverse), then B = X^T B through the Gram kernel into scratch
+  const size_t bytes = 1024 + align_up((size_t)m * m * 8, 256) + align_up((size_t)m * n * 8, 256);
+  char* base = static_cast<char*>(slot_buffer(ctx, SLOT_SPARE, bytes));
+  if (!base) return DB200_ERR_NOMEM;
+  Carve cv{base};
+  double* Xi = cv.take<double>((size_t)m * m);
+  double* T = cv.take<double>((size_t)m * n);
+  int st = trinv_upper(ctx, R, ldr, m, Xi, m);
+  if (!st) st = gram<double, double>(ctx, m, m, n, Xi, m, B, ldb, nullptr, 1.0, 0.0, T, m, false);
+  if (st) return st;
+  DB200_CUDA(ctx, cudaMemcpy2DAsync(B, sizeof(double) * ldb, T, sizeof(double) * m, sizeof(double) * m, n,
+                                    cudaMemcpyDeviceToDevice, ctx->stream));
+  return db200_synchronize(ctx);
+}
+
+int db200_svm_barrier(db200_context* ctx, int n, int r, const double* Z, int ldz, const float* y, double C,
+                      const db200_barrier_params* p, double* a, db200_svm_report* rep) {
+  if (!ctx) return DB200_ERR_INVALID;
+  if (n < 1 || r < 1 || !Z || ldz < n || !y || !a || !(C > 0)) return fail(ctx, DB200_ERR_INVALID, "svm_barrier: bad arguments");
+  db200_barrier_params P;
+  if (p) P = *p;
+  else db200_barrier_defaults(&P);
+  int st = svm_barrier_impl(ctx, n, r, Z, ldz, y, C, P, a, rep);
+  if (st && st != DB200_ERR_MAXITER) return st;
+  int s2 = db200_synchronize(ctx);
+  return s2 ? s2 : st;
+}
+
+int db200_lowrank(db200_context* ctx, int n, int d, int l, int q, const float* X, int ldx, const float* y,
+                  const float* Omega, int ldo, float gamma, double* Z, int ldz, db200_svm_report* rep) {
+  if (!ctx) return DB200_ERR_INVALID;
+  if (n < 1 || d < 1 || l < 1 || q < 0 || !X || ldx < d || !y || !Omega || ldo < n || !Z || ldz < n)
+    return fail(ctx, DB200_ERR_INVALID, "lowrank: bad arguments");
+  int st = lowrank_impl(ctx, n, d, l, q, X, ldx, y, Omega, ldo, gamma, Z, ldz, rep);
+  if (st) return st;
+  return db200_synchronize(ctx);
+}
+
+int db200_svm_solve(db200_context* ctx, int n, int d, int l, int q, const float* X, int ldx, const float* y,
+                    const float* Omega, int ldo, float gamma, double C, const db200_barrier_params* p, double* a,
+                    double* Z, int ldz, db200_svm_report* rep) {
+  if (!ctx) return DB200_ERR_INVALID;
+  EventTimer total(ctx->stream);
+  db200_svm_report local;
+  std::memset(&local, 0, sizeof(local));
+  int st = db200_lowrank(ctx, n, d, l, q, X, ldx, y, Omega, ldo, gamma, Z, ldz, &local);
+  if (st) return st;
+  st = db200_svm_barrier(ctx, n, l, Z, ldz, y, C, p, a, &local);
+  local.ms_total = total.stop_ms();
+  if (rep) *rep = local;
+  return st;
+}
+
+}  // extern "C"

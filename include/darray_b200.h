@@ -108,6 +108,78 @@ DB200_API int db200_rbf_block(db200_context* ctx, int m, int n, int d, const flo
 DB200_API int db200_lra_host(db200_context* ctx, int n, int d, int k, const float* X, int ldx, const float* Y,
                              const float* O, int ldo, float* A, int lda, float gamma);
 
+/* ------------------------------------------------------------------------------------------------------
+ * Dense FP64 linear algebra on a 1 x 1 DMatrix (device pointers, column major).
+ * ------------------------------------------------------------------------------------------------------ */
+
+/* In-place upper Cholesky A = R^T R of the n x n matrix A (only the upper triangle is read; the strictly lower
+ * part is zeroed), blocked right-looking with block size nb (<= 64; 0 = 64).  A non-positive pivot returns
+ * DB200_ERR_NOT_SPD (db200_last_error names the failing block).  Replaces cholesky_factorize(A, 'U', n, 0, bs)
+ * and cholesky_factorize_recursive (include/lapack_like.h:10-90), in FP64.  Synchronous. */
+DB200_API int db200_potrf(db200_context* ctx, int n, double* A, int lda, int nb);
+
+/* Orthonormalise the tall-skinny Y (n x l, n >= l) in place by CholeskyQR2 (FP64 Gram Y^T Y, Cholesky,
+ * Y <- Y R^-1, twice; falls back to shifted CholeskyQR3 when the first Gram is numerically singular) and
+ * return R (l x l upper, Y_in = Q R, positive diagonal).  Replaces tall_skinny_qr_factorize
+ * (include/lapack_like.h:283-379), which returns R and overwrites A with Q.  Synchronous. */
+DB200_API int db200_cholqr2(db200_context* ctx, int n, int l, double* Y, int ldy, double* R, int ldr);
+
+/* C(m x n) = alpha * A^T B + beta * C with A k x m and B k x n, FP64.  Replaces matrix_multiply("T","N")
+ * (include/blas_like.h:63-93) and multiply_matrix (include/cblas_like.h:40-60). */
+DB200_API int db200_gemm_tn(db200_context* ctx, int k, int m, int n, double alpha, const double* A, int lda,
+                            const double* B, int ldb, double beta, double* C, int ldc);
+
+/* B(m x n) <- U^-T B with U the upper triangle of the m x m matrix R.  Replaces triangular_solve("L","U","T","N")
+ * (include/blas_like.h:96-127). */
+DB200_API int db200_trsm_lutn(db200_context* ctx, int m, int n, const double* R, int ldr, double* B, int ldb);
+
+/* ------------------------------------------------------------------------------------------------------
+ * Kernel SVM: low-rank factor and barrier solve.
+ * ------------------------------------------------------------------------------------------------------ */
+
+/* Barrier-method constants, defaults from tests/testsvm.cpp:228-321 (t0 = 1, mu = 20, alpha = 0.1,
+ * beta = 0.5, Newton stop lambda^2/2 < 1e-6) with the barrier stop 2n/t < gap_tol * |f(a)|, gap_tol = 1e-6. */
+typedef struct db200_barrier_params {
+  double t0, mu, alpha, beta, gap_tol, newton_tol;
+  int max_outer, max_newton;
+} db200_barrier_params;
+
+/* What a solve did and where it ended. */
+typedef struct db200_svm_report {
+  double f;                /* dual objective f(a) = 0.5 a^T Z Z^T a - 1^T a at the returned a */
+  double gap_barrier;      /* 2n/t / |f|: the barrier method's duality-gap bound */
+  double gap_primal_dual;  /* (P(Z^T a) + f(a)) / |f|, P(w) = 0.5|w|^2 + C sum max(0, 1 - z_i.w) */
+  double t;                /* final barrier parameter */
+  double nu;               /* shift of the Nystrom core Cholesky */
+  int outer, newton;       /* barrier and Newton iterations */
+  int status;              /* DB200_OK, DB200_ERR_MAXITER (caps reached) */
+  double ms_sketch, ms_orth, ms_core, ms_barrier, ms_total;
+} db200_svm_report;
+
+DB200_API void db200_barrier_defaults(db200_barrier_params* p);
+
+/* Minimise f(a) = 0.5 a^T Z Z^T a - 1^T a over 0 < a < C by the log-barrier method with Newton steps solved
+ * through Sherman-Morrison-Woodbury on the r x r capacity matrix I + Z^T D^-1 Z (FP64 Cholesky), line search
+ * kept inside the box.  Z: n x r FP64 (labels folded in, z_i = y_i phi(x_i)), y: n labels (float, +-1) for the
+ * class-balanced start of tests/testsvm.cpp:192-212, a: n FP64 output.  Replaces the loop of
+ * tests/testsvm.cpp:228-321 over include/dbarrier.h:14-139 (f, gg, Grad_f, Grad_Phi, Grad, Hess_Phi,
+ * pre_conjgrad).  Synchronous; rep may be NULL. */
+DB200_API int db200_svm_barrier(db200_context* ctx, int n, int r, const double* Z, int ldz, const float* y, double C,
+                                const db200_barrier_params* p, double* a, db200_svm_report* rep);
+
+/* Low-rank factor Z (n x l FP64, Z Z^T ~ diag(y) K diag(y)) by the randomised range finder of
+ * tests/testsvm.cpp:86-170, corrected: Y = K Omega; Q = orth(Y); q times {Y = K Q; Q = orth(Y)};
+ * C = Q^T K Q; R^T R = C + nu I; Z = Q R^T.  K products use the fused kernel (db200_rbf_sketch), orth is
+ * db200_cholqr2.  X point-major (ldx >= d), y and Omega (n x l, ldo >= n) device.  Synchronous. */
+DB200_API int db200_lowrank(db200_context* ctx, int n, int d, int l, int q, const float* X, int ldx, const float* y,
+                            const float* Omega, int ldo, float gamma, double* Z, int ldz, db200_svm_report* rep);
+
+/* The whole path: db200_lowrank followed by db200_svm_barrier (tests/testsvm.cpp:34-329 at one rank).
+ * Outputs a (n, FP64) and Z (n x l FP64).  Synchronous; rep may be NULL. */
+DB200_API int db200_svm_solve(db200_context* ctx, int n, int d, int l, int q, const float* X, int ldx,
+                              const float* y, const float* Omega, int ldo, float gamma, double C,
+                              const db200_barrier_params* p, double* a, double* Z, int ldz, db200_svm_report* rep);
+
 /*
  * Allocation-free fused RBF x sketch.  No counterpart in the reference: it exists for callers that cannot call
  * cudaMalloc -- plugin hosts that own every device allocation and only lend a stream, processes under a hard

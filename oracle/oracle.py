@@ -121,14 +121,32 @@ def householder_qr(Y: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
 
 
 def cholqr2(Y: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
-    """CholeskyQR2: W = Y^T Y, R1 = chol(W), Q1 = Y R1^-1, then once more on Q1.  Returns (Q, R2 R1)."""
+    """CholeskyQR2: W = Y^T Y, R1 = chol(W), Q1 = Y R1^-1, then once more on Q1.  Returns (Q, R2 R1).
+    When the first Gram is numerically singular, shifted CholeskyQR3 (Fukaya et al. 2020): the first pass
+    factors W + s I with s = 11 (n l + l (l + 1)) u trace(W), followed by two plain passes."""
     import scipy.linalg as sl
     Y = np.asarray(Y, F64)
-    R1 = cholesky_upper(Y.T @ Y)
-    Q1 = sl.solve_triangular(R1, Y.T, trans="T", lower=False).T
-    R2 = cholesky_upper(Q1.T @ Q1)
-    Q = sl.solve_triangular(R2, Q1.T, trans="T", lower=False).T
-    return Q, R2 @ R1
+    n, l = Y.shape
+
+    def one(A, shift=0.0):
+        W = A.T @ A
+        if shift:
+            W = W + shift * np.trace(W) * np.eye(l)
+        R = cholesky_upper(W)
+        return sl.solve_triangular(R, A.T, trans="T", lower=False).T, R
+
+    try:
+        Q1, R1 = one(Y)
+        shifted = False
+    except np.linalg.LinAlgError:
+        Q1, R1 = one(Y, 11.0 * (n * l + l * (l + 1)) * np.finfo(F64).eps / 2)
+        shifted = True
+    Q, R2 = one(Q1)
+    R = R2 @ R1
+    if shifted:
+        Q, R3 = one(Q)
+        R = R3 @ R
+    return Q, R
 
 
 def sign_fix(Q: np.ndarray, R: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
