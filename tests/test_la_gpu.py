@@ -1,0 +1,137 @@
+"""FP64 dense linear algebra on the GPU (through the C ABI) against the FP64 oracle and the reference's own
+known answers.  Tolerances: FP64 results agree with numpy/LAPACK to relative 1e-11 (Cholesky, GEMM, TRSM) and
+CholeskyQR2 gives Q^T Q = I to 1e-13; against the reference's FP32 outputs (tests/golden) the bar is 1e-4."""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from darray_optimizer_b200._lib import DB200Error
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+G = np.load(Path(__file__).resolve().parent / "golden" / "reference_goldens.npz")
+
+
+def d64(a):
+    """column-major FP64 device copy of a 2-D array (torch tensor shaped (cols, rows))."""
+    import torch
+    a = np.asarray(a, np.float64)
+    return torch.from_numpy(np.ascontiguousarray(a.T)).cuda()
+
+
+def h64(t, m):
+    return np.asfortranarray(t.cpu().numpy()[:, :m].T)
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("nb", [64, 32, 17])
+def test_potrf_known_answer_min_matrix(gpu_ctx, nb):
+    # perftests/perftest_cholesky.cpp:46-84: chol(min(i+1, j+1)) = ones-upper; the reference checks A[n-1,n-1] == 1
+    A = G["chol_min_A"].astype(np.float64)
+    n = A.shape[0]
+    dA = d64(A)
+    gpu_ctx.potrf(n, dA.data_ptr(), n, nb)
+    R = h64(dA, n)
+    assert np.max(np.abs(R - np.triu(np.ones((n, n))))) < 1e-12
+    assert abs(R[n - 1, n - 1] - 1.0) < 1e-12
+    assert np.max(np.abs(R - G["chol_min_R_blocked"])) < 1e-4  # the reference's own FP32 factor
+
+
+@pytest.mark.parametrize("n", [10, 200, 528, 1040])
+def test_potrf_matches_oracle(gpu_ctx, n):
+    g = np.random.default_rng(n)
+    B = g.standard_normal((n, n))
+    A = B @ B.T / n + np.eye(n)
+    dA = d64(A)
+    gpu_ctx.potrf(n, dA.data_ptr(), n)
+    R = h64(dA, n)
+    assert rel(R, O.cholesky_upper(A)) < 1e-11
+    assert np.all(np.tril(R, -1) == 0)
+
+
+def test_potrf_test3_factor_and_reference(gpu_ctx):
+    A = G["chol_test3_A"].astype(np.float64)
+    dA = d64(A)
+    gpu_ctx.potrf(10, dA.data_ptr(), 10, 4)
+    assert rel(h64(dA, 10), G["chol_test3_R"].astype(np.float64)) < 1e-5
+
+
+def test_potrf_not_spd_reports_error(gpu_ctx):
+    A = np.eye(70)
+    A[40, 40] = -1.0
+    dA = d64(A)
+    with pytest.raises(DB200Error) as ei:
+        gpu_ctx.potrf(70, dA.data_ptr(), 70)
+    assert ei.value.status == -3  # DB200_ERR_NOT_SPD
+
+
+@pytest.mark.parametrize("n,l", [(5000, 138), (20000, 528), (500, 20)])
+def test_cholqr2_matches_oracle(gpu_ctx, n, l):
+    g = np.random.default_rng(l)
+    Y = g.standard_normal((n, l)) @ np.diag(np.logspace(0, -4, l))
+    dY = d64(Y)
+    dR = d64(np.zeros((l, l)))
+    gpu_ctx.cholqr2(n, l, dY.data_ptr(), n, dR.data_ptr(), l)
+    Q, R = h64(dY, n), h64(dR, l)
+    Qo, Ro = O.cholqr2(Y)
+    assert np.max(np.abs(Q.T @ Q - np.eye(l))) < 1e-13
+    assert rel(Q, Qo) < 1e-10 and rel(R, Ro) < 1e-10
+    assert rel(Q @ R, Y) < 1e-13
+
+
+def test_cholqr2_matches_reference_tsqr(gpu_ctx):
+    # tall_skinny_qr_factorize of the reference (FP32 Householder): same Q and R up to signs
+    A = G["tsqr_A"].astype(np.float64)
+    n, l = A.shape
+    dY = d64(A)
+    dR = d64(np.zeros((l, l)))
+    gpu_ctx.cholqr2(n, l, dY.data_ptr(), n, dR.data_ptr(), l)
+    Qr, Rr = O.sign_fix(G["tsqr_Q"].astype(np.float64), G["tsqr_R"].astype(np.float64))
+    assert rel(h64(dY, n), Qr) < 1e-5 and rel(h64(dR, l), Rr) < 1e-5
+
+
+def test_cholqr2_ill_conditioned_uses_shifted_variant(gpu_ctx):
+    n, l = 4000, 60
+    g = np.random.default_rng(1)
+    U, _ = np.linalg.qr(g.standard_normal((n, l)))
+    V, _ = np.linalg.qr(g.standard_normal((l, l)))
+    Y = U @ np.diag(np.logspace(0, -11, l)) @ V.T  # cond 1e11: the plain Gram is singular in FP64
+    dY = d64(Y)
+    dR = d64(np.zeros((l, l)))
+    gpu_ctx.cholqr2(n, l, dY.data_ptr(), n, dR.data_ptr(), l)
+    Q, R = h64(dY, n), h64(dR, l)
+    assert np.max(np.abs(Q.T @ Q - np.eye(l))) < 1e-12
+    assert rel(Q @ R, Y) < 1e-12
+    Qo, Ro = O.cholqr2(Y)
+    assert np.max(np.abs(Qo.T @ Qo - np.eye(l))) < 1e-12
+
+
+def test_gemm_tn_matches_oracle_and_reference(gpu_ctx):
+    A, B, C = (G[k].astype(np.float64) for k in ("mm_A", "mm_B", "mm_C"))
+    k, m = A.shape
+    n = B.shape[1]
+    dA, dB, dC = d64(A), d64(B), d64(C)
+    gpu_ctx.gemm_tn(k, m, n, -1.0, dA.data_ptr(), k, dB.data_ptr(), k, 1.0, dC.data_ptr(), m)
+    gpu_ctx.sync()
+    out = h64(dC, m)
+    assert rel(out, O.matmul_tn(A, B, C, alpha=-1.0, beta=1.0)) < 1e-13
+    assert rel(out, G["mm_out"].astype(np.float64)) < 1e-5
+
+
+@pytest.mark.parametrize("m,n", [(64, 7), (300, 41)])
+def test_trsm_lutn_matches_oracle(gpu_ctx, m, n):
+    g = np.random.default_rng(m)
+    U = np.triu(g.standard_normal((m, m))) + 8 * np.eye(m)
+    B = g.standard_normal((m, n))
+    dU, dB = d64(U), d64(B)
+    gpu_ctx.trsm_lutn(m, n, dU.data_ptr(), m, dB.data_ptr(), m)
+    assert rel(h64(dB, m), O.trsm_lutn(U, B)) < 1e-12
+    if m == 64:
+        dU2, dB2 = d64(G["trsm_U"]), d64(G["trsm_B"])
+        gpu_ctx.trsm_lutn(64, 7, dU2.data_ptr(), 64, dB2.data_ptr(), 64)
+        assert rel(h64(dB2, 64), G["trsm_X"].astype(np.float64)) < 1e-5
