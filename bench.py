@@ -104,34 +104,21 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------------------------------ distributed plumbing
+# One process per GPU, independent replicas: darray_optimizer_b200.replicas (NCCL barrier and max-over-ranks).
 def dist_init(n_gpus):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
-        import torch
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
-    return world, rank, local
+    from darray_optimizer_b200 import replicas
+    r = replicas.init()
+    return r.world, r.rank, r.local, r
 
 
-def barrier(world):
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
+def barrier(r):
+    from darray_optimizer_b200 import replicas
+    replicas.barrier(r)
 
 
-def all_max(x, world):
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+def all_max(x, r):
+    from darray_optimizer_b200 import replicas
+    return replicas.all_max(r, x)
 
 
 # ------------------------------------------------------------------------------------------ CPU baseline
@@ -164,8 +151,10 @@ def cpu_sample(w, Om, rows: int, seconds: float):
 
 
 def run_reference(args):
-    world, rank, _ = dist_init(args.gpus)
+    world, rank, _, rep = dist_init(args.gpus)
     if rank != 0:
+        from darray_optimizer_b200 import replicas
+        replicas.finalize(rep)
         return 0
     from darray_optimizer_b200 import datagen
     w = datagen.uniform_hyperplane(n=N_POINTS, d=D_FEAT)
@@ -189,13 +178,15 @@ def run_reference(args):
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+    from darray_optimizer_b200 import replicas
+    replicas.finalize(rep)
     return 0
 
 
 # ------------------------------------------------------------------------------------------ our arm
 def run_ours(args):
     import torch
-    world, rank, local = dist_init(args.gpus)
+    world, rank, local, rep = dist_init(args.gpus)
     torch.cuda.set_device(local)
     from darray_optimizer_b200 import datagen
     from darray_optimizer_b200._lib import Context
@@ -222,7 +213,7 @@ def run_ours(args):
     sampler = ClockSampler(local)
     sampler.start()
     time.sleep(0.3)
-    barrier(world)
+    barrier(rep)
     torch.cuda.synchronize()
     launches0 = ctx.launches()
     ctx.profile(True)
@@ -235,23 +226,69 @@ def run_ours(args):
     torch.cuda.synchronize()
     kernel_ms, kernel_count = ctx.profile_read()
     ctx.profile(False)
-    barrier(world)
+    barrier(rep)
     clocks = sampler.stop()
     launches = ctx.launches() - launches0
     ms = e0.elapsed_time(e1)
-    ms_max = all_max(ms, world)
+    ms_max = all_max(ms, rep)
     F = flops(n, d, l)
     value = world * F * args.steps / (ms_max / 1e3) / 1e12
 
     # end to end through the host-pointer LRA entry point (pinned host buffers, copies inside the timed region)
     e2e_val = h2d = d2h = None
     if not args.no_e2e:
-        e2e_val, h2d, d2h = e2e_run(ctx, w, Om, world, args.steps)
-    return finish(args, ctx, w, world, rank, ms_max, kernel_ms, kernel_count, launches, clocks, e2e_val, h2d, d2h,
-                  Om)
+        e2e_val, h2d, d2h = e2e_run(ctx, w, Om, rep, args.steps)
+    solve = None
+    if not args.no_solve and rank == 0:
+        solve = solve_run(ctx, w, X, y, O, args.n_test)
+    return finish(args, ctx, w, rep, ms_max, kernel_ms, kernel_count, launches, clocks, e2e_val, h2d, d2h, Om,
+                  solve)
 
 
-def e2e_run(ctx, w, Om, world, steps):
+def solve_run(ctx, w, X, y, O, n_test):
+    """The whole SVM path (db200_svm_solve: 3 kernel passes, CholeskyQR2, Nystrom core, barrier to gap 1e-6) in the
+    mixed precision and in the plain FP64 comparator, with held-out accuracy of both models."""
+    import torch
+    from darray_optimizer_b200 import datagen
+    n, d, l = w.n, w.d, w.l
+    Xt, yt = datagen.held_out(w, n_test)
+    dXt = torch.from_numpy(Xt).cuda()
+    out = {"workload": f"SVM solve to duality gap 1e-6 (n={n}, d={d}, l={l}, q={w.power_iters}, C={w.C})",
+           "n_test": n_test}
+
+    def one(precision):
+        Z = torch.zeros((l, n), dtype=torch.float64, device="cuda")
+        a = torch.zeros(n, dtype=torch.float64, device="cuda")
+        p = ctx.barrier_params(precision=precision)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rep = ctx.svm_solve(n, d, l, w.power_iters, X.data_ptr(), d, y.data_ptr(), O.data_ptr(), n, w.gamma, w.C,
+                            a.data_ptr(), Z.data_ptr(), n, params=p)
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t0
+        # held-out decision values sum_j a_j y_j K(x_t, x_j) through the FP64 kernel pass
+        dec = torch.zeros(n_test, dtype=torch.float64, device="cuda")
+        ctx.rbf_sketch_f64(n_test, n, d, 1, dXt.data_ptr(), d, X.data_ptr(), d, 0, y.data_ptr(), a.data_ptr(), n,
+                           dec.data_ptr(), n_test, w.gamma)
+        ctx.sync()
+        acc = float(np.mean(np.sign(dec.cpu().numpy()) == yt))
+        return el, rep, acc
+
+    one(0)  # warm-up: workspace growth, module load
+    t_mixed, rep_m, acc_m = one(0)
+    t_fp64, rep_f, acc_f = one(1)
+    out.update({"mixed_s": t_mixed, "fp64_s": t_fp64, "speedup_vs_fp64": t_fp64 / t_mixed,
+                "f_mixed": rep_m.f, "f_fp64": rep_f.f, "rel_f_diff": abs(rep_m.f - rep_f.f) / abs(rep_f.f),
+                "gap_pd_mixed": rep_m.gap_primal_dual, "gap_pd_fp64": rep_f.gap_primal_dual,
+                "gap_barrier_mixed": rep_m.gap_barrier, "gap_barrier_fp64": rep_f.gap_barrier,
+                "newton_mixed": rep_m.newton, "newton_fp64": rep_f.newton, "refine_mixed": rep_m.refine,
+                "acc_mixed": acc_m, "acc_fp64": acc_f,
+                "phases_ms_mixed": {k: getattr(rep_m, k) for k in ("ms_sketch", "ms_orth", "ms_core", "ms_barrier")},
+                "phases_ms_fp64": {k: getattr(rep_f, k) for k in ("ms_sketch", "ms_orth", "ms_core", "ms_barrier")}})
+    return out
+
+
+def e2e_run(ctx, w, Om, rep, steps):
     import torch
     n, d, l = w.n, w.d, w.l
     F = flops(n, d, l)
@@ -264,19 +301,21 @@ def e2e_run(ctx, w, Om, world, steps):
         ctx.lra_host(n, d, l, Xh.data_ptr(), d, yh.data_ptr(), Oh.data_ptr(), n, Ah.data_ptr(), n, w.gamma)
 
     e2e_step()
-    barrier(world)
+    barrier(rep)
     t0 = time.perf_counter()
     k2 = max(1, steps)
     for _ in range(k2):
         e2e_step()
-    e2e_s = all_max(time.perf_counter() - t0, world)
-    e2e_val = world * F * k2 / e2e_s / 1e12
+    e2e_s = all_max(time.perf_counter() - t0, rep)
+    e2e_val = rep.world * F * k2 / e2e_s / 1e12
     h2d = Xh.numel() * 4 + yh.numel() * 4 + Oh.numel() * 4
     d2h = Ah.numel() * 4
     return e2e_val, h2d, d2h
 
 
-def finish(args, ctx, w, world, rank, ms_max, kernel_ms, kernel_count, launches, clocks, e2e_val, h2d, d2h, Om):
+def finish(args, ctx, w, rep, ms_max, kernel_ms, kernel_count, launches, clocks, e2e_val, h2d, d2h, Om,
+           solve=None):
+    world, rank = rep.world, rep.rank
     n, d, l = w.n, w.d, w.l
     F = flops(n, d, l)
     value = world * F * args.steps / (ms_max / 1e3) / 1e12
@@ -305,15 +344,16 @@ def finish(args, ctx, w, world, rank, ms_max, kernel_ms, kernel_count, launches,
             "config": config({"parallelism": f"replicas x{world}", "n": n}), "clocks": clocks,
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches, "roofline": roof}
+    if solve is not None:
+        line["solve"] = solve
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, desc, threads = cpu_sample(w, Om, 256, args.cpu_seconds)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc}
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    from darray_optimizer_b200 import replicas
+    replicas.finalize(rep)
     return 0
 
 
@@ -326,6 +366,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg (profiling runs)")
+    ap.add_argument("--no-solve", action="store_true", help="skip the whole-solve leg (mixed vs plain FP64)")
+    ap.add_argument("--n-test", type=int, default=16384, help="held-out points for the solve leg's accuracy")
     ap.add_argument("--n", type=int, default=N_POINTS, help="points (default: the C2 workload, 131072)")
     args = ap.parse_args()
     if args.impl == "reference":

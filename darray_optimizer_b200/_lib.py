@@ -22,13 +22,15 @@ _i64 = ctypes.c_int64
 class BarrierParams(ctypes.Structure):
     _fields_ = [("t0", ctypes.c_double), ("mu", ctypes.c_double), ("alpha", ctypes.c_double),
                 ("beta", ctypes.c_double), ("gap_tol", ctypes.c_double), ("newton_tol", ctypes.c_double),
-                ("max_outer", ctypes.c_int), ("max_newton", ctypes.c_int)]
+                ("max_outer", ctypes.c_int), ("max_newton", ctypes.c_int), ("precision", ctypes.c_int),
+                ("refine_max", ctypes.c_int)]
 
 
 class SvmReport(ctypes.Structure):
     _fields_ = [("f", ctypes.c_double), ("gap_barrier", ctypes.c_double), ("gap_primal_dual", ctypes.c_double),
                 ("t", ctypes.c_double), ("nu", ctypes.c_double), ("outer", ctypes.c_int), ("newton", ctypes.c_int),
-                ("status", ctypes.c_int), ("ms_sketch", ctypes.c_double), ("ms_orth", ctypes.c_double),
+                ("status", ctypes.c_int), ("refine", ctypes.c_int), ("fallbacks", ctypes.c_int),
+                ("ms_sketch", ctypes.c_double), ("ms_orth", ctypes.c_double),
                 ("ms_core", ctypes.c_double), ("ms_barrier", ctypes.c_double), ("ms_total", ctypes.c_double)]
 
     def as_dict(self):
@@ -57,11 +59,31 @@ SIGNATURES = {
     "db200_barrier_defaults": (None, [ctypes.POINTER(BarrierParams)]),
     "db200_svm_barrier": (_c_int, [_vp, _c_int, _c_int, _vp, _c_int, _vp, _c_double, ctypes.POINTER(BarrierParams),
                                    _vp, ctypes.POINTER(SvmReport)]),
-    "db200_lowrank": (_c_int, [_vp, _c_int, _c_int, _c_int, _c_int, _vp, _c_int, _vp, _vp, _c_int, _c_float, _vp,
-                               _c_int, ctypes.POINTER(SvmReport)]),
+    "db200_lowrank": (_c_int, [_vp, _c_int, _c_int, _c_int, _c_int, _vp, _c_int, _vp, _vp, _c_int, _c_float, _c_int,
+                               _vp, _c_int, ctypes.POINTER(SvmReport)]),
+    "db200_gram_weighted": (_c_int, [_vp, _c_int, _c_int, _vp, _c_int, _vp, _vp, _c_int, _c_int]),
+    "db200_rbf_sketch_f64": (_c_int, [_vp, _c_int, _c_int, _c_int, _c_int, _vp, _c_int, _vp, _c_int, _vp, _vp, _vp,
+                                      _c_int, _vp, _c_int, _c_double]),
     "db200_svm_solve": (_c_int, [_vp, _c_int, _c_int, _c_int, _c_int, _vp, _c_int, _vp, _vp, _c_int, _c_float,
                                  _c_double, ctypes.POINTER(BarrierParams), _vp, _vp, _c_int,
                                  ctypes.POINTER(SvmReport)]),
+    "db200_default_context": (_vp, []),
+    "db200_release_default_context": (_c_int, []),
+    "db200_malloc": (_c_int, [_vp, ctypes.c_size_t, ctypes.POINTER(_vp)]),
+    "db200_free": (_c_int, [_vp, _vp]),
+    "db200_copy_to_device": (_c_int, [_vp, _vp, _vp, ctypes.c_size_t]),
+    "db200_copy_to_host": (_c_int, [_vp, _vp, _vp, ctypes.c_size_t]),
+    "db200_gemm": (_c_int, [_vp, ctypes.c_char, ctypes.c_char, _c_int, _c_int, _c_int, _c_double, _vp, _c_int, _vp,
+                            _c_int, _c_double, _vp, _c_int]),
+    "db200_sgemm": (_c_int, [_vp, ctypes.c_char, ctypes.c_char, _c_int, _c_int, _c_int, _c_float, _vp, _c_int, _vp,
+                             _c_int, _c_float, _vp, _c_int]),
+    "db200_svd_values": (_c_int, [_vp, _c_int, _vp, _c_int, _vp]),
+    "db200_knorm": (_c_int, [_vp, _c_int, _c_int, _c_int, _vp, _c_int, _vp, _vp, _c_int, _c_float,
+                             ctypes.POINTER(_c_double)]),
+    "db200_woodbury_solve": (_c_int, [_vp, _c_int, _c_int, _vp, _c_int, _vp, _vp, _vp]),
+    "db200_vec_update": (_c_int, [_vp, _c_int, _c_double, _vp, _c_double, _vp, _c_double]),
+    "db200_barrier_terms": (_c_int, [_vp, _c_int, _c_int, _vp, _c_int, _vp, _c_double, _c_double, _vp, _vp, _vp, _vp,
+                                     ctypes.POINTER(_c_double)]),
     "db200_rbf_sketch_noalloc": (_c_int, [_vp, _c_int, _c_int, _c_int, _c_int, _vp, _c_int, _vp, _c_int, _c_int, _vp,
                                           _vp, _vp, _c_int, _vp, _c_int, _c_float]),
 }
@@ -86,7 +108,7 @@ class DB200Error(RuntimeError):
 def header_functions() -> list[str]:
     """Names of every function declared in include/darray_b200.h."""
     text = HEADER.read_text()
-    return sorted(set(re.findall(r"^\s*(?:DB200_API\s+)?(?:int|void|const char\s*\*|void\s*\*|int64_t)\s*\*?\s*(db200_\w+)\s*\(",
+    return sorted(set(re.findall(r"^\s*(?:DB200_API\s+)?(?:int|void|const char\s*\*|void\s*\*|int64_t|db200_context\s*\*)\s*\*?\s*(db200_\w+)\s*\(",
                                  text, flags=re.M)))
 
 
@@ -193,10 +215,18 @@ class Context:
             self.check(st)
         return rep
 
-    def lowrank(self, n, d, l, q, X, ldx, y, Om, ldo, gamma, Z, ldz):
+    def lowrank(self, n, d, l, q, X, ldx, y, Om, ldo, gamma, Z, ldz, precision=0):
         rep = SvmReport()
-        self.check(self.lib.db200_lowrank(self.h, n, d, l, q, X, ldx, y, Om, ldo, gamma, Z, ldz, ctypes.byref(rep)))
+        self.check(self.lib.db200_lowrank(self.h, n, d, l, q, X, ldx, y, Om, ldo, gamma, precision, Z, ldz,
+                                          ctypes.byref(rep)))
         return rep
+
+    def gram_weighted(self, n, r, Z, ldz, w, M, ldm, use_tensor_cores):
+        return self.check(self.lib.db200_gram_weighted(self.h, n, r, Z, ldz, w, M, ldm, int(use_tensor_cores)))
+
+    def rbf_sketch_f64(self, m, n, d, l, Xi, ldxi, Xj, ldxj, yi, yj, Om, ldo, Y, ldy, gamma):
+        return self.check(self.lib.db200_rbf_sketch_f64(self.h, m, n, d, l, Xi, ldxi, Xj, ldxj, yi, yj, Om, ldo, Y,
+                                                        ldy, gamma))
 
     def svm_solve(self, n, d, l, q, X, ldx, y, Om, ldo, gamma, C, a, Z, ldz, params=None):
         rep = SvmReport()
@@ -204,6 +234,30 @@ class Context:
         self.check(self.lib.db200_svm_solve(self.h, n, d, l, q, X, ldx, y, Om, ldo, gamma, C, ctypes.byref(p), a, Z,
                                             ldz, ctypes.byref(rep)))
         return rep
+
+    def gemm(self, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc):
+        return self.check(self.lib.db200_gemm(self.h, ta.encode(), tb.encode(), m, n, k, alpha, A, lda, B, ldb, beta,
+                                              C, ldc))
+
+    def sgemm(self, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc):
+        return self.check(self.lib.db200_sgemm(self.h, ta.encode(), tb.encode(), m, n, k, alpha, A, lda, B, ldb,
+                                               beta, C, ldc))
+
+    def svd_values(self, n, A, lda, S):
+        return self.check(self.lib.db200_svd_values(self.h, n, A, lda, S))
+
+    def knorm(self, n, d, k, X, ldx, y, Z, ldz, gamma):
+        out = (_c_double * 3)()
+        self.check(self.lib.db200_knorm(self.h, n, d, k, X, ldx, y, Z, ldz, gamma, out))
+        return tuple(out)
+
+    def woodbury_solve(self, n, r, Z, ldz, diag, b, x):
+        return self.check(self.lib.db200_woodbury_solve(self.h, n, r, Z, ldz, diag, b, x))
+
+    def barrier_terms(self, n, k, Z, ldz, a, C, t, gradf, gradphi, grad, D):
+        fg = (_c_double * 2)()
+        self.check(self.lib.db200_barrier_terms(self.h, n, k, Z, ldz, a, C, t, gradf, gradphi, grad, D, fg))
+        return fg[0], fg[1]
 
     def rbf_block(self, m, n, d, Xi, ldxi, Xj, ldxj, layout, yi, yj, K, ldk, gamma):
         return self.check(self.lib.db200_rbf_block(self.h, m, n, d, Xi, ldxi, Xj, ldxj, layout, yi, yj, K, ldk,

@@ -62,7 +62,30 @@ def build(verbose: bool = False, force: bool = False) -> Path:
         if r.returncode != 0:
             sys.stderr.write(r.stdout + r.stderr)
             raise RuntimeError("nvcc link failed")
+    build_cpp_tests(verbose)
     return LIB
+
+
+CPP_TESTS = [ROOT / "tests" / "cpp" / "test_dropin.cpp"]
+CPP_BIN = ROOT / "tests" / "cpp" / "_bin"
+
+
+def build_cpp_tests(verbose: bool = False) -> None:
+    """Compile the C++ drop-in tests (host code over include/darray_b200/ and the C ABI) next to their sources."""
+    CPP_BIN.mkdir(exist_ok=True)
+    hdr_time = _newest(HEADERS)
+    for src in CPP_TESTS:
+        out = CPP_BIN / src.stem
+        if out.exists() and out.stat().st_mtime >= max(src.stat().st_mtime, hdr_time, LIB.stat().st_mtime):
+            continue
+        cmd = ["g++", "-O2", "-std=c++17", f"-I{ROOT / 'include'}", str(src), "-o", str(out), f"-L{LIBDIR}",
+               "-ldarray_b200", "-Wl,-rpath,$ORIGIN/../../../darray_optimizer_b200/lib"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError(f"g++ failed on {src.name}")
 
 
 if __name__ == "__main__":

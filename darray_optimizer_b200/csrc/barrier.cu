@@ -171,6 +171,83 @@ __global__ void __launch_bounds__(THREADS) linesearch_kernel(int n, const double
   block_sum_add<2 * T>(sums, out);
 }
 
+// gradf = Z w - 1, gradphi = (-1/a + 1/(C-a))/t, grad = gradf + gradphi, D = (1/a^2 + 1/(C-a)^2)/t
+// (include/dbarrier.h:48-81 one by one); red: [0] += sum a, [1] += sum(log a + log(C - a)).
+__global__ void __launch_bounds__(THREADS) terms_kernel(int n, int r, const double* __restrict__ Z, long long ld,
+                                                        const double* __restrict__ w, const double* __restrict__ a,
+                                                        double C, double t, double* gf, double* gp, double* g,
+                                                        double* D, double* red) {
+  __shared__ double sw[MAX_R_SMEM];
+  for (int k = threadIdx.x; k < r; k += blockDim.x) sw[k] = w[k];
+  __syncthreads();
+  double sums[2] = {0.0, 0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double ai = a[i], ci = C - ai;
+    const double f1 = row_dot(Z, ld, i, r, sw) - 1.0;
+    const double p1 = ((-1.0 / ai) + (1.0 / ci)) / t;
+    gf[i] = f1;
+    gp[i] = p1;
+    g[i] = f1 + p1;
+    D[i] = ((1.0 / (ai * ai)) + (1.0 / (ci * ci))) / t;
+    sums[0] += ai;
+    sums[1] += log(ai) + log(ci);
+  }
+  block_sum_add<2>(sums, red);
+}
+
+// Negated residual of the Newton system (Z Z^T + D) s = -g:  res = g + Z v + s / dinv  with v = Z^T s.
+// red: [0] += |res|^2, [1] += |g|^2.
+__global__ void __launch_bounds__(THREADS) residual_kernel(int n, int r, const double* __restrict__ Z, long long ld,
+                                                           const double* __restrict__ v, const double* __restrict__ g,
+                                                           const double* __restrict__ dinv,
+                                                           const double* __restrict__ s, double* __restrict__ res,
+                                                           double* red) {
+  __shared__ double sv[MAX_R_SMEM];
+  for (int k = threadIdx.x; k < r; k += blockDim.x) sv[k] = v[k];
+  __syncthreads();
+  double sums[2] = {0.0, 0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double gi = g[i];
+    const double ri = gi + row_dot(Z, ld, i, r, sv) + s[i] / dinv[i];
+    res[i] = ri;
+    sums[0] += ri * ri;
+    sums[1] += gi * gi;
+  }
+  block_sum_add<2>(sums, red);
+}
+
+// Line-search inputs for a direction s: red [0] += g.s, [1] += sum s, [2] min feasible step (init DBL_MAX).
+__global__ void __launch_bounds__(THREADS) step_stats_kernel(int n, const double* __restrict__ g,
+                                                             const double* __restrict__ s,
+                                                             const double* __restrict__ a, double C, double* red) {
+  double sums[2] = {0.0, 0.0};
+  double tmax = DBL_MAX;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double si = s[i], ai = a[i];
+    sums[0] += g[i] * si;
+    sums[1] += si;
+    if (si < 0.0) tmax = fmin(tmax, -ai / si);
+    else if (si > 0.0) tmax = fmin(tmax, (C - ai) / si);
+  }
+  block_sum_add<2>(sums, red);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) tmax = fmin(tmax, __shfl_xor_sync(0xffffffffu, tmax, o));
+  if (threadIdx.x % 32 == 0) atomic_min_pos(red + 2, tmax);
+}
+
+__global__ void reciprocal_kernel(int n, const double* x, double* y) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = 1.0 / x[i];
+}
+
+__global__ void vec_update_kernel(int n, double alpha, const double* x, double beta, double* y, double gamma) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    y[i] = (x ? alpha * x[i] : 0.0) + (beta != 0.0 ? beta * y[i] : 0.0) + gamma;
+}
+
+__global__ void negate_kernel(int n, const double* x, double* y) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = -x[i];
+}
+
 __global__ void axpy_kernel(int n, double alpha, const double* __restrict__ x, double* __restrict__ y) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = fma(alpha, x[i], y[i]);
 }
@@ -185,6 +262,10 @@ __global__ void __launch_bounds__(THREADS) hinge_kernel(int n, int r, const doub
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     sums[0] += fmax(0.0, 1.0 - row_dot(Z, ld, i, r, sw));
   block_sum_add<1>(sums, red);
+}
+
+__global__ void scale_diag_kernel(double* M, int ldm, int r, double factor) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < r; i += gridDim.x * blockDim.x) M[(long long)i * ldm + i] *= factor;
 }
 
 __global__ void add_identity_kernel(double* M, int ldm, int r) {
@@ -260,6 +341,52 @@ int bar_linesearch16(db200_context* ctx, int n, const double* a, const double* s
   return DB200_OK;
 }
 
+int bar_terms(db200_context* ctx, int n, int r, const double* Z, long long ld, const double* w, const double* a,
+              double C, double t, double* gf, double* gp, double* g, double* D, double* red) {
+  if (r > MAX_R_SMEM) return fail(ctx, DB200_ERR_UNSUPPORTED, "barrier: rank > 4096");
+  terms_kernel<<<rows_grid(ctx, n), THREADS, 0, ctx->stream>>>(n, r, Z, ld, w, a, C, t, gf, gp, g, D, red);
+  DB200_CUDA(ctx, cudaGetLastError());
+  count_launch(ctx);
+  return DB200_OK;
+}
+
+int bar_residual(db200_context* ctx, int n, int r, const double* Z, long long ld, const double* v, const double* g,
+                 const double* dinv, const double* s, double* res, double* red) {
+  residual_kernel<<<rows_grid(ctx, n), THREADS, 0, ctx->stream>>>(n, r, Z, ld, v, g, dinv, s, res, red);
+  DB200_CUDA(ctx, cudaGetLastError());
+  count_launch(ctx);
+  return DB200_OK;
+}
+
+int bar_step_stats(db200_context* ctx, int n, const double* g, const double* s, const double* a, double C,
+                   double* red) {
+  step_stats_kernel<<<rows_grid(ctx, n), THREADS, 0, ctx->stream>>>(n, g, s, a, C, red);
+  DB200_CUDA(ctx, cudaGetLastError());
+  count_launch(ctx);
+  return DB200_OK;
+}
+
+int bar_reciprocal(db200_context* ctx, int n, const double* x, double* y) {
+  reciprocal_kernel<<<rows_grid(ctx, n), THREADS, 0, ctx->stream>>>(n, x, y);
+  DB200_CUDA(ctx, cudaGetLastError());
+  count_launch(ctx);
+  return DB200_OK;
+}
+
+int bar_vec_update(db200_context* ctx, int n, double alpha, const double* x, double beta, double* y, double gamma) {
+  vec_update_kernel<<<rows_grid(ctx, n), THREADS, 0, ctx->stream>>>(n, alpha, x, beta, y, gamma);
+  DB200_CUDA(ctx, cudaGetLastError());
+  count_launch(ctx);
+  return DB200_OK;
+}
+
+int bar_negate(db200_context* ctx, int n, const double* x, double* y) {
+  negate_kernel<<<rows_grid(ctx, n), THREADS, 0, ctx->stream>>>(n, x, y);
+  DB200_CUDA(ctx, cudaGetLastError());
+  count_launch(ctx);
+  return DB200_OK;
+}
+
 int bar_axpy(db200_context* ctx, int n, double alpha, const double* x, double* y) {
   axpy_kernel<<<rows_grid(ctx, n), THREADS, 0, ctx->stream>>>(n, alpha, x, y);
   DB200_CUDA(ctx, cudaGetLastError());
@@ -277,6 +404,13 @@ int bar_hinge(db200_context* ctx, int n, int r, const double* Z, long long ld, c
 
 int bar_add_identity(db200_context* ctx, double* M, int ldm, int r) {
   add_identity_kernel<<<(r + 255) / 256, 256, 0, ctx->stream>>>(M, ldm, r);
+  DB200_CUDA(ctx, cudaGetLastError());
+  count_launch(ctx);
+  return DB200_OK;
+}
+
+int bar_scale_diag(db200_context* ctx, double* M, int ldm, int r, double factor) {
+  scale_diag_kernel<<<(r + 255) / 256, 256, 0, ctx->stream>>>(M, ldm, r, factor);
   DB200_CUDA(ctx, cudaGetLastError());
   count_launch(ctx);
   return DB200_OK;

@@ -20,9 +20,28 @@ int bar_gemv_t(db200_context* ctx, int n, int r, const double* Z, long long ld, 
 int bar_linesearch16(db200_context* ctx, int n, const double* a, const double* s, double C, const double* taus,
                      double* out);
 int bar_axpy(db200_context* ctx, int n, double alpha, const double* x, double* y);
+// gradf, gradphi, grad, D of include/dbarrier.h:48-81 separately; red: [0] += sum a, [1] += sum logs.
+int bar_terms(db200_context* ctx, int n, int r, const double* Z, long long ld, const double* w, const double* a,
+              double C, double t, double* gf, double* gp, double* g, double* D, double* red);
+int bar_reciprocal(db200_context* ctx, int n, const double* x, double* y);
+// res = g + Z v + s/dinv (v = Z^T s: the negated Newton residual); red [0] += |res|^2, [1] += |g|^2
+int bar_residual(db200_context* ctx, int n, int r, const double* Z, long long ld, const double* v, const double* g,
+                 const double* dinv, const double* s, double* res, double* red);
+// red [0] += g.s, [1] += sum s, [2] min feasible step (init DBL_MAX)
+int bar_step_stats(db200_context* ctx, int n, const double* g, const double* s, const double* a, double C,
+                   double* red);
+
+// gram_tc.cu: M (upper, FP64) += (D^-1/2 Z)^T (D^-1/2 Z) on the tensor cores, split bf16
+size_t gram_tc_scratch_bytes(int n, int r);
+int gram_tc_weighted(db200_context* ctx, int n, int r, const double* Z, long long ldz, const double* w, double* M,
+                     int ldm, void* scratch);
+int bar_negate(db200_context* ctx, int n, const double* x, double* y);
+// y = alpha x + beta y + gamma (x may be null)
+int bar_vec_update(db200_context* ctx, int n, double alpha, const double* x, double beta, double* y, double gamma);
 // red[0] = sum max(0, 1 - (Z w)_i)
 int bar_hinge(db200_context* ctx, int n, int r, const double* Z, long long ld, const double* w, double* red);
 int bar_add_identity(db200_context* ctx, double* M, int ldm, int r);
+int bar_scale_diag(db200_context* ctx, double* M, int ldm, int r, double factor);
 int bar_dot(db200_context* ctx, int r, const double* x, const double* y, double* out);
 
 }  // namespace db200

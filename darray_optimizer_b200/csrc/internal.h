@@ -89,7 +89,7 @@ int pack_sketch(db200_context* ctx, const float* Omega, int ldo, const float* yj
                 void* op);
 
 struct SketchPlan {
-  int n_panels = 1, panel = 16, lrows = 16;
+  int n_panels = 1, panel = 16, lrows = 16, g_bufs = 2;
 };
 SketchPlan plan_sketch(int l);
 int feature_pad(int d);  // dp: padded feature count of the split operand

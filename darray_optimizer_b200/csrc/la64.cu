@@ -88,7 +88,7 @@ __global__ void __launch_bounds__(256) gram_kernel(int n, int p, int q, const TA
 template <typename TA, typename TC>
 __global__ void __launch_bounds__(256) gemm_nn_kernel(int n, int p, int q, const TA* __restrict__ A, long long lda,
                                                       const double* __restrict__ B, int ldb, int transB,
-                                                      double beta, TC* C, long long ldc) {
+                                                      double alpha, double beta, TC* C, long long ldc) {
   const int i0 = blockIdx.x * TB, j0 = blockIdx.y * TB;
   __shared__ double sA[TK][TB + 1];
   __shared__ double sB[TK][TB + 1];
@@ -136,7 +136,7 @@ __global__ void __launch_bounds__(256) gemm_nn_kernel(int n, int p, int q, const
       const int j = j0 + tx * 4 + b;
       if (j >= q) continue;
       TC* dst = C + (long long)j * ldc + i;
-      double v = acc[a][b];
+      double v = alpha * acc[a][b];
       if (beta != 0.0) v += beta * (double)*dst;
       *dst = (TC)v;
     }
@@ -352,6 +352,85 @@ __global__ void convert_kernel(const TS* src, long long lds, TD* dst, long long 
   }
 }
 
+// C (float) = alpha * T (double) + beta * C
+__global__ void axpby_f32_kernel(float* C, long long ldc, const double* T, long long ldt, int m, int n, double alpha,
+                                 double beta) {
+  const long long total = (long long)m * n;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e % m), j = (int)(e / m);
+    float* c = C + j * ldc + i;
+    double v = alpha * T[j * ldt + i];
+    if (beta != 0.0) v += beta * (double)*c;
+    *c = (float)v;
+  }
+}
+
+// out[0] += sum of squares of the m x n float block
+__global__ void sumsq_f32_kernel(const float* A, long long lda, int m, int n, double* out) {
+  double s = 0.0;
+  const long long total = (long long)m * n;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+    const double v = A[(e / m) * lda + (e % m)];
+    s = fma(v, v, s);
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  __shared__ double w[32];
+  if (threadIdx.x % 32 == 0) w[threadIdx.x / 32] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int k = 0; k < (int)(blockDim.x / 32); ++k) t += w[k];
+    atomicAdd(out, t);
+  }
+}
+
+// FP64 kernel block from a Gram block: K[i + j*ldk] = yi_i yj_j exp(-gamma max(si_i + sj_j - 2 G, 0)) in place
+// (G = Xi^T Xj formed by the FP64 Gram kernel); the comparator arithmetic of include/dkernel.cu:116-129 in FP64.
+__global__ void rbf_from_gram_f64_kernel(double* K, long long ldk, int m, int n, const double* si, const double* sj,
+                                         const float* yi, const float* yj, double gamma) {
+  const long long total = (long long)m * n;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e % m), j = (int)(e / m);
+    double* k = K + j * ldk + i;
+    const double d2 = fmax(si[i] + sj[j] - 2.0 * *k, 0.0);
+    double v = exp(-gamma * d2);
+    if (yi) v *= (double)yi[i];
+    if (yj) v *= (double)yj[j];
+    *k = v;
+  }
+}
+
+// s_i = sum_k x_ik^2 in FP64 for point-major X (d x n, ldx): vecnorm (include/dkernel.cu:102-114) in FP64
+__global__ void rownorm_f64_kernel(const float* X, long long ldx, int n, int d, double* s) {
+  const int lane = threadIdx.x % 32;
+  const long long warps = (long long)gridDim.x * (blockDim.x / 32);
+  for (long long i = blockIdx.x * (long long)(blockDim.x / 32) + threadIdx.x / 32; i < n; i += warps) {
+    double acc = 0.0;
+    for (int k = lane; k < d; k += 32) {
+      const double x = X[i * ldx + k];
+      acc = fma(x, x, acc);
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) s[i] = acc;
+  }
+}
+
+// Sort v[0..n) descending in place (rank sort, one CTA, n <= 8192).
+__global__ void sort_desc_kernel(double* v, int n) {
+  extern __shared__ double sv[];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) sv[i] = v[i];
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const double x = sv[i];
+    int rank = 0;
+    for (int j = 0; j < n; ++j) {
+      const double yj = sv[j];
+      rank += (yj > x) || (yj == x && j < i);
+    }
+    v[rank] = x;
+  }
+}
+
 __global__ void trace_kernel(const double* C, int ldc, int l, double* out) {
   double s = 0.0;
   for (int i = threadIdx.x; i < l; i += blockDim.x) s += C[(long long)i * ldc + i];
@@ -364,6 +443,68 @@ __global__ void trace_kernel(const double* C, int ldc, int l, double* out) {
     for (int k = 0; k < (int)(blockDim.x / 32); ++k) t += w[k];
     *out = t;
   }
+}
+
+// One-sided Jacobi (Hestenes) on the columns of an n x n matrix held in global memory, one CTA: every round
+// orthogonalises n/2 disjoint column pairs (round-robin tournament order), one warp per pair.  The singular
+// values are the final column norms.  status <- 1 if `max_sweeps` sweeps did not converge.
+__global__ void __launch_bounds__(1024) jacobi_svd_kernel(double* A, int lda, int n, int max_sweeps, double tol,
+                                                          double* S, int* status) {
+  __shared__ unsigned long long worst;
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32, nw = blockDim.x / 32;
+  const int np = (n + 1) & ~1;  // even number of players; index n is a dummy when n is odd
+  int sweep = 0;
+  for (; sweep < max_sweeps; ++sweep) {
+    if (threadIdx.x == 0) worst = 0ull;
+    __syncthreads();
+    for (int round = 0; round < np - 1; ++round) {
+      for (int k = warp; k < np / 2; k += nw) {
+        int p = (k == 0) ? 0 : ((k + round - 1) % (np - 1)) + 1;
+        int q = ((np - 1 - k + round - 1) % (np - 1)) + 1;
+        if (p >= n || q >= n) continue;
+        double* ap = A + (long long)p * lda;
+        double* aq = A + (long long)q * lda;
+        double al = 0, be = 0, ga = 0;
+        for (int i = lane; i < n; i += 32) {
+          const double x = ap[i], y = aq[i];
+          al = fma(x, x, al);
+          be = fma(y, y, be);
+          ga = fma(x, y, ga);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          al += __shfl_xor_sync(0xffffffffu, al, o);
+          be += __shfl_xor_sync(0xffffffffu, be, o);
+          ga += __shfl_xor_sync(0xffffffffu, ga, o);
+        }
+        const double denom = sqrt(al * be);
+        const double ratio = (denom > 0.0) ? fabs(ga) / denom : 0.0;
+        if (lane == 0) atomicMax(&worst, (unsigned long long)__double_as_longlong(ratio));
+        if (ratio > tol) {
+          const double zeta = (be - al) / (2.0 * ga);
+          const double t = copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+          const double c = 1.0 / sqrt(1.0 + t * t), s = c * t;
+          for (int i = lane; i < n; i += 32) {
+            const double x = ap[i], y = aq[i];
+            ap[i] = c * x - s * y;
+            aq[i] = s * x + c * y;
+          }
+        }
+      }
+      __syncthreads();
+    }
+    if (__longlong_as_double((long long)worst) <= tol) break;
+    __syncthreads();
+  }
+  for (int p = warp; p < n; p += nw) {
+    const double* ap = A + (long long)p * lda;
+    double s2 = 0;
+    for (int i = lane; i < n; i += 32) s2 = fma(ap[i], ap[i], s2);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    if (lane == 0) S[p] = sqrt(s2);
+  }
+  if (threadIdx.x == 0) *status = (sweep >= max_sweeps) ? 1 : 0;
 }
 
 inline unsigned grid_for(long long total, int threads, int cap) {
@@ -406,24 +547,25 @@ template int gram<double, float>(db200_context*, int, int, int, const double*, l
 
 template <typename TA, typename TC>
 int gemm_tall(db200_context* ctx, int n, int p, int q, const TA* A, long long lda, const double* B, int ldb,
-              bool transB, double beta, TC* C, long long ldc) {
+              bool transB, double beta, TC* C, long long ldc, double alpha) {
   if (n <= 0 || q <= 0) return DB200_OK;
   dim3 grid((n + TB - 1) / TB, (q + TB - 1) / TB);
   if (grid.y > 65535) return fail(ctx, DB200_ERR_UNSUPPORTED, "gemm_tall: q too large");
-  gemm_nn_kernel<TA, TC><<<grid, 256, 0, ctx->stream>>>(n, p, q, A, lda, B, ldb, transB ? 1 : 0, beta, C, ldc);
+  gemm_nn_kernel<TA, TC><<<grid, 256, 0, ctx->stream>>>(n, p, q, A, lda, B, ldb, transB ? 1 : 0, alpha, beta, C,
+                                                        ldc);
   DB200_CUDA(ctx, cudaGetLastError());
   count_launch(ctx);
   return DB200_OK;
 }
 
 template int gemm_tall<float, double>(db200_context*, int, int, int, const float*, long long, const double*, int,
-                                      bool, double, double*, long long);
+                                      bool, double, double*, long long, double);
 template int gemm_tall<double, double>(db200_context*, int, int, int, const double*, long long, const double*, int,
-                                       bool, double, double*, long long);
+                                       bool, double, double*, long long, double);
 template int gemm_tall<double, float>(db200_context*, int, int, int, const double*, long long, const double*, int,
-                                      bool, double, float*, long long);
+                                      bool, double, float*, long long, double);
 template int gemm_tall<float, float>(db200_context*, int, int, int, const float*, long long, const double*, int,
-                                     bool, double, float*, long long);
+                                     bool, double, float*, long long, double);
 
 int potrf_upper(db200_context* ctx, double* A, int lda, int l, int* d_status, int* d_bad, int nb) {
   if (nb < 1 || nb > 64) nb = 64;
@@ -499,6 +641,53 @@ template int convert<double, float>(db200_context*, const double*, long long, fl
 template int convert<float, double>(db200_context*, const float*, long long, double*, long long, int, int);
 template int convert<double, double>(db200_context*, const double*, long long, double*, long long, int, int);
 template int convert<float, float>(db200_context*, const float*, long long, float*, long long, int, int);
+
+int jacobi_svd_values(db200_context* ctx, double* A, int lda, int n, double* S, int* d_status) {
+  jacobi_svd_kernel<<<1, 1024, 0, ctx->stream>>>(A, lda, n, 40, 1e-15, S, d_status);
+  DB200_CUDA(ctx, cudaGetLastError());
+  count_launch(ctx);
+  return DB200_OK;
+}
+
+int axpby_f32(db200_context* ctx, float* C, long long ldc, const double* T, long long ldt, int m, int n,
+              double alpha, double beta) {
+  axpby_f32_kernel<<<grid_for((long long)m * n, 256, 8 * ctx->num_sms), 256, 0, ctx->stream>>>(C, ldc, T, ldt, m, n,
+                                                                                                alpha, beta);
+  DB200_CUDA(ctx, cudaGetLastError());
+  count_launch(ctx);
+  return DB200_OK;
+}
+
+int sumsq_f32(db200_context* ctx, const float* A, long long lda, int m, int n, double* d_out) {
+  sumsq_f32_kernel<<<grid_for((long long)m * n, 256, 8 * ctx->num_sms), 256, 0, ctx->stream>>>(A, lda, m, n, d_out);
+  DB200_CUDA(ctx, cudaGetLastError());
+  count_launch(ctx);
+  return DB200_OK;
+}
+
+int rbf_from_gram_f64(db200_context* ctx, double* K, long long ldk, int m, int n, const double* si, const double* sj,
+                      const float* yi, const float* yj, double gamma) {
+  rbf_from_gram_f64_kernel<<<grid_for((long long)m * n, 256, 16 * ctx->num_sms), 256, 0, ctx->stream>>>(
+      K, ldk, m, n, si, sj, yi, yj, gamma);
+  DB200_CUDA(ctx, cudaGetLastError());
+  count_launch(ctx);
+  return DB200_OK;
+}
+
+int rownorm_f64(db200_context* ctx, const float* X, long long ldx, int n, int d, double* s) {
+  rownorm_f64_kernel<<<grid_for((long long)n * 32, 256, 16 * ctx->num_sms), 256, 0, ctx->stream>>>(X, ldx, n, d, s);
+  DB200_CUDA(ctx, cudaGetLastError());
+  count_launch(ctx);
+  return DB200_OK;
+}
+
+int sort_desc(db200_context* ctx, double* v, int n) {
+  if (n > 8192) return fail(ctx, DB200_ERR_UNSUPPORTED, "sort_desc: n > 8192");
+  sort_desc_kernel<<<1, 1024, sizeof(double) * n, ctx->stream>>>(v, n);
+  DB200_CUDA(ctx, cudaGetLastError());
+  count_launch(ctx);
+  return DB200_OK;
+}
 
 int trace(db200_context* ctx, const double* C, int ldc, int l, double* d_out) {
   trace_kernel<<<1, 1024, 0, ctx->stream>>>(C, ldc, l, d_out);

@@ -13,7 +13,7 @@ int gram(db200_context* ctx, int n, int p, int q, const TA* A, long long lda, co
 // C[n x q] = A[n x p] * op(B) + beta * C,  op(B) = B (p x q, ldb) or B^T (B stored q x p) when transB.
 template <typename TA, typename TC>
 int gemm_tall(db200_context* ctx, int n, int p, int q, const TA* A, long long lda, const double* B, int ldb,
-              bool transB, double beta, TC* C, long long ldc);
+              bool transB, double beta, TC* C, long long ldc, double alpha = 1.0);
 
 // In-place upper Cholesky (A = R^T R) with block size nb <= 64; the strictly lower part is zeroed.  A
 // non-positive pivot sets *d_status = DB200_ERR_NOT_SPD and *d_bad = first row of the failing block.
@@ -32,5 +32,21 @@ int mirror_upper(db200_context* ctx, double* C, int ldc, int l);
 template <typename TS, typename TD>
 int convert(db200_context* ctx, const TS* src, long long lds, TD* dst, long long ldd, int m, int n);
 int trace(db200_context* ctx, const double* C, int ldc, int l, double* d_out);
+// C (float) = alpha * T (double) + beta * C
+int axpby_f32(db200_context* ctx, float* C, long long ldc, const double* T, long long ldt, int m, int n,
+              double alpha, double beta);
+// *d_out += sum of squares of an m x n float block
+int sumsq_f32(db200_context* ctx, const float* A, long long lda, int m, int n, double* d_out);
+// K = yi yj exp(-gamma max(si + sj - 2 G, 0)) in place over an m x n FP64 Gram block
+int rbf_from_gram_f64(db200_context* ctx, double* K, long long ldk, int m, int n, const double* si, const double* sj,
+                      const float* yi, const float* yj, double gamma);
+// FP64 squared norms of the n points of a point-major float matrix
+int rownorm_f64(db200_context* ctx, const float* X, long long ldx, int n, int d, double* s);
+// sort descending, n <= 8192
+int sort_desc(db200_context* ctx, double* v, int n);
+
+// Singular values of the n x n matrix A (destroyed) by one-sided Jacobi, unsorted; *d_status = 1 if the sweep
+// cap was reached.  Restates svd (include/lapack_like.h:389-413), which returns only S.
+int jacobi_svd_values(db200_context* ctx, double* A, int lda, int n, double* S, int* d_status);
 
 }  // namespace db200

@@ -1,5 +1,9 @@
 // Fused RBF-kernel tile engine for sm_100a (tcgen05 + TMEM + TMA).
 //
+// Squared distances use the GEMM form ||x||^2 + ||y||^2 - 2 x.y of include/dkernel.cu:116-129 with x split into
+// bf16 hi + lo; the norms are formed from the same split products as the cross term, so the sum cancels to fp32
+// round-off on the diagonal instead of leaving the split's representation error (~3 * 2^-18 ||x||^2).
+//
 // One CTA owns a 128-row block of points i and one panel of sketch columns.  It streams every 128-column
 // block of points j and, per tile:
 //   MMA1  G   = Xi . Xj^T  in TMEM (fp32), from split-bf16 operands: hi.hi + hi.lo + lo.hi
@@ -30,14 +34,18 @@ constexpr int CHUNK_BYTES = BM * KC * 2;  // one 128 x 64 bf16 chunk = 16 KB
 constexpr int NUM_THREADS = 320;
 constexpr int NUM_EPI_WARPS = 8;
 constexpr int TMEM_COLS = 512;
-constexpr int TMEM_G0 = 0;       // two G buffers of 128 columns
-constexpr int TMEM_Y = 256;      // sketch accumulator, up to 256 columns
+constexpr int SMEM_LIMIT = 232448;  // dynamic shared memory per block on sm_100
 constexpr float LOG2E = 1.4426950408889634f;
 
+// Runtime plan of one launch: TMEM columns (G buffers, the bf16 P tile, the Y panel) and ring depths.
 struct TileArgs {
   int m, n;            // valid rows / columns
   int dp;              // padded feature count; packed row = [hi(dp) | lo(dp)]
   int n_itiles, n_jtiles, n_panels, panel, l;
+  int g_bufs;          // 1 or 2 TMEM buffers of 128 columns for G
+  int tmem_p, tmem_y;  // first TMEM column of the P tile (64 columns) and of the Y panel
+  int nsx, nso;        // Xj and Omega ring stages
+  int om_box;          // rows per Omega TMA box (TMA boxes are at most 256 rows; wider panels take two)
   float c_row, c_dot;  // -gamma*log2e, 2*gamma*log2e
   const float* si;
   const float* sj;
@@ -49,24 +57,19 @@ struct TileArgs {
 };
 
 struct SmemLayout {
-  int nkc;       // chunks per packed row
-  int nsx;       // Xj ring stages
-  int nso;       // Omega ring stages
-  int om_stage;  // bytes per Omega stage
-  size_t off_xi, off_xj, off_om, off_p, off_bar, total;
+  int nkc;  // chunks per packed row
+  int om_stage;
+  size_t off_xi, off_xj, off_om, off_bar, total;
 };
 
-__host__ __device__ inline SmemLayout make_layout(int dp, int panel, int mode) {
+__host__ __device__ inline SmemLayout make_layout(int dp, int panel, int nsx, int nso) {
   SmemLayout L;
   L.nkc = (2 * dp) / KC;
-  L.nsx = (mode == RBF_MODE_SKETCH) ? 4 : 8;
-  L.nso = (mode == RBF_MODE_SKETCH) ? 2 : 0;
   L.om_stage = panel * 128;
   L.off_xi = 0;
   L.off_xj = L.off_xi + (size_t)L.nkc * CHUNK_BYTES;
-  L.off_om = L.off_xj + (size_t)L.nsx * CHUNK_BYTES;
-  L.off_p = L.off_om + (size_t)L.nso * L.om_stage;
-  L.off_bar = L.off_p + ((mode == RBF_MODE_SKETCH) ? 2 * CHUNK_BYTES : 0);
+  L.off_om = L.off_xj + (size_t)nsx * CHUNK_BYTES;
+  L.off_bar = L.off_om + (size_t)nso * L.om_stage;
   L.total = L.off_bar + 512;  // barriers, TMEM slot, abort flag
   return L;
 }
@@ -93,15 +96,14 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                     const __grid_constant__ CUtensorMap tm_om, TileArgs args) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  const SmemLayout L = make_layout(args.dp, args.panel, MODE);
+  const SmemLayout L = make_layout(args.dp, args.panel, args.nsx, args.nso);
+  const int nsx = args.nsx, nso = args.nso, gb = args.g_bufs;
   const uint32_t s_xi = smem_u32(smem + L.off_xi);
   const uint32_t s_xj = smem_u32(smem + L.off_xj);
   const uint32_t s_om = smem_u32(smem + L.off_om);
-  const uint32_t s_p = smem_u32(smem + L.off_p);
   const uint32_t s_bar = smem_u32(smem + L.off_bar);
   auto bar = [&](int idx) -> uint32_t { return s_bar + 8u * (uint32_t)idx; };
-  const int XJ_FULL = B_XJ_FULL0, XJ_EMPTY = B_XJ_FULL0 + L.nsx, OM_FULL = XJ_EMPTY + L.nsx,
-            OM_EMPTY = OM_FULL + L.nso;
+  const int XJ_FULL = B_XJ_FULL0, XJ_EMPTY = B_XJ_FULL0 + nsx, OM_FULL = XJ_EMPTY + nsx, OM_EMPTY = OM_FULL + nso;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + L.off_bar + 400);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + L.off_bar + 408);
 
@@ -122,11 +124,11 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
     mbar_init(bar(B_Y_FULL), 1);
     mbar_init(bar(B_Y_EMPTY), NUM_EPI_WARPS);
     mbar_init(bar(B_DRAIN), 1);
-    for (int s = 0; s < L.nsx; ++s) {
+    for (int s = 0; s < nsx; ++s) {
       mbar_init(bar(XJ_FULL + s), 1);
       mbar_init(bar(XJ_EMPTY + s), 1);
     }
-    for (int s = 0; s < L.nso; ++s) {
+    for (int s = 0; s < nso; ++s) {
       mbar_init(bar(OM_FULL + s), 1);
       mbar_init(bar(OM_EMPTY + s), 1);
     }
@@ -160,17 +162,19 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
           tma_load_2d(s_xi + c * CHUNK_BYTES, &tm_xi, bar(B_XI_FULL), c * KC, it * BM);
         for (int jt = 0; jt < args.n_jtiles && ok; ++jt) {
           for (int c = 0; c < L.nkc; ++c, ++kx) {
-            const uint32_t s = kx % L.nsx, ph = (kx / L.nsx) & 1;
+            const uint32_t s = kx % nsx, ph = (kx / nsx) & 1;
             if (!mbar_wait(bar(XJ_EMPTY + s), ph ^ 1, abort_flag)) { ok = false; break; }
             mbar_arrive_expect_tx(bar(XJ_FULL + s), CHUNK_BYTES);
             tma_load_2d(s_xj + s * CHUNK_BYTES, &tm_xj, bar(XJ_FULL + s), c * KC, jt * BN);
           }
           if (MODE == RBF_MODE_SKETCH) {
             for (int c = 0; c < 2 && ok; ++c, ++ko) {
-              const uint32_t s = ko % L.nso, ph = (ko / L.nso) & 1;
+              const uint32_t s = ko % nso, ph = (ko / nso) & 1;
               if (!mbar_wait(bar(OM_EMPTY + s), ph ^ 1, abort_flag)) { ok = false; break; }
               mbar_arrive_expect_tx(bar(OM_FULL + s), L.om_stage);
-              tma_load_2d(s_om + s * L.om_stage, &tm_om, bar(OM_FULL + s), jt * BN + c * KC, pn * args.panel);
+              for (int r0 = 0; r0 < args.panel; r0 += args.om_box)
+                tma_load_2d(s_om + s * L.om_stage + r0 * 128, &tm_om, bar(OM_FULL + s), jt * BN + c * KC,
+                            pn * args.panel + r0);
             }
           }
         }
@@ -178,10 +182,10 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
       if (!ok) {
         // Drain: wait (time-bounded, ignoring the abort flag) for the loads this thread issued.
         volatile int never = 0;
-        for (uint32_t k = (kx > (uint32_t)L.nsx ? kx - L.nsx : 0); k < kx; ++k)
-          mbar_wait(bar(XJ_FULL + k % L.nsx), (k / L.nsx) & 1, &never);
-        for (uint32_t k = (ko > (uint32_t)L.nso ? ko - L.nso : 0); k < ko; ++k)
-          mbar_wait(bar(OM_FULL + k % L.nso), (k / L.nso) & 1, &never);
+        for (uint32_t k = (kx > (uint32_t)nsx ? kx - nsx : 0); k < kx; ++k)
+          mbar_wait(bar(XJ_FULL + k % nsx), (k / nsx) & 1, &never);
+        for (uint32_t k = (ko > (uint32_t)nso ? ko - nso : 0); k < ko; ++k)
+          mbar_wait(bar(OM_FULL + k % nso), (k / nso) & 1, &never);
         if (xi_loads > 0) mbar_wait(bar(B_XI_FULL), (xi_loads - 1) & 1, &never);
       }
     }
@@ -190,33 +194,40 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
     // ------------------------------------------------------------ MMA issuer
     if (lane == 0) {
       const uint32_t idesc_g = idesc_f16(BM, BN, true);
-      const uint32_t idesc_y = idesc_f16(BM, args.panel, true);
+      // sketch panel: one MMA of N <= 256 columns, or 256 + (panel - 256)
+      const int n1 = args.panel > 256 ? 256 : args.panel, n2 = args.panel - n1;
+      const uint32_t idesc_y1 = idesc_f16(BM, n1, true);
+      const uint32_t idesc_y2 = idesc_f16(BM, n2 > 0 ? n2 : 16, true);
       const int dp = args.dp;
       uint32_t kx = 0, ko = 0, kg = 0, kp = 0, items_done = 0;
       bool ok = true;
+      // Descriptors are affine in the shared address (start address in the low 14 bits, in 16-byte units):
+      // build the base descriptors once and add offsets.
+      const uint64_t dxi = sdesc_k_sw128(s_xi), dxj = sdesc_k_sw128(s_xj), dom = sdesc_k_sw128(s_om);
 
       auto issue_mma1 = [&]() -> bool {
-        const uint32_t b = kg & 1, ph = (kg >> 1) & 1;
+        const uint32_t b = kg % gb, ph = (kg / gb) & 1;
         if (!mbar_wait(bar(B_G_EMPTY0 + b), ph ^ 1, abort_flag)) return false;
         tc_fence_after();
-        const uint32_t d_tmem = tmem_base + TMEM_G0 + b * BN;
+        const uint32_t d_tmem = tmem_base + b * BN;
         bool first = true;
         for (int c = 0; c < L.nkc; ++c, ++kx) {
-          const uint32_t s = kx % L.nsx, sph = (kx / L.nsx) & 1;
+          const uint32_t s = kx % nsx, sph = (kx / nsx) & 1;
           if (!mbar_wait(bar(XJ_FULL + s), sph, abort_flag)) return false;
           tc_fence_after();
+#pragma unroll
           for (int ks = 0; ks < KC / 16; ++ks) {
             const int o = c * KC + ks * 16;  // K offset of this slice inside the packed row
-            const uint64_t bdesc = sdesc_k_sw128(s_xj + s * CHUNK_BYTES + ks * 32);
+            const uint64_t bdesc = dxj + ((s * CHUNK_BYTES + ks * 32) >> 4);
             if (o < dp) {  // B slice is hi_j: pair with hi_i and lo_i
               const int oh = o, ol = dp + o;
-              umma_f16(d_tmem, sdesc_k_sw128(s_xi + (oh / KC) * CHUNK_BYTES + (oh % KC) * 2), bdesc, idesc_g,
+              umma_f16(d_tmem, dxi + (((oh / KC) * CHUNK_BYTES + (oh % KC) * 2) >> 4), bdesc, idesc_g,
                        first ? 0u : 1u);
               first = false;
-              umma_f16(d_tmem, sdesc_k_sw128(s_xi + (ol / KC) * CHUNK_BYTES + (ol % KC) * 2), bdesc, idesc_g, 1u);
+              umma_f16(d_tmem, dxi + (((ol / KC) * CHUNK_BYTES + (ol % KC) * 2) >> 4), bdesc, idesc_g, 1u);
             } else {  // B slice is lo_j: pair with hi_i
               const int oh = o - dp;
-              umma_f16(d_tmem, sdesc_k_sw128(s_xi + (oh / KC) * CHUNK_BYTES + (oh % KC) * 2), bdesc, idesc_g, 1u);
+              umma_f16(d_tmem, dxi + (((oh / KC) * CHUNK_BYTES + (oh % KC) * 2) >> 4), bdesc, idesc_g, 1u);
             }
           }
           umma_commit(bar(XJ_EMPTY + s));
@@ -240,12 +251,17 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
             if (!mbar_wait(bar(B_P_FULL), kp & 1, abort_flag)) { ok = false; break; }
             tc_fence_after();
             for (int c = 0; c < 2 && ok; ++c, ++ko) {
-              const uint32_t s = ko % L.nso, sph = (ko / L.nso) & 1;
+              const uint32_t s = ko % nso, sph = (ko / nso) & 1;
               if (!mbar_wait(bar(OM_FULL + s), sph, abort_flag)) { ok = false; break; }
               tc_fence_after();
+#pragma unroll
               for (int ks = 0; ks < KC / 16; ++ks) {
-                umma_f16(tmem_base + TMEM_Y, sdesc_k_sw128(s_p + c * CHUNK_BYTES + ks * 32),
-                         sdesc_k_sw128(s_om + s * L.om_stage + ks * 32), idesc_y, (jt | c | ks) ? 1u : 0u);
+                // A = P (bf16 in TMEM, 8 columns per 16-wide K step), B = Omega~ rows of this panel
+                const uint32_t a_tmem = tmem_base + args.tmem_p + c * 32 + ks * 8;
+                const uint64_t bdesc = dom + ((s * L.om_stage + ks * 32) >> 4);
+                const uint32_t acc = (jt | c | ks) ? 1u : 0u;
+                umma_f16_ts(tmem_base + args.tmem_y, a_tmem, bdesc, idesc_y1, acc);
+                if (n2 > 0) umma_f16_ts(tmem_base + args.tmem_y + 256, a_tmem, bdesc + ((256 * 128) >> 4), idesc_y2, acc);
               }
               umma_commit(bar(OM_EMPTY + s));
             }
@@ -279,11 +295,11 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
       const float a_i = args.c_row * args.si[i];  // si is padded to n_itiles*BM
       const float y_i = (i < args.m && args.yi) ? args.yi[i] : 1.0f;
       for (int jt = 0; jt < args.n_jtiles; ++jt) {
-        const uint32_t b = kg & 1, ph = (kg >> 1) & 1;
+        const uint32_t b = kg % gb, ph = (kg / gb) & 1;
         if (!__all_sync(0xffffffffu, mbar_wait(bar(B_G_FULL0 + b), ph, abort_flag))) { ok = false; break; }
         tc_fence_after();
         float v[64];
-        const uint32_t tcol = tmem_base + t_lane + TMEM_G0 + b * BN + h * 64;
+        const uint32_t tcol = tmem_base + t_lane + b * BN + h * 64;
 #pragma unroll
         for (int c = 0; c < 4; ++c) tmem_ld16(tcol + c * 16, v + c * 16);
         tmem_wait_ld();
@@ -304,15 +320,15 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
         }
 
         if (MODE == RBF_MODE_SKETCH) {
-          if (!__all_sync(0xffffffffu, mbar_wait(bar(B_P_EMPTY), (kp & 1) ^ 1, abort_flag))) { ok = false; break; }
-          const uint32_t base = s_p + h * CHUNK_BYTES + (row >> 3) * 1024 + (row & 7) * 128;
+          uint32_t pk[32];
 #pragma unroll
-          for (int g = 0; g < 8; ++g) {
-            const uint32_t addr = base + ((uint32_t)(g ^ (row & 7)) << 4);
-            st_shared_v4(addr, pack_bf16x2(v[8 * g + 0], v[8 * g + 1]), pack_bf16x2(v[8 * g + 2], v[8 * g + 3]),
-                         pack_bf16x2(v[8 * g + 4], v[8 * g + 5]), pack_bf16x2(v[8 * g + 6], v[8 * g + 7]));
-          }
-          fence_proxy_async_smem();
+          for (int c = 0; c < 32; ++c) pk[c] = pack_bf16x2(v[2 * c], v[2 * c + 1]);
+          if (!__all_sync(0xffffffffu, mbar_wait(bar(B_P_EMPTY), (kp & 1) ^ 1, abort_flag))) { ok = false; break; }
+          tc_fence_after();
+          // P row = this thread's row; j in [64h, 64h + 64) -> TMEM columns tmem_p + 32h .. + 31
+          tmem_st32(tmem_base + t_lane + args.tmem_p + h * 32, pk);
+          tmem_wait_st();
+          tc_fence_before();
           __syncwarp();
           if (lane == 0) mbar_arrive(bar(B_P_FULL));
           ++kp;
@@ -337,7 +353,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
         const int half = args.panel / 2;
         for (int cc = 0; cc < half; cc += 8) {
           float yv[8];
-          tmem_ld8(tmem_base + t_lane + TMEM_Y + h * half + cc, yv);
+          tmem_ld8(tmem_base + t_lane + args.tmem_y + h * half + cc, yv);
           tmem_wait_ld();
           if (i < args.m) {
 #pragma unroll
@@ -377,7 +393,10 @@ __global__ void pack_points_kernel(const float* __restrict__ X, long long sp, lo
       const __nv_bfloat16 lo = __float2bfloat16_rn(x - __bfloat162float(hi));
       row[k] = hi;
       row[dp + k] = lo;
-      acc = fmaf(x, x, acc);
+      // ||x||^2 from the same split products the distance MMA forms (hi.hi + 2 hi.lo), so that
+      // ||x||^2 + ||y||^2 - 2 x.y cancels to ~fp32 round-off for coincident points
+      const float h = __bfloat162float(hi), l = __bfloat162float(lo);
+      acc = fmaf(h, h, fmaf(2.0f * h, l, acc));
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
@@ -433,10 +452,14 @@ bool make_tmap(CUtensorMap* tm, const void* base, uint64_t inner, uint64_t outer
 
 int feature_pad(int d) { return round_up(d < 1 ? 1 : d, 32); }
 
+// Sketch panels: with one 128-column G buffer, P (64 columns) and Y fit a panel of up to 320 columns; with two
+// G buffers, up to 192.  Take whichever needs fewer panels (ties: two G buffers, which overlap better).
 SketchPlan plan_sketch(int l) {
   SketchPlan p;
-  const int lpad = round_up(l, 16);
-  p.n_panels = (lpad + 255) / 256;
+  const int lpad = round_up(l < 1 ? 1 : l, 16);
+  const int np1 = (lpad + 319) / 320, np2 = (lpad + 191) / 192;
+  p.g_bufs = (np2 <= np1) ? 2 : 1;
+  p.n_panels = (p.g_bufs == 2) ? np2 : np1;
   p.panel = round_up((lpad + p.n_panels - 1) / p.n_panels, 16);
   p.lrows = p.n_panels * p.panel;
   return p;
@@ -473,26 +496,40 @@ int launch_rbf_tiles(db200_context* ctx, int mode, const PackedPoints& pi, const
                      int ldo) {
   if (pi.dp != pj.dp || pi.dp > 128) return fail(ctx, DB200_ERR_UNSUPPORTED, "rbf tiles: feature count > 128");
   if (pi.npad % BM || pj.npad % BN) return fail(ctx, DB200_ERR_INVALID, "rbf tiles: unpadded operands");
-  if (mode == RBF_MODE_SKETCH && (plan.panel % 16 || plan.panel > 256 || plan.panel < 16))
+  if (mode == RBF_MODE_SKETCH && (plan.panel % 16 || plan.panel > 320 || plan.panel < 16 ||
+                                  plan.panel + 64 + 128 * plan.g_bufs > TMEM_COLS))
     return fail(ctx, DB200_ERR_INVALID, "rbf tiles: bad sketch panel");
   CUtensorMap tm_xi, tm_xj, tm_om;
   const int kp = 2 * pi.dp;
   if (!make_tmap(&tm_xi, pi.xp, kp, pi.npad, kp, BM) || !make_tmap(&tm_xj, pj.xp, kp, pj.npad, kp, BN))
     return fail(ctx, DB200_ERR_CUDA, "cuTensorMapEncodeTiled failed for the point operands");
+  TileArgs a;
   if (mode == RBF_MODE_SKETCH) {
-    if (!make_tmap(&tm_om, op, pj.npad, plan.lrows, pj.npad, plan.panel))
+    // a TMA box has at most 256 rows: a wider panel is loaded as two boxes of panel/2 rows (a multiple of 8)
+    a.om_box = plan.panel > 256 ? plan.panel / 2 : plan.panel;
+    if (!make_tmap(&tm_om, op, pj.npad, plan.lrows, pj.npad, a.om_box))
       return fail(ctx, DB200_ERR_CUDA, "cuTensorMapEncodeTiled failed for the sketch operand");
+    a.n_panels = plan.n_panels;
+    a.panel = plan.panel;
+    a.g_bufs = plan.g_bufs;
+    a.tmem_p = 128 * plan.g_bufs;
+    a.tmem_y = a.tmem_p + 64;
+    a.nso = 2;
   } else {
     tm_om = tm_xj;  // unused
+    a.n_panels = 1;
+    a.panel = 16;
+    a.g_bufs = 2;
+    a.tmem_p = 256;
+    a.tmem_y = 320;
+    a.nso = 0;
+    a.om_box = 16;
   }
-  TileArgs a;
   a.m = pi.n;
   a.n = pj.n;
   a.dp = pi.dp;
   a.n_itiles = pi.npad / BM;
   a.n_jtiles = pj.npad / BN;
-  a.n_panels = (mode == RBF_MODE_SKETCH) ? plan.n_panels : 1;
-  a.panel = (mode == RBF_MODE_SKETCH) ? plan.panel : 16;
   a.l = l;
   a.c_row = -gamma * LOG2E;
   a.c_dot = 2.0f * gamma * LOG2E;
@@ -503,7 +540,16 @@ int launch_rbf_tiles(db200_context* ctx, int mode, const PackedPoints& pi, const
   a.out = out;
   a.ldo = ldo;
   a.status = ctx->d_status;
-  const SmemLayout L = make_layout(a.dp, a.panel, mode);
+  // the Xj ring takes whatever shared memory is left (2..8 stages)
+  {
+    const SmemLayout L0 = make_layout(a.dp, a.panel, 0, a.nso);
+    const long long left = (long long)SMEM_LIMIT - 1024 - (long long)L0.total;
+    int nsx = (int)(left / CHUNK_BYTES);
+    if (nsx > 8) nsx = 8;
+    if (nsx < 2) return fail(ctx, DB200_ERR_UNSUPPORTED, "rbf tiles: shared memory plan does not fit");
+    a.nsx = nsx;
+  }
+  const SmemLayout L = make_layout(a.dp, a.panel, a.nsx, a.nso);
   const size_t smem = L.total + 1024;
   const int n_items = a.n_itiles * a.n_panels;
   const int grid = n_items < ctx->num_sms ? n_items : ctx->num_sms;

@@ -150,8 +150,10 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
   if (r > 4096) return fail(ctx, DB200_ERR_UNSUPPORTED, "svm_barrier: r > 4096");
   EventTimer timer(ctx->stream);
   const size_t rr = (size_t)r * r;
-  const size_t bytes = 4096 + 3 * align_up((size_t)n * 8, 256) + 6 * align_up((size_t)r * 8, 256) +
-                       2 * align_up(rr * 8, 256) + 4096;
+  const bool mixed = (P.precision == DB200_MIXED);
+  const size_t tc_bytes = mixed ? gram_tc_scratch_bytes(n, r) : 0;
+  const size_t bytes = 4096 + 5 * align_up((size_t)n * 8, 256) + 6 * align_up((size_t)r * 8, 256) +
+                       2 * align_up(rr * 8, 256) + align_up(tc_bytes, 256) + 4096;
   char* base = static_cast<char*>(slot_buffer(ctx, SLOT_BAR, bytes));
   if (!base) return DB200_ERR_NOMEM;
   Carve cv{base};
@@ -168,6 +170,11 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
   double* u = cv.take<double>(r);
   double* M = cv.take<double>(rr);
   double* L = cv.take<double>(rr);
+  double* res = cv.take<double>(n);
+  double* delta = cv.take<double>(n);
+  void* tc_scratch = mixed ? static_cast<void*>(cv.take<char>(tc_bytes)) : nullptr;
+  int refine_total = 0, fallbacks_total = 0;
+  bool tc_ok = true;
 
   // class-balanced start (tests/testsvm.cpp:192-212)
   std::vector<float> hy(n);
@@ -207,17 +214,81 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
       const double suma = h[0], sumlog = h[1], dmax = h[2], dmin = h[3], ww = h[8];
       if (dmax / dmin > 1e18) break;  // tests/testsvm.cpp:258-263
       const double lastg = 0.5 * ww - suma - sumlog / t;
-      // capacity matrix M = I + Z^T D^-1 Z and right-hand side u = -Z^T D^-1 g
-      if ((st = gram<double, double>(ctx, n, r, r, Z, ldz, Z, ldz, dinv, 1.0, 0.0, M, r, true))) return st;
-      if ((st = bar_add_identity(ctx, M, r, r))) return st;
-      if ((st = bar_gemv_t(ctx, n, r, Z, ldz, g, dinv, -1.0, u))) return st;
-      DB200_CUDA(ctx, cudaMemsetAsync(d_pair, 0, 2 * sizeof(int), ctx->stream));
-      if ((st = potrf_upper(ctx, M, r, r, d_pair, d_pair + 1))) return st;
-      if ((st = transpose64(ctx, M, r, r, r, L, r))) return st;
-      if ((st = trsv_upper(ctx, M, L, r, r, u, true))) return st;   // R^T z = rhs
-      if ((st = trsv_upper(ctx, M, L, r, r, u, false))) return st;  // R u = z
-      if ((st = bar_init_red(ctx, red, 2, 0, 1))) return st;
-      if ((st = bar_direction(ctx, n, r, Z, ldz, u, g, dinv, a, C, s, red))) return st;
+      // Newton direction s = -(Z Z^T + D)^-1 g by Woodbury.  Mixed: capacity matrix M = I + Z^T D^-1 Z on the
+      // tensor cores (split bf16) factored in FP64, then iterative refinement against the exact FP64 operator
+      // until the relative residual is <= 1e-10; a step that does not get there is recomputed with the FP64
+      // capacity matrix.  FP64: the capacity matrix on the FP64 pipes, no refinement.
+      auto newton_dir = [&](bool use_tc, bool* converged) -> int {
+        int s2;
+        *converged = true;
+        if (use_tc) {
+          DB200_CUDA(ctx, cudaMemsetAsync(M, 0, sizeof(double) * rr, ctx->stream));
+          if ((s2 = gram_tc_weighted(ctx, n, r, Z, ldz, dinv, M, r, tc_scratch))) return s2;
+        } else {
+          if ((s2 = gram<double, double>(ctx, n, r, r, Z, ldz, Z, ldz, dinv, 1.0, 0.0, M, r, true))) return s2;
+        }
+        if ((s2 = bar_add_identity(ctx, M, r, r))) return s2;
+        if ((s2 = bar_gemv_t(ctx, n, r, Z, ldz, g, dinv, -1.0, u))) return s2;
+        if (use_tc) {
+          // the split-bf16 Gram carries an error of ~1e-5 of its largest entries, which can exceed the identity
+          // floor; a relative diagonal shift (x10 until the FP64 Cholesky succeeds) keeps it positive definite
+          DB200_CUDA(ctx, cudaMemcpyAsync(L, M, sizeof(double) * rr, cudaMemcpyDeviceToDevice, ctx->stream));
+          double eps = 1e-5;
+          for (int tries = 0; tries < 6; ++tries) {
+            DB200_CUDA(ctx, cudaMemsetAsync(d_pair, 0, 2 * sizeof(int), ctx->stream));
+            if ((s2 = potrf_upper(ctx, M, r, r, d_pair, d_pair + 1))) return s2;
+            int pst = 0, bad = 0;
+            if ((s2 = read_status(ctx, d_pair, &pst, &bad))) return s2;
+            if (pst == 0) break;
+            DB200_CUDA(ctx, cudaMemcpyAsync(M, L, sizeof(double) * rr, cudaMemcpyDeviceToDevice, ctx->stream));
+            if ((s2 = bar_scale_diag(ctx, M, r, r, 1.0 + eps))) return s2;
+            eps *= 10.0;
+          }
+        } else {
+          DB200_CUDA(ctx, cudaMemsetAsync(d_pair, 0, 2 * sizeof(int), ctx->stream));
+          if ((s2 = potrf_upper(ctx, M, r, r, d_pair, d_pair + 1))) return s2;
+        }
+        if ((s2 = transpose64(ctx, M, r, r, r, L, r))) return s2;
+        if ((s2 = trsv_upper(ctx, M, L, r, r, u, true))) return s2;   // R^T z = rhs
+        if ((s2 = trsv_upper(ctx, M, L, r, r, u, false))) return s2;  // R u = z
+        if ((s2 = bar_init_red(ctx, red, 2, 0, 1))) return s2;
+        if ((s2 = bar_direction(ctx, n, r, Z, ldz, u, g, dinv, a, C, s, red))) return s2;
+        if (!use_tc) return DB200_OK;
+        // iterative refinement against the exact FP64 operator: s += H~^-1 (-g - H s)
+        *converged = false;
+        double prev = 0.0;
+        for (int it = 0; it <= P.refine_max; ++it) {
+          if ((s2 = bar_gemv_t(ctx, n, r, Z, ldz, s, nullptr, 1.0, v))) return s2;
+          if ((s2 = bar_init_red(ctx, red + 16, 2, 0, 0))) return s2;
+          if ((s2 = bar_residual(ctx, n, r, Z, ldz, v, g, dinv, s, res, red + 16))) return s2;
+          if ((s2 = fetch(red + 16, 2))) return s2;
+          const double rn = std::sqrt(h[0]), gn = std::sqrt(h[1]);
+          if (rn <= 1e-10 * gn) {
+            *converged = true;
+            break;
+          }
+          if (it == P.refine_max || (it > 0 && rn >= 0.5 * prev) || !std::isfinite(rn)) break;
+          prev = rn;
+          if ((s2 = bar_gemv_t(ctx, n, r, Z, ldz, res, dinv, -1.0, u))) return s2;
+          if ((s2 = trsv_upper(ctx, M, L, r, r, u, true))) return s2;
+          if ((s2 = trsv_upper(ctx, M, L, r, r, u, false))) return s2;
+          if ((s2 = bar_init_red(ctx, red + 16, 2, 0, 1))) return s2;
+          if ((s2 = bar_direction(ctx, n, r, Z, ldz, u, res, dinv, a, C, delta, red + 16))) return s2;
+          if ((s2 = bar_axpy(ctx, n, 1.0, delta, s))) return s2;
+          ++refine_total;
+        }
+        if ((s2 = bar_init_red(ctx, red, 2, 0, 1))) return s2;
+        return bar_step_stats(ctx, n, g, s, a, C, red);
+      };
+      bool conv = true;
+      if ((st = newton_dir(mixed && tc_ok, &conv))) return st;
+      if (mixed && tc_ok && !conv) {
+        // the barrier's D only grows more ill-conditioned with t: once the tensor-core preconditioner misses the
+        // tolerance, the remaining Newton steps use the FP64 capacity matrix directly
+        ++fallbacks_total;
+        tc_ok = false;
+        if ((st = newton_dir(false, &conv))) return st;
+      }
       if ((st = bar_gemv_t(ctx, n, r, Z, ldz, s, nullptr, 1.0, v))) return st;
       if ((st = bar_dot(ctx, r, w, v, sc + 1))) return st;
       if ((st = bar_dot(ctx, r, v, v, sc + 2))) return st;
@@ -288,6 +359,8 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
     rep->gap_barrier = 2.0 * n / t / std::fabs(fa);
     rep->gap_primal_dual = (primal + fa) / std::fabs(fa);
     rep->status = status;
+    rep->refine = refine_total;
+    rep->fallbacks = fallbacks_total;
     rep->ms_barrier = timer.stop_ms();
   }
   return status == DB200_ERR_MAXITER ? DB200_ERR_MAXITER : DB200_OK;
@@ -295,47 +368,70 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
 
 // ---------------------------------------------------------------------------------------------- low rank
 int lowrank_impl(db200_context* ctx, int n, int d, int l, int q, const float* X, int ldx, const float* y,
-                 const float* Omega, int ldo, float gamma, double* Z, int ldz, db200_svm_report* rep) {
+                 const float* Omega, int ldo, float gamma, int precision, double* Z, int ldz, db200_svm_report* rep) {
   if (l > n) return fail(ctx, DB200_ERR_INVALID, "lowrank: l > n");
+  const bool fp64 = (precision == DB200_FP64);
   const size_t nl = (size_t)n * l, ll = (size_t)l * l;
-  const size_t bytes = 4096 + 2 * align_up(nl * 4, 256) + align_up(nl * 8, 256) + 3 * align_up(ll * 8, 256) + 4096;
+  const size_t bytes = 4096 + 2 * align_up(nl * 4, 256) + 2 * align_up(nl * 8, 256) + 3 * align_up(ll * 8, 256) + 4096;
   char* base = static_cast<char*>(slot_buffer(ctx, SLOT_PIPE, bytes));
   if (!base) return DB200_ERR_NOMEM;
   Carve cv{base};
   int* d_pair = cv.take<int>(4);
   double* d_scalar = cv.take<double>(4);
-  float* Y32 = cv.take<float>(nl);
-  float* Qf = cv.take<float>(nl);
+  float* Y32 = cv.take<float>(nl);  // mixed: kernel-pass output (fp32 accumulation)
+  float* Qf = cv.take<float>(nl);   // mixed: Q as the next pass's test matrix
   double* Q = cv.take<double>(nl);
+  double* Y64 = cv.take<double>(nl);  // FP64: kernel-pass output
   double* Cm = cv.take<double>(ll);
   double* R = cv.take<double>(ll);
   double ms_sketch = 0, ms_orth = 0, ms_core = 0;
   int st;
 
-  auto sketch = [&](const float* Om, int ldom) -> int {
+  // one pass Y = diag(y) K diag(y) Om, into Y32 (mixed) or Y64 (FP64)
+  auto sketch_f32 = [&](const float* Om, int ldom) -> int {
     EventTimer tm(ctx->stream);
     int s2 = db200_rbf_sketch(ctx, n, n, d, l, X, ldx, X, ldx, DB200_POINT_MAJOR, y, y, Om, ldom, Y32, n, gamma);
     ms_sketch += tm.stop_ms();
     return s2;
   };
+  auto sketch_f64 = [&](const double* Om, int ldom) -> int {
+    EventTimer tm(ctx->stream);
+    int s2 = db200_rbf_sketch_f64(ctx, n, n, d, l, X, ldx, X, ldx, y, y, Om, ldom, Y64, n, gamma);
+    ms_sketch += tm.stop_ms();
+    return s2;
+  };
   auto orth = [&]() -> int {
     EventTimer tm(ctx->stream);
-    int s2 = convert<float, double>(ctx, Y32, n, Q, n, n, l);
+    int s2 = fp64 ? DB200_OK : convert<float, double>(ctx, Y32, n, Q, n, n, l);
+    if (!s2 && fp64)
+      s2 = (cudaMemcpyAsync(Q, Y64, sizeof(double) * nl, cudaMemcpyDeviceToDevice, ctx->stream) == cudaSuccess)
+               ? DB200_OK
+               : DB200_ERR_CUDA;
     if (!s2) s2 = cholqr2_impl(ctx, n, l, Q, n, nullptr, 0);
-    if (!s2) s2 = convert<double, float>(ctx, Q, n, Qf, n, n, l);
+    if (!s2 && !fp64) s2 = convert<double, float>(ctx, Q, n, Qf, n, n, l);
     ms_orth += tm.stop_ms();
     return s2;
   };
-  if ((st = sketch(Omega, ldo))) return st;
+  if (fp64) {
+    // the FP64 comparator takes Omega in FP64
+    if ((st = convert<float, double>(ctx, Omega, ldo, Q, n, n, l))) return st;
+    if ((st = sketch_f64(Q, n))) return st;
+  } else {
+    if ((st = sketch_f32(Omega, ldo))) return st;
+  }
   if ((st = orth())) return st;
   for (int it = 0; it < q; ++it) {
-    if ((st = sketch(Qf, n))) return st;
+    if ((st = fp64 ? sketch_f64(Q, n) : sketch_f32(Qf, n))) return st;
     if ((st = orth())) return st;
   }
-  if ((st = sketch(Qf, n))) return st;  // Y32 = K Q
+  if ((st = fp64 ? sketch_f64(Q, n) : sketch_f32(Qf, n))) return st;  // Y = K Q
   EventTimer tcore(ctx->stream);
   // C = Q^T (K Q), symmetrised; R^T R = C + nu I with nu = 1e-7 trace(C)/l, x10 until positive definite
-  if ((st = gram<double, float>(ctx, n, l, l, Q, n, Y32, n, nullptr, 1.0, 0.0, Cm, l, false))) return st;
+  if (fp64) {
+    if ((st = gram<double, double>(ctx, n, l, l, Q, n, Y64, n, nullptr, 1.0, 0.0, Cm, l, false))) return st;
+  } else {
+    if ((st = gram<double, float>(ctx, n, l, l, Q, n, Y32, n, nullptr, 1.0, 0.0, Cm, l, false))) return st;
+  }
   if ((st = symmetrize(ctx, Cm, l, l, 0.0))) return st;
   if ((st = trace(ctx, Cm, l, l, d_scalar))) return st;
   double tr = 0;
@@ -382,6 +478,8 @@ void db200_barrier_defaults(db200_barrier_params* p) {
   p->newton_tol = 1e-6;
   p->max_outer = 60;
   p->max_newton = 200;
+  p->precision = DB200_MIXED;
+  p->refine_max = 6;
 }
 
 int db200_potrf(db200_context* ctx, int n, double* A, int lda, int nb) {
@@ -449,11 +547,12 @@ int db200_svm_barrier(db200_context* ctx, int n, int r, const double* Z, int ldz
 }
 
 int db200_lowrank(db200_context* ctx, int n, int d, int l, int q, const float* X, int ldx, const float* y,
-                  const float* Omega, int ldo, float gamma, double* Z, int ldz, db200_svm_report* rep) {
+                  const float* Omega, int ldo, float gamma, int precision, double* Z, int ldz, db200_svm_report* rep) {
   if (!ctx) return DB200_ERR_INVALID;
-  if (n < 1 || d < 1 || l < 1 || q < 0 || !X || ldx < d || !y || !Omega || ldo < n || !Z || ldz < n)
+  if (n < 1 || d < 1 || l < 1 || q < 0 || !X || ldx < d || !y || !Omega || ldo < n || !Z || ldz < n ||
+      (precision != DB200_MIXED && precision != DB200_FP64))
     return fail(ctx, DB200_ERR_INVALID, "lowrank: bad arguments");
-  int st = lowrank_impl(ctx, n, d, l, q, X, ldx, y, Omega, ldo, gamma, Z, ldz, rep);
+  int st = lowrank_impl(ctx, n, d, l, q, X, ldx, y, Omega, ldo, gamma, precision, Z, ldz, rep);
   if (st) return st;
   return db200_synchronize(ctx);
 }
@@ -465,9 +564,12 @@ int db200_svm_solve(db200_context* ctx, int n, int d, int l, int q, const float*
   EventTimer total(ctx->stream);
   db200_svm_report local;
   std::memset(&local, 0, sizeof(local));
-  int st = db200_lowrank(ctx, n, d, l, q, X, ldx, y, Omega, ldo, gamma, Z, ldz, &local);
+  db200_barrier_params P;
+  if (p) P = *p;
+  else db200_barrier_defaults(&P);
+  int st = db200_lowrank(ctx, n, d, l, q, X, ldx, y, Omega, ldo, gamma, P.precision, Z, ldz, &local);
   if (st) return st;
-  st = db200_svm_barrier(ctx, n, l, Z, ldz, y, C, p, a, &local);
+  st = db200_svm_barrier(ctx, n, l, Z, ldz, y, C, &P, a, &local);
   local.ms_total = total.stop_ms();
   if (rep) *rep = local;
   return st;

@@ -56,6 +56,11 @@ def two_gaussians(n: int = 4096, d: int = 32, seed: int = 1) -> Workload:
     return Workload("two_gaussians", X, y, 1.0 / d, 128, 10, 1, 1.0, seed)
 
 
+def _two_gaussians_points(g, n, d):
+    y = np.where(g.random(n) < 0.5, 1.0, -1.0).astype(np.float32)
+    return (g.standard_normal((n, d)) + 0.5 * y[:, None]).astype(np.float32), y
+
+
 def uniform_hyperplane(n: int = 131072, d: int = 128, seed: int = 2, flip: float = 0.05) -> Workload:
     """Config 2: x ~ U[0,1)^d float32; y = sign(w.(x - mean)) for a seeded w, 5% of labels flipped;
     gamma = 0.5/d, r = 512 + 16, q = 1, C = 10."""
@@ -66,7 +71,8 @@ def uniform_hyperplane(n: int = 131072, d: int = 128, seed: int = 2, flip: float
     y = np.where(s >= 0, 1.0, -1.0)
     flips = g.random(n) < flip
     y[flips] = -y[flips]
-    return Workload("uniform_hyperplane", X, y.astype(np.float32), 0.5 / d, 512, 16, 1, 10.0, seed)
+    return Workload("uniform_hyperplane", X, y.astype(np.float32), 0.5 / d, 512, 16, 1, 10.0, seed,
+                    meta={"w": w, "mean": X.mean(axis=0, dtype=np.float64), "flip": flip})
 
 
 def sparse_binary(n: int = 262144, d: int = 123, seed: int = 3, p: float = 0.11) -> Workload:
@@ -81,7 +87,29 @@ def sparse_binary(n: int = 262144, d: int = 123, seed: int = 3, p: float = 0.11)
     s = X.astype(np.float64) @ w
     b = -s.mean()
     y = np.where(s + b + g.normal(0.0, 0.5, n) >= 0, 1.0, -1.0).astype(np.float32)
-    return Workload("sparse_binary", X, y, 0.05, 1024, 16, 1, 1.0, seed, meta={"b": b})
+    return Workload("sparse_binary", X, y, 0.05, 1024, 16, 1, 1.0, seed, meta={"b": b, "w": w, "p": p})
+
+
+def held_out(w: Workload, n_test: int) -> tuple[np.ndarray, np.ndarray]:
+    """Test points from the same distribution and labelling rule as `w` (same hyperplane / class means), drawn
+    from an independent stream (seed + 1 of the Philox family)."""
+    g = rng(w.seed + 1)
+    d = w.d
+    if w.name == "two_gaussians":
+        return _two_gaussians_points(g, n_test, d)
+    if w.name == "uniform_hyperplane":
+        X = g.random((n_test, d), dtype=np.float32)
+        s = (X.astype(np.float64) - w.meta["mean"]) @ w.meta["w"]
+        y = np.where(s >= 0, 1.0, -1.0)
+        flips = g.random(n_test) < w.meta["flip"]
+        y[flips] = -y[flips]
+        return X, y.astype(np.float32)
+    if w.name == "sparse_binary":
+        X = (g.random((n_test, d)) < w.meta["p"]).astype(np.float32)
+        s = X.astype(np.float64) @ w.meta["w"] + w.meta["b"]
+        y = np.where(s + g.normal(0.0, 0.5, n_test) >= 0, 1.0, -1.0).astype(np.float32)
+        return X, y
+    raise ValueError(w.name)
 
 
 CONFIGS = {

@@ -142,7 +142,18 @@ DB200_API int db200_trsm_lutn(db200_context* ctx, int m, int n, const double* R,
 typedef struct db200_barrier_params {
   double t0, mu, alpha, beta, gap_tol, newton_tol;
   int max_outer, max_newton;
+  int precision;   /* DB200_MIXED (default) or DB200_FP64, see below */
+  int refine_max;  /* iterative-refinement steps per Newton solve in DB200_MIXED (default 6) */
 } db200_barrier_params;
+
+/* Precision of the path.
+ * DB200_MIXED: kernel passes on the tensor cores in split bf16 (fp32 accumulation); the Woodbury capacity matrix
+ *   I + Z^T D^-1 Z formed on the tensor cores (split bf16) and factored in FP64 while each Newton step refined
+ *   against the exact FP64 operator (Z Z^T + D) reaches relative residual 1e-10, the FP64 capacity matrix after;
+ *   objective, gradients, gap and line search in FP64.
+ * DB200_FP64: plain FP64 everywhere (FP64 kernel blocks and products, FP64 capacity matrix): the comparator. */
+#define DB200_MIXED 0
+#define DB200_FP64 1
 
 /* What a solve did and where it ended. */
 typedef struct db200_svm_report {
@@ -153,6 +164,9 @@ typedef struct db200_svm_report {
   double nu;               /* shift of the Nystrom core Cholesky */
   int outer, newton;       /* barrier and Newton iterations */
   int status;              /* DB200_OK, DB200_ERR_MAXITER (caps reached) */
+  int refine;              /* iterative-refinement steps taken (DB200_MIXED) */
+  int fallbacks;           /* DB200_MIXED: 1 if a Newton step missed the refinement tolerance with the tensor-core
+                              capacity matrix, after which the FP64 capacity matrix was used */
   double ms_sketch, ms_orth, ms_core, ms_barrier, ms_total;
 } db200_svm_report;
 
@@ -169,16 +183,86 @@ DB200_API int db200_svm_barrier(db200_context* ctx, int n, int r, const double* 
 
 /* Low-rank factor Z (n x l FP64, Z Z^T ~ diag(y) K diag(y)) by the randomised range finder of
  * tests/testsvm.cpp:86-170, corrected: Y = K Omega; Q = orth(Y); q times {Y = K Q; Q = orth(Y)};
- * C = Q^T K Q; R^T R = C + nu I; Z = Q R^T.  K products use the fused kernel (db200_rbf_sketch), orth is
- * db200_cholqr2.  X point-major (ldx >= d), y and Omega (n x l, ldo >= n) device.  Synchronous. */
+ * C = Q^T K Q; R^T R = C + nu I; Z = Q R^T.  K products use the fused kernel (db200_rbf_sketch) with
+ * precision DB200_MIXED or the FP64 comparator (db200_rbf_sketch_f64) with DB200_FP64; orth is db200_cholqr2.
+ * X point-major (ldx >= d), y and Omega (n x l, ldo >= n) device.  Synchronous. */
 DB200_API int db200_lowrank(db200_context* ctx, int n, int d, int l, int q, const float* X, int ldx, const float* y,
-                            const float* Omega, int ldo, float gamma, double* Z, int ldz, db200_svm_report* rep);
+                            const float* Omega, int ldo, float gamma, int precision, double* Z, int ldz,
+                            db200_svm_report* rep);
 
 /* The whole path: db200_lowrank followed by db200_svm_barrier (tests/testsvm.cpp:34-329 at one rank).
  * Outputs a (n, FP64) and Z (n x l FP64).  Synchronous; rep may be NULL. */
 DB200_API int db200_svm_solve(db200_context* ctx, int n, int d, int l, int q, const float* X, int ldx,
                               const float* y, const float* Omega, int ldo, float gamma, double C,
                               const db200_barrier_params* p, double* a, double* Z, int ldz, db200_svm_report* rep);
+
+/* ------------------------------------------------------------------------------------------------------
+ * Support for the one-rank DArray mirror (the headers under include/darray_b200/) and other host callers.
+ * ------------------------------------------------------------------------------------------------------ */
+
+/* Process-wide context on device 0 with its own stream (created on first use), the counterpart of the
+ * reference's global handles set up by cuda_init() (include/dkernel.cu:12-17, 28-35). */
+DB200_API db200_context* db200_default_context(void);
+DB200_API int db200_release_default_context(void);
+
+/* Device memory and stream-ordered copies on the context's stream (db200_copy_to_host also synchronizes). */
+DB200_API int db200_malloc(db200_context* ctx, size_t bytes, void** ptr);
+DB200_API int db200_free(db200_context* ctx, void* ptr);
+DB200_API int db200_copy_to_device(db200_context* ctx, void* dst, const void* src, size_t bytes);
+DB200_API int db200_copy_to_host(db200_context* ctx, void* dst, const void* src, size_t bytes);
+
+/* C(m x n) = alpha op(A) op(B) + beta C, FP64, op in {N, T}; (T, T) is not provided.  Replaces
+ * multiply_matrix<double> (include/cblas_like.h:51-60). */
+DB200_API int db200_gemm(db200_context* ctx, char transA, char transB, int m, int n, int k, double alpha,
+                         const double* A, int lda, const double* B, int ldb, double beta, double* C, int ldc);
+
+/* C(m x n) = alpha op(A) B + beta C on FP32 data with FP64 accumulation, op(A) in {N, T} as in tc_sgemm
+ * (include/dkernel.cu:234-275) and tc_gemm (:194-231, which ignored beta). */
+DB200_API int db200_sgemm(db200_context* ctx, char transA, char transB, int m, int n, int k, float alpha,
+                          const float* A, int lda, const float* B, int ldb, float beta, float* C, int ldc);
+
+/* Singular values (descending) of the n x n matrix A, FP64 one-sided Jacobi; A is destroyed.  Replaces svd
+ * (include/lapack_like.h:389-413), which returns only the singular values.  Synchronous. */
+DB200_API int db200_svd_values(db200_context* ctx, int n, double* A, int lda, double* S);
+
+/* Residual of a low-rank factor: out3 = {||K||_F, ||K - Z Z^T||_F, ratio} with K = diag(y) K(X, X) diag(y),
+ * X point-major (ldx >= d), Z n x k FP64.  Replaces Knorm (include/dkernel.h:50-76), corrected to measure
+ * K - Z Z^T and to accumulate over every block.  Synchronous. */
+DB200_API int db200_knorm(db200_context* ctx, int n, int d, int k, const float* X, int ldx, const float* y,
+                          const double* Z, int ldz, float gamma, double* out3);
+
+/* x = (Z Z^T + diag(g))^-1 b by Sherman-Morrison-Woodbury with an FP64 Cholesky of I + Z^T g^-1 Z (Z n x r).
+ * Solves the system pre_conjgrad (include/dbarrier.h:84-139) iterates on, exactly.  Synchronous. */
+DB200_API int db200_woodbury_solve(db200_context* ctx, int n, int r, const double* Z, int ldz, const double* diag,
+                                   const double* b, double* x);
+
+/* Upper triangle of M(r x r) = Z^T diag(w) Z for Z n x r FP64 (w may be NULL = ones): the capacity-matrix
+ * SYRK of the Woodbury Newton step (symmetric_update, include/cblas_like.h:62-69, with a row weight).
+ * use_tensor_cores = 0: FP64 pipes; 1: tcgen05 split bf16 (hi.hi + hi.lo + lo.hi, relative error ~1e-5).
+ * Stream-ordered. */
+DB200_API int db200_gram_weighted(db200_context* ctx, int n, int r, const double* Z, int ldz, const double* w,
+                                  double* M, int ldm, int use_tensor_cores);
+
+/* Plain FP64 kernel x sketch (device pointers), the comparator of db200_rbf_sketch:
+ *     Y(m x l, FP64) = diag(yi) K(Xi, Xj) diag(yj) Omega(n x l, FP64)
+ * with FP64 distances, exp and products on the FP64 pipes (row blocks of K are materialised in FP64).
+ * Xi, Xj point-major float (ldxi, ldxj >= d).  Stream-ordered. */
+DB200_API int db200_rbf_sketch_f64(db200_context* ctx, int m, int n, int d, int l, const float* Xi, int ldxi,
+                                   const float* Xj, int ldxj, const float* yi, const float* yj, const double* Omega,
+                                   int ldo, double* Y, int ldy, double gamma);
+
+/* y = alpha x + beta y + gamma elementwise on n FP64 device values (x may be NULL): the vector updates of
+ * include/dbarrier.h:60-73 (Grad = Grad_f + Grad_Phi) and of the D + n I shift of pre_conjgrad. */
+DB200_API int db200_vec_update(db200_context* ctx, int n, double alpha, const double* x, double beta, double* y,
+                               double gamma);
+
+/* The barrier terms at a (device vectors of length n, any output may be NULL): gradf = Z Z^T a - 1 (Grad_f),
+ * gradphi = (-1/a + 1/(C-a))/t (Grad_Phi), grad = gradf + gradphi (Grad), D = (1/a^2 + 1/(C-a)^2)/t (Hess_Phi),
+ * and on the host f_gg[0] = f(a) = 0.5 a^T Z Z^T a - 1^T a (f), f_gg[1] = f(a) - sum(log a + log(C-a))/t (gg).
+ * include/dbarrier.h:14-81.  Synchronous. */
+DB200_API int db200_barrier_terms(db200_context* ctx, int n, int k, const double* Z, int ldz, const double* a,
+                                  double C, double t, double* gradf, double* gradphi, double* grad, double* D,
+                                  double* f_gg);
 
 /*
  * Allocation-free fused RBF x sketch.  No counterpart in the reference: it exists for callers that cannot call

@@ -135,3 +135,66 @@ def test_trsm_lutn_matches_oracle(gpu_ctx, m, n):
         dU2, dB2 = d64(G["trsm_U"]), d64(G["trsm_B"])
         gpu_ctx.trsm_lutn(64, 7, dU2.data_ptr(), 64, dB2.data_ptr(), 64)
         assert rel(h64(dB2, 64), G["trsm_X"].astype(np.float64)) < 1e-5
+
+
+def test_svd_values_match_reference_and_oracle(gpu_ctx):
+    A = G["svd_A"].astype(np.float64)
+    n = A.shape[0]
+    dA = d64(A)
+    import torch
+    dS = torch.zeros(n, dtype=torch.float64, device="cuda")
+    gpu_ctx.svd_values(n, dA.data_ptr(), n, dS.data_ptr())
+    S = dS.cpu().numpy()
+    assert rel(S, O.svd_values(A)) < 1e-12
+    assert rel(S, G["svd_S"].astype(np.float64)) < 1e-5  # the reference's sgesvd
+
+
+@pytest.mark.parametrize("ta", ["N", "T"])
+def test_sgemm_matches_numpy(gpu_ctx, ta):
+    import torch
+    g = np.random.default_rng(3)
+    m, n, k = 70, 45, 300
+    A = g.standard_normal((m, k) if ta == "N" else (k, m)).astype(np.float32)
+    B = g.standard_normal((k, n)).astype(np.float32)
+    C = g.standard_normal((m, n)).astype(np.float32)
+    dA = torch.from_numpy(np.ascontiguousarray(A.T)).cuda()
+    dB = torch.from_numpy(np.ascontiguousarray(B.T)).cuda()
+    dC = torch.from_numpy(np.ascontiguousarray(C.T)).cuda()
+    lda = A.shape[0]
+    gpu_ctx.sgemm(ta, "N", m, n, k, 1.5, dA.data_ptr(), lda, dB.data_ptr(), k, -0.5, dC.data_ptr(), m)
+    gpu_ctx.sync()
+    opA = A.astype(np.float64) if ta == "N" else A.astype(np.float64).T
+    ref = 1.5 * opA @ B - 0.5 * C
+    assert rel(dC.cpu().numpy().T, ref) < 1e-6
+
+
+@pytest.mark.parametrize("ta,tb", [("N", "N"), ("N", "T"), ("T", "N")])
+def test_gemm_matches_numpy(gpu_ctx, ta, tb):
+    g = np.random.default_rng(4)
+    m, n, k = 90, 33, 200
+    A = g.standard_normal((m, k) if ta == "N" else (k, m))
+    B = g.standard_normal((k, n) if tb == "N" else (n, k))
+    C = g.standard_normal((m, n))
+    dA, dB, dC = d64(A), d64(B), d64(C)
+    gpu_ctx.gemm(ta, tb, m, n, k, 2.0, dA.data_ptr(), A.shape[0], dB.data_ptr(), B.shape[0], 0.25, dC.data_ptr(), m)
+    gpu_ctx.sync()
+    opA = A if ta == "N" else A.T
+    opB = B if tb == "N" else B.T
+    assert rel(h64(dC, m), 2.0 * opA @ opB + 0.25 * C) < 1e-13
+
+
+@pytest.mark.parametrize("n,r,tc", [(2048, 56, 1), (5000, 300, 1), (131, 70, 1), (5000, 300, 0)])
+def test_gram_weighted_matches_numpy(gpu_ctx, n, r, tc):
+    """Capacity-matrix SYRK Z^T diag(w) Z: FP64 pipes to 1e-13, tensor-core split bf16 to 1e-5 (upper triangle)."""
+    import torch
+    g = np.random.default_rng(n + r)
+    Z = g.standard_normal((n, r)) * 0.3
+    w = np.exp(g.uniform(-6, 6, n))
+    dZ = d64(Z)
+    dw = torch.from_numpy(w).cuda()
+    dM = d64(np.full((r, r), 7.0))
+    gpu_ctx.gram_weighted(n, r, dZ.data_ptr(), n, dw.data_ptr(), dM.data_ptr(), r, tc)
+    gpu_ctx.sync()
+    M = np.triu(h64(dM, r))
+    ref = np.triu(Z.T @ (w[:, None] * Z))
+    assert rel(M, ref) < (1e-5 if tc else 1e-13)

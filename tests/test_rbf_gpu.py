@@ -113,3 +113,21 @@ def test_rbf_sketch_two_calls_reuse_workspace(gpu_ctx):
         gpu_ctx.sync()
         outs.append(colmajor_host(Y, n))
     assert np.array_equal(outs[0], outs[1])  # deterministic: same tiles, same order
+
+
+@pytest.mark.parametrize("m,n,d,l", [(300, 777, 33, 40), (1000, 1000, 128, 138)])
+def test_rbf_sketch_f64_matches_oracle(gpu_ctx, m, n, d, l):
+    """The plain FP64 comparator pass agrees with the FP64 oracle to relative 1e-12."""
+    import torch
+    Xi = _points(m, d, 31, 0.5)
+    Xj = Xi if m == n else _points(n, d, 32, 0.5)
+    yi, yj = _labels(m, 5), _labels(n, 6)
+    Om = np.asfortranarray(np.random.default_rng(2).standard_normal((n, l)))
+    gamma = 1.0 / d
+    Yref = O.sketch(Xi, Xj, yi, yj, Om, gamma)
+    dXi, dXj, dyi, dyj = dev(Xi), dev(Xj), dev(yi), dev(yj)
+    dOm = torch.from_numpy(np.ascontiguousarray(Om.T)).cuda()
+    Y = torch.zeros((l, m), dtype=torch.float64, device="cuda")
+    gpu_ctx.rbf_sketch_f64(m, n, d, l, ptr(dXi), d, ptr(dXj), d, ptr(dyi), ptr(dyj), ptr(dOm), n, ptr(Y), m, gamma)
+    gpu_ctx.sync()
+    assert rel_fro(Y.cpu().numpy().T, Yref) <= 1e-12
