@@ -67,6 +67,11 @@ DB200_API void* db200_stream(const db200_context* ctx);
 /* Number of kernels this library has launched on this context since creation (launch accounting). */
 DB200_API int64_t db200_launch_count(const db200_context* ctx);
 
+/* Failure-path self-test of the bounded device waits: queues a kernel that waits on a flag nothing sets and
+ * gives up after limit_ms (1..5000).  The next db200_synchronize returns DB200_ERR_TIMEOUT and clears it; the
+ * context remains usable.  Stream-ordered. */
+DB200_API int db200_selftest_wait_timeout(db200_context* ctx, int limit_ms);
+
 /* Enable (1) or disable (0) CUDA-event timing of every tcgen05 tile-kernel launch on the context's stream;
  * db200_profile_read() returns the summed kernel time (ms) and the number of timed launches since the last
  * read, then clears them.  Both synchronize the stream. */

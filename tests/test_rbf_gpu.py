@@ -131,3 +131,23 @@ def test_rbf_sketch_f64_matches_oracle(gpu_ctx, m, n, d, l):
     gpu_ctx.rbf_sketch_f64(m, n, d, l, ptr(dXi), d, ptr(dXj), d, ptr(dyi), ptr(dyj), ptr(dOm), n, ptr(Y), m, gamma)
     gpu_ctx.sync()
     assert rel_fro(Y.cpu().numpy().T, Yref) <= 1e-12
+
+
+def test_bounded_wait_expiry_reports_timeout_and_context_survives(gpu_ctx):
+    """A device wait on a flag nothing sets runs out after 20 ms: DB200_ERR_TIMEOUT at synchronize, then the same
+    context runs a sketch normally."""
+    from darray_optimizer_b200._lib import DB200Error
+    assert gpu_ctx.lib.db200_selftest_wait_timeout(gpu_ctx.h, 20) == 0
+    with pytest.raises(DB200Error) as ei:
+        gpu_ctx.sync()
+    assert ei.value.status == -6  # DB200_ERR_TIMEOUT
+    gpu_ctx.sync()  # the status word was cleared
+    n, d, l = 256, 16, 16
+    X = _points(n, d, 3)
+    y = _labels(n, 3)
+    Om = np.asfortranarray(np.random.default_rng(1).standard_normal((n, l)).astype(np.float32))
+    dX, dy, dO = dev(X), dev(y), dev(Om)
+    Y = colmajor_empty(n, l)
+    gpu_ctx.rbf_sketch(n, n, d, l, ptr(dX), d, ptr(dX), d, POINT_MAJOR, ptr(dy), ptr(dy), ptr(dO), n, ptr(Y), n, 0.1)
+    gpu_ctx.sync()
+    assert rel_fro(colmajor_host(Y, n), O.sketch(X, X, y, y, Om, 0.1)) <= 1e-2
