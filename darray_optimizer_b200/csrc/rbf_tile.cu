@@ -13,8 +13,9 @@
 // so the kernel matrix is never written to HBM in SKETCH mode.  Algorithm restated from
 // include/dkernel.cu:102-129 (vecnorm, rbf) and :151-178 / :194-231 (distance GEMM, rbf, sketch GEMM).
 //
-// Warp roles (320 threads): warp 0 = TMA producer, warp 1 = TMEM allocator + MMA issuer,
-// warps 2..9 = epilogue (two warps per TMEM lane quadrant, each owning 64 of the 128 tile columns).
+// Warp roles (352 threads): warp 0 = TMA producer of the point tiles, warp 10 = TMA producer of the sketch
+// operand, warp 1 = TMEM allocator + MMA issuer, warps 2..9 = epilogue (two warps per TMEM lane quadrant, each
+// owning 64 of the 128 tile columns).  Two producers keep the Xj stream running while the Omega ring is full.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cstdio>
@@ -31,7 +32,7 @@ constexpr int BM = 128;          // rows of i per CTA (UMMA M)
 constexpr int BN = 128;          // columns of j per tile
 constexpr int KC = 64;           // bf16 elements per 128-byte swizzled row chunk
 constexpr int CHUNK_BYTES = BM * KC * 2;  // one 128 x 64 bf16 chunk = 16 KB
-constexpr int NUM_THREADS = 320;
+constexpr int NUM_THREADS = 352;  // warp 0 Xi/Xj TMA, warp 1 MMA, warps 2..9 epilogue, warp 10 Omega TMA
 constexpr int NUM_EPI_WARPS = 8;
 constexpr int TMEM_COLS = 512;
 constexpr int SMEM_LIMIT = 232448;  // dynamic shared memory per block on sm_100
@@ -148,26 +149,30 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
 
-  if (warp == 0) {
-    // ------------------------------------------------------------ TMA producer
+  if (warp == 0 || warp == 10) {
+    // ------------------------------------------------------------ TMA producers
     if (lane == 0) {
+      const bool points = (warp == 0);
       uint32_t kx = 0, ko = 0, items_done = 0, xi_loads = 0;
       bool ok = true;
       for (int item = blockIdx.x; item < n_items && ok; item += gridDim.x, ++items_done) {
         const int it = item % args.n_itiles, pn = item / args.n_itiles;
-        if (!mbar_wait(bar(B_XI_EMPTY), (items_done & 1) ^ 1, abort_flag)) { ok = false; break; }
-        mbar_arrive_expect_tx(bar(B_XI_FULL), L.nkc * CHUNK_BYTES);
-        ++xi_loads;
-        for (int c = 0; c < L.nkc; ++c)
-          tma_load_2d(s_xi + c * CHUNK_BYTES, &tm_xi, bar(B_XI_FULL), c * KC, it * BM);
+        if (points) {
+          if (!mbar_wait(bar(B_XI_EMPTY), (items_done & 1) ^ 1, abort_flag)) { ok = false; break; }
+          mbar_arrive_expect_tx(bar(B_XI_FULL), L.nkc * CHUNK_BYTES);
+          ++xi_loads;
+          for (int c = 0; c < L.nkc; ++c)
+            tma_load_2d(s_xi + c * CHUNK_BYTES, &tm_xi, bar(B_XI_FULL), c * KC, it * BM);
+        }
         for (int jt = 0; jt < args.n_jtiles && ok; ++jt) {
-          for (int c = 0; c < L.nkc; ++c, ++kx) {
-            const uint32_t s = kx % nsx, ph = (kx / nsx) & 1;
-            if (!mbar_wait(bar(XJ_EMPTY + s), ph ^ 1, abort_flag)) { ok = false; break; }
-            mbar_arrive_expect_tx(bar(XJ_FULL + s), CHUNK_BYTES);
-            tma_load_2d(s_xj + s * CHUNK_BYTES, &tm_xj, bar(XJ_FULL + s), c * KC, jt * BN);
-          }
-          if (MODE == RBF_MODE_SKETCH) {
+          if (points) {
+            for (int c = 0; c < L.nkc; ++c, ++kx) {
+              const uint32_t s = kx % nsx, ph = (kx / nsx) & 1;
+              if (!mbar_wait(bar(XJ_EMPTY + s), ph ^ 1, abort_flag)) { ok = false; break; }
+              mbar_arrive_expect_tx(bar(XJ_FULL + s), CHUNK_BYTES);
+              tma_load_2d(s_xj + s * CHUNK_BYTES, &tm_xj, bar(XJ_FULL + s), c * KC, jt * BN);
+            }
+          } else if (MODE == RBF_MODE_SKETCH) {
             for (int c = 0; c < 2 && ok; ++c, ++ko) {
               const uint32_t s = ko % nso, ph = (ko / nso) & 1;
               if (!mbar_wait(bar(OM_EMPTY + s), ph ^ 1, abort_flag)) { ok = false; break; }
@@ -194,8 +199,8 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
     // ------------------------------------------------------------ MMA issuer
     if (lane == 0) {
       const uint32_t idesc_g = idesc_f16(BM, BN, true);
-      // sketch panel: one MMA of N <= 256 columns, or 256 + (panel - 256)
-      const int n1 = args.panel > 256 ? 256 : args.panel, n2 = args.panel - n1;
+      // sketch panel: one MMA of N <= 256 columns, or two of about half each (multiples of 16)
+      const int n1 = args.panel > 256 ? (args.panel / 32) * 16 : args.panel, n2 = args.panel - n1;
       const uint32_t idesc_y1 = idesc_f16(BM, n1, true);
       const uint32_t idesc_y2 = idesc_f16(BM, n2 > 0 ? n2 : 16, true);
       const int dp = args.dp;
@@ -261,7 +266,8 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
                 const uint64_t bdesc = dom + ((s * L.om_stage + ks * 32) >> 4);
                 const uint32_t acc = (jt | c | ks) ? 1u : 0u;
                 umma_f16_ts(tmem_base + args.tmem_y, a_tmem, bdesc, idesc_y1, acc);
-                if (n2 > 0) umma_f16_ts(tmem_base + args.tmem_y + 256, a_tmem, bdesc + ((256 * 128) >> 4), idesc_y2, acc);
+                if (n2 > 0)
+                  umma_f16_ts(tmem_base + args.tmem_y + n1, a_tmem, bdesc + ((n1 * 128) >> 4), idesc_y2, acc);
               }
               umma_commit(bar(OM_EMPTY + s));
             }
@@ -280,7 +286,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
       mbar_wait(bar(B_DRAIN), 0, &never);
     }
     __syncwarp();
-  } else {
+  } else if (warp >= 2 && warp <= 9) {
     // ------------------------------------------------------------ epilogue
     const int ew = warp - 2;              // 0..7
     const int q = warp & 3;               // TMEM lane quadrant this warp may access
