@@ -91,13 +91,14 @@ enum {
   B_XJ_FULL0,  // nsx full, then nsx empty, then nso full, nso empty
 };
 
-template <int MODE>
+template <int MODE, int DP, bool TWO_Y>
 __global__ void __launch_bounds__(NUM_THREADS, 1)
     rbf_tile_kernel(const __grid_constant__ CUtensorMap tm_xi, const __grid_constant__ CUtensorMap tm_xj,
                     const __grid_constant__ CUtensorMap tm_om, TileArgs args) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  const SmemLayout L = make_layout(args.dp, args.panel, args.nsx, args.nso);
+  constexpr int NKC = (2 * DP) / KC;  // 64-element chunks per packed row [hi | lo]
+  const SmemLayout L = make_layout(DP, args.panel, args.nsx, args.nso);
   const int nsx = args.nsx, nso = args.nso, gb = args.g_bufs;
   const uint32_t s_xi = smem_u32(smem + L.off_xi);
   const uint32_t s_xj = smem_u32(smem + L.off_xj);
@@ -197,94 +198,108 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
     __syncwarp();
   } else if (warp == 1) {
     // ------------------------------------------------------------ MMA issuer
-    if (lane == 0) {
-      const uint32_t idesc_g = idesc_f16(BM, BN, true);
-      // sketch panel: one MMA of N <= 256 columns, or two of about half each (multiples of 16)
-      const int n1 = args.panel > 256 ? (args.panel / 32) * 16 : args.panel, n2 = args.panel - n1;
-      const uint32_t idesc_y1 = idesc_f16(BM, n1, true);
-      const uint32_t idesc_y2 = idesc_f16(BM, n2 > 0 ? n2 : 16, true);
-      const int dp = args.dp;
-      uint32_t kx = 0, ko = 0, kg = 0, kp = 0, items_done = 0;
-      bool ok = true;
-      // Descriptors are affine in the shared address (start address in the low 14 bits, in 16-byte units):
-      // build the base descriptors once and add offsets.
-      const uint64_t dxi = sdesc_k_sw128(s_xi), dxj = sdesc_k_sw128(s_xj), dom = sdesc_k_sw128(s_om);
+    // The whole warp runs the schedule converged and waits together; one elected lane issues each block of
+    // MMAs.  Every branch between MMAs is resolved at compile time (DP, TWO_Y): a lone issuing lane that waits
+    // on mbarriers or branches between MMAs cannot keep the tensor pipe fed.
+    constexpr uint32_t idesc_g = idesc_f16(BM, BN, true);
+    const int n1 = TWO_Y ? (args.panel / 32) * 16 : args.panel, n2 = args.panel - n1;
+    const uint32_t idesc_y1 = idesc_f16(BM, n1, true);
+    const uint32_t idesc_y2 = idesc_f16(BM, TWO_Y ? n2 : 16, true);
+    const uint32_t y2_boff = (uint32_t)(n1 * 128) >> 4;
+    const uint32_t om_stage16 = (uint32_t)L.om_stage >> 4;
+    uint32_t xs = 0, xph = 0, os = 0, oph = 0, gbi = 0, gph = 0, pph = 0, items_done = 0;
+    bool ok = true;
+    // Descriptors are affine in the shared address (start address in the low 14 bits, in 16-byte units):
+    // build the base descriptors once and add offsets.
+    const uint64_t dxi = sdesc_k_sw128(s_xi), dxj = sdesc_k_sw128(s_xj), dom = sdesc_k_sw128(s_om);
+    auto wait_all = [&](uint32_t b, uint32_t parity) -> bool {
+      return __all_sync(0xffffffffu, mbar_wait(b, parity, abort_flag));
+    };
 
-      auto issue_mma1 = [&]() -> bool {
-        const uint32_t b = kg % gb, ph = (kg / gb) & 1;
-        if (!mbar_wait(bar(B_G_EMPTY0 + b), ph ^ 1, abort_flag)) return false;
+    auto issue_mma1 = [&]() -> bool {
+      if (!wait_all(bar(B_G_EMPTY0 + gbi), gph ^ 1)) return false;
+      tc_fence_after();
+      const uint32_t d_tmem = tmem_base + gbi * BN;
+#pragma unroll
+      for (int c = 0; c < NKC; ++c) {
+        if (!wait_all(bar(XJ_FULL + xs), xph)) return false;
         tc_fence_after();
-        const uint32_t d_tmem = tmem_base + b * BN;
-        bool first = true;
-        for (int c = 0; c < L.nkc; ++c, ++kx) {
-          const uint32_t s = kx % nsx, sph = (kx / nsx) & 1;
-          if (!mbar_wait(bar(XJ_FULL + s), sph, abort_flag)) return false;
-          tc_fence_after();
+        if (elect_one()) {
+          const uint64_t bbase = dxj + ((xs * CHUNK_BYTES) >> 4);
 #pragma unroll
           for (int ks = 0; ks < KC / 16; ++ks) {
-            const int o = c * KC + ks * 16;  // K offset of this slice inside the packed row
-            const uint64_t bdesc = dxj + ((s * CHUNK_BYTES + ks * 32) >> 4);
-            if (o < dp) {  // B slice is hi_j: pair with hi_i and lo_i
-              const int oh = o, ol = dp + o;
+            const int o = c * KC + ks * 16;  // K offset of this slice inside the packed row [hi | lo]
+            const uint64_t bdesc = bbase + ((ks * 32) >> 4);
+            if (o < DP) {  // B slice is hi_j: pair with hi_i and lo_i
+              const int oh = o, ol = DP + o;
               umma_f16(d_tmem, dxi + (((oh / KC) * CHUNK_BYTES + (oh % KC) * 2) >> 4), bdesc, idesc_g,
-                       first ? 0u : 1u);
-              first = false;
+                       o == 0 ? 0u : 1u);
               umma_f16(d_tmem, dxi + (((ol / KC) * CHUNK_BYTES + (ol % KC) * 2) >> 4), bdesc, idesc_g, 1u);
             } else {  // B slice is lo_j: pair with hi_i
-              const int oh = o - dp;
+              const int oh = o - DP;
               umma_f16(d_tmem, dxi + (((oh / KC) * CHUNK_BYTES + (oh % KC) * 2) >> 4), bdesc, idesc_g, 1u);
             }
           }
-          umma_commit(bar(XJ_EMPTY + s));
+          umma_commit(bar(XJ_EMPTY + xs));
+          if (c == NKC - 1) umma_commit(bar(B_G_FULL0 + gbi));
         }
-        umma_commit(bar(B_G_FULL0 + b));
-        ++kg;
-        return true;
-      };
+        __syncwarp();
+        if (++xs == (uint32_t)nsx) { xs = 0; xph ^= 1; }
+      }
+      if (++gbi == (uint32_t)gb) { gbi = 0; gph ^= 1; }
+      return true;
+    };
 
-      for (int item = blockIdx.x; item < n_items && ok; item += gridDim.x, ++items_done) {
-        if (!mbar_wait(bar(B_XI_FULL), items_done & 1, abort_flag)) { ok = false; break; }
+    for (int item = blockIdx.x; item < n_items && ok; item += gridDim.x, ++items_done) {
+      if (!wait_all(bar(B_XI_FULL), items_done & 1)) { ok = false; break; }
+      tc_fence_after();
+      if (MODE == RBF_MODE_SKETCH && items_done > 0) {
+        if (!wait_all(bar(B_Y_EMPTY), (items_done - 1) & 1)) { ok = false; break; }
         tc_fence_after();
-        if (MODE == RBF_MODE_SKETCH && items_done > 0) {
-          if (!mbar_wait(bar(B_Y_EMPTY), (items_done - 1) & 1, abort_flag)) { ok = false; break; }
+      }
+      if (!issue_mma1()) { ok = false; break; }
+      for (int jt = 0; jt < args.n_jtiles; ++jt) {
+        if (jt + 1 < args.n_jtiles && !issue_mma1()) { ok = false; break; }
+        if (MODE == RBF_MODE_SKETCH) {
+          if (!wait_all(bar(B_P_FULL), pph)) { ok = false; break; }
           tc_fence_after();
-        }
-        if (!issue_mma1()) { ok = false; break; }
-        for (int jt = 0; jt < args.n_jtiles; ++jt) {
-          if (jt + 1 < args.n_jtiles && !issue_mma1()) { ok = false; break; }
-          if (MODE == RBF_MODE_SKETCH) {
-            if (!mbar_wait(bar(B_P_FULL), kp & 1, abort_flag)) { ok = false; break; }
+          pph ^= 1;
+#pragma unroll
+          for (int c = 0; c < 2; ++c) {
+            if (!wait_all(bar(OM_FULL + os), oph)) { ok = false; break; }
             tc_fence_after();
-            for (int c = 0; c < 2 && ok; ++c, ++ko) {
-              const uint32_t s = ko % nso, sph = (ko / nso) & 1;
-              if (!mbar_wait(bar(OM_FULL + s), sph, abort_flag)) { ok = false; break; }
-              tc_fence_after();
+            if (elect_one()) {
+              const uint64_t bbase = dom + os * om_stage16;
 #pragma unroll
               for (int ks = 0; ks < KC / 16; ++ks) {
                 // A = P (bf16 in TMEM, 8 columns per 16-wide K step), B = Omega~ rows of this panel
                 const uint32_t a_tmem = tmem_base + args.tmem_p + c * 32 + ks * 8;
-                const uint64_t bdesc = dom + ((s * L.om_stage + ks * 32) >> 4);
-                const uint32_t acc = (jt | c | ks) ? 1u : 0u;
+                const uint64_t bdesc = bbase + ((ks * 32) >> 4);
+                const uint32_t acc = (jt > 0 || c > 0 || ks > 0) ? 1u : 0u;
                 umma_f16_ts(tmem_base + args.tmem_y, a_tmem, bdesc, idesc_y1, acc);
-                if (n2 > 0)
-                  umma_f16_ts(tmem_base + args.tmem_y + n1, a_tmem, bdesc + ((n1 * 128) >> 4), idesc_y2, acc);
+                if (TWO_Y) umma_f16_ts(tmem_base + args.tmem_y + n1, a_tmem, bdesc + y2_boff, idesc_y2, acc);
               }
-              umma_commit(bar(OM_EMPTY + s));
+              umma_commit(bar(OM_EMPTY + os));
+              if (c == 1) umma_commit(bar(B_P_EMPTY));
             }
-            if (!ok) break;
-            umma_commit(bar(B_P_EMPTY));
-            ++kp;
+            __syncwarp();
+            if (++os == (uint32_t)nso) { os = 0; oph ^= 1; }
           }
+          if (!ok) break;
         }
-        if (!ok) break;
+      }
+      if (!ok) break;
+      if (elect_one()) {
         umma_commit(bar(B_XI_EMPTY));
         if (MODE == RBF_MODE_SKETCH) umma_commit(bar(B_Y_FULL));
       }
-      // All MMAs issued by this thread must be complete before TMEM is released.
-      umma_commit(bar(B_DRAIN));
-      volatile int never = 0;
-      mbar_wait(bar(B_DRAIN), 0, &never);
+      __syncwarp();
     }
+    // All MMAs issued by this warp must be complete before TMEM is released.
+    if (elect_one()) umma_commit(bar(B_DRAIN));
+    __syncwarp();
+    volatile int never = 0;
+    mbar_wait(bar(B_DRAIN), 0, &never);
     __syncwarp();
   } else if (warp >= 2 && warp <= 9) {
     // ------------------------------------------------------------ epilogue
@@ -454,6 +469,18 @@ bool make_tmap(CUtensorMap* tm, const void* base, uint64_t inner, uint64_t outer
   return r == CUDA_SUCCESS;
 }
 
+template <int DP>
+cudaError_t launch_tile_kernel(int mode, bool two_y, int grid, size_t smem, cudaStream_t st, const CUtensorMap& tm_xi,
+                               const CUtensorMap& tm_xj, const CUtensorMap& tm_om, const TileArgs& a) {
+  auto k = (mode == RBF_MODE_SKETCH) ? (two_y ? rbf_tile_kernel<RBF_MODE_SKETCH, DP, true>
+                                              : rbf_tile_kernel<RBF_MODE_SKETCH, DP, false>)
+                                     : rbf_tile_kernel<RBF_MODE_KBLOCK, DP, false>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  k<<<grid, NUM_THREADS, smem, st>>>(tm_xi, tm_xj, tm_om, a);
+  return cudaGetLastError();
+}
+
 }  // namespace
 
 int feature_pad(int d) { return round_up(d < 1 ? 1 : d, 32); }
@@ -561,15 +588,16 @@ int launch_rbf_tiles(db200_context* ctx, int mode, const PackedPoints& pi, const
   const int grid = n_items < ctx->num_sms ? n_items : ctx->num_sms;
   cudaEvent_t e0 = nullptr;
   prof_begin(ctx, &e0);
-  if (mode == RBF_MODE_SKETCH) {
-    DB200_CUDA(ctx, cudaFuncSetAttribute(rbf_tile_kernel<RBF_MODE_SKETCH>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    rbf_tile_kernel<RBF_MODE_SKETCH><<<grid, NUM_THREADS, smem, ctx->stream>>>(tm_xi, tm_xj, tm_om, a);
-  } else {
-    DB200_CUDA(ctx, cudaFuncSetAttribute(rbf_tile_kernel<RBF_MODE_KBLOCK>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    rbf_tile_kernel<RBF_MODE_KBLOCK><<<grid, NUM_THREADS, smem, ctx->stream>>>(tm_xi, tm_xj, tm_om, a);
+  const bool two_y = (mode == RBF_MODE_SKETCH) && a.panel > 256;
+  cudaError_t err = cudaSuccess;
+  switch (a.dp) {
+    case 32: err = launch_tile_kernel<32>(mode, two_y, grid, smem, ctx->stream, tm_xi, tm_xj, tm_om, a); break;
+    case 64: err = launch_tile_kernel<64>(mode, two_y, grid, smem, ctx->stream, tm_xi, tm_xj, tm_om, a); break;
+    case 96: err = launch_tile_kernel<96>(mode, two_y, grid, smem, ctx->stream, tm_xi, tm_xj, tm_om, a); break;
+    case 128: err = launch_tile_kernel<128>(mode, two_y, grid, smem, ctx->stream, tm_xi, tm_xj, tm_om, a); break;
+    default: return fail(ctx, DB200_ERR_UNSUPPORTED, "rbf tiles: padded feature count not in {32, 64, 96, 128}");
   }
+  DB200_CUDA(ctx, err);
   DB200_CUDA(ctx, cudaGetLastError());
   prof_end(ctx, e0);
   count_launch(ctx);
