@@ -213,7 +213,7 @@ static int check_points(db200_context* ctx, int m, int d, const float* X, int ld
 static int pack_pair(db200_context* ctx, int m, int n, int d, const float* Xi, int ldxi, const float* Xj, int ldxj,
                      int layout, size_t extra_bytes, PackedPoints& pi, PackedPoints& pj, Carve& carve) {
   const int dp = feature_pad(d);
-  const int mpad = round_up(m, 128), npad = round_up(n, 128);
+  const int mpad = point_pad(m), npad = point_pad(n);
   const bool same = (Xi == Xj && ldxi == ldxj && m == n);
   size_t bytes = 4096 + (size_t)mpad * (2 * dp * 2 + 4) + extra_bytes + 4 * 256;
   if (!same) bytes += (size_t)npad * (2 * dp * 2 + 4);
@@ -262,7 +262,7 @@ int db200_rbf_sketch(db200_context* ctx, int m, int n, int d, int l, const float
   if (!st) st = check_points(ctx, n, d, Xj, ldxj, x_layout);
   if (st) return st;
   const SketchPlan plan = plan_sketch(l);
-  const int npad = round_up(n, 128);
+  const int npad = point_pad(n);
   PackedPoints pi, pj;
   Carve carve{nullptr};
   st = pack_pair(ctx, m, n, d, Xi, ldxi, Xj, ldxj, x_layout, (size_t)plan.lrows * npad * 2 + 256, pi, pj, carve);

@@ -93,6 +93,9 @@ struct SketchPlan {
 };
 SketchPlan plan_sketch(int l);
 int feature_pad(int d);  // dp: padded feature count of the split operand
+// Packed point counts are padded to whole 256-row tiles (one CTA pair of the tile kernel), on both sides, so that
+// a set used as rows and as columns packs once.
+inline int point_pad(int n) { return round_up(n < 1 ? 1 : n, 256); }
 
 // Launch the fused tile kernel.  For RBF_MODE_SKETCH, `op` is the packed Omega^T and `out` is Y (m x l, column
 // major, leading dimension ldo); for RBF_MODE_KBLOCK, `out` is the kernel block K (m x n, column major).

@@ -63,7 +63,7 @@ extern "C" int db200_rbf_sketch_noalloc(void* stream, int m, int n, int d, int l
 
   // Scratch layout: [status | Xi packed | Xi norms | Xj packed | Xj norms | Omega^T packed], 256-byte aligned.
   const int dp = feature_pad(d);
-  const int mpad = round_up(m, 128), npad = round_up(n, 128);
+  const int mpad = point_pad(m), npad = point_pad(n);
   const bool same = (Xi == Xj && ldxi == ldxj && m == n);
   const SketchPlan plan = plan_sketch(l);
   size_t need = 256;

@@ -13,9 +13,12 @@
 // so the kernel matrix is never written to HBM in SKETCH mode.  Algorithm restated from
 // include/dkernel.cu:102-129 (vecnorm, rbf) and :151-178 / :194-231 (distance GEMM, rbf, sketch GEMM).
 //
-// Warp roles (352 threads): warp 0 = TMA producer of the point tiles, warp 10 = TMA producer of the sketch
-// operand, warp 1 = TMEM allocator + MMA issuer, warps 2..9 = epilogue (two warps per TMEM lane quadrant, each
-// owning 64 of the 128 tile columns).  Two producers keep the Xj stream running while the Omega ring is full.
+// Warp roles (608 threads): warp 0 = TMA producer of the point tiles, warp 18 = TMA producer of the sketch
+// operand, warp 1 = TMEM allocator + MMA issuer, warps 2..17 = epilogue (four warps per TMEM lane quadrant, each
+// owning 32 of the 128 tile columns).  Two producers keep the Xj stream running while the Omega ring is full;
+// sixteen epilogue warps keep the exp/pack of one tile shorter than the distance MMA of the next, so the P tile
+// is ready when the tensor pipe reaches it.  P is handed over in two halves (j 0..63, 64..127), one per K chunk
+// of the sketch MMA.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cstdio>
@@ -28,26 +31,32 @@ namespace db200 {
 
 namespace {
 
-constexpr int BM = 128;          // rows of i per CTA (UMMA M)
-constexpr int BN = 128;          // columns of j per tile
-constexpr int KC = 64;           // bf16 elements per 128-byte swizzled row chunk
-constexpr int CHUNK_BYTES = BM * KC * 2;  // one 128 x 64 bf16 chunk = 16 KB
-constexpr int NUM_THREADS = 352;  // warp 0 Xi/Xj TMA, warp 1 MMA, warps 2..9 epilogue, warp 10 Omega TMA
-constexpr int NUM_EPI_WARPS = 8;
+constexpr int BM = 128;                    // rows of i per CTA (TMEM lanes)
+constexpr int PAIR_M = 256;                // rows of i per CTA pair (UMMA M of the 2-SM instructions)
+constexpr int BN = 128;                    // columns of j per tile
+constexpr int BN_HALF = BN / 2;            // rows of Xj each CTA of the pair holds per tile
+constexpr int KC = 64;                     // bf16 elements per 128-byte swizzled row chunk
+constexpr int XI_CHUNK = BM * KC * 2;      // 128 x 64 bf16 = 16 KB
+constexpr int XJ_CHUNK = BN_HALF * KC * 2; // 64 x 64 bf16 = 8 KB
+constexpr int NUM_EPI_WARPS = 16;
+constexpr int EPI_COLS = BN / (NUM_EPI_WARPS / 4);  // tile columns per epilogue warp (32)
+constexpr int OM_WARP = 2 + NUM_EPI_WARPS;          // Omega producer warp (18)
+constexpr int NUM_THREADS = 32 * (OM_WARP + 1);     // 608
 constexpr int TMEM_COLS = 512;
 constexpr int SMEM_LIMIT = 232448;  // dynamic shared memory per block on sm_100
+constexpr int BAR_BYTES = 1024;     // barrier region: barriers, TMEM slot, abort flag
+constexpr int MAX_NSX = 16, MAX_NSO = 4;
 constexpr float LOG2E = 1.4426950408889634f;
 
 // Runtime plan of one launch: TMEM columns (G buffers, the bf16 P tile, the Y panel) and ring depths.
 struct TileArgs {
-  int m, n;            // valid rows / columns
-  int dp;              // padded feature count; packed row = [hi(dp) | lo(dp)]
-  int n_itiles, n_jtiles, n_panels, panel, l;
-  int g_bufs;          // 1 or 2 TMEM buffers of 128 columns for G
-  int tmem_p, tmem_y;  // first TMEM column of the P tile (64 columns) and of the Y panel
-  int nsx, nso;        // Xj and Omega ring stages
-  int om_box;          // rows per Omega TMA box (TMA boxes are at most 256 rows; wider panels take two)
-  float c_row, c_dot;  // -gamma*log2e, 2*gamma*log2e
+  int m, n;              // valid rows / columns
+  int n_itiles, n_jtiles, n_panels, panel, l;  // n_itiles counts 256-row pair tiles
+  int n1, n2;            // sketch MMA split of the panel: N = n1 (+ n2) columns, n2 = 0 for one instruction
+  int g_bufs;            // 1 or 2 TMEM buffers of 128 columns for G
+  int tmem_p, tmem_y;    // first TMEM column of the P tile (64 columns) and of the Y panel
+  int nsx, nso;          // Xj and Omega ring stages
+  float c_row, c_dot;    // -gamma*log2e, 2*gamma*log2e
   const float* si;
   const float* sj;
   const float* yi;
@@ -58,43 +67,56 @@ struct TileArgs {
 };
 
 struct SmemLayout {
-  int nkc;  // chunks per packed row
-  int om_stage;
-  size_t off_xi, off_xj, off_om, off_bar, total;
+  int om_stage;  // bytes of one Omega stage in one CTA: (panel / 2) rows x 128 B
+  size_t off_xi, off_xj, off_om, off_sj, off_bar, total;
 };
+constexpr int SJ_BYTES = NUM_EPI_WARPS * 2 * EPI_COLS * 4;  // per epilogue warp: two tiles' column norms
 
 __host__ __device__ inline SmemLayout make_layout(int dp, int panel, int nsx, int nso) {
   SmemLayout L;
-  L.nkc = (2 * dp) / KC;
-  L.om_stage = panel * 128;
+  const int nkc = (2 * dp) / KC;
+  L.om_stage = (panel / 2) * 128;
   L.off_xi = 0;
-  L.off_xj = L.off_xi + (size_t)L.nkc * CHUNK_BYTES;
-  L.off_om = L.off_xj + (size_t)nsx * CHUNK_BYTES;
-  L.off_bar = L.off_om + (size_t)nso * L.om_stage;
-  L.total = L.off_bar + 512;  // barriers, TMEM slot, abort flag
+  L.off_xj = L.off_xi + (size_t)nkc * XI_CHUNK;
+  L.off_om = L.off_xj + (size_t)nsx * XJ_CHUNK;
+  L.off_sj = L.off_om + (size_t)nso * L.om_stage;
+  L.off_bar = L.off_sj + SJ_BYTES;
+  L.total = L.off_bar + BAR_BYTES;
   return L;
 }
 
-// Barrier slots (8 bytes each) after off_bar.
+// Barrier slots (8 bytes each) after off_bar.  "leader" barriers are only used in CTA 0 of the pair (the MMA
+// issuer waits on them; CTA 1 arrives remotely or its TMA completes on them); "pair" barriers exist in both CTAs
+// and are signalled by the leader's multicast tcgen05.commit.
 enum {
-  B_XI_FULL = 0,
-  B_XI_EMPTY,
-  B_G_FULL0,
+  B_XI_FULL = 0,  // leader: both CTAs' Xi bytes
+  B_XI_EMPTY,     // pair
+  B_G_FULL0,      // pair
   B_G_FULL1,
-  B_G_EMPTY0,
+  B_G_EMPTY0,     // leader: 2 x NUM_EPI_WARPS arrivals
   B_G_EMPTY1,
-  B_P_FULL,
-  B_P_EMPTY,
-  B_Y_FULL,
-  B_Y_EMPTY,
-  B_DRAIN,
-  B_XJ_FULL0,  // nsx full, then nsx empty, then nso full, nso empty
+  B_P_FULL0,      // leader: P half h, 2 x NUM_EPI_WARPS / 2 arrivals
+  B_P_FULL1,
+  B_P_EMPTY0,     // pair
+  B_P_EMPTY1,
+  B_Y_FULL,       // pair
+  B_Y_EMPTY,      // leader: 2 x NUM_EPI_WARPS arrivals
+  B_DRAIN,        // pair
+  B_XJ_FULL0,     // nsx full (leader), nsx empty (pair), nso full (leader), nso empty (pair)
 };
+constexpr int TMEM_SLOT_OFF = 960, ABORT_OFF = 968;
+static_assert((B_XJ_FULL0 + 2 * MAX_NSX + 2 * MAX_NSO) * 8 <= TMEM_SLOT_OFF, "barrier region too small");
 
+// One CTA pair (cluster of 2) owns a 256-row block of points i (128 rows per CTA, rank r holds rows 128r..) and one
+// panel of sketch columns.  The leader (rank 0) issues every MMA as cta_group::2 with M = 256: A (Xi, P) is each
+// CTA's own 128 rows, B (Xj, Omega~) is split by rows between the two CTAs, the accumulators (G, Y) sit in each
+// CTA's tensor memory for its own rows.  Each CTA loads its own operand halves with TMA and the completion is
+// counted on the leader's barrier.
 template <int MODE, int DP, bool TWO_Y>
 __global__ void __launch_bounds__(NUM_THREADS, 1)
     rbf_tile_kernel(const __grid_constant__ CUtensorMap tm_xi, const __grid_constant__ CUtensorMap tm_xj,
-                    const __grid_constant__ CUtensorMap tm_om, TileArgs args) {
+                    const __grid_constant__ CUtensorMap tm_om1, const __grid_constant__ CUtensorMap tm_om2,
+                    TileArgs args) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   constexpr int NKC = (2 * DP) / KC;  // 64-element chunks per packed row [hi | lo]
@@ -106,12 +128,19 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
   const uint32_t s_bar = smem_u32(smem + L.off_bar);
   auto bar = [&](int idx) -> uint32_t { return s_bar + 8u * (uint32_t)idx; };
   const int XJ_FULL = B_XJ_FULL0, XJ_EMPTY = B_XJ_FULL0 + nsx, OM_FULL = XJ_EMPTY + nsx, OM_EMPTY = OM_FULL + nso;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + L.off_bar + 400);
-  volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + L.off_bar + 408);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + L.off_bar + TMEM_SLOT_OFF);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + L.off_bar + ABORT_OFF);
 
   const int warp = threadIdx.x / 32;
   const int lane = threadIdx.x % 32;
+  const uint32_t rank = cluster_ctarank();
+  const bool leader = (rank == 0);
+  const int cid = (int)cluster_id_x(), ncl = (int)cluster_count_x();
   const int n_items = args.n_itiles * args.n_panels;
+  // leader-side barrier addresses in the shared::cluster window
+  auto lbar = [&](int idx) -> uint32_t { return mapa_shared(bar(idx), 0); };
+  // a wait that gives up also stops the other CTA of the pair
+  auto give_up = [&]() { st_shared_remote_u32(mapa_shared(smem_u32((const void*)abort_flag), rank ^ 1u), 1u); };
 
   if (threadIdx.x == 0) {
     *abort_flag = 0;
@@ -119,12 +148,14 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
     mbar_init(bar(B_XI_EMPTY), 1);
     mbar_init(bar(B_G_FULL0), 1);
     mbar_init(bar(B_G_FULL1), 1);
-    mbar_init(bar(B_G_EMPTY0), NUM_EPI_WARPS);
-    mbar_init(bar(B_G_EMPTY1), NUM_EPI_WARPS);
-    mbar_init(bar(B_P_FULL), NUM_EPI_WARPS);
-    mbar_init(bar(B_P_EMPTY), 1);
+    mbar_init(bar(B_G_EMPTY0), 2 * NUM_EPI_WARPS);
+    mbar_init(bar(B_G_EMPTY1), 2 * NUM_EPI_WARPS);
+    mbar_init(bar(B_P_FULL0), NUM_EPI_WARPS);
+    mbar_init(bar(B_P_FULL1), NUM_EPI_WARPS);
+    mbar_init(bar(B_P_EMPTY0), 1);
+    mbar_init(bar(B_P_EMPTY1), 1);
     mbar_init(bar(B_Y_FULL), 1);
-    mbar_init(bar(B_Y_EMPTY), NUM_EPI_WARPS);
+    mbar_init(bar(B_Y_EMPTY), 2 * NUM_EPI_WARPS);
     mbar_init(bar(B_DRAIN), 1);
     for (int s = 0; s < nsx; ++s) {
       mbar_init(bar(XJ_FULL + s), 1);
@@ -139,225 +170,249 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
   if (warp == 0 && lane == 0) {
     prefetch_tmap(&tm_xi);
     prefetch_tmap(&tm_xj);
-    if (MODE == RBF_MODE_SKETCH) prefetch_tmap(&tm_om);
+  }
+  if (warp == OM_WARP && lane == 0 && MODE == RBF_MODE_SKETCH) {
+    prefetch_tmap(&tm_om1);
+    if (TWO_Y) prefetch_tmap(&tm_om2);
   }
   if (warp == 1) {
-    tmem_alloc(smem_u32(tmem_slot), TMEM_COLS);
-    tmem_relinquish();
+    tmem_alloc_pair(smem_u32(tmem_slot), TMEM_COLS);
+    tmem_relinquish_pair();
   }
   tc_fence_before();
-  __syncthreads();
+  cluster_sync_all();  // barriers initialised and TMEM allocated in both CTAs before any cross-CTA traffic
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
 
-  if (warp == 0 || warp == 10) {
-    // ------------------------------------------------------------ TMA producers
+  if (warp == 0 || warp == OM_WARP) {
+    // ------------------------------------------------------------ TMA producers (both CTAs)
     if (lane == 0) {
       const bool points = (warp == 0);
-      uint32_t kx = 0, ko = 0, items_done = 0, xi_loads = 0;
+      uint32_t xs = 0, xph = 0, os = 0, oph = 0, items_done = 0;
       bool ok = true;
-      for (int item = blockIdx.x; item < n_items && ok; item += gridDim.x, ++items_done) {
+      for (int item = cid; item < n_items && ok; item += ncl, ++items_done) {
         const int it = item % args.n_itiles, pn = item / args.n_itiles;
         if (points) {
           if (!mbar_wait(bar(B_XI_EMPTY), (items_done & 1) ^ 1, abort_flag)) { ok = false; break; }
-          mbar_arrive_expect_tx(bar(B_XI_FULL), L.nkc * CHUNK_BYTES);
-          ++xi_loads;
-          for (int c = 0; c < L.nkc; ++c)
-            tma_load_2d(s_xi + c * CHUNK_BYTES, &tm_xi, bar(B_XI_FULL), c * KC, it * BM);
+          if (leader) mbar_arrive_expect_tx(bar(B_XI_FULL), 2 * NKC * XI_CHUNK);
+          for (int c = 0; c < NKC; ++c)
+            tma_load_2d_pair(s_xi + c * XI_CHUNK, &tm_xi, lbar(B_XI_FULL), c * KC, it * PAIR_M + (int)rank * BM);
         }
         for (int jt = 0; jt < args.n_jtiles && ok; ++jt) {
           if (points) {
-            for (int c = 0; c < L.nkc; ++c, ++kx) {
-              const uint32_t s = kx % nsx, ph = (kx / nsx) & 1;
-              if (!mbar_wait(bar(XJ_EMPTY + s), ph ^ 1, abort_flag)) { ok = false; break; }
-              mbar_arrive_expect_tx(bar(XJ_FULL + s), CHUNK_BYTES);
-              tma_load_2d(s_xj + s * CHUNK_BYTES, &tm_xj, bar(XJ_FULL + s), c * KC, jt * BN);
+            for (int c = 0; c < NKC; ++c) {
+              if (!mbar_wait(bar(XJ_EMPTY + xs), xph ^ 1, abort_flag)) { ok = false; break; }
+              if (leader) mbar_arrive_expect_tx(bar(XJ_FULL + xs), 2 * XJ_CHUNK);
+              tma_load_2d_pair(s_xj + xs * XJ_CHUNK, &tm_xj, lbar(XJ_FULL + xs), c * KC,
+                               jt * BN + (int)rank * BN_HALF);
+              if (++xs == (uint32_t)nsx) { xs = 0; xph ^= 1; }
             }
           } else if (MODE == RBF_MODE_SKETCH) {
-            for (int c = 0; c < 2 && ok; ++c, ++ko) {
-              const uint32_t s = ko % nso, ph = (ko / nso) & 1;
-              if (!mbar_wait(bar(OM_EMPTY + s), ph ^ 1, abort_flag)) { ok = false; break; }
-              mbar_arrive_expect_tx(bar(OM_FULL + s), L.om_stage);
-              for (int r0 = 0; r0 < args.panel; r0 += args.om_box)
-                tma_load_2d(s_om + s * L.om_stage + r0 * 128, &tm_om, bar(OM_FULL + s), jt * BN + c * KC,
-                            pn * args.panel + r0);
+            for (int c = 0; c < 2; ++c) {
+              if (!mbar_wait(bar(OM_EMPTY + os), oph ^ 1, abort_flag)) { ok = false; break; }
+              if (leader) mbar_arrive_expect_tx(bar(OM_FULL + os), 2 * L.om_stage);
+              // rows of this CTA: [r*n1/2, (r+1)*n1/2) of the first instruction's n1 columns, then the same
+              // half of the second instruction's n2 columns
+              const uint32_t dst = s_om + os * L.om_stage;
+              const int x = jt * BN + c * KC, y0 = pn * args.panel;
+              tma_load_2d_pair(dst, &tm_om1, lbar(OM_FULL + os), x, y0 + (int)rank * (args.n1 / 2));
+              if (TWO_Y)
+                tma_load_2d_pair(dst + (args.n1 / 2) * 128, &tm_om2, lbar(OM_FULL + os), x,
+                                 y0 + args.n1 + (int)rank * (args.n2 / 2));
+              if (++os == (uint32_t)nso) { os = 0; oph ^= 1; }
             }
           }
         }
       }
       if (!ok) {
-        // Drain: wait (time-bounded, ignoring the abort flag) for the loads this thread issued.
-        volatile int never = 0;
-        for (uint32_t k = (kx > (uint32_t)nsx ? kx - nsx : 0); k < kx; ++k)
-          mbar_wait(bar(XJ_FULL + k % nsx), (k / nsx) & 1, &never);
-        for (uint32_t k = (ko > (uint32_t)nso ? ko - nso : 0); k < ko; ++k)
-          mbar_wait(bar(OM_FULL + k % nso), (k / nso) & 1, &never);
-        if (xi_loads > 0) mbar_wait(bar(B_XI_FULL), (xi_loads - 1) & 1, &never);
+        give_up();
+        // Loads this lane issued complete on the leader's barriers, which this CTA cannot observe: give them
+        // time to land in shared memory before the pair tears down (bulk copies take microseconds).
+        const uint64_t t0 = global_timer_ns();
+        while (global_timer_ns() - t0 < 200000ull) {
+        }
       }
     }
     __syncwarp();
   } else if (warp == 1) {
-    // ------------------------------------------------------------ MMA issuer
+    // ------------------------------------------------------------ MMA issuer (leader CTA only)
     // The whole warp runs the schedule converged and waits together; one elected lane issues each block of
     // MMAs.  Every branch between MMAs is resolved at compile time (DP, TWO_Y): a lone issuing lane that waits
     // on mbarriers or branches between MMAs cannot keep the tensor pipe fed.
-    constexpr uint32_t idesc_g = idesc_f16(BM, BN, true);
-    const int n1 = TWO_Y ? (args.panel / 32) * 16 : args.panel, n2 = args.panel - n1;
-    const uint32_t idesc_y1 = idesc_f16(BM, n1, true);
-    const uint32_t idesc_y2 = idesc_f16(BM, TWO_Y ? n2 : 16, true);
-    const uint32_t y2_boff = (uint32_t)(n1 * 128) >> 4;
-    const uint32_t om_stage16 = (uint32_t)L.om_stage >> 4;
-    uint32_t xs = 0, xph = 0, os = 0, oph = 0, gbi = 0, gph = 0, pph = 0, items_done = 0;
-    bool ok = true;
-    // Descriptors are affine in the shared address (start address in the low 14 bits, in 16-byte units):
-    // build the base descriptors once and add offsets.
-    const uint64_t dxi = sdesc_k_sw128(s_xi), dxj = sdesc_k_sw128(s_xj), dom = sdesc_k_sw128(s_om);
-    auto wait_all = [&](uint32_t b, uint32_t parity) -> bool {
-      return __all_sync(0xffffffffu, mbar_wait(b, parity, abort_flag));
-    };
+    if (leader) {
+      constexpr uint32_t idesc_g = idesc_f16(PAIR_M, BN, true);
+      const uint32_t idesc_y1 = idesc_f16(PAIR_M, args.n1, true);
+      const uint32_t idesc_y2 = idesc_f16(PAIR_M, TWO_Y ? args.n2 : 16, true);
+      const uint32_t y2_boff = (uint32_t)((args.n1 / 2) * 128) >> 4;
+      const uint32_t om_stage16 = (uint32_t)L.om_stage >> 4;
+      uint32_t xs = 0, xph = 0, os = 0, oph = 0, gbi = 0, gph = 0, pph = 0, items_done = 0;
+      bool ok = true;
+      // Descriptors are affine in the shared address (start address in the low 14 bits, in 16-byte units):
+      // build the base descriptors once and add offsets.
+      const uint64_t dxi = sdesc_k_sw128(s_xi), dxj = sdesc_k_sw128(s_xj), dom = sdesc_k_sw128(s_om);
+      auto wait_all = [&](uint32_t b, uint32_t parity) -> bool {
+        return __all_sync(0xffffffffu, mbar_wait(b, parity, abort_flag));
+      };
 
-    auto issue_mma1 = [&]() -> bool {
-      if (!wait_all(bar(B_G_EMPTY0 + gbi), gph ^ 1)) return false;
-      tc_fence_after();
-      const uint32_t d_tmem = tmem_base + gbi * BN;
-#pragma unroll
-      for (int c = 0; c < NKC; ++c) {
-        if (!wait_all(bar(XJ_FULL + xs), xph)) return false;
+      auto issue_mma1 = [&]() -> bool {
+        if (!wait_all(bar(B_G_EMPTY0 + gbi), gph ^ 1)) return false;
         tc_fence_after();
-        if (elect_one()) {
-          const uint64_t bbase = dxj + ((xs * CHUNK_BYTES) >> 4);
+        const uint32_t d_tmem = tmem_base + gbi * BN;
 #pragma unroll
-          for (int ks = 0; ks < KC / 16; ++ks) {
-            const int o = c * KC + ks * 16;  // K offset of this slice inside the packed row [hi | lo]
-            const uint64_t bdesc = bbase + ((ks * 32) >> 4);
-            if (o < DP) {  // B slice is hi_j: pair with hi_i and lo_i
-              const int oh = o, ol = DP + o;
-              umma_f16(d_tmem, dxi + (((oh / KC) * CHUNK_BYTES + (oh % KC) * 2) >> 4), bdesc, idesc_g,
-                       o == 0 ? 0u : 1u);
-              umma_f16(d_tmem, dxi + (((ol / KC) * CHUNK_BYTES + (ol % KC) * 2) >> 4), bdesc, idesc_g, 1u);
-            } else {  // B slice is lo_j: pair with hi_i
-              const int oh = o - DP;
-              umma_f16(d_tmem, dxi + (((oh / KC) * CHUNK_BYTES + (oh % KC) * 2) >> 4), bdesc, idesc_g, 1u);
+        for (int c = 0; c < NKC; ++c) {
+          if (!wait_all(bar(XJ_FULL + xs), xph)) return false;
+          tc_fence_after();
+          if (elect_one()) {
+            const uint64_t bbase = dxj + ((xs * XJ_CHUNK) >> 4);
+#pragma unroll
+            for (int ks = 0; ks < KC / 16; ++ks) {
+              const int o = c * KC + ks * 16;  // K offset of this slice inside the packed row [hi | lo]
+              const uint64_t bdesc = bbase + ((ks * 32) >> 4);
+              if (o < DP) {  // B slice is hi_j: pair with hi_i and lo_i
+                const int oh = o, ol = DP + o;
+                umma_f16_pair(d_tmem, dxi + (((oh / KC) * XI_CHUNK + (oh % KC) * 2) >> 4), bdesc, idesc_g,
+                              o == 0 ? 0u : 1u);
+                umma_f16_pair(d_tmem, dxi + (((ol / KC) * XI_CHUNK + (ol % KC) * 2) >> 4), bdesc, idesc_g, 1u);
+              } else {  // B slice is lo_j: pair with hi_i
+                const int oh = o - DP;
+                umma_f16_pair(d_tmem, dxi + (((oh / KC) * XI_CHUNK + (oh % KC) * 2) >> 4), bdesc, idesc_g, 1u);
+              }
             }
+            umma_commit_pair(bar(XJ_EMPTY + xs));
+            if (c == NKC - 1) umma_commit_pair(bar(B_G_FULL0 + gbi));
           }
-          umma_commit(bar(XJ_EMPTY + xs));
-          if (c == NKC - 1) umma_commit(bar(B_G_FULL0 + gbi));
+          __syncwarp();
+          if (++xs == (uint32_t)nsx) { xs = 0; xph ^= 1; }
+        }
+        if (++gbi == (uint32_t)gb) { gbi = 0; gph ^= 1; }
+        return true;
+      };
+
+      for (int item = cid; item < n_items && ok; item += ncl, ++items_done) {
+        if (!wait_all(bar(B_XI_FULL), items_done & 1)) { ok = false; break; }
+        tc_fence_after();
+        if (MODE == RBF_MODE_SKETCH && items_done > 0) {
+          if (!wait_all(bar(B_Y_EMPTY), (items_done - 1) & 1)) { ok = false; break; }
+          tc_fence_after();
+        }
+        if (!issue_mma1()) { ok = false; break; }
+        for (int jt = 0; jt < args.n_jtiles; ++jt) {
+          if (jt + 1 < args.n_jtiles && !issue_mma1()) { ok = false; break; }
+          if (MODE == RBF_MODE_SKETCH) {
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+              // K chunk c of the sketch MMA reads P half c (j in [64c, 64c + 64))
+              if (!wait_all(bar(B_P_FULL0 + c), pph)) { ok = false; break; }
+              if (!wait_all(bar(OM_FULL + os), oph)) { ok = false; break; }
+              tc_fence_after();
+              if (elect_one()) {
+                const uint64_t bbase = dom + os * om_stage16;
+#pragma unroll
+                for (int ks = 0; ks < KC / 16; ++ks) {
+                  // A = P (bf16 in TMEM, 8 columns per 16-wide K step), B = Omega~ rows of this panel
+                  const uint32_t a_tmem = tmem_base + args.tmem_p + c * 32 + ks * 8;
+                  const uint64_t bdesc = bbase + ((ks * 32) >> 4);
+                  const uint32_t acc = (jt > 0 || c > 0 || ks > 0) ? 1u : 0u;
+                  umma_f16_ts_pair(tmem_base + args.tmem_y, a_tmem, bdesc, idesc_y1, acc);
+                  if (TWO_Y)
+                    umma_f16_ts_pair(tmem_base + args.tmem_y + args.n1, a_tmem, bdesc + y2_boff, idesc_y2, acc);
+                }
+                umma_commit_pair(bar(OM_EMPTY + os));
+                umma_commit_pair(bar(B_P_EMPTY0 + c));
+              }
+              __syncwarp();
+              if (++os == (uint32_t)nso) { os = 0; oph ^= 1; }
+            }
+            if (!ok) break;
+            pph ^= 1;
+          }
+        }
+        if (!ok) break;
+        if (elect_one()) {
+          umma_commit_pair(bar(B_XI_EMPTY));
+          if (MODE == RBF_MODE_SKETCH) umma_commit_pair(bar(B_Y_FULL));
         }
         __syncwarp();
-        if (++xs == (uint32_t)nsx) { xs = 0; xph ^= 1; }
       }
-      if (++gbi == (uint32_t)gb) { gbi = 0; gph ^= 1; }
-      return true;
-    };
-
-    for (int item = blockIdx.x; item < n_items && ok; item += gridDim.x, ++items_done) {
-      if (!wait_all(bar(B_XI_FULL), items_done & 1)) { ok = false; break; }
-      tc_fence_after();
-      if (MODE == RBF_MODE_SKETCH && items_done > 0) {
-        if (!wait_all(bar(B_Y_EMPTY), (items_done - 1) & 1)) { ok = false; break; }
-        tc_fence_after();
-      }
-      if (!issue_mma1()) { ok = false; break; }
-      for (int jt = 0; jt < args.n_jtiles; ++jt) {
-        if (jt + 1 < args.n_jtiles && !issue_mma1()) { ok = false; break; }
-        if (MODE == RBF_MODE_SKETCH) {
-          if (!wait_all(bar(B_P_FULL), pph)) { ok = false; break; }
-          tc_fence_after();
-          pph ^= 1;
-#pragma unroll
-          for (int c = 0; c < 2; ++c) {
-            if (!wait_all(bar(OM_FULL + os), oph)) { ok = false; break; }
-            tc_fence_after();
-            if (elect_one()) {
-              const uint64_t bbase = dom + os * om_stage16;
-#pragma unroll
-              for (int ks = 0; ks < KC / 16; ++ks) {
-                // A = P (bf16 in TMEM, 8 columns per 16-wide K step), B = Omega~ rows of this panel
-                const uint32_t a_tmem = tmem_base + args.tmem_p + c * 32 + ks * 8;
-                const uint64_t bdesc = bbase + ((ks * 32) >> 4);
-                const uint32_t acc = (jt > 0 || c > 0 || ks > 0) ? 1u : 0u;
-                umma_f16_ts(tmem_base + args.tmem_y, a_tmem, bdesc, idesc_y1, acc);
-                if (TWO_Y) umma_f16_ts(tmem_base + args.tmem_y + n1, a_tmem, bdesc + y2_boff, idesc_y2, acc);
-              }
-              umma_commit(bar(OM_EMPTY + os));
-              if (c == 1) umma_commit(bar(B_P_EMPTY));
-            }
-            __syncwarp();
-            if (++os == (uint32_t)nso) { os = 0; oph ^= 1; }
-          }
-          if (!ok) break;
-        }
-      }
-      if (!ok) break;
-      if (elect_one()) {
-        umma_commit(bar(B_XI_EMPTY));
-        if (MODE == RBF_MODE_SKETCH) umma_commit(bar(B_Y_FULL));
-      }
+      if (!ok && lane == 0) give_up();
+      // All MMAs issued by this warp must be complete before TMEM is released (in both CTAs).
+      if (elect_one()) umma_commit_pair(bar(B_DRAIN));
       __syncwarp();
     }
-    // All MMAs issued by this warp must be complete before TMEM is released.
-    if (elect_one()) umma_commit(bar(B_DRAIN));
-    __syncwarp();
     volatile int never = 0;
     mbar_wait(bar(B_DRAIN), 0, &never);
     __syncwarp();
-  } else if (warp >= 2 && warp <= 9) {
-    // ------------------------------------------------------------ epilogue
-    const int ew = warp - 2;              // 0..7
+  } else if (warp >= 2 && warp < 2 + NUM_EPI_WARPS) {
+    // ------------------------------------------------------------ epilogue (both CTAs, own rows)
+    const int ew = warp - 2;              // 0..15
     const int q = warp & 3;               // TMEM lane quadrant this warp may access
-    const int h = ew >> 2;                // column half of the tile
-    const int row = 32 * q + lane;        // row inside the 128-row block
+    const int qc = ew >> 2;               // column quarter of the tile (32 columns)
+    const int h = qc >> 1;                // P half (K chunk of the sketch MMA) these columns belong to
+    const int row = 32 * q + lane;        // row inside this CTA's 128 rows
     const uint32_t t_lane = (uint32_t)(32 * q) << 16;
+    // Column norms of this warp's 32 columns, double-buffered per warp in shared memory: lane l fetches the value
+    // for the next tile from global memory before the current tile's exp, and parks it here afterwards, so the
+    // global latency never sits between a G tile and its P tile.
+    float* sjbuf = reinterpret_cast<float*>(smem + L.off_sj) + ew * 2 * EPI_COLS;
     uint32_t kg = 0, kp = 0, items_done = 0;
     bool ok = true;
-    for (int item = blockIdx.x; item < n_items && ok; item += gridDim.x, ++items_done) {
+    for (int item = cid; item < n_items && ok; item += ncl, ++items_done) {
       const int it = item % args.n_itiles, pn = item / args.n_itiles;
-      const int i = it * BM + row;
-      const float a_i = args.c_row * args.si[i];  // si is padded to n_itiles*BM
+      const int i = it * PAIR_M + (int)rank * BM + row;
+      const float a_i = args.c_row * args.si[i];  // si is padded to n_itiles * PAIR_M
       const float y_i = (i < args.m && args.yi) ? args.yi[i] : 1.0f;
+      sjbuf[lane] = args.sj[qc * EPI_COLS + lane];  // tile 0 of this item
+      __syncwarp();
       for (int jt = 0; jt < args.n_jtiles; ++jt) {
+        // sj is padded to n_jtiles * BN
+        const float sj_next = (jt + 1 < args.n_jtiles) ? args.sj[(jt + 1) * BN + qc * EPI_COLS + lane] : 0.0f;
         const uint32_t b = kg % gb, ph = (kg / gb) & 1;
         if (!__all_sync(0xffffffffu, mbar_wait(bar(B_G_FULL0 + b), ph, abort_flag))) { ok = false; break; }
         tc_fence_after();
-        float v[64];
-        const uint32_t tcol = tmem_base + t_lane + b * BN + h * 64;
-#pragma unroll
-        for (int c = 0; c < 4; ++c) tmem_ld16(tcol + c * 16, v + c * 16);
+        float v[EPI_COLS];
+        const uint32_t tcol = tmem_base + t_lane + b * BN + qc * EPI_COLS;
+        tmem_ld16(tcol, v);
+        tmem_ld16(tcol + 16, v + 16);
         tmem_wait_ld();
         tc_fence_before();
         __syncwarp();
-        if (lane == 0) mbar_arrive(bar(B_G_EMPTY0 + b));
+        if (lane == 0) mbar_arrive_remote(lbar(B_G_EMPTY0 + b));
         ++kg;
 
-        const int j0 = jt * BN + h * 64;
-        const float4* sj4 = reinterpret_cast<const float4*>(args.sj + j0);
+        const int j0 = jt * BN + qc * EPI_COLS;
+        const float4* sj4 = reinterpret_cast<const float4*>(sjbuf + (jt & 1) * EPI_COLS);
 #pragma unroll
-        for (int c = 0; c < 16; ++c) {
-          const float4 s4 = __ldg(sj4 + c);
+        for (int c = 0; c < EPI_COLS / 4; ++c) {
+          const float4 s4 = sj4[c];
           v[4 * c + 0] = fast_exp2(fminf(fmaf(args.c_dot, v[4 * c + 0], fmaf(args.c_row, s4.x, a_i)), 0.0f));
           v[4 * c + 1] = fast_exp2(fminf(fmaf(args.c_dot, v[4 * c + 1], fmaf(args.c_row, s4.y, a_i)), 0.0f));
           v[4 * c + 2] = fast_exp2(fminf(fmaf(args.c_dot, v[4 * c + 2], fmaf(args.c_row, s4.z, a_i)), 0.0f));
           v[4 * c + 3] = fast_exp2(fminf(fmaf(args.c_dot, v[4 * c + 3], fmaf(args.c_row, s4.w, a_i)), 0.0f));
         }
 
+        sjbuf[((jt + 1) & 1) * EPI_COLS + lane] = sj_next;
+        __syncwarp();
         if (MODE == RBF_MODE_SKETCH) {
-          uint32_t pk[32];
+          uint32_t pk[EPI_COLS / 2];
 #pragma unroll
-          for (int c = 0; c < 32; ++c) pk[c] = pack_bf16x2(v[2 * c], v[2 * c + 1]);
-          if (!__all_sync(0xffffffffu, mbar_wait(bar(B_P_EMPTY), (kp & 1) ^ 1, abort_flag))) { ok = false; break; }
+          for (int c = 0; c < EPI_COLS / 2; ++c) pk[c] = pack_bf16x2(v[2 * c], v[2 * c + 1]);
+          if (!__all_sync(0xffffffffu, mbar_wait(bar(B_P_EMPTY0 + h), (kp & 1) ^ 1, abort_flag))) {
+            ok = false;
+            break;
+          }
           tc_fence_after();
-          // P row = this thread's row; j in [64h, 64h + 64) -> TMEM columns tmem_p + 32h .. + 31
-          tmem_st32(tmem_base + t_lane + args.tmem_p + h * 32, pk);
+          // P row = this thread's row; j in [32qc, 32qc + 32) -> TMEM columns tmem_p + 16qc .. + 15
+          tmem_st16(tmem_base + t_lane + args.tmem_p + qc * (EPI_COLS / 2), pk);
           tmem_wait_st();
           tc_fence_before();
           __syncwarp();
-          if (lane == 0) mbar_arrive(bar(B_P_FULL));
+          if (lane == 0) mbar_arrive_remote(lbar(B_P_FULL0 + h));
           ++kp;
         } else {
           if (i < args.m) {
             float* out = args.out + i;
 #pragma unroll
-            for (int c = 0; c < 64; ++c) {
+            for (int c = 0; c < EPI_COLS; ++c) {
               const int j = j0 + c;
               if (j < args.n) {
                 const float yj = args.yj ? __ldg(args.yj + j) : 1.0f;
@@ -371,33 +426,35 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
       if (MODE == RBF_MODE_SKETCH) {
         if (!__all_sync(0xffffffffu, mbar_wait(bar(B_Y_FULL), items_done & 1, abort_flag))) { ok = false; break; }
         tc_fence_after();
-        const int half = args.panel / 2;
-        for (int cc = 0; cc < half; cc += 8) {
-          float yv[8];
-          tmem_ld8(tmem_base + t_lane + args.tmem_y + h * half + cc, yv);
+        const int quarter = args.panel / 4;  // panel is a multiple of 16
+        for (int cc = 0; cc < quarter; cc += 4) {
+          float yv[4];
+          tmem_ld4(tmem_base + t_lane + args.tmem_y + qc * quarter + cc, yv);
           tmem_wait_ld();
           if (i < args.m) {
 #pragma unroll
-            for (int e = 0; e < 8; ++e) {
-              const int col = pn * args.panel + h * half + cc + e;
+            for (int e = 0; e < 4; ++e) {
+              const int col = pn * args.panel + qc * quarter + cc + e;
               if (col < args.l) args.out[i + (size_t)col * args.ldo] = y_i * yv[e];
             }
           }
         }
         tc_fence_before();
         __syncwarp();
-        if (lane == 0) mbar_arrive(bar(B_Y_EMPTY));
+        if (lane == 0) mbar_arrive_remote(lbar(B_Y_EMPTY));
       }
     }
+    if (!ok && lane == 0) give_up();
     __syncwarp();
   }
 
-  __syncthreads();
+  // Neither CTA may leave (or free TMEM) while the other can still touch its shared memory or tensor memory:
+  // every role above ends after a bounded wait, then the pair meets here.
+  tc_fence_before();
+  cluster_sync_all();
+  tc_fence_after();
   if (threadIdx.x == 0 && *abort_flag) atomicExch(args.status, DB200_ERR_TIMEOUT);
-  if (warp == 1) {
-    tc_fence_after();
-    tmem_dealloc(tmem_base, TMEM_COLS);
-  }
+  if (warp == 1) tmem_dealloc_pair(tmem_base, TMEM_COLS);
 }
 
 // ------------------------------------------------------------------ packing kernels
@@ -470,15 +527,35 @@ bool make_tmap(CUtensorMap* tm, const void* base, uint64_t inner, uint64_t outer
 }
 
 template <int DP>
-cudaError_t launch_tile_kernel(int mode, bool two_y, int grid, size_t smem, cudaStream_t st, const CUtensorMap& tm_xi,
-                               const CUtensorMap& tm_xj, const CUtensorMap& tm_om, const TileArgs& a) {
+cudaError_t launch_tile_kernel(int mode, bool two_y, int max_clusters, int n_items, size_t smem, cudaStream_t st,
+                               const CUtensorMap& tm_xi, const CUtensorMap& tm_xj, const CUtensorMap& tm_om1,
+                               const CUtensorMap& tm_om2, const TileArgs& a) {
   auto k = (mode == RBF_MODE_SKETCH) ? (two_y ? rbf_tile_kernel<RBF_MODE_SKETCH, DP, true>
                                               : rbf_tile_kernel<RBF_MODE_SKETCH, DP, false>)
                                      : rbf_tile_kernel<RBF_MODE_KBLOCK, DP, false>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  k<<<grid, NUM_THREADS, smem, st>>>(tm_xi, tm_xj, tm_om, a);
-  return cudaGetLastError();
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 2;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(2 * max_clusters));
+  cfg.blockDim = dim3(NUM_THREADS);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  // persistent: as many pairs as can be resident at once, no more than there are items
+  int resident = 0;
+  e = cudaOccupancyMaxActiveClusters(&resident, k, &cfg);
+  if (e != cudaSuccess) return e;
+  if (resident < 1) return cudaErrorInvalidConfiguration;
+  int clusters = resident < max_clusters ? resident : max_clusters;
+  if (clusters > n_items) clusters = n_items;
+  cfg.gridDim = dim3((unsigned)(2 * clusters));
+  return cudaLaunchKernelEx(&cfg, k, tm_xi, tm_xj, tm_om1, tm_om2, a);
 }
 
 }  // namespace
@@ -528,40 +605,44 @@ int launch_rbf_tiles(db200_context* ctx, int mode, const PackedPoints& pi, const
                      const float* yj, const void* op, const SketchPlan& plan, int l, float gamma, float* out,
                      int ldo) {
   if (pi.dp != pj.dp || pi.dp > 128) return fail(ctx, DB200_ERR_UNSUPPORTED, "rbf tiles: feature count > 128");
-  if (pi.npad % BM || pj.npad % BN) return fail(ctx, DB200_ERR_INVALID, "rbf tiles: unpadded operands");
+  if (pi.npad % PAIR_M || pj.npad % BN) return fail(ctx, DB200_ERR_INVALID, "rbf tiles: unpadded operands");
   if (mode == RBF_MODE_SKETCH && (plan.panel % 16 || plan.panel > 320 || plan.panel < 16 ||
                                   plan.panel + 64 + 128 * plan.g_bufs > TMEM_COLS))
     return fail(ctx, DB200_ERR_INVALID, "rbf tiles: bad sketch panel");
-  CUtensorMap tm_xi, tm_xj, tm_om;
+  CUtensorMap tm_xi, tm_xj, tm_om1, tm_om2;
   const int kp = 2 * pi.dp;
-  if (!make_tmap(&tm_xi, pi.xp, kp, pi.npad, kp, BM) || !make_tmap(&tm_xj, pj.xp, kp, pj.npad, kp, BN))
+  if (!make_tmap(&tm_xi, pi.xp, kp, pi.npad, kp, BM) || !make_tmap(&tm_xj, pj.xp, kp, pj.npad, kp, BN_HALF))
     return fail(ctx, DB200_ERR_CUDA, "cuTensorMapEncodeTiled failed for the point operands");
   TileArgs a;
   if (mode == RBF_MODE_SKETCH) {
-    // a TMA box has at most 256 rows: a wider panel is loaded as two boxes of panel/2 rows (a multiple of 8)
-    a.om_box = plan.panel > 256 ? plan.panel / 2 : plan.panel;
-    if (!make_tmap(&tm_om, op, pj.npad, plan.lrows, pj.npad, a.om_box))
-      return fail(ctx, DB200_ERR_CUDA, "cuTensorMapEncodeTiled failed for the sketch operand");
     a.n_panels = plan.n_panels;
     a.panel = plan.panel;
+    // one sketch MMA of N = panel columns, or two of about half each (multiples of 16, each <= 256); each CTA of
+    // the pair holds half of every instruction's B rows, loaded as one TMA box per instruction
+    a.n1 = plan.panel > 256 ? (plan.panel / 32) * 16 : plan.panel;
+    a.n2 = plan.panel - a.n1;
+    if (!make_tmap(&tm_om1, op, pj.npad, plan.lrows, pj.npad, a.n1 / 2) ||
+        (a.n2 > 0 && !make_tmap(&tm_om2, op, pj.npad, plan.lrows, pj.npad, a.n2 / 2)))
+      return fail(ctx, DB200_ERR_CUDA, "cuTensorMapEncodeTiled failed for the sketch operand");
+    if (a.n2 == 0) tm_om2 = tm_om1;  // unused
     a.g_bufs = plan.g_bufs;
     a.tmem_p = 128 * plan.g_bufs;
     a.tmem_y = a.tmem_p + 64;
-    a.nso = 2;
+    a.nso = MAX_NSO;
   } else {
-    tm_om = tm_xj;  // unused
+    tm_om1 = tm_om2 = tm_xj;  // unused
     a.n_panels = 1;
     a.panel = 16;
+    a.n1 = 16;
+    a.n2 = 0;
     a.g_bufs = 2;
     a.tmem_p = 256;
     a.tmem_y = 320;
     a.nso = 0;
-    a.om_box = 16;
   }
   a.m = pi.n;
   a.n = pj.n;
-  a.dp = pi.dp;
-  a.n_itiles = pi.npad / BM;
+  a.n_itiles = pi.npad / PAIR_M;
   a.n_jtiles = pj.npad / BN;
   a.l = l;
   a.c_row = -gamma * LOG2E;
@@ -573,32 +654,34 @@ int launch_rbf_tiles(db200_context* ctx, int mode, const PackedPoints& pi, const
   a.out = out;
   a.ldo = ldo;
   a.status = ctx->d_status;
-  // the Xj ring takes whatever shared memory is left (2..8 stages)
+  // the Xj ring takes whatever shared memory is left
   {
-    const SmemLayout L0 = make_layout(a.dp, a.panel, 0, a.nso);
+    const SmemLayout L0 = make_layout(pi.dp, a.panel, 0, a.nso);
     const long long left = (long long)SMEM_LIMIT - 1024 - (long long)L0.total;
-    int nsx = (int)(left / CHUNK_BYTES);
-    if (nsx > 8) nsx = 8;
+    int nsx = (int)(left / XJ_CHUNK);
+    if (nsx > MAX_NSX) nsx = MAX_NSX;
     if (nsx < 2) return fail(ctx, DB200_ERR_UNSUPPORTED, "rbf tiles: shared memory plan does not fit");
     a.nsx = nsx;
   }
-  const SmemLayout L = make_layout(a.dp, a.panel, a.nsx, a.nso);
+  const SmemLayout L = make_layout(pi.dp, a.panel, a.nsx, a.nso);
   const size_t smem = L.total + 1024;
   const int n_items = a.n_itiles * a.n_panels;
-  const int grid = n_items < ctx->num_sms ? n_items : ctx->num_sms;
+  const int max_clusters = ctx->num_sms / 2;
   cudaEvent_t e0 = nullptr;
   prof_begin(ctx, &e0);
-  const bool two_y = (mode == RBF_MODE_SKETCH) && a.panel > 256;
+  const bool two_y = (mode == RBF_MODE_SKETCH) && a.n2 > 0;
   cudaError_t err = cudaSuccess;
-  switch (a.dp) {
-    case 32: err = launch_tile_kernel<32>(mode, two_y, grid, smem, ctx->stream, tm_xi, tm_xj, tm_om, a); break;
-    case 64: err = launch_tile_kernel<64>(mode, two_y, grid, smem, ctx->stream, tm_xi, tm_xj, tm_om, a); break;
-    case 96: err = launch_tile_kernel<96>(mode, two_y, grid, smem, ctx->stream, tm_xi, tm_xj, tm_om, a); break;
-    case 128: err = launch_tile_kernel<128>(mode, two_y, grid, smem, ctx->stream, tm_xi, tm_xj, tm_om, a); break;
+#define DB200_TILE_LAUNCH(DPV)                                                                                    \
+  launch_tile_kernel<DPV>(mode, two_y, max_clusters, n_items, smem, ctx->stream, tm_xi, tm_xj, tm_om1, tm_om2, a)
+  switch (pi.dp) {
+    case 32: err = DB200_TILE_LAUNCH(32); break;
+    case 64: err = DB200_TILE_LAUNCH(64); break;
+    case 96: err = DB200_TILE_LAUNCH(96); break;
+    case 128: err = DB200_TILE_LAUNCH(128); break;
     default: return fail(ctx, DB200_ERR_UNSUPPORTED, "rbf tiles: padded feature count not in {32, 64, 96, 128}");
   }
+#undef DB200_TILE_LAUNCH
   DB200_CUDA(ctx, err);
-  DB200_CUDA(ctx, cudaGetLastError());
   prof_end(ctx, e0);
   count_launch(ctx);
   return DB200_OK;
