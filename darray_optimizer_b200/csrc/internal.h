@@ -84,7 +84,7 @@ struct PackedPoints {
 int pack_points(db200_context* ctx, const float* X, int ldx, int layout, int n, int d, int dp, int npad, void* xp,
                 float* norms);
 
-// Omega^T (bf16, [lrows][njpad]) with the column labels folded in: Op[c][j] = y_j * Omega[j + c*ldo].
+// Omega^T (fp16, [lrows][njpad]) with the column labels folded in: Op[c][j] = y_j * Omega[j + c*ldo].
 int pack_sketch(db200_context* ctx, const float* Omega, int ldo, const float* yj, int n, int l, int njpad, int lrows,
                 void* op);
 

@@ -92,11 +92,14 @@ def test_rbf_sketch_matches_oracle(gpu_ctx, m, n, d, l):
                        ldy, gamma)
     gpu_ctx.sync()
     Yg = colmajor_host(Y, m)
-    assert rel_fro(Yg, Yref) <= 1e-2
+    # fp16 P and Omega~ in the sketch product: ~3e-4 relative in Frobenius norm
+    err = rel_fro(Yg, Yref)
+    assert err <= 2e-3, err
     # every column against the RMS column norm, so a dropped panel cannot hide behind the global norm
     # (single columns can nearly cancel when K has a dominant constant mode, so not per-column relative)
     rms_col = np.linalg.norm(Yref) / np.sqrt(l)
-    assert (np.linalg.norm(Yg - Yref, axis=0) / rms_col).max() <= 3e-2
+    col = (np.linalg.norm(Yg - Yref, axis=0) / rms_col).max()
+    assert col <= 6e-3, col
 
 
 def test_rbf_sketch_two_calls_reuse_workspace(gpu_ctx):
@@ -150,4 +153,5 @@ def test_bounded_wait_expiry_reports_timeout_and_context_survives(gpu_ctx):
     Y = colmajor_empty(n, l)
     gpu_ctx.rbf_sketch(n, n, d, l, ptr(dX), d, ptr(dX), d, POINT_MAJOR, ptr(dy), ptr(dy), ptr(dO), n, ptr(Y), n, 0.1)
     gpu_ctx.sync()
-    assert rel_fro(colmajor_host(Y, n), O.sketch(X, X, y, y, Om, 0.1)) <= 1e-2
+    err = rel_fro(colmajor_host(Y, n), O.sketch(X, X, y, y, Om, 0.1))
+    assert err <= 2e-3, err

@@ -18,7 +18,7 @@ from util import colmajor_empty, colmajor_host, dev, ptr, rel_fro
 pytestmark = pytest.mark.gpu
 
 POINT_MAJOR = 0
-TOL = 1e-2
+TOL = 2e-3
 
 
 def _case(seed, n, d, l, m=None):
