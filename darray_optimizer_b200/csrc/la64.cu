@@ -21,58 +21,96 @@ __device__ __forceinline__ double ld64(const T* p) { return (double)__ldg(p); }
 
 // C[p x q] (+)= alpha * A^T diag(w) B over rows [r0, r1) of A (n x p) and B (n x q); FP64 accumulation.
 // grid.z splits the rows; partial tiles are added with FP64 atomics when grid.z > 1.
+//
+// 128 x 128 output tile per CTA, 256 threads, each thread an 8 x 8 register block: rows {4ty..4ty+3,
+// 64+4ty..64+4ty+3} x columns {4tx..4tx+3, 64+4tx..64+4tx+3}, read from shared memory as 128-bit pairs, so 8
+// shared loads feed 64 FMAs (the 4 x 4 blocking of a 64 x 64 tile needs one load per two FMAs and is
+// shared-memory bound at about half the FP64 rate).  Tiles of 16 rows of A and B are staged transposed
+// (k-major) in shared memory with coalesced column reads from global memory (16 consecutive rows = 128 bytes).
+constexpr int GT = 128;        // Gram output tile
+constexpr int GK = 8;          // rows per stage
+constexpr int GPAD = GT + 2;   // padded shared row (keeps 16-byte alignment of the pairs)
+
 template <typename TA, typename TBt>
-__global__ void __launch_bounds__(256) gram_kernel(int n, int p, int q, const TA* __restrict__ A, long long lda,
-                                                   const TBt* __restrict__ B, long long ldb,
-                                                   const double* __restrict__ w, double alpha, double* C, int ldc,
-                                                   int rows_per_split, int upper_only, int atomic) {
+__global__ void __launch_bounds__(256, 1) gram_kernel(int n, int p, int q, const TA* __restrict__ A, long long lda,
+                                                      const TBt* __restrict__ B, long long ldb,
+                                                      const double* __restrict__ w, double alpha, double* C, int ldc,
+                                                      int rows_per_split, int upper_only, int atomic) {
   const int bi = blockIdx.x, bj = blockIdx.y;
   if (upper_only && bi > bj) return;
-  const int i0 = bi * TB, j0 = bj * TB;
+  const int i0 = bi * GT, j0 = bj * GT;
   const int r0 = blockIdx.z * rows_per_split;
   const int r1 = min(n, r0 + rows_per_split);
-  __shared__ double sA[TK][TB + 1];
-  __shared__ double sB[TK][TB + 1];
+  __shared__ __align__(16) double sA[2][GK][GPAD];
+  __shared__ __align__(16) double sB[2][GK][GPAD];
   const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-  double acc[4][4];
+  double acc[8][8];
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
+  for (int a = 0; a < 8; ++a)
 #pragma unroll
-    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
-  for (int k0 = r0; k0 < r1; k0 += TK) {
-    // 256 threads load 16 x 64 of A and of B: thread -> (kk = t % 16, col = t / 16 + 16 * s)
-    const int kk = threadIdx.x % TK;
+    for (int b = 0; b < 8; ++b) acc[a][b] = 0.0;
+  const int kk = threadIdx.x % GK;   // row inside the stage this thread loads
+  const int c0 = threadIdx.x / GK;   // first column it loads (then +32, +64, +96)
+  double va[4], vb[4];
+  auto fetch = [&](int k0) {
     const int k = k0 + kk;
-    const double wk = (w && k < r1) ? w[k] : 1.0;
+    const bool kin = k < r1;
+    const double wk = (w && kin) ? w[k] : 1.0;
 #pragma unroll
     for (int s = 0; s < 4; ++s) {
-      const int c = threadIdx.x / TK + 16 * s;
+      const int c = c0 + 32 * s;
       const int ia = i0 + c, jb = j0 + c;
-      sA[kk][c] = (k < r1 && ia < p) ? wk * ld64(A + (long long)ia * lda + k) : 0.0;
-      sB[kk][c] = (k < r1 && jb < q) ? ld64(B + (long long)jb * ldb + k) : 0.0;
+      va[s] = (kin && ia < p) ? wk * ld64(A + (long long)ia * lda + k) : 0.0;
+      vb[s] = (kin && jb < q) ? ld64(B + (long long)jb * ldb + k) : 0.0;
     }
-    __syncthreads();
+  };
+  auto park = [&](int buf) {
 #pragma unroll
-    for (int t = 0; t < TK; ++t) {
-      double av[4], bv[4];
-#pragma unroll
-      for (int a = 0; a < 4; ++a) av[a] = sA[t][ty * 4 + a];
-#pragma unroll
-      for (int b = 0; b < 4; ++b) bv[b] = sB[t][tx * 4 + b];
-#pragma unroll
-      for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
+    for (int s = 0; s < 4; ++s) {
+      sA[buf][kk][c0 + 32 * s] = va[s];
+      sB[buf][kk][c0 + 32 * s] = vb[s];
     }
+  };
+  int buf = 0;
+  if (r0 < r1) {
+    fetch(r0);
+    park(0);
+  }
+  __syncthreads();
+  for (int k0 = r0; k0 < r1; k0 += GK) {
+    // the next stage's global loads are in flight while this stage is multiplied
+    const bool more = k0 + GK < r1;
+    if (more) fetch(k0 + GK);
+#pragma unroll
+    for (int t = 0; t < GK; ++t) {
+      double av[8], bv[8];
+      const double2* ra = reinterpret_cast<const double2*>(&sA[buf][t][0]);
+      const double2* rb = reinterpret_cast<const double2*>(&sB[buf][t][0]);
+      double2 x;
+      x = ra[2 * ty];      av[0] = x.x; av[1] = x.y;
+      x = ra[2 * ty + 1];  av[2] = x.x; av[3] = x.y;
+      x = ra[32 + 2 * ty]; av[4] = x.x; av[5] = x.y;
+      x = ra[33 + 2 * ty]; av[6] = x.x; av[7] = x.y;
+      x = rb[2 * tx];      bv[0] = x.x; bv[1] = x.y;
+      x = rb[2 * tx + 1];  bv[2] = x.x; bv[3] = x.y;
+      x = rb[32 + 2 * tx]; bv[4] = x.x; bv[5] = x.y;
+      x = rb[33 + 2 * tx]; bv[6] = x.x; bv[7] = x.y;
+#pragma unroll
+      for (int a = 0; a < 8; ++a)
+#pragma unroll
+        for (int b = 0; b < 8; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
+    }
+    if (more) park(buf ^ 1);  // the other buffer was last read one stage ago, before the barrier below
     __syncthreads();
+    buf ^= 1;
   }
 #pragma unroll
-  for (int a = 0; a < 4; ++a) {
-    const int i = i0 + ty * 4 + a;
+  for (int a = 0; a < 8; ++a) {
+    const int i = i0 + (a < 4 ? 4 * ty + a : 64 + 4 * ty + a - 4);
     if (i >= p) continue;
 #pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      const int j = j0 + tx * 4 + b;
+    for (int b = 0; b < 8; ++b) {
+      const int j = j0 + (b < 4 ? 4 * tx + b : 64 + 4 * tx + b - 4);
       if (j >= q) continue;
       if (upper_only && i > j) continue;
       double* dst = C + (long long)j * ldc + i;
@@ -523,11 +561,28 @@ int gram(db200_context* ctx, int n, int p, int q, const TA* A, long long lda, co
   scale_kernel<<<grid_for((long long)p * q, 256, 4096), 256, 0, ctx->stream>>>(C, ldc, p, q, beta, upper_only ? 1 : 0);
   count_launch(ctx);
   if (n <= 0) return DB200_OK;
-  const int tp = (p + TB - 1) / TB, tq = (q + TB - 1) / TB;
+  const int tp = (p + GT - 1) / GT, tq = (q + GT - 1) / GT;
   const int tiles = upper_only ? (tp * (tp + 1)) / 2 : tp * tq;
-  int splits = (4 * ctx->num_sms + tiles - 1) / tiles;
+  // row splits: fill whole waves of one CTA per SM (at least two waves' worth of CTAs)
+  int splits = 1;
+  {
+    const int sms = ctx->num_sms;
+    int best = 1;
+    double best_eff = -1.0;
+    for (int waves = 2; waves <= 8; ++waves) {
+      const int sp = (waves * sms) / tiles;
+      if (sp < 1) continue;
+      const long long ctas = (long long)sp * tiles;
+      const double eff = (double)ctas / (double)(((ctas + sms - 1) / sms) * sms);
+      if (eff > best_eff + 1e-9) {
+        best_eff = eff;
+        best = sp;
+      }
+    }
+    splits = best;
+  }
   int rows = (n + splits - 1) / splits;
-  rows = round_up(rows < TK ? TK : rows, TK);
+  rows = round_up(rows < GK ? GK : rows, GK);
   splits = (n + rows - 1) / rows;
   if (splits > 65535) return fail(ctx, DB200_ERR_UNSUPPORTED, "gram: too many row splits");
   dim3 grid(tp, tq, splits);
