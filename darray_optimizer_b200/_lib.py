@@ -36,6 +36,21 @@ class SvmReport(ctypes.Structure):
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
+
+class LandmarkReport(ctypes.Structure):
+    _fields_ = [("used_fallback", ctypes.c_int), ("rank", ctypes.c_int), ("residual_est", ctypes.c_double),
+                ("residual_fallback", ctypes.c_double), ("ms_features", ctypes.c_double),
+                ("ms_predict", ctypes.c_double), ("ms_select", ctypes.c_double), ("ms_factor", ctypes.c_double),
+                ("ms_residual", ctypes.c_double), ("ms_fallback", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_u64 = ctypes.c_uint64
+_fp = ctypes.POINTER(ctypes.c_float)
+_dp = ctypes.POINTER(ctypes.c_double)
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     "db200_create": (_c_int, [ctypes.POINTER(_vp), _c_int, _vp]),
@@ -87,6 +102,29 @@ SIGNATURES = {
                                      ctypes.POINTER(_c_double)]),
     "db200_rbf_sketch_noalloc": (_c_int, [_vp, _c_int, _c_int, _c_int, _c_int, _vp, _c_int, _vp, _c_int, _c_int, _vp,
                                           _vp, _vp, _c_int, _vp, _c_int, _c_float]),
+    # learned landmarks
+    "db200_knn_distance": (_c_int, [_vp, _c_int, _c_int, _vp, _c_int, _c_int, _vp, _c_int, _vp]),
+    "db200_leverage_features": (_c_int, [_vp, _c_int, _c_int, _vp, _c_int, _vp, _vp]),
+    "db200_ridge_leverage": (_c_int, [_vp, _c_int, _c_int, _vp, _c_int, _c_double, _vp]),
+    "db200_mlp_create": (_c_int, [_vp, _c_int, _c_int, _c_int, _u64, ctypes.POINTER(_vp)]),
+    "db200_mlp_destroy": (None, [_vp]),
+    "db200_mlp_param_count": (_c_int, [_vp]),
+    "db200_mlp_get_params": (_c_int, [_vp, _vp, _fp]),
+    "db200_mlp_set_params": (_c_int, [_vp, _vp, _fp]),
+    "db200_mlp_set_input_scaling": (_c_int, [_vp, _vp, _fp, _fp]),
+    "db200_mlp_forward": (_c_int, [_vp, _vp, _c_int, _vp, _vp]),
+    "db200_mlp_gradients": (_c_int, [_vp, _vp, _c_int, _vp, _vp, _fp, _vp]),
+    "db200_mlp_adam_step": (_c_int, [_vp, _vp, _c_int, _vp, _vp, _c_float, _fp]),
+    "db200_gumbel_keys": (_c_int, [_vp, _c_int, _vp, _u64, _vp]),
+    "db200_select_topk": (_c_int, [_vp, _c_int, _vp, _c_int, _vp]),
+    "db200_landmark_factor": (_c_int, [_vp, _c_int, _c_int, _vp, _c_int, _vp, _c_float, _c_int, _vp, _vp, _c_int,
+                                       _dp]),
+    "db200_residual_estimate": (_c_int, [_vp, _c_int, _c_int, _vp, _c_int, _vp, _c_float, _c_int, _vp, _c_int,
+                                         _c_int, _vp, _dp]),
+    "db200_svm_solve_landmarks": (_c_int, [_vp, _c_int, _c_int, _c_int, _vp, _c_int, _vp, _c_float, _c_double, _vp,
+                                           _u64, _c_int, _c_int, _c_double, _vp, _c_int, _c_int, _c_int,
+                                           ctypes.POINTER(BarrierParams), _vp, _vp, _c_int, ctypes.POINTER(SvmReport),
+                                           ctypes.POINTER(LandmarkReport)]),
 }
 
 STATUS = {
@@ -263,3 +301,99 @@ class Context:
     def rbf_block(self, m, n, d, Xi, ldxi, Xj, ldxj, layout, yi, yj, K, ldk, gamma):
         return self.check(self.lib.db200_rbf_block(self.h, m, n, d, Xi, ldxi, Xj, ldxj, layout, yi, yj, K, ldk,
                                                    gamma))
+
+    # ------------------------------------------------------------------ learned landmarks
+    def knn_distance(self, n, d, X, ldx, s, ref_idx, k, out):
+        return self.check(self.lib.db200_knn_distance(self.h, n, d, X, ldx, s, ref_idx, k, out))
+
+    def leverage_features(self, n, d, X, ldx, knn, F):
+        return self.check(self.lib.db200_leverage_features(self.h, n, d, X, ldx, knn, F))
+
+    def ridge_leverage(self, n, r, Z, ldz, lam, lev):
+        return self.check(self.lib.db200_ridge_leverage(self.h, n, r, Z, ldz, lam, lev))
+
+    def gumbel_keys(self, n, logits, seed, keys):
+        return self.check(self.lib.db200_gumbel_keys(self.h, n, logits, seed, keys))
+
+    def select_topk(self, n, keys, k, idx):
+        return self.check(self.lib.db200_select_topk(self.h, n, keys, k, idx))
+
+    def landmark_factor(self, n, d, X, ldx, y, gamma, r, idx, Z, ldz):
+        nu = _c_double()
+        self.check(self.lib.db200_landmark_factor(self.h, n, d, X, ldx, y, gamma, r, idx, Z, ldz, ctypes.byref(nu)))
+        return nu.value
+
+    def residual_estimate(self, n, d, X, ldx, y, gamma, r, Z, ldz, s, sample_idx):
+        est = _c_double()
+        self.check(self.lib.db200_residual_estimate(self.h, n, d, X, ldx, y, gamma, r, Z, ldz, s, sample_idx,
+                                                    ctypes.byref(est)))
+        return est.value
+
+    def svm_solve_landmarks(self, n, d, r, X, ldx, y, gamma, C, net, seed, s_knn, s_res, tol, Omega, ldo, l_fb, q,
+                            a, Z, ldz, params=None):
+        rep, lrep = SvmReport(), LandmarkReport()
+        p = params or self.barrier_params()
+        st = self.lib.db200_svm_solve_landmarks(self.h, n, d, r, X, ldx, y, gamma, C, net.h, seed, s_knn, s_res, tol,
+                                                Omega, ldo, l_fb, q, ctypes.byref(p), a, Z, ldz, ctypes.byref(rep),
+                                                ctypes.byref(lrep))
+        if st not in (0, -4):
+            self.check(st)
+        return rep, lrep
+
+
+class Mlp:
+    """The leverage MLP (db200_mlp): `hidden` ReLU layers of `width`, one linear output, on one context."""
+
+    def __init__(self, ctx: Context, in_dim: int, width: int = 256, hidden: int = 3, seed: int = 0):
+        self.ctx = ctx
+        h = _vp()
+        ctx.check(ctx.lib.db200_mlp_create(ctx.h, in_dim, width, hidden, seed, ctypes.byref(h)))
+        self.h = h
+        self.in_dim, self.width, self.hidden = in_dim, width, hidden
+
+    @property
+    def nparams(self) -> int:
+        return int(self.ctx.lib.db200_mlp_param_count(self.h))
+
+    def get_params(self):
+        import numpy as np
+        out = np.empty(self.nparams, dtype=np.float32)
+        self.ctx.check(self.ctx.lib.db200_mlp_get_params(self.ctx.h, self.h, out.ctypes.data_as(_fp)))
+        return out
+
+    def set_params(self, params):
+        import numpy as np
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        assert p.size == self.nparams
+        self.ctx.check(self.ctx.lib.db200_mlp_set_params(self.ctx.h, self.h, p.ctypes.data_as(_fp)))
+
+    def set_input_scaling(self, mean, scale):
+        import numpy as np
+        m = np.ascontiguousarray(mean, dtype=np.float32)
+        s = np.ascontiguousarray(scale, dtype=np.float32)
+        self.ctx.check(self.ctx.lib.db200_mlp_set_input_scaling(self.ctx.h, self.h, m.ctypes.data_as(_fp),
+                                                               s.ctypes.data_as(_fp)))
+
+    def forward(self, m, F, out):
+        return self.ctx.check(self.ctx.lib.db200_mlp_forward(self.ctx.h, self.h, m, F, out))
+
+    def gradients(self, m, F, target, grads):
+        loss = ctypes.c_float()
+        self.ctx.check(self.ctx.lib.db200_mlp_gradients(self.ctx.h, self.h, m, F, target, ctypes.byref(loss), grads))
+        return loss.value
+
+    def adam_step(self, m, F, target, lr):
+        loss = ctypes.c_float()
+        self.ctx.check(self.ctx.lib.db200_mlp_adam_step(self.ctx.h, self.h, m, F, target, lr, ctypes.byref(loss)))
+        return loss.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.lib.db200_mlp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -20,9 +20,10 @@ struct db200_context {
   void* io = nullptr;            // device staging for the host-pointer entry points
   size_t io_size = 0;
   // Further grow-only device buffers, one per call level so nested calls never share one:
-  // [0] dense linear algebra internals, [1] low-rank / solve pipeline, [2] barrier solver, [3] spare.
-  void* slot[4] = {nullptr, nullptr, nullptr, nullptr};
-  size_t slot_size[4] = {0, 0, 0, 0};
+  // [0] dense linear algebra internals, [1] low-rank / solve pipeline, [2] barrier solver, [3] spare,
+  // [4] learned-landmark pipeline (features, scores, landmark indices).
+  void* slot[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  size_t slot_size[5] = {0, 0, 0, 0, 0};
   double* h_pinned = nullptr;    // small pinned host staging area for scalar readbacks
   std::string last_error;
   long long launches = 0;        // kernels launched through this context
@@ -51,7 +52,7 @@ void prof_end(db200_context* ctx, cudaEvent_t e0);
 // Grow-only workspace; returns nullptr on failure (ctx->last_error set).
 void* workspace(db200_context* ctx, size_t bytes);
 void* io_buffer(db200_context* ctx, size_t bytes);
-enum { SLOT_LA = 0, SLOT_PIPE = 1, SLOT_BAR = 2, SLOT_SPARE = 3 };
+enum { SLOT_LA = 0, SLOT_PIPE = 1, SLOT_BAR = 2, SLOT_SPARE = 3, SLOT_LAND = 4 };
 void* slot_buffer(db200_context* ctx, int slot, size_t bytes);
 
 inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }

@@ -90,6 +90,36 @@ def sparse_binary(n: int = 262144, d: int = 123, seed: int = 3, p: float = 0.11)
     return Workload("sparse_binary", X, y, 0.05, 1024, 16, 1, 1.0, seed, meta={"b": b, "w": w, "p": p})
 
 
+def _mixture_points(g, n, meta):
+    comp = g.integers(0, meta["means"].shape[0], size=n)
+    d = meta["means"].shape[1]
+    X = np.empty((n, d), dtype=np.float64)
+    z = g.standard_normal((n, d))
+    for c in range(meta["means"].shape[0]):
+        sel = comp == c
+        if sel.any():
+            X[sel] = meta["means"][c] + (z[sel] * meta["scales"][c]) @ meta["rotations"][c].T
+    return X.astype(np.float32), meta["labels"][comp].astype(np.float32)
+
+
+def mixture(n: int = 524288, d: int = 64, seed: int = 5, components: int = 32, scale_lo: float = 0.1,
+            scale_hi: float = 3.0, mean_sd: float = 4.0) -> Workload:
+    """Config 5: a mixture of `components` anisotropic Gaussians with equal weights.  Component c has mean
+    ~ N(0, mean_sd^2 I), a random rotation (orthogonal factor of a Gaussian matrix) and per-axis scales log-uniform
+    in [scale_lo, scale_hi]; its label is a seeded random sign.  gamma = 1/d, r = 2048 landmarks, C = 1."""
+    g = rng(seed)
+    means = g.standard_normal((components, d)) * mean_sd
+    rot = np.empty((components, d, d))
+    for c in range(components):
+        q, r = np.linalg.qr(g.standard_normal((d, d)))
+        rot[c] = q * np.sign(np.diag(r))[None, :]
+    scales = np.exp(g.uniform(np.log(scale_lo), np.log(scale_hi), size=(components, d)))
+    labels = np.where(g.random(components) < 0.5, 1.0, -1.0)
+    meta = {"means": means, "rotations": rot, "scales": scales, "labels": labels}
+    X, y = _mixture_points(g, n, meta)
+    return Workload("mixture", X, y, 1.0 / d, 2048, 16, 1, 1.0, seed, meta=meta)
+
+
 def held_out(w: Workload, n_test: int) -> tuple[np.ndarray, np.ndarray]:
     """Test points from the same distribution and labelling rule as `w` (same hyperplane / class means), drawn
     from an independent stream (seed + 1 of the Philox family)."""
@@ -109,6 +139,8 @@ def held_out(w: Workload, n_test: int) -> tuple[np.ndarray, np.ndarray]:
         s = X.astype(np.float64) @ w.meta["w"] + w.meta["b"]
         y = np.where(s + g.normal(0.0, 0.5, n_test) >= 0, 1.0, -1.0).astype(np.float32)
         return X, y
+    if w.name == "mixture":
+        return _mixture_points(g, n_test, w.meta)
     raise ValueError(w.name)
 
 
@@ -116,6 +148,7 @@ CONFIGS = {
     "c1": two_gaussians,
     "c2": uniform_hyperplane,
     "c3": sparse_binary,
+    "c5": mixture,
 }
 
 

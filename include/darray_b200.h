@@ -291,6 +291,89 @@ DB200_API int db200_rbf_sketch_noalloc(void* stream, int m, int n, int d, int l,
                                        const float* Xj, int ldxj, int x_layout, const float* yi, const float* yj,
                                        const float* Omega, int ldo, float* Y, int ldy, float gamma);
 
+/* ------------------------------------------------------------------------------------------------------------
+ * Learned Nystrom landmarks.  No counterpart in the reference, which always sketches with a Gaussian Omega
+ * (include/dkernel.h:13-46, tests/testsvm.cpp:94-134): a small MLP predicts per-point ridge leverage scores, r
+ * landmarks are drawn by those scores, and the factor Z = K(:, L) chol(K(L, L))^-1 replaces the Gaussian sketch
+ * when a sampled residual estimate meets the tolerance; otherwise the Gaussian pipeline (db200_lowrank) runs.
+ * All pointers are device pointers; points are point-major float (ldx >= d).
+ * ------------------------------------------------------------------------------------------------------------ */
+
+/* Distance from each of the n points to its k-th nearest neighbour among the s reference points ref_idx
+ * (indices into X; a point is never its own neighbour).  k <= 16.  out: n floats.  Stream-ordered. */
+DB200_API int db200_knn_distance(db200_context* ctx, int n, int d, const float* X, int ldx, int s, const int* ref_idx,
+                                 int k, float* out);
+
+/* Leverage-model inputs, row-major n x (d + 2): [x_i, ||x_i||, knn_i].  Stream-ordered. */
+DB200_API int db200_leverage_features(db200_context* ctx, int n, int d, const float* X, int ldx, const float* knn,
+                                      float* F);
+
+/* Ridge leverage scores of K ~ Z Z^T (Z n x r FP64): lev_i = z_i^T (Z^T Z + lambda I)^-1 z_i, in FP64 (Gram,
+ * Cholesky, triangular inverse, row sums of squares).  Synchronous. */
+DB200_API int db200_ridge_leverage(db200_context* ctx, int n, int r, const double* Z, int ldz, double lambda,
+                                   double* lev);
+
+/* The leverage MLP: in_dim inputs (standardised with a per-input mean and scale), `hidden` ReLU layers of `width`
+ * units, one linear output.  Weights and activations are bf16 in the forward pass, accumulation fp32; master
+ * weights, gradients and Adam moments fp32.  Flat parameter order: for each layer l, W_l (out x in, row major)
+ * then b_l. */
+typedef struct db200_mlp db200_mlp;
+DB200_API int db200_mlp_create(db200_context* ctx, int in_dim, int width, int hidden, unsigned long long seed,
+                               db200_mlp** out);
+DB200_API void db200_mlp_destroy(db200_mlp* net);
+DB200_API int db200_mlp_param_count(const db200_mlp* net);
+/* Copy the fp32 master parameters to / from host memory (param_count floats). */
+DB200_API int db200_mlp_get_params(db200_context* ctx, const db200_mlp* net, float* host);
+DB200_API int db200_mlp_set_params(db200_context* ctx, db200_mlp* net, const float* host);
+/* Input standardisation: x' = (x - mean) * scale (host arrays of in_dim floats). */
+DB200_API int db200_mlp_set_input_scaling(db200_context* ctx, db200_mlp* net, const float* mean, const float* scale);
+/* out[i] = net(F[i, :]) for m rows of F (device, row-major m x in_dim).  Stream-ordered. */
+DB200_API int db200_mlp_forward(db200_context* ctx, const db200_mlp* net, int m, const float* F, float* out);
+/* Loss 0.5 mean_i (net(F_i) - t_i)^2 and its gradient with respect to the flat parameters (device array of
+ * param_count floats).  loss: host.  Synchronous. */
+DB200_API int db200_mlp_gradients(db200_context* ctx, db200_mlp* net, int m, const float* F, const float* target,
+                                  float* loss, float* grads);
+/* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8) on the loss above; loss (host, may be NULL). */
+DB200_API int db200_mlp_adam_step(db200_context* ctx, db200_mlp* net, int m, const float* F, const float* target,
+                                  float lr, float* loss);
+
+/* Gumbel keys for sampling without replacement proportional to exp(logits): keys_i = logits_i + G_i, G_i a
+ * seeded standard Gumbel variate; the k largest keys are a weighted sample (Gumbel top-k).  Stream-ordered. */
+DB200_API int db200_gumbel_keys(db200_context* ctx, int n, const float* logits, unsigned long long seed, float* keys);
+/* Indices of the k largest keys (any order).  Synchronous. */
+DB200_API int db200_select_topk(db200_context* ctx, int n, const float* keys, int k, int* idx);
+
+/* Nystrom factor on landmarks idx (r indices): C = diag(y) K(:, L) diag(y_L) (n x r, fused tile kernel),
+ * W = C(L, :) in FP64, R^T R = W + nu I (shifted Cholesky, nu = 1e-7 tr(W)/r, x10 until positive definite),
+ * Z = C R^-1 (n x r FP64), so diag(y) K diag(y) ~ Z Z^T.  nu_out: host, may be NULL.  Synchronous. */
+DB200_API int db200_landmark_factor(db200_context* ctx, int n, int d, const float* X, int ldx, const float* y,
+                                    float gamma, int r, const int* idx, double* Z, int ldz, double* nu_out);
+
+/* Sampled residual ||Q(:, S) - Z Z(S, :)^T||_F / ||Q(:, S)||_F with Q = diag(y) K diag(y) over s columns S
+ * (indices): an estimate of ||Q - Z Z^T||_F / ||Q||_F.  est: host.  Synchronous. */
+DB200_API int db200_residual_estimate(db200_context* ctx, int n, int d, const float* X, int ldx, const float* y,
+                                      float gamma, int r, const double* Z, int ldz, int s, const int* sample_idx,
+                                      double* est);
+
+typedef struct {
+  int used_fallback;     /* 1 when the Gaussian sketch replaced the landmark factor */
+  int rank;              /* columns of Z actually used by the barrier */
+  double residual_est;   /* sampled residual of the landmark factor */
+  double residual_fallback; /* sampled residual of the Gaussian factor (fallback only, else 0) */
+  double ms_features, ms_predict, ms_select, ms_factor, ms_residual, ms_fallback;
+} db200_landmark_report;
+
+/* Learned-landmark SVM solve: features (8-NN distance over s_knn reference points) -> MLP log-leverage ->
+ * Gumbel top-r landmarks -> Nystrom factor -> sampled residual estimate (s_res columns); if the estimate exceeds
+ * tol the Gaussian pipeline db200_lowrank(l_fb = Omega's columns, q) builds the factor instead; then the barrier
+ * (db200_svm_barrier) on the factor.  Z: n x max(r, l_fb) FP64, a: n.  Synchronous. */
+DB200_API int db200_svm_solve_landmarks(db200_context* ctx, int n, int d, int r, const float* X, int ldx,
+                                        const float* y, float gamma, double C, const db200_mlp* net,
+                                        unsigned long long seed, int s_knn, int s_res, double tol,
+                                        const float* Omega, int ldo, int l_fb, int q,
+                                        const db200_barrier_params* params, double* a, double* Z, int ldz,
+                                        db200_svm_report* rep, db200_landmark_report* lrep);
+
 #ifdef __cplusplus
 }
 #endif

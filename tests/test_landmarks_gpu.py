@@ -1,0 +1,161 @@
+"""GPU parity of the learned-landmark path (csrc/landmarks.cu) against the FP64 oracle (oracle/landmarks.py):
+k-NN features, the MLP forward / gradient / Adam step with bf16 weights and activations, ridge leverage, Gumbel
+top-k selection, the landmark Nystrom factor, the sampled residual and the end-to-end solve with and without the
+Gaussian fallback."""
+import numpy as np
+import pytest
+
+from oracle import landmarks as LO
+from tests.util import dev, ptr, rel_fro
+
+pytestmark = pytest.mark.gpu
+
+
+def _mixture(n, seed, d=64):
+    from darray_optimizer_b200 import datagen
+    return datagen.mixture(n=n, d=d, seed=seed)
+
+
+def test_knn_distance_and_features(gpu_ctx):
+    import torch
+    w = _mixture(3000, 11)
+    g = np.random.default_rng(0)
+    ref = np.sort(g.choice(3000, size=1000, replace=False)).astype(np.int32)
+    dX, dref = dev(w.X), dev(ref)
+    out = torch.empty(3000, dtype=torch.float32, device="cuda")
+    gpu_ctx.knn_distance(3000, 64, ptr(dX), 64, 1000, ptr(dref), 8, ptr(out))
+    F = torch.empty((3000, 66), dtype=torch.float32, device="cuda")
+    gpu_ctx.leverage_features(3000, 64, ptr(dX), 64, ptr(out), ptr(F))
+    gpu_ctx.sync()
+    ref_knn = LO.knn_distance(w.X, ref, 8)
+    got = out.cpu().numpy()
+    assert np.max(np.abs(got - ref_knn) / ref_knn) <= 1e-4
+    assert rel_fro(F.cpu().numpy(), LO.leverage_features(w.X, ref_knn)) <= 1e-5
+
+
+def _net_and_data(gpu_ctx, m=512, in_dim=66, width=256, hidden=3, seed=3):
+    from darray_optimizer_b200._lib import Mlp
+    g = np.random.default_rng(seed)
+    net = Mlp(gpu_ctx, in_dim, width, hidden, seed=seed)
+    F = (g.standard_normal((m, in_dim)) * 2 + 1).astype(np.float32)
+    t = g.standard_normal(m).astype(np.float32)
+    mean = F.mean(0).astype(np.float32)
+    scale = (1.0 / F.std(0)).astype(np.float32)
+    net.set_input_scaling(mean, scale)
+    return net, F, t, mean, scale
+
+
+def test_mlp_forward_and_gradients_match_oracle(gpu_ctx):
+    import torch
+    net, F, t, mean, scale = _net_and_data(gpu_ctx)
+    p = net.get_params()
+    dF, dt = dev(F), dev(t)
+    out = torch.empty(F.shape[0], dtype=torch.float32, device="cuda")
+    net.forward(F.shape[0], ptr(dF), ptr(out))
+    grads = torch.empty(net.nparams, dtype=torch.float32, device="cuda")
+    loss = net.gradients(F.shape[0], ptr(dF), ptr(dt), ptr(grads))
+    gpu_ctx.sync()
+    ref_out, _ = LO.mlp_forward(p, F, mean, scale, 256, 3)
+    assert rel_fro(out.cpu().numpy(), ref_out) <= 5e-3
+    ref_loss, ref_grad = LO.mlp_loss_grad(p, F, t, mean, scale, 256, 3)
+    assert abs(loss - ref_loss) <= 5e-3 * abs(ref_loss)
+    g = grads.cpu().numpy()
+    layout, _ = LO.mlp_layout(66, 256, 3)
+    for ow, ob, fi, fo in layout:  # every layer's weights and biases
+        assert rel_fro(g[ow:ow + fi * fo], ref_grad[ow:ow + fi * fo]) <= 2e-2
+        assert rel_fro(g[ob:ob + fo], ref_grad[ob:ob + fo]) <= 2e-2
+
+
+def test_mlp_adam_step_matches_oracle(gpu_ctx):
+    net, F, t, mean, scale = _net_and_data(gpu_ctx, seed=4)
+    p0 = net.get_params().astype(np.float64)
+    dF, dt = dev(F), dev(t)
+    lr = 1e-3
+    net.adam_step(F.shape[0], ptr(dF), ptr(dt), lr)
+    p1 = net.get_params().astype(np.float64)
+    _, g = LO.mlp_loss_grad(p0, F, t, mean, scale, 256, 3)
+    ref, _, _ = LO.adam(p0, g, np.zeros_like(p0), np.zeros_like(p0), 1, lr)
+    # the first Adam step moves every parameter with a non-negligible gradient by ~lr * sign(g)
+    big = np.abs(g) > 1e-3 * np.abs(g).max()
+    assert np.mean(np.sign(p1 - p0)[big] == np.sign(ref - p0)[big]) >= 0.98
+    assert rel_fro((p1 - p0)[big], (ref - p0)[big]) <= 5e-2
+
+
+def test_mlp_training_reduces_loss(gpu_ctx):
+    from darray_optimizer_b200._lib import Mlp
+    import torch
+    g = np.random.default_rng(5)
+    F = g.standard_normal((4096, 8)).astype(np.float32)
+    t = (np.sin(F[:, 0]) + F[:, 1] * F[:, 2]).astype(np.float32)
+    net = Mlp(gpu_ctx, 8, 64, 3, seed=1)
+    dF, dt = dev(F), dev(t)
+    losses = [net.adam_step(4096, ptr(dF), ptr(dt), 3e-3) for _ in range(300)]
+    assert losses[-1] < 0.2 * losses[0]
+
+
+def test_ridge_leverage_matches_oracle(gpu_ctx):
+    import torch
+    g = np.random.default_rng(6)
+    Z = np.asfortranarray(g.standard_normal((2000, 64)))
+    dZ = dev(Z)
+    lev = torch.empty(2000, dtype=torch.float64, device="cuda")
+    gpu_ctx.ridge_leverage(2000, 64, ptr(dZ), 2000, 5.0, ptr(lev))
+    assert rel_fro(lev.cpu().numpy(), LO.ridge_leverage(Z, 5.0)) <= 1e-10
+
+
+def test_gumbel_topk_matches_oracle(gpu_ctx):
+    import torch
+    g = np.random.default_rng(7)
+    logits = (g.standard_normal(50000) * 2).astype(np.float32)
+    dl = dev(logits)
+    keys = torch.empty(50000, dtype=torch.float32, device="cuda")
+    gpu_ctx.gumbel_keys(50000, ptr(dl), 1234, ptr(keys))
+    idx = torch.empty(700, dtype=torch.int32, device="cuda")
+    gpu_ctx.select_topk(50000, ptr(keys), 700, ptr(idx))
+    kg = keys.cpu().numpy()
+    kr = LO.gumbel_keys(logits, 1234)
+    assert np.max(np.abs(kg - kr)) <= 1e-5
+    got = idx.cpu().numpy()
+    assert np.array_equal(got, np.sort(got))
+    assert np.array_equal(got, LO.topk_indices(kg, 700))  # exact selection on the GPU's own keys
+
+
+def test_landmark_factor_and_residual_match_oracle(gpu_ctx):
+    import torch
+    w = _mixture(2048, 12)
+    n, r = 2048, 256
+    g = np.random.default_rng(8)
+    idx = np.sort(g.choice(n, size=r, replace=False)).astype(np.int32)
+    S = np.sort(g.choice(n, size=128, replace=False)).astype(np.int32)
+    dX, dy, didx, dS = dev(w.X), dev(w.y), dev(idx), dev(S)
+    Z = torch.zeros((r, n), dtype=torch.float64, device="cuda")
+    gpu_ctx.landmark_factor(n, 64, ptr(dX), 64, ptr(dy), w.gamma, r, ptr(didx), ptr(Z), n)
+    est = gpu_ctx.residual_estimate(n, 64, ptr(dX), 64, ptr(dy), w.gamma, r, ptr(Z), n, 128, ptr(dS))
+    Zg = Z.cpu().numpy().T
+    Zr, _ = LO.landmark_factor(w.X, w.y, w.gamma, idx)
+    # K(:, L) comes from the fp32 tile kernel (split-bf16 distances, fp32 exp); W = K(L, L) is near singular
+    assert rel_fro(Zg @ Zg.T, Zr @ Zr.T) <= 5e-4
+    ref = LO.residual_estimate(w.X, w.y, w.gamma, Zr, S)
+    assert abs(est - ref) <= 1e-2 * ref
+
+
+@pytest.mark.parametrize("tol,expect_fallback", [(1e9, 0), (0.0, 1)])
+def test_svm_solve_landmarks_end_to_end(gpu_ctx, tol, expect_fallback):
+    import torch
+    from darray_optimizer_b200._lib import Mlp
+    w = _mixture(8192, 13)
+    n, d, r, l_fb = 8192, 64, 512, 528
+    net = Mlp(gpu_ctx, d + 2, 256, 3, seed=2)
+    dX, dy = dev(w.X), dev(w.y)
+    Om = np.random.default_rng(9).standard_normal((n, l_fb)).astype(np.float32)
+    dO = dev(np.ascontiguousarray(Om.T))
+    a = torch.zeros(n, dtype=torch.float64, device="cuda")
+    Z = torch.zeros((l_fb, n), dtype=torch.float64, device="cuda")
+    rep, lrep = gpu_ctx.svm_solve_landmarks(n, d, r, ptr(dX), d, ptr(dy), w.gamma, w.C, net, 77, 2048, 256, tol,
+                                            ptr(dO), n, l_fb, 1, ptr(a), ptr(Z), n)
+    assert lrep.used_fallback == expect_fallback
+    assert lrep.rank == (l_fb if expect_fallback else r)
+    assert 0.0 < lrep.residual_est < 1.0
+    assert rep.gap_barrier < 1e-6 and rep.gap_primal_dual < 1e-6  # both relative to |f|
+    av = a.cpu().numpy()
+    assert np.all(av >= 0) and np.all(av <= w.C)
