@@ -149,6 +149,7 @@ int db200_destroy(db200_context* ctx) {
   if (ctx->io) cudaFree(ctx->io);
   for (void* p : ctx->slot)
     if (p) cudaFree(p);
+  if (ctx->tile_table) cudaFree(ctx->tile_table);
   if (ctx->d_status) cudaFree(ctx->d_status);
   if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);

@@ -25,6 +25,8 @@ struct db200_context {
   void* slot[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   size_t slot_size[5] = {0, 0, 0, 0, 0};
   double* h_pinned = nullptr;    // small pinned host staging area for scalar readbacks
+  void* tile_table = nullptr;    // instance table of the tile engine (grow-only)
+  size_t tile_table_size = 0;
   std::string last_error;
   long long launches = 0;        // kernels launched through this context
   // Optional per-launch timing of the tcgen05 tile kernels (CUDA events on the launching stream).
@@ -98,10 +100,39 @@ int feature_pad(int d);  // dp: padded feature count of the split operand
 // a set used as rows and as columns packs once.
 inline int point_pad(int n) { return round_up(n < 1 ? 1 : n, 256); }
 
-// Launch the fused tile kernel.  For RBF_MODE_SKETCH, `op` is the packed Omega^T and `out` is Y (m x l, column
-// major, leading dimension ldo); for RBF_MODE_KBLOCK, `out` is the kernel block K (m x n, column major).
+// One problem of the fused tile engine: Y = diag(yi) K(Xi, Xj) diag(yj) Omega (SKETCH, `op` = packed Omega^T) or
+// the kernel block (KBLOCK), written to `out` (column major, leading dimension ldo).
+struct TileJob {
+  PackedPoints pi, pj;
+  const float* yi = nullptr;
+  const float* yj = nullptr;
+  const void* op = nullptr;
+  SketchPlan plan;
+  int l = 0;
+  float gamma = 0.f;
+  float* out = nullptr;
+  long long ldo = 0;
+};
+// A prepared launch: the instance table is on the device; launch_rbf_plan only launches (graph-capturable).
+struct TilePlan {
+  int mode = 0, count = 0, n_items = 0, nsx = 0, nso = 0, nkc_max = 0, panel_max = 0;
+  size_t smem = 0;
+  const void* table = nullptr;
+  alignas(64) unsigned char tm1[4 * 128];  // instance 0's tensor maps (kernel parameters of one-instance launches)
+};
+size_t tile_table_bytes(int count);
+// Build the instance table of `count` jobs and copy it to the device (table_storage if given, else a context
+// buffer).  Stream-ordered.
+int prepare_rbf_tiles(db200_context* ctx, int mode, const TileJob* jobs, int count, void* table_storage,
+                      size_t table_capacity, TilePlan* plan);
+// One persistent launch over every work item of the prepared jobs.
+int launch_rbf_plan(db200_context* ctx, const TilePlan& plan);
+
+// Launch the fused tile kernel for one problem.  For RBF_MODE_SKETCH, `op` is the packed Omega^T and `out` is Y
+// (m x l, column major, leading dimension ldo); for RBF_MODE_KBLOCK, `out` is the kernel block K (m x n, column
+// major).  table_storage: device memory for the one-instance table (NULL: a context buffer).
 int launch_rbf_tiles(db200_context* ctx, int mode, const PackedPoints& pi, const PackedPoints& pj, const float* yi,
                      const float* yj, const void* op, const SketchPlan& plan, int l, float gamma, float* out,
-                     int ldo);
+                     int ldo, void* table_storage = nullptr, size_t table_capacity = 0);
 
 }  // namespace db200

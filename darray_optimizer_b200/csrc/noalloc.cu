@@ -61,7 +61,8 @@ extern "C" int db200_rbf_sketch_noalloc(void* stream, int m, int n, int d, int l
     return DB200_ERR_INVALID;
   }
 
-  // Scratch layout: [status | Xi packed | Xi norms | Xj packed | Xj norms | Omega^T packed], 256-byte aligned.
+  // Scratch layout: [status | Xi packed | Xi norms | Xj packed | Xj norms | Omega^T packed | tile table],
+  // 256-byte aligned.
   const int dp = feature_pad(d);
   const int mpad = point_pad(m), npad = point_pad(n);
   const bool same = (Xi == Xj && ldxi == ldxj && m == n);
@@ -74,6 +75,7 @@ extern "C" int db200_rbf_sketch_noalloc(void* stream, int m, int n, int d, int l
     need = align_up(need + (size_t)npad * 4, 256);
   }
   need = align_up(need + (size_t)plan.lrows * npad * 2, 256);
+  need = align_up(need + tile_table_bytes(1), 256);
   if (need > (size_t)DB200_NOALLOC_SCRATCH_BYTES) {
     std::fprintf(stderr,
                  "db200_rbf_sketch_noalloc: m=%d n=%d d=%d l=%d needs %zu bytes of scratch, more than the fixed "
@@ -121,7 +123,10 @@ extern "C" int db200_rbf_sketch_noalloc(void* stream, int m, int n, int d, int l
   }
   void* op = carve.take<uint16_t>((size_t)plan.lrows * npad);
   if ((st = pack_sketch(&ctx, Omega, ldo, yj, n, l, npad, plan.lrows, op))) return st;
-  if ((st = launch_rbf_tiles(&ctx, RBF_MODE_SKETCH, pi, pj, yi, nullptr, op, plan, l, gamma, Y, ldy))) return st;
+  void* table = carve.take<char>(tile_table_bytes(1));  // the tile engine's one-instance table
+  if ((st = launch_rbf_tiles(&ctx, RBF_MODE_SKETCH, pi, pj, yi, nullptr, op, plan, l, gamma, Y, ldy, table,
+                             tile_table_bytes(1))))
+    return st;
 
   // Synchronous: wait, then report a device-side wait that gave up.
   if (cudaStreamSynchronize(ctx.stream) != cudaSuccess) return DB200_ERR_CUDA;

@@ -23,8 +23,12 @@
 // sketch MMA.
 #include <cuda.h>
 #include <cudaTypedefs.h>
+#include <algorithm>
 #include <cstdio>
+#include <cstring>
 #include <mutex>
+#include <type_traits>
+#include <vector>
 
 #include "internal.h"
 #include "ptx.cuh"
@@ -50,21 +54,35 @@ constexpr int BAR_BYTES = 1024;     // barrier region: barriers, TMEM slot, abor
 constexpr int MAX_NSX = 16, MAX_NSO = 4;
 constexpr float LOG2E = 1.4426950408889634f;
 
-// Runtime plan of one launch: TMEM columns (G buffers, the fp16 P tile, the Y panel) and ring depths.
-struct TileArgs {
+// One instance of the tile engine.  A launch walks a work list over a table of instances in global memory (one
+// instance for the single-problem entry points, many for the batched one); work item k belongs to the instance
+// with the largest item_begin <= k and covers one 256-row block of its points i and one panel of its sketch.
+struct alignas(64) TileInst {
+  CUtensorMap tm_xi, tm_xj, tm_om1, tm_om2;  // packed points (rows i, rows j) and the two Omega~ row boxes
+  const float* si;       // squared norms, padded to n_itiles * 256 / n_jtiles * 128
+  const float* sj;
+  const float* yi;
+  const float* yj;
+  float* out;
+  long long ldo;
   int m, n;              // valid rows / columns
   int n_itiles, n_jtiles, n_panels, panel, l;  // n_itiles counts 256-row pair tiles
   int n1, n2;            // sketch MMA split of the panel: N = n1 (+ n2) columns, n2 = 0 for one instruction
   int g_bufs;            // 1 or 2 TMEM buffers of 128 columns for G
   int tmem_p, tmem_y;    // first TMEM column of the P tile (64 columns) and of the Y panel
-  int nsx, nso;          // Xj and Omega ring stages
+  int nkc;               // 64-element chunks per packed row [hi | lo]: 1..4 (feature pad 32..128)
+  int item_begin;        // first work item of this instance
   float c_row, c_dot;    // -gamma*log2e, 2*gamma*log2e
-  const float* si;
-  const float* sj;
-  const float* yi;
-  const float* yj;
-  float* out;
-  int ldo;
+};
+
+struct LaunchArgs {
+  // A one-instance launch carries its tensor maps as kernel parameters (read through the constant bank);
+  // batched launches read them from the instance table in global memory.
+  CUtensorMap tm1[4];
+  const TileInst* inst;
+  int count, n_items;
+  int nsx, nso;          // Xj and Omega ring stages
+  int nkc_max, panel_max;  // shared-memory layout covers every instance
   int* status;
 };
 
@@ -74,9 +92,8 @@ struct SmemLayout {
 };
 constexpr int SJ_BYTES = NUM_EPI_WARPS * 2 * EPI_COLS * 4;  // per epilogue warp: two tiles' column norms
 
-__host__ __device__ inline SmemLayout make_layout(int dp, int panel, int nsx, int nso) {
+__host__ __device__ inline SmemLayout make_layout(int nkc, int panel, int nsx, int nso) {
   SmemLayout L;
-  const int nkc = (2 * dp) / KC;
   L.om_stage = (panel / 2) * 128;
   L.off_xi = 0;
   L.off_xj = L.off_xi + (size_t)nkc * XI_CHUNK;
@@ -109,21 +126,145 @@ enum {
 constexpr int TMEM_SLOT_OFF = 960, ABORT_OFF = 968;
 static_assert((B_XJ_FULL0 + 2 * MAX_NSX + 2 * MAX_NSO) * 8 <= TMEM_SLOT_OFF, "barrier region too small");
 
+// work item k -> instance (binary search over item_begin; the table is tiny and cached)
+__device__ __forceinline__ int find_inst(const TileInst* inst, int count, int k) {
+  int lo = 0, hi = count - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(&inst[mid].item_begin) <= k) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <int V>
+using IntC = std::integral_constant<int, V>;
+
+// State of the MMA issuer: ring positions and phases, carried across tiles, items and instances.
+struct Issuer {
+  uint32_t tmem_base, s_bar, om_stage16;
+  uint64_t dxi, dxj, dom;
+  int nsx, nso, XJ_FULL, XJ_EMPTY, OM_FULL, OM_EMPTY;
+  volatile int* abort_flag;
+  uint32_t xs, xph, os, oph, pph;
+  uint32_t guse0, guse1, gnext;  // uses of G buffer 0 / 1 (their phases) and the next buffer to fill
+};
+
+__device__ __forceinline__ bool issuer_wait(const Issuer& S, int idx, uint32_t parity) {
+  return __all_sync(0xffffffffu, mbar_wait(S.s_bar + 8u * (uint32_t)idx, parity, S.abort_flag));
+}
+
+// Distance MMA of one tile into the next G buffer, for a packed row of 2 * DP elements (split bf16).
+template <int DP>
+__device__ __forceinline__ bool issue_mma1(Issuer& S, int g_bufs) {
+  constexpr uint32_t idesc_g = idesc_f16(PAIR_M, BN, true);
+  constexpr int NKC = (2 * DP) / KC;
+  const uint32_t gbuf = S.gnext;
+  const uint32_t guse = gbuf ? S.guse1 : S.guse0;
+  if (!issuer_wait(S, B_G_EMPTY0 + (int)gbuf, (guse & 1) ^ 1)) return false;
+  tc_fence_after();
+  const uint32_t d_tmem = S.tmem_base + gbuf * BN;
+#pragma unroll
+  for (int c = 0; c < NKC; ++c) {
+    if (!issuer_wait(S, S.XJ_FULL + (int)S.xs, S.xph)) return false;
+    tc_fence_after();
+    if (elect_one()) {
+      const uint64_t bbase = S.dxj + ((S.xs * XJ_CHUNK) >> 4);
+#pragma unroll
+      for (int ks = 0; ks < KC / 16; ++ks) {
+        const int o = c * KC + ks * 16;  // K offset of this slice inside the packed row [hi | lo]
+        const uint64_t bdesc = bbase + ((ks * 32) >> 4);
+        if (o < DP) {  // B slice is hi_j: pair with hi_i and lo_i
+          const int oh = o, ol = DP + o;
+          umma_f16_pair(d_tmem, S.dxi + (((oh / KC) * XI_CHUNK + (oh % KC) * 2) >> 4), bdesc, idesc_g,
+                        o == 0 ? 0u : 1u);
+          umma_f16_pair(d_tmem, S.dxi + (((ol / KC) * XI_CHUNK + (ol % KC) * 2) >> 4), bdesc, idesc_g, 1u);
+        } else {  // B slice is lo_j: pair with hi_i
+          const int oh = o - DP;
+          umma_f16_pair(d_tmem, S.dxi + (((oh / KC) * XI_CHUNK + (oh % KC) * 2) >> 4), bdesc, idesc_g, 1u);
+        }
+      }
+      umma_commit_pair(S.s_bar + 8u * (uint32_t)(S.XJ_EMPTY + (int)S.xs));
+      if (c == NKC - 1) umma_commit_pair(S.s_bar + 8u * (uint32_t)(B_G_FULL0 + (int)gbuf));
+    }
+    __syncwarp();
+    if (++S.xs == (uint32_t)S.nsx) { S.xs = 0; S.xph ^= 1; }
+  }
+  if (gbuf) ++S.guse1;
+  else ++S.guse0;
+  S.gnext = (g_bufs == 2) ? (gbuf ^ 1u) : 0u;
+  return true;
+}
+
+// Per-item constants of the sketch MMA.
+struct SketchMma {
+  uint32_t idesc_y1, idesc_y2, y2_boff, tmem_p, tmem_y, tmem_y2;
+};
+
+// Sketch MMA of one tile: two K chunks of 64, one per P half.  fp16 operands (P in [0, 1], Omega~ Gaussian: both
+// well inside fp16 range, 3 more mantissa bits than bf16 at the same tensor rate).
+template <bool TWO>
+__device__ __forceinline__ bool issue_mma2(Issuer& S, const SketchMma& Y, int jt) {
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+    // K chunk c of the sketch MMA reads P half c (j in [64c, 64c + 64))
+    if (!issuer_wait(S, B_P_FULL0 + c, S.pph)) return false;
+    if (!issuer_wait(S, S.OM_FULL + (int)S.os, S.oph)) return false;
+    tc_fence_after();
+    if (elect_one()) {
+      const uint64_t bbase = S.dom + S.os * S.om_stage16;
+#pragma unroll
+      for (int ks = 0; ks < KC / 16; ++ks) {
+        // A = P (fp16 in TMEM, 8 columns per 16-wide K step), B = Omega~ rows of this panel
+        const uint32_t a_tmem = Y.tmem_p + c * 32 + ks * 8;
+        const uint64_t bdesc = bbase + ((ks * 32) >> 4);
+        const uint32_t acc = (jt > 0 || c > 0 || ks > 0) ? 1u : 0u;
+        umma_f16_ts_pair(Y.tmem_y, a_tmem, bdesc, Y.idesc_y1, acc);
+        if (TWO) umma_f16_ts_pair(Y.tmem_y2, a_tmem, bdesc + Y.y2_boff, Y.idesc_y2, acc);
+      }
+      umma_commit_pair(S.s_bar + 8u * (uint32_t)(S.OM_EMPTY + (int)S.os));
+      umma_commit_pair(S.s_bar + 8u * (uint32_t)(B_P_EMPTY0 + c));
+    }
+    __syncwarp();
+    if (++S.os == (uint32_t)S.nso) { S.os = 0; S.oph ^= 1; }
+  }
+  S.pph ^= 1;
+  return true;
+}
+
+// All MMAs of one work item (every j tile, distance MMA one tile ahead of the sketch MMA), specialised for the
+// instance's feature width and panel split so the hot loop carries no dispatch.
+template <int MODE, int DP, bool TWO>
+__device__ __forceinline__ bool issue_item(Issuer& S, const SketchMma& Y, int njt, int g_bufs) {
+  if (!issue_mma1<DP>(S, g_bufs)) return false;
+  for (int jt = 0; jt < njt; ++jt) {
+    if (jt + 1 < njt && !issue_mma1<DP>(S, g_bufs)) return false;
+    if (MODE == RBF_MODE_SKETCH && !issue_mma2<TWO>(S, Y, jt)) return false;
+  }
+  return true;
+}
+
+template <int MODE, bool TWO>
+__device__ __forceinline__ bool issue_item_dp(Issuer& S, const SketchMma& Y, int nkc, int njt, int g_bufs) {
+  switch (nkc) {
+    case 1: return issue_item<MODE, 32, TWO>(S, Y, njt, g_bufs);
+    case 2: return issue_item<MODE, 64, TWO>(S, Y, njt, g_bufs);
+    case 3: return issue_item<MODE, 96, TWO>(S, Y, njt, g_bufs);
+    default: return issue_item<MODE, 128, TWO>(S, Y, njt, g_bufs);
+  }
+}
+
 // One CTA pair (cluster of 2) owns a 256-row block of points i (128 rows per CTA, rank r holds rows 128r..) and one
 // panel of sketch columns.  The leader (rank 0) issues every MMA as cta_group::2 with M = 256: A (Xi, P) is each
 // CTA's own 128 rows, B (Xj, Omega~) is split by rows between the two CTAs, the accumulators (G, Y) sit in each
 // CTA's tensor memory for its own rows.  Each CTA loads its own operand halves with TMA and the completion is
-// counted on the leader's barrier.
-template <int MODE, int DP, bool TWO_Y>
-__global__ void __launch_bounds__(NUM_THREADS, 1)
-    rbf_tile_kernel(const __grid_constant__ CUtensorMap tm_xi, const __grid_constant__ CUtensorMap tm_xj,
-                    const __grid_constant__ CUtensorMap tm_om1, const __grid_constant__ CUtensorMap tm_om2,
-                    TileArgs args) {
+// counted on the leader's barrier.  All rings and barrier phases run on across work items and instances.
+template <int MODE>
+__global__ void __launch_bounds__(NUM_THREADS, 1) rbf_tile_kernel(const __grid_constant__ LaunchArgs args) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  constexpr int NKC = (2 * DP) / KC;  // 64-element chunks per packed row [hi | lo]
-  const SmemLayout L = make_layout(DP, args.panel, args.nsx, args.nso);
-  const int nsx = args.nsx, nso = args.nso, gb = args.g_bufs;
+  const SmemLayout L = make_layout(args.nkc_max, args.panel_max, args.nsx, args.nso);
+  const int nsx = args.nsx, nso = args.nso;
   const uint32_t s_xi = smem_u32(smem + L.off_xi);
   const uint32_t s_xj = smem_u32(smem + L.off_xj);
   const uint32_t s_om = smem_u32(smem + L.off_om);
@@ -138,7 +279,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
   const uint32_t rank = cluster_ctarank();
   const bool leader = (rank == 0);
   const int cid = (int)cluster_id_x(), ncl = (int)cluster_count_x();
-  const int n_items = args.n_itiles * args.n_panels;
+  const int n_items = args.n_items;
   // leader-side barrier addresses in the shared::cluster window
   auto lbar = [&](int idx) -> uint32_t { return mapa_shared(bar(idx), 0); };
   // a wait that gives up also stops the other CTA of the pair
@@ -169,14 +310,6 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
     }
     fence_mbarrier_init();
   }
-  if (warp == 0 && lane == 0) {
-    prefetch_tmap(&tm_xi);
-    prefetch_tmap(&tm_xj);
-  }
-  if (warp == OM_WARP && lane == 0 && MODE == RBF_MODE_SKETCH) {
-    prefetch_tmap(&tm_om1);
-    if (TWO_Y) prefetch_tmap(&tm_om2);
-  }
   if (warp == 1) {
     tmem_alloc_pair(smem_u32(tmem_slot), TMEM_COLS);
     tmem_relinquish_pair();
@@ -191,36 +324,57 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
     if (lane == 0) {
       const bool points = (warp == 0);
       uint32_t xs = 0, xph = 0, os = 0, oph = 0, items_done = 0;
+      int last = -1;
       bool ok = true;
       for (int item = cid; item < n_items && ok; item += ncl, ++items_done) {
-        const int it = item % args.n_itiles, pn = item / args.n_itiles;
+        const int b = find_inst(args.inst, args.count, item);
+        const TileInst* I = args.inst + b;
+        const int li = item - I->item_begin;
+        const int it = li % I->n_itiles, pn = li / I->n_itiles;
+        const int nkc = I->nkc, njt = I->n_jtiles;
+        const bool one = (args.count == 1);
+        const CUtensorMap* t_xi = one ? &args.tm1[0] : &I->tm_xi;
+        const CUtensorMap* t_xj = one ? &args.tm1[1] : &I->tm_xj;
+        const CUtensorMap* t_om1 = one ? &args.tm1[2] : &I->tm_om1;
+        const CUtensorMap* t_om2 = one ? &args.tm1[3] : &I->tm_om2;
+        if (b != last) {
+          if (points) {
+            prefetch_tmap(t_xi);
+            prefetch_tmap(t_xj);
+          } else if (MODE == RBF_MODE_SKETCH) {
+            prefetch_tmap(t_om1);
+            if (I->n2 > 0) prefetch_tmap(t_om2);
+          }
+          last = b;
+        }
         if (points) {
           if (!mbar_wait(bar(B_XI_EMPTY), (items_done & 1) ^ 1, abort_flag)) { ok = false; break; }
-          if (leader) mbar_arrive_expect_tx(bar(B_XI_FULL), 2 * NKC * XI_CHUNK);
-          for (int c = 0; c < NKC; ++c)
-            tma_load_2d_pair(s_xi + c * XI_CHUNK, &tm_xi, lbar(B_XI_FULL), c * KC, it * PAIR_M + (int)rank * BM);
+          if (leader) mbar_arrive_expect_tx(bar(B_XI_FULL), 2 * nkc * XI_CHUNK);
+          for (int c = 0; c < nkc; ++c)
+            tma_load_2d_pair(s_xi + c * XI_CHUNK, t_xi, lbar(B_XI_FULL), c * KC, it * PAIR_M + (int)rank * BM);
         }
-        for (int jt = 0; jt < args.n_jtiles && ok; ++jt) {
+        const int n1 = I->n1, n2 = I->n2, panel = I->panel;
+        for (int jt = 0; jt < njt && ok; ++jt) {
           if (points) {
-            for (int c = 0; c < NKC; ++c) {
+            for (int c = 0; c < nkc; ++c) {
               if (!mbar_wait(bar(XJ_EMPTY + xs), xph ^ 1, abort_flag)) { ok = false; break; }
               if (leader) mbar_arrive_expect_tx(bar(XJ_FULL + xs), 2 * XJ_CHUNK);
-              tma_load_2d_pair(s_xj + xs * XJ_CHUNK, &tm_xj, lbar(XJ_FULL + xs), c * KC,
+              tma_load_2d_pair(s_xj + xs * XJ_CHUNK, t_xj, lbar(XJ_FULL + xs), c * KC,
                                jt * BN + (int)rank * BN_HALF);
               if (++xs == (uint32_t)nsx) { xs = 0; xph ^= 1; }
             }
           } else if (MODE == RBF_MODE_SKETCH) {
             for (int c = 0; c < 2; ++c) {
               if (!mbar_wait(bar(OM_EMPTY + os), oph ^ 1, abort_flag)) { ok = false; break; }
-              if (leader) mbar_arrive_expect_tx(bar(OM_FULL + os), 2 * L.om_stage);
+              if (leader) mbar_arrive_expect_tx(bar(OM_FULL + os), panel * 128);
               // rows of this CTA: [r*n1/2, (r+1)*n1/2) of the first instruction's n1 columns, then the same
               // half of the second instruction's n2 columns
               const uint32_t dst = s_om + os * L.om_stage;
-              const int x = jt * BN + c * KC, y0 = pn * args.panel;
-              tma_load_2d_pair(dst, &tm_om1, lbar(OM_FULL + os), x, y0 + (int)rank * (args.n1 / 2));
-              if (TWO_Y)
-                tma_load_2d_pair(dst + (args.n1 / 2) * 128, &tm_om2, lbar(OM_FULL + os), x,
-                                 y0 + args.n1 + (int)rank * (args.n2 / 2));
+              const int x = jt * BN + c * KC, y0 = pn * panel;
+              tma_load_2d_pair(dst, t_om1, lbar(OM_FULL + os), x, y0 + (int)rank * (n1 / 2));
+              if (n2 > 0)
+                tma_load_2d_pair(dst + (n1 / 2) * 128, t_om2, lbar(OM_FULL + os), x,
+                                 y0 + n1 + (int)rank * (n2 / 2));
               if (++os == (uint32_t)nso) { os = 0; oph ^= 1; }
             }
           }
@@ -239,98 +393,52 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
   } else if (warp == 1) {
     // ------------------------------------------------------------ MMA issuer (leader CTA only)
     // The whole warp runs the schedule converged and waits together; one elected lane issues each block of
-    // MMAs.  Every branch between MMAs is resolved at compile time (DP, TWO_Y): a lone issuing lane that waits
-    // on mbarriers or branches between MMAs cannot keep the tensor pipe fed.
+    // MMAs.  Within a block every branch is resolved at compile time: the feature width and the panel split are
+    // dispatched once per work item to specialised loops, since a lone issuing lane that waits on mbarriers or
+    // branches between MMAs cannot keep the tensor pipe fed.
     if (leader) {
-      constexpr uint32_t idesc_g = idesc_f16(PAIR_M, BN, true);
-      // sketch MMA in fp16 (P in [0, 1], Omega~ Gaussian: both well inside fp16 range, 3 more mantissa bits
-      // than bf16 at the same tensor rate)
-      const uint32_t idesc_y1 = idesc_f16(PAIR_M, args.n1, false);
-      const uint32_t idesc_y2 = idesc_f16(PAIR_M, TWO_Y ? args.n2 : 16, false);
-      const uint32_t y2_boff = (uint32_t)((args.n1 / 2) * 128) >> 4;
-      const uint32_t om_stage16 = (uint32_t)L.om_stage >> 4;
-      uint32_t xs = 0, xph = 0, os = 0, oph = 0, gbi = 0, gph = 0, pph = 0, items_done = 0;
-      bool ok = true;
+      Issuer S;
+      S.tmem_base = tmem_base;
+      S.s_bar = s_bar;
+      S.om_stage16 = (uint32_t)L.om_stage >> 4;
       // Descriptors are affine in the shared address (start address in the low 14 bits, in 16-byte units):
       // build the base descriptors once and add offsets.
-      const uint64_t dxi = sdesc_k_sw128(s_xi), dxj = sdesc_k_sw128(s_xj), dom = sdesc_k_sw128(s_om);
-      auto wait_all = [&](uint32_t b, uint32_t parity) -> bool {
-        return __all_sync(0xffffffffu, mbar_wait(b, parity, abort_flag));
-      };
-
-      auto issue_mma1 = [&]() -> bool {
-        if (!wait_all(bar(B_G_EMPTY0 + gbi), gph ^ 1)) return false;
-        tc_fence_after();
-        const uint32_t d_tmem = tmem_base + gbi * BN;
-#pragma unroll
-        for (int c = 0; c < NKC; ++c) {
-          if (!wait_all(bar(XJ_FULL + xs), xph)) return false;
-          tc_fence_after();
-          if (elect_one()) {
-            const uint64_t bbase = dxj + ((xs * XJ_CHUNK) >> 4);
-#pragma unroll
-            for (int ks = 0; ks < KC / 16; ++ks) {
-              const int o = c * KC + ks * 16;  // K offset of this slice inside the packed row [hi | lo]
-              const uint64_t bdesc = bbase + ((ks * 32) >> 4);
-              if (o < DP) {  // B slice is hi_j: pair with hi_i and lo_i
-                const int oh = o, ol = DP + o;
-                umma_f16_pair(d_tmem, dxi + (((oh / KC) * XI_CHUNK + (oh % KC) * 2) >> 4), bdesc, idesc_g,
-                              o == 0 ? 0u : 1u);
-                umma_f16_pair(d_tmem, dxi + (((ol / KC) * XI_CHUNK + (ol % KC) * 2) >> 4), bdesc, idesc_g, 1u);
-              } else {  // B slice is lo_j: pair with hi_i
-                const int oh = o - DP;
-                umma_f16_pair(d_tmem, dxi + (((oh / KC) * XI_CHUNK + (oh % KC) * 2) >> 4), bdesc, idesc_g, 1u);
-              }
-            }
-            umma_commit_pair(bar(XJ_EMPTY + xs));
-            if (c == NKC - 1) umma_commit_pair(bar(B_G_FULL0 + gbi));
-          }
-          __syncwarp();
-          if (++xs == (uint32_t)nsx) { xs = 0; xph ^= 1; }
-        }
-        if (++gbi == (uint32_t)gb) { gbi = 0; gph ^= 1; }
-        return true;
-      };
-
+      S.dxi = sdesc_k_sw128(s_xi);
+      S.dxj = sdesc_k_sw128(s_xj);
+      S.dom = sdesc_k_sw128(s_om);
+      S.nsx = nsx;
+      S.nso = nso;
+      S.XJ_FULL = XJ_FULL;
+      S.XJ_EMPTY = XJ_EMPTY;
+      S.OM_FULL = OM_FULL;
+      S.OM_EMPTY = OM_EMPTY;
+      S.abort_flag = abort_flag;
+      S.xs = S.xph = S.os = S.oph = S.pph = 0;
+      S.guse0 = S.guse1 = 0;
+      S.gnext = 0;
+      uint32_t items_done = 0;
+      bool ok = true;
       for (int item = cid; item < n_items && ok; item += ncl, ++items_done) {
-        if (!wait_all(bar(B_XI_FULL), items_done & 1)) { ok = false; break; }
+        // every per-instance value in registers before the tile loop (no global reads between MMAs)
+        const TileInst* I = args.inst + find_inst(args.inst, args.count, item);
+        const int nkc = I->nkc, njt = I->n_jtiles, g_bufs = I->g_bufs;
+        const int n1 = I->n1, n2 = I->n2;
+        const bool two = n2 > 0;
+        SketchMma Y;
+        Y.idesc_y1 = idesc_f16(PAIR_M, n1, false);
+        Y.idesc_y2 = idesc_f16(PAIR_M, two ? n2 : 16, false);
+        Y.y2_boff = (uint32_t)((n1 / 2) * 128) >> 4;
+        Y.tmem_p = tmem_base + (uint32_t)I->tmem_p;
+        Y.tmem_y = tmem_base + (uint32_t)I->tmem_y;
+        Y.tmem_y2 = Y.tmem_y + (uint32_t)n1;
+        if (!issuer_wait(S, B_XI_FULL, items_done & 1)) { ok = false; break; }
         tc_fence_after();
         if (MODE == RBF_MODE_SKETCH && items_done > 0) {
-          if (!wait_all(bar(B_Y_EMPTY), (items_done - 1) & 1)) { ok = false; break; }
+          // the previous item's Y (and P) columns may overlap this instance's G buffers: wait for the drain
+          if (!issuer_wait(S, B_Y_EMPTY, (items_done - 1) & 1)) { ok = false; break; }
           tc_fence_after();
         }
-        if (!issue_mma1()) { ok = false; break; }
-        for (int jt = 0; jt < args.n_jtiles; ++jt) {
-          if (jt + 1 < args.n_jtiles && !issue_mma1()) { ok = false; break; }
-          if (MODE == RBF_MODE_SKETCH) {
-#pragma unroll
-            for (int c = 0; c < 2; ++c) {
-              // K chunk c of the sketch MMA reads P half c (j in [64c, 64c + 64))
-              if (!wait_all(bar(B_P_FULL0 + c), pph)) { ok = false; break; }
-              if (!wait_all(bar(OM_FULL + os), oph)) { ok = false; break; }
-              tc_fence_after();
-              if (elect_one()) {
-                const uint64_t bbase = dom + os * om_stage16;
-#pragma unroll
-                for (int ks = 0; ks < KC / 16; ++ks) {
-                  // A = P (fp16 in TMEM, 8 columns per 16-wide K step), B = Omega~ rows of this panel
-                  const uint32_t a_tmem = tmem_base + args.tmem_p + c * 32 + ks * 8;
-                  const uint64_t bdesc = bbase + ((ks * 32) >> 4);
-                  const uint32_t acc = (jt > 0 || c > 0 || ks > 0) ? 1u : 0u;
-                  umma_f16_ts_pair(tmem_base + args.tmem_y, a_tmem, bdesc, idesc_y1, acc);
-                  if (TWO_Y)
-                    umma_f16_ts_pair(tmem_base + args.tmem_y + args.n1, a_tmem, bdesc + y2_boff, idesc_y2, acc);
-                }
-                umma_commit_pair(bar(OM_EMPTY + os));
-                umma_commit_pair(bar(B_P_EMPTY0 + c));
-              }
-              __syncwarp();
-              if (++os == (uint32_t)nso) { os = 0; oph ^= 1; }
-            }
-            if (!ok) break;
-            pph ^= 1;
-          }
-        }
+        ok = two ? issue_item_dp<MODE, true>(S, Y, nkc, njt, g_bufs) : issue_item_dp<MODE, false>(S, Y, nkc, njt, g_bufs);
         if (!ok) break;
         if (elect_one()) {
           umma_commit_pair(bar(B_XI_EMPTY));
@@ -358,21 +466,36 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
     // for the next tile from global memory before the current tile's exp, and parks it here afterwards, so the
     // global latency never sits between a G tile and its P tile.
     float* sjbuf = reinterpret_cast<float*>(smem + L.off_sj) + ew * 2 * EPI_COLS;
-    uint32_t kg = 0, kp = 0, items_done = 0;
+    uint32_t kp = 0, items_done = 0;
+    uint32_t guse0 = 0, guse1 = 0, gnext = 0;  // the same G-buffer sequence as the MMA issuer
     bool ok = true;
     for (int item = cid; item < n_items && ok; item += ncl, ++items_done) {
-      const int it = item % args.n_itiles, pn = item / args.n_itiles;
+      const TileInst* I = args.inst + find_inst(args.inst, args.count, item);
+      const int li = item - I->item_begin;
+      const int it = li % I->n_itiles, pn = li / I->n_itiles;
+      const int njt = I->n_jtiles, g_bufs = I->g_bufs, m = I->m;
+      const float c_row = I->c_row, c_dot = I->c_dot;
+      const float* sj = I->sj;
+      const uint32_t t_p = tmem_base + t_lane + (uint32_t)I->tmem_p + (uint32_t)(qc * (EPI_COLS / 2));
+      const long long ldo = I->ldo;
+      const int n_cols = I->n;
+      const float* const yj_all = I->yj;
       const int i = it * PAIR_M + (int)rank * BM + row;
-      const float a_i = args.c_row * args.si[i];  // si is padded to n_itiles * PAIR_M
-      const float y_i = (i < args.m && args.yi) ? args.yi[i] : 1.0f;
-      sjbuf[lane] = args.sj[qc * EPI_COLS + lane];  // tile 0 of this item
+      float* const out_i = I->out + i;
+      const float a_i = c_row * I->si[i];  // si is padded to n_itiles * PAIR_M
+      const float y_i = (i < m && I->yi) ? I->yi[i] : 1.0f;
+      sjbuf[lane] = sj[qc * EPI_COLS + lane];  // tile 0 of this item
       __syncwarp();
-      for (int jt = 0; jt < args.n_jtiles; ++jt) {
+      for (int jt = 0; jt < njt; ++jt) {
         // sj is padded to n_jtiles * BN
-        const float sj_next = (jt + 1 < args.n_jtiles) ? args.sj[(jt + 1) * BN + qc * EPI_COLS + lane] : 0.0f;
-        const uint32_t b = kg % gb, ph = (kg / gb) & 1;
-        if (!__all_sync(0xffffffffu, mbar_wait(bar(B_G_FULL0 + b), ph, abort_flag))) { ok = false; break; }
+        const float sj_next = (jt + 1 < njt) ? sj[(jt + 1) * BN + qc * EPI_COLS + lane] : 0.0f;
+        const uint32_t b = gnext;
+        const uint32_t guse = b ? guse1 : guse0;
+        if (!__all_sync(0xffffffffu, mbar_wait(bar(B_G_FULL0 + b), guse & 1, abort_flag))) { ok = false; break; }
         tc_fence_after();
+        if (b) ++guse1;
+        else ++guse0;
+        gnext = (g_bufs == 2) ? (b ^ 1u) : 0u;
         float v[EPI_COLS];
         const uint32_t tcol = tmem_base + t_lane + b * BN + qc * EPI_COLS;
         tmem_ld16(tcol, v);
@@ -381,17 +504,16 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
         tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive_remote(lbar(B_G_EMPTY0 + b));
-        ++kg;
 
         const int j0 = jt * BN + qc * EPI_COLS;
         const float4* sj4 = reinterpret_cast<const float4*>(sjbuf + (jt & 1) * EPI_COLS);
 #pragma unroll
         for (int c = 0; c < EPI_COLS / 4; ++c) {
           const float4 s4 = sj4[c];
-          v[4 * c + 0] = fast_exp2(fminf(fmaf(args.c_dot, v[4 * c + 0], fmaf(args.c_row, s4.x, a_i)), 0.0f));
-          v[4 * c + 1] = fast_exp2(fminf(fmaf(args.c_dot, v[4 * c + 1], fmaf(args.c_row, s4.y, a_i)), 0.0f));
-          v[4 * c + 2] = fast_exp2(fminf(fmaf(args.c_dot, v[4 * c + 2], fmaf(args.c_row, s4.z, a_i)), 0.0f));
-          v[4 * c + 3] = fast_exp2(fminf(fmaf(args.c_dot, v[4 * c + 3], fmaf(args.c_row, s4.w, a_i)), 0.0f));
+          v[4 * c + 0] = fast_exp2(fminf(fmaf(c_dot, v[4 * c + 0], fmaf(c_row, s4.x, a_i)), 0.0f));
+          v[4 * c + 1] = fast_exp2(fminf(fmaf(c_dot, v[4 * c + 1], fmaf(c_row, s4.y, a_i)), 0.0f));
+          v[4 * c + 2] = fast_exp2(fminf(fmaf(c_dot, v[4 * c + 2], fmaf(c_row, s4.z, a_i)), 0.0f));
+          v[4 * c + 3] = fast_exp2(fminf(fmaf(c_dot, v[4 * c + 3], fmaf(c_row, s4.w, a_i)), 0.0f));
         }
 
         sjbuf[((jt + 1) & 1) * EPI_COLS + lane] = sj_next;
@@ -406,21 +528,20 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
           }
           tc_fence_after();
           // P row = this thread's row; j in [32qc, 32qc + 32) -> TMEM columns tmem_p + 16qc .. + 15
-          tmem_st16(tmem_base + t_lane + args.tmem_p + qc * (EPI_COLS / 2), pk);
+          tmem_st16(t_p, pk);
           tmem_wait_st();
           tc_fence_before();
           __syncwarp();
           if (lane == 0) mbar_arrive_remote(lbar(B_P_FULL0 + h));
           ++kp;
         } else {
-          if (i < args.m) {
-            float* out = args.out + i;
+          if (i < m) {
 #pragma unroll
             for (int c = 0; c < EPI_COLS; ++c) {
               const int j = j0 + c;
-              if (j < args.n) {
-                const float yj = args.yj ? __ldg(args.yj + j) : 1.0f;
-                out[(size_t)j * args.ldo] = y_i * yj * v[c];
+              if (j < n_cols) {
+                const float yj = yj_all ? __ldg(yj_all + j) : 1.0f;
+                out_i[(size_t)j * ldo] = y_i * yj * v[c];
               }
             }
           }
@@ -430,16 +551,17 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
       if (MODE == RBF_MODE_SKETCH) {
         if (!__all_sync(0xffffffffu, mbar_wait(bar(B_Y_FULL), items_done & 1, abort_flag))) { ok = false; break; }
         tc_fence_after();
-        const int quarter = args.panel / 4;  // panel is a multiple of 16
+        const int panel = I->panel, l = I->l;
+        const int quarter = panel / 4;  // panel is a multiple of 16
         for (int cc = 0; cc < quarter; cc += 4) {
           float yv[4];
-          tmem_ld4(tmem_base + t_lane + args.tmem_y + qc * quarter + cc, yv);
+          tmem_ld4(tmem_base + t_lane + I->tmem_y + qc * quarter + cc, yv);
           tmem_wait_ld();
-          if (i < args.m) {
+          if (i < m) {
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
-              const int col = pn * args.panel + qc * quarter + cc + e;
-              if (col < args.l) args.out[i + (size_t)col * args.ldo] = y_i * yv[e];
+              const int col = pn * panel + qc * quarter + cc + e;
+              if (col < l) out_i[(size_t)col * ldo] = y_i * yv[e];
             }
           }
         }
@@ -530,13 +652,9 @@ bool make_tmap(CUtensorMap* tm, const void* base, uint64_t inner, uint64_t outer
   return r == CUDA_SUCCESS;
 }
 
-template <int DP>
-cudaError_t launch_tile_kernel(int mode, bool two_y, int max_clusters, int n_items, size_t smem, cudaStream_t st,
-                               const CUtensorMap& tm_xi, const CUtensorMap& tm_xj, const CUtensorMap& tm_om1,
-                               const CUtensorMap& tm_om2, const TileArgs& a) {
-  auto k = (mode == RBF_MODE_SKETCH) ? (two_y ? rbf_tile_kernel<RBF_MODE_SKETCH, DP, true>
-                                              : rbf_tile_kernel<RBF_MODE_SKETCH, DP, false>)
-                                     : rbf_tile_kernel<RBF_MODE_KBLOCK, DP, false>;
+template <int MODE>
+cudaError_t launch_kernel(const LaunchArgs& a, size_t smem, int max_clusters, cudaStream_t st) {
+  auto k = rbf_tile_kernel<MODE>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   cudaLaunchAttribute attr[1];
@@ -557,9 +675,9 @@ cudaError_t launch_tile_kernel(int mode, bool two_y, int max_clusters, int n_ite
   if (e != cudaSuccess) return e;
   if (resident < 1) return cudaErrorInvalidConfiguration;
   int clusters = resident < max_clusters ? resident : max_clusters;
-  if (clusters > n_items) clusters = n_items;
+  if (clusters > a.n_items) clusters = a.n_items;
   cfg.gridDim = dim3((unsigned)(2 * clusters));
-  return cudaLaunchKernelEx(&cfg, k, tm_xi, tm_xj, tm_om1, tm_om2, a);
+  return cudaLaunchKernelEx(&cfg, k, a);
 }
 
 }  // namespace
@@ -605,91 +723,153 @@ int pack_sketch(db200_context* ctx, const float* Omega, int ldo, const float* yj
   return DB200_OK;
 }
 
-int launch_rbf_tiles(db200_context* ctx, int mode, const PackedPoints& pi, const PackedPoints& pj, const float* yi,
-                     const float* yj, const void* op, const SketchPlan& plan, int l, float gamma, float* out,
-                     int ldo) {
-  if (pi.dp != pj.dp || pi.dp > 128) return fail(ctx, DB200_ERR_UNSUPPORTED, "rbf tiles: feature count > 128");
-  if (pi.npad % PAIR_M || pj.npad % BN) return fail(ctx, DB200_ERR_INVALID, "rbf tiles: unpadded operands");
-  if (mode == RBF_MODE_SKETCH && (plan.panel % 16 || plan.panel > 320 || plan.panel < 16 ||
-                                  plan.panel + 64 + 128 * plan.g_bufs > TMEM_COLS))
-    return fail(ctx, DB200_ERR_INVALID, "rbf tiles: bad sketch panel");
-  CUtensorMap tm_xi, tm_xj, tm_om1, tm_om2;
-  const int kp = 2 * pi.dp;
-  if (!make_tmap(&tm_xi, pi.xp, kp, pi.npad, kp, BM) || !make_tmap(&tm_xj, pj.xp, kp, pj.npad, kp, BN_HALF))
-    return fail(ctx, DB200_ERR_CUDA, "cuTensorMapEncodeTiled failed for the point operands");
-  TileArgs a;
-  if (mode == RBF_MODE_SKETCH) {
-    a.n_panels = plan.n_panels;
-    a.panel = plan.panel;
-    // one sketch MMA of N = panel columns, or two of about half each (multiples of 16, each <= 256); each CTA of
-    // the pair holds half of every instruction's B rows, loaded as one TMA box per instruction
-    a.n1 = plan.panel > 256 ? (plan.panel / 32) * 16 : plan.panel;
-    a.n2 = plan.panel - a.n1;
-    if (!make_tmap(&tm_om1, op, pj.npad, plan.lrows, pj.npad, a.n1 / 2, CU_TENSOR_MAP_DATA_TYPE_FLOAT16) ||
-        (a.n2 > 0 &&
-         !make_tmap(&tm_om2, op, pj.npad, plan.lrows, pj.npad, a.n2 / 2, CU_TENSOR_MAP_DATA_TYPE_FLOAT16)))
-      return fail(ctx, DB200_ERR_CUDA, "cuTensorMapEncodeTiled failed for the sketch operand");
-    if (a.n2 == 0) tm_om2 = tm_om1;  // unused
-    a.g_bufs = plan.g_bufs;
-    a.tmem_p = 128 * plan.g_bufs;
-    a.tmem_y = a.tmem_p + 64;
-    a.nso = MAX_NSO;
-  } else {
-    tm_om1 = tm_om2 = tm_xj;  // unused
-    a.n_panels = 1;
-    a.panel = 16;
-    a.n1 = 16;
-    a.n2 = 0;
-    a.g_bufs = 2;
-    a.tmem_p = 256;
-    a.tmem_y = 320;
-    a.nso = 0;
+size_t tile_table_bytes(int count) { return (size_t)count * sizeof(TileInst); }
+
+int prepare_rbf_tiles(db200_context* ctx, int mode, const TileJob* jobs, int count, void* table_storage,
+                      size_t table_capacity, TilePlan* plan) {
+  if (count < 1 || !jobs || !plan) return fail(ctx, DB200_ERR_INVALID, "rbf tiles: empty job list");
+  std::vector<TileInst> host((size_t)count);
+  int items = 0, nkc_max = 1, panel_max = 16;
+  for (int b = 0; b < count; ++b) {
+    const TileJob& J = jobs[b];
+    const PackedPoints &pi = J.pi, &pj = J.pj;
+    if (pi.dp != pj.dp || pi.dp > 128 || pi.dp % 32)
+      return fail(ctx, DB200_ERR_UNSUPPORTED, "rbf tiles: padded feature count not in {32, 64, 96, 128}");
+    if (pi.npad % PAIR_M || pj.npad % BN) return fail(ctx, DB200_ERR_INVALID, "rbf tiles: unpadded operands");
+    const SketchPlan& P = J.plan;
+    if (mode == RBF_MODE_SKETCH && (P.panel % 16 || P.panel > 320 || P.panel < 16 || P.n_panels < 1 ||
+                                    (P.g_bufs != 1 && P.g_bufs != 2) || P.panel + 64 + 128 * P.g_bufs > TMEM_COLS ||
+                                    P.n_panels * P.panel < J.l || P.lrows < P.n_panels * P.panel))
+      return fail(ctx, DB200_ERR_INVALID, "rbf tiles: bad sketch panel plan");
+    TileInst& I = host[(size_t)b];
+    std::memset(&I, 0, sizeof(I));
+    const int kp = 2 * pi.dp;
+    if (!make_tmap(&I.tm_xi, pi.xp, kp, pi.npad, kp, BM) || !make_tmap(&I.tm_xj, pj.xp, kp, pj.npad, kp, BN_HALF))
+      return fail(ctx, DB200_ERR_CUDA, "cuTensorMapEncodeTiled failed for the point operands");
+    if (mode == RBF_MODE_SKETCH) {
+      I.n_panels = P.n_panels;
+      I.panel = P.panel;
+      // one sketch MMA of N = panel columns, or two of about half each (multiples of 16, each <= 256); each CTA
+      // of the pair holds half of every instruction's B rows, loaded as one TMA box per instruction
+      I.n1 = P.panel > 256 ? (P.panel / 32) * 16 : P.panel;
+      I.n2 = P.panel - I.n1;
+      if (!make_tmap(&I.tm_om1, J.op, pj.npad, P.lrows, pj.npad, I.n1 / 2, CU_TENSOR_MAP_DATA_TYPE_FLOAT16) ||
+          (I.n2 > 0 &&
+           !make_tmap(&I.tm_om2, J.op, pj.npad, P.lrows, pj.npad, I.n2 / 2, CU_TENSOR_MAP_DATA_TYPE_FLOAT16)))
+        return fail(ctx, DB200_ERR_CUDA, "cuTensorMapEncodeTiled failed for the sketch operand");
+      if (I.n2 == 0) I.tm_om2 = I.tm_om1;  // unused
+      I.g_bufs = P.g_bufs;
+      I.tmem_p = 128 * P.g_bufs;
+      I.tmem_y = I.tmem_p + 64;
+    } else {
+      I.tm_om1 = I.tm_om2 = I.tm_xj;  // unused
+      I.n_panels = 1;
+      I.panel = 16;
+      I.n1 = 16;
+      I.n2 = 0;
+      I.g_bufs = 2;
+      I.tmem_p = 256;
+      I.tmem_y = 320;
+    }
+    I.m = pi.n;
+    I.n = pj.n;
+    I.n_itiles = pi.npad / PAIR_M;
+    I.n_jtiles = pj.npad / BN;
+    I.l = J.l;
+    I.nkc = kp / KC;
+    I.c_row = -J.gamma * LOG2E;
+    I.c_dot = 2.0f * J.gamma * LOG2E;
+    I.si = pi.norms;
+    I.sj = pj.norms;
+    I.yi = J.yi;
+    I.yj = J.yj;
+    I.out = J.out;
+    I.ldo = J.ldo;
+    I.item_begin = items;
+    items += I.n_itiles * I.n_panels;
+    nkc_max = std::max(nkc_max, I.nkc);
+    panel_max = std::max(panel_max, I.panel);
   }
-  a.m = pi.n;
-  a.n = pj.n;
-  a.n_itiles = pi.npad / PAIR_M;
-  a.n_jtiles = pj.npad / BN;
-  a.l = l;
-  a.c_row = -gamma * LOG2E;
-  a.c_dot = 2.0f * gamma * LOG2E;
-  a.si = pi.norms;
-  a.sj = pj.norms;
-  a.yi = yi;
-  a.yj = yj;
-  a.out = out;
-  a.ldo = ldo;
-  a.status = ctx->d_status;
-  // the Xj ring takes whatever shared memory is left
-  {
-    const SmemLayout L0 = make_layout(pi.dp, a.panel, 0, a.nso);
+  TilePlan T;
+  T.mode = mode;
+  T.count = count;
+  T.n_items = items;
+  T.nkc_max = nkc_max;
+  T.panel_max = panel_max;
+  T.nso = (mode == RBF_MODE_SKETCH) ? MAX_NSO : 0;
+  {  // the Xj ring takes whatever shared memory is left
+    const SmemLayout L0 = make_layout(nkc_max, panel_max, 0, T.nso);
     const long long left = (long long)SMEM_LIMIT - 1024 - (long long)L0.total;
     int nsx = (int)(left / XJ_CHUNK);
     if (nsx > MAX_NSX) nsx = MAX_NSX;
     if (nsx < 2) return fail(ctx, DB200_ERR_UNSUPPORTED, "rbf tiles: shared memory plan does not fit");
-    a.nsx = nsx;
+    T.nsx = nsx;
   }
-  const SmemLayout L = make_layout(pi.dp, a.panel, a.nsx, a.nso);
-  const size_t smem = L.total + 1024;
-  const int n_items = a.n_itiles * a.n_panels;
-  const int max_clusters = ctx->num_sms / 2;
+  T.smem = make_layout(nkc_max, panel_max, T.nsx, T.nso).total + 1024;
+  const size_t bytes = tile_table_bytes(count);
+  void* d = table_storage;
+  if (d) {
+    if (table_capacity < bytes) return fail(ctx, DB200_ERR_TOO_LARGE, "rbf tiles: instance table storage too small");
+  } else {
+    if (bytes > ctx->tile_table_size) {
+      DB200_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+      if (ctx->tile_table) cudaFree(ctx->tile_table);
+      ctx->tile_table = nullptr;
+      ctx->tile_table_size = 0;
+      DB200_CUDA(ctx, cudaMalloc(&ctx->tile_table, bytes));
+      ctx->tile_table_size = bytes;
+    }
+    d = ctx->tile_table;
+  }
+  // pageable source: the copy is staged before the call returns, so `host` may go out of scope
+  DB200_CUDA(ctx, cudaMemcpyAsync(d, host.data(), bytes, cudaMemcpyHostToDevice, ctx->stream));
+  T.table = d;
+  static_assert(sizeof(T.tm1) == 4 * sizeof(CUtensorMap), "tensor map copy");
+  std::memcpy(T.tm1, &host[0].tm_xi, sizeof(T.tm1));
+  *plan = T;
+  return DB200_OK;
+}
+
+int launch_rbf_plan(db200_context* ctx, const TilePlan& T) {
+  LaunchArgs a;
+  std::memcpy(a.tm1, T.tm1, sizeof(a.tm1));
+  a.inst = static_cast<const TileInst*>(T.table);
+  a.count = T.count;
+  a.n_items = T.n_items;
+  a.nsx = T.nsx;
+  a.nso = T.nso;
+  a.nkc_max = T.nkc_max;
+  a.panel_max = T.panel_max;
+  a.status = ctx->d_status;
   cudaEvent_t e0 = nullptr;
   prof_begin(ctx, &e0);
-  const bool two_y = (mode == RBF_MODE_SKETCH) && a.n2 > 0;
-  cudaError_t err = cudaSuccess;
-#define DB200_TILE_LAUNCH(DPV)                                                                                    \
-  launch_tile_kernel<DPV>(mode, two_y, max_clusters, n_items, smem, ctx->stream, tm_xi, tm_xj, tm_om1, tm_om2, a)
-  switch (pi.dp) {
-    case 32: err = DB200_TILE_LAUNCH(32); break;
-    case 64: err = DB200_TILE_LAUNCH(64); break;
-    case 96: err = DB200_TILE_LAUNCH(96); break;
-    case 128: err = DB200_TILE_LAUNCH(128); break;
-    default: return fail(ctx, DB200_ERR_UNSUPPORTED, "rbf tiles: padded feature count not in {32, 64, 96, 128}");
-  }
-#undef DB200_TILE_LAUNCH
+  const int max_clusters = ctx->num_sms / 2;
+  cudaError_t err = (T.mode == RBF_MODE_SKETCH) ? launch_kernel<RBF_MODE_SKETCH>(a, T.smem, max_clusters, ctx->stream)
+                                                : launch_kernel<RBF_MODE_KBLOCK>(a, T.smem, max_clusters, ctx->stream);
   DB200_CUDA(ctx, err);
   prof_end(ctx, e0);
   count_launch(ctx);
   return DB200_OK;
+}
+
+int launch_rbf_tiles(db200_context* ctx, int mode, const PackedPoints& pi, const PackedPoints& pj, const float* yi,
+                     const float* yj, const void* op, const SketchPlan& plan, int l, float gamma, float* out,
+                     int ldo, void* table_storage, size_t table_capacity) {
+  TileJob J;
+  J.pi = pi;
+  J.pj = pj;
+  J.yi = yi;
+  J.yj = yj;
+  J.op = op;
+  J.plan = plan;
+  J.l = l;
+  J.gamma = gamma;
+  J.out = out;
+  J.ldo = ldo;
+  TilePlan T;
+  int st = prepare_rbf_tiles(ctx, mode, &J, 1, table_storage, table_capacity, &T);
+  if (st) return st;
+  return launch_rbf_plan(ctx, T);
 }
 
 }  // namespace db200
