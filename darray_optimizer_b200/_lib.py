@@ -47,6 +47,31 @@ class LandmarkReport(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class SketchJob(ctypes.Structure):
+    _fields_ = [("m", ctypes.c_int), ("n", ctypes.c_int), ("d", ctypes.c_int), ("l", ctypes.c_int),
+                ("Xi", ctypes.c_void_p), ("ldxi", ctypes.c_int), ("Xj", ctypes.c_void_p), ("ldxj", ctypes.c_int),
+                ("yi", ctypes.c_void_p), ("yj", ctypes.c_void_p), ("Omega", ctypes.c_void_p), ("ldo", ctypes.c_int),
+                ("Y", ctypes.c_void_p), ("ldy", ctypes.c_int), ("gamma", ctypes.c_float),
+                ("n_panels", ctypes.c_int), ("panel", ctypes.c_int), ("g_bufs", ctypes.c_int)]
+
+
+class SvmInstance(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int), ("d", ctypes.c_int), ("l", ctypes.c_int), ("X", ctypes.c_void_p),
+                ("ldx", ctypes.c_int), ("y", ctypes.c_void_p), ("gamma", ctypes.c_float), ("C", ctypes.c_double),
+                ("Omega", ctypes.c_void_p), ("ldo", ctypes.c_int), ("Z", ctypes.c_void_p), ("ldz", ctypes.c_int),
+                ("a", ctypes.c_void_p), ("n_panels", ctypes.c_int), ("panel", ctypes.c_int),
+                ("g_bufs", ctypes.c_int)]
+
+
+class BatchReport(ctypes.Structure):
+    _fields_ = [("ms_pack", ctypes.c_double), ("ms_sketch", ctypes.c_double), ("ms_orth", ctypes.c_double),
+                ("ms_core", ctypes.c_double), ("ms_barrier", ctypes.c_double), ("ms_total", ctypes.c_double),
+                ("kernel_passes", ctypes.c_int), ("graph_replays", ctypes.c_int), ("workers", ctypes.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 _u64 = ctypes.c_uint64
 _fp = ctypes.POINTER(ctypes.c_float)
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -102,6 +127,11 @@ SIGNATURES = {
                                      ctypes.POINTER(_c_double)]),
     "db200_rbf_sketch_noalloc": (_c_int, [_vp, _c_int, _c_int, _c_int, _c_int, _vp, _c_int, _vp, _c_int, _c_int, _vp,
                                           _vp, _vp, _c_int, _vp, _c_int, _c_float]),
+    # batched instances
+    "db200_rbf_sketch_batched": (_c_int, [_vp, _c_int, ctypes.POINTER(SketchJob)]),
+    "db200_svm_solve_batched": (_c_int, [_vp, _c_int, ctypes.POINTER(SvmInstance), _c_int,
+                                         ctypes.POINTER(BarrierParams), _c_int, _c_int, ctypes.POINTER(SvmReport),
+                                         ctypes.POINTER(BatchReport)]),
     # learned landmarks
     "db200_knn_distance": (_c_int, [_vp, _c_int, _c_int, _vp, _c_int, _c_int, _vp, _c_int, _vp]),
     "db200_leverage_features": (_c_int, [_vp, _c_int, _c_int, _vp, _c_int, _vp, _vp]),
@@ -301,6 +331,22 @@ class Context:
     def rbf_block(self, m, n, d, Xi, ldxi, Xj, ldxj, layout, yi, yj, K, ldk, gamma):
         return self.check(self.lib.db200_rbf_block(self.h, m, n, d, Xi, ldxi, Xj, ldxj, layout, yi, yj, K, ldk,
                                                    gamma))
+
+    # ------------------------------------------------------------------ batched instances
+    def rbf_sketch_batched(self, jobs):
+        arr = (SketchJob * len(jobs))(*jobs)
+        return self.check(self.lib.db200_rbf_sketch_batched(self.h, len(jobs), arr))
+
+    def svm_solve_batched(self, instances, q=1, params=None, use_graph=True, workers=8):
+        arr = (SvmInstance * len(instances))(*instances)
+        reps = (SvmReport * len(instances))()
+        brep = BatchReport()
+        p = params or self.barrier_params()
+        st = self.lib.db200_svm_solve_batched(self.h, len(instances), arr, q, ctypes.byref(p), int(use_graph),
+                                              workers, reps, ctypes.byref(brep))
+        if st not in (0, -4):
+            self.check(st)
+        return list(reps), brep
 
     # ------------------------------------------------------------------ learned landmarks
     def knn_distance(self, n, d, X, ldx, s, ref_idx, k, out):

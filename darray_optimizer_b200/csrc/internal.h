@@ -116,6 +116,7 @@ struct TileJob {
 // A prepared launch: the instance table is on the device; launch_rbf_plan only launches (graph-capturable).
 struct TilePlan {
   int mode = 0, count = 0, n_items = 0, nsx = 0, nso = 0, nkc_max = 0, panel_max = 0;
+  int clusters = 0;  // persistent grid: CTA pairs resident at once (at most one per item)
   size_t smem = 0;
   const void* table = nullptr;
   alignas(64) unsigned char tm1[4 * 128];  // instance 0's tensor maps (kernel parameters of one-instance launches)
@@ -127,6 +128,15 @@ int prepare_rbf_tiles(db200_context* ctx, int mode, const TileJob* jobs, int cou
                       size_t table_capacity, TilePlan* plan);
 // One persistent launch over every work item of the prepared jobs.
 int launch_rbf_plan(db200_context* ctx, const TilePlan& plan);
+
+// ------------------------------------------------------------------ SVM pipeline pieces (svm.cpp)
+// Orthonormalise Y (n x l, FP64) in place by CholeskyQR2 (shifted CholeskyQR3 when the Gram is not positive
+// definite); R (l x l) optional.
+int cholqr2_impl(db200_context* ctx, int n, int l, double* Y, int ldy, double* Rout, int ldr);
+// Nystrom core: C = Q^T Yk (Yk = K Q), symmetrised; R^T R = C + nu I (shifted Cholesky); Z = Q R^T.
+template <typename TY>
+int nystrom_core(db200_context* ctx, int n, int l, const double* Q, const TY* Yk, double* Cm, double* R, int* d_pair,
+                 double* d_scalar, double* Z, int ldz, double* nu_out);
 
 // Launch the fused tile kernel for one problem.  For RBF_MODE_SKETCH, `op` is the packed Omega^T and `out` is Y
 // (m x l, column major, leading dimension ldo); for RBF_MODE_KBLOCK, `out` is the kernel block K (m x n, column

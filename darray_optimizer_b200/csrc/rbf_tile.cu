@@ -652,32 +652,45 @@ bool make_tmap(CUtensorMap* tm, const void* base, uint64_t inner, uint64_t outer
   return r == CUDA_SUCCESS;
 }
 
-template <int MODE>
-cudaError_t launch_kernel(const LaunchArgs& a, size_t smem, int max_clusters, cudaStream_t st) {
-  auto k = rbf_tile_kernel<MODE>;
-  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  cudaLaunchAttribute attr[1];
+cudaLaunchConfig_t launch_config(cudaLaunchAttribute* attr, int clusters, size_t smem, cudaStream_t st) {
   attr[0].id = cudaLaunchAttributeClusterDimension;
   attr[0].val.clusterDim.x = 2;
   attr[0].val.clusterDim.y = 1;
   attr[0].val.clusterDim.z = 1;
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)(2 * max_clusters));
+  cfg.gridDim = dim3((unsigned)(2 * clusters));
   cfg.blockDim = dim3(NUM_THREADS);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  // persistent: as many pairs as can be resident at once, no more than there are items
+  return cfg;
+}
+
+// Persistent grid size: as many CTA pairs as can be resident at once, no more than there are items.  Not
+// stream-ordered (so launches can be captured in a CUDA graph afterwards).
+template <int MODE>
+cudaError_t plan_clusters(size_t smem, int max_clusters, int n_items, int* clusters) {
+  auto k = rbf_tile_kernel<MODE>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  cudaLaunchAttribute attr[1];
+  cudaLaunchConfig_t cfg = launch_config(attr, max_clusters, smem, nullptr);
   int resident = 0;
   e = cudaOccupancyMaxActiveClusters(&resident, k, &cfg);
   if (e != cudaSuccess) return e;
   if (resident < 1) return cudaErrorInvalidConfiguration;
-  int clusters = resident < max_clusters ? resident : max_clusters;
-  if (clusters > a.n_items) clusters = a.n_items;
-  cfg.gridDim = dim3((unsigned)(2 * clusters));
-  return cudaLaunchKernelEx(&cfg, k, a);
+  int c = resident < max_clusters ? resident : max_clusters;
+  if (c > n_items) c = n_items;
+  *clusters = c;
+  return cudaSuccess;
+}
+
+template <int MODE>
+cudaError_t launch_kernel(const LaunchArgs& a, size_t smem, int clusters, cudaStream_t st) {
+  cudaLaunchAttribute attr[1];
+  cudaLaunchConfig_t cfg = launch_config(attr, clusters, smem, st);
+  return cudaLaunchKernelEx(&cfg, rbf_tile_kernel<MODE>, a);
 }
 
 }  // namespace
@@ -806,6 +819,12 @@ int prepare_rbf_tiles(db200_context* ctx, int mode, const TileJob* jobs, int cou
     T.nsx = nsx;
   }
   T.smem = make_layout(nkc_max, panel_max, T.nsx, T.nso).total + 1024;
+  {
+    const int max_clusters = ctx->num_sms / 2;
+    cudaError_t e = (mode == RBF_MODE_SKETCH) ? plan_clusters<RBF_MODE_SKETCH>(T.smem, max_clusters, items, &T.clusters)
+                                              : plan_clusters<RBF_MODE_KBLOCK>(T.smem, max_clusters, items, &T.clusters);
+    DB200_CUDA(ctx, e);
+  }
   const size_t bytes = tile_table_bytes(count);
   void* d = table_storage;
   if (d) {
@@ -843,9 +862,8 @@ int launch_rbf_plan(db200_context* ctx, const TilePlan& T) {
   a.status = ctx->d_status;
   cudaEvent_t e0 = nullptr;
   prof_begin(ctx, &e0);
-  const int max_clusters = ctx->num_sms / 2;
-  cudaError_t err = (T.mode == RBF_MODE_SKETCH) ? launch_kernel<RBF_MODE_SKETCH>(a, T.smem, max_clusters, ctx->stream)
-                                                : launch_kernel<RBF_MODE_KBLOCK>(a, T.smem, max_clusters, ctx->stream);
+  cudaError_t err = (T.mode == RBF_MODE_SKETCH) ? launch_kernel<RBF_MODE_SKETCH>(a, T.smem, T.clusters, ctx->stream)
+                                                : launch_kernel<RBF_MODE_KBLOCK>(a, T.smem, T.clusters, ctx->stream);
   DB200_CUDA(ctx, err);
   prof_end(ctx, e0);
   count_launch(ctx);

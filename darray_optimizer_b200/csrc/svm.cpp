@@ -367,6 +367,41 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
 }
 
 // ---------------------------------------------------------------------------------------------- low rank
+template <typename TY>
+int nystrom_core(db200_context* ctx, int n, int l, const double* Q, const TY* Yk, double* Cm, double* R, int* d_pair,
+                 double* d_scalar, double* Z, int ldz, double* nu_out) {
+  // C = Q^T (K Q), symmetrised; R^T R = C + nu I with nu = 1e-7 trace(C)/l, x10 until positive definite
+  int st = gram<double, TY>(ctx, n, l, l, Q, n, Yk, n, nullptr, 1.0, 0.0, Cm, l, false);
+  if (st) return st;
+  if ((st = symmetrize(ctx, Cm, l, l, 0.0))) return st;
+  if ((st = trace(ctx, Cm, l, l, d_scalar))) return st;
+  double tr = 0;
+  DB200_CUDA(ctx, cudaMemcpyAsync(&tr, d_scalar, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  DB200_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  const size_t ll = (size_t)l * l;
+  double nu = 1e-7 * std::max(tr, 1e-300) / l;
+  bool ok = false;
+  for (int tries = 0; tries < 12 && !ok; ++tries) {
+    DB200_CUDA(ctx, cudaMemcpyAsync(R, Cm, sizeof(double) * ll, cudaMemcpyDeviceToDevice, ctx->stream));
+    if ((st = symmetrize(ctx, R, l, l, nu))) return st;
+    DB200_CUDA(ctx, cudaMemsetAsync(d_pair, 0, 2 * sizeof(int), ctx->stream));
+    if ((st = potrf_upper(ctx, R, l, l, d_pair, d_pair + 1))) return st;
+    int pst = 0, bad = 0;
+    if ((st = read_status(ctx, d_pair, &pst, &bad))) return st;
+    if (pst == 0) ok = true;
+    else nu *= 10.0;
+  }
+  if (!ok) return fail(ctx, DB200_ERR_NOT_SPD, "lowrank: Q^T K Q + nu I not positive definite after 12 shifts");
+  // Z = Q R^T
+  if ((st = gemm_tall<double, double>(ctx, n, l, l, Q, n, R, l, true, 0.0, Z, ldz))) return st;
+  if (nu_out) *nu_out = nu;
+  return DB200_OK;
+}
+template int nystrom_core<float>(db200_context*, int, int, const double*, const float*, double*, double*, int*,
+                                 double*, double*, int, double*);
+template int nystrom_core<double>(db200_context*, int, int, const double*, const double*, double*, double*, int*,
+                                  double*, double*, int, double*);
+
 int lowrank_impl(db200_context* ctx, int n, int d, int l, int q, const float* X, int ldx, const float* y,
                  const float* Omega, int ldo, float gamma, int precision, double* Z, int ldz, db200_svm_report* rep) {
   if (l > n) return fail(ctx, DB200_ERR_INVALID, "lowrank: l > n");
@@ -426,32 +461,10 @@ int lowrank_impl(db200_context* ctx, int n, int d, int l, int q, const float* X,
   }
   if ((st = fp64 ? sketch_f64(Q, n) : sketch_f32(Qf, n))) return st;  // Y = K Q
   EventTimer tcore(ctx->stream);
-  // C = Q^T (K Q), symmetrised; R^T R = C + nu I with nu = 1e-7 trace(C)/l, x10 until positive definite
-  if (fp64) {
-    if ((st = gram<double, double>(ctx, n, l, l, Q, n, Y64, n, nullptr, 1.0, 0.0, Cm, l, false))) return st;
-  } else {
-    if ((st = gram<double, float>(ctx, n, l, l, Q, n, Y32, n, nullptr, 1.0, 0.0, Cm, l, false))) return st;
-  }
-  if ((st = symmetrize(ctx, Cm, l, l, 0.0))) return st;
-  if ((st = trace(ctx, Cm, l, l, d_scalar))) return st;
-  double tr = 0;
-  DB200_CUDA(ctx, cudaMemcpyAsync(&tr, d_scalar, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-  DB200_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  double nu = 1e-7 * std::max(tr, 1e-300) / l;
-  bool ok = false;
-  for (int tries = 0; tries < 12 && !ok; ++tries) {
-    DB200_CUDA(ctx, cudaMemcpyAsync(R, Cm, sizeof(double) * ll, cudaMemcpyDeviceToDevice, ctx->stream));
-    if ((st = symmetrize(ctx, R, l, l, nu))) return st;
-    DB200_CUDA(ctx, cudaMemsetAsync(d_pair, 0, 2 * sizeof(int), ctx->stream));
-    if ((st = potrf_upper(ctx, R, l, l, d_pair, d_pair + 1))) return st;
-    int pst = 0, bad = 0;
-    if ((st = read_status(ctx, d_pair, &pst, &bad))) return st;
-    if (pst == 0) ok = true;
-    else nu *= 10.0;
-  }
-  if (!ok) return fail(ctx, DB200_ERR_NOT_SPD, "lowrank: Q^T K Q + nu I not positive definite after 12 shifts");
-  // Z = Q R^T
-  if ((st = gemm_tall<double, double>(ctx, n, l, l, Q, n, R, l, true, 0.0, Z, ldz))) return st;
+  double nu = 0;
+  st = fp64 ? nystrom_core<double>(ctx, n, l, Q, Y64, Cm, R, d_pair, d_scalar, Z, ldz, &nu)
+            : nystrom_core<float>(ctx, n, l, Q, Y32, Cm, R, d_pair, d_scalar, Z, ldz, &nu);
+  if (st) return st;
   ms_core = tcore.stop_ms();
   if (rep) {
     rep->nu = nu;

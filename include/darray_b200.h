@@ -292,6 +292,67 @@ DB200_API int db200_rbf_sketch_noalloc(void* stream, int m, int n, int d, int l,
                                        const float* Omega, int ldo, float* Y, int ldy, float gamma);
 
 /* ------------------------------------------------------------------------------------------------------------
+ * Batched instances: many independent problems of uneven n, d, l, gamma and C (hyperparameter grids, one-vs-rest
+ * classes) in one persistent launch of the tile engine.  The reference runs one problem per process
+ * (tests/testsvm.cpp:34-329); these entry points have no counterpart there.
+ * ------------------------------------------------------------------------------------------------------------ */
+
+/* One sketch problem Y (m x l) = diag(yi) K(Xi, Xj) diag(yj) Omega (n x l), as db200_rbf_sketch, plus an optional
+ * tile plan: n_panels sketch panels of `panel` columns (a multiple of 16, <= 320) with g_bufs (1 or 2) distance
+ * buffers in tensor memory, panel + 64 + 128 g_bufs <= 512; n_panels = 0 selects the default plan. */
+typedef struct {
+  int m, n, d, l;
+  const float* Xi;
+  int ldxi;
+  const float* Xj;
+  int ldxj;
+  const float* yi;
+  const float* yj;
+  const float* Omega;
+  int ldo;
+  float* Y;
+  int ldy;
+  float gamma;
+  int n_panels, panel, g_bufs;
+} db200_sketch_job;
+
+/* Every job's K.Omega in one persistent launch (work items of all jobs interleaved over the CTA pairs).  Device
+ * pointers, point-major points.  Stream-ordered. */
+DB200_API int db200_rbf_sketch_batched(db200_context* ctx, int count, const db200_sketch_job* jobs);
+
+/* One SVM instance of db200_svm_solve_batched (device pointers). */
+typedef struct {
+  int n, d, l;           /* points, features, sketch width */
+  const float* X;        /* point-major, ldx >= d */
+  int ldx;
+  const float* y;        /* labels +-1 */
+  float gamma;
+  double C;
+  const float* Omega;    /* n x l Gaussian test matrix, column major */
+  int ldo;
+  double* Z;             /* out: n x l FP64 factor, diag(y) K diag(y) ~ Z Z^T */
+  int ldz;
+  double* a;             /* out: n dual variables */
+  int n_panels, panel, g_bufs;  /* tile plan of the sketch passes; n_panels = 0: default */
+} db200_svm_instance;
+
+typedef struct {
+  double ms_pack, ms_sketch, ms_orth, ms_core, ms_barrier, ms_total;
+  int kernel_passes;     /* persistent launches over all instances */
+  int graph_replays;     /* of those, replays of a captured CUDA graph (test-matrix packing + tile launch) */
+  int workers;           /* host threads (each with its own context and stream) running the barriers */
+} db200_batch_report;
+
+/* Mixed-precision SVM solves of `count` instances: the q + 2 kernel passes of every instance run as single
+ * persistent launches over all instances (after the first, replayed from a captured CUDA graph when use_graph),
+ * CholeskyQR2 and the Nystrom core per instance in FP64, then the barrier of each instance
+ * (db200_svm_barrier with `params`) on `workers` host threads with their own contexts and streams.  reports: count
+ * entries (barrier results per instance).  Returns the first failing instance's status.  Synchronous. */
+DB200_API int db200_svm_solve_batched(db200_context* ctx, int count, const db200_svm_instance* inst, int q,
+                                      const db200_barrier_params* params, int use_graph, int workers,
+                                      db200_svm_report* reports, db200_batch_report* brep);
+
+/* ------------------------------------------------------------------------------------------------------------
  * Learned Nystrom landmarks.  No counterpart in the reference, which always sketches with a Gaussian Omega
  * (include/dkernel.h:13-46, tests/testsvm.cpp:94-134): a small MLP predicts per-point ridge leverage scores, r
  * landmarks are drawn by those scores, and the factor Z = K(:, L) chol(K(L, L))^-1 replaces the Gaussian sketch

@@ -1,0 +1,119 @@
+"""Batched instances on the GPU: many sketch problems of uneven n, d, l and gamma in one persistent launch
+(db200_rbf_sketch_batched) against the FP64 oracle and bit-for-bit against one launch per problem; explicit tile
+plans; and the batched SVM solve (db200_svm_solve_batched: batched kernel passes, CUDA-graph replay, worker
+threads) against per-instance db200_svm_solve on the same inputs."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.util import dev, ptr, rel_fro
+
+pytestmark = pytest.mark.gpu
+
+
+def _problem(n, d, l, seed):
+    g = np.random.default_rng(seed)
+    X = g.random((n, d), dtype=np.float32)
+    y = np.where(g.random(n) < 0.5, 1.0, -1.0).astype(np.float32)
+    Om = np.asfortranarray(g.standard_normal((n, l)).astype(np.float32))
+    return X, y, Om
+
+
+def _job(dX, dy, dOm, dY, n, d, l, gamma, plan=(0, 0, 0)):
+    from darray_optimizer_b200._lib import SketchJob
+    return SketchJob(n, n, d, l, ptr(dX), d, ptr(dX), d, ptr(dy), ptr(dy), ptr(dOm), n, ptr(dY), n, gamma, *plan)
+
+
+SHAPES = [(1000, 16, 40, 0.5), (3000, 64, 144, 1.0 / 64), (2500, 128, 272, 0.5 / 128), (600, 7, 330, 0.2),
+          (4096, 100, 96, 0.01)]
+
+
+def test_batched_sketch_matches_oracle_and_single_launches(gpu_ctx):
+    import torch
+    bufs, jobs, refs = [], [], []
+    for k, (n, d, l, gamma) in enumerate(SHAPES):
+        X, y, Om = _problem(n, d, l, 100 + k)
+        dX, dy, dOm = dev(X), dev(y), dev(Om)
+        dY = torch.zeros((l, n), dtype=torch.float32, device="cuda")
+        bufs.append((dX, dy, dOm, dY))
+        jobs.append(_job(dX, dy, dOm, dY, n, d, l, gamma))
+        refs.append((X, y, Om, gamma))
+    gpu_ctx.rbf_sketch_batched(jobs)
+    gpu_ctx.sync()
+    for k, ((n, d, l, gamma), (dX, dy, dOm, dY), (X, y, Om, _)) in enumerate(zip(SHAPES, bufs, refs)):
+        Yb = dY.cpu().numpy().T.copy()
+        err = rel_fro(Yb, O.sketch(X, X, y, y, Om, gamma))
+        assert err <= 2e-3, (k, err)
+        single = torch.zeros((l, n), dtype=torch.float32, device="cuda")
+        gpu_ctx.rbf_sketch(n, n, d, l, ptr(dX), d, ptr(dX), d, 0, ptr(dy), ptr(dy), ptr(dOm), n, ptr(single), n,
+                           gamma)
+        gpu_ctx.sync()
+        assert np.array_equal(single.cpu().numpy().T, Yb), k  # same tiles, same order
+
+
+@pytest.mark.parametrize("plan", [(1, 272, 1), (2, 144, 2), (3, 96, 2)])
+def test_explicit_tile_plans_agree_with_default(gpu_ctx, plan):
+    import torch
+    n, d, l, gamma = 2048, 64, 272, 1.0 / 64
+    X, y, Om = _problem(n, d, l, 7)
+    dX, dy, dOm = dev(X), dev(y), dev(Om)
+    outs = []
+    for p in [(0, 0, 0), plan]:
+        dY = torch.zeros((l, n), dtype=torch.float32, device="cuda")
+        gpu_ctx.rbf_sketch_batched([_job(dX, dy, dOm, dY, n, d, l, gamma, p)])
+        gpu_ctx.sync()
+        outs.append(dY.cpu().numpy())
+    assert rel_fro(outs[1], outs[0]) <= 1e-6
+
+
+def test_bad_tile_plan_is_rejected(gpu_ctx):
+    import torch
+    from darray_optimizer_b200._lib import DB200Error
+    n, d, l = 512, 16, 100
+    X, y, Om = _problem(n, d, l, 8)
+    dX, dy, dOm = dev(X), dev(y), dev(Om)
+    dY = torch.zeros((l, n), dtype=torch.float32, device="cuda")
+    with pytest.raises(DB200Error):  # 64-column panels cannot hold 100 columns
+        gpu_ctx.rbf_sketch_batched([_job(dX, dy, dOm, dY, n, d, l, 0.1, (1, 64, 2))])
+
+
+def _instances(specs):
+    import torch
+    from darray_optimizer_b200 import datagen
+    from darray_optimizer_b200._lib import SvmInstance
+    keep, inst = [], []
+    for k, (gen, n, d, l, gamma, C) in enumerate(specs):
+        w = datagen.two_gaussians(n=n, d=d, seed=200 + k) if gen == 1 else datagen.uniform_hyperplane(n=n, d=d,
+                                                                                                      seed=300 + k)
+        Om = np.asfortranarray(datagen.rng(400 + k).standard_normal((n, l), dtype=np.float32))
+        dX, dy, dOm = dev(w.X), dev(w.y), dev(Om)
+        Z = torch.zeros((l, n), dtype=torch.float64, device="cuda")
+        a = torch.zeros(n, dtype=torch.float64, device="cuda")
+        keep.append((dX, dy, dOm, Z, a))
+        inst.append(SvmInstance(n, d, l, ptr(dX), d, ptr(dy), gamma, C, ptr(dOm), n, ptr(Z), n, ptr(a), 0, 0, 0))
+    return keep, inst
+
+
+SPECS = [(1, 2048, 16, 144, 2.0 ** -3 / 16, 0.5), (2, 4096, 64, 272, 2.0 ** -1 / 64, 4.0),
+         (1, 3000, 128, 200, 2.0 ** -5 / 128, 1.0), (2, 2560, 16, 176, 1.0 / 16, 32.0)]
+
+
+@pytest.mark.parametrize("use_graph,workers", [(True, 3), (False, 1)])
+def test_batched_solve_matches_single_solves(gpu_ctx, use_graph, workers):
+    keep, inst = _instances(SPECS)
+    reps, brep = gpu_ctx.svm_solve_batched(inst, q=1, use_graph=use_graph, workers=workers)
+    assert brep.kernel_passes == 3 and brep.graph_replays == (2 if use_graph else 0)
+    assert brep.workers == min(workers, len(SPECS))
+    for k, ((gen, n, d, l, gamma, C), (dX, dy, dOm, Z, a), r) in enumerate(zip(SPECS, keep, reps)):
+        assert r.gap_barrier < 1e-6 and r.gap_primal_dual < 1e-6, k
+        za = a.cpu().numpy()
+        assert np.all(za >= 0) and np.all(za <= C)
+        # the same instance through the single-problem path: same kernels, same result
+        import torch
+        Z1 = torch.zeros_like(Z)
+        a1 = torch.zeros_like(a)
+        rep1 = gpu_ctx.svm_solve(n, d, l, 1, ptr(dX), d, ptr(dy), ptr(dOm), n, gamma, C, ptr(a1), ptr(Z1), n)
+        assert abs(rep1.f - r.f) <= 1e-9 * abs(rep1.f), (k, rep1.f, r.f)
+        assert rel_fro(Z1.cpu().numpy(), Z.cpu().numpy()) <= 1e-12
