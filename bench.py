@@ -259,8 +259,11 @@ def run_ours(args):
     solve = None
     if not args.no_solve and rank == 0:
         solve = solve_run(ctx, w, X, y, O, args.n_test)
+    batch = None
+    if not args.no_batch and rank == 0:
+        batch = batch_run(ctx)
     return finish(args, ctx, w, rep, ms_max, kernel_ms, kernel_count, launches, clocks, e2e_val, h2d, d2h, Om,
-                  solve)
+                  solve, batch)
 
 
 def solve_run(ctx, w, X, y, O, n_test):
@@ -306,6 +309,36 @@ def solve_run(ctx, w, X, y, O, n_test):
     return out
 
 
+def batch_run(ctx, count=64, workers=8):
+    """Batched form: `count` SVM instances of uneven n, d, gamma and C (darray_optimizer_b200.batched.workload) in
+    one db200_svm_solve_batched call -- batched persistent kernel passes replayed from a CUDA graph, tile plans from
+    the autotuner, barriers on worker threads -- against the same instances solved one after another."""
+    from darray_optimizer_b200 import autotune, batched
+    specs = batched.workload(count)
+    bufs = batched.upload(specs)
+    tuner = autotune.Tuner(ctx)
+    t0 = time.perf_counter()
+    for s in specs:
+        tuner.plan(s["n"], s["d"], s["l"])
+    tuning_s = time.perf_counter() - t0
+    batched.solve_batched(ctx, specs, bufs, tuner, use_graph=True, workers=workers)  # warm-up (buffers, contexts)
+    wall, reps, brep, plans = batched.solve_batched(ctx, specs, bufs, tuner, use_graph=True, workers=workers)
+    seq_wall, seq_reps = batched.solve_sequential(ctx, specs, bufs)
+    gpd = [r.gap_primal_dual for r in reps]
+    gb = [r.gap_barrier for r in reps]
+    return {"workload": f"{count} SVM instances, n log-uniform [2048, 65536], d in {{16, 64, 128}}, two-Gaussians / "
+                        "uniform-hyperplane data, gamma in 2^[-6..1]/d x C in 2^[-2..5], r = min(256, n/16) + 16, q = 1",
+            "instances": count, "wall_s": wall, "solves_per_s": count / wall,
+            "sequential_wall_s": seq_wall, "sequential_solves_per_s": count / seq_wall,
+            "speedup_vs_sequential": seq_wall / wall,
+            "gap_primal_dual_max": max(gpd), "gap_barrier_max": max(gb),
+            "gap_primal_dual": gpd, "newton": [r.newton for r in reps], "n": [s["n"] for s in specs],
+            "d": [s["d"] for s in specs],
+            "f_rel_diff_vs_sequential_max": max(abs(a.f - b.f) / abs(b.f) for a, b in zip(reps, seq_reps)),
+            "phases_ms": brep.as_dict(), "autotune_s": tuning_s,
+            "tile_plans": {k: v["plan"] for k, v in tuner.cache.items()}}
+
+
 def e2e_run(ctx, w, Om, rep, steps):
     import torch
     n, d, l = w.n, w.d, w.l
@@ -332,7 +365,7 @@ def e2e_run(ctx, w, Om, rep, steps):
 
 
 def finish(args, ctx, w, rep, ms_max, kernel_ms, kernel_count, launches, clocks, e2e_val, h2d, d2h, Om,
-           solve=None):
+           solve=None, batch=None):
     world, rank = rep.world, rep.rank
     n, d, l = w.n, w.d, w.l
     F = flops(n, d, l)
@@ -371,6 +404,8 @@ def finish(args, ctx, w, rep, ms_max, kernel_ms, kernel_count, launches, clocks,
             "gpu_launches": launches, "roofline": roof}
     if solve is not None:
         line["solve"] = solve
+    if batch is not None:
+        line["batch"] = batch
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, desc, threads = cpu_sample(w, Om, 256, args.cpu_seconds)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc}
@@ -392,6 +427,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg (profiling runs)")
     ap.add_argument("--no-solve", action="store_true", help="skip the whole-solve leg (mixed vs plain FP64)")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-instances leg")
     ap.add_argument("--n-test", type=int, default=16384, help="held-out points for the solve leg's accuracy")
     ap.add_argument("--n", type=int, default=N_POINTS, help="points (default: the C2 workload, 131072)")
     args = ap.parse_args()

@@ -326,36 +326,42 @@ int db200_svm_solve_batched(db200_context* ctx, int count, const db200_svm_insta
   if (st) return st;
   DB200_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
 
-  // ---- barriers: workers pull instances off a shared counter, each on its own context and stream
+  // ---- barriers: workers pull instances off a shared counter, largest first, each on its own context and stream
   if (workers < 1) workers = 1;
   if (workers > count) workers = count;
   R.workers = workers;
+  std::vector<int> order((size_t)count);
+  for (int b = 0; b < count; ++b) order[(size_t)b] = b;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+    return (double)inst[x].n * inst[x].l * inst[x].l > (double)inst[y].n * inst[y].l * inst[y].l;
+  });
   std::vector<db200_svm_report> rep((size_t)count);
   std::vector<int> status((size_t)count, DB200_OK);
   std::atomic<int> next{0};
-  const auto wall_b = std::chrono::steady_clock::now();
   auto run = [&](db200_context* w) {
-    for (int b = next.fetch_add(1); b < count; b = next.fetch_add(1)) {
+    for (int k = next.fetch_add(1); k < count; k = next.fetch_add(1)) {
+      const int b = order[(size_t)k];
       const db200_svm_instance& I = inst[b];
       std::memset(&rep[(size_t)b], 0, sizeof(db200_svm_report));
       status[(size_t)b] = db200_svm_barrier(w, I.n, I.l, I.Z, I.ldz, I.y, I.C, &P, I.a, &rep[(size_t)b]);
       rep[(size_t)b].nu = nus[(size_t)b];
     }
   };
+  if (workers > 1) {
+    while ((int)ctx->workers.size() < workers) {
+      db200_context* w = nullptr;
+      const int cst = db200_create(&w, ctx->device, DB200_OWN_STREAM);
+      if (cst) return fail(ctx, cst, "svm_solve_batched: worker context");
+      ctx->workers.push_back(w);
+    }
+  }
+  const auto wall_b = std::chrono::steady_clock::now();
   if (workers == 1) {
     run(ctx);
   } else {
-    std::vector<db200_context*> wctx((size_t)workers, nullptr);
-    int cst = DB200_OK;
-    for (int k = 0; k < workers && !cst; ++k) cst = db200_create(&wctx[(size_t)k], ctx->device, DB200_OWN_STREAM);
-    if (cst) {
-      for (db200_context* w : wctx) db200_destroy(w);
-      return fail(ctx, cst, "svm_solve_batched: worker context");
-    }
     std::vector<std::thread> th;
-    for (int k = 0; k < workers; ++k) th.emplace_back([&, k]() { run(wctx[(size_t)k]); });
+    for (int k = 0; k < workers; ++k) th.emplace_back([&, k]() { run(ctx->workers[(size_t)k]); });
     for (std::thread& t : th) t.join();
-    for (db200_context* w : wctx) db200_destroy(w);
   }
   R.ms_barrier = wall_ms(wall_b);
   R.ms_total = wall_ms(wall0);

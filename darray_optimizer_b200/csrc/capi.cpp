@@ -144,6 +144,8 @@ int db200_destroy(db200_context* ctx) {
   if (!ctx) return DB200_OK;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (db200_context* w : ctx->workers) db200_destroy(w);
+  ctx->workers.clear();
   prof_clear(ctx);
   if (ctx->ws) cudaFree(ctx->ws);
   if (ctx->io) cudaFree(ctx->io);

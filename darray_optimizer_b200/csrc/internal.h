@@ -27,6 +27,9 @@ struct db200_context {
   double* h_pinned = nullptr;    // small pinned host staging area for scalar readbacks
   void* tile_table = nullptr;    // instance table of the tile engine (grow-only)
   size_t tile_table_size = 0;
+  // Worker contexts (own stream and buffers each) of the batched solve, kept across calls so their buffers stay
+  // grown and no call pays context creation.
+  std::vector<db200_context*> workers;
   std::string last_error;
   long long launches = 0;        // kernels launched through this context
   // Optional per-launch timing of the tcgen05 tile kernels (CUDA events on the launching stream).

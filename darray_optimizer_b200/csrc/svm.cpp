@@ -191,6 +191,7 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
 
   double t = P.t0;
   int total_newton = 0, outer = 0, status = DB200_OK;
+  double prev_pd = -1.0;  // primal-dual gap at the previous outer step whose barrier bound was met
   double h[64];
   int st;
   auto fetch = [&](const double* d_src, int count) -> int {
@@ -340,7 +341,16 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
     if ((st = fetch(red, 9))) return st;
     suma_now = h[0];
     fa = 0.5 * h[8] - suma_now;
-    if (2.0 * n / t < P.gap_tol * std::fabs(fa)) break;
+    if (2.0 * n / t < P.gap_tol * std::fabs(fa)) {
+      // The barrier bound is met.  Stop once the true primal-dual gap at w = Z^T a is within tolerance too, or
+      // when a further outer step no longer halves it (it is then limited by the inexact Newton solves, not t).
+      if ((st = bar_dot(ctx, r, w, w, sc))) return st;
+      if ((st = bar_hinge(ctx, n, r, Z, ldz, w, sc + 3))) return st;
+      if ((st = fetch(sc, 4))) return st;
+      const double pd = (0.5 * h[0] + C * h[3] + fa) / std::fabs(fa);
+      if (pd < P.gap_tol || (prev_pd >= 0 && pd > 0.5 * prev_pd)) break;
+      prev_pd = pd;
+    }
     t *= P.mu;
   }
   if (outer > P.max_outer) {
