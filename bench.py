@@ -262,8 +262,115 @@ def run_ours(args):
     batch = None
     if not args.no_batch and rank == 0:
         batch = batch_run(ctx)
+    extra = {}
+    if args.c3 and rank == 0:
+        extra["c3"] = c3_run(ctx)
+    if args.c5 and rank == 0:
+        extra["c5"] = c5_run(ctx)
     return finish(args, ctx, w, rep, ms_max, kernel_ms, kernel_count, launches, clocks, e2e_val, h2d, d2h, Om,
-                  solve, batch)
+                  solve, batch, extra)
+
+
+def sampled_sketch_error(w, Yg_rows, rows, Om_rows_fn, block=64):
+    """Relative error of GPU sketch rows against the FP64 oracle on a row sample (size-independent check)."""
+    from oracle import oracle as O
+    Om = Om_rows_fn()
+    ref = O.sketch(w.X[rows], w.X, w.y[rows], w.y, Om, w.gamma, block=block)
+    return float(np.linalg.norm(Yg_rows - ref) / np.linalg.norm(ref))
+
+
+def c3_run(ctx, n=262144, n_test=16384, steps=3):
+    """Sparse-binary workload (n = 262144, d = 123 in {0, 1}, gamma = 0.05, r = 1024 + 16, C = 1): sketch-pass
+    throughput, the mixed solve to gap 1e-6, held-out accuracy, and the sketch against the FP64 oracle on 64
+    sampled rows."""
+    import torch
+    from darray_optimizer_b200 import datagen
+    w = datagen.sparse_binary(n=n)
+    d, l = w.d, w.l
+    X = torch.from_numpy(w.X).cuda()
+    y = torch.from_numpy(w.y).cuda()
+    Om_h = datagen.rng(w.seed + 7919).standard_normal((n, l), dtype=np.float32)
+    O = torch.from_numpy(np.ascontiguousarray(Om_h.T)).cuda()
+    Y = torch.empty((l, n), dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def step():
+        ctx.rbf_sketch(n, n, d, l, X.data_ptr(), d, X.data_ptr(), d, 0, y.data_ptr(), y.data_ptr(), O.data_ptr(), n,
+                       Y.data_ptr(), n, w.gamma)
+    for _ in range(2):
+        step()
+    ctx.sync()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        step()
+    e1.record(stream)
+    ctx.sync()
+    ms = e0.elapsed_time(e1) / steps
+    rows = np.sort(np.random.default_rng(3).choice(n, 64, replace=False))
+    err = sampled_sketch_error(w, Y.cpu().numpy().T[rows], rows, lambda: Om_h)
+    Z = torch.zeros((l, n), dtype=torch.float64, device="cuda")
+    a = torch.zeros(n, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    rep = ctx.svm_solve(n, d, l, w.power_iters, X.data_ptr(), d, y.data_ptr(), O.data_ptr(), n, w.gamma, w.C,
+                        a.data_ptr(), Z.data_ptr(), n)
+    torch.cuda.synchronize()
+    solve_s = time.perf_counter() - t0
+    Xt, yt = datagen.held_out(w, n_test)
+    dXt = torch.from_numpy(Xt).cuda()
+    dec = torch.zeros(n_test, dtype=torch.float64, device="cuda")
+    ctx.rbf_sketch_f64(n_test, n, d, 1, dXt.data_ptr(), d, X.data_ptr(), d, 0, y.data_ptr(), a.data_ptr(), n,
+                       dec.data_ptr(), n_test, w.gamma)
+    ctx.sync()
+    acc = float(np.mean(np.sign(dec.cpu().numpy()) == yt))
+    return {"workload": f"C3 sparse binary (n={n}, d={d} in {{0,1}}, p=0.11, gamma={w.gamma}, l={l}, q=1, C={w.C})",
+            "sketch_ms": ms, "sketch_tflops": flops(n, d, l) / ms / 1e9, "sketch_rel_err_64_rows_vs_fp64": err,
+            "solve_s": solve_s, "f": rep.f, "gap_barrier": rep.gap_barrier, "gap_primal_dual": rep.gap_primal_dual,
+            "newton": rep.newton, "test_accuracy": acc, "n_test": n_test,
+            "phases_ms": {k: getattr(rep, k) for k in ("ms_sketch", "ms_orth", "ms_core", "ms_barrier")}}
+
+
+def c5_run(ctx, n=524288, r=2048, n_test=16384, tol=1e-2):
+    """Learned-landmark workload (mixture of 32 rotated anisotropic Gaussians, n = 524288, d = 64, r = 2048):
+    the learned-landmark solve (model features -> MLP -> Gumbel top-r -> Nystrom factor -> sampled residual,
+    Gaussian-sketch fallback above tol), and the residual of uniform landmarks at the same r."""
+    import torch
+    from darray_optimizer_b200 import datagen, landmarks
+    w = datagen.mixture(n=n, d=64)
+    d = w.d
+    l_fb = r + 16
+    net = landmarks.load_model(ctx)
+    X = torch.from_numpy(w.X).cuda()
+    y = torch.from_numpy(w.y).cuda()
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(w.seed)
+    O = torch.randn((l_fb, n), dtype=torch.float32, device="cuda", generator=gen)  # n x l_fb Gaussian, column major
+    Z = torch.zeros((l_fb, n), dtype=torch.float64, device="cuda")
+    a = torch.zeros(n, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    rep, lrep = ctx.svm_solve_landmarks(n, d, r, X.data_ptr(), d, y.data_ptr(), w.gamma, w.C, net, 11, 16384, 512,
+                                        tol, O.data_ptr(), n, l_fb, 1, a.data_ptr(), Z.data_ptr(), n)
+    torch.cuda.synchronize()
+    solve_s = time.perf_counter() - t0
+    Xt, yt = datagen.held_out(w, n_test)
+    dXt = torch.from_numpy(Xt).cuda()
+    dec = torch.zeros(n_test, dtype=torch.float64, device="cuda")
+    ctx.rbf_sketch_f64(n_test, n, d, 1, dXt.data_ptr(), d, X.data_ptr(), d, 0, y.data_ptr(), a.data_ptr(), n,
+                       dec.data_ptr(), n_test, w.gamma)
+    ctx.sync()
+    acc = float(np.mean(np.sign(dec.cpu().numpy()) == yt))
+    del Z, a
+    uniform = landmarks.landmark_residual(ctx, w, r, None, 11)
+    return {"workload": f"C5 mixture of 32 rotated anisotropic Gaussians (n={n}, d={d}, gamma=1/d, r={r}, C={w.C})",
+            "solve_s": solve_s, "used_fallback": lrep.used_fallback, "rank": lrep.rank,
+            "residual_est_learned": lrep.residual_est, "residual_est_uniform_landmarks": uniform,
+            "residual_est_fallback": lrep.residual_fallback, "tol": tol,
+            "landmark_ms": {k: getattr(lrep, k) for k in ("ms_features", "ms_predict", "ms_select", "ms_factor",
+                                                         "ms_residual", "ms_fallback")},
+            "f": rep.f, "gap_barrier": rep.gap_barrier, "gap_primal_dual": rep.gap_primal_dual, "newton": rep.newton,
+            "ms_barrier": rep.ms_barrier, "test_accuracy": acc, "n_test": n_test}
 
 
 def solve_run(ctx, w, X, y, O, n_test):
@@ -365,7 +472,7 @@ def e2e_run(ctx, w, Om, rep, steps):
 
 
 def finish(args, ctx, w, rep, ms_max, kernel_ms, kernel_count, launches, clocks, e2e_val, h2d, d2h, Om,
-           solve=None, batch=None):
+           solve=None, batch=None, extra=None):
     world, rank = rep.world, rep.rank
     n, d, l = w.n, w.d, w.l
     F = flops(n, d, l)
@@ -406,6 +513,8 @@ def finish(args, ctx, w, rep, ms_max, kernel_ms, kernel_count, launches, clocks,
         line["solve"] = solve
     if batch is not None:
         line["batch"] = batch
+    if extra:
+        line.update(extra)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, desc, threads = cpu_sample(w, Om, 256, args.cpu_seconds)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc}
@@ -428,6 +537,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg (profiling runs)")
     ap.add_argument("--no-solve", action="store_true", help="skip the whole-solve leg (mixed vs plain FP64)")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-instances leg")
+    ap.add_argument("--c3", action="store_true", help="add the sparse-binary leg (n = 262144, l = 1040)")
+    ap.add_argument("--c5", action="store_true", help="add the learned-landmark leg (n = 524288, r = 2048)")
     ap.add_argument("--n-test", type=int, default=16384, help="held-out points for the solve leg's accuracy")
     ap.add_argument("--n", type=int, default=N_POINTS, help="points (default: the C2 workload, 131072)")
     args = ap.parse_args()
