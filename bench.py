@@ -258,7 +258,7 @@ def run_ours(args):
         e2e_val, h2d, d2h = e2e_run(ctx, w, Om, rep, args.steps)
     solve = None
     if not args.no_solve and rank == 0:
-        solve = solve_run(ctx, w, X, y, O, args.n_test)
+        solve = solve_run(ctx, w, X, y, O, args.n_test, mixed_only=args.solve_mixed_only)
     batch = None
     if not args.no_batch and rank == 0:
         batch = batch_run(ctx)
@@ -373,7 +373,7 @@ def c5_run(ctx, n=524288, r=2048, n_test=16384, tol=1e-2):
             "ms_barrier": rep.ms_barrier, "test_accuracy": acc, "n_test": n_test}
 
 
-def solve_run(ctx, w, X, y, O, n_test):
+def solve_run(ctx, w, X, y, O, n_test, mixed_only=False):
     """The whole SVM path (db200_svm_solve: 3 kernel passes, CholeskyQR2, Nystrom core, barrier to gap 1e-6) in the
     mixed precision and in the plain FP64 comparator, with held-out accuracy of both models."""
     import torch
@@ -404,6 +404,12 @@ def solve_run(ctx, w, X, y, O, n_test):
 
     one(0)  # warm-up: workspace growth, module load
     t_mixed, rep_m, acc_m = one(0)
+    if mixed_only:
+        out.update({"mixed_s": t_mixed, "f_mixed": rep_m.f, "gap_pd_mixed": rep_m.gap_primal_dual,
+                    "gap_barrier_mixed": rep_m.gap_barrier, "newton_mixed": rep_m.newton, "acc_mixed": acc_m,
+                    "phases_ms_mixed": {k: getattr(rep_m, k) for k in ("ms_sketch", "ms_orth", "ms_core",
+                                                                        "ms_barrier")}})
+        return out
     t_fp64, rep_f, acc_f = one(1)
     out.update({"mixed_s": t_mixed, "fp64_s": t_fp64, "speedup_vs_fp64": t_fp64 / t_mixed,
                 "f_mixed": rep_m.f, "f_fp64": rep_f.f, "rel_f_diff": abs(rep_m.f - rep_f.f) / abs(rep_f.f),
@@ -537,6 +543,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg (profiling runs)")
     ap.add_argument("--no-solve", action="store_true", help="skip the whole-solve leg (mixed vs plain FP64)")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-instances leg")
+    ap.add_argument("--solve-mixed-only", action="store_true",
+                    help="solve leg without the plain FP64 comparator (profiling runs)")
     ap.add_argument("--c3", action="store_true", help="add the sparse-binary leg (n = 262144, l = 1040)")
     ap.add_argument("--c5", action="store_true", help="add the learned-landmark leg (n = 524288, r = 2048)")
     ap.add_argument("--n-test", type=int, default=16384, help="held-out points for the solve leg's accuracy")

@@ -22,17 +22,28 @@ __device__ __forceinline__ double ld64(const T* p) { return (double)__ldg(p); }
 // C[p x q] (+)= alpha * A^T diag(w) B over rows [r0, r1) of A (n x p) and B (n x q); FP64 accumulation.
 // grid.z splits the rows; partial tiles are added with FP64 atomics when grid.z > 1.
 //
-// 128 x 128 output tile per CTA, 256 threads, each thread an 8 x 8 register block: rows {4ty..4ty+3,
-// 64+4ty..64+4ty+3} x columns {4tx..4tx+3, 64+4tx..64+4tx+3}, read from shared memory as 128-bit pairs, so 8
-// shared loads feed 64 FMAs (the 4 x 4 blocking of a 64 x 64 tile needs one load per two FMAs and is
-// shared-memory bound at about half the FP64 rate).  Tiles of 16 rows of A and B are staged transposed
-// (k-major) in shared memory with coalesced column reads from global memory (16 consecutive rows = 128 bytes).
+// FP64 tensor cores (mma.sync.m16n8k8.f64): 128 x 128 output tile per CTA, 8 warps of 32 x 64 (2 x 8 MMA tiles,
+// 64 accumulators per thread).  Stages of 8 rows of A and B are fetched into registers one stage ahead (coalesced
+// column reads: consecutive threads walk consecutive rows) and parked transposed (k-major) in a double-buffered
+// shared tile; per stage a warp loads 2 A fragments (4 doubles each) and 8 B fragments (2 doubles each) for 16
+// MMAs.  Fragment layouts of m16n8k8 (g = lane / 4, t = lane % 4): A (16 x 8, row) a0..a3 = A[g][t], A[g+8][t],
+// A[g][t+4], A[g+8][t+4]; B (8 x 8, col) b0, b1 = B[t][g], B[t+4][g]; C (16 x 8) c0, c1 = C[g][2t + 0, 1],
+// c2, c3 = C[g+8][2t + 0, 1].
 constexpr int GT = 128;        // Gram output tile
 constexpr int GK = 8;          // rows per stage
-constexpr int GPAD = GT + 2;   // padded shared row (keeps 16-byte alignment of the pairs)
+constexpr int GPAD = GT + 8;   // padded shared row: 4 consecutive k rows land 16 banks apart
+
+__device__ __forceinline__ void dmma16(double* d, const double* a, const double* b) {
+  asm volatile("mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+               "{%0,%1,%2,%3};"
+               : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+               : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+}
+
+constexpr int GTHREADS = 256;
 
 template <typename TA, typename TBt>
-__global__ void __launch_bounds__(256, 1) gram_kernel(int n, int p, int q, const TA* __restrict__ A, long long lda,
+__global__ void __launch_bounds__(GTHREADS, 1) gram_kernel(int n, int p, int q, const TA* __restrict__ A, long long lda,
                                                       const TBt* __restrict__ B, long long ldb,
                                                       const double* __restrict__ w, double alpha, double* C, int ldc,
                                                       int rows_per_split, int upper_only, int atomic) {
@@ -43,12 +54,16 @@ __global__ void __launch_bounds__(256, 1) gram_kernel(int n, int p, int q, const
   const int r1 = min(n, r0 + rows_per_split);
   __shared__ __align__(16) double sA[2][GK][GPAD];
   __shared__ __align__(16) double sB[2][GK][GPAD];
-  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-  double acc[8][8];
+  const int lane = threadIdx.x % 32, warp = threadIdx.x / 32;
+  const int wm = warp / 2, wn = warp % 2;  // warp tile: rows 32 wm .. +31, columns 64 wn .. +63
+  const int fr = lane / 4, fk = lane % 4;  // fragment row / k index of this lane
+  double acc[2][8][4];
 #pragma unroll
-  for (int a = 0; a < 8; ++a)
+  for (int a = 0; a < 2; ++a)
 #pragma unroll
-    for (int b = 0; b < 8; ++b) acc[a][b] = 0.0;
+    for (int b = 0; b < 8; ++b)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) acc[a][b][e] = 0.0;
   const int kk = threadIdx.x % GK;   // row inside the stage this thread loads
   const int c0 = threadIdx.x / GK;   // first column it loads (then +32, +64, +96)
   double va[4], vb[4];
@@ -81,43 +96,52 @@ __global__ void __launch_bounds__(256, 1) gram_kernel(int n, int p, int q, const
     // the next stage's global loads are in flight while this stage is multiplied
     const bool more = k0 + GK < r1;
     if (more) fetch(k0 + GK);
+    {
+      double af[2][4], bf[8][2];
 #pragma unroll
-    for (int t = 0; t < GK; ++t) {
-      double av[8], bv[8];
-      const double2* ra = reinterpret_cast<const double2*>(&sA[buf][t][0]);
-      const double2* rb = reinterpret_cast<const double2*>(&sB[buf][t][0]);
-      double2 x;
-      x = ra[2 * ty];      av[0] = x.x; av[1] = x.y;
-      x = ra[2 * ty + 1];  av[2] = x.x; av[3] = x.y;
-      x = ra[32 + 2 * ty]; av[4] = x.x; av[5] = x.y;
-      x = ra[33 + 2 * ty]; av[6] = x.x; av[7] = x.y;
-      x = rb[2 * tx];      bv[0] = x.x; bv[1] = x.y;
-      x = rb[2 * tx + 1];  bv[2] = x.x; bv[3] = x.y;
-      x = rb[32 + 2 * tx]; bv[4] = x.x; bv[5] = x.y;
-      x = rb[33 + 2 * tx]; bv[6] = x.x; bv[7] = x.y;
+      for (int a = 0; a < 2; ++a) {
+        const int r = 32 * wm + 16 * a + fr;
+        af[a][0] = sA[buf][fk][r];
+        af[a][1] = sA[buf][fk][r + 8];
+        af[a][2] = sA[buf][fk + 4][r];
+        af[a][3] = sA[buf][fk + 4][r + 8];
+      }
 #pragma unroll
-      for (int a = 0; a < 8; ++a)
+      for (int b = 0; b < 8; ++b) {
+        const int c = 64 * wn + 8 * b + fr;
+        bf[b][0] = sB[buf][fk][c];
+        bf[b][1] = sB[buf][fk + 4][c];
+      }
 #pragma unroll
-        for (int b = 0; b < 8; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
+      for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 8; ++b) dmma16(acc[a][b], af[a], bf[b]);
     }
     if (more) park(buf ^ 1);  // the other buffer was last read one stage ago, before the barrier below
     __syncthreads();
     buf ^= 1;
   }
 #pragma unroll
-  for (int a = 0; a < 8; ++a) {
-    const int i = i0 + (a < 4 ? 4 * ty + a : 64 + 4 * ty + a - 4);
-    if (i >= p) continue;
+  for (int a = 0; a < 2; ++a) {
 #pragma unroll
-    for (int b = 0; b < 8; ++b) {
-      const int j = j0 + (b < 4 ? 4 * tx + b : 64 + 4 * tx + b - 4);
-      if (j >= q) continue;
-      if (upper_only && i > j) continue;
-      double* dst = C + (long long)j * ldc + i;
-      if (atomic)
-        atomicAdd(dst, alpha * acc[a][b]);
-      else
-        *dst += alpha * acc[a][b];
+    for (int h = 0; h < 2; ++h) {
+      const int i = i0 + 32 * wm + 16 * a + 8 * h + fr;
+      if (i >= p) continue;
+#pragma unroll
+      for (int b = 0; b < 8; ++b) {
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int j = j0 + 64 * wn + 8 * b + 2 * fk + e;
+          if (j >= q) continue;
+          if (upper_only && i > j) continue;
+          double* dst = C + (long long)j * ldc + i;
+          const double v = alpha * acc[a][b][2 * h + e];
+          if (atomic)
+            atomicAdd(dst, v);
+          else
+            *dst += v;
+        }
+      }
     }
   }
 }
@@ -586,7 +610,7 @@ int gram(db200_context* ctx, int n, int p, int q, const TA* A, long long lda, co
   splits = (n + rows - 1) / rows;
   if (splits > 65535) return fail(ctx, DB200_ERR_UNSUPPORTED, "gram: too many row splits");
   dim3 grid(tp, tq, splits);
-  gram_kernel<TA, TBt><<<grid, 256, 0, ctx->stream>>>(n, p, q, A, lda, B, ldb, w, alpha, C, ldc, rows,
+  gram_kernel<TA, TBt><<<grid, GTHREADS, 0, ctx->stream>>>(n, p, q, A, lda, B, ldb, w, alpha, C, ldc, rows,
                                                      upper_only ? 1 : 0, splits > 1 ? 1 : 0);
   DB200_CUDA(ctx, cudaGetLastError());
   count_launch(ctx);
@@ -633,9 +657,9 @@ int potrf_upper(db200_context* ctx, double* A, int lda, int l, int* d_status, in
       potrf_panel_kernel<<<(rest + 127) / 128, 128, 0, ctx->stream>>>(A, lda, k0, kb, l, d_status);
       count_launch(ctx);
       // trailing update A22 -= A12^T A12 (upper triangle only)
-      const int tp = (rest + TB - 1) / TB;
+      const int tp = (rest + GT - 1) / GT;
       dim3 grid(tp, tp, 1);
-      gram_kernel<double, double><<<grid, 256, 0, ctx->stream>>>(kb, rest, rest, A + (long long)(k0 + kb) * lda + k0,
+      gram_kernel<double, double><<<grid, GTHREADS, 0, ctx->stream>>>(kb, rest, rest, A + (long long)(k0 + kb) * lda + k0,
                                                                  lda, A + (long long)(k0 + kb) * lda + k0, lda, nullptr,
                                                                  -1.0, A + (long long)(k0 + kb) * lda + k0 + kb, lda,
                                                                  kb, 1, 0);
