@@ -205,73 +205,99 @@ __global__ void __launch_bounds__(256) gemm_nn_kernel(int n, int p, int q, const
   }
 }
 
-// Unblocked upper Cholesky of one diagonal block (kb <= 64) held in shared memory.  status <- DB200_ERR_NOT_SPD
-// and *bad <- global pivot index on a non-positive (or NaN) pivot.
-__global__ void __launch_bounds__(256) potrf_diag_kernel(double* A, int lda, int k0, int kb, int* status,
-                                                         int* bad) {
-  __shared__ double s[64][65];
-  __shared__ int fail;
-  if (threadIdx.x == 0) fail = 0;
-  for (int e = threadIdx.x; e < kb * kb; e += blockDim.x) {
-    const int i = e % kb, j = e / kb;
-    s[i][j] = A[(long long)(k0 + j) * lda + k0 + i];
+// One block column of the right-looking blocked upper Cholesky: the kb x kb diagonal block (kb <= 64) is factored
+// in every CTA (redundantly; 64 steps with one barrier each, the block's elements in registers), CTA 0 writes
+// R11 back (zeros below its diagonal), and CTA c >= 1 overwrites the 64 panel columns
+// [k0 + kb + 64 (c - 1), +64) with R11^-T A12 by forward substitution (one warp per 8 columns, the solution held
+// two rows per lane and broadcast by shuffles).  On a non-positive or NaN pivot nothing is written,
+// status <- DB200_ERR_NOT_SPD and *bad <- k0 (first failing block).  A block column after a failed one returns
+// at once.  Follows cholesky_factorize (include/lapack_like.h:10-57): potrf of the diagonal block, trsm of the
+// panel, syrk of the trailing matrix (the last is the DMMA gram_kernel launched after this one).
+__global__ void __launch_bounds__(256) potrf_block_kernel(double* A, int lda, int k0, int kb, int l, int* status,
+                                                          int* bad) {
+  if (*(volatile int*)status) return;
+  __shared__ double rs[64][65];  // staging, then R11 (row-major: rs[i][j] = R[k0 + i][k0 + j])
+  __shared__ double rowk[2][64];
+  __shared__ double inv[64];
+  const int t = threadIdx.x;
+  // stage the diagonal block coalesced (column j contiguous in i)
+  for (int e = t; e < 64 * 64; e += 256) {
+    const int i = e & 63, j = e >> 6;
+    rs[i][j] = (i < kb && j < kb && i <= j) ? A[(long long)(k0 + j) * lda + k0 + i] : 0.0;
   }
   __syncthreads();
-  for (int k = 0; k < kb; ++k) {
-    if (threadIdx.x == 0) {
-      const double piv = s[k][k];
-      if (!(piv > 0.0)) {
-        fail = 1;
-      } else {
-        s[k][k] = sqrt(piv);
-      }
+  // thread t owns column j = t & 63, rows i = rg + 4 q (q = 0..15)
+  const int j = t & 63, rg = t >> 6;
+  double a[16];
+#pragma unroll
+  for (int q = 0; q < 16; ++q) a[q] = rs[rg + 4 * q][j];
+  bool failed = false;
+#pragma unroll
+  for (int k = 0; k < 64; ++k) {
+    if (k >= kb) break;
+    if (rg == (k & 3)) rowk[k & 1][j] = a[k >> 2];
+    __syncthreads();  // row k published; also orders the staging reads before the first rs write below
+    const double piv = rowk[k & 1][k];
+    if (!(piv > 0.0)) {  // the same value in every thread: a uniform exit
+      failed = true;
+      break;
     }
-    __syncthreads();
-    if (fail) break;
-    const double rkk = s[k][k];
-    for (int j = k + 1 + threadIdx.x; j < kb; j += blockDim.x) s[k][j] /= rkk;
-    __syncthreads();
-    // trailing update of the upper triangle: s[i][j] -= s[k][i] * s[k][j], k < i <= j
-    const int m = kb - k - 1;
-    for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
-      const int i = k + 1 + e % m, j = k + 1 + e / m;
-      if (i <= j) s[i][j] -= s[k][i] * s[k][j];
+    const double u = 1.0 / piv;
+    const double ckj = rowk[k & 1][j] * u;
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const int i = rg + 4 * q;
+      if (i > k) a[q] -= rowk[k & 1][i] * ckj;  // i > j entries are never read back
     }
-    __syncthreads();
+    if (rg == (k & 3)) {
+      const double s = sqrt(piv);
+      rs[k][j] = (j == k) ? s : ((j > k) ? a[k >> 2] / s : 0.0);
+      if (j == k) inv[k] = 1.0 / s;
+    }
   }
-  if (fail) {
-    if (threadIdx.x == 0) {
-      if (atomicCAS(status, 0, DB200_ERR_NOT_SPD) == 0) *bad = k0;
+  if (failed) {
+    if (blockIdx.x == 0 && t == 0 && atomicCAS(status, 0, DB200_ERR_NOT_SPD) == 0) *bad = k0;
+    return;
+  }
+  __syncthreads();
+  if (blockIdx.x == 0) {
+    for (int e = t; e < kb * 64; e += 256) {
+      const int i = e & 63, jj = e >> 6;
+      if (i < kb) A[(long long)(k0 + jj) * lda + k0 + i] = (i <= jj) ? rs[i][jj] : 0.0;
     }
     return;
   }
-  for (int e = threadIdx.x; e < kb * kb; e += blockDim.x) {
-    const int i = e % kb, j = e / kb;
-    A[(long long)(k0 + j) * lda + k0 + i] = (i <= j) ? s[i][j] : 0.0;
+  // panel: x = R11^-T b for 8 columns per warp; lane holds rows lane and lane + 32
+  const int warp = t >> 5, lane = t & 31;
+  const int c0 = k0 + kb + (blockIdx.x - 1) * 64 + warp * 8;
+  double v[8][2];
+#pragma unroll
+  for (int cc = 0; cc < 8; ++cc) {
+    const bool ok = c0 + cc < l;
+    const double* col = A + (long long)(c0 + cc) * lda + k0;
+    v[cc][0] = (ok && lane < kb) ? col[lane] : 0.0;
+    v[cc][1] = (ok && lane + 32 < kb) ? col[lane + 32] : 0.0;
   }
-}
-
-// Panel solve A12 <- R11^-T A12 for the kb x (l - k0 - kb) panel right of the diagonal block: one thread per
-// column, forward substitution with R11^T (lower).
-__global__ void __launch_bounds__(128) potrf_panel_kernel(double* A, int lda, int k0, int kb, int l, const int* status) {
-  if (*status) return;
-  __shared__ double r[64][65];
-  for (int e = threadIdx.x; e < kb * kb; e += blockDim.x) {
-    const int i = e % kb, j = e / kb;
-    r[i][j] = A[(long long)(k0 + j) * lda + k0 + i];
+#pragma unroll
+  for (int i = 0; i < 64; ++i) {
+    if (i >= kb) break;
+    const double ri = inv[i];
+    const double r0 = rs[i][lane], r1 = rs[i][lane + 32];  // R[i][row] for this lane's two rows
+#pragma unroll
+    for (int cc = 0; cc < 8; ++cc) {
+      const double x = __shfl_sync(0xffffffffu, v[cc][i >> 5], i & 31) * ri;
+      if (lane == (i & 31)) v[cc][i >> 5] = x;
+      if (i < 32 && lane > i) v[cc][0] -= r0 * x;
+      if (lane + 32 > i) v[cc][1] -= r1 * x;
+    }
   }
-  __syncthreads();
-  const int col = k0 + kb + blockIdx.x * blockDim.x + threadIdx.x;
-  if (col >= l) return;
-  double* c = A + (long long)col * lda + k0;
-  double x[64];
-#pragma unroll 4
-  for (int i = 0; i < kb; ++i) {
-    double v = c[i];
-    for (int k = 0; k < i; ++k) v -= r[k][i] * x[k];
-    x[i] = v / r[i][i];
+#pragma unroll
+  for (int cc = 0; cc < 8; ++cc) {
+    if (c0 + cc >= l) continue;
+    double* col = A + (long long)(c0 + cc) * lda + k0;
+    if (lane < kb) col[lane] = v[cc][0];
+    if (lane + 32 < kb) col[lane + 32] = v[cc][1];
   }
-  for (int i = 0; i < kb; ++i) c[i] = x[i];
 }
 
 // Zero the strictly lower triangle of an l x l matrix.
@@ -307,55 +333,80 @@ __global__ void trinv_upper_kernel(const double* R, int ldr, int l, double* X, i
 // inner product reads a contiguous column):
 //   mode 0: solve R^T y = b   (forward; row i of R^T = column i of R)
 //   mode 1: solve R x = y     (backward; row i of R = column i of L)
-// x/b in place, FP64.  Blocks of 32 rows: all warps form the off-block inner products, warp 0 solves the
-// 32 x 32 triangle.
-__global__ void __launch_bounds__(1024) trsv_kernel(const double* R, const double* L, int ld, int l, double* x,
-                                                    int mode) {
+// x/b in place, FP64, x staged in shared memory (l <= 4096).  Blocks of 32 rows: the 16 warps form the off-block
+// inner products (two rows each), then warp 0 solves the 32 x 32 triangle from registers it loaded before the
+// inner products (so the 32 sequential steps carry no memory latency), with the diagonal applied as a
+// reciprocal computed once per block.  Follows triangular_solve (include/blas_like.h:96-140) for one column.
+__global__ void __launch_bounds__(512) trsv_kernel(const double* R, const double* L, int ld, int l, double* x,
+                                                   int mode) {
+  __shared__ double xs[4096];
   __shared__ double part[32];
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  for (int i = threadIdx.x; i < l; i += blockDim.x) xs[i] = x[i];
   const int nb = (l + 31) / 32;
+  const double* T = (mode == 0) ? R : L;  // column i0 + lane of T holds this lane's triangle coefficients
   for (int bb = 0; bb < nb; ++bb) {
     const int blk = (mode == 0) ? bb : nb - 1 - bb;
     const int i0 = blk * 32;
-    const int i = i0 + warp;
-    // off-block contribution for row i
-    double s = 0.0;
-    if (i < l) {
-      if (mode == 0) {  // sum_{k < i0} R[k, i] x_k
-        const double* col = R + (long long)i * ld;
-        for (int k = lane; k < i0; k += 32) s += col[k] * x[k];
-      } else {  // sum_{k >= i0 + 32} R[i, k] x_k = sum L[k, i] x_k
-        const double* col = L + (long long)i * ld;
-        for (int k = i0 + 32 + lane; k < l; k += 32) s += col[k] * x[k];
-      }
-    }
+    const int bl = min(32, l - i0);
+    double tri[32];
+    double dinv = 0.0;
+    if (warp == 0) {
+      const double* c = T + (long long)(i0 + lane) * ld + i0;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) part[warp] = s;
+      for (int r = 0; r < 32; ++r) tri[r] = (lane < bl && r < bl) ? c[r] : 0.0;
+    }
+    __syncthreads();  // xs of the previous block (and the initial staging) visible
+    // off-block contribution for rows i0 + warp and i0 + warp + 16
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int i = i0 + warp + 16 * h;
+      double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+      if (i < l) {
+        const double* col = T + (long long)i * ld;
+        const int kbeg = (mode == 0) ? 0 : i0 + 32, kend = (mode == 0) ? i0 : l;
+        int k = kbeg + lane;
+        for (; k + 96 < kend; k += 128) {
+          s0 += col[k] * xs[k];
+          s1 += col[k + 32] * xs[k + 32];
+          s2 += col[k + 64] * xs[k + 64];
+          s3 += col[k + 96] * xs[k + 96];
+        }
+        for (; k < kend; k += 32) s0 += col[k] * xs[k];
+      }
+      double s = (s0 + s1) + (s2 + s3);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      if (lane == 0) part[warp + 16 * h] = s;
+    }
     __syncthreads();
     if (warp == 0) {
-      const int bl = min(32, l - i0);
-      double v = (lane < bl) ? x[i0 + lane] - part[lane] : 0.0;
-      // solve the bl x bl triangle, one row per step
+      double dg = 1.0;
+#pragma unroll
+      for (int r = 0; r < 32; ++r)
+        if (r == lane && lane < bl) dg = tri[r];
+      dinv = (lane < bl) ? 1.0 / dg : 0.0;
+      double v = (lane < bl) ? xs[i0 + lane] - part[lane] : 0.0;
       if (mode == 0) {
-        for (int r = 0; r < bl; ++r) {
-          const double rr = R[(long long)(i0 + r) * ld + i0 + r];
-          const double xr = __shfl_sync(0xffffffffu, v, r) / rr;
+#pragma unroll
+        for (int r = 0; r < 32; ++r) {
+          const double xr = __shfl_sync(0xffffffffu, v * dinv, r);
           if (lane == r) v = xr;
-          if (lane > r && lane < bl) v -= R[(long long)(i0 + lane) * ld + i0 + r] * xr;
+          if (lane > r) v -= tri[r] * xr;
         }
       } else {
-        for (int r = bl - 1; r >= 0; --r) {
-          const double rr = R[(long long)(i0 + r) * ld + i0 + r];
-          const double xr = __shfl_sync(0xffffffffu, v, r) / rr;
+#pragma unroll
+        for (int r = 31; r >= 0; --r) {
+          const double xr = __shfl_sync(0xffffffffu, v * dinv, r);
           if (lane == r) v = xr;
-          if (lane < r) v -= R[(long long)(i0 + r) * ld + i0 + lane] * xr;
+          if (lane < r) v -= tri[r] * xr;
         }
       }
-      if (lane < bl) x[i0 + lane] = v;
+      if (lane < bl) xs[i0 + lane] = v;
     }
-    __syncthreads();
   }
+  __syncthreads();
+  for (int i = threadIdx.x; i < l; i += blockDim.x) x[i] = xs[i];
 }
 
 __global__ void transpose_kernel(const double* A, int lda, int m, int n, double* B, int ldb) {
@@ -650,12 +701,10 @@ int potrf_upper(db200_context* ctx, double* A, int lda, int l, int* d_status, in
   if (nb < 1 || nb > 64) nb = 64;
   for (int k0 = 0; k0 < l; k0 += nb) {
     const int kb = (l - k0 < nb) ? l - k0 : nb;
-    potrf_diag_kernel<<<1, 256, 0, ctx->stream>>>(A, lda, k0, kb, d_status, d_bad);
-    count_launch(ctx);
     const int rest = l - k0 - kb;
+    potrf_block_kernel<<<1 + (rest + 63) / 64, 256, 0, ctx->stream>>>(A, lda, k0, kb, l, d_status, d_bad);
+    count_launch(ctx);
     if (rest > 0) {
-      potrf_panel_kernel<<<(rest + 127) / 128, 128, 0, ctx->stream>>>(A, lda, k0, kb, l, d_status);
-      count_launch(ctx);
       // trailing update A22 -= A12^T A12 (upper triangle only)
       const int tp = (rest + GT - 1) / GT;
       dim3 grid(tp, tp, 1);
@@ -680,7 +729,8 @@ int trinv_upper(db200_context* ctx, const double* R, int ldr, int l, double* X, 
 }
 
 int trsv_upper(db200_context* ctx, const double* R, const double* L, int ld, int l, double* x, bool transposed) {
-  trsv_kernel<<<1, 1024, 0, ctx->stream>>>(R, L, ld, l, x, transposed ? 0 : 1);
+  if (l > 4096) return fail(ctx, DB200_ERR_UNSUPPORTED, "trsv: l > 4096");
+  trsv_kernel<<<1, 512, 0, ctx->stream>>>(R, L, ld, l, x, transposed ? 0 : 1);
   DB200_CUDA(ctx, cudaGetLastError());
   count_launch(ctx);
   return DB200_OK;

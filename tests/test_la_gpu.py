@@ -54,6 +54,19 @@ def test_potrf_matches_oracle(gpu_ctx, n):
     assert np.all(np.tril(R, -1) == 0)
 
 
+@pytest.mark.parametrize("n,nb", [(1, 64), (63, 64), (65, 64), (130, 17), (191, 32), (2064, 64)])
+def test_potrf_ragged_blocks(gpu_ctx, n, nb):
+    # partial diagonal blocks, partial 64-column panel chunks and block sizes below 64
+    g = np.random.default_rng(n + nb)
+    B = g.standard_normal((n, n))
+    A = B @ B.T / n + 0.5 * np.eye(n)
+    dA = d64(A)
+    gpu_ctx.potrf(n, dA.data_ptr(), n, nb)
+    R = h64(dA, n)
+    assert rel(R, O.cholesky_upper(A)) < 1e-11
+    assert np.all(np.tril(R, -1) == 0)
+
+
 def test_potrf_test3_factor_and_reference(gpu_ctx):
     A = G["chol_test3_A"].astype(np.float64)
     dA = d64(A)

@@ -171,6 +171,25 @@ def test_woodbury_solve_matches_dense_solve(gpu_ctx):
     assert np.linalg.norm(A @ G["pcg_x"] - bp) <= 1e-2  # the reference's PCG stopping rule
 
 
+@pytest.mark.parametrize("r", [1, 31, 33, 97, 528, 1040, 2064])
+def test_woodbury_solve_ragged_and_large_rank(gpu_ctx, r):
+    # every shape of the 32-row triangular-solve blocks (partial last block, one block, many) and of the 64-column
+    # Cholesky block columns, against a dense FP64 solve of the same system
+    import torch
+    g = np.random.default_rng(r)
+    n = max(2 * r, 256)
+    Z = g.standard_normal((n, r)) / np.sqrt(r)
+    diag = np.exp(g.uniform(-3, 3, n))
+    b = g.standard_normal(n)
+    dZ, dd, db = dev(Z, np.float64), dev(diag, np.float64), dev(b, np.float64)
+    dx = torch.zeros(n, dtype=torch.float64, device="cuda")
+    gpu_ctx.woodbury_solve(n, r, dZ.data_ptr(), n, dd.data_ptr(), db.data_ptr(), dx.data_ptr())
+    x = dx.cpu().numpy()
+    H = Z @ Z.T + np.diag(diag)
+    x_ref = np.linalg.solve(H, b)
+    assert np.linalg.norm(x - x_ref) <= 1e-10 * np.linalg.norm(x_ref)
+
+
 def test_knorm_matches_oracle(gpu_ctx, c1_small):
     w, lr = c1_small
     n, k = lr.Z.shape
