@@ -407,6 +407,7 @@ def solve_run(ctx, w, X, y, O, n_test, mixed_only=False):
     if mixed_only:
         out.update({"mixed_s": t_mixed, "f_mixed": rep_m.f, "gap_pd_mixed": rep_m.gap_primal_dual,
                     "gap_barrier_mixed": rep_m.gap_barrier, "newton_mixed": rep_m.newton, "acc_mixed": acc_m,
+                    "refine_mixed": rep_m.refine, "fallbacks_mixed": rep_m.fallbacks,
                     "phases_ms_mixed": {k: getattr(rep_m, k) for k in ("ms_sketch", "ms_orth", "ms_core",
                                                                         "ms_barrier")}})
         return out
@@ -416,6 +417,7 @@ def solve_run(ctx, w, X, y, O, n_test, mixed_only=False):
                 "gap_pd_mixed": rep_m.gap_primal_dual, "gap_pd_fp64": rep_f.gap_primal_dual,
                 "gap_barrier_mixed": rep_m.gap_barrier, "gap_barrier_fp64": rep_f.gap_barrier,
                 "newton_mixed": rep_m.newton, "newton_fp64": rep_f.newton, "refine_mixed": rep_m.refine,
+                "fallbacks_mixed": rep_m.fallbacks,
                 "acc_mixed": acc_m, "acc_fp64": acc_f,
                 "phases_ms_mixed": {k: getattr(rep_m, k) for k in ("ms_sketch", "ms_orth", "ms_core", "ms_barrier")},
                 "phases_ms_fp64": {k: getattr(rep_f, k) for k in ("ms_sketch", "ms_orth", "ms_core", "ms_barrier")}})

@@ -31,7 +31,7 @@ int bar_residual(db200_context* ctx, int n, int r, const double* Z, long long ld
 int bar_step_stats(db200_context* ctx, int n, const double* g, const double* s, const double* a, double C,
                    double* red);
 
-// gram_tc.cu: M (upper, FP64) += (D^-1/2 Z)^T (D^-1/2 Z) on the tensor cores, split bf16
+// gram_tc.cu: M (upper, FP64) += (D^-1/2 Z)^T (D^-1/2 Z) on the int8 tensor cores (Ozaki slices)
 size_t gram_tc_scratch_bytes(int n, int r);
 int gram_tc_weighted(db200_context* ctx, int n, int r, const double* Z, long long ldz, const double* w, double* M,
                      int ldm, void* scratch);

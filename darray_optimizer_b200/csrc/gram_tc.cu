@@ -1,11 +1,30 @@
-// Tensor-core (tcgen05) weighted Gram for the Woodbury capacity matrix of the Newton step:
+// Tensor-core weighted Gram for the Woodbury capacity matrix of the Newton step:
 //     M += Z~^T Z~,   Z~ = diag(sqrt(w)) Z   (Z: n x r FP64 column major, w = D^-1 >= 0)
-// The operand is split into bf16 hi + lo (hi.hi + hi.lo + lo.hi, fp32 accumulation in TMEM, relative error of
-// the products ~2^-16), the n dimension is split across CTAs and each CTA adds its 128 x 128 tile into the FP64
-// matrix with FP64 atomics.  The barrier solver refines the resulting Newton step against the exact FP64
-// operator (Z Z^T + D), so the tensor-core Gram only has to be a good preconditioner.
+// computed exactly in integers on the int8 tensor cores (the Ozaki splitting scheme: Ozaki, Ogita, Oishi and Rump,
+// "Error-free transformations of matrix multiplication by using fast routines of matrix multiplication and its
+// applications", Numer. Algorithms 59 (2012); Ootomo, Ozaki and Yokota, "DGEMM on integer matrix multiplication
+// unit", IJHPCA 2024).
+//
+//  1. The rows are cut into chunks of 16384.  In every chunk c each column p of Z~ is scaled by 2^-e_cp, e_cp the
+//     exponent just above the chunk's largest |entry| of that column, so that x = Z~[i, p] 2^-e_cp lies in (-1, 1).
+//  2. x is cut into KS signed 7-bit digits by truncation, x = sum_s d_s 2^-7s + (remainder < 2^-7 KS), d_s in
+//     [-127, 127] (the base-128 digits of floor(|x| 2^(7 KS)) with the sign of x), stored as KS int8 slices
+//     [s][p][i] (i contiguous).  One pass reads a column chunk (128 KB) for its maximum and again, from L2, to
+//     slice it.
+//  3. M[p, q] = sum_c 2^(e_cp + e_cq) sum_{s,t} 2^-7(s+t) (D_s^T D_t)_c[p, q].  The products with s + t <= KS + 1
+//     are kept (the rest lie below the truncation); all products of one group g = s + t share a scale, so each
+//     group is a single s32 accumulator in TMEM fed by tcgen05.mma kind::i8 (exact integer sums:
+//     KS * 16384 * 127^2 < 2^31).  A CTA's k range lies inside one chunk.
+//  4. The epilogue folds the groups in FP64 (Horner in 2^-7), scales by 2^(e_cp + e_cq) and adds the 128 x 64 tile
+//     into M with FP64 atomics (the n dimension is split across CTAs).
+//
+// The result differs from the exact Z~^T Z~ by the dropped groups and the truncation only, about
+// 1e-12 ||Z~_p|| ||Z~_q|| for KS = 7 (measured), next to FP64 accumulation's ~1e-16 sqrt(n).  The barrier solver
+// still refines each Newton step against the exact FP64 operator and falls back to the FP64 Gram if refinement
+// stalls.
 #include <cuda.h>
 #include <cudaTypedefs.h>
+#include <algorithm>
 #include <mutex>
 
 #include "internal.h"
@@ -14,25 +33,42 @@
 namespace db200 {
 namespace {
 
-constexpr int TM = 128;                       // output tile (rows and columns of M)
-constexpr int KCH = 64;                       // k chunk: 64 bf16 = one 128-byte swizzled row
-constexpr int OPB = TM * KCH * 2;             // one operand chunk, 16 KB
-constexpr int STAGE = 4 * OPB;                // Ahi, Alo, Bhi, Blo
-constexpr int NSTAGE = 3;
-constexpr int THREADS = 192;                  // warp 0 TMA, warp 1 MMA, warps 2..5 epilogue
+constexpr int KS = 8;                          // int8 digits per value (groups g = s + t in [2, KS + 1])
+constexpr int TM = 128;                        // M tile: rows p of M
+constexpr int TN = 64;                         // N tile: columns q of M
+constexpr int KB = 64;                         // k bytes per stage: one 64-byte swizzled row per operand row
+constexpr int ASL = TM * KB;                   // one A slice per stage, 8 KB
+constexpr int BSL = TN * KB;                   // one B slice per stage, 4 KB
+constexpr int STAGE = KS * (ASL + BSL);        // 96 KB
+constexpr int NSTAGE = 2;
+constexpr int CH = 16384;                      // rows per scaling chunk (and at most per CTA: exact s32 sums)
+constexpr int MAX_CHUNKS = CH / KB;            // k chunks (64 rows) per scaling chunk
+constexpr int TMEM_COLS = 512;                 // KS * TN columns of s32 groups
+constexpr int THREADS = 192;                   // warp 0 TMA, warp 1 MMA, warps 2..5 epilogue
+static_assert(KS * TN <= TMEM_COLS, "group accumulators exceed TMEM");
+static_assert((long long)KS * MAX_CHUNKS * KB * 127 * 127 < (1LL << 31), "s32 group sums could overflow");
 
 struct GramArgs {
-  int r;          // valid rows / columns of M
-  int ntiles;     // tiles per side
-  int kchunks;    // total k chunks (npad / 64)
-  int chunks_per_split;
+  int r;                // valid rows / columns of M
+  int nq;               // q tiles (64 wide); p tiles are 128 high and tile pairs keep tj >= 2 ti
+  int kchunks;          // npad / 64
+  int chunks_per_split;  // divides MAX_CHUNKS: a CTA's k range lies in one scaling chunk
+  int rpad;
+  const int* exps;       // e_cp at [c * rpad + p]
   double* M;
   int ldm;
   int* status;
 };
 
+// e with m < 2^e for m >= 0 (floor(log2 m) + 1 from the IEEE exponent field); 0 for m == 0.
+__device__ __forceinline__ int exp_above(double m) {
+  const unsigned long long bits = (unsigned long long)__double_as_longlong(m);
+  const int biased = (int)((bits >> 52) & 0x7ff);
+  return bits == 0 ? 0 : biased - 1022;
+}
+
 __global__ void __launch_bounds__(THREADS, 1)
-    gram_tc_kernel(const __grid_constant__ CUtensorMap tm_hi, const __grid_constant__ CUtensorMap tm_lo, GramArgs g) {
+    gram_i8_kernel(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ CUtensorMap tm_b, GramArgs g) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const uint32_t s_op = smem_u32(smem);
@@ -44,14 +80,13 @@ __global__ void __launch_bounds__(THREADS, 1)
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + NSTAGE * STAGE + 256);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + NSTAGE * STAGE + 264);
 
-  // tile pair (upper triangle only) and k range of this CTA
-  int tpair = blockIdx.x;
-  int ti = 0;
-  while (tpair >= g.ntiles - ti) {
-    tpair -= g.ntiles - ti;
+  // tile pair (p tile ti, q tile tj >= 2 ti: the upper triangle) and k range of this CTA
+  int idx = blockIdx.x, ti = 0;
+  while (idx >= g.nq - 2 * ti) {
+    idx -= g.nq - 2 * ti;
     ++ti;
   }
-  const int tj = ti + tpair;
+  const int tj = 2 * ti + idx;
   const int k0 = blockIdx.y * g.chunks_per_split;
   const int k1 = min(g.kchunks, k0 + g.chunks_per_split);
   const int nk = k1 - k0;
@@ -68,7 +103,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     fence_mbarrier_init();
   }
   if (warp == 1) {
-    tmem_alloc(smem_u32(tmem_slot), 128);
+    tmem_alloc(smem_u32(tmem_slot), TMEM_COLS);
     tmem_relinquish();
   }
   tc_fence_before();
@@ -77,23 +112,27 @@ __global__ void __launch_bounds__(THREADS, 1)
   const uint32_t tmem = *tmem_slot;
 
   if (warp == 0) {
-    if (lane == 0 && nk > 0) {
-      prefetch_tmap(&tm_hi);
-      prefetch_tmap(&tm_lo);
-      int issued = 0;
-      for (int k = 0; k < nk; ++k, ++issued) {
-        const int s = k % NSTAGE;
-        const uint32_t ph = (k / NSTAGE) & 1;
-        if (!mbar_wait(empty(s), ph ^ 1, abort_flag)) break;
-        mbar_arrive_expect_tx(full(s), STAGE);
-        const uint32_t base = s_op + s * STAGE;
-        const int x = (k0 + k) * KCH;
-        tma_load_2d(base + 0 * OPB, &tm_hi, full(s), x, ti * TM);
-        tma_load_2d(base + 1 * OPB, &tm_lo, full(s), x, ti * TM);
-        tma_load_2d(base + 2 * OPB, &tm_hi, full(s), x, tj * TM);
-        tma_load_2d(base + 3 * OPB, &tm_lo, full(s), x, tj * TM);
+    if (nk > 0) {
+      if (lane == 0) {
+        prefetch_tmap(&tm_a);
+        prefetch_tmap(&tm_b);
       }
-      if (*abort_flag) {
+      int issued = 0;
+      for (int k = 0; k < nk; ++k) {
+        const int s = k % NSTAGE;
+        if (!__all_sync(0xffffffffu, mbar_wait(empty(s), ((k / NSTAGE) & 1) ^ 1, abort_flag))) break;
+        if (elect_one()) {
+          mbar_arrive_expect_tx(full(s), STAGE);
+          const uint32_t base = s_op + s * STAGE;
+          const int x = (k0 + k) * KB;
+          tma_load_3d(base, &tm_a, full(s), x, ti * TM, 0);             // KS slices x 128 rows x 64 bytes
+          tma_load_3d(base + KS * ASL, &tm_b, full(s), x, tj * TN, 0);  // KS slices x 64 rows x 64 bytes
+        }
+        __syncwarp();
+        ++issued;
+      }
+      if (*abort_flag && lane == 0) {
+        // let the copies in flight land before the CTA exits (bounded waits)
         volatile int never = 0;
         for (int k = (issued > NSTAGE ? issued - NSTAGE : 0); k < issued; ++k)
           mbar_wait(full(k % NSTAGE), (k / NSTAGE) & 1, &never);
@@ -101,27 +140,32 @@ __global__ void __launch_bounds__(THREADS, 1)
     }
     __syncwarp();
   } else if (warp == 1) {
-    if (lane == 0) {
-      const uint32_t idesc = idesc_f16(TM, TM, true);
-      bool ok = true;
-      for (int k = 0; k < nk && ok; ++k) {
-        const int s = k % NSTAGE;
-        if (!mbar_wait(full(s), (k / NSTAGE) & 1, abort_flag)) {
-          ok = false;
-          break;
-        }
-        tc_fence_after();
+    const uint32_t idesc = idesc_i8(TM, TN);
+    for (int k = 0; k < nk; ++k) {
+      const int s = k % NSTAGE;
+      if (!__all_sync(0xffffffffu, mbar_wait(full(s), (k / NSTAGE) & 1, abort_flag))) break;
+      tc_fence_after();
+      if (elect_one()) {
         const uint32_t base = s_op + s * STAGE;
+        const uint32_t first = (k > 0) ? 1u : 0u;
 #pragma unroll
-        for (int ks = 0; ks < KCH / 16; ++ks) {
-          const uint64_t ahi = sdesc_k_sw128(base + 0 * OPB + ks * 32), alo = sdesc_k_sw128(base + 1 * OPB + ks * 32);
-          const uint64_t bhi = sdesc_k_sw128(base + 2 * OPB + ks * 32), blo = sdesc_k_sw128(base + 3 * OPB + ks * 32);
-          umma_f16(tmem, ahi, bhi, idesc, (k | ks) ? 1u : 0u);
-          umma_f16(tmem, ahi, blo, idesc, 1u);
-          umma_f16(tmem, alo, bhi, idesc, 1u);
+        for (int sa = 0; sa < KS; ++sa) {
+#pragma unroll
+          for (int tb = 0; tb < KS - sa; ++tb) {
+#pragma unroll
+            for (int kk = 0; kk < KB / 32; ++kk) {
+              const uint64_t da = sdesc_k_sw64(base + sa * ASL + kk * 32);
+              const uint64_t db = sdesc_k_sw64(base + KS * ASL + tb * BSL + kk * 32);
+              // group sa + tb is opened by its sa == 0 product in the first k chunk
+              umma_i8(tmem + (uint32_t)((sa + tb) * TN), da, db, idesc, (sa > 0 || kk > 0) ? 1u : first);
+            }
+          }
         }
         umma_commit(empty(s));
       }
+      __syncwarp();
+    }
+    if (elect_one()) {
       umma_commit(done);
       umma_commit(drain);
       volatile int never = 0;
@@ -134,15 +178,26 @@ __global__ void __launch_bounds__(THREADS, 1)
     if (ok) {
       tc_fence_after();
       const int row = ti * TM + 32 * q + lane;
-      for (int c0 = 0; c0 < TM; c0 += 16) {
-        float v[16];
-        tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + c0, v);
-        tmem_wait_ld();
+      const int* ex = g.exps + (size_t)(k0 / MAX_CHUNKS) * g.rpad;
+      const int ep = ex[row];
+      for (int c0 = 0; c0 < TN; c0 += 16) {
+        double v[16];
+#pragma unroll
+        for (int e = 0; e < 16; ++e) v[e] = 0.0;
+#pragma unroll
+        for (int gi = KS - 1; gi >= 0; --gi) {
+          float raw[16];
+          tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(gi * TN + c0), raw);
+          tmem_wait_ld();
+#pragma unroll
+          for (int e = 0; e < 16; ++e) v[e] = v[e] * 0.0078125 + (double)__float_as_int(raw[e]);
+        }
         if (row < g.r) {
 #pragma unroll
           for (int e = 0; e < 16; ++e) {
-            const int col = tj * TM + c0 + e;
-            if (col < g.r && row <= col) atomicAdd(g.M + (long long)col * g.ldm + row, (double)v[e]);
+            const int col = tj * TN + c0 + e;
+            if (col < g.r && row <= col)
+              atomicAdd(g.M + (long long)col * g.ldm + row, ldexp(v[e], ep + ex[col] - 14));
           }
         }
       }
@@ -153,22 +208,64 @@ __global__ void __launch_bounds__(THREADS, 1)
   if (threadIdx.x == 0 && *abort_flag) atomicExch(g.status, DB200_ERR_TIMEOUT);
   if (warp == 1) {
     tc_fence_after();
-    tmem_dealloc(tmem, 128);
+    tmem_dealloc(tmem, TMEM_COLS);
   }
 }
 
-// Z~^T split into bf16 hi / lo, [rpad][npad] each: out[c][i] = sqrt(w_i) Z[i + c*ldz] (zero padding).
-__global__ void pack_scaled_t_kernel(const double* __restrict__ Z, long long ldz, const double* __restrict__ w, int n,
-                                     int r, int npad, int rpad, __nv_bfloat16* __restrict__ hi,
-                                     __nv_bfloat16* __restrict__ lo) {
-  const long long total = (long long)npad * rpad;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(e % npad), c = (int)(e / npad);
-    float x = 0.f;
-    if (i < n && c < r) x = (float)(sqrt(w ? w[i] : 1.0) * Z[i + (long long)c * ldz]);
-    const __nv_bfloat16 h = __float2bfloat16_rn(x);
-    hi[e] = h;
-    lo[e] = __float2bfloat16_rn(x - __bfloat162float(h));
+// sw[i] = sqrt(w_i) (1 without weights), computed once per Gram.
+__global__ void sqrt_weights_kernel(const double* __restrict__ w, int n, double* __restrict__ sw) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) sw[i] = w ? sqrt(w[i]) : 1.0;
+}
+
+// One CTA per (column p < rpad, chunk c): e_cp from the chunk's largest |sw_i Z[i, p]|, then the KS digit slices
+// [s][p][i] of the chunk (zero for padding rows and columns); one thread handles 8 consecutive rows at a time.
+// 1024 threads per CTA keep the chunks in flight (two per SM, 128 KB each) inside L2 for the second read.
+__global__ void __launch_bounds__(1024) slice_kernel(const double* __restrict__ Z, long long ldz,
+                                                    const double* __restrict__ sw, int n, int r, int npad, int rpad,
+                                                    int* __restrict__ exps, int8_t* __restrict__ slices) {
+  const int p = blockIdx.x, c = blockIdx.y;
+  const int i0 = c * CH, i1 = min(npad, i0 + CH);
+  const int iv = min(n, i1);  // rows below iv hold data
+  const double* col = Z + (long long)p * ldz;
+  __shared__ double part[32];
+  double m = 0.0;
+  if (p < r)
+    for (int i = i0 + threadIdx.x; i < iv; i += blockDim.x) m = fmax(m, fabs(sw[i] * col[i]));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if (threadIdx.x % 32 == 0) part[threadIdx.x / 32] = m;
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < 32; ++k) m = fmax(m, part[k]);
+  const int e = exp_above(m);
+  if (threadIdx.x == 0) exps[(size_t)c * rpad + p] = e;
+  const double scale = ldexp(1.0, 7 * KS - e);  // |sw Z| 2^(7 KS - e) < 2^(7 KS): an exact fixed-point value
+  const size_t slice_bytes = (size_t)rpad * npad;
+  for (int i8 = i0 + 8 * threadIdx.x; i8 < i1; i8 += 8 * blockDim.x) {
+    uint32_t lo[KS], hi[KS];
+#pragma unroll
+    for (int s = 0; s < KS; ++s) lo[s] = hi[s] = 0u;
+    if (p < r && m > 0.0) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int i = i8 + j;
+        const double v = (i < iv) ? sw[i] * col[i] : 0.0;
+        const unsigned long long u = __double2ull_rz(fabs(v) * scale);  // floor(|x| 2^(7 KS)), x = v 2^-e
+        const bool neg = v < 0.0;
+#pragma unroll
+        for (int s = 0; s < KS; ++s) {
+          const uint32_t d = (uint32_t)(u >> (7 * (KS - 1 - s))) & 127u;  // digit s + 1 of |x| in base 128
+          const uint32_t byte = (neg ? (0u - d) : d) & 0xffu;
+          if (j < 4)
+            lo[s] |= byte << (8 * j);
+          else
+            hi[s] |= byte << (8 * (j - 4));
+        }
+      }
+    }
+#pragma unroll
+    for (int s = 0; s < KS; ++s)
+      *reinterpret_cast<uint2*>(slices + s * slice_bytes + (size_t)p * npad + i8) = make_uint2(lo[s], hi[s]);
   }
 }
 
@@ -185,60 +282,83 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
-bool tmap_rows(CUtensorMap* tm, const void* base, uint64_t inner, uint64_t rows) {
+// 3-D map over the slices (x = i bytes, y = p, z = slice), box 64 bytes x box_rows x KS, 64-byte swizzle.
+bool tmap_slices(CUtensorMap* tm, const void* base, uint64_t npad, uint64_t rpad, uint32_t box_rows) {
   auto enc = encode_fn();
   if (!enc) return false;
-  cuuint64_t dims[2] = {inner, rows};
-  cuuint64_t strides[1] = {inner * 2};
-  cuuint32_t box[2] = {KCH, TM};
-  cuuint32_t estr[2] = {1, 1};
-  return enc(tm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
-             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+  cuuint64_t dims[3] = {npad, rpad, (cuuint64_t)KS};
+  cuuint64_t strides[2] = {npad, npad * rpad};
+  cuuint32_t box[3] = {(cuuint32_t)KB, box_rows, (cuuint32_t)KS};
+  cuuint32_t estr[3] = {1, 1, 1};
+  return enc(tm, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void*>(base), dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 }  // namespace
 
 size_t gram_tc_scratch_bytes(int n, int r) {
-  const size_t npad = (size_t)round_up(n, KCH), rpad = (size_t)round_up(r, TM);
-  return 2 * align_up(npad * rpad * 2, 256) + 512;
+  const size_t npad = (size_t)round_up(n, KB), rpad = (size_t)round_up(r, TM);
+  const size_t nchunk = (npad + CH - 1) / CH;
+  return align_up((size_t)KS * npad * rpad, 256) + align_up(nchunk * rpad * sizeof(int), 256) +
+         align_up((size_t)n * sizeof(double), 256) + 512;
 }
 
 // M (upper triangle, FP64, r x r) += Z~^T Z~ with Z~ = diag(sqrt(w)) Z.  `scratch` holds gram_tc_scratch_bytes.
 int gram_tc_weighted(db200_context* ctx, int n, int r, const double* Z, long long ldz, const double* w, double* M,
                      int ldm, void* scratch) {
-  const int npad = round_up(n, KCH), rpad = round_up(r, TM);
+  if (n <= 0 || r <= 0) return DB200_OK;
+  const int npad = round_up(n, KB), rpad = round_up(r, TM);
+  const int nchunk = (npad + CH - 1) / CH;
   Carve cv{static_cast<char*>(scratch)};
-  __nv_bfloat16* hi = cv.take<__nv_bfloat16>((size_t)npad * rpad);
-  __nv_bfloat16* lo = cv.take<__nv_bfloat16>((size_t)npad * rpad);
-  const long long total = (long long)npad * rpad;
-  long long blocks = (total + 255) / 256;
-  if (blocks > 16LL * ctx->num_sms) blocks = 16LL * ctx->num_sms;
-  pack_scaled_t_kernel<<<(unsigned)blocks, 256, 0, ctx->stream>>>(Z, ldz, w, n, r, npad, rpad, hi, lo);
+  int8_t* slices = cv.take<int8_t>((size_t)KS * npad * rpad);
+  int* exps = cv.take<int>((size_t)nchunk * rpad);
+  double* sw = cv.take<double>(n);
+  sqrt_weights_kernel<<<(unsigned)std::min((n + 255) / 256, 1024), 256, 0, ctx->stream>>>(w, n, sw);
   DB200_CUDA(ctx, cudaGetLastError());
   count_launch(ctx);
-  CUtensorMap thi, tlo;
-  if (!tmap_rows(&thi, hi, npad, rpad) || !tmap_rows(&tlo, lo, npad, rpad))
+  slice_kernel<<<dim3(rpad, nchunk), 1024, 0, ctx->stream>>>(Z, ldz, sw, n, r, npad, rpad, exps, slices);
+  DB200_CUDA(ctx, cudaGetLastError());
+  count_launch(ctx);
+  CUtensorMap ta, tb;
+  if (!tmap_slices(&ta, slices, npad, rpad, TM) || !tmap_slices(&tb, slices, npad, rpad, TN))
     return fail(ctx, DB200_ERR_CUDA, "gram_tc: cuTensorMapEncodeTiled failed");
   GramArgs a;
   a.r = r;
-  a.ntiles = rpad / TM;
-  a.kchunks = npad / KCH;
-  const int pairs = a.ntiles * (a.ntiles + 1) / 2;
-  int splits = (2 * ctx->num_sms + pairs - 1) / pairs;
-  if (splits > a.kchunks) splits = a.kchunks;
-  if (splits < 1) splits = 1;
-  a.chunks_per_split = (a.kchunks + splits - 1) / splits;
-  splits = (a.kchunks + a.chunks_per_split - 1) / a.chunks_per_split;
+  a.rpad = rpad;
+  a.exps = exps;
+  const int np = rpad / TM;
+  a.nq = round_up(r, TN) / TN;
+  a.kchunks = npad / KB;
+  const int pairs = np * a.nq - np * (np - 1);
+  // k range per CTA: a power of two of 64-row chunks dividing the scaling chunk; pick the one with the least
+  // modelled time, waves x (chunks per CTA + 8), the 8 standing for a CTA's fill and epilogue
+  {
+    const int sms = ctx->num_sms;
+    long long best = -1;
+    int best_cps = MAX_CHUNKS;
+    for (int cps = MAX_CHUNKS; cps >= 4; cps /= 2) {
+      const long long splits = (a.kchunks + cps - 1) / cps;
+      const long long waves = (splits * pairs + sms - 1) / sms;
+      const long long cost = waves * (long long)(cps + 8);
+      if (best < 0 || cost < best) {
+        best = cost;
+        best_cps = cps;
+      }
+    }
+    a.chunks_per_split = best_cps;
+  }
+  const int splits = (a.kchunks + a.chunks_per_split - 1) / a.chunks_per_split;
+  if (splits > 65535) return fail(ctx, DB200_ERR_UNSUPPORTED, "gram_tc: too many row splits");
   a.M = M;
   a.ldm = ldm;
   a.status = ctx->d_status;
   const size_t smem = NSTAGE * STAGE + 512 + 1024;
-  DB200_CUDA(ctx, cudaFuncSetAttribute(gram_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  DB200_CUDA(ctx, cudaFuncSetAttribute(gram_i8_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   dim3 grid(pairs, splits);
   cudaEvent_t e0 = nullptr;
   prof_begin(ctx, &e0);
-  gram_tc_kernel<<<grid, THREADS, smem, ctx->stream>>>(thi, tlo, a);
+  gram_i8_kernel<<<grid, THREADS, smem, ctx->stream>>>(ta, tb, a);
   DB200_CUDA(ctx, cudaGetLastError());
   prof_end(ctx, e0);
   count_launch(ctx);

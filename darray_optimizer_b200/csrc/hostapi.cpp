@@ -211,7 +211,7 @@ int db200_gram_weighted(db200_context* ctx, int n, int r, const double* Z, int l
   if (!use_tensor_cores) return gram<double, double>(ctx, n, r, r, Z, ldz, Z, ldz, w, 1.0, 0.0, M, ldm, true);
   void* scratch = slot_buffer(ctx, SLOT_SPARE, gram_tc_scratch_bytes(n, r));
   if (!scratch) return DB200_ERR_NOMEM;
-  for (int j = 0; j < r; ++j) DB200_CUDA(ctx, cudaMemsetAsync(M + (size_t)j * ldm, 0, sizeof(double) * r, ctx->stream));
+  DB200_CUDA(ctx, cudaMemset2DAsync(M, sizeof(double) * ldm, 0, sizeof(double) * r, r, ctx->stream));
   return gram_tc_weighted(ctx, n, r, Z, ldz, w, M, ldm, scratch);
 }
 

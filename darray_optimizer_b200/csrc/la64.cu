@@ -13,9 +13,6 @@ namespace db200 {
 
 namespace {
 
-constexpr int TB = 64;  // output tile
-constexpr int TK = 16;  // k step
-
 template <typename T>
 __device__ __forceinline__ double ld64(const T* p) { return (double)__ldg(p); }
 
@@ -146,61 +143,100 @@ __global__ void __launch_bounds__(GTHREADS, 1) gram_kernel(int n, int p, int q, 
   }
 }
 
-// C[n x q] = A[n x p] * op(B) (+ beta * C);  op(B) = B (p x q) or B^T (B is q x p) when transB.
+// C[n x q] = alpha * A[n x p] * op(B) + beta * C (op(B) = B, p x q, or B^T with B q x p when transB) on the FP64
+// tensor cores: one 128 x 128 tile of C per CTA with the whole reduction over p inside it, the warp layout and
+// m16n8k8 fragments of gram_kernel.  Stages of 8 columns of A (128 contiguous rows each, one coalesced 256-byte
+// read per warp and column) and 8 rows of op(B) are fetched into registers one stage ahead and parked k-major in
+// a double-buffered shared tile.
 template <typename TA, typename TC>
-__global__ void __launch_bounds__(256) gemm_nn_kernel(int n, int p, int q, const TA* __restrict__ A, long long lda,
-                                                      const double* __restrict__ B, int ldb, int transB,
-                                                      double alpha, double beta, TC* C, long long ldc) {
-  const int i0 = blockIdx.x * TB, j0 = blockIdx.y * TB;
-  __shared__ double sA[TK][TB + 1];
-  __shared__ double sB[TK][TB + 1];
-  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-  double acc[4][4];
+__global__ void __launch_bounds__(GTHREADS, 1) tall_kernel(int n, int p, int q, const TA* __restrict__ A, long long lda,
+                                                           const double* __restrict__ B, int ldb, int transB,
+                                                           double alpha, double beta, TC* C, long long ldc) {
+  const int i0 = blockIdx.x * GT, j0 = blockIdx.y * GT;
+  __shared__ __align__(16) double sA[2][GK][GPAD];
+  __shared__ __align__(16) double sB[2][GK][GPAD];
+  const int lane = threadIdx.x % 32, warp = threadIdx.x / 32;
+  const int wm = warp / 2, wn = warp % 2;
+  const int fr = lane / 4, fk = lane % 4;
+  double acc[2][8][4];
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
+  for (int a = 0; a < 2; ++a)
 #pragma unroll
-    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
-  for (int k0 = 0; k0 < p; k0 += TK) {
-    // A tile 64 rows x 16 k: consecutive threads -> consecutive rows (coalesced)
+    for (int b = 0; b < 8; ++b)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) acc[a][b][e] = 0.0;
+  // A: column k0 + ak, rows i0 + ar + 32 s.  op(B): row k0 + bk, columns j0 + bj + 32 s (B^T rows are contiguous
+  // in j, B's columns contiguous in k: consecutive threads walk the contiguous index either way).
+  const int ak = threadIdx.x / 32, ar = threadIdx.x % 32;
+  const int bk = transB ? threadIdx.x / 32 : threadIdx.x % GK;
+  const int bj = transB ? threadIdx.x % 32 : threadIdx.x / GK;
+  double va[4], vb[4];
+  auto fetch = [&](int k0) {
+    const int ka = k0 + ak, kb = k0 + bk;
 #pragma unroll
     for (int s = 0; s < 4; ++s) {
-      const int e = threadIdx.x + 256 * s;
-      const int r = e % TB, kk = e / TB;
-      const int i = i0 + r, k = k0 + kk;
-      sA[kk][r] = (i < n && k < p) ? ld64(A + (long long)k * lda + i) : 0.0;
-      const int jc = e % TB;
-      const int j = j0 + jc;
-      double bv = 0.0;
-      if (j < q && k < p) bv = transB ? B[(long long)k * ldb + j] : B[(long long)j * ldb + k];
-      sB[kk][jc] = bv;
+      const int i = i0 + ar + 32 * s, j = j0 + bj + 32 * s;
+      va[s] = (ka < p && i < n) ? ld64(A + (long long)ka * lda + i) : 0.0;
+      vb[s] = (kb < p && j < q) ? (transB ? B[(long long)kb * ldb + j] : B[(long long)j * ldb + kb]) : 0.0;
     }
-    __syncthreads();
+  };
+  auto park = [&](int buf) {
 #pragma unroll
-    for (int t = 0; t < TK; ++t) {
-      double av[4], bv[4];
-#pragma unroll
-      for (int a = 0; a < 4; ++a) av[a] = sA[t][ty + 16 * a];
-#pragma unroll
-      for (int b = 0; b < 4; ++b) bv[b] = sB[t][tx * 4 + b];
-#pragma unroll
-      for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
+    for (int s = 0; s < 4; ++s) {
+      sA[buf][ak][ar + 32 * s] = va[s];
+      sB[buf][bk][bj + 32 * s] = vb[s];
     }
+  };
+  int buf = 0;
+  fetch(0);
+  park(0);
+  __syncthreads();
+  for (int k0 = 0; k0 < p; k0 += GK) {
+    const bool more = k0 + GK < p;
+    if (more) fetch(k0 + GK);
+    {
+      double af[2][4], bf[8][2];
+#pragma unroll
+      for (int a = 0; a < 2; ++a) {
+        const int r = 32 * wm + 16 * a + fr;
+        af[a][0] = sA[buf][fk][r];
+        af[a][1] = sA[buf][fk][r + 8];
+        af[a][2] = sA[buf][fk + 4][r];
+        af[a][3] = sA[buf][fk + 4][r + 8];
+      }
+#pragma unroll
+      for (int b = 0; b < 8; ++b) {
+        const int c = 64 * wn + 8 * b + fr;
+        bf[b][0] = sB[buf][fk][c];
+        bf[b][1] = sB[buf][fk + 4][c];
+      }
+#pragma unroll
+      for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 8; ++b) dmma16(acc[a][b], af[a], bf[b]);
+    }
+    if (more) park(buf ^ 1);
     __syncthreads();
+    buf ^= 1;
   }
 #pragma unroll
-  for (int a = 0; a < 4; ++a) {
-    const int i = i0 + ty + 16 * a;
-    if (i >= n) continue;
+  for (int a = 0; a < 2; ++a) {
 #pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      const int j = j0 + tx * 4 + b;
-      if (j >= q) continue;
-      TC* dst = C + (long long)j * ldc + i;
-      double v = alpha * acc[a][b];
-      if (beta != 0.0) v += beta * (double)*dst;
-      *dst = (TC)v;
+    for (int h = 0; h < 2; ++h) {
+      const int i = i0 + 32 * wm + 16 * a + 8 * h + fr;
+      if (i >= n) continue;
+#pragma unroll
+      for (int b = 0; b < 8; ++b) {
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int j = j0 + 64 * wn + 8 * b + 2 * fk + e;
+          if (j >= q) continue;
+          TC* dst = C + (long long)j * ldc + i;
+          double v = alpha * acc[a][b][2 * h + e];
+          if (beta != 0.0) v += beta * (double)*dst;
+          *dst = (TC)v;
+        }
+      }
     }
   }
 }
@@ -679,10 +715,10 @@ template <typename TA, typename TC>
 int gemm_tall(db200_context* ctx, int n, int p, int q, const TA* A, long long lda, const double* B, int ldb,
               bool transB, double beta, TC* C, long long ldc, double alpha) {
   if (n <= 0 || q <= 0) return DB200_OK;
-  dim3 grid((n + TB - 1) / TB, (q + TB - 1) / TB);
+  dim3 grid((n + GT - 1) / GT, (q + GT - 1) / GT);
   if (grid.y > 65535) return fail(ctx, DB200_ERR_UNSUPPORTED, "gemm_tall: q too large");
-  gemm_nn_kernel<TA, TC><<<grid, 256, 0, ctx->stream>>>(n, p, q, A, lda, B, ldb, transB ? 1 : 0, alpha, beta, C,
-                                                        ldc);
+  tall_kernel<TA, TC><<<grid, GTHREADS, 0, ctx->stream>>>(n, p, q, A, lda, B, ldb, transB ? 1 : 0, alpha, beta, C,
+                                                          ldc);
   DB200_CUDA(ctx, cudaGetLastError());
   count_launch(ctx);
   return DB200_OK;

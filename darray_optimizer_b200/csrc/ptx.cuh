@@ -88,6 +88,16 @@ __device__ __forceinline__ void tma_load_2d(uint32_t smem_dst, const void* tmap,
       : "memory");
 }
 
+// 3-D tiled load (box x, y, z; x innermost), completing on `bar`.
+__device__ __forceinline__ void tma_load_3d(uint32_t smem_dst, const void* tmap, uint32_t bar, int32_t x, int32_t y,
+                                            int32_t z) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];" ::
+          "r"(smem_dst),
+      "l"(tmap), "r"(bar), "r"(x), "r"(y), "r"(z)
+      : "memory");
+}
+
 __device__ __forceinline__ void prefetch_tmap(const void* tmap) {
   asm volatile("prefetch.tensormap [%0];" ::"l"(tmap) : "memory");
 }
@@ -130,6 +140,18 @@ __device__ __forceinline__ void umma_f16_ts(uint32_t d_tmem, uint32_t a_tmem, ui
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d_tmem),
       "r"(a_tmem), "l"(b_desc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+// D[tmem] (+)= A[smem desc] * B[smem desc]^T, kind::i8 (signed 8-bit inputs, K = 32 per instruction, exact s32
+// accumulation).
+__device__ __forceinline__ void umma_i8(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                        uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
       : "memory");
 }
 
@@ -316,6 +338,27 @@ __device__ __forceinline__ uint64_t sdesc_k_sw128(uint32_t smem_addr) {
   d |= (uint64_t)1 << 46;             // descriptor version for sm_100
   d |= (uint64_t)2 << 61;             // SWIZZLE_128B
   return d;
+}
+
+// Shared-memory matrix descriptor for a K-major operand in the 64-byte swizzle: rows of 64 bytes, 8-row atoms of
+// 512 bytes (SBO), atoms contiguous; the K offset inside the row is added to the start address.
+__device__ __forceinline__ uint64_t sdesc_k_sw64(uint32_t smem_addr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((smem_addr & 0x3FFFFu) >> 4);
+  d |= (uint64_t)1 << 16;            // LBO (unused for swizzled K-major)
+  d |= (uint64_t)(512u >> 4) << 32;  // SBO
+  d |= (uint64_t)1 << 46;            // descriptor version for sm_100
+  d |= (uint64_t)4 << 61;            // SWIZZLE_64B
+  return d;
+}
+
+// Instruction descriptor, kind::i8: A/B signed 8-bit (fmt 1), D s32 (fmt 2), both K-major.
+__host__ __device__ constexpr uint32_t idesc_i8(int M, int N) {
+  return (2u << 4)                      // D format s32
+         | (1u << 7)                    // A signed
+         | (1u << 10)                   // B signed
+         | ((uint32_t)(N >> 3) << 17)   // N / 8
+         | ((uint32_t)(M >> 4) << 24);  // M / 16
 }
 
 // Instruction descriptor, kind::f16: A/B bf16 (fmt 1) or f16 (fmt 0), D f32, both K-major.

@@ -216,7 +216,8 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
       if (dmax / dmin > 1e18) break;  // tests/testsvm.cpp:258-263
       const double lastg = 0.5 * ww - suma - sumlog / t;
       // Newton direction s = -(Z Z^T + D)^-1 g by Woodbury.  Mixed: capacity matrix M = I + Z^T D^-1 Z on the
-      // tensor cores (split bf16) factored in FP64, then iterative refinement against the exact FP64 operator
+      // int8 tensor cores (Ozaki slices, ~1e-12 of the column norms) factored in FP64, then iterative refinement
+      // against the exact FP64 operator
       // until the relative residual is <= 1e-10; a step that does not get there is recomputed with the FP64
       // capacity matrix.  FP64: the capacity matrix on the FP64 pipes, no refinement.
       auto newton_dir = [&](bool use_tc, bool* converged) -> int {
@@ -231,10 +232,11 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
         if ((s2 = bar_add_identity(ctx, M, r, r))) return s2;
         if ((s2 = bar_gemv_t(ctx, n, r, Z, ldz, g, dinv, -1.0, u))) return s2;
         if (use_tc) {
-          // the split-bf16 Gram carries an error of ~1e-5 of its largest entries, which can exceed the identity
-          // floor; a relative diagonal shift (x10 until the FP64 Cholesky succeeds) keeps it positive definite
+          // the sliced Gram's error (~1e-12 of the column norms) can exceed the identity floor of a capacity
+          // matrix with a huge dynamic range; a relative diagonal shift (x10 until the FP64 Cholesky succeeds)
+          // keeps it positive definite
           DB200_CUDA(ctx, cudaMemcpyAsync(L, M, sizeof(double) * rr, cudaMemcpyDeviceToDevice, ctx->stream));
-          double eps = 1e-5;
+          double eps = 1e-11;
           for (int tries = 0; tries < 6; ++tries) {
             DB200_CUDA(ctx, cudaMemsetAsync(d_pair, 0, 2 * sizeof(int), ctx->stream));
             if ((s2 = potrf_upper(ctx, M, r, r, d_pair, d_pair + 1))) return s2;

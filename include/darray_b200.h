@@ -153,7 +153,8 @@ typedef struct db200_barrier_params {
 
 /* Precision of the path.
  * DB200_MIXED: kernel passes on the tensor cores in split bf16 (fp32 accumulation); the Woodbury capacity matrix
- *   I + Z^T D^-1 Z formed on the tensor cores (split bf16) and factored in FP64 while each Newton step refined
+ *   I + Z^T D^-1 Z formed exactly in integers on the int8 tensor cores from 7 signed 7-bit slices of every column
+ *   (Ozaki scheme, error ~1e-12 of the column norms) and factored in FP64 while each Newton step refined
  *   against the exact FP64 operator (Z Z^T + D) reaches relative residual 1e-10, the FP64 capacity matrix after;
  *   objective, gradients, gap and line search in FP64.
  * DB200_FP64: plain FP64 everywhere (FP64 kernel blocks and products, FP64 capacity matrix): the comparator. */
@@ -243,7 +244,8 @@ DB200_API int db200_woodbury_solve(db200_context* ctx, int n, int r, const doubl
 
 /* Upper triangle of M(r x r) = Z^T diag(w) Z for Z n x r FP64 (w may be NULL = ones): the capacity-matrix
  * SYRK of the Woodbury Newton step (symmetric_update, include/cblas_like.h:62-69, with a row weight).
- * use_tensor_cores = 0: FP64 pipes; 1: tcgen05 split bf16 (hi.hi + hi.lo + lo.hi, relative error ~1e-5).
+ * use_tensor_cores = 0: FP64 pipes (mma.sync f64); 1: tcgen05 kind::i8 on 7 signed 7-bit slices per value with
+ * exact s32 sums (Ozaki scheme; error ~1e-12 ||z_p|| ||z_q||, z_p = column p of diag(sqrt(w)) Z).
  * Stream-ordered. */
 DB200_API int db200_gram_weighted(db200_context* ctx, int n, int r, const double* Z, int ldz, const double* w,
                                   double* M, int ldm, int use_tensor_cores);

@@ -198,7 +198,8 @@ def test_gemm_matches_numpy(gpu_ctx, ta, tb):
 
 @pytest.mark.parametrize("n,r,tc", [(2048, 56, 1), (5000, 300, 1), (131, 70, 1), (5000, 300, 0)])
 def test_gram_weighted_matches_numpy(gpu_ctx, n, r, tc):
-    """Capacity-matrix SYRK Z^T diag(w) Z: FP64 pipes to 1e-13, tensor-core split bf16 to 1e-5 (upper triangle)."""
+    """Capacity-matrix SYRK Z^T diag(w) Z: FP64 pipes to 1e-13, int8 tensor cores (7 Ozaki slices) to 1e-11
+    (upper triangle)."""
     import torch
     g = np.random.default_rng(n + r)
     Z = g.standard_normal((n, r)) * 0.3
@@ -210,4 +211,32 @@ def test_gram_weighted_matches_numpy(gpu_ctx, n, r, tc):
     gpu_ctx.sync()
     M = np.triu(h64(dM, r))
     ref = np.triu(Z.T @ (w[:, None] * Z))
-    assert rel(M, ref) < (1e-5 if tc else 1e-13)
+    assert rel(M, ref) < (1e-11 if tc else 1e-13)
+
+
+@pytest.mark.parametrize("n,r,spread", [(3000, 56, 6.0), (1500, 150, 30.0), (131, 70, 6.0), (4096, 200, 2.0),
+                                         (40000, 40, 10.0)])
+def test_gram_int8_matches_sliced_oracle(gpu_ctx, n, r, spread):
+    """The int8 tensor-core Gram equals the exact-integer CPU restatement of the same slicing up to FP64 rounding
+    of the final scaling and the split-k atomic additions, including a zero column and zero weights, with weights
+    spanning up to 1e26 (the barrier's D^-1 late in a solve)."""
+    import torch
+    from oracle import ozaki
+    g = np.random.default_rng(n + r + int(spread))
+    Z = g.standard_normal((n, r)) * np.exp(g.uniform(-3, 3, r))[None, :]
+    Z[:, r // 3] = 0.0
+    w = np.exp(g.uniform(-spread, spread, n))
+    w[::17] = 0.0
+    dZ, dw = d64(Z), torch.from_numpy(w).cuda()
+    dM = d64(np.zeros((r, r)))
+    gpu_ctx.gram_weighted(n, r, dZ.data_ptr(), n, dw.data_ptr(), dM.data_ptr(), r, 1)
+    gpu_ctx.sync()
+    M = h64(dM, r)
+    S = ozaki.sliced_gram(Z, w, 8)
+    exact = Z.T @ (w[:, None] * Z)
+    d = np.sqrt(np.diag(exact))
+    scale = np.outer(d, d) + 1e-300
+    iu = np.triu_indices(r)
+    assert np.max(np.abs(M - S)[iu] / scale[iu]) < 1e-14
+    assert np.max(np.abs(M - exact)[iu] / scale[iu]) < 1e-11
+    assert np.all(np.tril(M, -1) == 0)

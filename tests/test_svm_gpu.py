@@ -51,7 +51,8 @@ def test_barrier_matches_oracle_on_same_factor(gpu_ctx, c1_small, precision):
     p = gpu_ctx.barrier_params(precision=precision)
     rep = gpu_ctx.svm_barrier(n, r, dZ.data_ptr(), n, dy.data_ptr(), w.C, da.data_ptr(), params=p)
     if precision == 0:
-        assert rep.refine > 0
+        # the int8 (Ozaki) capacity matrix is accurate enough that no Newton step falls back to the FP64 one
+        assert rep.fallbacks == 0
     a = da.cpu().numpy()
     assert rep.status == 0
     tol = 1e-9 if precision == 1 else 1e-8  # mixed: Newton steps refined to relative residual 1e-10
