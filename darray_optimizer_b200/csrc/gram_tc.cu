@@ -23,6 +23,7 @@
 // still refines each Newton step against the exact FP64 operator and falls back to the FP64 Gram if refinement
 // stalls.
 #include <cuda.h>
+#include <cooperative_groups.h>
 #include <cudaTypedefs.h>
 #include <algorithm>
 #include <mutex>
@@ -47,6 +48,8 @@ constexpr int TMEM_COLS = 512;                 // KS * TN columns of s32 groups
 constexpr int THREADS = 192;                   // warp 0 TMA, warp 1 MMA, warps 2..5 epilogue
 static_assert(KS * TN <= TMEM_COLS, "group accumulators exceed TMEM");
 static_assert((long long)KS * MAX_CHUNKS * KB * 127 * 127 < (1LL << 31), "s32 group sums could overflow");
+constexpr int SLICE_CTAS = 4;                  // CTAs (of 256 threads x 16 rows) per scaling chunk
+static_assert(SLICE_CTAS * 256 * 16 == CH, "slice_kernel covers a scaling chunk per cluster");
 
 struct GramArgs {
   int r;                // valid rows / columns of M
@@ -217,55 +220,82 @@ __global__ void sqrt_weights_kernel(const double* __restrict__ w, int n, double*
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) sw[i] = w ? sqrt(w[i]) : 1.0;
 }
 
-// One CTA per (column p < rpad, chunk c): e_cp from the chunk's largest |sw_i Z[i, p]|, then the KS digit slices
-// [s][p][i] of the chunk (zero for padding rows and columns); one thread handles 8 consecutive rows at a time.
-// 1024 threads per CTA keep the chunks in flight (two per SM, 128 KB each) inside L2 for the second read.
-__global__ void __launch_bounds__(1024) slice_kernel(const double* __restrict__ Z, long long ldz,
-                                                    const double* __restrict__ sw, int n, int r, int npad, int rpad,
-                                                    int* __restrict__ exps, int8_t* __restrict__ slices) {
-  const int p = blockIdx.x, c = blockIdx.y;
-  const int i0 = c * CH, i1 = min(npad, i0 + CH);
-  const int iv = min(n, i1);  // rows below iv hold data
+// One cluster of SLICE_CTAS CTAs (256 threads each) per (column p < rpad, chunk c of 16384 rows); each thread holds
+// 16 consecutive rows in registers.  The CTAs exchange their largest |sw_i Z[i, p]| through distributed shared
+// memory, which gives e_cp; then every thread writes its 16 bytes of each of the KS digit slices [s][p][i] (zero
+// for padding rows and columns).  Four CTAs per SM overlap one CTA's loads with another's stores.  VEC: Z and ldz
+// allow 16-byte loads.
+template <bool VEC>
+__global__ void __cluster_dims__(1, SLICE_CTAS, 1) __launch_bounds__(256)
+    slice_kernel(const double* __restrict__ Z, long long ldz, const double* __restrict__ sw, int n, int r, int npad,
+                 int rpad, int* __restrict__ exps, int8_t* __restrict__ slices) {
+  constexpr int RPT = 16;  // rows per thread
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  const int rank = (int)cluster.block_rank();
+  const int p = blockIdx.x, c = blockIdx.y / SLICE_CTAS;
+  const int i0 = c * CH + (rank * 256 + threadIdx.x) * RPT;
   const double* col = Z + (long long)p * ldz;
-  __shared__ double part[32];
+  double v[RPT];
+  if (p < r && VEC && i0 + RPT <= n) {
+#pragma unroll
+    for (int j = 0; j < RPT; j += 2) {
+      const double2 z = __ldg(reinterpret_cast<const double2*>(col + i0 + j));
+      const double2 ww = __ldg(reinterpret_cast<const double2*>(sw + i0 + j));
+      v[j] = ww.x * z.x;
+      v[j + 1] = ww.y * z.y;
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < RPT; ++j) v[j] = (p < r && i0 + j < n) ? sw[i0 + j] * col[i0 + j] : 0.0;
+  }
   double m = 0.0;
-  if (p < r)
-    for (int i = i0 + threadIdx.x; i < iv; i += blockDim.x) m = fmax(m, fabs(sw[i] * col[i]));
+#pragma unroll
+  for (int j = 0; j < RPT; ++j) m = fmax(m, fabs(v[j]));
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  __shared__ double part[8];
+  __shared__ double cta_max;
   if (threadIdx.x % 32 == 0) part[threadIdx.x / 32] = m;
   __syncthreads();
+  if (threadIdx.x == 0) {
 #pragma unroll
-  for (int k = 0; k < 32; ++k) m = fmax(m, part[k]);
+    for (int k = 1; k < 8; ++k) m = fmax(m, part[k]);
+    cta_max = m;
+  }
+  cluster.sync();
+#pragma unroll
+  for (int k = 0; k < SLICE_CTAS; ++k) m = fmax(m, *cluster.map_shared_rank(&cta_max, k));
+  cluster.sync();  // every CTA has read the others' maxima before any of them exits
   const int e = exp_above(m);
-  if (threadIdx.x == 0) exps[(size_t)c * rpad + p] = e;
-  const double scale = ldexp(1.0, 7 * KS - e);  // |sw Z| 2^(7 KS - e) < 2^(7 KS): an exact fixed-point value
+  if (rank == 0 && threadIdx.x == 0) exps[(size_t)c * rpad + p] = e;
+  if (i0 >= npad) return;
+  // floor(|x| 2^(7 KS)), x = v 2^-e in (-1, 1): exact fixed point below 2^(7 KS); the sign per byte lane
+  const double scale = ldexp(1.0, 7 * KS - e);
+  unsigned long long u[RPT];
+  uint32_t neg[RPT / 4];
+#pragma unroll
+  for (int j = 0; j < RPT; ++j) u[j] = (m > 0.0) ? __double2ull_rz(fabs(v[j]) * scale) : 0ull;
+#pragma unroll
+  for (int w4 = 0; w4 < RPT / 4; ++w4) {
+    uint32_t nm = 0;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) nm |= (v[4 * w4 + b] < 0.0 ? 0xffu : 0u) << (8 * b);
+    neg[w4] = nm;
+  }
   const size_t slice_bytes = (size_t)rpad * npad;
-  for (int i8 = i0 + 8 * threadIdx.x; i8 < i1; i8 += 8 * blockDim.x) {
-    uint32_t lo[KS], hi[KS];
 #pragma unroll
-    for (int s = 0; s < KS; ++s) lo[s] = hi[s] = 0u;
-    if (p < r && m > 0.0) {
+  for (int s = 0; s < KS; ++s) {
+    const int sh = 7 * (KS - 1 - s);  // digit s + 1 of |x| in base 128
+    uint32_t wd[RPT / 4];
 #pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const int i = i8 + j;
-        const double v = (i < iv) ? sw[i] * col[i] : 0.0;
-        const unsigned long long u = __double2ull_rz(fabs(v) * scale);  // floor(|x| 2^(7 KS)), x = v 2^-e
-        const bool neg = v < 0.0;
+    for (int w4 = 0; w4 < RPT / 4; ++w4) {
+      uint32_t word = 0;
 #pragma unroll
-        for (int s = 0; s < KS; ++s) {
-          const uint32_t d = (uint32_t)(u >> (7 * (KS - 1 - s))) & 127u;  // digit s + 1 of |x| in base 128
-          const uint32_t byte = (neg ? (0u - d) : d) & 0xffu;
-          if (j < 4)
-            lo[s] |= byte << (8 * j);
-          else
-            hi[s] |= byte << (8 * (j - 4));
-        }
-      }
+      for (int b = 0; b < 4; ++b) word |= ((uint32_t)(u[4 * w4 + b] >> sh) & 127u) << (8 * b);
+      wd[w4] = __vsub4(word ^ neg[w4], neg[w4]);  // two's complement of the negative lanes
     }
-#pragma unroll
-    for (int s = 0; s < KS; ++s)
-      *reinterpret_cast<uint2*>(slices + s * slice_bytes + (size_t)p * npad + i8) = make_uint2(lo[s], hi[s]);
+    *reinterpret_cast<uint4*>(slices + s * slice_bytes + (size_t)p * npad + i0) = make_uint4(wd[0], wd[1], wd[2], wd[3]);
   }
 }
 
@@ -317,7 +347,13 @@ int gram_tc_weighted(db200_context* ctx, int n, int r, const double* Z, long lon
   sqrt_weights_kernel<<<(unsigned)std::min((n + 255) / 256, 1024), 256, 0, ctx->stream>>>(w, n, sw);
   DB200_CUDA(ctx, cudaGetLastError());
   count_launch(ctx);
-  slice_kernel<<<dim3(rpad, nchunk), 1024, 0, ctx->stream>>>(Z, ldz, sw, n, r, npad, rpad, exps, slices);
+  const bool vec = (reinterpret_cast<uintptr_t>(Z) % 16 == 0) && (ldz % 2 == 0);
+  if (vec)
+    slice_kernel<true><<<dim3(rpad, nchunk * SLICE_CTAS), 256, 0, ctx->stream>>>(Z, ldz, sw, n, r, npad, rpad, exps,
+                                                                                slices);
+  else
+    slice_kernel<false><<<dim3(rpad, nchunk * SLICE_CTAS), 256, 0, ctx->stream>>>(Z, ldz, sw, n, r, npad, rpad, exps,
+                                                                                 slices);
   DB200_CUDA(ctx, cudaGetLastError());
   count_launch(ctx);
   CUtensorMap ta, tb;
