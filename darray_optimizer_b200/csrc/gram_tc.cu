@@ -49,7 +49,7 @@ constexpr int THREADS = 192;                   // warp 0 TMA, warp 1 MMA, warps 
 static_assert(KS * TN <= TMEM_COLS, "group accumulators exceed TMEM");
 static_assert((long long)KS * MAX_CHUNKS * KB * 127 * 127 < (1LL << 31), "s32 group sums could overflow");
 constexpr int SLICE_CTAS = 4;                  // CTAs (of 256 threads x 16 rows) per scaling chunk
-static_assert(SLICE_CTAS * 256 * 16 == CH, "slice_kernel covers a scaling chunk per cluster");
+static_assert(SLICE_CTAS * 256 * 16 == CH && CH / SLICE_CTAS == 256 * 16, "slice_kernel covers a chunk per cluster");
 
 struct GramArgs {
   int r;                // valid rows / columns of M
@@ -220,42 +220,46 @@ __global__ void sqrt_weights_kernel(const double* __restrict__ w, int n, double*
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) sw[i] = w ? sqrt(w[i]) : 1.0;
 }
 
-// One cluster of SLICE_CTAS CTAs (256 threads each) per (column p < rpad, chunk c of 16384 rows); each thread holds
-// 16 consecutive rows in registers.  The CTAs exchange their largest |sw_i Z[i, p]| through distributed shared
-// memory, which gives e_cp; then every thread writes its 16 bytes of each of the KS digit slices [s][p][i] (zero
-// for padding rows and columns).  Four CTAs per SM overlap one CTA's loads with another's stores.  VEC: Z and ldz
-// allow 16-byte loads.
+// One cluster of SLICE_CTAS CTAs (256 threads, 4096 rows each) per (column p < rpad, chunk c of 16384 rows).
+//  1. Each thread loads 8 coalesced pairs of rows (lanes read adjacent 16-byte pairs) and keeps them in registers.
+//  2. The CTAs exchange their largest |sw_i Z[i, p]| through distributed shared memory, which gives e_cp.
+//  3. Each thread turns its 16 values into KS digits and parks them in a shared [KS][4096] byte tile.
+//  4. The CTA writes every slice row out with coalesced 16-byte stores (zero for padding rows and columns).
+// VEC: Z and ldz allow 16-byte loads.
 template <bool VEC>
 __global__ void __cluster_dims__(1, SLICE_CTAS, 1) __launch_bounds__(256)
     slice_kernel(const double* __restrict__ Z, long long ldz, const double* __restrict__ sw, int n, int r, int npad,
                  int rpad, int* __restrict__ exps, int8_t* __restrict__ slices) {
-  constexpr int RPT = 16;  // rows per thread
+  constexpr int ROWS = CH / SLICE_CTAS;  // 4096 rows per CTA
+  constexpr int ROUNDS = ROWS / 512;     // 8 rounds of 2 rows per thread
   namespace cg = cooperative_groups;
   cg::cluster_group cluster = cg::this_cluster();
   const int rank = (int)cluster.block_rank();
   const int p = blockIdx.x, c = blockIdx.y / SLICE_CTAS;
-  const int i0 = c * CH + (rank * 256 + threadIdx.x) * RPT;
+  const int base = c * CH + rank * ROWS;  // first row of this CTA
   const double* col = Z + (long long)p * ldz;
-  double v[RPT];
-  if (p < r && VEC && i0 + RPT <= n) {
+  __shared__ __align__(16) uint8_t stage[KS][ROWS];
+  __shared__ double part[8];
+  __shared__ double cta_max;
+  double v[2 * ROUNDS];
 #pragma unroll
-    for (int j = 0; j < RPT; j += 2) {
-      const double2 z = __ldg(reinterpret_cast<const double2*>(col + i0 + j));
-      const double2 ww = __ldg(reinterpret_cast<const double2*>(sw + i0 + j));
-      v[j] = ww.x * z.x;
-      v[j + 1] = ww.y * z.y;
+  for (int q = 0; q < ROUNDS; ++q) {
+    const int i = base + 512 * q + 2 * threadIdx.x;
+    if (p < r && VEC && i + 2 <= n) {
+      const double2 z = __ldg(reinterpret_cast<const double2*>(col + i));
+      const double2 ww = __ldg(reinterpret_cast<const double2*>(sw + i));
+      v[2 * q] = ww.x * z.x;
+      v[2 * q + 1] = ww.y * z.y;
+    } else {
+      v[2 * q] = (p < r && i < n) ? sw[i] * col[i] : 0.0;
+      v[2 * q + 1] = (p < r && i + 1 < n) ? sw[i + 1] * col[i + 1] : 0.0;
     }
-  } else {
-#pragma unroll
-    for (int j = 0; j < RPT; ++j) v[j] = (p < r && i0 + j < n) ? sw[i0 + j] * col[i0 + j] : 0.0;
   }
   double m = 0.0;
 #pragma unroll
-  for (int j = 0; j < RPT; ++j) m = fmax(m, fabs(v[j]));
+  for (int j = 0; j < 2 * ROUNDS; ++j) m = fmax(m, fabs(v[j]));
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-  __shared__ double part[8];
-  __shared__ double cta_max;
   if (threadIdx.x % 32 == 0) part[threadIdx.x / 32] = m;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -269,33 +273,31 @@ __global__ void __cluster_dims__(1, SLICE_CTAS, 1) __launch_bounds__(256)
   cluster.sync();  // every CTA has read the others' maxima before any of them exits
   const int e = exp_above(m);
   if (rank == 0 && threadIdx.x == 0) exps[(size_t)c * rpad + p] = e;
-  if (i0 >= npad) return;
-  // floor(|x| 2^(7 KS)), x = v 2^-e in (-1, 1): exact fixed point below 2^(7 KS); the sign per byte lane
+  if (base >= npad) return;
+  // floor(|x| 2^(7 KS)) with x = v 2^-e in (-1, 1): an exact fixed-point value below 2^(7 KS); digit s + 1 of |x|
+  // in base 128 is bits [7 (KS - 1 - s), +7), negated (two's complement byte) for x < 0
   const double scale = ldexp(1.0, 7 * KS - e);
-  unsigned long long u[RPT];
-  uint32_t neg[RPT / 4];
 #pragma unroll
-  for (int j = 0; j < RPT; ++j) u[j] = (m > 0.0) ? __double2ull_rz(fabs(v[j]) * scale) : 0ull;
+  for (int q = 0; q < ROUNDS; ++q) {
+    const unsigned long long u0 = (m > 0.0) ? __double2ull_rz(fabs(v[2 * q]) * scale) : 0ull;
+    const unsigned long long u1 = (m > 0.0) ? __double2ull_rz(fabs(v[2 * q + 1]) * scale) : 0ull;
+    const uint32_t n0 = v[2 * q] < 0.0 ? 0xffu : 0u, n1 = v[2 * q + 1] < 0.0 ? 0xffu : 0u;
 #pragma unroll
-  for (int w4 = 0; w4 < RPT / 4; ++w4) {
-    uint32_t nm = 0;
-#pragma unroll
-    for (int b = 0; b < 4; ++b) nm |= (v[4 * w4 + b] < 0.0 ? 0xffu : 0u) << (8 * b);
-    neg[w4] = nm;
+    for (int s = 0; s < KS; ++s) {
+      const int sh = 7 * (KS - 1 - s);
+      const uint32_t d0 = (uint32_t)(u0 >> sh) & 127u, d1 = (uint32_t)(u1 >> sh) & 127u;
+      const uint32_t b0 = ((d0 ^ n0) - n0) & 0xffu, b1 = ((d1 ^ n1) - n1) & 0xffu;
+      *reinterpret_cast<uint16_t*>(&stage[s][512 * q + 2 * threadIdx.x]) = (uint16_t)(b0 | (b1 << 8));
+    }
   }
+  __syncthreads();
   const size_t slice_bytes = (size_t)rpad * npad;
 #pragma unroll
   for (int s = 0; s < KS; ++s) {
-    const int sh = 7 * (KS - 1 - s);  // digit s + 1 of |x| in base 128
-    uint32_t wd[RPT / 4];
-#pragma unroll
-    for (int w4 = 0; w4 < RPT / 4; ++w4) {
-      uint32_t word = 0;
-#pragma unroll
-      for (int b = 0; b < 4; ++b) word |= ((uint32_t)(u[4 * w4 + b] >> sh) & 127u) << (8 * b);
-      wd[w4] = __vsub4(word ^ neg[w4], neg[w4]);  // two's complement of the negative lanes
-    }
-    *reinterpret_cast<uint4*>(slices + s * slice_bytes + (size_t)p * npad + i0) = make_uint4(wd[0], wd[1], wd[2], wd[3]);
+    const int off = 16 * threadIdx.x;  // 256 threads x 16 bytes = one 4096-row slice row
+    if (base + off >= npad) break;     // npad is a multiple of 64: a 16-byte store is wholly inside or outside
+    *reinterpret_cast<uint4*>(slices + s * slice_bytes + (size_t)p * npad + base + off) =
+        *reinterpret_cast<const uint4*>(&stage[s][off]);
   }
 }
 
