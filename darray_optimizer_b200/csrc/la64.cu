@@ -242,7 +242,8 @@ __global__ void __launch_bounds__(GTHREADS, 1) tall_kernel(int n, int p, int q, 
 }
 
 // One block column of the right-looking blocked upper Cholesky: the kb x kb diagonal block (kb <= 64) is factored
-// in every CTA (redundantly; 64 steps with one barrier each, the block's elements in registers), CTA 0 writes
+// in every CTA (redundantly; 64 steps with one barrier each, the block's elements in registers, only a reciprocal
+// of the pivot on the sequential path, the row scaling by 1/sqrt(pivot) done for all rows afterwards), CTA 0 writes
 // R11 back (zeros below its diagonal), and CTA c >= 1 overwrites the 64 panel columns
 // [k0 + kb + 64 (c - 1), +64) with R11^-T A12 by forward substitution (one warp per 8 columns, the solution held
 // two rows per lane and broadcast by shuffles).  On a non-positive or NaN pivot nothing is written,
@@ -255,6 +256,7 @@ __global__ void __launch_bounds__(256) potrf_block_kernel(double* A, int lda, in
   __shared__ double rs[64][65];  // staging, then R11 (row-major: rs[i][j] = R[k0 + i][k0 + j])
   __shared__ double rowk[2][64];
   __shared__ double inv[64];
+  __shared__ double dsq[64];
   const int t = threadIdx.x;
   // stage the diagonal block coalesced (column j contiguous in i)
   for (int e = t; e < 64 * 64; e += 256) {
@@ -271,7 +273,8 @@ __global__ void __launch_bounds__(256) potrf_block_kernel(double* A, int lda, in
 #pragma unroll
   for (int k = 0; k < 64; ++k) {
     if (k >= kb) break;
-    if (rg == (k & 3)) rowk[k & 1][j] = a[k >> 2];
+    const double own = a[k >> 2];  // this thread's element of row k (used by the row's owners only)
+    if (rg == (k & 3)) rowk[k & 1][j] = own;
     __syncthreads();  // row k published; also orders the staging reads before the first rs write below
     const double piv = rowk[k & 1][k];
     if (!(piv > 0.0)) {  // the same value in every thread: a uniform exit
@@ -285,16 +288,26 @@ __global__ void __launch_bounds__(256) potrf_block_kernel(double* A, int lda, in
       const int i = rg + 4 * q;
       if (i > k) a[q] -= rowk[k & 1][i] * ckj;  // i > j entries are never read back
     }
-    if (rg == (k & 3)) {
-      const double s = sqrt(piv);
-      rs[k][j] = (j == k) ? s : ((j > k) ? a[k >> 2] / s : 0.0);
-      if (j == k) inv[k] = 1.0 / s;
-    }
+    if (rg == (k & 3)) rs[k][j] = (j >= k) ? own : 0.0;  // row k as eliminated (pivot at j == k)
   }
   if (failed) {
     if (blockIdx.x == 0 && t == 0 && atomicCAS(status, 0, DB200_ERR_NOT_SPD) == 0) *bad = k0;
     return;
   }
+  // R[k][j] = a_kj / sqrt(a_kk), off the sequential path: square roots first, then every row in parallel
+  __syncthreads();
+  if (t < kb) {
+    const double sd = sqrt(rs[t][t]);
+    dsq[t] = sd;
+    inv[t] = 1.0 / sd;
+  }
+  __syncthreads();
+  for (int e = t; e < kb * 64; e += 256) {
+    const int i = e >> 6, jj = e & 63;
+    if (jj > i) rs[i][jj] /= dsq[i];
+  }
+  __syncthreads();
+  if (t < kb) rs[t][t] = dsq[t];
   __syncthreads();
   if (blockIdx.x == 0) {
     for (int e = t; e < kb * 64; e += 256) {
@@ -333,6 +346,45 @@ __global__ void __launch_bounds__(256) potrf_block_kernel(double* A, int lda, in
     double* col = A + (long long)(c0 + cc) * lda + k0;
     if (lane < kb) col[lane] = v[cc][0];
     if (lane + 32 < kb) col[lane + 32] = v[cc][1];
+  }
+}
+
+// Trailing update of the blocked Cholesky: C[m x m] (upper triangle) -= P^T P for the kb x m panel P (kb <= 64, the
+// rows of R12 just solved).  One 32 x 32 tile of C per CTA (upper tiles only) so that the few hundred tiles of an
+// r ~ 500..4000 factor spread over the whole GPU; the two 64 x 32 panel slices sit in shared memory and each of the
+// 256 threads forms 4 outputs with 64-long FP64 dot products.
+__global__ void __launch_bounds__(256) syrk_update_kernel(const double* __restrict__ P, int ldp, int kb, int m,
+                                                          double* C, int ldc, const int* status) {
+  if (*(volatile const int*)status) return;
+  int idx = blockIdx.x, bi = 0;
+  const int nt = (m + 31) / 32;
+  while (idx >= nt - bi) {  // upper tile pairs (bi <= bj), row by row
+    idx -= nt - bi;
+    ++bi;
+  }
+  const int bj = bi + idx;
+  const int i0 = bi * 32, j0 = bj * 32;
+  __shared__ double pi[64][33], pj[64][33];
+  for (int e = threadIdx.x; e < 64 * 32; e += 256) {
+    const int k = e & 63, c = e >> 6;  // consecutive threads walk k: one column of P is contiguous
+    pi[k][c] = (k < kb && i0 + c < m) ? P[(long long)(i0 + c) * ldp + k] : 0.0;
+    pj[k][c] = (k < kb && j0 + c < m) ? P[(long long)(j0 + c) * ldp + k] : 0.0;
+  }
+  __syncthreads();
+  const int ti = threadIdx.x & 31, tj = threadIdx.x >> 5;  // rows ti; columns tj + 8 b
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 8
+  for (int k = 0; k < 64; ++k) {
+    const double a = pi[k][ti];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[b] = fma(a, pj[k][tj + 8 * b], acc[b]);
+  }
+  const int i = i0 + ti;
+  if (i >= m) return;
+#pragma unroll
+  for (int b = 0; b < 4; ++b) {
+    const int j = j0 + tj + 8 * b;
+    if (j < m && i <= j) C[(long long)j * ldc + i] -= acc[b];
   }
 }
 
@@ -742,12 +794,10 @@ int potrf_upper(db200_context* ctx, double* A, int lda, int l, int* d_status, in
     count_launch(ctx);
     if (rest > 0) {
       // trailing update A22 -= A12^T A12 (upper triangle only)
-      const int tp = (rest + GT - 1) / GT;
-      dim3 grid(tp, tp, 1);
-      gram_kernel<double, double><<<grid, GTHREADS, 0, ctx->stream>>>(kb, rest, rest, A + (long long)(k0 + kb) * lda + k0,
-                                                                 lda, A + (long long)(k0 + kb) * lda + k0, lda, nullptr,
-                                                                 -1.0, A + (long long)(k0 + kb) * lda + k0 + kb, lda,
-                                                                 kb, 1, 0);
+      const int nt = (rest + 31) / 32;
+      syrk_update_kernel<<<nt * (nt + 1) / 2, 256, 0, ctx->stream>>>(A + (long long)(k0 + kb) * lda + k0, lda, kb,
+                                                                     rest, A + (long long)(k0 + kb) * lda + k0 + kb,
+                                                                     lda, d_status);
       count_launch(ctx);
     }
   }
