@@ -422,9 +422,10 @@ __global__ void trinv_upper_kernel(const double* R, int ldr, int l, double* X, i
 //   mode 0: solve R^T y = b   (forward; row i of R^T = column i of R)
 //   mode 1: solve R x = y     (backward; row i of R = column i of L)
 // x/b in place, FP64, x staged in shared memory (l <= 4096).  Blocks of 32 rows: the 16 warps form the off-block
-// inner products (two rows each), then warp 0 solves the 32 x 32 triangle from registers it loaded before the
-// inner products (so the 32 sequential steps carry no memory latency), with the diagonal applied as a
-// reciprocal computed once per block.  Follows triangular_solve (include/blas_like.h:96-140) for one column.
+// inner products (two rows each; the coefficients of the nearest 256 columns are loaded before the block's
+// barrier, overlapping the previous block's triangle), then warp 0 solves the 32 x 32 triangle from registers it
+// also loaded before the barrier (so the 32 sequential steps carry no memory latency), with the diagonal applied
+// as a reciprocal computed once per block.  Follows triangular_solve (include/blas_like.h:96-140) for one column.
 __global__ void __launch_bounds__(512) trsv_kernel(const double* R, const double* L, int ld, int l, double* x,
                                                    int mode) {
   __shared__ double xs[4096];
@@ -444,28 +445,52 @@ __global__ void __launch_bounds__(512) trsv_kernel(const double* R, const double
 #pragma unroll
       for (int r = 0; r < 32; ++r) tri[r] = (lane < bl && r < bl) ? c[r] : 0.0;
     }
-    __syncthreads();  // xs of the previous block (and the initial staging) visible
-    // off-block contribution for rows i0 + warp and i0 + warp + 16
+    // off-block coefficients of rows i0 + warp and i0 + warp + 16: the nearest 32 PF (= 256) columns are loaded
+    // into registers before the barrier (they do not depend on x), so their latency overlaps the previous block's
+    // triangle; a longer range finishes in the loop after the barrier
+    constexpr int PF = 8;
+    double pf[2][PF];
+    int kbeg[2], kend[2];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       const int i = i0 + warp + 16 * h;
-      double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-      if (i < l) {
-        const double* col = T + (long long)i * ld;
-        const int kbeg = (mode == 0) ? 0 : i0 + 32, kend = (mode == 0) ? i0 : l;
-        int k = kbeg + lane;
-        for (; k + 96 < kend; k += 128) {
-          s0 += col[k] * xs[k];
-          s1 += col[k + 32] * xs[k + 32];
-          s2 += col[k + 64] * xs[k + 64];
-          s3 += col[k + 96] * xs[k + 96];
-        }
-        for (; k < kend; k += 32) s0 += col[k] * xs[k];
-      }
-      double s = (s0 + s1) + (s2 + s3);
+      kbeg[h] = (mode == 0) ? 0 : i0 + 32;
+      kend[h] = (i < l) ? ((mode == 0) ? i0 : l) : kbeg[h];
+      // mode 0 reads the columns just below i0 first (nearest the diagonal), mode 1 those just after i0 + 32
+      const double* col = T + (long long)(i < l ? i : 0) * ld;
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-      if (lane == 0) part[warp + 16 * h] = s;
+      for (int u = 0; u < PF; ++u) {
+        const int k = (mode == 0) ? kend[h] - 1 - lane - 32 * u : kbeg[h] + lane + 32 * u;
+        pf[h][u] = (k >= kbeg[h] && k < kend[h]) ? col[k] : 0.0;
+      }
+    }
+    __syncthreads();  // xs of the previous block (and the initial staging) visible
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int i = i0 + warp + 16 * h;
+      double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+      for (int u = 0; u < PF; ++u) {
+        const int k = (mode == 0) ? kend[h] - 1 - lane - 32 * u : kbeg[h] + lane + 32 * u;
+        if (k >= kbeg[h] && k < kend[h]) {
+          if (u & 1)
+            s1 += pf[h][u] * xs[k];
+          else
+            s0 += pf[h][u] * xs[k];
+        }
+      }
+      if (kend[h] - kbeg[h] > 32 * PF) {
+        const double* col = T + (long long)i * ld;
+        if (mode == 0) {
+          for (int k = kbeg[h] + lane; k < kend[h] - 32 * PF; k += 32) s0 += col[k] * xs[k];
+        } else {
+          for (int k = kbeg[h] + 32 * PF + lane; k < kend[h]; k += 32) s1 += col[k] * xs[k];
+        }
+      }
+      double sum = s0 + s1;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+      if (lane == 0) part[warp + 16 * h] = sum;
     }
     __syncthreads();
     if (warp == 0) {

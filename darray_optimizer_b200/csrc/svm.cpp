@@ -220,6 +220,7 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
       // against the exact FP64 operator
       // until the relative residual is <= 1e-10; a step that does not get there is recomputed with the FP64
       // capacity matrix.  FP64: the capacity matrix on the FP64 pipes, no refinement.
+      bool v_current = false;  // v already holds Z^T s (set by a converged refinement check)
       auto newton_dir = [&](bool use_tc, bool* converged) -> int {
         int s2;
         *converged = true;
@@ -268,6 +269,7 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
           const double rn = std::sqrt(h[0]), gn = std::sqrt(h[1]);
           if (rn <= 1e-10 * gn) {
             *converged = true;
+            v_current = true;  // v = Z^T s for the final s: the line search below reuses it
             break;
           }
           if (it == P.refine_max || (it > 0 && rn >= 0.5 * prev) || !std::isfinite(rn)) break;
@@ -284,15 +286,17 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
         return bar_step_stats(ctx, n, g, s, a, C, red);
       };
       bool conv = true;
+      v_current = false;
       if ((st = newton_dir(mixed && tc_ok, &conv))) return st;
       if (mixed && tc_ok && !conv) {
         // the barrier's D only grows more ill-conditioned with t: once the tensor-core preconditioner misses the
         // tolerance, the remaining Newton steps use the FP64 capacity matrix directly
         ++fallbacks_total;
         tc_ok = false;
+        v_current = false;
         if ((st = newton_dir(false, &conv))) return st;
       }
-      if ((st = bar_gemv_t(ctx, n, r, Z, ldz, s, nullptr, 1.0, v))) return st;
+      if (!v_current && (st = bar_gemv_t(ctx, n, r, Z, ldz, s, nullptr, 1.0, v))) return st;
       if ((st = bar_dot(ctx, r, w, v, sc + 1))) return st;
       if ((st = bar_dot(ctx, r, v, v, sc + 2))) return st;
       DB200_CUDA(ctx, cudaMemcpyAsync(red + 8, sc + 1, 2 * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
