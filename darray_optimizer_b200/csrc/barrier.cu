@@ -65,15 +65,19 @@ __device__ __forceinline__ double row_dot(const double* __restrict__ Z, long lon
 __global__ void __launch_bounds__(THREADS) grad_hess_kernel(int n, int r, const double* __restrict__ Z, long long ld,
                                                             const double* __restrict__ w, const double* __restrict__ a,
                                                             double C, double t, double* __restrict__ g,
-                                                            double* __restrict__ dinv, double* red) {
+                                                            double* __restrict__ dinv, double* red,
+                                                            const double* __restrict__ zw_in,
+                                                            double* __restrict__ zw_out) {
   __shared__ double sw[MAX_R_SMEM];
-  for (int k = threadIdx.x; k < r; k += blockDim.x) sw[k] = w[k];
+  if (!zw_in)
+    for (int k = threadIdx.x; k < r; k += blockDim.x) sw[k] = w[k];
   __syncthreads();
   double sums[2] = {0.0, 0.0};
   double dmax = 0.0, dmin = DBL_MAX;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const double ai = a[i], ci = C - ai;
-    const double zw = row_dot(Z, ld, i, r, sw);
+    const double zw = zw_in ? zw_in[i] : row_dot(Z, ld, i, r, sw);
+    if (zw_out) zw_out[i] = zw;
     g[i] = (zw - 1.0) + ((-1.0 / ai) + (1.0 / ci)) / t;
     const double D = ((1.0 / (ai * ai)) + (1.0 / (ci * ci))) / t;
     dinv[i] = 1.0 / D;
@@ -201,14 +205,16 @@ __global__ void __launch_bounds__(THREADS) residual_kernel(int n, int r, const d
                                                            const double* __restrict__ v, const double* __restrict__ g,
                                                            const double* __restrict__ dinv,
                                                            const double* __restrict__ s, double* __restrict__ res,
-                                                           double* red) {
+                                                           double* red, double* __restrict__ zv_out) {
   __shared__ double sv[MAX_R_SMEM];
   for (int k = threadIdx.x; k < r; k += blockDim.x) sv[k] = v[k];
   __syncthreads();
   double sums[2] = {0.0, 0.0};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const double gi = g[i];
-    const double ri = gi + row_dot(Z, ld, i, r, sv) + s[i] / dinv[i];
+    const double zv = row_dot(Z, ld, i, r, sv);
+    if (zv_out) zv_out[i] = zv;
+    const double ri = gi + zv + s[i] / dinv[i];
     res[i] = ri;
     sums[0] += ri * ri;
     sums[1] += gi * gi;
@@ -301,9 +307,10 @@ int bar_init_red(db200_context* ctx, double* red, int nsum, int nmax, int nmin) 
 }
 
 int bar_grad_hess(db200_context* ctx, int n, int r, const double* Z, long long ld, const double* w, const double* a,
-                  double C, double t, double* g, double* dinv, double* red) {
+                  double C, double t, double* g, double* dinv, double* red, const double* zw_in, double* zw_out) {
   if (r > MAX_R_SMEM) return fail(ctx, DB200_ERR_UNSUPPORTED, "barrier: rank > 4096");
-  grad_hess_kernel<<<rows_grid(ctx, n), THREADS, 0, ctx->stream>>>(n, r, Z, ld, w, a, C, t, g, dinv, red);
+  grad_hess_kernel<<<rows_grid(ctx, n), THREADS, 0, ctx->stream>>>(n, r, Z, ld, w, a, C, t, g, dinv, red, zw_in,
+                                                                   zw_out);
   DB200_CUDA(ctx, cudaGetLastError());
   count_launch(ctx);
   return DB200_OK;
@@ -351,8 +358,8 @@ int bar_terms(db200_context* ctx, int n, int r, const double* Z, long long ld, c
 }
 
 int bar_residual(db200_context* ctx, int n, int r, const double* Z, long long ld, const double* v, const double* g,
-                 const double* dinv, const double* s, double* res, double* red) {
-  residual_kernel<<<rows_grid(ctx, n), THREADS, 0, ctx->stream>>>(n, r, Z, ld, v, g, dinv, s, res, red);
+                 const double* dinv, const double* s, double* res, double* red, double* zv_out) {
+  residual_kernel<<<rows_grid(ctx, n), THREADS, 0, ctx->stream>>>(n, r, Z, ld, v, g, dinv, s, res, red, zv_out);
   DB200_CUDA(ctx, cudaGetLastError());
   count_launch(ctx);
   return DB200_OK;

@@ -7,9 +7,11 @@ namespace db200 {
 // red[0..nsum) = 0, next nmax = 0 (for maxima of non-negative values), next nmin = DBL_MAX.
 int bar_init_red(db200_context* ctx, double* red, int nsum, int nmax, int nmin);
 // g = Z w - 1 + (-1/a + 1/(C-a))/t,  dinv = 1/D,  D = (1/a^2 + 1/(C-a)^2)/t  (include/dbarrier.h:48-81);
-// red: [0] += sum a, [1] += sum(log a + log(C-a)), [2] max D, [3] min D.
+// red: [0] += sum a, [1] += sum(log a + log(C-a)), [2] max D, [3] min D.  zw_in: Z w given (no pass over Z);
+// zw_out: Z w stored.
 int bar_grad_hess(db200_context* ctx, int n, int r, const double* Z, long long ld, const double* w, const double* a,
-                  double C, double t, double* g, double* dinv, double* red);
+                  double C, double t, double* g, double* dinv, double* red, const double* zw_in = nullptr,
+                  double* zw_out = nullptr);
 // s = -dinv (g + Z u);  red: [0] += g.s, [1] += sum s, [2] min feasible step (init DBL_MAX).
 int bar_direction(db200_context* ctx, int n, int r, const double* Z, long long ld, const double* u, const double* g,
                   const double* dinv, const double* a, double C, double* s, double* red);
@@ -24,9 +26,10 @@ int bar_axpy(db200_context* ctx, int n, double alpha, const double* x, double* y
 int bar_terms(db200_context* ctx, int n, int r, const double* Z, long long ld, const double* w, const double* a,
               double C, double t, double* gf, double* gp, double* g, double* D, double* red);
 int bar_reciprocal(db200_context* ctx, int n, const double* x, double* y);
-// res = g + Z v + s/dinv (v = Z^T s: the negated Newton residual); red [0] += |res|^2, [1] += |g|^2
+// res = g + Z v + s/dinv (v = Z^T s: the negated Newton residual); red [0] += |res|^2, [1] += |g|^2; zv_out: Z v
+// stored
 int bar_residual(db200_context* ctx, int n, int r, const double* Z, long long ld, const double* v, const double* g,
-                 const double* dinv, const double* s, double* res, double* red);
+                 const double* dinv, const double* s, double* res, double* red, double* zv_out = nullptr);
 // red [0] += g.s, [1] += sum s, [2] min feasible step (init DBL_MAX)
 int bar_step_stats(db200_context* ctx, int n, const double* g, const double* s, const double* a, double C,
                    double* red);

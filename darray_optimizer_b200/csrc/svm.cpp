@@ -152,7 +152,7 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
   const size_t rr = (size_t)r * r;
   const bool mixed = (P.precision == DB200_MIXED);
   const size_t tc_bytes = mixed ? gram_tc_scratch_bytes(n, r) : 0;
-  const size_t bytes = 4096 + 5 * align_up((size_t)n * 8, 256) + 6 * align_up((size_t)r * 8, 256) +
+  const size_t bytes = 4096 + 7 * align_up((size_t)n * 8, 256) + 6 * align_up((size_t)r * 8, 256) +
                        2 * align_up(rr * 8, 256) + align_up(tc_bytes, 256) + 4096;
   char* base = static_cast<char*>(slot_buffer(ctx, SLOT_BAR, bytes));
   if (!base) return DB200_ERR_NOMEM;
@@ -172,6 +172,8 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
   double* L = cv.take<double>(rr);
   double* res = cv.take<double>(n);
   double* delta = cv.take<double>(n);
+  double* zw = cv.take<double>(n);  // Z w for the current w = Z^T a (valid while zw_ok)
+  double* zv = cv.take<double>(n);  // Z v for v = Z^T s, written by a refinement check
   void* tc_scratch = mixed ? static_cast<void*>(cv.take<char>(tc_bytes)) : nullptr;
   int refine_total = 0, fallbacks_total = 0;
   bool tc_ok = true;
@@ -200,15 +202,25 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
     return DB200_OK;
   };
   double fa = 0.0, suma_now = 0.0;
+  // In the mixed path an accepted step a += tau s with v = Z^T s and zv = Z v both current (a converged refinement
+  // check) updates w += tau v and zw += tau zv, which saves the two passes over Z that recompute them; the
+  // outer step's stop test recomputes both from a.
+  bool zw_ok = false;
   for (outer = 1; outer <= P.max_outer; ++outer) {
     int ni = 0;
     while (true) {
       ++ni;
       ++total_newton;
       // gradient / Hessian diagonal at a
-      if ((st = bar_gemv_t(ctx, n, r, Z, ldz, a, nullptr, 1.0, w))) return st;
-      if ((st = bar_init_red(ctx, red, 2, 1, 1))) return st;
-      if ((st = bar_grad_hess(ctx, n, r, Z, ldz, w, a, C, t, g, dinv, red))) return st;
+      if (zw_ok) {
+        if ((st = bar_init_red(ctx, red, 2, 1, 1))) return st;
+        if ((st = bar_grad_hess(ctx, n, r, Z, ldz, w, a, C, t, g, dinv, red, zw, nullptr))) return st;
+      } else {
+        if ((st = bar_gemv_t(ctx, n, r, Z, ldz, a, nullptr, 1.0, w))) return st;
+        if ((st = bar_init_red(ctx, red, 2, 1, 1))) return st;
+        if ((st = bar_grad_hess(ctx, n, r, Z, ldz, w, a, C, t, g, dinv, red, nullptr, zw))) return st;
+        zw_ok = true;
+      }
       if ((st = bar_dot(ctx, r, w, w, sc))) return st;
       DB200_CUDA(ctx, cudaMemcpyAsync(red + 8, sc, sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
       if ((st = fetch(red, 9))) return st;
@@ -264,7 +276,7 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
         for (int it = 0; it <= P.refine_max; ++it) {
           if ((s2 = bar_gemv_t(ctx, n, r, Z, ldz, s, nullptr, 1.0, v))) return s2;
           if ((s2 = bar_init_red(ctx, red + 16, 2, 0, 0))) return s2;
-          if ((s2 = bar_residual(ctx, n, r, Z, ldz, v, g, dinv, s, res, red + 16))) return s2;
+          if ((s2 = bar_residual(ctx, n, r, Z, ldz, v, g, dinv, s, res, red + 16, zv))) return s2;
           if ((s2 = fetch(red + 16, 2))) return s2;
           const double rn = std::sqrt(h[0]), gn = std::sqrt(h[1]);
           if (rn <= 1e-10 * gn) {
@@ -329,7 +341,15 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
         tau = ht[15] * P.beta;
       }
       if (accepted < 0) accepted = 0.0;  // no decrease found: stop this Newton loop below
-      if (accepted > 0 && (st = bar_axpy(ctx, n, accepted, s, a))) return st;
+      if (accepted > 0) {
+        if ((st = bar_axpy(ctx, n, accepted, s, a))) return st;
+        if (v_current) {
+          if ((st = bar_axpy(ctx, r, accepted, v, w))) return st;
+          if ((st = bar_axpy(ctx, n, accepted, zv, zw))) return st;
+        } else {
+          zw_ok = false;
+        }
+      }
       if (lam2 / 2 < P.newton_tol) break;
       if (accepted == 0.0) break;
       if (ni > 1 && (lastg - newg) < 1e-9 * std::fabs(newg)) break;
@@ -341,7 +361,8 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
     // f(a) for the barrier stop
     if ((st = bar_gemv_t(ctx, n, r, Z, ldz, a, nullptr, 1.0, w))) return st;
     if ((st = bar_init_red(ctx, red, 2, 1, 1))) return st;
-    if ((st = bar_grad_hess(ctx, n, r, Z, ldz, w, a, C, t, g, dinv, red))) return st;
+    if ((st = bar_grad_hess(ctx, n, r, Z, ldz, w, a, C, t, g, dinv, red, nullptr, zw))) return st;
+    zw_ok = true;
     if ((st = bar_dot(ctx, r, w, w, sc))) return st;
     DB200_CUDA(ctx, cudaMemcpyAsync(red + 8, sc, sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
     if ((st = fetch(red, 9))) return st;
