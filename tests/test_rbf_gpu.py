@@ -71,6 +71,10 @@ def test_rbf_block_symmetric_unit_diagonal(gpu_ctx):
     (300, 777, 128, 200),
     (512, 512, 64, 528),
     (130, 4096, 32, 138),
+    # wider than one tile-kernel panel: the cluster kernel, 1, 2 and 4 super-panels, ragged m, n and d
+    (700, 900, 100, 600),
+    (300, 257, 7, 1040),
+    (1024, 2048, 128, 2064),
 ])
 def test_rbf_sketch_matches_oracle(gpu_ctx, m, n, d, l):
     Xi = _points(m, d, 11, 0.5)
