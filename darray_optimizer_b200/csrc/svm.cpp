@@ -244,25 +244,22 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
         }
         if ((s2 = bar_add_identity(ctx, M, r, r))) return s2;
         if ((s2 = bar_gemv_t(ctx, n, r, Z, ldz, g, dinv, -1.0, u))) return s2;
-        if (use_tc) {
-          // the sliced Gram's error (~1e-12 of the column norms) can exceed the identity floor of a capacity
-          // matrix with a huge dynamic range; a relative diagonal shift (x10 until the FP64 Cholesky succeeds)
-          // keeps it positive definite
-          DB200_CUDA(ctx, cudaMemcpyAsync(L, M, sizeof(double) * rr, cudaMemcpyDeviceToDevice, ctx->stream));
-          double eps = 1e-11;
-          for (int tries = 0; tries < 6; ++tries) {
-            DB200_CUDA(ctx, cudaMemsetAsync(d_pair, 0, 2 * sizeof(int), ctx->stream));
-            if ((s2 = potrf_upper(ctx, M, r, r, d_pair, d_pair + 1))) return s2;
-            int pst = 0, bad = 0;
-            if ((s2 = read_status(ctx, d_pair, &pst, &bad))) return s2;
-            if (pst == 0) break;
-            DB200_CUDA(ctx, cudaMemcpyAsync(M, L, sizeof(double) * rr, cudaMemcpyDeviceToDevice, ctx->stream));
-            if ((s2 = bar_scale_diag(ctx, M, r, r, 1.0 + eps))) return s2;
-            eps *= 10.0;
-          }
-        } else {
+        // A capacity matrix with a huge dynamic range (late in the barrier D^-1 spans ~18 orders) can sit on the
+        // edge of numerical positive definiteness: its last bits (the Gram's rounding and the order of its
+        // split-k additions) decide whether the FP64 Cholesky passes.  A relative diagonal shift, x10 from 1e-11 up
+        // to 1 until the Cholesky succeeds, keeps it positive definite; the shifted M still gives a descent
+        // direction, which the mixed path's refinement below corrects against the exact operator.
+        DB200_CUDA(ctx, cudaMemcpyAsync(L, M, sizeof(double) * rr, cudaMemcpyDeviceToDevice, ctx->stream));
+        double eps = 1e-11;
+        for (int tries = 0; tries < 12; ++tries) {
           DB200_CUDA(ctx, cudaMemsetAsync(d_pair, 0, 2 * sizeof(int), ctx->stream));
           if ((s2 = potrf_upper(ctx, M, r, r, d_pair, d_pair + 1))) return s2;
+          int pst = 0, bad = 0;
+          if ((s2 = read_status(ctx, d_pair, &pst, &bad))) return s2;
+          if (pst == 0 || tries == 11) break;
+          DB200_CUDA(ctx, cudaMemcpyAsync(M, L, sizeof(double) * rr, cudaMemcpyDeviceToDevice, ctx->stream));
+          if ((s2 = bar_scale_diag(ctx, M, r, r, 1.0 + eps))) return s2;
+          eps *= 10.0;
         }
         if ((s2 = transpose64(ctx, M, r, r, r, L, r))) return s2;
         if ((s2 = trsv_upper(ctx, M, L, r, r, u, true))) return s2;   // R^T z = rhs
