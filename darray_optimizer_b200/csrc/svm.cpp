@@ -44,9 +44,18 @@ struct LaStatus {
   int* d = nullptr;
 };
 
+// Scalar readbacks go through the context's pinned staging area: a copy into pageable memory is staged by the
+// driver and, from several threads at once (the batched solve's workers), serialises them.
+int read_scalar(db200_context* ctx, const double* d_src, double* out) {
+  DB200_CUDA(ctx, cudaMemcpyAsync(ctx->h_pinned, d_src, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  DB200_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  *out = ctx->h_pinned[0];
+  return DB200_OK;
+}
+
 int read_status(db200_context* ctx, int* d_pair, int* st, int* bad) {
-  int h[2] = {0, 0};
-  DB200_CUDA(ctx, cudaMemcpyAsync(h, d_pair, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+  int* h = reinterpret_cast<int*>(ctx->h_pinned);
+  DB200_CUDA(ctx, cudaMemcpyAsync(h, d_pair, 2 * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   DB200_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   *st = h[0];
   *bad = h[1];
@@ -63,8 +72,7 @@ int cholqr_pass(db200_context* ctx, int n, int l, const double* Yin, int ldin, d
     // shift = shift_rel * trace(W)
     if ((st = trace(ctx, R, l, l, d_scalar))) return st;
     double tr = 0;
-    DB200_CUDA(ctx, cudaMemcpyAsync(&tr, d_scalar, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    DB200_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if ((st = read_scalar(ctx, d_scalar, &tr))) return st;
     if ((st = mirror_upper(ctx, R, l, l))) return st;  // the Gram kernel formed the upper triangle only
     if ((st = symmetrize(ctx, R, l, l, shift_rel * tr))) return st;
   }
@@ -196,9 +204,11 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
   double prev_pd = -1.0;  // primal-dual gap at the previous outer step whose barrier bound was met
   double h[64];
   int st;
-  auto fetch = [&](const double* d_src, int count) -> int {
-    DB200_CUDA(ctx, cudaMemcpyAsync(h, d_src, sizeof(double) * count, cudaMemcpyDeviceToHost, ctx->stream));
+  auto fetch = [&](const double* d_src, int count) -> int {  // count <= 64 (pinned staging holds 512)
+    DB200_CUDA(ctx, cudaMemcpyAsync(ctx->h_pinned, d_src, sizeof(double) * count, cudaMemcpyDeviceToHost,
+                                    ctx->stream));
     DB200_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    std::memcpy(h, ctx->h_pinned, sizeof(double) * count);
     return DB200_OK;
   };
   double fa = 0.0, suma_now = 0.0;
@@ -410,8 +420,7 @@ int nystrom_core(db200_context* ctx, int n, int l, const double* Q, const TY* Yk
   if ((st = symmetrize(ctx, Cm, l, l, 0.0))) return st;
   if ((st = trace(ctx, Cm, l, l, d_scalar))) return st;
   double tr = 0;
-  DB200_CUDA(ctx, cudaMemcpyAsync(&tr, d_scalar, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-  DB200_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if ((st = read_scalar(ctx, d_scalar, &tr))) return st;
   const size_t ll = (size_t)l * l;
   double nu = 1e-7 * std::max(tr, 1e-300) / l;
   bool ok = false;
