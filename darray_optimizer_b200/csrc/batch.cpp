@@ -164,9 +164,13 @@ int db200_svm_solve_batched(db200_context* ctx, int count, const db200_svm_insta
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   };
 
+  if (workers < 1) workers = 1;
+  if (workers > count) workers = count;
+  R.workers = workers;
+
   // ---- device buffers: packed points and test matrices (workspace), per-instance pass outputs (pipeline slot)
   std::vector<SketchPlan> plans((size_t)count);
-  size_t wbytes = 4096, pbytes = 4096;
+  size_t wbytes = 4096, pbytes = 4096 + (size_t)workers * 256;
   for (int b = 0; b < count; ++b) {
     const db200_svm_instance& I = inst[b];
     plans[(size_t)b] = job_plan(I.l, I.n_panels, I.panel, I.g_bufs);
@@ -179,8 +183,13 @@ int db200_svm_solve_batched(db200_context* ctx, int count, const db200_svm_insta
   if (!ws || !base) return DB200_ERR_NOMEM;
   Carve cw{static_cast<char*>(ws)};
   Carve cp{base};
-  int* d_pair = cp.take<int>(4);
-  double* d_scalar = cp.take<double>(4);
+  // status pair and scalar of the Nystrom core, one set per worker
+  std::vector<int*> wpair((size_t)workers);
+  std::vector<double*> wscalar((size_t)workers);
+  for (int k = 0; k < workers; ++k) {
+    wpair[(size_t)k] = cp.take<int>(4);
+    wscalar[(size_t)k] = cp.take<double>(4);
+  }
   std::vector<Packed> pk((size_t)count);
   std::vector<float*> Y32((size_t)count), Qf((size_t)count);
   std::vector<double*> Q((size_t)count), Cm((size_t)count), Rm((size_t)count);
@@ -276,15 +285,76 @@ int db200_svm_solve_batched(db200_context* ctx, int count, const db200_svm_insta
     R.graph_replays += 1;
     return DB200_OK;
   };
+  // ---- worker contexts (own stream and buffers each), kept across calls so their buffers stay grown
+  if (workers > 1) {
+    while ((int)ctx->workers.size() < workers) {
+      db200_context* w = nullptr;
+      const int cst = db200_create(&w, ctx->device, DB200_OWN_STREAM);
+      if (cst) {
+        cleanup();
+        return fail(ctx, cst, "svm_solve_batched: worker context");
+      }
+      ctx->workers.push_back(w);
+    }
+  }
+  // largest instances first (LPT): the per-instance work grows with n l^2
+  std::vector<int> order((size_t)count);
+  for (int b = 0; b < count; ++b) order[(size_t)b] = b;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+    return (double)inst[x].n * inst[x].l * inst[x].l > (double)inst[y].n * inst[y].l * inst[y].l;
+  });
+  // Per-instance work fn(worker context, worker index, instance) on the worker pool, ordered after everything
+  // queued on the context's stream, with the context's stream ordered after all of it.  The steps of one instance
+  // (a few dozen small, latency-bound launches and host readbacks) overlap with other instances' this way.
+  auto parallel = [&](auto&& fn) -> int {
+    if (workers == 1) {
+      for (int k = 0; k < count; ++k) {
+        const int s2 = fn(ctx, 0, order[(size_t)k]);
+        if (s2) return s2;
+      }
+      return DB200_OK;
+    }
+    std::vector<cudaEvent_t> done((size_t)workers, nullptr);
+    cudaEvent_t ready = nullptr;
+    if (cudaEventCreateWithFlags(&ready, cudaEventDisableTiming) != cudaSuccess)
+      return fail(ctx, DB200_ERR_CUDA, "svm_solve_batched: event");
+    for (auto& e : done) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    cudaEventRecord(ready, ctx->stream);
+    std::atomic<int> nxt{0};
+    std::vector<int> wst((size_t)workers, DB200_OK);
+    std::vector<std::thread> th;
+    for (int k = 0; k < workers; ++k)
+      th.emplace_back([&, k]() {
+        db200_context* w = ctx->workers[(size_t)k];
+        if (cudaStreamWaitEvent(w->stream, ready, 0) != cudaSuccess) {
+          wst[(size_t)k] = fail(w, DB200_ERR_CUDA, "svm_solve_batched: stream wait");
+          return;
+        }
+        for (int i = nxt.fetch_add(1); i < count && !wst[(size_t)k]; i = nxt.fetch_add(1))
+          wst[(size_t)k] = fn(w, k, order[(size_t)i]);
+        cudaEventRecord(done[(size_t)k], w->stream);
+      });
+    for (std::thread& t : th) t.join();
+    int s2 = DB200_OK;
+    for (int k = 0; k < workers; ++k) {
+      cudaStreamWaitEvent(ctx->stream, done[(size_t)k], 0);
+      if (!s2 && wst[(size_t)k]) s2 = fail(ctx, wst[(size_t)k], ctx->workers[(size_t)k]->last_error);
+    }
+    // destroying an event whose record is still pending is deferred by the runtime until it completes
+    for (auto& e : done) cudaEventDestroy(e);
+    cudaEventDestroy(ready);
+    return s2;
+  };
   auto orth_all = [&]() -> int {
     Timer t(ctx->stream);
-    for (int b = 0; b < count; ++b) {
+    const int s2 = parallel([&](db200_context* w, int, int b) -> int {
       const db200_svm_instance& I = inst[b];
-      int s2 = convert<float, double>(ctx, Y32[(size_t)b], I.n, Q[(size_t)b], I.n, I.n, I.l);
-      if (!s2) s2 = cholqr2_impl(ctx, I.n, I.l, Q[(size_t)b], I.n, nullptr, 0);
-      if (!s2) s2 = convert<double, float>(ctx, Q[(size_t)b], I.n, Qf[(size_t)b], I.n, I.n, I.l);
-      if (s2) return s2;
-    }
+      int s3 = convert<float, double>(w, Y32[(size_t)b], I.n, Q[(size_t)b], I.n, I.n, I.l);
+      if (!s3) s3 = cholqr2_impl(w, I.n, I.l, Q[(size_t)b], I.n, nullptr, 0);
+      if (!s3) s3 = convert<double, float>(w, Q[(size_t)b], I.n, Qf[(size_t)b], I.n, I.n, I.l);
+      return s3;
+    });
+    if (s2) return s2;
     R.ms_orth += t.stop();
     return DB200_OK;
   };
@@ -315,11 +385,11 @@ int db200_svm_solve_batched(db200_context* ctx, int count, const db200_svm_insta
   std::vector<double> nus((size_t)count, 0.0);
   {
     Timer t(ctx->stream);
-    for (int b = 0; b < count && !st; ++b) {
+    st = parallel([&](db200_context* w, int k, int b) -> int {
       const db200_svm_instance& I = inst[b];
-      st = nystrom_core<float>(ctx, I.n, I.l, Q[(size_t)b], Y32[(size_t)b], Cm[(size_t)b], Rm[(size_t)b], d_pair,
-                               d_scalar, I.Z, I.ldz, &nus[(size_t)b]);
-    }
+      return nystrom_core<float>(w, I.n, I.l, Q[(size_t)b], Y32[(size_t)b], Cm[(size_t)b], Rm[(size_t)b],
+                                 wpair[(size_t)k], wscalar[(size_t)k], I.Z, I.ldz, &nus[(size_t)b]);
+    });
     R.ms_core = t.stop();
   }
   cleanup();
@@ -327,14 +397,6 @@ int db200_svm_solve_batched(db200_context* ctx, int count, const db200_svm_insta
   DB200_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
 
   // ---- barriers: workers pull instances off a shared counter, largest first, each on its own context and stream
-  if (workers < 1) workers = 1;
-  if (workers > count) workers = count;
-  R.workers = workers;
-  std::vector<int> order((size_t)count);
-  for (int b = 0; b < count; ++b) order[(size_t)b] = b;
-  std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
-    return (double)inst[x].n * inst[x].l * inst[x].l > (double)inst[y].n * inst[y].l * inst[y].l;
-  });
   std::vector<db200_svm_report> rep((size_t)count);
   std::vector<int> status((size_t)count, DB200_OK);
   std::atomic<int> next{0};
@@ -347,14 +409,6 @@ int db200_svm_solve_batched(db200_context* ctx, int count, const db200_svm_insta
       rep[(size_t)b].nu = nus[(size_t)b];
     }
   };
-  if (workers > 1) {
-    while ((int)ctx->workers.size() < workers) {
-      db200_context* w = nullptr;
-      const int cst = db200_create(&w, ctx->device, DB200_OWN_STREAM);
-      if (cst) return fail(ctx, cst, "svm_solve_batched: worker context");
-      ctx->workers.push_back(w);
-    }
-  }
   const auto wall_b = std::chrono::steady_clock::now();
   if (workers == 1) {
     run(ctx);
