@@ -25,3 +25,14 @@ g++ -O2 -std=c++17 -shared -fPIC -w \
     "$HERE/ref_driver.cpp" -o "$HERE/_ref/libdarray_ref.so" \
     "$BLAS_LIB" -Wl,--disable-new-dtags -Wl,-rpath,"$BLAS_DIR"
 echo "$HERE/_ref/libdarray_ref.so"
+
+# The reference's GPU kernel-block code (include/dkernel.cu: rbf_kernel, tc_gemm) compiled unmodified for
+# sm_100a, with the C wrappers of oracle/ref_gpu_shim.cpp, into oracle/_ref/libdkernel_ref.so.  Linked with
+# -Bsymbolic: the product library exports drop-in C++ symbols of the same names (rbf_kernel, tc_gemm, cuda_init),
+# and the wrappers must reach the reference's definitions even when both libraries sit in one process.
+if command -v nvcc > /dev/null && [ -f "$REF/include/dkernel.cu" ]; then
+  nvcc -O2 -std=c++17 -shared -Xcompiler -fPIC -w -gencode arch=compute_100a,code=sm_100a \
+      "$REF/include/dkernel.cu" "$HERE/ref_gpu_shim.cpp" -o "$HERE/_ref/libdkernel_ref.so" \
+      -Xlinker -Bsymbolic -lcublas -lcusolver
+  echo "$HERE/_ref/libdkernel_ref.so"
+fi
