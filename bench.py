@@ -267,6 +267,8 @@ def run_ours(args):
         extra["c3"] = c3_run(ctx)
     if args.c5 and rank == 0:
         extra["c5"] = c5_run(ctx)
+    if args.libsvm and rank == 0:
+        extra["libsvm"] = libsvm_run(ctx)
     return finish(args, ctx, w, rep, ms_max, kernel_ms, kernel_count, launches, clocks, e2e_val, h2d, d2h, Om,
                   solve, batch, extra)
 
@@ -479,6 +481,95 @@ def e2e_run(ctx, w, Om, rep, steps):
     return e2e_val, h2d, d2h
 
 
+def libsvm_run(ctx, n=N_POINTS, d=D_FEAT, steps=5, cpu_lines=8192):
+    """LIBSVM input leg: the C2 points written as LIBSVM text (six decimals, about 205 MB) and read back by the
+    GPU reader.  Device parse (text resident in HBM, CUDA events) against the HBM roofline of its algorithmic
+    bytes (text read once, X and y written once); end to end from a page-cached file through db200_read_libsvm
+    into host X and y (wall clock); the reference's own read_input_file<float> (include/read_input.h:8-36, built
+    into oracle/_ref) on the first cpu_lines lines of the same file as the CPU baseline."""
+    import ctypes
+    import tempfile
+    import torch
+    from darray_optimizer_b200 import datagen
+    from darray_optimizer_b200._lib import F32
+    w = datagen.uniform_hyperplane(n=n, d=d, seed=2)
+    text = datagen.libsvm_text(w.X, w.y, 6)
+    nbytes = len(text)
+    stream = torch.cuda.current_stream()
+    dtext = torch.frombuffer(bytearray(text), dtype=torch.uint8).cuda()
+    Xd = torch.zeros((n, d), dtype=torch.float32, device="cuda")
+    yd = torch.zeros(n, dtype=torch.float32, device="cuda")
+
+    def parse():
+        return ctx.libsvm_parse(dtext.data_ptr(), nbytes, n, d, F32, Xd.data_ptr(), d, yd.data_ptr())
+
+    for _ in range(2):
+        lines = parse()
+    torch.cuda.synchronize()
+    launches0 = ctx.launches()
+    times = []
+    for _ in range(steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        parse()  # synchronous: ends with a stream synchronize after its line-count readback
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    launches = (ctx.launches() - launches0) // steps
+    ms = statistics.median(times)
+    max_err = float((Xd.double().cpu() - torch.from_numpy(w.X).double()).abs().max())
+    labels_ok = bool(torch.equal(yd.cpu(), torch.from_numpy(w.y)))
+    alg_bytes = nbytes + n * d * 4 + n * 4
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    out = {"workload": f"C2 points as LIBSVM text (n={n}, d={d}, 6 decimals, {nbytes / 1e6:.1f} MB)",
+           "lines": lines, "device_parse_ms": ms, "device_parse_gbs": nbytes / (ms / 1e3) / 1e9,
+           "launches_per_parse": launches,
+           "roofline": {"bound": "hbm", "achieved": alg_bytes / (ms / 1e3) / 1e9, "peak": hbm, "unit": "GB/s",
+                        "frac": alg_bytes / (ms / 1e3) / 1e9 / hbm,
+                        "algorithmic_bytes": alg_bytes,
+                        "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650"},
+           "max_abs_err_vs_points": max_err, "labels_exact": labels_ok}
+    # end to end: page-cached file -> pinned staging -> device parse -> host X, y
+    with tempfile.NamedTemporaryFile(suffix=".libsvm", delete=False) as f:
+        f.write(text)
+        path = f.name
+    try:
+        Xh = np.zeros((n, d), np.float32)
+        yh = np.zeros(n, np.float32)
+        walls = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            ctx.read_libsvm(path, n, d, F32, Xh.ctypes.data, d, yh.ctypes.data)
+            walls.append(time.perf_counter() - t0)
+        e2e_s = statistics.median(walls)
+        out["e2e"] = {"s": e2e_s, "gbs": nbytes / e2e_s / 1e9, "same_as_device_parse": bool(
+            np.array_equal(Xh.view(np.uint32), Xd.cpu().numpy().view(np.uint32)))}
+        # CPU baseline: the reference's own reader on the first cpu_lines lines of the same file
+        ref_lib = ROOT / "oracle" / "_ref" / "libdarray_ref.so"
+        if ref_lib.exists():
+            lib = ctypes.CDLL(str(ref_lib))
+            fp = ctypes.POINTER(ctypes.c_float)
+            lib.ref_read_input_file_f32.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, fp, fp]
+            Xr = np.zeros((cpu_lines, d), np.float32)
+            yr = np.zeros(cpu_lines, np.float32)
+            t0 = time.perf_counter()
+            lib.ref_read_input_file_f32(path.encode(), cpu_lines, d, Xr.ctypes.data_as(fp), yr.ctypes.data_as(fp))
+            cs = time.perf_counter() - t0
+            pos = 0
+            for _ in range(cpu_lines):
+                pos = text.index(b"\n", pos) + 1
+            sample_bytes = pos
+            out["cpu_baseline"] = {"value": sample_bytes / cs / 1e9, "unit": "GB/s", "cores": 1, "kind": "reference",
+                                   "sample": f"read_input_file<float> on the first {cpu_lines} lines "
+                                             f"({sample_bytes / 1e6:.1f} MB) of the same file, {cs:.2f} s",
+                                   "same_as_gpu": bool(np.array_equal(Xr.view(np.uint32),
+                                                                      Xd[:cpu_lines].cpu().numpy().view(np.uint32)))}
+    finally:
+        os.unlink(path)
+    return out
+
+
 def finish(args, ctx, w, rep, ms_max, kernel_ms, kernel_count, launches, clocks, e2e_val, h2d, d2h, Om,
            solve=None, batch=None, extra=None):
     world, rank = rep.world, rep.rank
@@ -549,6 +640,8 @@ def main():
                     help="solve leg without the plain FP64 comparator (profiling runs)")
     ap.add_argument("--c3", action="store_true", help="add the sparse-binary leg (n = 262144, l = 1040)")
     ap.add_argument("--c5", action="store_true", help="add the learned-landmark leg (n = 524288, r = 2048)")
+    ap.add_argument("--libsvm", action="store_true",
+                    help="add the LIBSVM input leg (C2 points as text, GPU reader vs the reference's reader)")
     ap.add_argument("--n-test", type=int, default=16384, help="held-out points for the solve leg's accuracy")
     ap.add_argument("--n", type=int, default=N_POINTS, help="points (default: the C2 workload, 131072)")
     args = ap.parse_args()

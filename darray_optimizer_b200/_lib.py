@@ -155,6 +155,10 @@ SIGNATURES = {
                                            _u64, _c_int, _c_int, _c_double, _vp, _c_int, _c_int, _c_int,
                                            ctypes.POINTER(BarrierParams), _vp, _vp, _c_int, ctypes.POINTER(SvmReport),
                                            ctypes.POINTER(LandmarkReport)]),
+    "db200_libsvm_parse": (_c_int, [_vp, _vp, ctypes.c_longlong, _c_int, _c_int, _c_int, _vp, ctypes.c_longlong, _vp,
+                                    ctypes.POINTER(_c_int)]),
+    "db200_read_libsvm": (_c_int, [_vp, ctypes.c_char_p, _c_int, _c_int, _c_int, _vp, ctypes.c_longlong, _vp,
+                                   ctypes.POINTER(_c_int)]),
 }
 
 STATUS = {
@@ -164,6 +168,7 @@ STATUS = {
 }
 NOALLOC_SCRATCH_BYTES = 32 << 20
 POINT_MAJOR, FEATURE_MAJOR = 0, 1
+F32, F64 = 0, 1
 
 _lib = None
 
@@ -385,6 +390,19 @@ class Context:
         if st not in (0, -4):
             self.check(st)
         return rep, lrep
+
+    def libsvm_parse(self, text, nbytes, n, d, dtype, X, ldx, y):
+        """db200_libsvm_parse on device text; returns the lines parsed."""
+        lines = _c_int()
+        self.check(self.lib.db200_libsvm_parse(self.h, text, nbytes, n, d, dtype, X, ldx, y, ctypes.byref(lines)))
+        return lines.value
+
+    def read_libsvm(self, path, n, d, dtype, X, ldx, y):
+        """db200_read_libsvm into host X and y (pointers); returns the lines parsed."""
+        lines = _c_int()
+        self.check(self.lib.db200_read_libsvm(self.h, str(path).encode(), n, d, dtype, X, ldx, y,
+                                              ctypes.byref(lines)))
+        return lines.value
 
 
 class Mlp:

@@ -154,6 +154,7 @@ int db200_destroy(db200_context* ctx) {
   if (ctx->tile_table) cudaFree(ctx->tile_table);
   if (ctx->d_status) cudaFree(ctx->d_status);
   if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
+  if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return DB200_OK;

@@ -25,6 +25,8 @@ struct db200_context {
   void* slot[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   size_t slot_size[5] = {0, 0, 0, 0, 0};
   double* h_pinned = nullptr;    // small pinned host staging area for scalar readbacks
+  void* h_stage = nullptr;       // pinned host staging for file input (two halves, grow-only)
+  size_t h_stage_size = 0;
   void* tile_table = nullptr;    // instance table of the tile engine (grow-only)
   size_t tile_table_size = 0;
   // Worker contexts (own stream and buffers each) of the batched solve, kept across calls so their buffers stay

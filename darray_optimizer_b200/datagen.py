@@ -154,3 +154,40 @@ CONFIGS = {
 
 def make(name: str, **kw) -> Workload:
     return CONFIGS[name](**kw)
+
+
+def libsvm_text(X: np.ndarray, y: np.ndarray, decimals: int = 6) -> bytes:
+    """LIBSVM text "label 1:x 2:x ... d:x\\n" of dense points with 0 <= x < 10, every value written with
+    `decimals` decimals ("%.{decimals}f"), labels "1" / "-1".  Built column slot by column slot with numpy, so a
+    C2-sized file (131072 x 128, about 220 MB) takes a couple of seconds."""
+    X = np.asarray(X, np.float64)
+    n, d = X.shape
+    if n == 0:
+        return b""
+    if X.min() < 0 or X.max() >= 9.5:
+        raise ValueError("libsvm_text writes values in [0, 10) only")
+    scale = 10 ** decimals
+    q = np.rint(X * scale).astype(np.int64)  # value * 10^decimals, rounded
+    vw = 2 + decimals                         # "D.ddd..."
+    prefixes = [f" {k + 1}:".encode() for k in range(d)]
+    width = 2 + sum(len(p) + vw for p in prefixes) + 1
+    buf = np.full((n, width), ord(" "), np.uint8)
+    pos = 0
+    pos_lab = pos
+    pos += 2
+    neg = np.asarray(y) < 0
+    buf[:, pos_lab] = np.where(neg, ord("-"), ord(" "))
+    buf[:, pos_lab + 1] = ord("1")
+    for k, p in enumerate(prefixes):
+        buf[:, pos:pos + len(p)] = np.frombuffer(p, np.uint8)
+        pos += len(p)
+        v = q[:, k]
+        buf[:, pos] = ord("0") + v // scale
+        buf[:, pos + 1] = ord(".")
+        frac = v % scale
+        for j in range(decimals):
+            buf[:, pos + 2 + decimals - 1 - j] = ord("0") + frac % 10
+            frac //= 10
+        pos += vw
+    buf[:, pos] = ord("\n")
+    return buf.tobytes()

@@ -437,6 +437,39 @@ DB200_API int db200_svm_solve_landmarks(db200_context* ctx, int n, int d, int r,
                                         const db200_barrier_params* params, double* a, double* Z, int ldz,
                                         db200_svm_report* rep, db200_landmark_report* lrep);
 
+/* ------------------------------------------------------------------ LIBSVM text input */
+#define DB200_F32 0 /* float X and y */
+#define DB200_F64 1 /* double X and y */
+
+/* Parse the first n lines of LIBSVM text ("label index:value index:value ...", lines ended by '\n') held in
+ * device memory (`bytes` characters at `text`, any alignment) into device X and y, as read_input_file<T>
+ * (include/read_input.h:8-36) does on the host:
+ *   - tokens are separated by ' ' only (runs of blanks collapse); the first token of a line is the label and
+ *     y[i] = +1 when it converts (strtod, then to T) to exactly 1, else -1;
+ *   - every further token is "index:value": index = atoi of the part before the first ':', value = strtod of the
+ *     part after it (of the whole token when it has no ':'); X[(index - 1) + i*ldx] = value for index >= 1,
+ *     tokens with index < 1 are skipped; repeated indices keep the last value;
+ *   - values are correctly rounded to double and then, for DB200_F32, to float, so results are bit-identical to
+ *     the reference's; "inf", "infinity" and "nan" are accepted;
+ *   - entries of X and y that the text does not name keep their values.
+ * The reference indexes rows with stride d and ignores ldx; here the stride is ldx (>= d), the same at its call
+ * site (tests/testsvm.cpp:71, ldx = d).  lines_out (host, may be NULL) receives the lines parsed: min(n, lines in
+ * the text).  Where the reference's behaviour is undefined or would differ, the call fails instead, naming the
+ * first offending line in db200_last_error: DB200_ERR_INVALID for a feature index above d (the reference writes
+ * past the row) and for a last line of blanks only (the reference passes NULL to atof); DB200_ERR_UNSUPPORTED for
+ * hexadecimal values, "nan(...)" payloads, values with more than 38 significant digits and NUL bytes.
+ * dtype: DB200_F32 or DB200_F64.  Synchronous. */
+DB200_API int db200_libsvm_parse(db200_context* ctx, const char* text, long long bytes, int n, int d, int dtype,
+                                 void* X, long long ldx, void* y, int* lines_out);
+
+/* read_input_file<T>(filename, n, d, X, ldx, Y) (include/read_input.h:8-36) with HOST X and y: the file is read
+ * in 32 MiB pieces through pinned staging, each piece's copy to the device overlapping the next read, parsed by
+ * db200_libsvm_parse and X, y copied back (X and y are copied to the device first, so entries the file does not
+ * name keep their values).  A file that cannot be opened returns DB200_ERR_INVALID (the reference exits).
+ * Synchronous. */
+DB200_API int db200_read_libsvm(db200_context* ctx, const char* path, int n, int d, int dtype, void* X,
+                                long long ldx, void* y, int* lines_out);
+
 #ifdef __cplusplus
 }
 #endif

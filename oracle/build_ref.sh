@@ -20,7 +20,9 @@ if [ -z "$BLAS_LIB" ]; then
   exit 0
 fi
 mkdir -p "$HERE/_ref"
-g++ -O2 -std=c++17 -shared -fPIC -w \
+# -ftrivial-auto-var-init=zero: read_input_file passes an uninitialised `char* line` to getline
+# (include/read_input.h:15-19), which glibc only accepts as NULL; zero-initialising locals gives it that.
+g++ -O2 -std=c++17 -shared -fPIC -w -ftrivial-auto-var-init=zero \
     -I "$HERE/mpi_stub" -I "$REF/include" \
     "$HERE/ref_driver.cpp" -o "$HERE/_ref/libdarray_ref.so" \
     "$BLAS_LIB" -Wl,--disable-new-dtags -Wl,-rpath,"$BLAS_DIR"

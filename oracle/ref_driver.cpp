@@ -9,6 +9,7 @@
 #include "lapack_like.h"
 #include "blas_like.h"
 #include "dbarrier.h"
+#include "read_input.h"
 
 using DArray::DMatrix;
 using DArray::DMatrixDescriptor;
@@ -126,6 +127,14 @@ void ref_writemodel(const char* path, int n, int d, int k, double* a, double C, 
   auto A = lmat(a, n, 1), Zm = lmat(Z, n, k), Ym = lmat(Y, n, 1);
   LMatrix<double> Xm(d, n, d, X);
   DArray::writemodel<double>(std::string(path), n, d, k, A, C, Zm, Ym, Xm, gamma, minus, plus);
+}
+// read_input_file<T> (include/read_input.h:8-36): X is d x n column major (point-major), Y n labels.  The
+// reference indexes X with stride d and ignores ldx.
+void ref_read_input_file_f32(const char* filename, int n, int d, float* X, float* Y) {
+  read_input_file<float>(const_cast<char*>(filename), n, d, X, d, Y);
+}
+void ref_read_input_file_f64(const char* filename, int n, int d, double* X, double* Y) {
+  read_input_file<double>(const_cast<char*>(filename), n, d, X, d, Y);
 }
 
 }  // extern "C"
