@@ -8,7 +8,8 @@
 //   nl_count_kernel    newlines per 16 KB chunk                       (one block per chunk, 16-byte loads)
 //   nl_scan_kernel     exclusive prefix of the chunk counts, the line count
 //   nl_starts_kernel   byte offset of the start of every line < n     (block-wide ranks of the newlines)
-//   parse_kernel       one warp per line: token starts of a 512-byte window by ballot, one token per lane
+//   parse_kernel       one warp per line: a 512-byte window staged in shared memory (the next one already in
+//                      flight), token starts by ballot, one token per lane parsed in one pass
 //
 // Values are converted exactly as glibc's strtod does (correctly rounded to double; for float output the double
 // is then rounded to float, as the reference's `T value = atof(...)`).  Short decimals take Clinger's fast path
@@ -20,10 +21,18 @@
 // dereferences it).  Hexadecimal values, NaN payloads "nan(...)", values with more than 38 significant digits
 // and NUL bytes inside a line (the reference's C strings would end there) are rejected as unsupported rather
 // than read differently.
+#include <fcntl.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
+#include <vector>
 
 #include "internal.h"
 
@@ -96,7 +105,8 @@ __global__ void __launch_bounds__(NL_THREADS) nl_count_kernel(const unsigned cha
 }
 
 // One block: prefix[c] = newlines before chunk c; meta[0] = newlines in the text, meta[1] = lines to parse
-// (min(n, newlines + 1 if the text does not end with '\n')).
+// (min(n, newlines + 1 if the text does not end with '\n')).  meta[2] (lines that do not name all d features)
+// is counted by the parse kernel.
 __global__ void __launch_bounds__(1024) nl_scan_kernel(const int* counts, int nchunks, long long* prefix,
                                                        const unsigned char* text, long long bytes, int n,
                                                        long long* meta) {
@@ -184,25 +194,27 @@ __global__ void __launch_bounds__(NL_THREADS) nl_starts_kernel(const unsigned ch
 }
 
 // ------------------------------------------------------------------ number conversion
-__device__ __forceinline__ bool c_space(unsigned c) { return c == ' ' || (c >= 9 && c <= 13); }
 __device__ __forceinline__ bool c_digit(unsigned c) { return c - '0' < 10u; }
 __device__ __forceinline__ bool c_hex(unsigned c) { return c_digit(c) || ((c | 0x20u) - 'a' < 6u); }
+// C whitespace other than the blank, which ends a token
+__device__ __forceinline__ bool c_ctl_space(unsigned c) { return c >= 9u && c <= 13u; }
 
-// atoi: optional blanks, sign, digits.  Saturates far above any usable index instead of overflowing.
-__device__ long long parse_index(const unsigned char* p, const unsigned char* end) {
-  while (p < end && c_space(*p)) ++p;
-  bool neg = false;
-  if (p < end && (*p == '+' || *p == '-')) {
-    neg = (*p == '-');
-    ++p;
+// The bytes of one line as the token parser reads them, by offset q from a window start w0: the warp's staged
+// window in shared memory for 0 <= q < lim, global memory up to the line end beyond it, a blank past the line
+// end.  A token ends at its first blank.
+struct LineBytes {
+  const unsigned char* sm;
+  unsigned lim;           // WIN when the window is staged, 0 to read global memory only
+  long long w0;
+  const unsigned char* text;
+  long long e;            // line end
+  __device__ __forceinline__ unsigned at(int q) const {
+    if ((unsigned)q < lim) return sm[q];
+    const long long pos = w0 + q;
+    return (q >= 0 && pos < e) ? (unsigned)__ldg(text + pos) : (unsigned)' ';
   }
-  long long v = 0;
-  while (p < end && c_digit(*p)) {
-    if (v < (1ll << 40)) v = v * 10 + (*p - '0');
-    ++p;
-  }
-  return neg ? -v : v;
-}
+};
+__device__ __forceinline__ bool c_end(unsigned c) { return c == ' ' || c == 0u; }
 
 // Little-endian 32-bit limb arithmetic for the exact path (lengths in limbs, no leading zero limbs).
 __device__ int bn_mul_add(uint32_t* a, int n, uint32_t mul, uint32_t add) {
@@ -359,32 +371,39 @@ __device__ __noinline__ double slow_convert(uint64_t w_hi, uint64_t w_lo, int n_
   return ldexp((double)m, -1074);
 }
 
-// strtod over [p, end): returns E_NONE and the value, or an unsupported-form code.
-__device__ unsigned parse_value(const unsigned char* p, const unsigned char* end, double* out) {
+__device__ const double kPow10[23] = {1e0,  1e1,  1e2,  1e3,  1e4,  1e5,  1e6,  1e7,  1e8,  1e9,  1e10, 1e11,
+                                      1e12, 1e13, 1e14, 1e15, 1e16, 1e17, 1e18, 1e19, 1e20, 1e21, 1e22};
+
+// strtod of the token text from offset q (the token ends at its first blank): returns E_NONE and the value, or
+// an unsupported-form code.
+__device__ __forceinline__ unsigned parse_value(const LineBytes L, int q, double* out) {
   *out = 0.0;
-  while (p < end && c_space(*p)) ++p;
+  unsigned c = L.at(q);
+  while (c_ctl_space(c)) c = L.at(++q);
   bool neg = false;
-  if (p < end && (*p == '+' || *p == '-')) {
-    neg = (*p == '-');
-    ++p;
+  if (c == '+' || c == '-') {
+    neg = (c == '-');
+    c = L.at(++q);
   }
-  if (p < end && (((*p | 0x20u) == 'i') || ((*p | 0x20u) == 'n'))) {
-    if (end - p >= 3 && (p[0] | 0x20u) == 'i' && (p[1] | 0x20u) == 'n' && (p[2] | 0x20u) == 'f') {
+  if ((c | 0x20u) == 'i' || (c | 0x20u) == 'n') {
+    const unsigned c1 = L.at(q + 1) | 0x20u, c2 = L.at(q + 2) | 0x20u;
+    if ((c | 0x20u) == 'i' && c1 == 'n' && c2 == 'f') {
       *out = neg ? -INFINITY : INFINITY;
-    } else if (end - p >= 3 && (p[0] | 0x20u) == 'n' && (p[1] | 0x20u) == 'a' && (p[2] | 0x20u) == 'n') {
-      if (end - p >= 4 && p[3] == '(') return E_NANPAYLOAD;
+    } else if ((c | 0x20u) == 'n' && c1 == 'a' && c2 == 'n') {
+      if (L.at(q + 3) == '(') return E_NANPAYLOAD;
       *out = __longlong_as_double(neg ? (long long)0xfff8000000000000ull : 0x7ff8000000000000ll);
     }
     return E_NONE;  // otherwise no conversion: 0
   }
-  if (end - p >= 3 && p[0] == '0' && (p[1] | 0x20u) == 'x' &&
-      (c_hex(p[2]) || (p[2] == '.' && end - p >= 4 && c_hex(p[3]))))
-    return E_HEX;
+  if (c == '0' && (L.at(q + 1) | 0x20u) == 'x') {
+    const unsigned c2 = L.at(q + 2);
+    if (c_hex(c2) || (c2 == '.' && c_hex(L.at(q + 3)))) return E_HEX;
+  }
   uint64_t w_hi = 0, w_lo = 0;
   int nsig = 0, e10 = 0;
   bool any = false, dropped = false;
-  while (p < end && c_digit(*p)) {
-    const unsigned dg = *p - '0';
+  while (c_digit(c)) {
+    const unsigned dg = c - '0';
     any = true;
     if (nsig == 0 && dg == 0) {
     } else if (nsig < MAX_SIG) {
@@ -395,12 +414,12 @@ __device__ unsigned parse_value(const unsigned char* p, const unsigned char* end
       dropped |= dg != 0;
       ++e10;
     }
-    ++p;
+    c = L.at(++q);
   }
-  if (p < end && *p == '.') {
-    ++p;
-    while (p < end && c_digit(*p)) {
-      const unsigned dg = *p - '0';
+  if (c == '.') {
+    c = L.at(++q);
+    while (c_digit(c)) {
+      const unsigned dg = c - '0';
       any = true;
       if (nsig == 0 && dg == 0) {
         --e10;
@@ -412,22 +431,23 @@ __device__ unsigned parse_value(const unsigned char* p, const unsigned char* end
       } else {
         dropped |= dg != 0;
       }
-      ++p;
+      c = L.at(++q);
     }
   }
   if (!any) return E_NONE;  // no conversion
-  if (p < end && (*p | 0x20u) == 'e') {
-    const unsigned char* r = p + 1;
+  if ((c | 0x20u) == 'e') {
+    int r = q + 1;
+    unsigned cr = L.at(r);
     bool eneg = false;
-    if (r < end && (*r == '+' || *r == '-')) {
-      eneg = (*r == '-');
-      ++r;
+    if (cr == '+' || cr == '-') {
+      eneg = (cr == '-');
+      cr = L.at(++r);
     }
-    if (r < end && c_digit(*r)) {
+    if (c_digit(cr)) {
       int ev = 0;
-      while (r < end && c_digit(*r)) {
-        if (ev < 1000000) ev = ev * 10 + (*r - '0');
-        ++r;
+      while (c_digit(cr)) {
+        if (ev < 1000000) ev = ev * 10 + (int)(cr - '0');
+        cr = L.at(++r);
       }
       e10 += eneg ? -ev : ev;
     }
@@ -441,10 +461,8 @@ __device__ unsigned parse_value(const unsigned char* p, const unsigned char* end
   } else if (nsig + e10 < -323) {
     v = 0.0;
   } else if (nsig <= 19 && w_hi <= (1ull << 53) && e10 >= -22 && e10 <= 22) {
-    const double p10[23] = {1e0,  1e1,  1e2,  1e3,  1e4,  1e5,  1e6,  1e7,  1e8,  1e9,  1e10, 1e11,
-                            1e12, 1e13, 1e14, 1e15, 1e16, 1e17, 1e18, 1e19, 1e20, 1e21, 1e22};
     const double x = (double)w_hi;  // exact
-    v = e10 >= 0 ? __dmul_rn(x, p10[e10]) : __ddiv_rn(x, p10[-e10]);
+    v = e10 >= 0 ? __dmul_rn(x, __ldg(&kPow10[e10])) : __ddiv_rn(x, __ldg(&kPow10[-e10]));
   } else {
     v = nsig > 19 ? slow_convert(w_hi, w_lo, nsig - 19, e10) : slow_convert(w_hi, 0ull, 0, e10);
   }
@@ -467,20 +485,33 @@ __device__ __forceinline__ void report(unsigned long long* err, long long line, 
   atomicMin(err, ((unsigned long long)line << 8) | code);
 }
 
-// Parse one "index:value" token [p, end) of line i; returns the index written (0 when none).
+// Parse one "index:value" token of line i starting at `pos`, in one pass over its bytes; returns the index
+// written (0 when none).
 template <typename T>
-__device__ long long feature_token(const unsigned char* p, const unsigned char* end, long long i, int d, T* X,
-                                   long long ldx, unsigned long long* err) {
-  const unsigned char* colon = p;
-  while (colon < end && *colon != ':') ++colon;
-  const long long idx = parse_index(p, colon < end ? colon : end);
-  if (idx < 1) return 0;  // the reference's `index - 1 > -1` test
+__device__ __forceinline__ long long feature_token(const LineBytes L, int q, long long i, int d, T* X, long long ldx,
+                                                   unsigned long long* err) {
+  const int start = q;
+  unsigned c = L.at(q);
+  while (c_ctl_space(c)) c = L.at(++q);  // atoi: leading whitespace, sign, digits
+  bool neg = false;
+  if (c == '+' || c == '-') {
+    neg = (c == '-');
+    c = L.at(++q);
+  }
+  long long idx = 0;
+  while (c_digit(c)) {
+    if (idx < (1ll << 40)) idx = idx * 10 + (c - '0');
+    c = L.at(++q);
+  }
+  if (neg) idx = -idx;
+  while (!c_end(c) && c != ':') c = L.at(++q);  // the first ':' (atoi stopped at or before it)
+  if (idx < 1) return 0;                        // the reference's `index - 1 > -1` test
   if (idx > d) {
     report(err, i, E_INDEX);
     return 0;
   }
   double v;
-  const unsigned code = parse_value(colon < end ? colon + 1 : p, end, &v);
+  const unsigned code = parse_value(L, c == ':' ? q + 1 : start, &v);
   if (code != E_NONE) {
     report(err, i, code);
     return 0;
@@ -489,19 +520,32 @@ __device__ long long feature_token(const unsigned char* p, const unsigned char* 
   return idx;
 }
 
-__device__ __forceinline__ const unsigned char* token_end(const unsigned char* p, const unsigned char* e) {
-  while (p < e && *p != ' ') ++p;
-  return p;
+// 16 bytes of the text at offset o (aligned to 16 when AL), blanks outside the line [s, e).
+template <bool AL>
+__device__ __forceinline__ uint4 line_seg(const unsigned char* text, long long bytes, long long o, long long s,
+                                          long long e) {
+  uint4 v = load_seg<AL>(text, bytes, o);
+  const long long lo = s - o, hi = e - o;
+  if (lo > 0 || hi < 16) {
+    uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int k = 0; k < 16; ++k)
+      if (k < lo || k >= hi) w[k >> 2] = (w[k >> 2] & ~(0xffu << (8 * (k & 3)))) | (0x20u << (8 * (k & 3)));
+    v = make_uint4(w[0], w[1], w[2], w[3]);
+  }
+  return v;
 }
 
-template <typename T>
+template <typename T, bool AL>
 __global__ void __launch_bounds__(PARSE_THREADS) parse_kernel(const unsigned char* text, long long bytes,
-                                                              const long long* starts, const long long* meta,
+                                                              const long long* starts, long long* meta,
                                                               int d, T* X, long long ldx, T* y,
                                                               unsigned long long* err) {
+  __shared__ __align__(16) unsigned char stage_all[PARSE_THREADS / 32][WIN];
   __shared__ uint16_t tstart[PARSE_THREADS / 32][WIN / 2 + 2];
   const int lane = threadIdx.x % 32, wib = threadIdx.x / 32;
   uint16_t* sh = tstart[wib];
+  unsigned char* stage = stage_all[wib];
   const long long nl = meta[0], nlines = meta[1];
   const long long warps = (long long)gridDim.x * (PARSE_THREADS / 32);
   for (long long i = (long long)blockIdx.x * (PARSE_THREADS / 32) + wib; i < nlines; i += warps) {
@@ -511,23 +555,28 @@ __global__ void __launch_bounds__(PARSE_THREADS) parse_kernel(const unsigned cha
     long long tok = 0;       // tokens of this line seen so far
     long long maxidx = 0;    // largest feature index written so far
     bool simple = true;      // indices strictly increasing: no two tokens write one element
-    bool labelled = false;
-    for (long long w0 = s; w0 < e; w0 += WIN) {
-      unsigned char b[16];
-      const long long o = w0 + 16 * lane;
-#pragma unroll
-      for (int k = 0; k < 16; ++k) b[k] = (o + k < e) ? __ldg(text + o + k) : (unsigned char)' ';
+    long long named = 0;     // feature tokens written (distinct while `simple`)
+    // Windows of 512 bytes on 16-byte boundaries of the text, bytes outside [s, e) read as blanks.  The next
+    // window's segment is loaded into registers before the current window is parsed, so its memory latency hides
+    // behind the token work; tokens that cross a window's end read the rest through L1.
+    uint4 vn = line_seg<AL>(text, bytes, (s & ~15ll) + 16 * lane, s, e);
+    for (long long w0 = s & ~15ll; w0 < e; w0 += WIN) {
+      const uint4 v = vn;
+      reinterpret_cast<uint4*>(stage)[lane] = v;
+      if (w0 + WIN < e) vn = line_seg<AL>(text, bytes, w0 + WIN + 16 * lane, s, e);
+      const uint32_t wv[4] = {v.x, v.y, v.z, v.w};
       // The reference sees a line as a C string that a NUL byte would end: reject such text.
       bool has_nul = false;
 #pragma unroll
-      for (int k = 0; k < 16; ++k) has_nul |= (o + k < e && b[k] == 0);
+      for (int k = 0; k < 16; ++k) has_nul |= ((wv[k >> 2] >> (8 * (k & 3))) & 0xffu) == 0u;
       if (__any_sync(0xffffffffu, has_nul) && lane == 0) report(err, i, E_NUL);
-      const unsigned char prev_last = (unsigned char)__shfl_up_sync(0xffffffffu, (int)b[15], 1);
+      const unsigned last = (wv[3] >> 24) & 0xffu;
+      const unsigned prev_last = (unsigned)__shfl_up_sync(0xffffffffu, (int)last, 1);
       bool pb = lane == 0 ? prev_space : (prev_last == ' ');
       uint32_t m = 0;
 #pragma unroll
       for (int k = 0; k < 16; ++k) {
-        const bool sp = (b[k] == ' ');
+        const bool sp = ((wv[k >> 2] >> (8 * (k & 3))) & 0xffu) == ' ';
         if (!sp && pb) m |= 1u << k;
         pb = sp;
       }
@@ -547,20 +596,20 @@ __global__ void __launch_bounds__(PARSE_THREADS) parse_kernel(const unsigned cha
         sh[r++] = (uint16_t)(16 * lane + k);
       }
       __syncwarp();
+      const LineBytes L{stage, (unsigned)WIN, w0, text, e};
       for (int t0 = 0; t0 < total; t0 += 32) {
         const int t = t0 + lane;
         long long widx = 0;
         if (t < total) {
-          const unsigned char* p = text + w0 + sh[t];
-          const unsigned char* te = token_end(p, text + e);
+          const int q = sh[t];
           if (tok + t == 0) {
-            double v;
-            const unsigned code = parse_value(p, te, &v);
+            double lv64;
+            const unsigned code = parse_value(L, q, &lv64);
             if (code != E_NONE) report(err, i, code);
-            const T lv = to_t<T>(v);
+            const T lv = to_t<T>(lv64);
             y[i] = (lv == (T)1) ? (T)1 : (T)-1;
           } else {
-            widx = feature_token<T>(p, te, i, d, X, ldx, err);
+            widx = feature_token<T>(L, q, i, d, X, ldx, err);
           }
         }
         // every written index must exceed all earlier ones (token order = lane order within a round)
@@ -574,29 +623,31 @@ __global__ void __launch_bounds__(PARSE_THREADS) parse_kernel(const unsigned cha
         if (lane == 0) before = 0;
         before = before > maxidx ? before : maxidx;
         if (__any_sync(0xffffffffu, widx > 0 && widx <= before)) simple = false;
+        named += __popc(__ballot_sync(0xffffffffu, widx > 0));
         const long long rmax = __shfl_sync(0xffffffffu, incl, 31);
         maxidx = rmax > maxidx ? rmax : maxidx;
       }
-      labelled |= (tok == 0 && total > 0);
       tok += total;
-      prev_space = __shfl_sync(0xffffffffu, b[15] == ' ' ? 1 : 0, 31) != 0;
-      __syncwarp();
+      prev_space = __shfl_sync(0xffffffffu, last == ' ' ? 1 : 0, 31) != 0;
+      __syncwarp();  // the stage is rewritten by the next window
     }
-    if (!labelled && lane == 0) report(err, i, E_NOLABEL);
+    if (tok == 0 && lane == 0) report(err, i, E_NOLABEL);
+    // a line that leaves some of its row's d entries to the caller's values
+    if (lane == 0 && (!simple || named < d)) atomicAdd(reinterpret_cast<unsigned long long*>(meta) + 2, 1ull);
     if (!simple) {
       // Repeated or decreasing indices: replay the feature tokens in order so the last one written wins.
-      __syncwarp();
       if (lane == 0) {
-        const unsigned char* p = text + s;
-        const unsigned char* le = text + e;
-        long long t = 0;
-        while (p < le) {
-          while (p < le && *p == ' ') ++p;
-          if (p >= le) break;
-          const unsigned char* te = token_end(p, le);
-          if (t > 0) feature_token<T>(p, te, i, d, X, ldx, err);
+        long long pos = s, t = 0;
+        while (pos < e) {
+          const unsigned c = __ldg(text + pos);
+          if (c_end(c)) {  // blank (or NUL, already reported)
+            ++pos;
+            continue;
+          }
+          const LineBytes G{stage, 0u, pos, text, e};  // nothing staged: global memory from the token start
+          if (t > 0) feature_token<T>(G, 0, i, d, X, ldx, err);
           ++t;
-          p = te;
+          while (pos < e && !c_end(__ldg(text + pos))) ++pos;
         }
       }
       __syncwarp();
@@ -606,7 +657,7 @@ __global__ void __launch_bounds__(PARSE_THREADS) parse_kernel(const unsigned cha
 
 template <typename T>
 int parse_impl(db200_context* ctx, const unsigned char* text, long long bytes, int n, int d, T* X, long long ldx,
-               T* y, int* lines_out) {
+               T* y, int* lines_out, long long* partial_out) {
   const long long nchunks = bytes > 0 ? (bytes + CHUNK - 1) / CHUNK : 0;
   const size_t need = align_up((size_t)(nchunks + 1) * 4, 256) + align_up((size_t)(nchunks + 1) * 8, 256) +
                       align_up((size_t)(n + 2) * 8, 256) + 512;
@@ -616,9 +667,9 @@ int parse_impl(db200_context* ctx, const unsigned char* text, long long bytes, i
   int* counts = cv.take<int>((size_t)nchunks + 1);
   long long* prefix = cv.take<long long>((size_t)nchunks + 1);
   long long* starts = cv.take<long long>((size_t)n + 2);
-  long long* meta = cv.take<long long>(2);
+  long long* meta = cv.take<long long>(3);
   unsigned long long* err = cv.take<unsigned long long>(1);
-  DB200_CUDA(ctx, cudaMemsetAsync(meta, 0, 2 * sizeof(long long), ctx->stream));
+  DB200_CUDA(ctx, cudaMemsetAsync(meta, 0, 3 * sizeof(long long), ctx->stream));
   DB200_CUDA(ctx, cudaMemsetAsync(err, 0xff, sizeof(unsigned long long), ctx->stream));
   const bool al = (reinterpret_cast<uintptr_t>(text) & 15u) == 0;
   if (nchunks > 0) {
@@ -635,21 +686,26 @@ int parse_impl(db200_context* ctx, const unsigned char* text, long long bytes, i
     const long long cap = (long long)ctx->num_sms * 8;
     if (blocks > cap) blocks = cap;
     if (blocks < 1) blocks = 1;
-    parse_kernel<T><<<(unsigned)blocks, PARSE_THREADS, 0, ctx->stream>>>(text, bytes, starts, meta, d, X, ldx, y,
-                                                                          err);
+    if (al)
+      parse_kernel<T, true><<<(unsigned)blocks, PARSE_THREADS, 0, ctx->stream>>>(text, bytes, starts, meta, d, X,
+                                                                                ldx, y, err);
+    else
+      parse_kernel<T, false><<<(unsigned)blocks, PARSE_THREADS, 0, ctx->stream>>>(text, bytes, starts, meta, d, X,
+                                                                                 ldx, y, err);
     DB200_CUDA(ctx, cudaGetLastError());
     count_launch(ctx, 4);
   }
   // readback: lines parsed and the first error (pinned staging)
-  DB200_CUDA(ctx, cudaMemcpyAsync(ctx->h_pinned, meta, 2 * sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream));
-  DB200_CUDA(ctx, cudaMemcpyAsync(reinterpret_cast<char*>(ctx->h_pinned) + 16, err, sizeof(unsigned long long),
+  DB200_CUDA(ctx, cudaMemcpyAsync(ctx->h_pinned, meta, 3 * sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream));
+  DB200_CUDA(ctx, cudaMemcpyAsync(reinterpret_cast<char*>(ctx->h_pinned) + 24, err, sizeof(unsigned long long),
                                   cudaMemcpyDeviceToHost, ctx->stream));
   DB200_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  long long hm[2];
+  long long hm[3];
   unsigned long long he;
   std::memcpy(hm, ctx->h_pinned, sizeof(hm));
-  std::memcpy(&he, reinterpret_cast<char*>(ctx->h_pinned) + 16, sizeof(he));
+  std::memcpy(&he, reinterpret_cast<char*>(ctx->h_pinned) + 24, sizeof(he));
   if (lines_out) *lines_out = (int)hm[1];
+  if (partial_out) *partial_out = hm[2];
   if (he != ~0ull) {
     const long long line = (long long)(he >> 8);
     const unsigned code = (unsigned)(he & 0xffu);
@@ -663,6 +719,39 @@ int parse_impl(db200_context* ctx, const unsigned char* text, long long bytes, i
     return fail(ctx, st, "libsvm: line " + std::to_string(line + 1) + ": " + what);
   }
   return DB200_OK;
+}
+
+int parse_any(db200_context* ctx, const unsigned char* text, long long bytes, int n, int d, int dtype, void* X,
+              long long ldx, void* y, int* lines_out, long long* partial_out) {
+  return dtype == DB200_F32 ? parse_impl<float>(ctx, text, bytes, n, d, static_cast<float*>(X), ldx,
+                                                static_cast<float*>(y), lines_out, partial_out)
+                            : parse_impl<double>(ctx, text, bytes, n, d, static_cast<double*>(X), ldx,
+                                                 static_cast<double*>(y), lines_out, partial_out);
+}
+
+// Read [off, off + len) of the file into dst with up to `threads` concurrent preads.
+bool pread_parallel(int fd, char* dst, long long off, size_t len, int threads) {
+  constexpr size_t MIN_PART = 4u << 20;
+  int parts = (int)std::min<size_t>((size_t)threads, (len + MIN_PART - 1) / MIN_PART);
+  if (parts < 1) parts = 1;
+  const size_t step = (len + parts - 1) / parts;
+  std::atomic<bool> ok{true};
+  auto work = [&](int k) {
+    size_t a = (size_t)k * step, b = std::min(len, a + step);
+    while (a < b) {
+      const ssize_t r = ::pread(fd, dst + a, b - a, off + (long long)a);
+      if (r <= 0) {
+        ok = false;
+        return;
+      }
+      a += (size_t)r;
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int k = 1; k < parts; ++k) pool.emplace_back(work, k);
+  work(0);
+  for (auto& t : pool) t.join();
+  return ok;
 }
 
 }  // namespace
@@ -682,10 +771,7 @@ int db200_libsvm_parse(db200_context* ctx, const char* text, long long bytes, in
   if (n == 0 || bytes == 0) return DB200_OK;
   if (!text || !X || !y) return fail(ctx, DB200_ERR_INVALID, "db200_libsvm_parse: null pointer");
   const auto* t = reinterpret_cast<const unsigned char*>(text);
-  return dtype == DB200_F32 ? parse_impl<float>(ctx, t, bytes, n, d, static_cast<float*>(X), ldx,
-                                                static_cast<float*>(y), lines_out)
-                            : parse_impl<double>(ctx, t, bytes, n, d, static_cast<double*>(X), ldx,
-                                                 static_cast<double*>(y), lines_out);
+  return parse_any(ctx, t, bytes, n, d, dtype, X, ldx, y, lines_out, nullptr);
 }
 
 int db200_read_libsvm(db200_context* ctx, const char* path, int n, int d, int dtype, void* X, long long ldx,
@@ -694,17 +780,20 @@ int db200_read_libsvm(db200_context* ctx, const char* path, int n, int d, int dt
   if (lines_out) *lines_out = 0;
   if (!path || n < 0 || d < 1 || ldx < d || (dtype != DB200_F32 && dtype != DB200_F64))
     return fail(ctx, DB200_ERR_INVALID, "db200_read_libsvm: bad arguments");
-  FILE* f = std::fopen(path, "rb");
-  if (!f) return fail(ctx, DB200_ERR_INVALID, std::string("db200_read_libsvm: cannot open ") + path);
-  std::fseek(f, 0, SEEK_END);
-  const long long bytes = std::ftell(f);
-  std::fseek(f, 0, SEEK_SET);
-  if (n == 0 || bytes <= 0) {
-    std::fclose(f);
+  const int fd = ::open(path, O_RDONLY);
+  if (fd < 0) return fail(ctx, DB200_ERR_INVALID, std::string("db200_read_libsvm: cannot open ") + path);
+  struct stat stt;
+  const long long bytes = (::fstat(fd, &stt) == 0) ? (long long)stt.st_size : -1;
+  if (bytes < 0) {
+    ::close(fd);
+    return fail(ctx, DB200_ERR_INVALID, std::string("db200_read_libsvm: cannot stat ") + path);
+  }
+  if (n == 0 || bytes == 0) {
+    ::close(fd);
     return DB200_OK;
   }
   if (!X || !y) {
-    std::fclose(f);
+    ::close(fd);
     return fail(ctx, DB200_ERR_INVALID, "db200_read_libsvm: null pointer");
   }
   const size_t es = dtype == DB200_F32 ? 4 : 8;
@@ -712,10 +801,10 @@ int db200_read_libsvm(db200_context* ctx, const char* path, int n, int d, int dt
   const size_t off_x = align_up((size_t)bytes, 256), off_y = off_x + align_up(xbytes, 256);
   char* dev = static_cast<char*>(io_buffer(ctx, off_y + ybytes));
   if (!dev) {
-    std::fclose(f);
+    ::close(fd);
     return DB200_ERR_NOMEM;
   }
-  // File -> two pinned staging halves -> device, each copy overlapping the next read.
+  // File -> two pinned staging halves (parallel preads) -> device, each copy overlapping the next read.
   constexpr size_t PIECE = 32u << 20;
   int st = DB200_OK;
   if (ctx->h_stage_size < 2 * PIECE) {
@@ -730,11 +819,12 @@ int db200_read_libsvm(db200_context* ctx, const char* path, int n, int d, int dt
   if (!stage || cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming) != cudaSuccess)
     st = fail(ctx, DB200_ERR_NOMEM, "db200_read_libsvm: pinned staging");
+  const int threads = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
   long long done = 0;
   for (int k = 0; st == DB200_OK && done < bytes; k ^= 1) {
     const size_t len = (size_t)std::min<long long>((long long)PIECE, bytes - done);
     if (cudaEventSynchronize(ev[k]) != cudaSuccess) st = fail(ctx, DB200_ERR_CUDA, "db200_read_libsvm: event");
-    if (st == DB200_OK && std::fread(stage + k * PIECE, 1, len, f) != len)
+    if (st == DB200_OK && !pread_parallel(fd, stage + k * PIECE, done, len, threads))
       st = fail(ctx, DB200_ERR_INVALID, std::string("db200_read_libsvm: short read of ") + path);
     if (st == DB200_OK &&
         (cudaMemcpyAsync(dev + done, stage + k * PIECE, len, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess ||
@@ -742,18 +832,29 @@ int db200_read_libsvm(db200_context* ctx, const char* path, int n, int d, int dt
       st = fail(ctx, DB200_ERR_CUDA, "db200_read_libsvm: copy to device");
     done += (long long)len;
   }
-  std::fclose(f);
-  // entries the text does not name keep the caller's values, as in the reference
-  if (st == DB200_OK &&
-      (cudaMemcpyAsync(dev + off_x, X, xbytes, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess ||
-       cudaMemcpyAsync(dev + off_y, y, ybytes, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess))
-    st = fail(ctx, DB200_ERR_CUDA, "db200_read_libsvm: copy to device");
-  if (st == DB200_OK) st = db200_libsvm_parse(ctx, dev, bytes, n, d, dtype, dev + off_x, ldx, dev + off_y, lines_out);
-  if (st == DB200_OK &&
-      (cudaMemcpyAsync(X, dev + off_x, xbytes, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
-       cudaMemcpyAsync(y, dev + off_y, ybytes, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
+  ::close(fd);
+  // Parse once into the device buffers.  Only lines that leave some of their row's entries unnamed need the
+  // caller's X: then X's parsed rows go to the device first and the text is parsed again over them.  Rows and
+  // labels past the last line are never touched, so only the parsed rows come back.
+  int lines = 0;
+  long long partial = 0;
+  if (st == DB200_OK)
+    st = parse_any(ctx, reinterpret_cast<const unsigned char*>(dev), bytes, n, d, dtype, dev + off_x, ldx,
+                   dev + off_y, &lines, &partial);
+  const size_t rows_bytes = lines > 0 ? ((size_t)(lines - 1) * (size_t)ldx + (size_t)d) * es : 0;
+  if (st == DB200_OK && partial > 0) {
+    if (cudaMemcpyAsync(dev + off_x, X, rows_bytes, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess)
+      st = fail(ctx, DB200_ERR_CUDA, "db200_read_libsvm: copy to device");
+    if (st == DB200_OK)
+      st = parse_any(ctx, reinterpret_cast<const unsigned char*>(dev), bytes, n, d, dtype, dev + off_x, ldx,
+                     dev + off_y, &lines, nullptr);
+  }
+  if (st == DB200_OK && lines > 0 &&
+      (cudaMemcpyAsync(X, dev + off_x, rows_bytes, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
+       cudaMemcpyAsync(y, dev + off_y, (size_t)lines * es, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
        cudaStreamSynchronize(ctx->stream) != cudaSuccess))
     st = fail(ctx, DB200_ERR_CUDA, "db200_read_libsvm: copy to host");
+  if (lines_out) *lines_out = lines;
   cudaStreamSynchronize(ctx->stream);
   for (cudaEvent_t e : ev)
     if (e) cudaEventDestroy(e);

@@ -14,6 +14,7 @@
 #include "darray_b200/dbarrier.h"
 #include "darray_b200/dkernel.h"
 #include "darray_b200/lapack_like.h"
+#include "darray_b200/read_input.h"
 
 static int g_checks = 0;
 #define CHECK(cond, name)                                                 \
@@ -273,6 +274,22 @@ int main(int argc, char** argv) {
       res += (s - b[i]) * (s - b[i]);
     }
     CHECK(std::sqrt(res) < 1e-10, "pre_conjgrad system solved (residual < 1e-10, the reference stops at 1e-2)");
+  }
+  {  // tests/testsvm.cpp:71: read_input_file<float>(filename, n, d, x, d, y) on a small LIBSVM file
+    const char* path = "/tmp/darray_b200_dropin.libsvm";
+    std::FILE* f = std::fopen(path, "w");
+    std::fputs("+1 1:0.5 3:-2e-3\n-1 2:7\n2 1:1.25 2:0.1 3:3\n", f);
+    std::fclose(f);
+    const int n = 4, d = 3;
+    std::vector<float> x((size_t)n * d, 9.0f), y(n, 5.0f);
+    read_input_file<float>(const_cast<char*>(path), n, d, x.data(), d, y.data());
+    std::remove(path);
+    const float xe[12] = {0.5f, 9.0f, -2e-3f, 9.0f, 7.0f, 9.0f, 1.25f, 0.1f, 3.0f, 9.0f, 9.0f, 9.0f};
+    const float ye[4] = {1.0f, -1.0f, -1.0f, 5.0f};
+    bool same = true;
+    for (int i = 0; i < 12; ++i) same &= (x[i] == xe[i]);
+    for (int i = 0; i < 4; ++i) same &= (y[i] == ye[i]);
+    CHECK(same, "read_input_file (testsvm.cpp:71) reads labels and features, keeps unnamed entries");
   }
   std::printf("ALL %d CHECKS PASSED\n", g_checks);
   cuda_finalize();
