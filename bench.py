@@ -386,10 +386,10 @@ def solve_run(ctx, w, X, y, O, n_test, mixed_only=False):
     out = {"workload": f"SVM solve to duality gap 1e-6 (n={n}, d={d}, l={l}, q={w.power_iters}, C={w.C})",
            "n_test": n_test}
 
-    def one(precision):
+    def one(precision, bias=0):
         Z = torch.zeros((l, n), dtype=torch.float64, device="cuda")
         a = torch.zeros(n, dtype=torch.float64, device="cuda")
-        p = ctx.barrier_params(precision=precision)
+        p = ctx.barrier_params(precision=precision, bias=bias)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         rep = ctx.svm_solve(n, d, l, w.power_iters, X.data_ptr(), d, y.data_ptr(), O.data_ptr(), n, w.gamma, w.C,
@@ -401,11 +401,16 @@ def solve_run(ctx, w, X, y, O, n_test, mixed_only=False):
         ctx.rbf_sketch_f64(n_test, n, d, 1, dXt.data_ptr(), d, X.data_ptr(), d, 0, y.data_ptr(), a.data_ptr(), n,
                            dec.data_ptr(), n_test, w.gamma)
         ctx.sync()
-        acc = float(np.mean(np.sign(dec.cpu().numpy()) == yt))
+        acc = float(np.mean(np.sign(dec.cpu().numpy() + rep.b) == yt))
         return el, rep, acc
 
     one(0)  # warm-up: workspace growth, module load
     t_mixed, rep_m, acc_m = one(0)
+    # the SVM with a bias (the dual's y^T a = 0), which the reference leaves out
+    t_b, rep_b, acc_b = one(0, bias=1)
+    out["bias_mixed"] = {"s": t_b, "f": rep_b.f, "b": rep_b.b, "gap_pd": rep_b.gap_primal_dual,
+                         "gap_barrier": rep_b.gap_barrier, "newton": rep_b.newton, "refine": rep_b.refine,
+                         "fallbacks": rep_b.fallbacks, "acc": acc_b, "ms_barrier": rep_b.ms_barrier}
     if mixed_only:
         out.update({"mixed_s": t_mixed, "f_mixed": rep_m.f, "gap_pd_mixed": rep_m.gap_primal_dual,
                     "gap_barrier_mixed": rep_m.gap_barrier, "newton_mixed": rep_m.newton, "acc_mixed": acc_m,

@@ -23,7 +23,7 @@ class BarrierParams(ctypes.Structure):
     _fields_ = [("t0", ctypes.c_double), ("mu", ctypes.c_double), ("alpha", ctypes.c_double),
                 ("beta", ctypes.c_double), ("gap_tol", ctypes.c_double), ("newton_tol", ctypes.c_double),
                 ("max_outer", ctypes.c_int), ("max_newton", ctypes.c_int), ("precision", ctypes.c_int),
-                ("refine_max", ctypes.c_int)]
+                ("refine_max", ctypes.c_int), ("bias", ctypes.c_int)]
 
 
 class SvmReport(ctypes.Structure):
@@ -31,7 +31,8 @@ class SvmReport(ctypes.Structure):
                 ("t", ctypes.c_double), ("nu", ctypes.c_double), ("outer", ctypes.c_int), ("newton", ctypes.c_int),
                 ("status", ctypes.c_int), ("refine", ctypes.c_int), ("fallbacks", ctypes.c_int),
                 ("ms_sketch", ctypes.c_double), ("ms_orth", ctypes.c_double),
-                ("ms_core", ctypes.c_double), ("ms_barrier", ctypes.c_double), ("ms_total", ctypes.c_double)]
+                ("ms_core", ctypes.c_double), ("ms_barrier", ctypes.c_double), ("ms_total", ctypes.c_double),
+                ("b", ctypes.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

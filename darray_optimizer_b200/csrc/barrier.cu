@@ -260,13 +260,14 @@ __global__ void axpy_kernel(int n, double alpha, const double* __restrict__ x, d
 
 // Primal value pieces at w = Z^T a:  sum_i max(0, 1 - (Z w)_i)
 __global__ void __launch_bounds__(THREADS) hinge_kernel(int n, int r, const double* __restrict__ Z, long long ld,
-                                                        const double* __restrict__ w, double* red) {
+                                                        const double* __restrict__ w, double* red,
+                                                        const double* __restrict__ y, double b) {
   __shared__ double sw[MAX_R_SMEM];
   for (int k = threadIdx.x; k < r; k += blockDim.x) sw[k] = w[k];
   __syncthreads();
   double sums[1] = {0.0};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    sums[0] += fmax(0.0, 1.0 - row_dot(Z, ld, i, r, sw));
+    sums[0] += fmax(0.0, 1.0 - row_dot(Z, ld, i, r, sw) - (y ? y[i] * b : 0.0));
   block_sum_add<1>(sums, red);
 }
 
@@ -401,9 +402,10 @@ int bar_axpy(db200_context* ctx, int n, double alpha, const double* x, double* y
   return DB200_OK;
 }
 
-int bar_hinge(db200_context* ctx, int n, int r, const double* Z, long long ld, const double* w, double* red) {
+int bar_hinge(db200_context* ctx, int n, int r, const double* Z, long long ld, const double* w, double* red,
+              const double* y, double b) {
   DB200_CUDA(ctx, cudaMemsetAsync(red, 0, sizeof(double), ctx->stream));
-  hinge_kernel<<<rows_grid(ctx, n), THREADS, 0, ctx->stream>>>(n, r, Z, ld, w, red);
+  hinge_kernel<<<rows_grid(ctx, n), THREADS, 0, ctx->stream>>>(n, r, Z, ld, w, red, y, b);
   DB200_CUDA(ctx, cudaGetLastError());
   count_launch(ctx);
   return DB200_OK;

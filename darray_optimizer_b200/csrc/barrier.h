@@ -41,8 +41,9 @@ int gram_tc_weighted(db200_context* ctx, int n, int r, const double* Z, long lon
 int bar_negate(db200_context* ctx, int n, const double* x, double* y);
 // y = alpha x + beta y + gamma (x may be null)
 int bar_vec_update(db200_context* ctx, int n, double alpha, const double* x, double beta, double* y, double gamma);
-// red[0] = sum max(0, 1 - (Z w)_i)
-int bar_hinge(db200_context* ctx, int n, int r, const double* Z, long long ld, const double* w, double* red);
+// red[0] = sum max(0, 1 - (Z w)_i - y_i b)  (y null: no bias term)
+int bar_hinge(db200_context* ctx, int n, int r, const double* Z, long long ld, const double* w, double* red,
+              const double* y = nullptr, double b = 0.0);
 int bar_add_identity(db200_context* ctx, double* M, int ldm, int r);
 int bar_scale_diag(db200_context* ctx, double* M, int ldm, int r, double factor);
 int bar_dot(db200_context* ctx, int r, const double* x, const double* y, double* out);

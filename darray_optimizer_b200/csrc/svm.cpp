@@ -160,7 +160,7 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
   const size_t rr = (size_t)r * r;
   const bool mixed = (P.precision == DB200_MIXED);
   const size_t tc_bytes = mixed ? gram_tc_scratch_bytes(n, r) : 0;
-  const size_t bytes = 4096 + 7 * align_up((size_t)n * 8, 256) + 6 * align_up((size_t)r * 8, 256) +
+  const size_t bytes = 4096 + 10 * align_up((size_t)n * 8, 256) + 6 * align_up((size_t)r * 8, 256) +
                        2 * align_up(rr * 8, 256) + align_up(tc_bytes, 256) + 4096;
   char* base = static_cast<char*>(slot_buffer(ctx, SLOT_BAR, bytes));
   if (!base) return DB200_ERR_NOMEM;
@@ -168,7 +168,7 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
   double* red = cv.take<double>(64);
   double* taus = cv.take<double>(16);
   double* ls = cv.take<double>(32);
-  double* sc = cv.take<double>(8);  // scalars: [0] w.w, [1] w.v, [2] v.v, [3] hinge
+  double* sc = cv.take<double>(8);  // scalars: [0] w.w, [1] w.v, [2] v.v, [3] hinge, [4..6] products with y
   int* d_pair = cv.take<int>(4);
   double* g = cv.take<double>(n);
   double* dinv = cv.take<double>(n);
@@ -182,6 +182,9 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
   double* delta = cv.take<double>(n);
   double* zw = cv.take<double>(n);  // Z w for the current w = Z^T a (valid while zw_ok)
   double* zv = cv.take<double>(n);  // Z v for v = Z^T s, written by a refinement check
+  double* yd = cv.take<double>(n);  // labels in FP64 (bias mode)
+  double* sy = cv.take<double>(n);  // -H~^-1 y (bias mode)
+  double* gb = cv.take<double>(n);  // g + nu y (bias mode)
   void* tc_scratch = mixed ? static_cast<void*>(cv.take<char>(tc_bytes)) : nullptr;
   int refine_total = 0, fallbacks_total = 0;
   bool tc_ok = true;
@@ -193,11 +196,21 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
   double pval = 0, mval = 0;
   set_a0_host(hy, C, &pval, &mval);
   {
-    std::vector<double> ha(n);
-    for (int i = 0; i < n; ++i) ha[i] = (hy[i] == 1.0f) ? pval : mval;
+    std::vector<double> ha(n), hyd(n);
+    long plus = 0;
+    for (int i = 0; i < n; ++i) {
+      ha[i] = (hy[i] == 1.0f) ? pval : mval;
+      hyd[i] = (hy[i] == 1.0f) ? 1.0 : -1.0;
+      plus += hy[i] == 1.0f;
+    }
+    if (P.bias && (plus == 0 || plus == n))
+      return fail(ctx, DB200_ERR_INFEASIBLE, "svm_barrier: the bias needs both classes (y^T a = 0)");
     DB200_CUDA(ctx, cudaMemcpyAsync(a, ha.data(), sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+    if (P.bias)
+      DB200_CUDA(ctx, cudaMemcpyAsync(yd, hyd.data(), sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
     DB200_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   }
+  double bias_nu = 0.0;  // multiplier of y^T a = 0 at the last Newton step (the decision function's bias)
 
   double t = P.t0;
   int total_newton = 0, outer = 0, status = DB200_OK;
@@ -243,9 +256,9 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
       // until the relative residual is <= 1e-10; a step that does not get there is recomputed with the FP64
       // capacity matrix.  FP64: the capacity matrix on the FP64 pipes, no refinement.
       bool v_current = false;  // v already holds Z^T s (set by a converged refinement check)
-      auto newton_dir = [&](bool use_tc, bool* converged) -> int {
+      // Capacity matrix M = I + Z^T D^-1 Z and its Cholesky factor (upper in M, its transpose in L).
+      auto factor = [&](bool use_tc) -> int {
         int s2;
-        *converged = true;
         if (use_tc) {
           DB200_CUDA(ctx, cudaMemsetAsync(M, 0, sizeof(double) * rr, ctx->stream));
           if ((s2 = gram_tc_weighted(ctx, n, r, Z, ldz, dinv, M, r, tc_scratch))) return s2;
@@ -253,12 +266,11 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
           if ((s2 = gram<double, double>(ctx, n, r, r, Z, ldz, Z, ldz, dinv, 1.0, 0.0, M, r, true))) return s2;
         }
         if ((s2 = bar_add_identity(ctx, M, r, r))) return s2;
-        if ((s2 = bar_gemv_t(ctx, n, r, Z, ldz, g, dinv, -1.0, u))) return s2;
         // A capacity matrix with a huge dynamic range (late in the barrier D^-1 spans ~18 orders) can sit on the
         // edge of numerical positive definiteness: its last bits (the Gram's rounding and the order of its
         // split-k additions) decide whether the FP64 Cholesky passes.  A relative diagonal shift, x10 from 1e-11 up
         // to 1 until the Cholesky succeeds, keeps it positive definite; the shifted M still gives a descent
-        // direction, which the mixed path's refinement below corrects against the exact operator.
+        // direction, which the mixed path's refinement corrects against the exact operator.
         DB200_CUDA(ctx, cudaMemcpyAsync(L, M, sizeof(double) * rr, cudaMemcpyDeviceToDevice, ctx->stream));
         double eps = 1e-11;
         for (int tries = 0; tries < 12; ++tries) {
@@ -271,24 +283,32 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
           if ((s2 = bar_scale_diag(ctx, M, r, r, 1.0 + eps))) return s2;
           eps *= 10.0;
         }
-        if ((s2 = transpose64(ctx, M, r, r, r, L, r))) return s2;
+        return transpose64(ctx, M, r, r, r, L, r);
+      };
+      // out = -(Z Z^T + D)^-1 rhs by Woodbury on the factored capacity matrix.  With the tensor-core capacity
+      // matrix, iterative refinement against the exact FP64 operator (out += H~^-1 (-rhs - H out)) until the
+      // relative residual is <= 1e-10; *converged reports whether it got there.  track_v: a converged check
+      // leaves v = Z^T out and zv = Z v current.
+      auto solve = [&](const double* rhs, double* out, bool use_tc, bool* converged, bool track_v) -> int {
+        int s2;
+        *converged = true;
+        if ((s2 = bar_gemv_t(ctx, n, r, Z, ldz, rhs, dinv, -1.0, u))) return s2;
         if ((s2 = trsv_upper(ctx, M, L, r, r, u, true))) return s2;   // R^T z = rhs
         if ((s2 = trsv_upper(ctx, M, L, r, r, u, false))) return s2;  // R u = z
         if ((s2 = bar_init_red(ctx, red, 2, 0, 1))) return s2;
-        if ((s2 = bar_direction(ctx, n, r, Z, ldz, u, g, dinv, a, C, s, red))) return s2;
+        if ((s2 = bar_direction(ctx, n, r, Z, ldz, u, rhs, dinv, a, C, out, red))) return s2;
         if (!use_tc) return DB200_OK;
-        // iterative refinement against the exact FP64 operator: s += H~^-1 (-g - H s)
         *converged = false;
         double prev = 0.0;
         for (int it = 0; it <= P.refine_max; ++it) {
-          if ((s2 = bar_gemv_t(ctx, n, r, Z, ldz, s, nullptr, 1.0, v))) return s2;
+          if ((s2 = bar_gemv_t(ctx, n, r, Z, ldz, out, nullptr, 1.0, v))) return s2;
           if ((s2 = bar_init_red(ctx, red + 16, 2, 0, 0))) return s2;
-          if ((s2 = bar_residual(ctx, n, r, Z, ldz, v, g, dinv, s, res, red + 16, zv))) return s2;
+          if ((s2 = bar_residual(ctx, n, r, Z, ldz, v, rhs, dinv, out, res, red + 16, zv))) return s2;
           if ((s2 = fetch(red + 16, 2))) return s2;
           const double rn = std::sqrt(h[0]), gn = std::sqrt(h[1]);
           if (rn <= 1e-10 * gn) {
             *converged = true;
-            v_current = true;  // v = Z^T s for the final s: the line search below reuses it
+            if (track_v) v_current = true;  // v = Z^T out for the final out: the line search reuses it
             break;
           }
           if (it == P.refine_max || (it > 0 && rn >= 0.5 * prev) || !std::isfinite(rn)) break;
@@ -298,9 +318,78 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
           if ((s2 = trsv_upper(ctx, M, L, r, r, u, false))) return s2;
           if ((s2 = bar_init_red(ctx, red + 16, 2, 0, 1))) return s2;
           if ((s2 = bar_direction(ctx, n, r, Z, ldz, u, res, dinv, a, C, delta, red + 16))) return s2;
-          if ((s2 = bar_axpy(ctx, n, 1.0, delta, s))) return s2;
+          if ((s2 = bar_axpy(ctx, n, 1.0, delta, out))) return s2;
           ++refine_total;
         }
+        return DB200_OK;
+      };
+      // out = -H~^-1 rhs: one Woodbury application of the factored capacity matrix, no refinement.
+      auto apply = [&](const double* rhs, double* out, double* rd) -> int {
+        int s2;
+        if ((s2 = bar_gemv_t(ctx, n, r, Z, ldz, rhs, dinv, -1.0, u))) return s2;
+        if ((s2 = trsv_upper(ctx, M, L, r, r, u, true))) return s2;
+        if ((s2 = trsv_upper(ctx, M, L, r, r, u, false))) return s2;
+        if ((s2 = bar_init_red(ctx, rd, 2, 0, 1))) return s2;
+        return bar_direction(ctx, n, r, Z, ldz, u, rhs, dinv, a, C, out, rd);
+      };
+      // Newton direction s = -(Z Z^T + D)^-1 g.  Mixed: capacity matrix on the int8 tensor cores (Ozaki slices,
+      // ~1e-12 of the column norms) factored in FP64, then refinement; a step whose refinement misses 1e-10 is
+      // recomputed with the FP64 capacity matrix.  FP64: the capacity matrix on the FP64 pipes, no refinement.
+      //
+      // With the bias, the bordered system [H y; y^T 0][s; nu] = [-g; 0].  With s~_y = -H~^-1 y (one more
+      // application of the same factor): s = -H~^-1 g + nu s~_y with nu = -(y.s)/(y.s~_y) solves it for H~, and
+      // refinement on the bordered system reuses s~_y, each step one application like the unbordered refinement:
+      // res = g + nu y + H s, delta = -H~^-1 res, dnu = -(y.(s + delta))/(y.s~_y), s += delta + dnu s~_y,
+      // nu += dnu.  Every iterate keeps y^T s = 0, so the iterates keep y^T a = 0.
+      auto newton_dir = [&](bool use_tc, bool* converged) -> int {
+        int s2;
+        if ((s2 = factor(use_tc))) return s2;
+        if (!P.bias) {
+          if ((s2 = solve(g, s, use_tc, converged, true))) return s2;
+          if (!use_tc) return DB200_OK;  // bar_direction's statistics stand
+          if ((s2 = bar_init_red(ctx, red, 2, 0, 1))) return s2;
+          return bar_step_stats(ctx, n, g, s, a, C, red);
+        }
+        *converged = true;
+        if ((s2 = apply(g, s, red))) return s2;
+        if ((s2 = apply(yd, sy, red + 16))) return s2;
+        if ((s2 = bar_dot(ctx, n, yd, s, sc + 4))) return s2;
+        if ((s2 = bar_dot(ctx, n, yd, sy, sc + 5))) return s2;
+        if ((s2 = fetch(sc + 4, 2))) return s2;
+        const double ysy = h[1];
+        if (ysy == 0.0 || !std::isfinite(ysy))
+          return fail(ctx, DB200_ERR_NOT_SPD, "svm_barrier: bordered Newton system singular (y^T H^-1 y = 0)");
+        double nu = -h[0] / ysy;
+        if ((s2 = bar_axpy(ctx, n, nu, sy, s))) return s2;
+        if (use_tc) {
+          *converged = false;
+          double prev = 0.0;
+          for (int it = 0; it <= P.refine_max; ++it) {
+            DB200_CUDA(ctx, cudaMemcpyAsync(gb, g, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->stream));
+            if ((s2 = bar_axpy(ctx, n, nu, yd, gb))) return s2;
+            if ((s2 = bar_gemv_t(ctx, n, r, Z, ldz, s, nullptr, 1.0, v))) return s2;
+            if ((s2 = bar_init_red(ctx, red + 16, 2, 0, 0))) return s2;
+            if ((s2 = bar_residual(ctx, n, r, Z, ldz, v, gb, dinv, s, res, red + 16, zv))) return s2;
+            if ((s2 = fetch(red + 16, 2))) return s2;
+            const double rn = std::sqrt(h[0]), gn = std::sqrt(h[1]);
+            if (rn <= 1e-10 * gn) {
+              *converged = true;
+              v_current = true;  // v = Z^T s and zv = Z v for the final s
+              break;
+            }
+            if (it == P.refine_max || (it > 0 && rn >= 0.5 * prev) || !std::isfinite(rn)) break;
+            prev = rn;
+            if ((s2 = apply(res, delta, red + 16))) return s2;
+            if ((s2 = bar_axpy(ctx, n, 1.0, delta, s))) return s2;
+            if ((s2 = bar_dot(ctx, n, yd, s, sc + 6))) return s2;
+            if ((s2 = fetch(sc + 6, 1))) return s2;
+            const double dnu = -h[0] / ysy;
+            if ((s2 = bar_axpy(ctx, n, dnu, sy, s))) return s2;
+            nu += dnu;
+            ++refine_total;
+          }
+        }
+        bias_nu = nu;
         if ((s2 = bar_init_red(ctx, red, 2, 0, 1))) return s2;
         return bar_step_stats(ctx, n, g, s, a, C, red);
       };
@@ -379,7 +468,7 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
       // The barrier bound is met.  Stop once the true primal-dual gap at w = Z^T a is within tolerance too, or
       // when a further outer step no longer halves it (it is then limited by the inexact Newton solves, not t).
       if ((st = bar_dot(ctx, r, w, w, sc))) return st;
-      if ((st = bar_hinge(ctx, n, r, Z, ldz, w, sc + 3))) return st;
+      if ((st = bar_hinge(ctx, n, r, Z, ldz, w, sc + 3, P.bias ? yd : nullptr, bias_nu))) return st;
       if ((st = fetch(sc, 4))) return st;
       const double pd = (0.5 * h[0] + C * h[3] + fa) / std::fabs(fa);
       if (pd < P.gap_tol || (prev_pd >= 0 && pd > 0.5 * prev_pd)) break;
@@ -391,8 +480,8 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
     outer = P.max_outer;
     status = DB200_ERR_MAXITER;
   }
-  // primal-dual gap at w = Z^T a (w is current)
-  if ((st = bar_hinge(ctx, n, r, Z, ldz, w, sc + 3))) return st;
+  // primal-dual gap at w = Z^T a (w is current), with the bias when the dual carries y^T a = 0
+  if ((st = bar_hinge(ctx, n, r, Z, ldz, w, sc + 3, P.bias ? yd : nullptr, bias_nu))) return st;
   if ((st = fetch(sc, 4))) return st;
   const double primal = 0.5 * h[0] + C * h[3];
   if (rep) {
@@ -405,6 +494,7 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
     rep->status = status;
     rep->refine = refine_total;
     rep->fallbacks = fallbacks_total;
+    rep->b = P.bias ? bias_nu : 0.0;
     rep->ms_barrier = timer.stop_ms();
   }
   return status == DB200_ERR_MAXITER ? DB200_ERR_MAXITER : DB200_OK;
@@ -536,6 +626,7 @@ void db200_barrier_defaults(db200_barrier_params* p) {
   p->max_newton = 200;
   p->precision = DB200_MIXED;
   p->refine_max = 6;
+  p->bias = 0;
 }
 
 int db200_potrf(db200_context* ctx, int n, double* A, int lda, int nb) {

@@ -149,6 +149,10 @@ typedef struct db200_barrier_params {
   int max_outer, max_newton;
   int precision;   /* DB200_MIXED (default) or DB200_FP64, see below */
   int refine_max;  /* iterative-refinement steps per Newton solve in DB200_MIXED (default 6) */
+  int bias;        /* 0 (default): the reference's dual without a bias term.  1: the SVM with a bias, i.e. the
+                      dual's equality constraint y^T a = 0 kept by every Newton step (a bordered Woodbury solve:
+                      a second solve against y on the same capacity factor); the bias is reported in
+                      db200_svm_report.b and replaces the estimate of include/dbarrier.h:420-442 */
 } db200_barrier_params;
 
 /* Precision of the path.
@@ -165,7 +169,7 @@ typedef struct db200_barrier_params {
 typedef struct db200_svm_report {
   double f;                /* dual objective f(a) = 0.5 a^T Z Z^T a - 1^T a at the returned a */
   double gap_barrier;      /* 2n/t / |f|: the barrier method's duality-gap bound */
-  double gap_primal_dual;  /* (P(Z^T a) + f(a)) / |f|, P(w) = 0.5|w|^2 + C sum max(0, 1 - z_i.w) */
+  double gap_primal_dual;  /* (P(Z^T a, b) + f(a)) / |f|, P(w, b) = 0.5|w|^2 + C sum max(0, 1 - z_i.w - y_i b) */
   double t;                /* final barrier parameter */
   double nu;               /* shift of the Nystrom core Cholesky */
   int outer, newton;       /* barrier and Newton iterations */
@@ -174,6 +178,8 @@ typedef struct db200_svm_report {
   int fallbacks;           /* DB200_MIXED: 1 if a Newton step missed the refinement tolerance with the tensor-core
                               capacity matrix, after which the FP64 capacity matrix was used */
   double ms_sketch, ms_orth, ms_core, ms_barrier, ms_total;
+  double b;                /* bias of the decision function sum_i a_i y_i K(x_i, x) + b (params.bias = 1, else 0):
+                              the multiplier of y^T a = 0 at the last Newton step */
 } db200_svm_report;
 
 DB200_API void db200_barrier_defaults(db200_barrier_params* p);

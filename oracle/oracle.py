@@ -273,10 +273,24 @@ def newton_smw(Z, D, g) -> np.ndarray:
     return -Dinv * (g + Z @ u)
 
 
-def primal_value(Z, a, C) -> float:
-    """P(w) = 0.5 ||w||^2 + C sum max(0, 1 - z_i.w) at w = Z^T a (labels are folded into Z)."""
+def newton_smw_bias(Z, D, g, y) -> tuple[np.ndarray, float]:
+    """Newton step of the equality-constrained barrier subproblem (y^T a = 0): the bordered system
+    [H y; y^T 0] [s; nu] = [-g; 0] with H = Z Z^T + diag(D), solved by two Woodbury solves against one capacity
+    matrix: s_g = -H^-1 g, s_y = -H^-1 y, nu = -(y.s_g)/(y.s_y), s = s_g + nu s_y (so y.s = 0).  Returns s, nu."""
+    s_g = newton_smw(Z, D, g)
+    s_y = newton_smw(Z, D, np.asarray(y, F64))
+    nu = -float(y @ s_g) / float(y @ s_y)
+    return s_g + nu * s_y, nu
+
+
+def primal_value(Z, a, C, y=None, b=0.0) -> float:
+    """P(w, b) = 0.5 ||w||^2 + C sum max(0, 1 - (z_i.w + y_i b)) at w = Z^T a (labels are folded into Z); b = 0
+    for the reference's dual without bias."""
     w = Z.T @ a
-    return 0.5 * float(w @ w) + C * float(np.sum(np.maximum(0.0, 1.0 - Z @ w)))
+    m = Z @ w
+    if y is not None and b != 0.0:
+        m = m + np.asarray(y, F64) * b
+    return 0.5 * float(w @ w) + C * float(np.sum(np.maximum(0.0, 1.0 - m)))
 
 
 def initial_point(y, C) -> np.ndarray:
@@ -301,9 +315,10 @@ class BarrierResult:
     outer: int
     newton: int
     gap_barrier: float         # 2n/t / |f|
-    gap_primal_dual: float     # (P(Z^T a) + f(a)) / |f|
+    gap_primal_dual: float     # (P(Z^T a, b) + f(a)) / |f|
     status: str
     history: list = field(default_factory=list)
+    b: float = 0.0             # bias of the decision function (bias=True), from the last Newton step's multiplier
 
 
 def max_step(a, s, C, frac=0.99) -> float:
@@ -316,12 +331,21 @@ def max_step(a, s, C, frac=0.99) -> float:
 
 
 def svm_barrier(Z, y, C, t0=1.0, mu=20.0, alpha=0.1, beta=0.5, gap_tol=1e-6, newton_tol=1e-6,
-                max_outer=60, max_newton=200, a0=None) -> BarrierResult:
+                max_outer=60, max_newton=200, a0=None, bias=False) -> BarrierResult:
     """Barrier method of tests/testsvm.cpp:228-321 (constants t0=1, mu=20, alpha=0.1, beta=0.5; Newton stop
-    lambda^2/2 < 1e-6 or slow progress; D-condition stop at 1e18) with corrections 4-6."""
+    lambda^2/2 < 1e-6 or slow progress; D-condition stop at 1e18) with corrections 4-6.
+
+    bias=True adds the dual's equality constraint y^T a = 0 (the SVM with a bias term, which the reference
+    leaves out and estimates afterwards in include/dbarrier.h:420-442): the class-balanced start already satisfies
+    it, each Newton step solves the bordered system of newton_smw_bias so the iterates keep it, and the bias is
+    the step's multiplier nu (stationarity g + nu y = 0 gives y_i (g(x_i) + nu) = 1 on the margin)."""
     Z = np.asarray(Z, F64)
     n = Z.shape[0]
+    yv = np.asarray(y, F64)
+    if bias and (np.all(yv == 1) or np.all(yv != 1)):
+        raise ValueError("bias needs both classes")
     a = initial_point(y, C) if a0 is None else np.array(a0, F64)
+    b = 0.0
     t = t0
     total_newton = 0
     status = "converged"
@@ -337,7 +361,10 @@ def svm_barrier(Z, y, C, t0=1.0, mu=20.0, alpha=0.1, beta=0.5, gap_tol=1e-6, new
             D = hess_phi(a, C, t)
             if D.max() / D.min() > 1e18:
                 break
-            s = newton_smw(Z, D, g)
+            if bias:
+                s, b = newton_smw_bias(Z, D, g, yv)
+            else:
+                s = newton_smw(Z, D, g)
             lam2 = -float(g @ s)
             lastg = gg(a, Z, C, t)
             tau = max_step(a, s, C)
@@ -363,9 +390,9 @@ def svm_barrier(Z, y, C, t0=1.0, mu=20.0, alpha=0.1, beta=0.5, gap_tol=1e-6, new
     else:
         status = "outer_maxiter"
     fa = f(a, Z)
-    pd = (primal_value(Z, a, C) + fa) / abs(fa)
+    pd = (primal_value(Z, a, C, yv, b) + fa) / abs(fa)
     return BarrierResult(a=a, f=fa, t=t, outer=outer, newton=total_newton, gap_barrier=2 * n / t / abs(fa),
-                         gap_primal_dual=pd, status=status, history=hist)
+                         gap_primal_dual=pd, status=status, history=hist, b=b)
 
 
 def decision(Xtest, X, y, a, gamma, block=2048) -> np.ndarray:

@@ -105,3 +105,29 @@ def test_newton_smw_solves_the_newton_system():
     s = O.newton_smw(Z, D, r)
     H = Z @ Z.T + np.diag(D)
     assert np.allclose(H @ s, -r, rtol=1e-9, atol=1e-9)
+
+
+@pytest.mark.parametrize("C", [0.5, 4.0])
+def test_barrier_bias_matches_sklearn_svc(C):
+    """The oracle's SVM with a bias (dual constraint y^T a = 0, bordered Woodbury Newton steps) against an
+    independent solver: scikit-learn's SVC (libsvm SMO) on the same kernel Q = Z Z^T (labels unfolded).  Same dual
+    objective to 1e-6 relative, same bias to 1e-5, y^T a = 0 to round-off."""
+    from sklearn.svm import SVC
+    g = np.random.default_rng(1)
+    n, d = 400, 5
+    y = np.where(g.random(n) < 0.35, 1.0, -1.0)
+    X = g.standard_normal((n, d)) + 0.7 * y[:, None]
+    K = O.rbf_block(X, X, None, None, 0.3)
+    Q = y[:, None] * K * y[None, :]
+    ev, V = np.linalg.eigh(Q)
+    keep = ev > 1e-10 * ev.max()
+    Z = V[:, keep] * np.sqrt(ev[keep])
+    res = O.svm_barrier(Z, y, C, bias=True)
+    clf = SVC(C=C, kernel="precomputed", tol=1e-8).fit(y[:, None] * (Z @ Z.T) * y[None, :], y)
+    a_sk = np.zeros(n)
+    a_sk[clf.support_] = np.abs(clf.dual_coef_[0])
+    assert res.status == "converged"
+    assert abs(res.f - O.f(a_sk, Z)) <= 1e-6 * abs(res.f)
+    assert abs(res.b - clf.intercept_[0]) <= 1e-5
+    assert abs(float(y @ res.a)) <= 1e-10 * float(res.a.sum())
+    assert res.gap_primal_dual < 1e-6

@@ -66,6 +66,45 @@ def test_barrier_matches_oracle_on_same_factor(gpu_ctx, c1_small, precision):
     assert np.max(np.abs(a - ref.a)) <= 1e-6 * w.C
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_barrier_bias_matches_oracle(gpu_ctx, c1_small, precision):
+    """The SVM with a bias (the dual's y^T a = 0, bordered Woodbury Newton steps) against the oracle's, which
+    tests/test_oracle.py checks against scikit-learn's SVC: same objective and bias, y^T a = 0 kept."""
+    import torch
+    w, lr = c1_small
+    n, r = lr.Z.shape
+    ref = O.svm_barrier(lr.Z, w.y, w.C, bias=True)
+    dZ, dy = dev(lr.Z, np.float64), dev(w.y, np.float32)
+    da = torch.zeros(n, dtype=torch.float64, device="cuda")
+    p = gpu_ctx.barrier_params(precision=precision, bias=1)
+    rep = gpu_ctx.svm_barrier(n, r, dZ.data_ptr(), n, dy.data_ptr(), w.C, da.data_ptr(), params=p)
+    a = da.cpu().numpy()
+    assert rep.status == 0
+    tol = 1e-9 if precision == 1 else 1e-8
+    assert abs(rep.f - ref.f) <= tol * abs(ref.f)
+    assert abs(rep.b - ref.b) <= 1e-6 * max(1.0, abs(ref.b))
+    assert abs(float(w.y.astype(np.float64) @ a)) <= 1e-10 * float(a.sum())
+    assert rep.gap_barrier < 1e-6 and rep.gap_primal_dual < 1e-6
+    assert np.all(a > 0) and np.all(a < w.C)
+    assert np.max(np.abs(a - ref.a)) <= 1e-6 * w.C
+    # the bias changes the solution: the no-bias dual reaches a lower objective (fewer constraints)
+    nob = O.svm_barrier(lr.Z, w.y, w.C)
+    assert nob.f <= ref.f
+
+
+def test_barrier_bias_needs_both_classes(gpu_ctx, c1_small):
+    import torch
+    from darray_optimizer_b200._lib import DB200Error
+    w, lr = c1_small
+    n, r = lr.Z.shape
+    dZ, dy = dev(lr.Z, np.float64), dev(np.ones(n, np.float32), np.float32)
+    da = torch.zeros(n, dtype=torch.float64, device="cuda")
+    with pytest.raises(DB200Error) as e:
+        gpu_ctx.svm_barrier(n, r, dZ.data_ptr(), n, dy.data_ptr(), w.C, da.data_ptr(),
+                            params=gpu_ctx.barrier_params(bias=1))
+    assert e.value.status == -5  # DB200_ERR_INFEASIBLE
+
+
 def test_barrier_iteration_caps_report_maxiter(gpu_ctx, c1_small):
     import torch
     w, lr = c1_small
