@@ -269,6 +269,8 @@ def run_ours(args):
         extra["c5"] = c5_run(ctx)
     if args.libsvm and rank == 0:
         extra["libsvm"] = libsvm_run(ctx)
+    if args.lu and rank == 0:
+        extra["lu"] = lu_run(ctx)
     return finish(args, ctx, w, rep, ms_max, kernel_ms, kernel_count, launches, clocks, e2e_val, h2d, d2h, Om,
                   solve, batch, extra)
 
@@ -575,6 +577,53 @@ def libsvm_run(ctx, n=N_POINTS, d=D_FEAT, steps=5, cpu_lines=8192):
     return out
 
 
+def lu_run(ctx, n=8192, steps=3, cpu_n=4096):
+    """LU leg (perftests/perftest_lu.cpp's workload: uniform(-2, 2) FP32, partial pivoting): db200_lu_factorize on
+    an n x n matrix resident in HBM, GFLOP/s = (2/3) n^3 / time (CUDA events, a fresh copy of the matrix per
+    step); the reference's own lu_factorize_partial_pivot<float> (include/lapack_like.h:179-279, built into
+    oracle/_ref at one rank) on cpu_n x cpu_n as the CPU baseline."""
+    import ctypes
+    import torch
+    g = torch.Generator(device="cuda").manual_seed(8192)
+    A0 = (torch.rand((n, n), generator=g, device="cuda", dtype=torch.float32) * 4.0 - 2.0)
+    A = torch.empty_like(A0)
+    ipiv = torch.zeros(n, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream()
+    A.copy_(A0)
+    ctx.lu_factorize(n, n, A.data_ptr(), n, ipiv.data_ptr())  # warm-up
+    times = []
+    for _ in range(steps):
+        A.copy_(A0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ctx.lu_factorize(n, n, A.data_ptr(), n, ipiv.data_ptr())
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    ms = statistics.median(times)
+    piv = ipiv.cpu().numpy()
+    out = {"workload": f"LU with partial pivoting, n={n}, uniform(-2, 2) FP32", "ms": ms,
+           "gflops": 2.0 / 3.0 * n ** 3 / (ms / 1e3) / 1e9,
+           "pivots_valid": bool(np.all(piv >= np.arange(1, n + 1)) and np.all(piv <= n)),
+           # column-major L (strictly below the diagonal) is the strict upper triangle of the row-major view
+           "max_abs_l": float(torch.triu(A, diagonal=1).abs().max())}
+    ref_lib = ROOT / "oracle" / "_ref" / "libdarray_ref.so"
+    if ref_lib.exists():
+        lib = ctypes.CDLL(str(ref_lib))
+        fp, ip = ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_int)
+        lib.ref_lu.argtypes = [fp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ip]
+        Ah = np.asfortranarray(np.random.default_rng(0).uniform(-2, 2, (cpu_n, cpu_n)).astype(np.float32))
+        ph = np.zeros(cpu_n, np.int32)
+        t0 = time.perf_counter()
+        lib.ref_lu(Ah.ctypes.data_as(fp), cpu_n, cpu_n, 256, ph.ctypes.data_as(ip))
+        cs = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": 2.0 / 3.0 * cpu_n ** 3 / cs / 1e9, "unit": "GFLOP/s",
+                               "cores": os.cpu_count(), "kind": "reference",
+                               "sample": f"lu_factorize_partial_pivot<float>, n={cpu_n}, bs=256, one rank "
+                                         f"(OpenBLAS threads for its sgemm/strsm), {cs:.2f} s"}
+    return out
+
+
 def finish(args, ctx, w, rep, ms_max, kernel_ms, kernel_count, launches, clocks, e2e_val, h2d, d2h, Om,
            solve=None, batch=None, extra=None):
     world, rank = rep.world, rep.rank
@@ -647,6 +696,8 @@ def main():
     ap.add_argument("--c5", action="store_true", help="add the learned-landmark leg (n = 524288, r = 2048)")
     ap.add_argument("--libsvm", action="store_true",
                     help="add the LIBSVM input leg (C2 points as text, GPU reader vs the reference's reader)")
+    ap.add_argument("--lu", action="store_true",
+                    help="add the LU leg (n = 8192 FP32, partial pivoting; the reference's LU as CPU baseline)")
     ap.add_argument("--n-test", type=int, default=16384, help="held-out points for the solve leg's accuracy")
     ap.add_argument("--n", type=int, default=N_POINTS, help="points (default: the C2 workload, 131072)")
     args = ap.parse_args()

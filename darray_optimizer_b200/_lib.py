@@ -156,6 +156,7 @@ SIGNATURES = {
                                            _u64, _c_int, _c_int, _c_double, _vp, _c_int, _c_int, _c_int,
                                            ctypes.POINTER(BarrierParams), _vp, _vp, _c_int, ctypes.POINTER(SvmReport),
                                            ctypes.POINTER(LandmarkReport)]),
+    "db200_lu_factorize": (_c_int, [_vp, _c_int, _c_int, _c_int, _vp, _c_int, _vp, _c_int, _c_int]),
     "db200_libsvm_parse": (_c_int, [_vp, _vp, ctypes.c_longlong, _c_int, _c_int, _c_int, _vp, ctypes.c_longlong, _vp,
                                     ctypes.POINTER(_c_int)]),
     "db200_read_libsvm": (_c_int, [_vp, ctypes.c_char_p, _c_int, _c_int, _c_int, _vp, ctypes.c_longlong, _vp,
@@ -165,7 +166,7 @@ SIGNATURES = {
 STATUS = {
     0: "DB200_OK", -1: "DB200_ERR_INVALID", -2: "DB200_ERR_CUDA", -3: "DB200_ERR_NOT_SPD",
     -4: "DB200_ERR_MAXITER", -5: "DB200_ERR_INFEASIBLE", -6: "DB200_ERR_TIMEOUT", -7: "DB200_ERR_NOMEM",
-    -8: "DB200_ERR_UNSUPPORTED", -9: "DB200_ERR_TOO_LARGE",
+    -8: "DB200_ERR_UNSUPPORTED", -9: "DB200_ERR_TOO_LARGE", -10: "DB200_ERR_SINGULAR",
 }
 NOALLOC_SCRATCH_BYTES = 32 << 20
 POINT_MAJOR, FEATURE_MAJOR = 0, 1
@@ -391,6 +392,9 @@ class Context:
         if st not in (0, -4):
             self.check(st)
         return rep, lrep
+
+    def lu_factorize(self, m, n, A, lda, ipiv, pivot=1, nleft=0, swap_left_panels=1):
+        return self.check(self.lib.db200_lu_factorize(self.h, m, n, nleft, A, lda, ipiv, pivot, swap_left_panels))
 
     def libsvm_parse(self, text, nbytes, n, d, dtype, X, ldx, y):
         """db200_libsvm_parse on device text; returns the lines parsed."""

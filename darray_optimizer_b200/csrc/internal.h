@@ -78,6 +78,10 @@ struct Carve {
   }
 };
 
+// ------------------------------------------------------------------ LU (lu.cu)
+int lu_factorize(db200_context* ctx, int m, int n, int nleft, float* A, long long lda, int* ipiv, int pivot,
+                 int swap_left_panels);
+
 // ------------------------------------------------------------------ RBF tile engine (rbf_tile.cu)
 enum RbfMode { RBF_MODE_SKETCH = 0, RBF_MODE_KBLOCK = 1 };
 

@@ -37,6 +37,7 @@ extern "C" {
 #define DB200_ERR_NOMEM (-7)       /* device allocation failed */
 #define DB200_ERR_UNSUPPORTED (-8) /* shape outside what the kernels implement */
 #define DB200_ERR_TOO_LARGE (-9)   /* request exceeds the fixed scratch of db200_rbf_sketch_noalloc */
+#define DB200_ERR_SINGULAR (-10)   /* LU met a zero pivot */
 
 /* Layout of a point matrix X holding n points of d features. */
 #define DB200_POINT_MAJOR 0   /* x(i,k) = X[k + i*ldx]  (the reference's DMatrix X, d x n column major) */
@@ -442,6 +443,21 @@ DB200_API int db200_svm_solve_landmarks(db200_context* ctx, int n, int d, int r,
                                         const float* Omega, int ldo, int l_fb, int q,
                                         const db200_barrier_params* params, double* a, double* Z, int ldz,
                                         db200_svm_report* rep, db200_landmark_report* lrep);
+
+/* LU factorisation of the m x n FP32 matrix A (device, column major, lda >= m) in place: A = P L U with L unit
+ * lower (below the diagonal) and U upper, blocked right-looking with panels of 32 columns.  Replaces
+ * lu_factorize_partial_pivot (include/lapack_like.h:179-219, the unblocked panel of :220-279),
+ * lu_factorize_partial_pivot_replicate_panel (:134-177) and lu_factorize_no_pivot (:93-131):
+ *   pivot = 1: partial pivoting, the pivot of column j the row of largest |a| at or below j (the first such row on
+ *     ties, as the reference's scan); ipiv[j] (device, min(m, n) ints) = 1-based pivot row relative to A's first
+ *     row, as LAPACK and the reference record it;
+ *   pivot = 0: no interchanges (ipiv[j] = j + 1).
+ *   swap_left_panels = 1: every panel's interchanges also reach the columns of earlier panels and the nleft
+ *     columns that precede A in memory (A - nleft*lda ...), as lu_factorize_partial_pivot permutes the rows left
+ *     of the factored block (:212); 0: only the columns right of the panel, as the replicate_panel variant (:162).
+ * A zero pivot returns DB200_ERR_SINGULAR naming its column (the reference asserts).  Synchronous. */
+DB200_API int db200_lu_factorize(db200_context* ctx, int m, int n, int nleft, float* A, int lda, int* ipiv,
+                                 int pivot, int swap_left_panels);
 
 /* ------------------------------------------------------------------ LIBSVM text input */
 #define DB200_F32 0 /* float X and y */

@@ -1,5 +1,7 @@
 // One-rank mirror of include/blas_like.h: matrix_multiply (T,N) and triangular_solve (L,U,T) on the GPU.
 #pragma once
+#include <cassert>
+#include <vector>
 #include "cblas_like.h"
 #include "darray.h"
 #include "detail.h"
@@ -49,6 +51,29 @@ void triangular_solve(const char* side, const char* uplo, const char* transa, co
   upload(db, B, m, n, Bdesc.matrix.lld());
   check(db200_trsm_lutn(ctx(), m, n, da.p, m, db.p, m), "triangular_solve");
   download(B, m, n, Bdesc.matrix.lld(), db);
+}
+
+// C = alpha L U + beta C with L the unit lower triangle of A and U the upper triangle of B, all n x n
+// (include/blas_like.h:9-60: the product that checks an LU factorisation).  FP64 product on the GPU.
+template <typename T>
+void triangular_triangular_multiply(DMatrix<T>& A, DMatrix<T>& B, DMatrix<T>& C, T alpha, T beta) {
+  using namespace darray_b200::detail;
+  const int n = C.dims()[0];
+  assert(C.dims()[1] == n && A.dims()[0] == n && B.dims()[1] == n);
+  std::vector<double> L((size_t)n * n, 0.0), U((size_t)n * n, 0.0);
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < n; ++i) {
+      if (i > j) L[i + (size_t)j * n] = A(i, j);
+      else if (i == j) L[i + (size_t)j * n] = 1.0;
+      if (i <= j) U[i + (size_t)j * n] = B(i, j);
+    }
+  Dev<double> dl((size_t)n * n), du((size_t)n * n), dc((size_t)n * n);
+  upload(dl, L.data(), n, n, n);
+  upload(du, U.data(), n, n, n);
+  upload(dc, C.data(), n, n, C.lld());
+  check(db200_gemm(ctx(), 'N', 'N', n, n, n, (double)alpha, dl.p, n, du.p, n, (double)beta, dc.p, n),
+        "triangular_triangular_multiply");
+  download(C.data(), n, n, C.lld(), dc);
 }
 
 }  // namespace DArray

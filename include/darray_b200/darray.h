@@ -178,13 +178,14 @@ class LMatrix {
 template <typename T>
 class DMatrix {
  public:
-  DMatrix(Grid& grid, int m, int n) : m_grid(grid), m_dims{m, n}, m_lld(std::max(m, 1)) {
+  DMatrix(Grid& grid, int m, int n)
+      : m_grid(grid), m_dims{m, n}, m_lld(std::max(m, 1)), m_ipiv(std::max(m, 0), -1) {
     m_storage = std::shared_ptr<T[]>(new T[(size_t)m_lld * std::max(n, 1)]());
     m_data = m_storage.get();
   }
   // attach to a caller buffer holding the global block starting at (i1, j1)
   DMatrix(Grid& grid, int m, int n, T* buf, int ld, int i1, int j1)
-      : m_grid(grid), m_dims{m, n}, m_lld(ld), m_data(buf - (i1 + (size_t)j1 * ld)) {}
+      : m_grid(grid), m_dims{m, n}, m_lld(ld), m_ipiv(std::max(m, 0), -1), m_data(buf - (i1 + (size_t)j1 * ld)) {}
 
   DMatrix<T> clone() {
     DMatrix<T> A(m_grid, m_dims[0], m_dims[1]);
@@ -246,6 +247,29 @@ class DMatrix {
   LMatrix<T> copy_upper_to_lower(LMatrix<T> A, int, int) { return A; }
   LMatrix<T> copy_lower_to_upper(LMatrix<T> A, int, int) { return A; }
   static std::array<int, 2> global_to_local_index(std::array<int, 2> ij, int, int, int) { return ij; }
+  // pivot rows of the last LU factorisation, 1-based (include/darray.h:437-486)
+  std::vector<int>& ipiv() { return m_ipiv; }
+  // exchange rows i1 and i2 in columns [j1, j2)
+  void swap_rows(int i1, int i2, int j1, int j2) {
+    for (int j = j1; j < j2; ++j) std::swap(at(i1, j), at(i2, j));
+  }
+  // the row interchanges ipiv (1-based, relative to i1) applied in order to rows [i1, i2) of columns [j1, j2)
+  // (include/darray.h:1202-1212)
+  void permute_rows_ipiv(int i1, int j1, int i2, int j2, int* ipiv, int n_ipiv) {
+    (void)i2;
+    for (int k = 0; k < n_ipiv; ++k) {
+      const int p = ipiv[k] - 1 + i1;
+      if (p != i1 + k) swap_rows(i1 + k, p, j1, j2);
+    }
+  }
+  // the inverse: the same interchanges in reverse order (include/darray.h:1181-1200)
+  void permute_rows_inverse_ipiv(int i1, int j1, int i2, int j2, int* ipiv, int n_ipiv) {
+    (void)i2;
+    for (int k = n_ipiv - 1; k >= 0; --k) {
+      const int p = ipiv[k] - 1 + i1;
+      if (p != i1 + k) swap_rows(i1 + k, p, j1, j2);
+    }
+  }
   void substract(DMatrix<T>& A) {
     for (int j = 0; j < m_dims[1]; ++j)
       for (int i = 0; i < m_dims[0]; ++i) at(i, j) -= A.at(i, j);
@@ -269,6 +293,7 @@ class DMatrix {
   Grid m_grid;
   std::array<int, 2> m_dims;
   int m_lld;
+  std::vector<int> m_ipiv;
   std::shared_ptr<T[]> m_storage;
   T* m_data = nullptr;
 };

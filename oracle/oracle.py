@@ -260,6 +260,40 @@ def pre_conjgrad(Z, M, D, b, a, tol=1e-2, max_iter=100000) -> tuple[np.ndarray, 
     return x, it
 
 
+def lu_partial_pivot(A, pivot=True) -> tuple[np.ndarray, np.ndarray]:
+    """LU with partial pivoting, restated from lu_factorize_partial_pivot / lu_factorize_unblocked
+    (include/lapack_like.h:179-279) in FP64: for each column j the pivot is the first row of largest |a| at or
+    below j, the rows are swapped across the whole matrix, the column below the diagonal is scaled by the
+    reciprocal pivot and the trailing block takes the rank-1 update.  Returns the packed factors (L unit lower
+    below the diagonal, U on and above it) and ipiv (1-based pivot rows, as A.ipiv()).  pivot=False: no
+    interchanges."""
+    A = np.array(A, F64, order="F")
+    m, n = A.shape
+    mn = min(m, n)
+    ipiv = np.arange(1, mn + 1, dtype=np.int64)
+    for j in range(mn):
+        if pivot:
+            p = j + int(np.argmax(np.abs(A[j:, j])))  # argmax returns the first of equal values
+            ipiv[j] = p + 1
+            if p != j:
+                A[[j, p], :] = A[[p, j], :]
+        d = A[j, j]
+        if d == 0.0:
+            raise ZeroDivisionError(f"zero pivot in column {j + 1}")
+        A[j + 1:, j] *= 1.0 / d
+        A[j + 1:, j + 1:] -= np.outer(A[j + 1:, j], A[j, j + 1:])
+    return A, ipiv
+
+
+def lu_apply_ipiv(A, ipiv) -> np.ndarray:
+    """P A: the row interchanges ipiv (1-based) applied in order, as permute_rows_ipiv (include/darray.h:1202)."""
+    B = np.array(A, copy=True)
+    for i, p in enumerate(np.asarray(ipiv) - 1):
+        if p != i:
+            B[[i, p], :] = B[[p, i], :]
+    return B
+
+
 def newton_smw(Z, D, g) -> np.ndarray:
     """s = -(Z Z^T + diag(D))^-1 g by Sherman-Morrison-Woodbury: u solves (I + Z^T D^-1 Z) u = -Z^T D^-1 g,
     then s = -D^-1 (g + Z u)."""

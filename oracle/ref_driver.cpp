@@ -128,6 +128,17 @@ void ref_writemodel(const char* path, int n, int d, int k, double* a, double C, 
   LMatrix<double> Xm(d, n, d, X);
   DArray::writemodel<double>(std::string(path), n, d, k, A, C, Zm, Ym, Xm, gamma, minus, plus);
 }
+// lu_factorize_partial_pivot (include/lapack_like.h:179-219) on an m x n FP32 matrix (column major, in place)
+// with outer block bs; ipiv receives A.ipiv() (1-based global rows).  (The replicate_panel variant, :134-177,
+// does not compile when instantiated: :152 passes a std::vector<int> where permute_rows_ipiv takes int*.)
+void ref_lu(float* A, int m, int n, int bs, int* ipiv) {
+  DMatrix<float> M(grid(), m, n);
+  load(M, A, m, n);
+  DArray::lu_factorize_partial_pivot(M, 0, 0, m, n, bs);
+  store(M, A, m, n);
+  const int mn = m < n ? m : n;
+  for (int i = 0; i < mn; ++i) ipiv[i] = M.ipiv()[i];
+}
 // read_input_file<T> (include/read_input.h:8-36): X is d x n column major (point-major), Y n labels.  The
 // reference indexes X with stride d and ignores ldx.
 void ref_read_input_file_f32(const char* filename, int n, int d, float* X, float* Y) {

@@ -275,6 +275,21 @@ int main(int argc, char** argv) {
     }
     CHECK(std::sqrt(res) < 1e-10, "pre_conjgrad system solved (residual < 1e-10, the reference stops at 1e-2)");
   }
+  {  // tests/test4.cpp / perftests/perftest_lu.cpp: LU with partial pivoting, then P L U against A
+    const int n = 300;
+    DArray::DMatrix<float> A(g, n, n);
+    A.set_normal_seed(0, 1, 5);
+    auto A0 = A.clone();
+    auto A00 = A.clone();
+    DArray::lu_factorize_partial_pivot(A, 0, 0, n, n, 64);
+    DArray::triangular_triangular_multiply(A, A, A0, 1.0f, 0.0f);
+    A0.permute_rows_inverse_ipiv(0, 0, n, n, A.ipiv().data(), (int)A.ipiv().size());
+    const double fnA = A00.fnorm();
+    A00.substract(A0);
+    bool piv_ok = true;
+    for (int i = 0; i < n; ++i) piv_ok &= (A.ipiv()[i] >= i + 1 && A.ipiv()[i] <= n);
+    CHECK(piv_ok && A00.fnorm() / fnA < 1e-5, "test4 lu_factorize_partial_pivot: fnorm(A - P L U)/fnorm(A) < 1e-5");
+  }
   {  // tests/testsvm.cpp:71: read_input_file<float>(filename, n, d, x, d, y) on a small LIBSVM file
     const char* path = "/tmp/darray_b200_dropin.libsvm";
     std::FILE* f = std::fopen(path, "w");
