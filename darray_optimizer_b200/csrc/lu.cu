@@ -13,10 +13,12 @@
 // Pivots are recorded 1-based relative to the first row, like LAPACK's ipiv and the reference's.
 #include <cfloat>
 #include <cmath>
+#include <algorithm>
 #include <cstring>
 #include <string>
 
 #include "internal.h"
+#include "ptx.cuh"
 
 namespace db200 {
 
@@ -132,6 +134,172 @@ __global__ void __launch_bounds__(PANEL_THREADS) lu_panel_kernel(float* A, long 
   }
 }
 
+// ------------------------------------------------------------------ cooperative panel
+// The panel's rows split over G co-resident CTAs, each holding its slice (R rows x w columns) in shared memory.
+// Per column one grid barrier: before it every CTA publishes its best pivot candidate (value, row, the row's w
+// values) and the owner of row j publishes row j; after it every CTA picks the same pivot from the G candidates,
+// the owners of rows j and p exchange them in shared memory, and every CTA scales and updates its own rows.  The
+// published slots alternate between two buffers by column parity: a CTA writes slot (jj & 1) only after the
+// barrier of column jj - 1, which every CTA reaches after it has read the slots of column jj - 2.
+constexpr int CP_THREADS = 256;
+constexpr int CP_MAX_ROWS = 1536;   // rows per CTA held in shared memory (1536 x 32 x 4 B = 192 KB)
+constexpr int CAND = W + 2;         // candidate record: |value|, row, the row's W values
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Grid-wide barrier among the CTAs of a cooperative launch, bounded: a wait that exceeds the limit (or sees
+// another CTA's timeout) sets *status and returns false in every thread of the CTA.
+__device__ bool grid_barrier(unsigned* count, unsigned target, int* status) {
+  __syncthreads();
+  int ok = 1;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(count, 1u);
+    const uint64_t t0 = global_timer_ns();
+    while (ld_acquire_u32(count) < target) {
+      if (*reinterpret_cast<volatile int*>(status)) {
+        ok = 0;
+        break;
+      }
+      if (global_timer_ns() - t0 > DB200_WAIT_TIMEOUT_NS) {
+        atomicExch(status, 1);
+        ok = 0;
+        break;
+      }
+    }
+    __threadfence();
+  }
+  return __syncthreads_and(ok) != 0;
+}
+
+__global__ void __launch_bounds__(CP_THREADS) lu_panel_coop_kernel(float* A, long long lda, int m, int k, int w,
+                                                                   int R, int* ipiv, int pivot, int* singular,
+                                                                   unsigned* bar, unsigned bar_base, float* cand,
+                                                                   float* rowj, int* status) {
+  extern __shared__ float tile[];  // [W][R]: tile[c * R + i] = A[r0 + i, k + c]
+  __shared__ float urow[W];
+  __shared__ float red_v[CP_THREADS / 32];
+  __shared__ int red_i[CP_THREADS / 32];
+  __shared__ int s_win;
+  const int tid = threadIdx.x, lane = tid % 32, wid = tid / 32;
+  const int G = gridDim.x, b = blockIdx.x;
+  const int r0 = k + b * R;
+  const int rows = max(0, min(R, m - r0));
+  for (int e = tid; e < w * R; e += CP_THREADS) {
+    const int c = e / R, i = e % R;
+    tile[c * R + i] = i < rows ? A[(r0 + i) + (long long)(k + c) * lda] : 0.0f;
+  }
+  __syncthreads();
+  for (int jj = 0; jj < w; ++jj) {
+    const int j = k + jj, par = jj & 1;
+    float* my_cand = cand + ((size_t)par * G + b) * CAND;
+    // local candidate: the largest |a| of column jj among own rows >= j, the smallest row on ties
+    float bv = -1.0f;
+    int bi = m;
+    for (int i = tid; i < rows; i += CP_THREADS) {
+      const int r = r0 + i;
+      const float v = fabsf(tile[jj * R + i]);
+      if (r >= j && v > bv) {
+        bv = v;
+        bi = r;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ov > bv || (ov == bv && oi < bi)) {
+        bv = ov;
+        bi = oi;
+      }
+    }
+    if (lane == 0) {
+      red_v[wid] = bv;
+      red_i[wid] = bi;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      for (int q = 1; q < CP_THREADS / 32; ++q)
+        if (red_v[q] > bv || (red_v[q] == bv && red_i[q] < bi)) {
+          bv = red_v[q];
+          bi = red_i[q];
+        }
+      my_cand[0] = bv;
+      my_cand[1] = __int_as_float(bi);
+      s_win = bi;
+    }
+    __syncthreads();
+    const int lbi = s_win;
+    if (tid < w) my_cand[2 + tid] = (lbi < m) ? tile[tid * R + (lbi - r0)] : 0.0f;
+    if (j >= r0 && j < r0 + rows && tid < w) rowj[par * W + tid] = tile[tid * R + (j - r0)];
+    if (!grid_barrier(bar, bar_base + (unsigned)(jj + 1) * (unsigned)G, status)) return;
+    // the same pivot in every CTA: the largest candidate, the smallest row on ties (one warp scans the G records)
+    if (wid == 0) {
+      float gv = -1.0f;
+      int gb = -1, gi = m;
+      for (int q = lane; q < G; q += 32) {
+        const float* cq = cand + ((size_t)par * G + q) * CAND;
+        const float v = cq[0];
+        const int r = __float_as_int(cq[1]);
+        if (v > gv || (v == gv && r < gi)) {
+          gv = v;
+          gi = r;
+          gb = q;
+        }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const float ov = __shfl_xor_sync(0xffffffffu, gv, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, gi, o);
+        const int ob = __shfl_xor_sync(0xffffffffu, gb, o);
+        if (ov > gv || (ov == gv && oi < gi)) {
+          gv = ov;
+          gi = oi;
+          gb = ob;
+        }
+      }
+      if (lane == 0) {
+        s_win = pivot ? gb : -1;
+        if (b == 0) ipiv[j] = (pivot && gi < m) ? gi + 1 : j + 1;
+        red_i[0] = (pivot && gi < m) ? gi : j;
+      }
+    }
+    __syncthreads();
+    const int p = red_i[0], wb = s_win;
+    if (tid < w) {
+      const float* src = (wb >= 0 && p != j) ? cand + ((size_t)par * G + wb) * CAND + 2 : rowj + par * W;
+      urow[tid] = src[tid];
+    }
+    __syncthreads();
+    if (p != j && tid < w) {
+      if (p >= r0 && p < r0 + rows) tile[tid * R + (p - r0)] = rowj[par * W + tid];  // old row j to row p
+      if (j >= r0 && j < r0 + rows) tile[tid * R + (j - r0)] = urow[tid];           // pivot row to row j
+    }
+    __syncthreads();
+    const float d = urow[jj];
+    if (d == 0.0f) {
+      if (b == 0 && tid == 0) atomicCAS(singular, 0, j + 1);
+      continue;
+    }
+    const float inv = 1.0f / d;
+    for (int i = tid; i < rows; i += CP_THREADS) {
+      if (r0 + i <= j) continue;
+      const float l = tile[jj * R + i] * inv;
+      tile[jj * R + i] = l;
+      for (int c = jj + 1; c < w; ++c) tile[c * R + i] = fmaf(-l, urow[c], tile[c * R + i]);
+    }
+    __syncthreads();
+  }
+  for (int e = tid; e < w * R; e += CP_THREADS) {
+    const int c = e / R, i = e % R;
+    if (i < rows) A[(r0 + i) + (long long)(k + c) * lda] = tile[c * R + i];
+  }
+}
+
 // Row interchanges ipiv[k .. k+w) (1-based, relative to row 0) applied in order to columns [c0, c1) and
 // [c2, c3).
 __global__ void lu_laswp_kernel(float* A, long long lda, int k, int w, const int* ipiv, int c0, int c1, int c2,
@@ -223,12 +391,49 @@ __global__ void __launch_bounds__(256) lu_update_kernel(float* A, long long lda,
 int lu_factorize(db200_context* ctx, int m, int n, int nleft, float* A, long long lda, int* ipiv, int pivot,
                  int swap_left_panels) {
   const int mn = m < n ? m : n;
-  int* singular = static_cast<int*>(slot_buffer(ctx, SLOT_LA, 256));
-  if (!singular) return DB200_ERR_NOMEM;
-  DB200_CUDA(ctx, cudaMemsetAsync(singular, 0, sizeof(int), ctx->stream));
+  int* singular = nullptr;
+  // cooperative panel: scratch for the candidates, row j and the barrier counter; how many CTAs fit at once
+  static_assert(CP_MAX_ROWS * W * 4 <= 200 * 1024, "panel slice too large");
+  const size_t cp_smem = (size_t)CP_MAX_ROWS * W * sizeof(float);
+  char* scr = static_cast<char*>(slot_buffer(ctx, SLOT_LA, 256 + 2 * 4096 * CAND * sizeof(float) + 2 * W * 4 + 256));
+  if (!scr) return DB200_ERR_NOMEM;
+  singular = reinterpret_cast<int*>(scr);
+  unsigned* bar = reinterpret_cast<unsigned*>(scr + 64);
+  int* cstatus = reinterpret_cast<int*>(scr + 128);
+  float* cand = reinterpret_cast<float*>(scr + 256);
+  float* rowj = cand + 2 * 4096 * CAND;
+  DB200_CUDA(ctx, cudaMemsetAsync(scr, 0, 256, ctx->stream));
+  int coop_max = 0;
+  {
+    int coop = 0, per_sm = 0;
+    DB200_CUDA(ctx, cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, ctx->device));
+    DB200_CUDA(ctx, cudaFuncSetAttribute(lu_panel_coop_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)cp_smem));
+    DB200_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lu_panel_coop_kernel, CP_THREADS,
+                                                                  cp_smem));
+    if (coop && per_sm > 0) coop_max = std::min(ctx->num_sms * per_sm, 4096);
+  }
+  unsigned bar_base = 0;
   for (int k = 0; k < mn; k += W) {
     const int w = mn - k < W ? mn - k : W;
-    lu_panel_kernel<<<1, PANEL_THREADS, 0, ctx->stream>>>(A, lda, m, k, w, ipiv, pivot, singular);
+    const int rows = m - k;
+    // CTAs of at least 64 rows each, at most one slice of CP_MAX_ROWS per CTA
+    int G = std::min(coop_max, (rows + 63) / 64);
+    const int R = G > 0 ? (rows + G - 1) / G : 0;
+    if (G > 0 && R <= CP_MAX_ROWS) {
+      if (bar_base > 0x40000000u) {  // keep the monotone barrier target far from wrapping
+        DB200_CUDA(ctx, cudaMemsetAsync(bar, 0, sizeof(unsigned), ctx->stream));
+        bar_base = 0;
+      }
+      void* args[] = {&A, &lda, &m, &k, (void*)&w, (void*)&R, &ipiv, &pivot, &singular, &bar, &bar_base, &cand,
+                      &rowj, &cstatus};
+      DB200_CUDA(ctx, cudaLaunchCooperativeKernel((const void*)lu_panel_coop_kernel, dim3((unsigned)G),
+                                                  dim3(CP_THREADS), args, (size_t)R * W * sizeof(float),
+                                                  ctx->stream));
+      bar_base += (unsigned)w * (unsigned)G;
+    } else {
+      lu_panel_kernel<<<1, PANEL_THREADS, 0, ctx->stream>>>(A, lda, m, k, w, ipiv, pivot, singular);
+    }
     DB200_CUDA(ctx, cudaGetLastError());
     int launches = 1;
     if (pivot) {
@@ -259,10 +464,12 @@ int lu_factorize(db200_context* ctx, int m, int n, int nleft, float* A, long lon
     }
     count_launch(ctx, launches);
   }
-  int sing = 0;
-  DB200_CUDA(ctx, cudaMemcpyAsync(ctx->h_pinned, singular, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  int sing = 0, to = 0;
+  DB200_CUDA(ctx, cudaMemcpyAsync(ctx->h_pinned, scr, 256, cudaMemcpyDeviceToHost, ctx->stream));
   DB200_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   std::memcpy(&sing, ctx->h_pinned, sizeof(int));
+  std::memcpy(&to, reinterpret_cast<char*>(ctx->h_pinned) + 128, sizeof(int));
+  if (to) return fail(ctx, DB200_ERR_TIMEOUT, "lu_factorize: a panel's grid barrier gave up");
   if (sing) return fail(ctx, DB200_ERR_SINGULAR, "lu_factorize: zero pivot in column " + std::to_string(sing));
   return DB200_OK;
 }
