@@ -301,23 +301,35 @@ int db200_lra_host(db200_context* ctx, int n, int d, int k, const float* X, int 
   if (n < 0 || d < 1 || k < 0 || !X || !Y || !O || !A || ldx < d || ldo < n || lda < n)
     return fail(ctx, DB200_ERR_INVALID, "lra_host: bad arguments");
   if (n == 0 || k == 0) return DB200_OK;
+  // A result in page-locked host memory that the device can address is written by the kernel itself: its
+  // stores drain over the host link while the kernel runs, instead of a copy after it.  Pageable memory takes the
+  // staged copy.
+  float* direct = nullptr;
+  {
+    cudaPointerAttributes pa;
+    if (cudaPointerGetAttributes(&pa, A) == cudaSuccess && pa.type == cudaMemoryTypeHost && pa.devicePointer)
+      direct = static_cast<float*>(pa.devicePointer);
+    cudaGetLastError();  // an unregistered pointer may leave an error behind on older drivers
+  }
   const size_t bx = align_up(sizeof(float) * (size_t)n * d, 256), by = align_up(sizeof(float) * (size_t)n, 256),
                bo = align_up(sizeof(float) * (size_t)n * k, 256);
-  char* io = static_cast<char*>(io_buffer(ctx, bx + by + 2 * bo));
+  char* io = static_cast<char*>(io_buffer(ctx, bx + by + (direct ? 1 : 2) * bo));
   if (!io) return DB200_ERR_NOMEM;
   float* dX = reinterpret_cast<float*>(io);
   float* dY = reinterpret_cast<float*>(io + bx);
   float* dO = reinterpret_cast<float*>(io + bx + by);
-  float* dA = reinterpret_cast<float*>(io + bx + by + bo);
+  float* dA = direct ? direct : reinterpret_cast<float*>(io + bx + by + bo);
+  const int ldA = direct ? lda : n;
   DB200_CUDA(ctx, cudaMemcpy2DAsync(dX, sizeof(float) * d, X, sizeof(float) * ldx, sizeof(float) * d, n,
                                     cudaMemcpyHostToDevice, ctx->stream));
   DB200_CUDA(ctx, cudaMemcpyAsync(dY, Y, sizeof(float) * n, cudaMemcpyHostToDevice, ctx->stream));
   DB200_CUDA(ctx, cudaMemcpy2DAsync(dO, sizeof(float) * n, O, sizeof(float) * ldo, sizeof(float) * n, k,
                                     cudaMemcpyHostToDevice, ctx->stream));
-  int st = db200_rbf_sketch(ctx, n, n, d, k, dX, d, dX, d, DB200_POINT_MAJOR, dY, dY, dO, n, dA, n, gamma);
+  int st = db200_rbf_sketch(ctx, n, n, d, k, dX, d, dX, d, DB200_POINT_MAJOR, dY, dY, dO, n, dA, ldA, gamma);
   if (st) return st;
-  DB200_CUDA(ctx, cudaMemcpy2DAsync(A, sizeof(float) * lda, dA, sizeof(float) * n, sizeof(float) * n, k,
-                                    cudaMemcpyDeviceToHost, ctx->stream));
+  if (!direct)
+    DB200_CUDA(ctx, cudaMemcpy2DAsync(A, sizeof(float) * lda, dA, sizeof(float) * n, sizeof(float) * n, k,
+                                      cudaMemcpyDeviceToHost, ctx->stream));
   return db200_synchronize(ctx);
 }
 

@@ -108,8 +108,10 @@ DB200_API int db200_rbf_block(db200_context* ctx, int m, int n, int d, const flo
  *     A(n x k) = diag(Y) K(X, X) diag(Y) O
  * X is the d x n feature matrix (column major, ldx >= d: the reference's DMatrix X of tests/testsvm.cpp:76),
  * Y the n labels, O the n x k test matrix (ldo >= n), A the n x k result (lda >= n).  Copies in, runs the fused
- * kernel over every block (the reference stops after the first, include/dkernel.h:43) and copies out;
- * synchronous.  Stands in for the rbf_kernel + tc_gemm host round trips of include/dkernel.cu:132-231.
+ * kernel over every block (the reference stops after the first, include/dkernel.h:43) and copies out; when A is
+ * page-locked host memory the device can address (cudaMallocHost / cudaHostAlloc / registered), the kernel writes
+ * it directly and no copy follows.  Synchronous.  Stands in for the rbf_kernel + tc_gemm host round trips of
+ * include/dkernel.cu:132-231.
  */
 DB200_API int db200_lra_host(db200_context* ctx, int n, int d, int k, const float* X, int ldx, const float* Y,
                              const float* O, int ldo, float* A, int lda, float gamma);

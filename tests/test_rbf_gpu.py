@@ -159,3 +159,29 @@ def test_bounded_wait_expiry_reports_timeout_and_context_survives(gpu_ctx):
     gpu_ctx.sync()
     err = rel_fro(colmajor_host(Y, n), O.sketch(X, X, y, y, Om, 0.1))
     assert err <= 2e-3, err
+
+
+@pytest.mark.parametrize("pinned,pad", [(False, 0), (True, 0), (True, 5)])
+def test_lra_host_matches_oracle(gpu_ctx, pinned, pad):
+    """db200_lra_host (DArray::LRA's host-pointer convention): pageable result buffers take the staged copy,
+    page-locked ones are written by the kernel directly; both give the oracle's sketch (fp16 sketch operands:
+    relative Frobenius error <= 2e-3), and rows past n of a padded result stay untouched."""
+    import torch
+    n, d, k = 1000, 24, 40
+    X = _points(n, d, 21, 0.5)
+    y = _labels(n, 21)
+    g = np.random.default_rng(22)
+    Om = np.asfortranarray(g.standard_normal((n, k)).astype(np.float32))
+    gamma = 1.0 / d
+    ref = O.sketch(X, X, y, y, Om, gamma)
+    lda = n + pad
+    Xh = torch.from_numpy(np.ascontiguousarray(X))
+    yh = torch.from_numpy(y)
+    Oh = torch.from_numpy(np.ascontiguousarray(Om.T))
+    Ah = torch.full((k, lda), 7.0, dtype=torch.float32)
+    if pinned:
+        Xh, yh, Oh, Ah = Xh.pin_memory(), yh.pin_memory(), Oh.pin_memory(), Ah.pin_memory()
+    gpu_ctx.lra_host(n, d, k, Xh.data_ptr(), d, yh.data_ptr(), Oh.data_ptr(), n, Ah.data_ptr(), lda, gamma)
+    A = Ah.numpy()
+    assert rel_fro(A[:, :n].T, ref) <= 2e-3
+    assert np.all(A[:, n:] == 7.0)
