@@ -2,7 +2,9 @@
 learned-versus-uniform comparison.
 
 Training data (all on the GPU, through the library's own kernels):
-  * seeded mixture instances (datagen.mixture, n = 16384, d = 64);
+  * seeded instances of one workload family at n = 16384: the C5 mixture (datagen.mixture, d = 64; the default
+    model, landmark_model.npz) or the C2 uniform-hyperplane points (datagen.uniform_hyperplane, d = 128;
+    landmark_model_c2.npz);
   * inputs: [x, ||x||, distance to the 8th nearest neighbour] (db200_knn_distance over all points,
     db200_leverage_features);
   * targets: log ridge leverage scores of the instance's kernel matrix, centred per instance.  The scores come
@@ -12,8 +14,8 @@ Training data (all on the GPU, through the library's own kernels):
 Training: the MLP of db200_mlp (3 hidden ReLU layers of 256, bf16 weights and activations) by Adam on minibatches
 (db200_mlp_adam_step).  The model file holds the fp32 parameters, the input standardisation and the settings.
 
-    python -m darray_optimizer_b200.landmarks train --out <file.npz> [--instances 200]
-    python -m darray_optimizer_b200.landmarks evaluate [--model <file.npz>]
+    python -m darray_optimizer_b200.landmarks train [--config c5|c2] [--out <file.npz>] [--instances 200]
+    python -m darray_optimizer_b200.landmarks evaluate [--config c5|c2] [--model <file.npz>]
 """
 from __future__ import annotations
 
@@ -33,6 +35,11 @@ MODEL_PATH = PKG / "landmark_model.npz"
 WIDTH, HIDDEN, KNN_K = 256, 3, 8
 TRAIN_N, TRAIN_D, TRAIN_L = 16384, 64, 528
 DEFF_FRACTION = 1.0 / 64
+# workload families a model is trained on: generator of one seeded training instance, feature count, model file
+CONFIGS = {
+    "c5": (lambda seed: datagen.mixture(n=TRAIN_N, d=64, seed=seed), 64, MODEL_PATH),
+    "c2": (lambda seed: datagen.uniform_hyperplane(n=TRAIN_N, d=128, seed=seed), 128, PKG / "landmark_model_c2.npz"),
+}
 
 
 def _ptr(t):
@@ -93,13 +100,14 @@ def instance_targets(ctx: Context, w: datagen.Workload, l: int = TRAIN_L, q: int
 
 
 def train(ctx: Context, instances: int = 200, epochs: int = 8, batch: int = 8192, lr: float = 1e-3,
-          seed: int = 1, holdout: int = 10, log=print):
-    """Train the leverage model; returns (net, info)."""
+          seed: int = 1, holdout: int = 10, log=print, config: str = "c5"):
+    """Train the leverage model on `config`'s workload family; returns (net, mean, scale, info)."""
     import torch
+    make, dim, _ = CONFIGS[config]
     t0 = time.perf_counter()
     Fs, ts, lams = [], [], []
     for k in range(instances + holdout):
-        w = datagen.mixture(n=TRAIN_N, d=TRAIN_D, seed=10_000 + k)
+        w = make(10_000 + k)
         F, t, lam = instance_targets(ctx, w)
         Fs.append(F)
         ts.append(t)
@@ -111,7 +119,7 @@ def train(ctx: Context, instances: int = 200, epochs: int = 8, batch: int = 8192
     t_data = time.perf_counter() - t0
     mean = F_all.mean(0).cpu().numpy().astype(np.float32)
     scale = (1.0 / torch.clamp(F_all.std(0), min=1e-6)).cpu().numpy().astype(np.float32)
-    net = Mlp(ctx, TRAIN_D + 2, WIDTH, HIDDEN, seed=seed)
+    net = Mlp(ctx, dim + 2, WIDTH, HIDDEN, seed=seed)
     net.set_input_scaling(mean, scale)
     m = F_all.shape[0]
     gen = torch.Generator(device="cuda")
@@ -139,7 +147,7 @@ def train(ctx: Context, instances: int = 200, epochs: int = 8, batch: int = 8192
             val.append(float(sum(vl) / F_val.shape[0]))
         log(f"epoch {ep + 1}/{epochs}: train loss {np.mean(losses[-steps_per_epoch:]):.4f}"
             + (f", held-out loss {val[-1]:.4f}" if val else ""))
-    info = {"instances": instances, "holdout": holdout, "n": TRAIN_N, "d": TRAIN_D, "l": TRAIN_L,
+    info = {"config": config, "instances": instances, "holdout": holdout, "n": TRAIN_N, "d": dim, "l": TRAIN_L,
             "deff_fraction": DEFF_FRACTION, "lambda_median": float(np.median(lams)), "epochs": epochs,
             "batch": batch, "lr": lr, "seconds_data": t_data, "seconds_total": time.perf_counter() - t0,
             "loss_first": float(losses[0]), "loss_last_epoch": float(np.mean(losses[-steps_per_epoch:])),
@@ -149,7 +157,7 @@ def train(ctx: Context, instances: int = 200, epochs: int = 8, batch: int = 8192
 
 def save_model(path, net: Mlp, mean, scale, info):
     np.savez_compressed(path, params=net.get_params(), mean=mean, scale=scale, width=WIDTH, hidden=HIDDEN,
-                        in_dim=TRAIN_D + 2, info=json.dumps(info))
+                        in_dim=net.in_dim, info=json.dumps(info))
 
 
 def load_model(ctx: Context, path=MODEL_PATH) -> Mlp:
@@ -183,10 +191,11 @@ def landmark_residual(ctx: Context, w: datagen.Workload, r: int, net: Mlp | None
     return ctx.residual_estimate(n, d, _ptr(X), d, _ptr(y), w.gamma, r, _ptr(Z), n, S.numel(), _ptr(S))
 
 
-def evaluate(ctx: Context, net: Mlp, seeds=(90_001, 90_002, 90_003), n: int = TRAIN_N, r: int = 512):
+def evaluate(ctx: Context, net: Mlp, seeds=(90_001, 90_002, 90_003), r: int = 512, config: str = "c5"):
+    make = CONFIGS[config][0]
     out = []
     for s in seeds:
-        w = datagen.mixture(n=n, d=TRAIN_D, seed=s)
+        w = make(s)
         out.append({"seed": s, "learned": landmark_residual(ctx, w, r, net, s),
                     "uniform": landmark_residual(ctx, w, r, None, s)})
     return out
@@ -196,21 +205,23 @@ def main(argv=None):
     import torch
     ap = argparse.ArgumentParser()
     ap.add_argument("cmd", choices=["train", "evaluate"])
-    ap.add_argument("--out", default=str(MODEL_PATH))
-    ap.add_argument("--model", default=str(MODEL_PATH))
+    ap.add_argument("--config", choices=sorted(CONFIGS), default="c5")
+    ap.add_argument("--out", default=None)
+    ap.add_argument("--model", default=None)
     ap.add_argument("--instances", type=int, default=200)
     ap.add_argument("--epochs", type=int, default=8)
     args = ap.parse_args(argv)
     torch.cuda.init()
     ctx = Context(0, torch.cuda.current_stream().cuda_stream)
+    default_path = str(CONFIGS[args.config][2])
     if args.cmd == "train":
-        net, mean, scale, info = train(ctx, instances=args.instances, epochs=args.epochs)
-        info["evaluation"] = evaluate(ctx, net)
-        save_model(args.out, net, mean, scale, info)
+        net, mean, scale, info = train(ctx, instances=args.instances, epochs=args.epochs, config=args.config)
+        info["evaluation"] = evaluate(ctx, net, config=args.config)
+        save_model(args.out or default_path, net, mean, scale, info)
         print(json.dumps(info))
     else:
-        net = load_model(ctx, args.model)
-        print(json.dumps(evaluate(ctx, net)))
+        net = load_model(ctx, args.model or default_path)
+        print(json.dumps(evaluate(ctx, net, config=args.config)))
 
 
 if __name__ == "__main__":

@@ -11,7 +11,7 @@ pytestmark = pytest.mark.gpu
 def test_learned_landmarks_beat_uniform(gpu_ctx):
     from darray_optimizer_b200 import landmarks
     net = landmarks.load_model(gpu_ctx)
-    res = landmarks.evaluate(gpu_ctx, net, seeds=(90_011, 90_012, 90_013), n=16384, r=512)
+    res = landmarks.evaluate(gpu_ctx, net, seeds=(90_011, 90_012, 90_013), r=512)
     learned = np.array([r["learned"] for r in res])
     uniform = np.array([r["uniform"] for r in res])
     print("learned", learned, "uniform", uniform)
