@@ -50,12 +50,14 @@ def sketch_plan(l):
 
 def executed_flops(n, d, l):
     """Tensor-core flops the tile kernel actually issues per pass: three split products per padded feature for
-    the distance Gram, once per panel, plus the sketch product over the padded panel width."""
+    the distance Gram, once per panel, plus the sketch product over the sketch width padded to 16 (panels of
+    exact widths, e.g. 528 = 272 + 256)."""
     npad = -(-n // 256) * 256
     dp = -(-d // 32) * 32
-    panels, panel = sketch_plan(l)
+    panels, _ = sketch_plan(l)
+    lpad = -(-l // 16) * 16
     tiles = (npad / 128) ** 2
-    return 2.0 * tiles * panels * (3 * dp * 128 * 128 + 128 * panel * 128)
+    return 2.0 * tiles * (panels * 3 * dp * 128 * 128 + 128 * lpad * 128)
 
 
 def config(extra=None):
@@ -677,7 +679,7 @@ def finish(args, ctx, w, rep, ms_max, kernel_ms, kernel_count, launches, clocks,
                             else "fallback 1400 sustained"),
             "tensor_executed_tflops": executed, "tensor_executed_frac": executed / peak,
             "tensor_executed_note": "split-bf16 distance products (3 per feature) recomputed per sketch panel, "
-                                    "sketch product over the padded panel width"}
+                                    "sketch product over the width padded to 16"}
     traffic_file = ROOT / "profiles" / "rbf_sketch_traffic.json"
     if traffic_file.exists():
         try:

@@ -274,7 +274,7 @@ int db200_rbf_sketch(db200_context* ctx, int m, int n, int d, int l, const float
   void* op = carve.take<uint16_t>((size_t)plan.lrows * npad);
   st = pack_sketch(ctx, Omega, ldo, yj, n, l, npad, plan.lrows, op);
   if (st) return st;
-  return launch_rbf_tiles(ctx, RBF_MODE_SKETCH, pi, pj, yi, nullptr, op, plan, l, gamma, Y, ldy);
+  return launch_rbf_sketch_exact(ctx, pi, pj, yi, op, plan, l, gamma, Y, ldy);
 }
 
 int db200_rbf_block(db200_context* ctx, int m, int n, int d, const float* Xi, int ldxi, const float* Xj, int ldxj,

@@ -154,4 +154,8 @@ int launch_rbf_tiles(db200_context* ctx, int mode, const PackedPoints& pi, const
                      const float* yj, const void* op, const SketchPlan& plan, int l, float gamma, float* out,
                      int ldo, void* table_storage = nullptr, size_t table_capacity = 0);
 
+// The sketch as one launch over per-panel instances of exact widths (plan.n_panels panels covering roundup(l, 16)).
+int launch_rbf_sketch_exact(db200_context* ctx, const PackedPoints& pi, const PackedPoints& pj, const float* yi,
+                            const void* op, const SketchPlan& plan, int l, float gamma, float* out, int ldo);
+
 }  // namespace db200

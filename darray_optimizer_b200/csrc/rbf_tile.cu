@@ -890,4 +890,38 @@ int launch_rbf_tiles(db200_context* ctx, int mode, const PackedPoints& pi, const
   return launch_rbf_plan(ctx, T);
 }
 
+// A sketch wider than one panel as one launch over per-panel instances of exact widths: the padded width
+// roundup(l, 16) split into plan.n_panels panels of multiples of 16 that differ by at most 16 columns (528 =
+// 272 + 256 instead of 2 x 272), so no panel computes sketch columns past l beyond the last multiple of 16.
+int launch_rbf_sketch_exact(db200_context* ctx, const PackedPoints& pi, const PackedPoints& pj, const float* yi,
+                            const void* op, const SketchPlan& plan, int l, float gamma, float* out, int ldo) {
+  if (plan.n_panels <= 1)
+    return launch_rbf_tiles(ctx, RBF_MODE_SKETCH, pi, pj, yi, nullptr, op, plan, l, gamma, out, ldo);
+  const int units = (l + 15) / 16, np = plan.n_panels;
+  std::vector<TileJob> jobs((size_t)np);
+  int off = 0;
+  for (int p = 0; p < np; ++p) {
+    const int w = 16 * (units / np + (p < units % np ? 1 : 0));
+    TileJob& J = jobs[(size_t)p];
+    J.pi = pi;
+    J.pj = pj;
+    J.yi = yi;
+    J.yj = nullptr;
+    J.op = static_cast<const uint16_t*>(op) + (size_t)off * pj.npad;  // packed rows = sketch columns
+    J.plan.n_panels = 1;
+    J.plan.panel = w;
+    J.plan.lrows = w;
+    J.plan.g_bufs = (w + 64 + 2 * 128 <= TMEM_COLS) ? 2 : 1;
+    J.l = std::min(w, l - off);
+    J.gamma = gamma;
+    J.out = out + (size_t)off * ldo;
+    J.ldo = ldo;
+    off += w;
+  }
+  TilePlan T;
+  int st = prepare_rbf_tiles(ctx, RBF_MODE_SKETCH, jobs.data(), np, nullptr, 0, &T);
+  if (st) return st;
+  return launch_rbf_plan(ctx, T);
+}
+
 }  // namespace db200
