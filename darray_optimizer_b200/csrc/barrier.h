@@ -37,7 +37,7 @@ int bar_step_stats(db200_context* ctx, int n, const double* g, const double* s, 
 // gram_tc.cu: M (upper, FP64) += (D^-1/2 Z)^T (D^-1/2 Z) on the int8 tensor cores (Ozaki slices)
 size_t gram_tc_scratch_bytes(int n, int r);
 int gram_tc_weighted(db200_context* ctx, int n, int r, const double* Z, long long ldz, const double* w, double* M,
-                     int ldm, void* scratch);
+                     int ldm, void* scratch, int slices = 8);
 int bar_negate(db200_context* ctx, int n, const double* x, double* y);
 // y = alpha x + beta y + gamma (x may be null)
 int bar_vec_update(db200_context* ctx, int n, double alpha, const double* x, double beta, double* y, double gamma);

@@ -34,20 +34,21 @@
 namespace db200 {
 namespace {
 
-constexpr int KS = 8;                          // int8 digits per value (groups g = s + t in [2, KS + 1])
+constexpr int KS_MAX = 8;                      // int8 digits per value at most (groups g = s + t in [2, KS + 1])
 constexpr int TM = 128;                        // M tile: rows p of M
 constexpr int TN = 64;                         // N tile: columns q of M
 constexpr int KB = 64;                         // k bytes per stage: one 64-byte swizzled row per operand row
 constexpr int ASL = TM * KB;                   // one A slice per stage, 8 KB
 constexpr int BSL = TN * KB;                   // one B slice per stage, 4 KB
-constexpr int STAGE = KS * (ASL + BSL);        // 96 KB
+template <int KS>
+constexpr int stage_bytes() { return KS * (ASL + BSL); }  // 96 KB at 8 digits
 constexpr int NSTAGE = 2;
 constexpr int CH = 16384;                      // rows per scaling chunk (and at most per CTA: exact s32 sums)
 constexpr int MAX_CHUNKS = CH / KB;            // k chunks (64 rows) per scaling chunk
-constexpr int TMEM_COLS = 512;                 // KS * TN columns of s32 groups
+constexpr int TMEM_COLS = 512;                 // KS * TN columns of s32 groups (at most 512)
 constexpr int THREADS = 192;                   // warp 0 TMA, warp 1 MMA, warps 2..5 epilogue
-static_assert(KS * TN <= TMEM_COLS, "group accumulators exceed TMEM");
-static_assert((long long)KS * MAX_CHUNKS * KB * 127 * 127 < (1LL << 31), "s32 group sums could overflow");
+static_assert(KS_MAX * TN <= TMEM_COLS, "group accumulators exceed TMEM");
+static_assert((long long)KS_MAX * MAX_CHUNKS * KB * 127 * 127 < (1LL << 31), "s32 group sums could overflow");
 constexpr int SLICE_CTAS = 4;                  // CTAs (of 256 threads x 16 rows) per scaling chunk
 static_assert(SLICE_CTAS * 256 * 16 == CH && CH / SLICE_CTAS == 256 * 16, "slice_kernel covers a chunk per cluster");
 
@@ -70,8 +71,10 @@ __device__ __forceinline__ int exp_above(double m) {
   return bits == 0 ? 0 : biased - 1022;
 }
 
+template <int KS>
 __global__ void __launch_bounds__(THREADS, 1)
     gram_i8_kernel(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ CUtensorMap tm_b, GramArgs g) {
+  constexpr int STAGE = stage_bytes<KS>();
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const uint32_t s_op = smem_u32(smem);
@@ -226,7 +229,7 @@ __global__ void sqrt_weights_kernel(const double* __restrict__ w, int n, double*
 //  3. Each thread turns its 16 values into KS digits and parks them in a shared [KS][4096] byte tile.
 //  4. The CTA writes every slice row out with coalesced 16-byte stores (zero for padding rows and columns).
 // VEC: Z and ldz allow 16-byte loads.
-template <bool VEC>
+template <bool VEC, int KS>
 __global__ void __cluster_dims__(1, SLICE_CTAS, 1) __launch_bounds__(256)
     slice_kernel(const double* __restrict__ Z, long long ldz, const double* __restrict__ sw, int n, int r, int npad,
                  int rpad, int* __restrict__ exps, int8_t* __restrict__ slices) {
@@ -315,12 +318,12 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 }
 
 // 3-D map over the slices (x = i bytes, y = p, z = slice), box 64 bytes x box_rows x KS, 64-byte swizzle.
-bool tmap_slices(CUtensorMap* tm, const void* base, uint64_t npad, uint64_t rpad, uint32_t box_rows) {
+bool tmap_slices(CUtensorMap* tm, const void* base, uint64_t npad, uint64_t rpad, uint32_t box_rows, int ks) {
   auto enc = encode_fn();
   if (!enc) return false;
-  cuuint64_t dims[3] = {npad, rpad, (cuuint64_t)KS};
+  cuuint64_t dims[3] = {npad, rpad, (cuuint64_t)ks};
   cuuint64_t strides[2] = {npad, npad * rpad};
-  cuuint32_t box[3] = {(cuuint32_t)KB, box_rows, (cuuint32_t)KS};
+  cuuint32_t box[3] = {(cuuint32_t)KB, box_rows, (cuuint32_t)ks};
   cuuint32_t estr[3] = {1, 1, 1};
   return enc(tm, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void*>(base), dims, strides, box, estr,
              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
@@ -332,13 +335,15 @@ bool tmap_slices(CUtensorMap* tm, const void* base, uint64_t npad, uint64_t rpad
 size_t gram_tc_scratch_bytes(int n, int r) {
   const size_t npad = (size_t)round_up(n, KB), rpad = (size_t)round_up(r, TM);
   const size_t nchunk = (npad + CH - 1) / CH;
-  return align_up((size_t)KS * npad * rpad, 256) + align_up(nchunk * rpad * sizeof(int), 256) +
+  return align_up((size_t)KS_MAX * npad * rpad, 256) + align_up(nchunk * rpad * sizeof(int), 256) +
          align_up((size_t)n * sizeof(double), 256) + 512;
 }
 
-// M (upper triangle, FP64, r x r) += Z~^T Z~ with Z~ = diag(sqrt(w)) Z.  `scratch` holds gram_tc_scratch_bytes.
-int gram_tc_weighted(db200_context* ctx, int n, int r, const double* Z, long long ldz, const double* w, double* M,
-                     int ldm, void* scratch) {
+namespace {
+template <int KS>
+int gram_tc_run(db200_context* ctx, int n, int r, const double* Z, long long ldz, const double* w, double* M,
+                int ldm, void* scratch) {
+  constexpr int STAGE = stage_bytes<KS>();
   if (n <= 0 || r <= 0) return DB200_OK;
   const int npad = round_up(n, KB), rpad = round_up(r, TM);
   const int nchunk = (npad + CH - 1) / CH;
@@ -351,15 +356,15 @@ int gram_tc_weighted(db200_context* ctx, int n, int r, const double* Z, long lon
   count_launch(ctx);
   const bool vec = (reinterpret_cast<uintptr_t>(Z) % 16 == 0) && (ldz % 2 == 0);
   if (vec)
-    slice_kernel<true><<<dim3(rpad, nchunk * SLICE_CTAS), 256, 0, ctx->stream>>>(Z, ldz, sw, n, r, npad, rpad, exps,
+    slice_kernel<true, KS><<<dim3(rpad, nchunk * SLICE_CTAS), 256, 0, ctx->stream>>>(Z, ldz, sw, n, r, npad, rpad, exps,
                                                                                 slices);
   else
-    slice_kernel<false><<<dim3(rpad, nchunk * SLICE_CTAS), 256, 0, ctx->stream>>>(Z, ldz, sw, n, r, npad, rpad, exps,
+    slice_kernel<false, KS><<<dim3(rpad, nchunk * SLICE_CTAS), 256, 0, ctx->stream>>>(Z, ldz, sw, n, r, npad, rpad, exps,
                                                                                  slices);
   DB200_CUDA(ctx, cudaGetLastError());
   count_launch(ctx);
   CUtensorMap ta, tb;
-  if (!tmap_slices(&ta, slices, npad, rpad, TM) || !tmap_slices(&tb, slices, npad, rpad, TN))
+  if (!tmap_slices(&ta, slices, npad, rpad, TM, KS) || !tmap_slices(&tb, slices, npad, rpad, TN, KS))
     return fail(ctx, DB200_ERR_CUDA, "gram_tc: cuTensorMapEncodeTiled failed");
   GramArgs a;
   a.r = r;
@@ -392,15 +397,29 @@ int gram_tc_weighted(db200_context* ctx, int n, int r, const double* Z, long lon
   a.ldm = ldm;
   a.status = ctx->d_status;
   const size_t smem = NSTAGE * STAGE + 512 + 1024;
-  DB200_CUDA(ctx, cudaFuncSetAttribute(gram_i8_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  DB200_CUDA(ctx, cudaFuncSetAttribute(gram_i8_kernel<KS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   dim3 grid(pairs, splits);
   cudaEvent_t e0 = nullptr;
   prof_begin(ctx, &e0);
-  gram_i8_kernel<<<grid, THREADS, smem, ctx->stream>>>(ta, tb, a);
+  gram_i8_kernel<KS><<<grid, THREADS, smem, ctx->stream>>>(ta, tb, a);
   DB200_CUDA(ctx, cudaGetLastError());
   prof_end(ctx, e0);
   count_launch(ctx);
   return DB200_OK;
+}
+}  // namespace
+
+// M (upper triangle, FP64, r x r) += Z~^T Z~ with Z~ = diag(sqrt(w)) Z from `slices` int8 digits per value (5..8;
+// error about 2e-8, 3e-10, 3e-12, 3e-14 of ||Z~_p|| ||Z~_q||).  `scratch` holds gram_tc_scratch_bytes.
+int gram_tc_weighted(db200_context* ctx, int n, int r, const double* Z, long long ldz, const double* w, double* M,
+                     int ldm, void* scratch, int slices) {
+  switch (slices) {
+    case 5: return gram_tc_run<5>(ctx, n, r, Z, ldz, w, M, ldm, scratch);
+    case 6: return gram_tc_run<6>(ctx, n, r, Z, ldz, w, M, ldm, scratch);
+    case 7: return gram_tc_run<7>(ctx, n, r, Z, ldz, w, M, ldm, scratch);
+    case 8: return gram_tc_run<8>(ctx, n, r, Z, ldz, w, M, ldm, scratch);
+    default: return fail(ctx, DB200_ERR_INVALID, "gram_tc: slices must be 5..8");
+  }
 }
 
 }  // namespace db200

@@ -212,7 +212,7 @@ int db200_gram_weighted(db200_context* ctx, int n, int r, const double* Z, int l
   void* scratch = slot_buffer(ctx, SLOT_SPARE, gram_tc_scratch_bytes(n, r));
   if (!scratch) return DB200_ERR_NOMEM;
   DB200_CUDA(ctx, cudaMemset2DAsync(M, sizeof(double) * ldm, 0, sizeof(double) * r, r, ctx->stream));
-  return gram_tc_weighted(ctx, n, r, Z, ldz, w, M, ldm, scratch);
+  return gram_tc_weighted(ctx, n, r, Z, ldz, w, M, ldm, scratch, use_tensor_cores >= 5 ? use_tensor_cores : 8);
 }
 
 int db200_rbf_sketch_f64(db200_context* ctx, int m, int n, int d, int l, const float* Xi, int ldxi, const float* Xj,

@@ -187,6 +187,13 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
   double* gb = cv.take<double>(n);  // g + nu y (bias mode)
   void* tc_scratch = mixed ? static_cast<void*>(cv.take<char>(tc_bytes)) : nullptr;
   int refine_total = 0, fallbacks_total = 0;
+  // Tensor-core capacity matrix: 8 int8 digits per value (36 products, ~3e-14 of the column norms), after that
+  // the FP64 capacity matrix.  From r = 2048 the Gram (n r^2) outweighs the refinement passes (n r) that a coarser
+  // capacity matrix costs, so there the ladder starts at 6 digits (21 products, ~3e-10) while the refinement
+  // converges with it.  (Measured: 6 digits first cut the barrier at n = 524288, r = 2064 from 8.6 to 7.3 s, and
+  // lengthened it at r = 528 from 181 to 221 ms and at r = 1040 from 0.83 to 1.28 s.)
+  constexpr int kSlices[2] = {6, 8};
+  int tc_level = (r >= 2048) ? 0 : 1;  // index into kSlices; 2 = FP64
   bool tc_ok = true;
 
   // class-balanced start (tests/testsvm.cpp:192-212)
@@ -261,7 +268,7 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
         int s2;
         if (use_tc) {
           DB200_CUDA(ctx, cudaMemsetAsync(M, 0, sizeof(double) * rr, ctx->stream));
-          if ((s2 = gram_tc_weighted(ctx, n, r, Z, ldz, dinv, M, r, tc_scratch))) return s2;
+          if ((s2 = gram_tc_weighted(ctx, n, r, Z, ldz, dinv, M, r, tc_scratch, kSlices[tc_level]))) return s2;
         } else {
           if ((s2 = gram<double, double>(ctx, n, r, r, Z, ldz, Z, ldz, dinv, 1.0, 0.0, M, r, true))) return s2;
         }
@@ -396,11 +403,18 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
       bool conv = true;
       v_current = false;
       if ((st = newton_dir(mixed && tc_ok, &conv))) return st;
+      if (mixed && tc_ok && !conv && tc_level == 0) {
+        // the barrier's D only grows more ill-conditioned with t: once the 6-digit capacity matrix no longer
+        // preconditions well enough, this and the remaining Newton steps take the 8-digit one
+        tc_level = 1;
+        v_current = false;
+        if ((st = newton_dir(true, &conv))) return st;
+      }
       if (mixed && tc_ok && !conv) {
-        // the barrier's D only grows more ill-conditioned with t: once the tensor-core preconditioner misses the
-        // tolerance, the remaining Newton steps use the FP64 capacity matrix directly
+        // ... and once that misses the tolerance too, the FP64 capacity matrix
         ++fallbacks_total;
         tc_ok = false;
+        tc_level = 2;
         v_current = false;
         if ((st = newton_dir(false, &conv))) return st;
       }

@@ -253,8 +253,9 @@ DB200_API int db200_woodbury_solve(db200_context* ctx, int n, int r, const doubl
 
 /* Upper triangle of M(r x r) = Z^T diag(w) Z for Z n x r FP64 (w may be NULL = ones): the capacity-matrix
  * SYRK of the Woodbury Newton step (symmetric_update, include/cblas_like.h:62-69, with a row weight).
- * use_tensor_cores = 0: FP64 pipes (mma.sync f64); 1: tcgen05 kind::i8 on 7 signed 7-bit slices per value with
- * exact s32 sums (Ozaki scheme; error ~1e-12 ||z_p|| ||z_q||, z_p = column p of diag(sqrt(w)) Z).
+ * use_tensor_cores = 0: FP64 pipes (mma.sync f64); 1: tcgen05 kind::i8 on 8 signed 7-bit slices per value with
+ * exact s32 sums (Ozaki scheme; error ~3e-14 ||z_p|| ||z_q||, z_p = column p of diag(sqrt(w)) Z); 5..8: that many
+ * slices (error ~2e-8, 3e-10, 3e-12, 3e-14), products KS(KS + 1)/2 per 64-row chunk.
  * Stream-ordered. */
 DB200_API int db200_gram_weighted(db200_context* ctx, int n, int r, const double* Z, int ldz, const double* w,
                                   double* M, int ldm, int use_tensor_cores);

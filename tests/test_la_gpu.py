@@ -240,3 +240,28 @@ def test_gram_int8_matches_sliced_oracle(gpu_ctx, n, r, spread):
     assert np.max(np.abs(M - S)[iu] / scale[iu]) < 1e-14
     assert np.max(np.abs(M - exact)[iu] / scale[iu]) < 1e-11
     assert np.all(np.tril(M, -1) == 0)
+
+
+@pytest.mark.parametrize("slices,bound", [(5, 1e-7), (6, 2e-9), (7, 2e-11)])
+def test_gram_int8_fewer_slices_match_sliced_oracle(gpu_ctx, slices, bound):
+    """The int8 Gram with 5..7 digits per value (fewer tensor-core products, the barrier's first capacity
+    matrices) equals the exact-integer restatement of the same slicing, and stays within the slicing's error of the
+    exact Gram."""
+    import torch
+    from oracle import ozaki
+    n, r = 20000, 96
+    g = np.random.default_rng(slices)
+    Z = g.standard_normal((n, r)) * np.exp(g.uniform(-3, 3, r))[None, :]
+    w = np.exp(g.uniform(-8, 8, n))
+    dZ, dw = d64(Z), torch.from_numpy(w).cuda()
+    dM = d64(np.zeros((r, r)))
+    gpu_ctx.gram_weighted(n, r, dZ.data_ptr(), n, dw.data_ptr(), dM.data_ptr(), r, slices)
+    gpu_ctx.sync()
+    M = h64(dM, r)
+    S = ozaki.sliced_gram(Z, w, slices)
+    exact = Z.T @ (w[:, None] * Z)
+    d = np.sqrt(np.diag(exact))
+    scale = np.outer(d, d) + 1e-300
+    iu = np.triu_indices(r)
+    assert np.max(np.abs(M - S)[iu] / scale[iu]) < 1e-14
+    assert np.max(np.abs(M - exact)[iu] / scale[iu]) < bound
