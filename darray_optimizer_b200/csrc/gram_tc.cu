@@ -18,8 +18,9 @@
 //  4. The epilogue folds the groups in FP64 (Horner in 2^-7), scales by 2^(e_cp + e_cq) and adds the 128 x 64 tile
 //     into M with FP64 atomics (the n dimension is split across CTAs).
 //
-// The result differs from the exact Z~^T Z~ by the dropped groups and the truncation only, about
-// 1e-12 ||Z~_p|| ||Z~_q|| for KS = 7 (measured), next to FP64 accumulation's ~1e-16 sqrt(n).  The barrier solver
+// The result differs from the exact Z~^T Z~ by the dropped groups and the truncation only, about 2e-8, 3e-10,
+// 3e-12, 3e-14 of ||Z~_p|| ||Z~_q|| for KS = 5, 6, 7, 8 (measured), next to FP64 accumulation's ~1e-16 sqrt(n).  The
+// kernels are instantiated for each KS; the barrier solver
 // still refines each Newton step against the exact FP64 operator and falls back to the FP64 Gram if refinement
 // stalls.
 #include <cuda.h>

@@ -160,7 +160,8 @@ typedef struct db200_barrier_params {
 
 /* Precision of the path.
  * DB200_MIXED: kernel passes on the tensor cores in split bf16 (fp32 accumulation); the Woodbury capacity matrix
- *   I + Z^T D^-1 Z formed exactly in integers on the int8 tensor cores from 7 signed 7-bit slices of every column
+ *   I + Z^T D^-1 Z formed exactly in integers on the int8 tensor cores from 8 signed 7-bit slices of every column
+ *   (6 from r = 2048 while refinement converges with them)
  *   (Ozaki scheme, error ~1e-12 of the column norms) and factored in FP64 while each Newton step refined
  *   against the exact FP64 operator (Z Z^T + D) reaches relative residual 1e-10, the FP64 capacity matrix after;
  *   objective, gradients, gap and line search in FP64.
