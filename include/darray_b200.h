@@ -160,9 +160,9 @@ typedef struct db200_barrier_params {
 
 /* Precision of the path.
  * DB200_MIXED: kernel passes on the tensor cores in split bf16 (fp32 accumulation); the Woodbury capacity matrix
- *   I + Z^T D^-1 Z formed exactly in integers on the int8 tensor cores from 8 signed 7-bit slices of every column
- *   (6 from r = 2048 while refinement converges with them)
- *   (Ozaki scheme, error ~1e-12 of the column norms) and factored in FP64 while each Newton step refined
+ *   I + Z^T D^-1 Z formed in integers on the int8 tensor cores from 8 signed 7-bit slices of every column (Ozaki
+ *   scheme, error ~3e-14 of the column norms; from r = 2048 first 6 slices, ~3e-10, while refinement converges
+ *   with them) and factored in FP64 while each Newton step refined
  *   against the exact FP64 operator (Z Z^T + D) reaches relative residual 1e-10, the FP64 capacity matrix after;
  *   objective, gradients, gap and line search in FP64.
  * DB200_FP64: plain FP64 everywhere (FP64 kernel blocks and products, FP64 capacity matrix): the comparator. */
