@@ -350,7 +350,7 @@ int db200_svm_solve_batched(db200_context* ctx, int count, const db200_svm_insta
     const int s2 = parallel([&](db200_context* w, int, int b) -> int {
       const db200_svm_instance& I = inst[b];
       int s3 = convert<float, double>(w, Y32[(size_t)b], I.n, Q[(size_t)b], I.n, I.n, I.l);
-      if (!s3) s3 = cholqr2_impl(w, I.n, I.l, Q[(size_t)b], I.n, nullptr, 0);
+      if (!s3) s3 = cholqr2_impl(w, I.n, I.l, Q[(size_t)b], I.n, nullptr, 0, false);  // small n: FP64 Grams
       if (!s3) s3 = convert<double, float>(w, Q[(size_t)b], I.n, Qf[(size_t)b], I.n, I.n, I.l);
       return s3;
     });

@@ -140,8 +140,8 @@ int launch_rbf_plan(db200_context* ctx, const TilePlan& plan);
 
 // ------------------------------------------------------------------ SVM pipeline pieces (svm.cpp)
 // Orthonormalise Y (n x l, FP64) in place by CholeskyQR2 (shifted CholeskyQR3 when the Gram is not positive
-// definite); R (l x l) optional.
-int cholqr2_impl(db200_context* ctx, int n, int l, double* Y, int ldy, double* Rout, int ldr);
+// definite); R (l x l) optional.  tc_gram: Grams on the int8 tensor cores (Ozaki, 8 digits), else FP64 pipes.
+int cholqr2_impl(db200_context* ctx, int n, int l, double* Y, int ldy, double* Rout, int ldr, bool tc_gram);
 // Nystrom core: C = Q^T Yk (Yk = K Q), symmetrised; R^T R = C + nu I (shifted Cholesky); Z = Q R^T.
 template <typename TY>
 int nystrom_core(db200_context* ctx, int n, int l, const double* Q, const TY* Yk, double* Cm, double* R, int* d_pair,

@@ -65,9 +65,18 @@ int read_status(db200_context* ctx, int* d_pair, int* st, int* bad) {
 // One CholeskyQR pass Yout = Yin R^-1 with R = chol(Yin^T Yin + shift I); returns NOT_SPD without touching Yout
 // when the Gram is not positive definite.  W, Rinv: l x l scratch; R (l x l) receives the factor.
 int cholqr_pass(db200_context* ctx, int n, int l, const double* Yin, int ldin, double* Yout, int ldout, double* R,
-                double* Rinv, double shift_rel, int* d_pair, double* d_scalar) {
-  int st = gram<double, double>(ctx, n, l, l, Yin, ldin, Yin, ldin, nullptr, 1.0, 0.0, R, l, true);
-  if (st) return st;
+                double* Rinv, double shift_rel, int* d_pair, double* d_scalar, bool tc_gram) {
+  // Gram W = Y^T Y (upper triangle).  tc_gram: on the int8 tensor cores, 8 signed 7-bit digits per value, exact
+  // integer products, error ~3e-14 of ||y_p|| ||y_q||; otherwise on the FP64 pipes.  The Cholesky stays FP64.
+  int st = DB200_OK;
+  if (tc_gram) {
+    void* scratch = slot_buffer(ctx, SLOT_SPARE, gram_tc_scratch_bytes(n, l));
+    if (!scratch) return DB200_ERR_NOMEM;
+    DB200_CUDA(ctx, cudaMemsetAsync(R, 0, sizeof(double) * (size_t)l * l, ctx->stream));
+    if ((st = gram_tc_weighted(ctx, n, l, Yin, ldin, nullptr, R, l, scratch, 8))) return st;
+  } else if ((st = gram<double, double>(ctx, n, l, l, Yin, ldin, Yin, ldin, nullptr, 1.0, 0.0, R, l, true))) {
+    return st;
+  }
   if (shift_rel > 0.0) {
     // shift = shift_rel * trace(W)
     if ((st = trace(ctx, R, l, l, d_scalar))) return st;
@@ -88,7 +97,7 @@ int cholqr_pass(db200_context* ctx, int n, int l, const double* Yin, int ldin, d
 
 }  // namespace
 
-int cholqr2_impl(db200_context* ctx, int n, int l, double* Y, int ldy, double* Rout, int ldr) {
+int cholqr2_impl(db200_context* ctx, int n, int l, double* Y, int ldy, double* Rout, int ldr, bool tc_gram) {
   // slot layout: [pair | scalar | T (n x l) | R1 | R2 | R3 | Rinv | Racc]
   const size_t ll = (size_t)l * l;
   const size_t bytes = 1024 + align_up((size_t)n * l * 8, 256) + 5 * align_up(ll * 8, 256) + 1024;
@@ -103,24 +112,24 @@ int cholqr2_impl(db200_context* ctx, int n, int l, double* Y, int ldy, double* R
   double* R3 = cv.take<double>(ll);
   double* Rinv = cv.take<double>(ll);
   double* Racc = cv.take<double>(ll);
-  int st = cholqr_pass(ctx, n, l, Y, ldy, T, n, R1, Rinv, 0.0, d_pair, d_scalar);
+  int st = cholqr_pass(ctx, n, l, Y, ldy, T, n, R1, Rinv, 0.0, d_pair, d_scalar, tc_gram);
   bool shifted = false;
   if (st == DB200_ERR_NOT_SPD) {
     // shifted CholeskyQR3 (Fukaya, Kannan, Nakatsukasa, Yamamoto, Yanagisawa 2020): first pass with
     // shift 11 (n l + l (l + 1)) u ||Y||^2, ||Y||_2^2 <= trace(Y^T Y)
     const double u = 1.1102230246251565e-16;
     const double rel = 11.0 * ((double)n * l + (double)l * (l + 1)) * u;
-    st = cholqr_pass(ctx, n, l, Y, ldy, T, n, R1, Rinv, rel, d_pair, d_scalar);
+    st = cholqr_pass(ctx, n, l, Y, ldy, T, n, R1, Rinv, rel, d_pair, d_scalar, tc_gram);
     shifted = true;
   }
   if (st) return st;
   // second pass T -> Y
-  if ((st = cholqr_pass(ctx, n, l, T, n, Y, ldy, R2, Rinv, 0.0, d_pair, d_scalar))) return st;
+  if ((st = cholqr_pass(ctx, n, l, T, n, Y, ldy, R2, Rinv, 0.0, d_pair, d_scalar, tc_gram))) return st;
   // R = R2 R1 (upper * upper)
   if ((st = gemm_tall<double, double>(ctx, l, l, l, R2, l, R1, l, false, 0.0, Racc, l))) return st;
   if (shifted) {
     // third pass Y -> T, then copy back; R = R3 (R2 R1)
-    if ((st = cholqr_pass(ctx, n, l, Y, ldy, T, n, R3, Rinv, 0.0, d_pair, d_scalar))) return st;
+    if ((st = cholqr_pass(ctx, n, l, Y, ldy, T, n, R3, Rinv, 0.0, d_pair, d_scalar, tc_gram))) return st;
     DB200_CUDA(ctx, cudaMemcpy2DAsync(Y, sizeof(double) * ldy, T, sizeof(double) * n, sizeof(double) * n, l,
                                       cudaMemcpyDeviceToDevice, ctx->stream));
     if ((st = gemm_tall<double, double>(ctx, l, l, l, R3, l, Racc, l, false, 0.0, R1, l))) return st;
@@ -589,7 +598,9 @@ int lowrank_impl(db200_context* ctx, int n, int d, int l, int q, const float* X,
       s2 = (cudaMemcpyAsync(Q, Y64, sizeof(double) * nl, cudaMemcpyDeviceToDevice, ctx->stream) == cudaSuccess)
                ? DB200_OK
                : DB200_ERR_CUDA;
-    if (!s2) s2 = cholqr2_impl(ctx, n, l, Q, n, nullptr, 0);
+    // int8 Grams from n = 65536 (C2: CholeskyQR2 35 -> 28 ms, C3 207 -> 160 ms); below, the slicing's fixed
+    // cost outweighs the FP64 Gram
+    if (!s2) s2 = cholqr2_impl(ctx, n, l, Q, n, nullptr, 0, !fp64 && n >= 65536);
     if (!s2 && !fp64) s2 = convert<double, float>(ctx, Q, n, Qf, n, n, l);
     ms_orth += tm.stop_ms();
     return s2;
@@ -662,7 +673,7 @@ int db200_potrf(db200_context* ctx, int n, double* A, int lda, int nb) {
 int db200_cholqr2(db200_context* ctx, int n, int l, double* Y, int ldy, double* R, int ldr) {
   if (!ctx) return DB200_ERR_INVALID;
   if (n < l || l < 1 || !Y || ldy < n || (R && ldr < l)) return fail(ctx, DB200_ERR_INVALID, "cholqr2: bad arguments");
-  int st = cholqr2_impl(ctx, n, l, Y, ldy, R, ldr);
+  int st = cholqr2_impl(ctx, n, l, Y, ldy, R, ldr, false);
   if (st) return st;
   return db200_synchronize(ctx);
 }
