@@ -91,6 +91,7 @@ SIGNATURES = {
                                  _c_int, _c_float]),
     "db200_profile": (_c_int, [_vp, _c_int]),
     "db200_selftest_wait_timeout": (_c_int, [_vp, _c_int]),
+    "db200_selftest_grid_barrier_timeout": (_c_int, [_vp, _c_int]),
     "db200_profile_read": (_c_int, [_vp, ctypes.POINTER(_c_double), ctypes.POINTER(_i64)]),
     "db200_lra_host": (_c_int, [_vp, _c_int, _c_int, _c_int, _vp, _c_int, _vp, _vp, _c_int, _vp, _c_int, _c_float]),
     "db200_potrf": (_c_int, [_vp, _c_int, _vp, _c_int, _c_int]),

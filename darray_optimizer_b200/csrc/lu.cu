@@ -17,8 +17,8 @@
 #include <cstring>
 #include <string>
 
+#include "gridsync.cuh"
 #include "internal.h"
-#include "ptx.cuh"
 
 namespace db200 {
 
@@ -145,37 +145,6 @@ constexpr int CP_THREADS = 256;
 constexpr int CP_MAX_ROWS = 1536;   // rows per CTA held in shared memory (1536 x 32 x 4 B = 192 KB)
 constexpr int CAND = W + 2;         // candidate record: |value|, row, the row's W values
 
-__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
-  unsigned v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-
-// Grid-wide barrier among the CTAs of a cooperative launch, bounded: a wait that exceeds the limit (or sees
-// another CTA's timeout) sets *status and returns false in every thread of the CTA.
-__device__ bool grid_barrier(unsigned* count, unsigned target, int* status) {
-  __syncthreads();
-  int ok = 1;
-  if (threadIdx.x == 0) {
-    __threadfence();
-    atomicAdd(count, 1u);
-    const uint64_t t0 = global_timer_ns();
-    while (ld_acquire_u32(count) < target) {
-      if (*reinterpret_cast<volatile int*>(status)) {
-        ok = 0;
-        break;
-      }
-      if (global_timer_ns() - t0 > DB200_WAIT_TIMEOUT_NS) {
-        atomicExch(status, 1);
-        ok = 0;
-        break;
-      }
-    }
-    __threadfence();
-  }
-  return __syncthreads_and(ok) != 0;
-}
-
 __global__ void __launch_bounds__(CP_THREADS) lu_panel_coop_kernel(float* A, long long lda, int m, int k, int w,
                                                                    int R, int* ipiv, int pivot, int* singular,
                                                                    unsigned* bar, unsigned bar_base, float* cand,
@@ -236,7 +205,7 @@ __global__ void __launch_bounds__(CP_THREADS) lu_panel_coop_kernel(float* A, lon
     const int lbi = s_win;
     if (tid < w) my_cand[2 + tid] = (lbi < m) ? tile[tid * R + (lbi - r0)] : 0.0f;
     if (j >= r0 && j < r0 + rows && tid < w) rowj[par * W + tid] = tile[tid * R + (j - r0)];
-    if (!grid_barrier(bar, bar_base + (unsigned)(jj + 1) * (unsigned)G, status)) return;
+    if (!grid_barrier(bar, bar_base + (unsigned)(jj + 1) * (unsigned)G, status, 1, DB200_WAIT_TIMEOUT_NS)) return;
     // the same pivot in every CTA: the largest candidate, the smallest row on ties (one warp scans the G records)
     if (wid == 0) {
       float gv = -1.0f;

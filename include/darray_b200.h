@@ -72,6 +72,10 @@ DB200_API int64_t db200_launch_count(const db200_context* ctx);
  * gives up after limit_ms (1..5000).  The next db200_synchronize returns DB200_ERR_TIMEOUT and clears it; the
  * context remains usable.  Stream-ordered. */
 DB200_API int db200_selftest_wait_timeout(db200_context* ctx, int limit_ms);
+/* The same for the grid-wide barrier of the cooperative LU panel (db200_lu_factorize): four co-resident CTAs of
+ * which one never arrives; the other three give up after limit_ms (1..5000) and the next db200_synchronize
+ * returns DB200_ERR_TIMEOUT and clears it. */
+DB200_API int db200_selftest_grid_barrier_timeout(db200_context* ctx, int limit_ms);
 
 /* Enable (1) or disable (0) CUDA-event timing of every tcgen05 tile-kernel launch on the context's stream;
  * db200_profile_read() returns the summed kernel time (ms) and the number of timed launches since the last

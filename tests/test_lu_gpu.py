@@ -113,3 +113,19 @@ def test_lu_zero_pivot_is_reported(gpu_ctx):
     with pytest.raises(DB200Error) as e:
         gpu_lu(gpu_ctx, A)
     assert e.value.status == -10 and "column 6" in str(e.value)
+
+
+def test_grid_barrier_wait_gives_up(gpu_ctx):
+    """The LU panel's grid-wide barrier is bounded: with one CTA that never arrives, the others give up after
+    20 ms, DB200_ERR_TIMEOUT reaches the host at synchronize, and the context then factors a matrix normally."""
+    from darray_optimizer_b200._lib import DB200Error
+    assert gpu_ctx.lib.db200_selftest_grid_barrier_timeout(gpu_ctx.h, 20) == 0
+    with pytest.raises(DB200Error) as ei:
+        gpu_ctx.sync()
+    assert ei.value.status == -6  # DB200_ERR_TIMEOUT
+    gpu_ctx.sync()  # the status word was cleared
+    A = np.random.default_rng(31).uniform(-2, 2, (200, 200)).astype(np.float32)
+    LUo, ipo = O.lu_partial_pivot(A)
+    LUg, ipg = gpu_lu(gpu_ctx, A)
+    assert np.array_equal(ipg, ipo)
+    assert np.abs(LUg - LUo).max() <= 1e-4 * np.abs(LUo).max()
