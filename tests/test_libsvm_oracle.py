@@ -70,3 +70,22 @@ def test_oracle_line_counts_and_untouched_entries():
 def test_oracle_refuses_undefined_or_unsupported_input(name, text, n, d):
     with pytest.raises(LibsvmError):
         oracle_read(text, n, d, np.float32)
+
+
+def test_libsvm_text_writer_round_trips():
+    """datagen.libsvm_text (the bench's C2-as-text writer) against the oracle reader: every value comes back as
+    the float32 of its six-decimal rounding, every label as +-1, one line per point."""
+    from darray_optimizer_b200.datagen import libsvm_text
+    g = np.random.default_rng(5)
+    n, d = 300, 17
+    X = g.random((n, d))
+    X[0, 0], X[1, 1] = 0.0, 9.4999994  # the ends of the writer's [0, 10) range
+    y = np.where(g.random(n) < 0.5, 1.0, -1.0)
+    text = libsvm_text(X, y, 6)
+    assert text.count(b"\n") == n
+    Xo = np.full((n, d), FILL_X, np.float32)
+    Yo = np.full(n, FILL_Y, np.float32)
+    assert read_input_file(text, n, d, Xo, Yo, np.float32) == n
+    expect = np.array([[float(f"{v:.6f}") for v in row] for row in X], dtype=np.float32)
+    assert np.array_equal(Xo, expect)
+    assert np.array_equal(Yo, y.astype(np.float32))
