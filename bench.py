@@ -4,7 +4,10 @@
 (n = 131072 points, d = 128 features, sketch width l = 512 + 16, gamma = 0.5/d).
 
 Metric: K.Omega throughput in TFLOP/s with the algorithmic count F = 2 n^2 (d + l) per pass (distance Gram plus
-sketch product; the split-bf16 extra products are not counted).
+sketch product; the split-fp16 extra products are not counted).  The timed pass is the single fp16 sketch product;
+the line also times the compensated pass with promoted accumulation that the parity-grade mixed solve runs, the
+plain-FP64 fused pass against the measured FP64 tensor-core peak, and the whole solves (the "summary" key at the
+end of the line gathers the headline numbers).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -63,7 +66,7 @@ def executed_flops(n, d, l):
 def config(extra=None):
     c = {"workload": f"C2 fused RBF x sketch pass (uniform [0,1)^{D_FEAT}, hyperplane labels, 5% flipped)",
          "n": N_POINTS, "d": D_FEAT, "l": L_SKETCH, "gamma": 0.5 / D_FEAT,
-         "l2": "inputs larger than L2 (X 67 MB + Omega 277 MB fp32, packed 67 + 138 MB bf16, Y 277 MB)"}
+         "l2": "inputs larger than L2 (X 67 MB + Omega 277 MB fp32, packed 67 + 138 MB fp16, Y 277 MB)"}
     if extra:
         c.update(extra)
     return c
@@ -254,6 +257,10 @@ def run_ours(args):
     F = flops(n, d, l)
     value = world * F * args.steps / (ms_max / 1e3) / 1e12
 
+    # the sketch's error on 64 sampled rows against the FP64 pass, the compensated product the solve uses, and the
+    # plain-FP64 pass against the measured FP64 tensor-core peak (rank 0)
+    precision = precision_legs(ctx, w, X, y, O, Y) if rank == 0 else None
+
     # end to end through the host-pointer LRA entry point (pinned host buffers, copies inside the timed region)
     e2e_val = h2d = d2h = None
     if not args.no_e2e:
@@ -274,15 +281,70 @@ def run_ours(args):
     if args.lu and rank == 0:
         extra["lu"] = lu_run(ctx)
     return finish(args, ctx, w, rep, ms_max, kernel_ms, kernel_count, launches, clocks, e2e_val, h2d, d2h, Om,
-                  solve, batch, extra)
+                  solve, batch, extra, precision)
 
 
-def sampled_sketch_error(w, Yg_rows, rows, Om_rows_fn, block=64):
-    """Relative error of GPU sketch rows against the FP64 oracle on a row sample (size-independent check)."""
-    from oracle import oracle as O
-    Om = Om_rows_fn()
-    ref = O.sketch(w.X[rows], w.X, w.y[rows], w.y, Om, w.gamma, block=block)
-    return float(np.linalg.norm(Yg_rows - ref) / np.linalg.norm(ref))
+def precision_legs(ctx, w, X, y, O, Y, steps=3):
+    """At the C2 workload: (1) the timed single-product pass's error on 64 sampled rows against the FP64 pass;
+    (2) the compensated product with promoted accumulation (the mixed solve's passes): kernel time, TFLOP/s and
+    its sampled error; (3) one plain-FP64 fused pass (the comparator's) against the probed FP64 DMMA peak."""
+    import torch
+    from darray_optimizer_b200 import _lib
+    n, d, l = w.n, w.d, w.l
+    F = flops(n, d, l)
+    rows = np.sort(np.random.default_rng(11).choice(n, 64, replace=False))
+    O64 = O.double()
+    out = {"sampled_rows": 64, "err_single_vs_fp64": sampled_sketch_error(ctx, w, X, y, O64, Y, rows)}
+    Yc = torch.empty_like(Y)
+
+    def comp_step():
+        ctx.rbf_sketch_ex(n, n, d, l, X.data_ptr(), d, X.data_ptr(), d, 0, y.data_ptr(), y.data_ptr(), O.data_ptr(),
+                          n, Yc.data_ptr(), n, w.gamma, _lib.SKETCH_COMPENSATED_PROMOTED)
+    comp_step()
+    ctx.sync()
+    ctx.profile(True)
+    for _ in range(steps):
+        comp_step()
+    ctx.sync()
+    kms, cnt = ctx.profile_read()
+    ctx.profile(False)
+    per = kms / steps  # the pass is one launch (every panel in one work list)
+    out["compensated_promoted"] = {"ms_per_pass": per, "tflops": F / (per / 1e3) / 1e12,
+                                   "err_vs_fp64": sampled_sketch_error(ctx, w, X, y, O64, Yc, rows)}
+    dmma, dfma = ctx.probe_fp64_peak()
+    Y64 = torch.zeros((l, n), dtype=torch.float64, device="cuda")
+    s = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    ctx.rbf_sketch_f64(n, n, d, l, X.data_ptr(), d, X.data_ptr(), d, y.data_ptr(), y.data_ptr(), O64.data_ptr(), n,
+                       Y64.data_ptr(), n, w.gamma)
+    e1.record(s)
+    ctx.sync()
+    torch.cuda.synchronize()
+    ms64 = e0.elapsed_time(e1)
+    tf64 = F / (ms64 / 1e3) / 1e12
+    out["fp64_pass"] = {"ms": ms64, "tflops": tf64, "dmma_peak_tflops": dmma, "dfma_peak_tflops": dfma,
+                        "frac_of_dmma_peak": tf64 / dmma,
+                        "kernel": "rbf_sketch_f64_kernel (fused FP64 DMMA distances + exp + sketch, K never stored)"}
+    del Y64, O64, Yc
+    return out
+
+
+def sampled_sketch_error(ctx, w, X, y, Om64, Yg, rows):
+    """Relative Frobenius error of GPU sketch rows Yg[:, rows] (Yg: l x n storage of the n x l result) against the
+    plain-FP64 GPU pass (db200_rbf_sketch_f64, which the tests pin to the FP64 oracle to 1e-12) on the same rows:
+    a size-independent check of a full-size pass."""
+    import torch
+    n, d, l = w.n, w.d, w.l
+    idx = torch.from_numpy(np.asarray(rows, np.int64)).cuda()
+    Xr = X[idx].contiguous()
+    yr = y[idx].contiguous()
+    ref = torch.zeros((l, len(rows)), dtype=torch.float64, device="cuda")
+    ctx.rbf_sketch_f64(len(rows), n, d, l, Xr.data_ptr(), d, X.data_ptr(), d, yr.data_ptr(), y.data_ptr(),
+                       Om64.data_ptr(), n, ref.data_ptr(), len(rows), w.gamma)
+    ctx.sync()
+    got = Yg[:, idx].double()
+    return float(torch.linalg.norm(got - ref) / torch.linalg.norm(ref))
 
 
 def c3_run(ctx, n=262144, n_test=16384, steps=3):
@@ -314,7 +376,7 @@ def c3_run(ctx, n=262144, n_test=16384, steps=3):
     ctx.sync()
     ms = e0.elapsed_time(e1) / steps
     rows = np.sort(np.random.default_rng(3).choice(n, 64, replace=False))
-    err = sampled_sketch_error(w, Y.cpu().numpy().T[rows], rows, lambda: Om_h)
+    err = sampled_sketch_error(ctx, w, X, y, O.double(), Y, rows)
     Z = torch.zeros((l, n), dtype=torch.float64, device="cuda")
     a = torch.zeros(n, dtype=torch.float64, device="cuda")
     torch.cuda.synchronize()
@@ -428,7 +490,19 @@ def solve_run(ctx, w, X, y, O, n_test, mixed_only=False):
                            dec.data_ptr(), n_test, w.gamma)
         ctx.sync()
         acc = float(np.mean(np.sign(dec.cpu().numpy()) == yt))
-        return {"s": el, "used_fallback": lrep.used_fallback, "rank": lrep.rank,
+        # the plain-FP64 solve on the same landmarks (same seed): FP64 factor, FP64 barrier
+        rel_f = None
+        if not lrep.used_fallback:
+            idx = torch.zeros(r, dtype=torch.int32, device="cuda")
+            ctx.select_landmarks(n, d, r, X.data_ptr(), d, net, 11, 16384, idx.data_ptr())
+            Z64 = torch.zeros((r, n), dtype=torch.float64, device="cuda")
+            ctx.landmark_factor(n, d, X.data_ptr(), d, y.data_ptr(), w.gamma, r, idx.data_ptr(), Z64.data_ptr(), n,
+                                precision=1)
+            a64 = torch.zeros(n, dtype=torch.float64, device="cuda")
+            rep64 = ctx.svm_barrier(n, r, Z64.data_ptr(), n, y.data_ptr(), w.C, a64.data_ptr(),
+                                    params=ctx.barrier_params(precision=1))
+            rel_f = abs(rep.f - rep64.f) / abs(rep64.f)
+        return {"s": el, "used_fallback": lrep.used_fallback, "rank": lrep.rank, "rel_f_diff_vs_fp64_same_landmarks": rel_f,
                 "residual_est": lrep.residual_est, "residual_fallback": lrep.residual_fallback, "tol": tol,
                 "f": rep.f, "gap_pd": rep.gap_primal_dual, "gap_barrier": rep.gap_barrier, "acc": acc,
                 "ms_barrier": rep.ms_barrier,
@@ -451,7 +525,11 @@ def solve_run(ctx, w, X, y, O, n_test, mixed_only=False):
                     "phases_ms_mixed": {k: getattr(rep_m, k) for k in ("ms_sketch", "ms_orth", "ms_core",
                                                                         "ms_barrier")}})
         return out
+    t_fast, rep_q, acc_q = one(2)  # the single fp16 sketch product (DB200_MIXED_FAST)
     t_fp64, rep_f, acc_f = one(1)
+    out["fast_mixed"] = {"s": t_fast, "f": rep_q.f, "rel_f_diff": abs(rep_q.f - rep_f.f) / abs(rep_f.f),
+                         "gap_pd": rep_q.gap_primal_dual, "acc": acc_q,
+                         "phases_ms": {k: getattr(rep_q, k) for k in ("ms_sketch", "ms_orth", "ms_core", "ms_barrier")}}
     out.update({"mixed_s": t_mixed, "fp64_s": t_fp64, "speedup_vs_fp64": t_fp64 / t_mixed,
                 "f_mixed": rep_m.f, "f_fp64": rep_f.f, "rel_f_diff": abs(rep_m.f - rep_f.f) / abs(rep_f.f),
                 "gap_pd_mixed": rep_m.gap_primal_dual, "gap_pd_fp64": rep_f.gap_primal_dual,
@@ -655,8 +733,46 @@ def lu_run(ctx, n=8192, steps=3, cpu_n=4096):
     return out
 
 
+def summarize(line):
+    """The numbers a reader looks for first, gathered at the end of the JSON line (whose tail is what a truncated
+    log keeps): the solve times, speed-ups and parities, the compensated and FP64 passes, the batch."""
+    out = {"kernel_tflops": line["value"], "kernel_frac_of_sustained_bf16": line["roofline"]["frac"],
+           "e2e_tflops": (line.get("e2e") or {}).get("value")}
+    pr = line.get("precision") or {}
+    if pr:
+        out["sketch_err_single_vs_fp64"] = pr.get("err_single_vs_fp64")
+        cp = pr.get("compensated_promoted") or {}
+        out["compensated_pass_ms"] = cp.get("ms_per_pass")
+        out["compensated_tflops"] = cp.get("tflops")
+        out["sketch_err_compensated_vs_fp64"] = cp.get("err_vs_fp64")
+        fp = pr.get("fp64_pass") or {}
+        out["fp64_pass_tflops"] = fp.get("tflops")
+        out["fp64_pass_frac_of_dmma_peak"] = fp.get("frac_of_dmma_peak")
+    sv = line.get("solve") or {}
+    if sv:
+        ln = sv.get("learned_mixed") or {}
+        fa = sv.get("fast_mixed") or {}
+        out.update({"solve_mixed_s": sv.get("mixed_s"), "solve_learned_s": ln.get("s"), "solve_fp64_s": sv.get("fp64_s"),
+                    "speedup_mixed_vs_fp64": sv.get("speedup_vs_fp64"),
+                    "speedup_learned_vs_fp64": (sv["fp64_s"] / ln["s"]) if sv.get("fp64_s") and ln.get("s") else None,
+                    "rel_f_diff_mixed_vs_fp64": sv.get("rel_f_diff"),
+                    "rel_f_diff_learned_vs_fp64_same_landmarks": ln.get("rel_f_diff_vs_fp64_same_landmarks"),
+                    "rel_f_diff_fast_mixed_vs_fp64": fa.get("rel_f_diff"), "solve_fast_mixed_s": fa.get("s"),
+                    "gap_pd_mixed": sv.get("gap_pd_mixed"), "gap_pd_learned": ln.get("gap_pd"),
+                    "gap_pd_fp64": sv.get("gap_pd_fp64"), "acc_mixed": sv.get("acc_mixed"),
+                    "acc_learned": ln.get("acc"), "acc_fp64": sv.get("acc_fp64")})
+    bt = line.get("batch") or {}
+    if bt:
+        out.update({"batch_solves_per_s": bt.get("solves_per_s"), "batch_gap_pd_max": bt.get("gap_primal_dual_max"),
+                    "batch_speedup_vs_sequential": bt.get("speedup_vs_sequential")})
+    return out
+
+
+DETAIL_KEYS = ("gap_primal_dual", "newton", "n", "d", "tile_plans", "gap_pd_per_instance")
+
+
 def finish(args, ctx, w, rep, ms_max, kernel_ms, kernel_count, launches, clocks, e2e_val, h2d, d2h, Om,
-           solve=None, batch=None, extra=None):
+           solve=None, batch=None, extra=None, precision=None):
     world, rank = rep.world, rep.rank
     n, d, l = w.n, w.d, w.l
     F = flops(n, d, l)
@@ -678,7 +794,7 @@ def finish(args, ctx, w, rep, ms_max, kernel_ms, kernel_count, launches, clocks,
             "peak_source": ("MEASURED_PEAKS.json bf16_tflops_sustained (of measured)" if pk.exists()
                             else "fallback 1400 sustained"),
             "tensor_executed_tflops": executed, "tensor_executed_frac": executed / peak,
-            "tensor_executed_note": "split-bf16 distance products (3 per feature) recomputed per sketch panel, "
+            "tensor_executed_note": "split-fp16 distance products (3 per feature) recomputed per sketch panel, "
                                     "sketch product over the width padded to 16"}
     traffic_file = ROOT / "profiles" / "rbf_sketch_traffic.json"
     if traffic_file.exists():
@@ -689,20 +805,28 @@ def finish(args, ctx, w, rep, ms_max, kernel_ms, kernel_count, launches, clocks,
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "bf16", "data": "synthetic (seeded Philox)",
-            "config": config({"parallelism": f"replicas x{world}", "n": n}), "clocks": clocks,
+            "vs_baseline": None, "dtype": "fp16", "data": "synthetic (seeded Philox)",
+            "config": config({"n": n}), "clocks": clocks,
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches, "roofline": roof}
+    if precision is not None:
+        line["precision"] = precision
     if solve is not None:
         line["solve"] = solve
+    detail = {}
     if batch is not None:
-        line["batch"] = batch
+        # per-instance arrays and tile plans go to --detail-out; the line keeps the aggregates
+        detail["batch"] = {k: batch[k] for k in DETAIL_KEYS if k in batch}
+        line["batch"] = {k: v for k, v in batch.items() if k not in DETAIL_KEYS}
     if extra:
         line.update(extra)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, desc, threads = cpu_sample(w, Om, 256, args.cpu_seconds)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc}
     if rank == 0:
+        line["summary"] = summarize(line)
+        if args.detail_out:
+            Path(args.detail_out).write_text(json.dumps(detail, indent=1))
         print(json.dumps(line), flush=True)
     ctx.close()
     from darray_optimizer_b200 import replicas
@@ -731,6 +855,8 @@ def main():
                     help="add the LU leg (n = 8192 FP32, partial pivoting; the reference's LU as CPU baseline)")
     ap.add_argument("--n-test", type=int, default=16384, help="held-out points for the solve leg's accuracy")
     ap.add_argument("--n", type=int, default=N_POINTS, help="points (default: the C2 workload, 131072)")
+    ap.add_argument("--detail-out", default=None,
+                    help="write per-instance batch arrays and tile plans to this JSON file (kept off the line)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

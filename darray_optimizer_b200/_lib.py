@@ -87,9 +87,12 @@ SIGNATURES = {
     "db200_launch_count": (_i64, [_vp]),
     "db200_rbf_sketch": (_c_int, [_vp, _c_int, _c_int, _c_int, _c_int, _vp, _c_int, _vp, _c_int, _c_int, _vp, _vp,
                                   _vp, _c_int, _vp, _c_int, _c_float]),
+    "db200_rbf_sketch_ex": (_c_int, [_vp, _c_int, _c_int, _c_int, _c_int, _vp, _c_int, _vp, _c_int, _c_int, _vp,
+                                     _vp, _vp, _c_int, _vp, _c_int, _c_float, _c_int]),
     "db200_rbf_block": (_c_int, [_vp, _c_int, _c_int, _c_int, _vp, _c_int, _vp, _c_int, _c_int, _vp, _vp, _vp,
                                  _c_int, _c_float]),
     "db200_profile": (_c_int, [_vp, _c_int]),
+    "db200_probe_fp64_peak": (_c_int, [_vp, ctypes.POINTER(_c_double), ctypes.POINTER(_c_double)]),
     "db200_selftest_wait_timeout": (_c_int, [_vp, _c_int]),
     "db200_selftest_grid_barrier_timeout": (_c_int, [_vp, _c_int]),
     "db200_profile_read": (_c_int, [_vp, ctypes.POINTER(_c_double), ctypes.POINTER(_i64)]),
@@ -107,6 +110,8 @@ SIGNATURES = {
     "db200_gram_weighted": (_c_int, [_vp, _c_int, _c_int, _vp, _c_int, _vp, _vp, _c_int, _c_int]),
     "db200_rbf_sketch_f64": (_c_int, [_vp, _c_int, _c_int, _c_int, _c_int, _vp, _c_int, _vp, _c_int, _vp, _vp, _vp,
                                       _c_int, _vp, _c_int, _c_double]),
+    "db200_rbf_block_f64": (_c_int, [_vp, _c_int, _c_int, _c_int, _vp, _c_int, _vp, _c_int, _vp, _vp, _vp, _c_int,
+                                     _c_double]),
     "db200_svm_solve": (_c_int, [_vp, _c_int, _c_int, _c_int, _c_int, _vp, _c_int, _vp, _vp, _c_int, _c_float,
                                  _c_double, ctypes.POINTER(BarrierParams), _vp, _vp, _c_int,
                                  ctypes.POINTER(SvmReport)]),
@@ -151,8 +156,12 @@ SIGNATURES = {
     "db200_select_topk": (_c_int, [_vp, _c_int, _vp, _c_int, _vp]),
     "db200_landmark_factor": (_c_int, [_vp, _c_int, _c_int, _vp, _c_int, _vp, _c_float, _c_int, _vp, _vp, _c_int,
                                        _dp]),
+    "db200_landmark_factor_ex": (_c_int, [_vp, _c_int, _c_int, _vp, _c_int, _vp, _c_float, _c_int, _vp, _vp, _c_int,
+                                          _dp, _c_int]),
     "db200_residual_estimate": (_c_int, [_vp, _c_int, _c_int, _vp, _c_int, _vp, _c_float, _c_int, _vp, _c_int,
                                          _c_int, _vp, _dp]),
+    "db200_select_landmarks": (_c_int, [_vp, _c_int, _c_int, _c_int, _vp, _c_int, _vp, ctypes.c_ulonglong, _c_int,
+                                        _vp]),
     "db200_svm_solve_landmarks": (_c_int, [_vp, _c_int, _c_int, _c_int, _vp, _c_int, _vp, _c_float, _c_double, _vp,
                                            _u64, _c_int, _c_int, _c_double, _vp, _c_int, _c_int, _c_int,
                                            ctypes.POINTER(BarrierParams), _vp, _vp, _c_int, ctypes.POINTER(SvmReport),
@@ -170,6 +179,9 @@ STATUS = {
     -8: "DB200_ERR_UNSUPPORTED", -9: "DB200_ERR_TOO_LARGE", -10: "DB200_ERR_SINGULAR",
 }
 NOALLOC_SCRATCH_BYTES = 32 << 20
+# precisions of the SVM path and sketch products (include/darray_b200.h)
+MIXED, FP64, MIXED_FAST = 0, 1, 2
+SKETCH_SINGLE, SKETCH_P_SPLIT, SKETCH_COMPENSATED, SKETCH_COMPENSATED_PROMOTED = 0, 1, 2, 3
 POINT_MAJOR, FEATURE_MAJOR = 0, 1
 F32, F64 = 0, 1
 
@@ -253,6 +265,16 @@ class Context:
         return self.check(self.lib.db200_rbf_sketch(self.h, m, n, d, l, Xi, ldxi, Xj, ldxj, layout, yi, yj, Om,
                                                     ldo, Y, ldy, gamma))
 
+    def rbf_sketch_ex(self, m, n, d, l, Xi, ldxi, Xj, ldxj, layout, yi, yj, Om, ldo, Y, ldy, gamma, product):
+        return self.check(self.lib.db200_rbf_sketch_ex(self.h, m, n, d, l, Xi, ldxi, Xj, ldxj, layout, yi, yj, Om,
+                                                       ldo, Y, ldy, gamma, product))
+
+    def probe_fp64_peak(self):
+        """(DMMA, DFMA) TFLOP/s measured on this GPU."""
+        a, b = _c_double(), _c_double()
+        self.check(self.lib.db200_probe_fp64_peak(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
     def profile(self, enable: bool):
         return self.check(self.lib.db200_profile(self.h, 1 if enable else 0))
 
@@ -304,6 +326,9 @@ class Context:
     def rbf_sketch_f64(self, m, n, d, l, Xi, ldxi, Xj, ldxj, yi, yj, Om, ldo, Y, ldy, gamma):
         return self.check(self.lib.db200_rbf_sketch_f64(self.h, m, n, d, l, Xi, ldxi, Xj, ldxj, yi, yj, Om, ldo, Y,
                                                         ldy, gamma))
+
+    def rbf_block_f64(self, m, n, d, Xi, ldxi, Xj, ldxj, yi, yj, K, ldk, gamma):
+        return self.check(self.lib.db200_rbf_block_f64(self.h, m, n, d, Xi, ldxi, Xj, ldxj, yi, yj, K, ldk, gamma))
 
     def svm_solve(self, n, d, l, q, X, ldx, y, Om, ldo, gamma, C, a, Z, ldz, params=None):
         rep = SvmReport()
@@ -372,9 +397,14 @@ class Context:
     def select_topk(self, n, keys, k, idx):
         return self.check(self.lib.db200_select_topk(self.h, n, keys, k, idx))
 
-    def landmark_factor(self, n, d, X, ldx, y, gamma, r, idx, Z, ldz):
+    def landmark_factor(self, n, d, X, ldx, y, gamma, r, idx, Z, ldz, precision=None):
         nu = _c_double()
-        self.check(self.lib.db200_landmark_factor(self.h, n, d, X, ldx, y, gamma, r, idx, Z, ldz, ctypes.byref(nu)))
+        if precision is None:
+            self.check(self.lib.db200_landmark_factor(self.h, n, d, X, ldx, y, gamma, r, idx, Z, ldz,
+                                                      ctypes.byref(nu)))
+        else:
+            self.check(self.lib.db200_landmark_factor_ex(self.h, n, d, X, ldx, y, gamma, r, idx, Z, ldz,
+                                                         ctypes.byref(nu), precision))
         return nu.value
 
     def residual_estimate(self, n, d, X, ldx, y, gamma, r, Z, ldz, s, sample_idx):
@@ -382,6 +412,9 @@ class Context:
         self.check(self.lib.db200_residual_estimate(self.h, n, d, X, ldx, y, gamma, r, Z, ldz, s, sample_idx,
                                                     ctypes.byref(est)))
         return est.value
+
+    def select_landmarks(self, n, d, r, X, ldx, net, seed, s_knn, idx):
+        return self.check(self.lib.db200_select_landmarks(self.h, n, d, r, X, ldx, net.h, seed, s_knn, idx))
 
     def svm_solve_landmarks(self, n, d, r, X, ldx, y, gamma, C, net, seed, s_knn, s_res, tol, Omega, ldo, l_fb, q,
                             a, Z, ldz, params=None):

@@ -56,10 +56,20 @@ struct Packed {
 
 size_t packed_bytes(int m, int n, int d, bool same, const SketchPlan& plan) {
   const int dp = feature_pad(d), mpad = point_pad(m), npad = point_pad(n);
-  size_t b = align_up((size_t)mpad * 2 * dp * 2, 256) + align_up((size_t)mpad * 4, 256);
-  if (!same) b += align_up((size_t)npad * 2 * dp * 2, 256) + align_up((size_t)npad * 4, 256);
-  b += align_up((size_t)plan.lrows * npad * 2, 256);
+  size_t b = align_up((size_t)mpad * 2 * dp * 2, 256) + align_up(packed_norm_floats(mpad) * 4, 256);
+  if (!same) b += align_up((size_t)npad * 2 * dp * 2, 256) + align_up(packed_norm_floats(npad) * 4, 256);
+  b += align_up(packed_sketch_halves(plan, npad) * 2, 256);
   return b;
+}
+
+// The plan of a compensated sketch (comp = 2) with promoted accumulation: the explicit plan when it leaves tensor
+// memory for P_lo and takes one instruction per panel, else the default compensated plan.
+SketchPlan comp_plan(const SketchPlan& p, int l) {
+  SketchPlan c = p;
+  c.comp = 2;
+  if (!(c.panel <= 256 && c.panel + 128 + 128 * c.g_bufs <= 512)) c = plan_sketch(l, 2);
+  c.promote = 2;  // accumulation promoted every two j tiles, as in db200_lowrank's mixed passes
+  return c;
 }
 
 int pack_problem(db200_context* ctx, int m, int n, int d, const float* Xi, int ldxi, const float* Xj, int ldxj,
@@ -67,7 +77,7 @@ int pack_problem(db200_context* ctx, int m, int n, int d, const float* Xi, int l
   const int dp = feature_pad(d), mpad = point_pad(m), npad = point_pad(n);
   const bool same = (Xi == Xj && ldxi == ldxj && m == n);
   void* xpi = cv.take<uint16_t>((size_t)mpad * 2 * dp);
-  float* ni = cv.take<float>(mpad);
+  float* ni = cv.take<float>(packed_norm_floats(mpad));
   int st = pack_points(ctx, Xi, ldxi, DB200_POINT_MAJOR, m, d, dp, mpad, xpi, ni);
   if (st) return st;
   P->pi.xp = xpi;
@@ -79,7 +89,7 @@ int pack_problem(db200_context* ctx, int m, int n, int d, const float* Xi, int l
     P->pj = P->pi;
   } else {
     void* xpj = cv.take<uint16_t>((size_t)npad * 2 * dp);
-    float* nj = cv.take<float>(npad);
+    float* nj = cv.take<float>(packed_norm_floats(npad));
     if ((st = pack_points(ctx, Xj, ldxj, DB200_POINT_MAJOR, n, d, dp, npad, xpj, nj))) return st;
     P->pj.xp = xpj;
     P->pj.norms = nj;
@@ -87,7 +97,7 @@ int pack_problem(db200_context* ctx, int m, int n, int d, const float* Xi, int l
     P->pj.npad = npad;
     P->pj.dp = dp;
   }
-  P->op = cv.take<uint16_t>((size_t)plan.lrows * npad);
+  P->op = cv.take<uint16_t>(packed_sketch_halves(plan, npad));
   P->plan = plan;
   P->npad_i = mpad;
   P->npad_j = npad;
@@ -171,10 +181,14 @@ int db200_svm_solve_batched(db200_context* ctx, int count, const db200_svm_insta
   // ---- device buffers: packed points and test matrices (workspace), per-instance pass outputs (pipeline slot)
   std::vector<SketchPlan> plans((size_t)count);
   size_t wbytes = 4096, pbytes = 4096 + (size_t)workers * 256;
+  int njobs = 0;  // tile-engine instances: default multi-panel plans split into exact-width panels
   for (int b = 0; b < count; ++b) {
     const db200_svm_instance& I = inst[b];
     plans[(size_t)b] = job_plan(I.l, I.n_panels, I.panel, I.g_bufs);
+    // kernel passes with the compensated sketch product unless the fast mixed form is asked for
+    if (P.precision != DB200_MIXED_FAST) plans[(size_t)b] = comp_plan(plans[(size_t)b], I.l);
     wbytes += packed_bytes(I.n, I.n, I.d, true, plans[(size_t)b]);
+    njobs += (I.n_panels <= 0) ? plans[(size_t)b].n_panels : 1;
     const size_t nl = (size_t)I.n * I.l, ll = (size_t)I.l * I.l;
     pbytes += 2 * align_up(nl * 4, 256) + align_up(nl * 8, 256) + 2 * align_up(ll * 8, 256);
   }
@@ -209,34 +223,42 @@ int db200_svm_solve_batched(db200_context* ctx, int count, const db200_svm_insta
     if (st) return st;
     R.ms_pack = t.stop();
   }
-  std::vector<TileJob> tj((size_t)count);
+  // Tile-engine instances.  A default plan of several panels is split into exact-width panels, as the
+  // single-problem path splits it, so each instance's passes are the single solve's to the bit; an explicit
+  // (autotuned) plan is kept as one instance of equal panels.
+  std::vector<TileJob> tj;
+  tj.reserve((size_t)njobs);
   for (int b = 0; b < count; ++b) {
-    TileJob& T = tj[(size_t)b];
+    TileJob T;
     T.pi = pk[(size_t)b].pi;
     T.pj = pk[(size_t)b].pj;
     T.yi = inst[b].y;
     T.op = pk[(size_t)b].op;
     T.plan = pk[(size_t)b].plan;
+    T.om_lo = T.plan.lrows;
     T.l = inst[b].l;
     T.gamma = inst[b].gamma;
     T.out = Y32[(size_t)b];
     T.ldo = inst[b].n;
+    if (inst[b].n_panels <= 0) exact_panel_jobs(T, tj);
+    else tj.push_back(T);
   }
+  const int nj = (int)tj.size();
   TilePlan tplan;
-  if ((st = prepare_rbf_tiles(ctx, RBF_MODE_SKETCH, tj.data(), count, nullptr, 0, &tplan))) return st;
+  if ((st = prepare_rbf_tiles(ctx, RBF_MODE_SKETCH, tj.data(), nj, nullptr, 0, &tplan))) return st;
 
   // ---- one kernel pass over every instance: pack each test matrix (Omega, or Q from the previous pass), then one
   // persistent launch.  After the first Q pass the sequence is captured once and replayed.
-  auto enqueue_pass = [&](bool from_omega) -> int {
+  auto enqueue_pass = [&](bool from_omega, const TilePlan& tp) -> int {
     for (int b = 0; b < count; ++b) {
       const db200_svm_instance& I = inst[b];
       const float* src = from_omega ? I.Omega : Qf[(size_t)b];
       const int lds = from_omega ? I.ldo : I.n;
       int s2 = pack_sketch(ctx, src, lds, I.y, I.n, I.l, pk[(size_t)b].npad_j, pk[(size_t)b].plan.lrows,
-                           pk[(size_t)b].op);
+                           pk[(size_t)b].op, pk[(size_t)b].plan.comp);
       if (s2) return s2;
     }
-    return launch_rbf_plan(ctx, tplan);
+    return launch_rbf_plan(ctx, tp);
   };
   cudaStream_t cs = nullptr;
   cudaGraphExec_t qpass = nullptr;
@@ -247,7 +269,7 @@ int db200_svm_solve_batched(db200_context* ctx, int count, const db200_svm_insta
     if (ev) cudaEventDestroy(ev);
   };
   auto q_pass = [&]() -> int {
-    if (!use_graph) return enqueue_pass(false);
+    if (!use_graph) return enqueue_pass(false, tplan);
     if (!qpass) {
       // capture on a private stream (the context's stream may be the legacy default stream)
       if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess ||
@@ -263,7 +285,7 @@ int db200_svm_solve_batched(db200_context* ctx, int count, const db200_svm_insta
       if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
         s2 = fail(ctx, DB200_ERR_CUDA, "svm_solve_batched: begin capture");
       } else {
-        s2 = enqueue_pass(false);
+        s2 = enqueue_pass(false, tplan);
         const cudaError_t e = cudaStreamEndCapture(cs, &g);
         if (!s2 && e != cudaSuccess) s2 = cuda_fail(ctx, e, "cudaStreamEndCapture");
       }
@@ -360,7 +382,7 @@ int db200_svm_solve_batched(db200_context* ctx, int count, const db200_svm_insta
   };
   {
     Timer t(ctx->stream);
-    st = enqueue_pass(true);
+    st = enqueue_pass(true, tplan);
     R.kernel_passes += 1;
     if (!st) R.ms_sketch += t.stop();
   }

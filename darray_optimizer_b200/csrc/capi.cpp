@@ -219,13 +219,13 @@ static int pack_pair(db200_context* ctx, int m, int n, int d, const float* Xi, i
   const int dp = feature_pad(d);
   const int mpad = point_pad(m), npad = point_pad(n);
   const bool same = (Xi == Xj && ldxi == ldxj && m == n);
-  size_t bytes = 4096 + (size_t)mpad * (2 * dp * 2 + 4) + extra_bytes + 4 * 256;
-  if (!same) bytes += (size_t)npad * (2 * dp * 2 + 4);
+  size_t bytes = 4096 + (size_t)mpad * (2 * dp * 2 + 8) + extra_bytes + 4 * 256;
+  if (!same) bytes += (size_t)npad * (2 * dp * 2 + 8);
   void* ws = workspace(ctx, bytes);
   if (!ws) return DB200_ERR_NOMEM;
   carve = Carve{static_cast<char*>(ws)};
   void* xpi = carve.take<uint16_t>((size_t)mpad * 2 * dp);
-  float* ni = carve.take<float>(mpad);
+  float* ni = carve.take<float>(packed_norm_floats(mpad));
   int st = pack_points(ctx, Xi, ldxi, layout, m, d, dp, mpad, xpi, ni);
   if (st) return st;
   pi.xp = xpi;
@@ -237,7 +237,7 @@ static int pack_pair(db200_context* ctx, int m, int n, int d, const float* Xi, i
     pj = pi;
   } else {
     void* xpj = carve.take<uint16_t>((size_t)npad * 2 * dp);
-    float* nj = carve.take<float>(npad);
+    float* nj = carve.take<float>(packed_norm_floats(npad));
     st = pack_points(ctx, Xj, ldxj, layout, n, d, dp, npad, xpj, nj);
     if (st) return st;
     pj.xp = xpj;
@@ -249,11 +249,14 @@ static int pack_pair(db200_context* ctx, int m, int n, int d, const float* Xi, i
   return DB200_OK;
 }
 
-int db200_rbf_sketch(db200_context* ctx, int m, int n, int d, int l, const float* Xi, int ldxi, const float* Xj,
-                     int ldxj, int x_layout, const float* yi, const float* yj, const float* Omega, int ldo, float* Y,
-                     int ldy, float gamma) {
+int db200_rbf_sketch_ex(db200_context* ctx, int m, int n, int d, int l, const float* Xi, int ldxi, const float* Xj,
+                        int ldxj, int x_layout, const float* yi, const float* yj, const float* Omega, int ldo,
+                        float* Y, int ldy, float gamma, int product) {
   if (!ctx) return DB200_ERR_INVALID;
   if (m < 0 || n < 0 || d < 1 || l < 0) return fail(ctx, DB200_ERR_INVALID, "rbf_sketch: negative size");
+  if (product != DB200_SKETCH_SINGLE && product != DB200_SKETCH_P_SPLIT && product != DB200_SKETCH_COMPENSATED &&
+      product != DB200_SKETCH_COMPENSATED_PROMOTED)
+    return fail(ctx, DB200_ERR_INVALID, "rbf_sketch: unknown sketch product");
   if (m == 0 || l == 0) return DB200_OK;
   if (d > 128) return fail(ctx, DB200_ERR_UNSUPPORTED, "rbf_sketch: d > 128 not supported");
   if (!Y || ldy < m) return fail(ctx, DB200_ERR_INVALID, "rbf_sketch: bad Y / ldy");
@@ -265,16 +268,27 @@ int db200_rbf_sketch(db200_context* ctx, int m, int n, int d, int l, const float
   int st = check_points(ctx, m, d, Xi, ldxi, x_layout);
   if (!st) st = check_points(ctx, n, d, Xj, ldxj, x_layout);
   if (st) return st;
-  const SketchPlan plan = plan_sketch(l);
+  SketchPlan plan = plan_sketch(l, product == DB200_SKETCH_COMPENSATED_PROMOTED ? 2 : product);
+  // accumulation chunks of two j tiles (256 points): the truncation loss of the tensor cores' fp32 accumulation
+  // stays at ~48 steps x 2^-25 of a value
+  if (product == DB200_SKETCH_COMPENSATED_PROMOTED) plan.promote = 2;
   const int npad = point_pad(n);
+  const size_t op_halves = packed_sketch_halves(plan, npad);
   PackedPoints pi, pj;
   Carve carve{nullptr};
-  st = pack_pair(ctx, m, n, d, Xi, ldxi, Xj, ldxj, x_layout, (size_t)plan.lrows * npad * 2 + 256, pi, pj, carve);
+  st = pack_pair(ctx, m, n, d, Xi, ldxi, Xj, ldxj, x_layout, op_halves * 2 + 256, pi, pj, carve);
   if (st) return st;
-  void* op = carve.take<uint16_t>((size_t)plan.lrows * npad);
-  st = pack_sketch(ctx, Omega, ldo, yj, n, l, npad, plan.lrows, op);
+  void* op = carve.take<uint16_t>(op_halves);
+  st = pack_sketch(ctx, Omega, ldo, yj, n, l, npad, plan.lrows, op, plan.comp);
   if (st) return st;
   return launch_rbf_sketch_exact(ctx, pi, pj, yi, op, plan, l, gamma, Y, ldy);
+}
+
+int db200_rbf_sketch(db200_context* ctx, int m, int n, int d, int l, const float* Xi, int ldxi, const float* Xj,
+                     int ldxj, int x_layout, const float* yi, const float* yj, const float* Omega, int ldo, float* Y,
+                     int ldy, float gamma) {
+  return db200_rbf_sketch_ex(ctx, m, n, d, l, Xi, ldxi, Xj, ldxj, x_layout, yi, yj, Omega, ldo, Y, ldy, gamma,
+                             DB200_SKETCH_SINGLE);
 }
 
 int db200_rbf_block(db200_context* ctx, int m, int n, int d, const float* Xi, int ldxi, const float* Xj, int ldxj,

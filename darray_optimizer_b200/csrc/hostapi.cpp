@@ -221,29 +221,35 @@ int db200_rbf_sketch_f64(db200_context* ctx, int m, int n, int d, int l, const f
   if (!ctx) return DB200_ERR_INVALID;
   if (m < 0 || n < 0 || d < 1 || l < 0 || !Xi || !Xj || ldxi < d || ldxj < d || !Omega || ldo < n || !Y || ldy < m)
     return fail(ctx, DB200_ERR_INVALID, "rbf_sketch_f64: bad arguments");
-  if (m == 0 || l == 0 || n == 0) return DB200_OK;
-  // row blocks of K in FP64: G = Xi_b^T Xj (FP64 Gram of the point matrices), K = y y exp(..), Y_b = K Omega
-  long long b = (1LL << 29) / ((long long)n * 8);  // <= 512 MB per block
-  if (b > m) b = m;
-  if (b < 64) b = 64;
-  const size_t bytes = 1024 + align_up((size_t)b * n * 8, 256) + align_up((size_t)(m + n) * 8, 256) + 1024;
+  if (m == 0 || l == 0) return DB200_OK;
+  if (n == 0) {
+    DB200_CUDA(ctx, cudaMemset2DAsync(Y, sizeof(double) * (size_t)ldy, 0, sizeof(double) * (size_t)m, (size_t)l,
+                                      ctx->stream));
+    return DB200_OK;
+  }
+  if (d > 256) return fail(ctx, DB200_ERR_UNSUPPORTED, "rbf_sketch_f64: d > 256 not supported");
+  // one fused launch: FP64 DMMA distances, FP64 exp, FP64 DMMA sketch product; K never leaves the SM
+  return rbf_sketch_f64_fused(ctx, m, n, d, l, Xi, ldxi, Xj, ldxj, yi, yj, Omega, ldo, Y, ldy, gamma);
+}
+
+int db200_rbf_block_f64(db200_context* ctx, int m, int n, int d, const float* Xi, int ldxi, const float* Xj,
+                        int ldxj, const float* yi, const float* yj, double* K, int ldk, double gamma) {
+  if (!ctx) return DB200_ERR_INVALID;
+  if (m < 0 || n < 0 || d < 1 || !Xi || !Xj || ldxi < d || ldxj < d || !K || ldk < m)
+    return fail(ctx, DB200_ERR_INVALID, "rbf_block_f64: bad arguments");
+  if (m == 0 || n == 0) return DB200_OK;
+  const size_t bytes = 1024 + align_up((size_t)(m + n) * 8, 256) + 1024;
   char* base = static_cast<char*>(slot_buffer(ctx, SLOT_SPARE, bytes));
   if (!base) return DB200_ERR_NOMEM;
   Carve cv{base};
   double* si = cv.take<double>(m);
   double* sj = cv.take<double>(n);
-  double* K = cv.take<double>((size_t)b * n);
   int st = rownorm_f64(ctx, Xi, ldxi, m, d, si);
   if (!st) st = rownorm_f64(ctx, Xj, ldxj, n, d, sj);
-  if (st) return st;
-  for (long long i0 = 0; i0 < m; i0 += b) {
-    const int rb = (int)((m - i0 < b) ? m - i0 : b);
-    if ((st = gram<float, float>(ctx, d, rb, n, Xi + i0 * ldxi, ldxi, Xj, ldxj, nullptr, 1.0, 0.0, K, rb, false)))
-      return st;
-    if ((st = rbf_from_gram_f64(ctx, K, rb, rb, n, si + i0, sj, yi ? yi + i0 : nullptr, yj, gamma))) return st;
-    if ((st = gemm_tall<double, double>(ctx, rb, n, l, K, rb, Omega, ldo, false, 0.0, Y + i0, ldy))) return st;
-  }
-  return DB200_OK;
+  // G = Xi Xj^T on the FP64 tensor cores (the Gram kernel over the d features), then K in place
+  if (!st) st = gram<float, float>(ctx, d, m, n, Xi, ldxi, Xj, ldxj, nullptr, 1.0, 0.0, K, ldk, false);
+  if (!st) st = rbf_from_gram_f64(ctx, K, ldk, m, n, si, sj, yi, yj, gamma);
+  return st;
 }
 
 int db200_vec_update(db200_context* ctx, int n, double alpha, const double* x, double beta, double* y,

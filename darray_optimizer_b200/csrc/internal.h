@@ -86,24 +86,34 @@ int lu_factorize(db200_context* ctx, int m, int n, int nleft, float* A, long lon
 enum RbfMode { RBF_MODE_SKETCH = 0, RBF_MODE_KBLOCK = 1 };
 
 struct PackedPoints {
-  const void* xp = nullptr;   // bf16 [npad][2*dp]: [hi | lo] split of each point
-  const float* norms = nullptr;  // fp32 [npad], ||x||^2 (zero on padding rows)
+  const void* xp = nullptr;   // fp16 [npad][2*dp]: [hi | lo] split of each point scaled by the set's 2^e
+  const float* norms = nullptr;  // fp32: ||x||^2 [npad] (zero on padding rows), then max |x| bits and 2^-e
   int n = 0, npad = 0, dp = 0;
 };
+// floats of the norms-and-scale array of a packed set of npad points
+inline size_t packed_norm_floats(int npad) { return (size_t)npad + 64; }
 
-// Pack points into the split-bf16 operand layout plus squared norms.
+// Pack points into the split-fp16 operand layout (one power-of-two scale for the set) plus squared norms and the
+// scale (norms must hold packed_norm_floats(npad) floats).  Two kernels: the set's max |x|, then the split.
 // layout: DB200_POINT_MAJOR (x_ik = X[k + i*ldx]) or DB200_FEATURE_MAJOR (x_ik = X[i + k*ldx]).
 int pack_points(db200_context* ctx, const float* X, int ldx, int layout, int n, int d, int dp, int npad, void* xp,
                 float* norms);
 
-// Omega^T (fp16, [lrows][njpad]) with the column labels folded in: Op[c][j] = y_j * Omega[j + c*ldo].
+// Omega^T (fp16, [lrows][njpad]) with the column labels folded in: Op[c][j] = y_j * Omega[j + c*ldo]; with
+// comp = 2 a second [lrows][njpad] block follows with the lo parts (fp16 of the hi rounding's residual).
 int pack_sketch(db200_context* ctx, const float* Omega, int ldo, const float* yj, int n, int l, int njpad, int lrows,
-                void* op);
+                void* op, int comp = 0);
 
+// comp: sketch product P.Om (0), + P_lo.Om (1), + P_hi.Om_lo (2, compensated); promote: j tiles per TMEM
+// accumulation chunk, each chunk added into Y in fp32 (0: one accumulation over all j)
 struct SketchPlan {
-  int n_panels = 1, panel = 16, lrows = 16, g_bufs = 2;
+  int n_panels = 1, panel = 16, lrows = 16, g_bufs = 2, comp = 0, promote = 0;
 };
-SketchPlan plan_sketch(int l);
+SketchPlan plan_sketch(int l, int comp = 0);
+// halves (2-byte elements) of the packed Omega~ operand for a plan over njpad points
+inline size_t packed_sketch_halves(const SketchPlan& p, int njpad) {
+  return (size_t)p.lrows * njpad * (p.comp == 2 ? 2 : 1);
+}
 int feature_pad(int d);  // dp: padded feature count of the split operand
 // Packed point counts are padded to whole 256-row tiles (one CTA pair of the tile kernel), on both sides, so that
 // a set used as rows and as columns packs once.
@@ -117,6 +127,7 @@ struct TileJob {
   const float* yj = nullptr;
   const void* op = nullptr;
   SketchPlan plan;
+  int om_lo = 0;  // comp = 2: row offset of the lo rows of Omega~ from `op`
   int l = 0;
   float gamma = 0.f;
   float* out = nullptr;
@@ -124,7 +135,7 @@ struct TileJob {
 };
 // A prepared launch: the instance table is on the device; launch_rbf_plan only launches (graph-capturable).
 struct TilePlan {
-  int mode = 0, count = 0, n_items = 0, nsx = 0, nso = 0, nkc_max = 0, panel_max = 0;
+  int mode = 0, count = 0, n_items = 0, nsx = 0, nso = 0, nkc_max = 0, panel_max = 0, om_mult = 1;
   int clusters = 0;  // persistent grid: CTA pairs resident at once (at most one per item)
   size_t smem = 0;
   const void* table = nullptr;
@@ -154,6 +165,9 @@ int launch_rbf_tiles(db200_context* ctx, int mode, const PackedPoints& pi, const
                      const float* yj, const void* op, const SketchPlan& plan, int l, float gamma, float* out,
                      int ldo, void* table_storage = nullptr, size_t table_capacity = 0);
 
+// Per-panel instances of exact widths for a multi-panel sketch job (plan.n_panels panels covering roundup(l, 16)),
+// appended to `out`; a one-panel job is appended as it is.
+void exact_panel_jobs(const TileJob& base, std::vector<TileJob>& out);
 // The sketch as one launch over per-panel instances of exact widths (plan.n_panels panels covering roundup(l, 16)).
 int launch_rbf_sketch_exact(db200_context* ctx, const PackedPoints& pi, const PackedPoints& pj, const float* yi,
                             const void* op, const SketchPlan& plan, int l, float gamma, float* out, int ldo);

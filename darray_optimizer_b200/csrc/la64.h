@@ -42,6 +42,10 @@ int rbf_from_gram_f64(db200_context* ctx, double* K, long long ldk, int m, int n
                       const float* yi, const float* yj, double gamma);
 // FP64 squared norms of the n points of a point-major float matrix
 int rownorm_f64(db200_context* ctx, const float* X, long long ldx, int n, int d, double* s);
+// Fused FP64 RBF x sketch (rbf64.cu): Y = diag(yi) K(Xi, Xj) diag(yj) Omega, FP64 throughout, K never stored.
+int rbf_sketch_f64_fused(db200_context* ctx, int m, int n, int d, int l, const float* Xi, int ldxi, const float* Xj,
+                         int ldxj, const float* yi, const float* yj, const double* Omega, int ldo, double* Y, int ldy,
+                         double gamma);
 // sort descending, n <= 8192
 int sort_desc(db200_context* ctx, double* v, int n);
 

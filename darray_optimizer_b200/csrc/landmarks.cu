@@ -739,20 +739,22 @@ int db200_select_topk(db200_context* ctx, int n, const float* keys, int k, int* 
 }
 
 // ------------------------------------------------------------------ landmark factor and residual
-int db200_landmark_factor(db200_context* ctx, int n, int d, const float* X, int ldx, const float* y, float gamma, int r,
-                          const int* idx, double* Z, int ldz, double* nu_out) {
-  if (!ctx) return DB200_ERR_INVALID;
-  if (n < 1 || d < 1 || d > 128 || ldx < d || r < 1 || r > n || !X || !y || !idx || !Z || ldz < n)
-    return fail(ctx, DB200_ERR_INVALID, "landmark_factor: bad arguments");
+}  // extern "C"
+
+// Nystrom factor on landmarks idx; TC = float: C from the tcgen05 tile engine (KBLOCK mode, fp32), TC = double: C
+// from the FP64 kernel block (FP64 tensor-core Gram, FP64 exp), the comparator.
+template <typename TC>
+static int landmark_factor_impl(db200_context* ctx, int n, int d, const float* X, int ldx, const float* y,
+                                float gamma, int r, const int* idx, double* Z, int ldz, double* nu_out) {
   const size_t rr = (size_t)r * r;
-  const size_t bytes = 4096 + align_up((size_t)n * r * 4, 256) + 3 * align_up(rr * 8, 256) +
+  const size_t bytes = 4096 + align_up((size_t)n * r * sizeof(TC), 256) + 3 * align_up(rr * 8, 256) +
                        align_up((size_t)r * d * 4, 256) + align_up((size_t)r * 4, 256);
   char* base = static_cast<char*>(slot_buffer(ctx, SLOT_PIPE, bytes));
   if (!base) return DB200_ERR_NOMEM;
   Carve cv{base};
   int* d_pair = cv.take<int>(4);
   double* d_scalar = cv.take<double>(4);
-  float* Cm = cv.take<float>((size_t)n * r);
+  TC* Cm = cv.take<TC>((size_t)n * r);
   double* W = cv.take<double>(rr);
   double* R = cv.take<double>(rr);
   double* Xinv = cv.take<double>(rr);
@@ -762,10 +764,14 @@ int db200_landmark_factor(db200_context* ctx, int n, int d, const float* X, int 
   gather_f32_kernel<<<blocks_for(r, 256, 1024), 256, 0, ctx->stream>>>(y, idx, r, yL);
   DB200_CUDA(ctx, cudaGetLastError());
   count_launch(ctx, 2);
-  // C = diag(y) K(:, L) diag(y_L): the fused tile kernel in kernel-block mode
-  int st = db200_rbf_block(ctx, n, r, d, X, ldx, XL, d, DB200_POINT_MAJOR, y, yL, Cm, n, gamma);
+  // C = diag(y) K(:, L) diag(y_L)
+  int st;
+  if constexpr (sizeof(TC) == 4)
+    st = db200_rbf_block(ctx, n, r, d, X, ldx, XL, d, DB200_POINT_MAJOR, y, yL, Cm, n, gamma);
+  else
+    st = db200_rbf_block_f64(ctx, n, r, d, X, ldx, XL, d, y, yL, Cm, n, (double)gamma);
   if (st) return st;
-  gather_matrix_rows_kernel<float><<<blocks_for((long long)rr, 256, 4096), 256, 0, ctx->stream>>>(Cm, n, idx, r, r, W);
+  gather_matrix_rows_kernel<TC><<<blocks_for((long long)rr, 256, 4096), 256, 0, ctx->stream>>>(Cm, n, idx, r, r, W);
   DB200_CUDA(ctx, cudaGetLastError());
   count_launch(ctx);
   if ((st = symmetrize(ctx, W, r, r, 0.0))) return st;
@@ -789,9 +795,26 @@ int db200_landmark_factor(db200_context* ctx, int n, int d, const float* X, int 
   if (!ok) return fail(ctx, DB200_ERR_NOT_SPD, "landmark_factor: K(L, L) + nu I not positive definite after 12 shifts");
   // Z = C R^-1
   if ((st = trinv_upper(ctx, R, r, r, Xinv, r))) return st;
-  if ((st = gemm_tall<float, double>(ctx, n, r, r, Cm, n, Xinv, r, false, 0.0, Z, ldz))) return st;
+  if ((st = gemm_tall<TC, double>(ctx, n, r, r, Cm, n, Xinv, r, false, 0.0, Z, ldz))) return st;
   if (nu_out) *nu_out = nu;
   return db200_synchronize(ctx);
+}
+
+extern "C" {
+
+int db200_landmark_factor(db200_context* ctx, int n, int d, const float* X, int ldx, const float* y, float gamma, int r,
+                          const int* idx, double* Z, int ldz, double* nu_out) {
+  return db200_landmark_factor_ex(ctx, n, d, X, ldx, y, gamma, r, idx, Z, ldz, nu_out, DB200_MIXED);
+}
+
+int db200_landmark_factor_ex(db200_context* ctx, int n, int d, const float* X, int ldx, const float* y, float gamma,
+                             int r, const int* idx, double* Z, int ldz, double* nu_out, int precision) {
+  if (!ctx) return DB200_ERR_INVALID;
+  if (n < 1 || d < 1 || d > 128 || ldx < d || r < 1 || r > n || !X || !y || !idx || !Z || ldz < n ||
+      (precision != DB200_MIXED && precision != DB200_FP64 && precision != DB200_MIXED_FAST))
+    return fail(ctx, DB200_ERR_INVALID, "landmark_factor: bad arguments");
+  return precision == DB200_FP64 ? landmark_factor_impl<double>(ctx, n, d, X, ldx, y, gamma, r, idx, Z, ldz, nu_out)
+                                 : landmark_factor_impl<float>(ctx, n, d, X, ldx, y, gamma, r, idx, Z, ldz, nu_out);
 }
 
 int db200_residual_estimate(db200_context* ctx, int n, int d, const float* X, int ldx, const float* y, float gamma,
@@ -834,6 +857,57 @@ int db200_residual_estimate(db200_context* ctx, int n, int d, const float* X, in
 }
 
 // ------------------------------------------------------------------ the learned-landmark solve
+// Landmark selection of the learned solve: k-NN features over sk reference points -> MLP log-leverage -> Gumbel
+// keys -> top r.  Scratch F, knn, logits, keys, ref come from the caller's carve; idx receives r device indices.
+static int select_landmarks_impl(db200_context* ctx, int n, int d, int r, const float* X, int ldx, const db200_mlp* net,
+                                 unsigned long long seed, int sk, float* F, float* knn, float* logits, float* keys,
+                                 int* ref, int* idx, db200_landmark_report* L) {
+  const std::vector<int> h_ref = sample_indices(n, sk, seed ^ 0x6b6e6eull);
+  DB200_CUDA(ctx, cudaMemcpyAsync(ref, h_ref.data(), sizeof(int) * sk, cudaMemcpyHostToDevice, ctx->stream));
+  int st;
+  {
+    LandTimer t(ctx->stream);
+    if ((st = knn_distance(ctx, n, d, X, ldx, sk, ref, 8, knn))) return st;
+    if ((st = db200_leverage_features(ctx, n, d, X, ldx, knn, F))) return st;
+    L->ms_features = t.stop();
+  }
+  {
+    LandTimer t(ctx->stream);
+    if ((st = db200_mlp_forward(ctx, net, n, F, logits))) return st;
+    L->ms_predict = t.stop();
+  }
+  {
+    LandTimer t(ctx->stream);
+    if ((st = db200_gumbel_keys(ctx, n, logits, seed, keys))) return st;
+    if ((st = db200_select_topk(ctx, n, keys, r, idx))) return st;
+    L->ms_select = t.stop();
+  }
+  return DB200_OK;
+}
+
+int db200_select_landmarks(db200_context* ctx, int n, int d, int r, const float* X, int ldx, const db200_mlp* net,
+                           unsigned long long seed, int s_knn, int* idx) {
+  if (!ctx) return DB200_ERR_INVALID;
+  if (n < 2 || d < 1 || d > 128 || ldx < d || r < 1 || r > n || !X || !net || net->in != d + 2 || s_knn < 9 || !idx)
+    return fail(ctx, DB200_ERR_INVALID, "select_landmarks: bad arguments (model input must be d + 2)");
+  const int sk = std::min(s_knn, n);
+  const size_t bytes = 4096 + align_up((size_t)n * (d + 2) * 4, 256) + 3 * align_up((size_t)n * 4, 256) +
+                       align_up((size_t)sk * 4, 256);
+  char* base = static_cast<char*>(slot_buffer(ctx, SLOT_LAND, bytes));
+  if (!base) return DB200_ERR_NOMEM;
+  Carve cv{base};
+  float* F = cv.take<float>((size_t)n * (d + 2));
+  float* knn = cv.take<float>(n);
+  float* logits = cv.take<float>(n);
+  float* keys = cv.take<float>(n);
+  int* ref = cv.take<int>(sk);
+  db200_landmark_report L;
+  std::memset(&L, 0, sizeof(L));
+  int st = select_landmarks_impl(ctx, n, d, r, X, ldx, net, seed, sk, F, knn, logits, keys, ref, idx, &L);
+  if (st) return st;
+  return db200_synchronize(ctx);
+}
+
 int db200_svm_solve_landmarks(db200_context* ctx, int n, int d, int r, const float* X, int ldx, const float* y,
                               float gamma, double C, const db200_mlp* net, unsigned long long seed, int s_knn,
                               int s_res, double tol, const float* Omega, int ldo, int l_fb, int q,
@@ -861,32 +935,21 @@ int db200_svm_solve_landmarks(db200_context* ctx, int n, int d, int r, const flo
   int* idx = cv.take<int>(r);
   int* ref = cv.take<int>(sk);
   int* res = cv.take<int>(sr);
-  const std::vector<int> h_ref = sample_indices(n, sk, seed ^ 0x6b6e6eull);
   const std::vector<int> h_res = sample_indices(n, sr, seed ^ 0x726573ull);
-  DB200_CUDA(ctx, cudaMemcpyAsync(ref, h_ref.data(), sizeof(int) * sk, cudaMemcpyHostToDevice, ctx->stream));
   DB200_CUDA(ctx, cudaMemcpyAsync(res, h_res.data(), sizeof(int) * sr, cudaMemcpyHostToDevice, ctx->stream));
-  int st;
-  {
-    LandTimer t(ctx->stream);
-    if ((st = knn_distance(ctx, n, d, X, ldx, sk, ref, 8, knn))) return st;
-    if ((st = db200_leverage_features(ctx, n, d, X, ldx, knn, F))) return st;
-    L.ms_features = t.stop();
-  }
-  {
-    LandTimer t(ctx->stream);
-    if ((st = db200_mlp_forward(ctx, net, n, F, logits))) return st;
-    L.ms_predict = t.stop();
-  }
-  {
-    LandTimer t(ctx->stream);
-    if ((st = db200_gumbel_keys(ctx, n, logits, seed, keys))) return st;
-    if ((st = db200_select_topk(ctx, n, keys, r, idx))) return st;
-    L.ms_select = t.stop();
-  }
+  int st = select_landmarks_impl(ctx, n, d, r, X, ldx, net, seed, sk, F, knn, logits, keys, ref, idx, &L);
+  if (st) return st;
   {
     LandTimer t(ctx->stream);
     double nu = 0;
-    if ((st = db200_landmark_factor(ctx, n, d, X, ldx, y, gamma, r, idx, Z, ldz, &nu))) return st;
+    // The landmark columns C = K(:, L) cost n r d, a fraction r / n of one Gaussian kernel pass: the parity-grade
+    // mixed form (and the FP64 one) takes them in FP64, whose factor then matches the FP64 Nystrom factor on the
+    // same landmarks to round-off; the fast mixed form takes the tile engine's fp32 block (~1e-6 from FP64 in f).
+    db200_barrier_params Pf;
+    if (params) Pf = *params;
+    else db200_barrier_defaults(&Pf);
+    const int cprec = (Pf.precision == DB200_MIXED_FAST) ? DB200_MIXED_FAST : DB200_FP64;
+    if ((st = db200_landmark_factor_ex(ctx, n, d, X, ldx, y, gamma, r, idx, Z, ldz, &nu, cprec))) return st;
     R.nu = nu;
     L.ms_factor = t.stop();
   }

@@ -3,12 +3,11 @@
 // Some callers cannot allocate device memory: plugin hosts that hand out a stream but own every allocation
 // (the library must not call cudaMalloc/cudaFree behind their allocator), code running under a strict
 // memory budget, or a process that must not touch the allocator between set-up and a latency-critical phase.
-// This entry point serves them.  Its scratch (packed split-bf16 points, norms, packed Omega^T and the device
-// status word) lives in one file-scope __device__ array of DB200_NOALLOC_SCRATCH_BYTES, which every GPU that
+// This entry point serves them.  Its scratch (packed split-fp16 points, norms and scales, packed Omega^T and the
+// device status word) lives in one file-scope __device__ array of DB200_NOALLOC_SCRATCH_BYTES, which every GPU that
 // loads the library holds until the process exits.  Nothing here calls cudaMalloc, cudaFree or any allocating
 // library routine.
 #include <cstdio>
-#include <mutex>
 
 #include "internal.h"
 
@@ -19,25 +18,19 @@ namespace {
 // must be obtained with cudaGetSymbolAddress on each device before a kernel may use it.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[DB200_NOALLOC_SCRATCH_BYTES];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_setup_mutex;
-void* g_scratch_addr[kMaxDevices] = {};
-
-// Resolve the scratch array's device address on the current device (once per device).
+// Resolve the scratch array's device address in the current context.  Done on every call rather than cached per
+// device: an address is only valid in the context it was resolved in, and a caller may make its own context
+// current on the device, or reset the device, between calls.  The lookup costs microseconds against a call that
+// waits for its kernels anyway.
 int scratch_address(int device, void** out) {
-  if (device < 0 || device >= kMaxDevices) return DB200_ERR_UNSUPPORTED;
-  std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (!g_scratch_addr[device]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p) {
-      std::fprintf(stderr, "db200_rbf_sketch_noalloc: cudaGetSymbolAddress failed on device %d: %s\n", device,
-                   cudaGetErrorString(e));
-      return DB200_ERR_CUDA;
-    }
-    g_scratch_addr[device] = p;
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p) {
+    std::fprintf(stderr, "db200_rbf_sketch_noalloc: cudaGetSymbolAddress failed on device %d: %s\n", device,
+                 cudaGetErrorString(e));
+    return DB200_ERR_CUDA;
   }
-  *out = g_scratch_addr[device];
+  *out = p;
   return DB200_OK;
 }
 
@@ -51,8 +44,16 @@ extern "C" int db200_rbf_sketch_noalloc(void* stream, int m, int n, int d, int l
                                         const float* Omega, int ldo, float* Y, int ldy, float gamma) {
   if (m < 0 || n < 0 || d < 1 || l < 0) return DB200_ERR_INVALID;
   if (m == 0 || l == 0) return DB200_OK;
-  if (n < 1 || d > 128) return DB200_ERR_UNSUPPORTED;
-  if (!Xi || !Xj || !Omega || !Y || ldo < n || ldy < m) return DB200_ERR_INVALID;
+  if (d > 128) return DB200_ERR_UNSUPPORTED;
+  if (!Y || ldy < m) return DB200_ERR_INVALID;
+  if (n == 0) {
+    // an empty sum: Y = 0, as db200_rbf_sketch gives (a memset allocates nothing)
+    cudaStream_t st0 = static_cast<cudaStream_t>(stream);
+    if (cudaMemset2DAsync(Y, sizeof(float) * (size_t)ldy, 0, sizeof(float) * (size_t)m, (size_t)l, st0) != cudaSuccess)
+      return DB200_ERR_CUDA;
+    return cudaStreamSynchronize(st0) == cudaSuccess ? DB200_OK : DB200_ERR_CUDA;
+  }
+  if (!Xi || !Xj || !Omega || ldo < n) return DB200_ERR_INVALID;
   if (x_layout == DB200_POINT_MAJOR) {
     if (ldxi < d || ldxj < d) return DB200_ERR_INVALID;
   } else if (x_layout == DB200_FEATURE_MAJOR) {
@@ -69,12 +70,12 @@ extern "C" int db200_rbf_sketch_noalloc(void* stream, int m, int n, int d, int l
   const SketchPlan plan = plan_sketch(l);
   size_t need = 256;
   need = align_up(need + (size_t)mpad * 2 * dp * 2, 256);
-  need = align_up(need + (size_t)mpad * 4, 256);
+  need = align_up(need + packed_norm_floats(mpad) * 4, 256);
   if (!same) {
     need = align_up(need + (size_t)npad * 2 * dp * 2, 256);
-    need = align_up(need + (size_t)npad * 4, 256);
+    need = align_up(need + packed_norm_floats(npad) * 4, 256);
   }
-  need = align_up(need + (size_t)plan.lrows * npad * 2, 256);
+  need = align_up(need + packed_sketch_halves(plan, npad) * 2, 256);
   need = align_up(need + tile_table_bytes(1), 256);
   if (need > (size_t)DB200_NOALLOC_SCRATCH_BYTES) {
     std::fprintf(stderr,
@@ -102,7 +103,7 @@ extern "C" int db200_rbf_sketch_noalloc(void* stream, int m, int n, int d, int l
 
   PackedPoints pi, pj;
   void* xpi = carve.take<uint16_t>((size_t)mpad * 2 * dp);
-  float* ni = carve.take<float>(mpad);
+  float* ni = carve.take<float>(packed_norm_floats(mpad));
   if ((st = pack_points(&ctx, Xi, ldxi, x_layout, m, d, dp, mpad, xpi, ni))) return st;
   pi.xp = xpi;
   pi.norms = ni;
@@ -113,7 +114,7 @@ extern "C" int db200_rbf_sketch_noalloc(void* stream, int m, int n, int d, int l
     pj = pi;
   } else {
     void* xpj = carve.take<uint16_t>((size_t)npad * 2 * dp);
-    float* nj = carve.take<float>(npad);
+    float* nj = carve.take<float>(packed_norm_floats(npad));
     if ((st = pack_points(&ctx, Xj, ldxj, x_layout, n, d, dp, npad, xpj, nj))) return st;
     pj.xp = xpj;
     pj.norms = nj;
@@ -121,7 +122,7 @@ extern "C" int db200_rbf_sketch_noalloc(void* stream, int m, int n, int d, int l
     pj.npad = npad;
     pj.dp = dp;
   }
-  void* op = carve.take<uint16_t>((size_t)plan.lrows * npad);
+  void* op = carve.take<uint16_t>(packed_sketch_halves(plan, npad));
   if ((st = pack_sketch(&ctx, Omega, ldo, yj, n, l, npad, plan.lrows, op))) return st;
   void* table = carve.take<char>(tile_table_bytes(1));  // the tile engine's one-instance table
   if ((st = launch_rbf_tiles(&ctx, RBF_MODE_SKETCH, pi, pj, yi, nullptr, op, plan, l, gamma, Y, ldy, table,
@@ -129,8 +130,11 @@ extern "C" int db200_rbf_sketch_noalloc(void* stream, int m, int n, int d, int l
     return st;
 
   // Synchronous: wait, then report a device-side wait that gave up.
-  if (cudaStreamSynchronize(ctx.stream) != cudaSuccess) return DB200_ERR_CUDA;
+  // The status read is ordered on the caller's stream only: a cudaMemcpy on the legacy default stream would also
+  // wait for every other blocking stream of the process.
   int dev_status = 0;
-  if (cudaMemcpy(&dev_status, ctx.d_status, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return DB200_ERR_CUDA;
+  if (cudaMemcpyAsync(&dev_status, ctx.d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream) != cudaSuccess)
+    return DB200_ERR_CUDA;
+  if (cudaStreamSynchronize(ctx.stream) != cudaSuccess) return DB200_ERR_CUDA;
   return dev_status;
 }

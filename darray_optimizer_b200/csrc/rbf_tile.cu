@@ -1,17 +1,26 @@
 // Fused RBF-kernel tile engine for sm_100a (tcgen05 + TMEM + TMA).
 //
-// Squared distances use the GEMM form ||x||^2 + ||y||^2 - 2 x.y of include/dkernel.cu:116-129 with x split into
-// bf16 hi + lo; the norms are formed from the same split products as the cross term, so the sum cancels to fp32
-// round-off on the diagonal instead of leaving the split's representation error (~3 * 2^-18 ||x||^2).
+// Squared distances use the GEMM form ||x||^2 + ||y||^2 - 2 x.y of include/dkernel.cu:116-129.  Each point set is
+// scaled by one power of two 2^e (largest |coordinate| just below 2^14, so every product and sum stays far inside
+// fp16 and fp32) and split into fp16 hi + lo (22 significant bits; a bf16 split keeps 16, whose representation
+// error ~2^-17 |x| left the dual objective 3e-6 from FP64 at n = 4096, d = 32).  The norms are formed from the
+// same split products as the cross term, so the sum cancels to fp32 round-off on the diagonal instead of leaving
+// the split's representation error.  The epilogue undoes the scales: x.y = 2^-(e_I + e_J) G.
 //
 // A CTA pair (cluster of 2) owns a 256-row block of points i and one panel of sketch columns.  It streams every
 // 128-column block of points j and, per tile:
-//   MMA1  G   = Xi . Xj^T  in TMEM (fp32), from split-bf16 operands: hi.hi + hi.lo + lo.hi
-//   epi   P   = exp2(min(a_i + b_j + c*G, 0)),  a = -gamma*log2(e)*||x||^2,  c = 2*gamma*log2(e)
+//   MMA1  G   = Xi . Xj^T  in TMEM (fp32), from split-fp16 operands: hi.hi + hi.lo + lo.hi
+//   epi   P   = exp2(min(a_i + b_j + c G, 0)),  a = -gamma*log2(e)*||x||^2,  c = 2*gamma*log2(e) 2^-(e_I+e_J)
 //   MMA2  Y  += P . Omega~_j   (SKETCH mode; P is written to tensor memory as the fp16 A operand, Omega~ is fp16)
 //         or  K[i, j] = y_i y_j P   stored as fp32 (KBLOCK mode)
 // so the kernel matrix is never written to HBM in SKETCH mode.  Algorithm restated from
 // include/dkernel.cu:102-129 (vecnorm, rbf) and :151-178 / :194-231 (distance GEMM, rbf, sketch GEMM).
+//
+// Compensated sketch (SKETCH mode, per instance): P is also split into fp16 hi + lo (P_lo = fp16(P - P_hi), in a
+// second 64-column TMEM tile) and Omega~ into hi + lo rows, and MMA2 issues P_hi.Om_hi + P_lo.Om_hi (+ P_hi.Om_lo)
+// into the same fp32 accumulator: ~22-bit operands instead of 11.  The single fp16 product's rounding of P (2^-12
+// of a kernel value, which at n = 131072 is half the size of the sketch's tail entries) moves the range finder's
+// subspace enough to leave the dual objective ~4e-4 from FP64; the compensated product brings it to ~1e-7.
 //
 // Both MMAs are issued by the pair leader as tcgen05 cta_group::2 instructions with M = 256: each CTA supplies its
 // own 128 rows of A (Xi in shared memory, P in tensor memory) and half of the rows of B (Xj, Omega~), and holds
@@ -41,9 +50,9 @@ constexpr int BM = 128;                    // rows of i per CTA (TMEM lanes)
 constexpr int PAIR_M = 256;                // rows of i per CTA pair (UMMA M of the 2-SM instructions)
 constexpr int BN = 128;                    // columns of j per tile
 constexpr int BN_HALF = BN / 2;            // rows of Xj each CTA of the pair holds per tile
-constexpr int KC = 64;                     // bf16 elements per 128-byte swizzled row chunk
-constexpr int XI_CHUNK = BM * KC * 2;      // 128 x 64 bf16 = 16 KB
-constexpr int XJ_CHUNK = BN_HALF * KC * 2; // 64 x 64 bf16 = 8 KB
+constexpr int KC = 64;                     // 16-bit elements per 128-byte swizzled row chunk
+constexpr int XI_CHUNK = BM * KC * 2;      // 128 x 64 fp16 = 16 KB
+constexpr int XJ_CHUNK = BN_HALF * KC * 2; // 64 x 64 fp16 = 8 KB
 constexpr int NUM_EPI_WARPS = 16;
 constexpr int EPI_COLS = BN / (NUM_EPI_WARPS / 4);  // tile columns per epilogue warp (32)
 constexpr int OM_WARP = 2 + NUM_EPI_WARPS;          // Omega producer warp (18)
@@ -61,6 +70,8 @@ struct alignas(64) TileInst {
   CUtensorMap tm_xi, tm_xj, tm_om1, tm_om2;  // packed points (rows i, rows j) and the two Omega~ row boxes
   const float* si;       // squared norms, padded to n_itiles * 256 / n_jtiles * 128
   const float* sj;
+  const float* fi;       // the point sets' scales 2^-e of the packed operands (one float each)
+  const float* fj;
   const float* yi;
   const float* yj;
   float* out;
@@ -69,8 +80,11 @@ struct alignas(64) TileInst {
   int n_itiles, n_jtiles, n_panels, panel, l;  // n_itiles counts 256-row pair tiles
   int n1, n2;            // sketch MMA split of the panel: N = n1 (+ n2) columns, n2 = 0 for one instruction
   int g_bufs;            // 1 or 2 TMEM buffers of 128 columns for G
-  int tmem_p, tmem_y;    // first TMEM column of the P tile (64 columns) and of the Y panel
+  int tmem_p, tmem_y;    // first TMEM column of the P tile (64 columns, 128 with P_lo) and of the Y panel
   int nkc;               // 64-element chunks per packed row [hi | lo]: 1..4 (feature pad 32..128)
+  int comp;              // sketch product: 0 = P.Om, 1 = + P_lo.Om, 2 = + P_hi.Om_lo (compensated)
+  int om_lo;             // row offset of the Omega~ lo rows inside the packed operand (comp = 2)
+  int promote;           // j tiles per TMEM accumulation chunk, each chunk added into Y in fp32 (0: whole item)
   int item_begin;        // first work item of this instance
   float c_row, c_dot;    // -gamma*log2e, 2*gamma*log2e
 };
@@ -83,18 +97,19 @@ struct LaunchArgs {
   int count, n_items;
   int nsx, nso;          // Xj and Omega ring stages
   int nkc_max, panel_max;  // shared-memory layout covers every instance
+  int om_mult;           // Omega stage copies: 1, or 2 when an instance loads hi and lo rows (comp = 2)
   int* status;
 };
 
 struct SmemLayout {
-  int om_stage;  // bytes of one Omega stage in one CTA: (panel / 2) rows x 128 B
+  int om_stage;  // bytes of one Omega stage in one CTA: (panel / 2) rows x 128 B, twice with lo rows
   size_t off_xi, off_xj, off_om, off_sj, off_bar, total;
 };
 constexpr int SJ_BYTES = NUM_EPI_WARPS * 2 * EPI_COLS * 4;  // per epilogue warp: two tiles' column norms
 
-__host__ __device__ inline SmemLayout make_layout(int nkc, int panel, int nsx, int nso) {
+__host__ __device__ inline SmemLayout make_layout(int nkc, int panel, int nsx, int nso, int om_mult) {
   SmemLayout L;
-  L.om_stage = (panel / 2) * 128;
+  L.om_stage = (panel / 2) * 128 * om_mult;
   L.off_xi = 0;
   L.off_xj = L.off_xi + (size_t)nkc * XI_CHUNK;
   L.off_om = L.off_xj + (size_t)nsx * XJ_CHUNK;
@@ -148,16 +163,17 @@ struct Issuer {
   volatile int* abort_flag;
   uint32_t xs, xph, os, oph, pph;
   uint32_t guse0, guse1, gnext;  // uses of G buffer 0 / 1 (their phases) and the next buffer to fill
+  uint32_t ydone;                // Y accumulations committed to the epilogue so far (B_Y_FULL phases)
 };
 
 __device__ __forceinline__ bool issuer_wait(const Issuer& S, int idx, uint32_t parity) {
   return __all_sync(0xffffffffu, mbar_wait(S.s_bar + 8u * (uint32_t)idx, parity, S.abort_flag));
 }
 
-// Distance MMA of one tile into the next G buffer, for a packed row of 2 * DP elements (split bf16).
+// Distance MMA of one tile into the next G buffer, for a packed row of 2 * DP elements (split fp16).
 template <int DP>
 __device__ __forceinline__ bool issue_mma1(Issuer& S, int g_bufs) {
-  constexpr uint32_t idesc_g = idesc_f16(PAIR_M, BN, true);
+  constexpr uint32_t idesc_g = idesc_f16(PAIR_M, BN, false);
   constexpr int NKC = (2 * DP) / KC;
   const uint32_t gbuf = S.gnext;
   const uint32_t guse = gbuf ? S.guse1 : S.guse0;
@@ -198,12 +214,14 @@ __device__ __forceinline__ bool issue_mma1(Issuer& S, int g_bufs) {
 
 // Per-item constants of the sketch MMA.
 struct SketchMma {
-  uint32_t idesc_y1, idesc_y2, y2_boff, tmem_p, tmem_y, tmem_y2;
+  uint32_t idesc_y1, idesc_y2, y2_boff, lo_boff, tmem_p, tmem_y, tmem_y2;
 };
 
 // Sketch MMA of one tile: two K chunks of 64, one per P half.  fp16 operands (P in [0, 1], Omega~ Gaussian: both
-// well inside fp16 range, 3 more mantissa bits than bf16 at the same tensor rate).
-template <bool TWO>
+// well inside fp16 range, 3 more mantissa bits than bf16 at the same tensor rate).  COMP >= 1 adds P_lo.Om_hi
+// (P_lo 64 TMEM columns after P_hi), COMP = 2 also P_hi.Om_lo (the lo rows follow the hi rows in each Omega
+// stage); compensated panels take one instruction (N <= 256).
+template <bool TWO, int COMP>
 __device__ __forceinline__ bool issue_mma2(Issuer& S, const SketchMma& Y, int jt) {
 #pragma unroll
   for (int c = 0; c < 2; ++c) {
@@ -221,6 +239,8 @@ __device__ __forceinline__ bool issue_mma2(Issuer& S, const SketchMma& Y, int jt
         const uint32_t acc = (jt > 0 || c > 0 || ks > 0) ? 1u : 0u;
         umma_f16_ts_pair(Y.tmem_y, a_tmem, bdesc, Y.idesc_y1, acc);
         if (TWO) umma_f16_ts_pair(Y.tmem_y2, a_tmem, bdesc + Y.y2_boff, Y.idesc_y2, acc);
+        if (COMP >= 1) umma_f16_ts_pair(Y.tmem_y, a_tmem + 64, bdesc, Y.idesc_y1, 1u);
+        if (COMP >= 2) umma_f16_ts_pair(Y.tmem_y, a_tmem, bdesc + Y.lo_boff, Y.idesc_y1, 1u);
       }
       umma_commit_pair(S.s_bar + 8u * (uint32_t)(S.OM_EMPTY + (int)S.os));
       umma_commit_pair(S.s_bar + 8u * (uint32_t)(B_P_EMPTY0 + c));
@@ -233,24 +253,90 @@ __device__ __forceinline__ bool issue_mma2(Issuer& S, const SketchMma& Y, int jt
 }
 
 // All MMAs of one work item (every j tile, distance MMA one tile ahead of the sketch MMA), specialised for the
-// instance's feature width and panel split so the hot loop carries no dispatch.
-template <int MODE, int DP, bool TWO>
-__device__ __forceinline__ bool issue_item(Issuer& S, const SketchMma& Y, int njt, int g_bufs) {
+// instance's feature width and panel split so the hot loop carries no dispatch.  With promote = T > 0 the sketch
+// accumulator restarts every T tiles: each chunk is committed to the epilogue, which adds it into Y in fp32
+// (round to nearest), and the next chunk waits for that drain.  The tensor cores' fp32 accumulation truncates, so
+// a sum over all n points loses ~2^-25 of its value per accumulation step, always toward zero; chunks of T tiles
+// bound that loss by the steps in one chunk.
+template <int MODE, int DP, bool TWO, int COMP>
+__device__ __forceinline__ bool issue_item(Issuer& S, const SketchMma& Y, int njt, int g_bufs, int promote) {
   if (!issue_mma1<DP>(S, g_bufs)) return false;
   for (int jt = 0; jt < njt; ++jt) {
     if (jt + 1 < njt && !issue_mma1<DP>(S, g_bufs)) return false;
-    if (MODE == RBF_MODE_SKETCH && !issue_mma2<TWO>(S, Y, jt)) return false;
+    if (MODE == RBF_MODE_SKETCH) {
+      const int jc = promote ? jt % promote : jt;  // tile inside the accumulation chunk (0: fresh accumulator)
+      if (promote && jc == 0 && jt > 0) {
+        if (!issuer_wait(S, B_Y_EMPTY, (S.ydone - 1) & 1)) return false;
+        tc_fence_after();
+      }
+      if (!issue_mma2<TWO, COMP>(S, Y, jc)) return false;
+      if (promote && (jc == promote - 1 || jt == njt - 1)) {
+        if (elect_one()) umma_commit_pair(S.s_bar + 8u * (uint32_t)B_Y_FULL);
+        __syncwarp();
+        ++S.ydone;
+      }
+    }
   }
   return true;
 }
 
-template <int MODE, bool TWO>
-__device__ __forceinline__ bool issue_item_dp(Issuer& S, const SketchMma& Y, int nkc, int njt, int g_bufs) {
+template <int MODE, bool TWO, int COMP>
+__device__ __forceinline__ bool issue_item_dp(Issuer& S, const SketchMma& Y, int nkc, int njt, int g_bufs,
+                                              int promote) {
   switch (nkc) {
-    case 1: return issue_item<MODE, 32, TWO>(S, Y, njt, g_bufs);
-    case 2: return issue_item<MODE, 64, TWO>(S, Y, njt, g_bufs);
-    case 3: return issue_item<MODE, 96, TWO>(S, Y, njt, g_bufs);
-    default: return issue_item<MODE, 128, TWO>(S, Y, njt, g_bufs);
+    case 1: return issue_item<MODE, 32, TWO, COMP>(S, Y, njt, g_bufs, promote);
+    case 2: return issue_item<MODE, 64, TWO, COMP>(S, Y, njt, g_bufs, promote);
+    case 3: return issue_item<MODE, 96, TWO, COMP>(S, Y, njt, g_bufs, promote);
+    default: return issue_item<MODE, 128, TWO, COMP>(S, Y, njt, g_bufs, promote);
+  }
+}
+
+// Dispatch of one work item to the loop specialised for its panel split and sketch product (KBLOCK items and
+// compensated panels take one instruction).
+template <int MODE>
+__device__ __forceinline__ bool issue_item_any(Issuer& S, const SketchMma& Y, int nkc, int njt, int g_bufs, bool two,
+                                               int comp, int promote) {
+  if (MODE != RBF_MODE_SKETCH) return issue_item_dp<MODE, false, 0>(S, Y, nkc, njt, g_bufs, 0);
+  if (comp == 2) return issue_item_dp<MODE, false, 2>(S, Y, nkc, njt, g_bufs, promote);
+  if (comp == 1) return issue_item_dp<MODE, false, 1>(S, Y, nkc, njt, g_bufs, promote);
+  return two ? issue_item_dp<MODE, true, 0>(S, Y, nkc, njt, g_bufs, promote)
+             : issue_item_dp<MODE, false, 0>(S, Y, nkc, njt, g_bufs, promote);
+}
+
+// Drain of the sketch accumulator by one epilogue warp: its 32 rows (TMEM lanes from t_lane) x panel/4 columns,
+// 16 columns per TMEM load batch.  accumulate: add into Y with fire-and-forget fp32 reductions (red.global.add,
+// round to nearest, done in L2, so the drain never waits on a global load) instead of storing; every element has
+// one owner thread, whose first chunk stores and later chunks add, in program order.  Kept out of line: its
+// registers would otherwise stay reserved across the epilogue's exp loop.
+__device__ __noinline__ void drain_sketch_chunk(const TileInst* I, int item, uint32_t rank, int row, int qc,
+                                                uint32_t t_lane_base, bool accumulate) {
+  const int li = item - I->item_begin;
+  const int pn = li / I->n_itiles, m = I->m;
+  const int i = (li % I->n_itiles) * PAIR_M + (int)rank * BM + row;
+  float* const out_i = I->out + i;
+  const long long ldo = I->ldo;
+  const float y_i = (i < m && I->yi) ? I->yi[i] : 1.0f;
+  const int panel = I->panel, l = I->l;
+  const int quarter = panel / 4;  // panel is a multiple of 16
+  for (int cc = 0; cc < quarter; cc += 16) {
+    float yv[16];
+    const int nc = min(16, quarter - cc);  // a multiple of 4
+    const uint32_t ta = t_lane_base + I->tmem_y + qc * quarter + cc;
+#pragma unroll
+    for (int q4 = 0; q4 < 4; ++q4)
+      if (4 * q4 < nc) tmem_ld4(ta + 4 * q4, yv + 4 * q4);
+    tmem_wait_ld();
+    if (i < m) {
+      const int col0 = pn * panel + qc * quarter + cc;
+#pragma unroll
+      for (int e = 0; e < 16; ++e) {
+        if (e < nc && col0 + e < l) {
+          float* dst = out_i + (size_t)(col0 + e) * ldo;
+          if (accumulate) atomicAdd(dst, y_i * yv[e]);  // result unused: compiles to a reduction
+          else *dst = y_i * yv[e];
+        }
+      }
+    }
   }
 }
 
@@ -263,7 +349,7 @@ template <int MODE>
 __global__ void __launch_bounds__(NUM_THREADS, 1) rbf_tile_kernel(const __grid_constant__ LaunchArgs args) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  const SmemLayout L = make_layout(args.nkc_max, args.panel_max, args.nsx, args.nso);
+  const SmemLayout L = make_layout(args.nkc_max, args.panel_max, args.nsx, args.nso, args.om_mult);
   const int nsx = args.nsx, nso = args.nso;
   const uint32_t s_xi = smem_u32(smem + L.off_xi);
   const uint32_t s_xj = smem_u32(smem + L.off_xj);
@@ -354,6 +440,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1) rbf_tile_kernel(const __grid_c
             tma_load_2d_pair(s_xi + c * XI_CHUNK, t_xi, lbar(B_XI_FULL), c * KC, it * PAIR_M + (int)rank * BM);
         }
         const int n1 = I->n1, n2 = I->n2, panel = I->panel;
+        const int om_lo = (I->comp == 2) ? I->om_lo : -1;  // lo rows of Omega~ follow the hi rows in each stage
         for (int jt = 0; jt < njt && ok; ++jt) {
           if (points) {
             for (int c = 0; c < nkc; ++c) {
@@ -366,15 +453,18 @@ __global__ void __launch_bounds__(NUM_THREADS, 1) rbf_tile_kernel(const __grid_c
           } else if (MODE == RBF_MODE_SKETCH) {
             for (int c = 0; c < 2; ++c) {
               if (!mbar_wait(bar(OM_EMPTY + os), oph ^ 1, abort_flag)) { ok = false; break; }
-              if (leader) mbar_arrive_expect_tx(bar(OM_FULL + os), panel * 128);
+              if (leader) mbar_arrive_expect_tx(bar(OM_FULL + os), panel * 128 * (om_lo >= 0 ? 2 : 1));
               // rows of this CTA: [r*n1/2, (r+1)*n1/2) of the first instruction's n1 columns, then the same
-              // half of the second instruction's n2 columns
+              // half of the second instruction's n2 columns (or, compensated, of the lo rows)
               const uint32_t dst = s_om + os * L.om_stage;
               const int x = jt * BN + c * KC, y0 = pn * panel;
               tma_load_2d_pair(dst, t_om1, lbar(OM_FULL + os), x, y0 + (int)rank * (n1 / 2));
               if (n2 > 0)
                 tma_load_2d_pair(dst + (n1 / 2) * 128, t_om2, lbar(OM_FULL + os), x,
                                  y0 + n1 + (int)rank * (n2 / 2));
+              if (om_lo >= 0)
+                tma_load_2d_pair(dst + (n1 / 2) * 128, t_om1, lbar(OM_FULL + os), x,
+                                 om_lo + y0 + (int)rank * (n1 / 2));
               if (++os == (uint32_t)nso) { os = 0; oph ^= 1; }
             }
           }
@@ -416,6 +506,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1) rbf_tile_kernel(const __grid_c
       S.xs = S.xph = S.os = S.oph = S.pph = 0;
       S.guse0 = S.guse1 = 0;
       S.gnext = 0;
+      S.ydone = 0;
       uint32_t items_done = 0;
       bool ok = true;
       for (int item = cid; item < n_items && ok; item += ncl, ++items_done) {
@@ -428,23 +519,26 @@ __global__ void __launch_bounds__(NUM_THREADS, 1) rbf_tile_kernel(const __grid_c
         Y.idesc_y1 = idesc_f16(PAIR_M, n1, false);
         Y.idesc_y2 = idesc_f16(PAIR_M, two ? n2 : 16, false);
         Y.y2_boff = (uint32_t)((n1 / 2) * 128) >> 4;
+        Y.lo_boff = Y.y2_boff;  // compensated panels take one instruction: the lo rows sit where n2's would
+        const int comp = I->comp, promote = I->promote;
         Y.tmem_p = tmem_base + (uint32_t)I->tmem_p;
         Y.tmem_y = tmem_base + (uint32_t)I->tmem_y;
         Y.tmem_y2 = Y.tmem_y + (uint32_t)n1;
         if (!issuer_wait(S, B_XI_FULL, items_done & 1)) { ok = false; break; }
         tc_fence_after();
-        if (MODE == RBF_MODE_SKETCH && items_done > 0) {
+        if (MODE == RBF_MODE_SKETCH && S.ydone > 0) {
           // the previous item's Y (and P) columns may overlap this instance's G buffers: wait for the drain
-          if (!issuer_wait(S, B_Y_EMPTY, (items_done - 1) & 1)) { ok = false; break; }
+          if (!issuer_wait(S, B_Y_EMPTY, (S.ydone - 1) & 1)) { ok = false; break; }
           tc_fence_after();
         }
-        ok = two ? issue_item_dp<MODE, true>(S, Y, nkc, njt, g_bufs) : issue_item_dp<MODE, false>(S, Y, nkc, njt, g_bufs);
+        ok = issue_item_any<MODE>(S, Y, nkc, njt, g_bufs, two, comp, promote);
         if (!ok) break;
         if (elect_one()) {
           umma_commit_pair(bar(B_XI_EMPTY));
-          if (MODE == RBF_MODE_SKETCH) umma_commit_pair(bar(B_Y_FULL));
+          if (MODE == RBF_MODE_SKETCH && !promote) umma_commit_pair(bar(B_Y_FULL));
         }
         __syncwarp();
+        if (MODE == RBF_MODE_SKETCH && !promote) ++S.ydone;
       }
       if (!ok && lane == 0) give_up();
       // All MMAs issued by this warp must be complete before TMEM is released (in both CTAs).
@@ -466,7 +560,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1) rbf_tile_kernel(const __grid_c
     // for the next tile from global memory before the current tile's exp, and parks it here afterwards, so the
     // global latency never sits between a G tile and its P tile.
     float* sjbuf = reinterpret_cast<float*>(smem + L.off_sj) + ew * 2 * EPI_COLS;
-    uint32_t kp = 0, items_done = 0;
+    uint32_t kp = 0, items_done = 0, ydone = 0;  // ydone: Y accumulations drained (B_Y_FULL phases)
     uint32_t guse0 = 0, guse1 = 0, gnext = 0;  // the same G-buffer sequence as the MMA issuer
     bool ok = true;
     for (int item = cid; item < n_items && ok; item += ncl, ++items_done) {
@@ -474,7 +568,9 @@ __global__ void __launch_bounds__(NUM_THREADS, 1) rbf_tile_kernel(const __grid_c
       const int li = item - I->item_begin;
       const int it = li % I->n_itiles, pn = li / I->n_itiles;
       const int njt = I->n_jtiles, g_bufs = I->g_bufs, m = I->m;
-      const float c_row = I->c_row, c_dot = I->c_dot;
+      const bool p_lo = (I->comp >= 1);
+      const int promote = (MODE == RBF_MODE_SKETCH) ? I->promote : 0;
+      const float c_row = I->c_row;
       const float* sj = I->sj;
       const uint32_t t_p = tmem_base + t_lane + (uint32_t)I->tmem_p + (uint32_t)(qc * (EPI_COLS / 2));
       const long long ldo = I->ldo;
@@ -483,9 +579,20 @@ __global__ void __launch_bounds__(NUM_THREADS, 1) rbf_tile_kernel(const __grid_c
       const int i = it * PAIR_M + (int)rank * BM + row;
       float* const out_i = I->out + i;
       const float a_i = c_row * I->si[i];  // si is padded to n_itiles * PAIR_M
+      const float c_dot = I->c_dot * *I->fi * *I->fj;  // x_i.x_j = 2^-(e_I + e_J) G
       const float y_i = (i < m && I->yi) ? I->yi[i] : 1.0f;
       sjbuf[lane] = sj[qc * EPI_COLS + lane];  // tile 0 of this item
       __syncwarp();
+      auto drain = [&](bool accumulate) -> bool {
+        if (!__all_sync(0xffffffffu, mbar_wait(bar(B_Y_FULL), ydone & 1, abort_flag))) return false;
+        tc_fence_after();
+        drain_sketch_chunk(I, item, rank, row, qc, tmem_base + t_lane, accumulate);
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive_remote(lbar(B_Y_EMPTY));
+        ++ydone;
+        return true;
+      };
       for (int jt = 0; jt < njt; ++jt) {
         // sj is padded to n_jtiles * BN
         const float sj_next = (jt + 1 < njt) ? sj[(jt + 1) * BN + qc * EPI_COLS + lane] : 0.0f;
@@ -519,9 +626,16 @@ __global__ void __launch_bounds__(NUM_THREADS, 1) rbf_tile_kernel(const __grid_c
         sjbuf[((jt + 1) & 1) * EPI_COLS + lane] = sj_next;
         __syncwarp();
         if (MODE == RBF_MODE_SKETCH) {
-          uint32_t pk[EPI_COLS / 2];
+          // P_hi = fp16(P); with the compensated product also P_lo = fp16(P - P_hi), the exact residual of the hi
+          // rounding (|P_lo| <= 2^-12 P), written 64 TMEM columns after P_hi
+          uint32_t pk[EPI_COLS / 2], pl[EPI_COLS / 2];
 #pragma unroll
-          for (int c = 0; c < EPI_COLS / 2; ++c) pk[c] = pack_f16x2(v[2 * c], v[2 * c + 1]);
+          for (int c = 0; c < EPI_COLS / 2; ++c) {
+            const __half2 hh = __floats2half2_rn(v[2 * c], v[2 * c + 1]);
+            pk[c] = *reinterpret_cast<const uint32_t*>(&hh);
+            const float2 hf = __half22float2(hh);
+            pl[c] = pack_f16x2(v[2 * c] - hf.x, v[2 * c + 1] - hf.y);
+          }
           if (!__all_sync(0xffffffffu, mbar_wait(bar(B_P_EMPTY0 + h), (kp & 1) ^ 1, abort_flag))) {
             ok = false;
             break;
@@ -529,11 +643,16 @@ __global__ void __launch_bounds__(NUM_THREADS, 1) rbf_tile_kernel(const __grid_c
           tc_fence_after();
           // P row = this thread's row; j in [32qc, 32qc + 32) -> TMEM columns tmem_p + 16qc .. + 15
           tmem_st16(t_p, pk);
+          if (p_lo) tmem_st16(t_p + 64, pl);
           tmem_wait_st();
           tc_fence_before();
           __syncwarp();
           if (lane == 0) mbar_arrive_remote(lbar(B_P_FULL0 + h));
           ++kp;
+          if (promote && ((jt + 1) % promote == 0 || jt == njt - 1)) {
+            // this tile closed an accumulation chunk: add it into Y (the first chunk stores)
+            if (!drain(jt >= promote)) { ok = false; break; }
+          }
         } else {
           if (i < m) {
 #pragma unroll
@@ -548,26 +667,8 @@ __global__ void __launch_bounds__(NUM_THREADS, 1) rbf_tile_kernel(const __grid_c
         }
       }
       if (!ok) break;
-      if (MODE == RBF_MODE_SKETCH) {
-        if (!__all_sync(0xffffffffu, mbar_wait(bar(B_Y_FULL), items_done & 1, abort_flag))) { ok = false; break; }
-        tc_fence_after();
-        const int panel = I->panel, l = I->l;
-        const int quarter = panel / 4;  // panel is a multiple of 16
-        for (int cc = 0; cc < quarter; cc += 4) {
-          float yv[4];
-          tmem_ld4(tmem_base + t_lane + I->tmem_y + qc * quarter + cc, yv);
-          tmem_wait_ld();
-          if (i < m) {
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-              const int col = pn * panel + qc * quarter + cc + e;
-              if (col < l) out_i[(size_t)col * ldo] = y_i * yv[e];
-            }
-          }
-        }
-        tc_fence_before();
-        __syncwarp();
-        if (lane == 0) mbar_arrive_remote(lbar(B_Y_EMPTY));
+      if (MODE == RBF_MODE_SKETCH && !promote) {
+        if (!drain(false)) { ok = false; break; }
       }
     }
     if (!ok && lane == 0) give_up();
@@ -584,32 +685,76 @@ __global__ void __launch_bounds__(NUM_THREADS, 1) rbf_tile_kernel(const __grid_c
 }
 
 // ------------------------------------------------------------------ packing kernels
-__global__ void pack_points_kernel(const float* __restrict__ X, long long sp, long long sf, int n, int d, int dp,
-                                   int npad, __nv_bfloat16* __restrict__ Xp, float* __restrict__ norms) {
-  const int lane = threadIdx.x & 31;
-  const long long warps = (long long)gridDim.x * (blockDim.x / 32);
-  for (long long i = (long long)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32; i < npad; i += warps) {
-    float acc = 0.f;
-    __nv_bfloat16* row = Xp + i * (2 * dp);
-    for (int k = lane; k < dp; k += 32) {
-      const float x = (i < n && k < d) ? X[i * sp + (long long)k * sf] : 0.f;
-      const __nv_bfloat16 hi = __float2bfloat16_rn(x);
-      const __nv_bfloat16 lo = __float2bfloat16_rn(x - __bfloat162float(hi));
-      row[k] = hi;
-      row[dp + k] = lo;
-      // ||x||^2 from the same split products the distance MMA forms (hi.hi + 2 hi.lo), so that
-      // ||x||^2 + ||y||^2 - 2 x.y cancels to ~fp32 round-off for coincident points
-      const float h = __bfloat162float(hi), l = __bfloat162float(lo);
-      acc = fmaf(h, h, fmaf(2.0f * h, l, acc));
-    }
+// Largest |x_ik| of a point set (non-negative floats order like their bit patterns): block maxima, then one
+// atomicMax per block into *out, which the caller zeroes first.
+__global__ void absmax_points_kernel(const float* __restrict__ X, long long sp, long long sf, int n, int d,
+                                     unsigned* __restrict__ out) {
+  const long long total = (long long)n * d;
+  float mx = 0.f;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long i = e / d, k = e % d;
+    const float a = fabsf(X[i * sp + k * sf]);
+    if (a <= 3.0e38f) mx = fmaxf(mx, a);  // NaN and inf do not set the scale
+  }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if (lane == 0) norms[i] = acc;
+  for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  __shared__ float wmax[32];
+  if ((threadIdx.x & 31) == 0) wmax[threadIdx.x / 32] = mx;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    mx = (threadIdx.x < blockDim.x / 32) ? wmax[threadIdx.x] : 0.f;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (threadIdx.x == 0) atomicMax(out, __float_as_uint(mx));
   }
 }
 
+// One warp per point.  Every point of the set is scaled by the same 2^e, e = 14 - ceil(log2 max |x_ik|) (largest
+// |coordinate| in [2^13, 2^14)), and split into fp16 hi = fp16(2^e x), lo = fp16(2^e x - hi).  norms[i] =
+// ||x||^2 (0 on padding rows) and norms[npad + 1] = 2^-e; norms[npad] holds the set's max |x| bits from
+// absmax_points_kernel.  d <= dp <= 128, so each lane holds its (up to 4) coordinates in registers.
+__global__ void pack_points_kernel(const float* __restrict__ X, long long sp, long long sf, int n, int d, int dp,
+                                   int npad, __half* __restrict__ Xp, float* __restrict__ norms) {
+  const int lane = threadIdx.x & 31;
+  const long long warps = (long long)gridDim.x * (blockDim.x / 32);
+  const float mx = __uint_as_float(*reinterpret_cast<const unsigned*>(norms + npad));
+  int e = 0;
+  if (mx > 0.f) {
+    int ex = 0;
+    frexpf(mx, &ex);  // mx = f 2^ex, f in [0.5, 1)
+    e = min(max(14 - ex, -120), 120);
+  }
+  const float sc = ldexpf(1.0f, e);
+  if (blockIdx.x == 0 && threadIdx.x == 0) norms[npad + 1] = ldexpf(1.0f, -e);
+  for (long long i = (long long)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32; i < npad; i += warps) {
+    float acc = 0.f;
+    __half* row = Xp + i * (2 * dp);
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const int k = lane + 32 * t;
+      if (k < dp) {
+        const float x = ((i < n && k < d) ? X[i * sp + (long long)k * sf] : 0.f) * sc;  // exact: power of two
+        const __half hi = __float2half_rn(x);
+        const __half lo = __float2half_rn(x - __half2float(hi));
+        row[k] = hi;
+        row[dp + k] = lo;
+        // ||x||^2 from the same split products the distance MMA forms (hi.hi + 2 hi.lo), so that
+        // ||x||^2 + ||y||^2 - 2 x.y cancels to ~fp32 round-off for coincident points
+        const float h = __half2float(hi), l = __half2float(lo);
+        acc = fmaf(h, h, fmaf(2.0f * h, l, acc));
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) norms[i] = ldexpf(acc, -2 * e);
+  }
+}
+
+// Omega~^T rows in fp16: Op[c][j] = fp16(y_j Omega[j + c*ldo]) for c < lrows; with `comp`, rows lrows + c hold
+// the lo parts fp16(y_j Omega - hi).
 __global__ void pack_sketch_kernel(const float* __restrict__ Om, long long ldo, const float* __restrict__ yj, int n,
-                                   int l, int njpad, int lrows, __half* __restrict__ Op) {
+                                   int l, int njpad, int lrows, int comp, __half* __restrict__ Op) {
   const long long total = (long long)njpad * lrows;
   for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
        e += (long long)gridDim.x * blockDim.x) {
@@ -617,7 +762,9 @@ __global__ void pack_sketch_kernel(const float* __restrict__ Om, long long ldo, 
     const int c = (int)(e / njpad);
     float v = 0.f;
     if (j < n && c < l) v = Om[j + (long long)c * ldo] * (yj ? yj[j] : 1.0f);
-    Op[e] = __float2half_rn(v);
+    const __half hi = __float2half_rn(v);
+    Op[e] = hi;
+    if (comp) Op[total + e] = __float2half_rn(v - __half2float(hi));
   }
 }
 
@@ -698,15 +845,19 @@ cudaError_t launch_kernel(const LaunchArgs& a, size_t smem, int clusters, cudaSt
 int feature_pad(int d) { return round_up(d < 1 ? 1 : d, 32); }
 
 // Sketch panels: with one 128-column G buffer, P (64 columns) and Y fit a panel of up to 320 columns; with two
-// G buffers, up to 192.  Take whichever needs fewer panels (ties: two G buffers, which overlap better).
-SketchPlan plan_sketch(int l) {
+// G buffers, up to 192.  Take whichever needs fewer panels (ties: two G buffers, which overlap better).  The
+// compensated product (comp >= 1) keeps P_lo beside P (128 columns): panels of up to 256 / 128 columns.
+SketchPlan plan_sketch(int l, int comp) {
   SketchPlan p;
+  const int pcols = comp ? 128 : 64;
+  const int w1 = TMEM_COLS - 128 - pcols, w2 = TMEM_COLS - 256 - pcols;
   const int lpad = round_up(l < 1 ? 1 : l, 16);
-  const int np1 = (lpad + 319) / 320, np2 = (lpad + 191) / 192;
+  const int np1 = (lpad + w1 - 1) / w1, np2 = (lpad + w2 - 1) / w2;
   p.g_bufs = (np2 <= np1) ? 2 : 1;
   p.n_panels = (p.g_bufs == 2) ? np2 : np1;
   p.panel = round_up((lpad + p.n_panels - 1) / p.n_panels, 16);
   p.lrows = p.n_panels * p.panel;
+  p.comp = comp;
   return p;
 }
 
@@ -714,23 +865,32 @@ int pack_points(db200_context* ctx, const float* X, int ldx, int layout, int n, 
                 float* norms) {
   const long long sp = (layout == DB200_POINT_MAJOR) ? ldx : 1;
   const long long sf = (layout == DB200_POINT_MAJOR) ? 1 : ldx;
+  unsigned* mx = reinterpret_cast<unsigned*>(norms + npad);
+  DB200_CUDA(ctx, cudaMemsetAsync(mx, 0, sizeof(unsigned), ctx->stream));
+  if (n > 0) {
+    long long mblocks = ((long long)n * d + 255) / 256;
+    if (mblocks > (long long)ctx->num_sms * 4) mblocks = (long long)ctx->num_sms * 4;
+    absmax_points_kernel<<<(unsigned)mblocks, 256, 0, ctx->stream>>>(X, sp, sf, n, d, mx);
+    DB200_CUDA(ctx, cudaGetLastError());
+    count_launch(ctx);
+  }
   const int threads = 256;
   long long blocks = ((long long)npad * 32 + threads - 1) / threads;
   if (blocks > 65535LL * 4) blocks = 65535LL * 4;
   pack_points_kernel<<<(unsigned)blocks, threads, 0, ctx->stream>>>(X, sp, sf, n, d, dp, npad,
-                                                                    static_cast<__nv_bfloat16*>(xp), norms);
+                                                                    static_cast<__half*>(xp), norms);
   DB200_CUDA(ctx, cudaGetLastError());
   count_launch(ctx);
   return DB200_OK;
 }
 
 int pack_sketch(db200_context* ctx, const float* Omega, int ldo, const float* yj, int n, int l, int njpad, int lrows,
-                void* op) {
+                void* op, int comp) {
   const long long total = (long long)njpad * lrows;
   long long blocks = (total + 255) / 256;
   if (blocks > (long long)ctx->num_sms * 32) blocks = (long long)ctx->num_sms * 32;
   pack_sketch_kernel<<<(unsigned)blocks, 256, 0, ctx->stream>>>(Omega, ldo, yj, n, l, njpad, lrows,
-                                                                static_cast<__half*>(op));
+                                                                comp == 2 ? 1 : 0, static_cast<__half*>(op));
   DB200_CUDA(ctx, cudaGetLastError());
   count_launch(ctx);
   return DB200_OK;
@@ -742,7 +902,7 @@ int prepare_rbf_tiles(db200_context* ctx, int mode, const TileJob* jobs, int cou
                       size_t table_capacity, TilePlan* plan) {
   if (count < 1 || !jobs || !plan) return fail(ctx, DB200_ERR_INVALID, "rbf tiles: empty job list");
   std::vector<TileInst> host((size_t)count);
-  int items = 0, nkc_max = 1, panel_max = 16;
+  int items = 0, nkc_max = 1, panel_max = 16, om_mult = 1;
   for (int b = 0; b < count; ++b) {
     const TileJob& J = jobs[b];
     const PackedPoints &pi = J.pi, &pj = J.pj;
@@ -750,9 +910,12 @@ int prepare_rbf_tiles(db200_context* ctx, int mode, const TileJob* jobs, int cou
       return fail(ctx, DB200_ERR_UNSUPPORTED, "rbf tiles: padded feature count not in {32, 64, 96, 128}");
     if (pi.npad % PAIR_M || pj.npad % BN) return fail(ctx, DB200_ERR_INVALID, "rbf tiles: unpadded operands");
     const SketchPlan& P = J.plan;
+    const int pcols = P.comp ? 128 : 64;  // P (and P_lo) columns of tensor memory
     if (mode == RBF_MODE_SKETCH && (P.panel % 16 || P.panel > 320 || P.panel < 16 || P.n_panels < 1 ||
-                                    (P.g_bufs != 1 && P.g_bufs != 2) || P.panel + 64 + 128 * P.g_bufs > TMEM_COLS ||
-                                    P.n_panels * P.panel < J.l || P.lrows < P.n_panels * P.panel))
+                                    (P.g_bufs != 1 && P.g_bufs != 2) || P.panel + pcols + 128 * P.g_bufs > TMEM_COLS ||
+                                    P.n_panels * P.panel < J.l || P.lrows < P.n_panels * P.panel ||
+                                    P.comp < 0 || P.comp > 2 || (P.comp && P.panel > 256) || P.promote < 0 ||
+                                    (P.comp == 2 && J.om_lo < P.lrows)))
       return fail(ctx, DB200_ERR_INVALID, "rbf tiles: bad sketch panel plan");
     TileInst& I = host[(size_t)b];
     std::memset(&I, 0, sizeof(I));
@@ -766,14 +929,20 @@ int prepare_rbf_tiles(db200_context* ctx, int mode, const TileJob* jobs, int cou
       // of the pair holds half of every instruction's B rows, loaded as one TMA box per instruction
       I.n1 = P.panel > 256 ? (P.panel / 32) * 16 : P.panel;
       I.n2 = P.panel - I.n1;
-      if (!make_tmap(&I.tm_om1, J.op, pj.npad, P.lrows, pj.npad, I.n1 / 2, CU_TENSOR_MAP_DATA_TYPE_FLOAT16) ||
+      // compensated (comp = 2): the lo rows of this job's panel columns start om_lo rows after its hi rows
+      const int om_rows = (P.comp == 2) ? J.om_lo + P.lrows : P.lrows;
+      if (!make_tmap(&I.tm_om1, J.op, pj.npad, om_rows, pj.npad, I.n1 / 2, CU_TENSOR_MAP_DATA_TYPE_FLOAT16) ||
           (I.n2 > 0 &&
-           !make_tmap(&I.tm_om2, J.op, pj.npad, P.lrows, pj.npad, I.n2 / 2, CU_TENSOR_MAP_DATA_TYPE_FLOAT16)))
+           !make_tmap(&I.tm_om2, J.op, pj.npad, om_rows, pj.npad, I.n2 / 2, CU_TENSOR_MAP_DATA_TYPE_FLOAT16)))
         return fail(ctx, DB200_ERR_CUDA, "cuTensorMapEncodeTiled failed for the sketch operand");
       if (I.n2 == 0) I.tm_om2 = I.tm_om1;  // unused
       I.g_bufs = P.g_bufs;
       I.tmem_p = 128 * P.g_bufs;
-      I.tmem_y = I.tmem_p + 64;
+      I.tmem_y = I.tmem_p + pcols;
+      I.comp = P.comp;
+      I.om_lo = (P.comp == 2) ? J.om_lo : 0;
+      I.promote = P.promote;
+      om_mult = std::max(om_mult, P.comp == 2 ? 2 : 1);
     } else {
       I.tm_om1 = I.tm_om2 = I.tm_xj;  // unused
       I.n_panels = 1;
@@ -794,6 +963,8 @@ int prepare_rbf_tiles(db200_context* ctx, int mode, const TileJob* jobs, int cou
     I.c_dot = 2.0f * J.gamma * LOG2E;
     I.si = pi.norms;
     I.sj = pj.norms;
+    I.fi = pi.norms + pi.npad + 1;  // the pack writes the set's scale after the norms and the max |x|
+    I.fj = pj.norms + pj.npad + 1;
     I.yi = J.yi;
     I.yj = J.yj;
     I.out = J.out;
@@ -810,15 +981,16 @@ int prepare_rbf_tiles(db200_context* ctx, int mode, const TileJob* jobs, int cou
   T.nkc_max = nkc_max;
   T.panel_max = panel_max;
   T.nso = (mode == RBF_MODE_SKETCH) ? MAX_NSO : 0;
+  T.om_mult = om_mult;
   {  // the Xj ring takes whatever shared memory is left
-    const SmemLayout L0 = make_layout(nkc_max, panel_max, 0, T.nso);
+    const SmemLayout L0 = make_layout(nkc_max, panel_max, 0, T.nso, om_mult);
     const long long left = (long long)SMEM_LIMIT - 1024 - (long long)L0.total;
     int nsx = (int)(left / XJ_CHUNK);
     if (nsx > MAX_NSX) nsx = MAX_NSX;
     if (nsx < 2) return fail(ctx, DB200_ERR_UNSUPPORTED, "rbf tiles: shared memory plan does not fit");
     T.nsx = nsx;
   }
-  T.smem = make_layout(nkc_max, panel_max, T.nsx, T.nso).total + 1024;
+  T.smem = make_layout(nkc_max, panel_max, T.nsx, T.nso, om_mult).total + 1024;
   {
     const int max_clusters = ctx->num_sms / 2;
     cudaError_t e = (mode == RBF_MODE_SKETCH) ? plan_clusters<RBF_MODE_SKETCH>(T.smem, max_clusters, items, &T.clusters)
@@ -857,6 +1029,7 @@ int launch_rbf_plan(db200_context* ctx, const TilePlan& T) {
   a.n_items = T.n_items;
   a.nsx = T.nsx;
   a.nso = T.nso;
+  a.om_mult = T.om_mult;
   a.nkc_max = T.nkc_max;
   a.panel_max = T.panel_max;
   a.status = ctx->d_status;
@@ -880,6 +1053,7 @@ int launch_rbf_tiles(db200_context* ctx, int mode, const PackedPoints& pi, const
   J.yj = yj;
   J.op = op;
   J.plan = plan;
+  J.om_lo = plan.lrows;  // a compensated Omega~ packs its lo rows after all hi rows
   J.l = l;
   J.gamma = gamma;
   J.out = out;
@@ -890,36 +1064,53 @@ int launch_rbf_tiles(db200_context* ctx, int mode, const PackedPoints& pi, const
   return launch_rbf_plan(ctx, T);
 }
 
-// A sketch wider than one panel as one launch over per-panel instances of exact widths: the padded width
-// roundup(l, 16) split into plan.n_panels panels of multiples of 16 that differ by at most 16 columns (528 =
-// 272 + 256 instead of 2 x 272), so no panel computes sketch columns past l beyond the last multiple of 16.
-int launch_rbf_sketch_exact(db200_context* ctx, const PackedPoints& pi, const PackedPoints& pj, const float* yi,
-                            const void* op, const SketchPlan& plan, int l, float gamma, float* out, int ldo) {
-  if (plan.n_panels <= 1)
-    return launch_rbf_tiles(ctx, RBF_MODE_SKETCH, pi, pj, yi, nullptr, op, plan, l, gamma, out, ldo);
-  const int units = (l + 15) / 16, np = plan.n_panels;
-  std::vector<TileJob> jobs((size_t)np);
+// A sketch wider than one panel as per-panel instances of exact widths: the padded width roundup(l, 16) split into
+// plan.n_panels panels of multiples of 16 that differ by at most 16 columns (528 = 272 + 256 instead of 2 x 272),
+// so no panel computes sketch columns past l beyond the last multiple of 16.  `base` carries the points, labels,
+// packed Omega~ (plan.lrows hi rows, then as many lo rows when compensated) and the output.
+void exact_panel_jobs(const TileJob& base, std::vector<TileJob>& out) {
+  const SketchPlan& plan = base.plan;
+  if (plan.n_panels <= 1) {
+    TileJob J = base;
+    J.om_lo = plan.lrows;
+    out.push_back(J);
+    return;
+  }
+  const int l = base.l, units = (l + 15) / 16, np = plan.n_panels;
   int off = 0;
   for (int p = 0; p < np; ++p) {
     const int w = 16 * (units / np + (p < units % np ? 1 : 0));
-    TileJob& J = jobs[(size_t)p];
-    J.pi = pi;
-    J.pj = pj;
-    J.yi = yi;
-    J.yj = nullptr;
-    J.op = static_cast<const uint16_t*>(op) + (size_t)off * pj.npad;  // packed rows = sketch columns
+    TileJob J = base;
+    J.op = static_cast<const uint16_t*>(base.op) + (size_t)off * base.pj.npad;  // packed rows = sketch columns
     J.plan.n_panels = 1;
     J.plan.panel = w;
     J.plan.lrows = w;
-    J.plan.g_bufs = (w + 64 + 2 * 128 <= TMEM_COLS) ? 2 : 1;
+    J.plan.g_bufs = (w + (plan.comp ? 128 : 64) + 2 * 128 <= TMEM_COLS) ? 2 : 1;
+    J.om_lo = plan.lrows;  // lo rows of the whole packed operand follow its plan.lrows hi rows
     J.l = std::min(w, l - off);
-    J.gamma = gamma;
-    J.out = out + (size_t)off * ldo;
-    J.ldo = ldo;
+    J.out = base.out + (size_t)off * base.ldo;
+    out.push_back(J);
     off += w;
   }
+}
+
+int launch_rbf_sketch_exact(db200_context* ctx, const PackedPoints& pi, const PackedPoints& pj, const float* yi,
+                            const void* op, const SketchPlan& plan, int l, float gamma, float* out, int ldo) {
+  TileJob base;
+  base.pi = pi;
+  base.pj = pj;
+  base.yi = yi;
+  base.yj = nullptr;  // folded into the packed Omega~
+  base.op = op;
+  base.plan = plan;
+  base.l = l;
+  base.gamma = gamma;
+  base.out = out;
+  base.ldo = ldo;
+  std::vector<TileJob> jobs;
+  exact_panel_jobs(base, jobs);
   TilePlan T;
-  int st = prepare_rbf_tiles(ctx, RBF_MODE_SKETCH, jobs.data(), np, nullptr, 0, &T);
+  int st = prepare_rbf_tiles(ctx, RBF_MODE_SKETCH, jobs.data(), (int)jobs.size(), nullptr, 0, &T);
   if (st) return st;
   return launch_rbf_plan(ctx, T);
 }

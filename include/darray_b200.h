@@ -83,21 +83,51 @@ DB200_API int db200_selftest_grid_barrier_timeout(db200_context* ctx, int limit_
 DB200_API int db200_profile(db200_context* ctx, int enable);
 DB200_API int db200_profile_read(db200_context* ctx, double* total_ms, int64_t* count);
 
+/* Measured FP64 throughput of this GPU in TFLOP/s: back-to-back mma.sync.m16n8k8.f64 (the FP64 tensor-core tiles
+ * of the FP64 kernels) and back-to-back FP64 FMAs, operands in registers, 32 warps per SM, timed with CUDA events
+ * (~60 ms).  The denominator of the FP64 kernels' roofline fractions.  Synchronous. */
+DB200_API int db200_probe_fp64_peak(db200_context* ctx, double* dmma_tflops, double* dfma_tflops);
+
 /*
  * Fused RBF kernel x sketch (device pointers):
  *     Y(m x l) = diag(yi) * K(Xi, Xj) * diag(yj) * Omega,   K(a,b) = exp(-gamma * ||x_a - x_b||^2)
- * The kernel block K is never stored: squared distances come from split-bf16 tensor-core products
- * (||x||^2 + ||y||^2 - 2 x.y), exp is applied in the epilogue and the bf16 tile feeds the sketch product,
- * accumulated in fp32.  Replaces rbf_kernel (include/dkernel.cu:132) followed by tc_gemm
- * (include/dkernel.cu:194) inside DArray::LRA (include/dkernel.h:13-46), for the whole n x n matrix.
+ * The kernel block K is never stored: squared distances come from split-fp16 tensor-core products on points
+ * scaled by powers of two (||x||^2 + ||y||^2 - 2 x.y, 22 significant bits per coordinate), exp is applied in the
+ * epilogue and the fp16 tile feeds the sketch product, accumulated in fp32.  Replaces rbf_kernel
+ * (include/dkernel.cu:132) followed by tc_gemm (include/dkernel.cu:194) inside DArray::LRA
+ * (include/dkernel.h:13-46), for the whole n x n matrix.
  *   Xi, Xj : points in `x_layout` (DB200_POINT_MAJOR or DB200_FEATURE_MAJOR) with leading dims ldxi/ldxj
  *   yi, yj : labels of length m and n (NULL means all ones)
  *   Omega  : n x l column major (ldo >= n);  Y : m x l column major (ldy >= m)
- * Supports d <= 128.
+ * Supports d <= 128.  The sketch product is the single fp16 product (DB200_SKETCH_SINGLE below).
  */
 DB200_API int db200_rbf_sketch(db200_context* ctx, int m, int n, int d, int l, const float* Xi, int ldxi, const float* Xj,
                      int ldxj, int x_layout, const float* yi, const float* yj, const float* Omega, int ldo, float* Y,
                      int ldy, float gamma);
+
+/* Sketch products of db200_rbf_sketch_ex.
+ * DB200_SKETCH_SINGLE: P . Omega~ with both in fp16 (11 significant bits each), fp32 accumulation.  Relative
+ *   error of Y ~3e-4.
+ * DB200_SKETCH_P_SPLIT: adds P_lo . Omega~, P_lo = fp16(P - fp16(P)), so the kernel values carry ~22 bits.
+ * DB200_SKETCH_COMPENSATED: adds P_hi . Omega~_lo as well (Omega~ also hi + lo): ~22-bit operands, ~2x the tensor
+ *   work of DB200_SKETCH_SINGLE at l = 528.  What remains is the tensor cores' fp32 accumulation, which truncates
+ *   toward zero: a sum over n points shrinks by ~2^-25 per accumulation step (1e-5 to 3e-5 relative at n = 4096 -
+ *   8192).  The range finder of an SVM solve needs this product to match the FP64 path's dual objective to 1e-6:
+ *   the single product's rounding of P shifts the sketched subspace enough to move the objective by ~4e-4 at
+ *   n = 131072; the shrink does not matter there (the subspace is scale free).
+ * DB200_SKETCH_COMPENSATED_PROMOTED: the compensated product with the accumulator restarted every 256 points j and
+ *   each chunk added into Y in fp32 with round-to-nearest, so the shrink is that of one chunk (~1e-6 relative).
+ *   The kernel passes of the mixed SVM path use it: at n = 131072 the dual objective then lies 2.5e-7 from the
+ *   FP64 path's (3.1e-6 with only the final pass promoted, whose Y scales the core C = Q^T K Q). */
+#define DB200_SKETCH_SINGLE 0
+#define DB200_SKETCH_P_SPLIT 1
+#define DB200_SKETCH_COMPENSATED 2
+#define DB200_SKETCH_COMPENSATED_PROMOTED 3
+
+/* db200_rbf_sketch with a choice of sketch product (DB200_SKETCH_*).  Same arguments and layout otherwise. */
+DB200_API int db200_rbf_sketch_ex(db200_context* ctx, int m, int n, int d, int l, const float* Xi, int ldxi,
+                                  const float* Xj, int ldxj, int x_layout, const float* yi, const float* yj,
+                                  const float* Omega, int ldo, float* Y, int ldy, float gamma, int product);
 
 /*
  * Materialised RBF block (device pointers):  K(m x n) = diag(yi) * exp(-gamma * D2(Xi, Xj)) * diag(yj),
@@ -163,15 +193,20 @@ typedef struct db200_barrier_params {
 } db200_barrier_params;
 
 /* Precision of the path.
- * DB200_MIXED: kernel passes on the tensor cores in split bf16 (fp32 accumulation); the Woodbury capacity matrix
+ * DB200_MIXED: kernel passes on the tensor cores, distances in split fp16 and the compensated sketch product with
+ *   promoted fp32 accumulation (DB200_SKETCH_COMPENSATED_PROMOTED), which keeps the dual objective within ~3e-7
+ *   of the FP64 path's; the Woodbury capacity matrix
  *   I + Z^T D^-1 Z formed in integers on the int8 tensor cores from 8 signed 7-bit slices of every column (Ozaki
  *   scheme, error ~3e-14 of the column norms; from r = 2048 first 6 slices, ~3e-10, while refinement converges
  *   with them) and factored in FP64 while each Newton step refined
  *   against the exact FP64 operator (Z Z^T + D) reaches relative residual 1e-10, the FP64 capacity matrix after;
  *   objective, gradients, gap and line search in FP64.
- * DB200_FP64: plain FP64 everywhere (FP64 kernel blocks and products, FP64 capacity matrix): the comparator. */
+ * DB200_FP64: plain FP64 everywhere (FP64 kernel blocks and products, FP64 capacity matrix): the comparator.
+ * DB200_MIXED_FAST: DB200_MIXED with the single fp16 sketch product (DB200_SKETCH_SINGLE) in the kernel passes:
+ *   half the tensor work of the compensated passes, dual objective ~4e-4 from the FP64 path's at n = 131072. */
 #define DB200_MIXED 0
 #define DB200_FP64 1
+#define DB200_MIXED_FAST 2
 
 /* What a solve did and where it ended. */
 typedef struct db200_svm_report {
@@ -267,11 +302,18 @@ DB200_API int db200_gram_weighted(db200_context* ctx, int n, int r, const double
 
 /* Plain FP64 kernel x sketch (device pointers), the comparator of db200_rbf_sketch:
  *     Y(m x l, FP64) = diag(yi) K(Xi, Xj) diag(yj) Omega(n x l, FP64)
- * with FP64 distances, exp and products on the FP64 pipes (row blocks of K are materialised in FP64).
- * Xi, Xj point-major float (ldxi, ldxj >= d).  Stream-ordered. */
+ * with FP64 norms, distances, exp and products in one fused launch on the FP64 tensor cores
+ * (mma.sync.m16n8k8.f64): each CTA keeps 64 rows of Xi in shared memory and streams the points j, so K is never
+ * stored.  Xi, Xj point-major float (ldxi, ldxj >= d), d <= 256.  Stream-ordered. */
 DB200_API int db200_rbf_sketch_f64(db200_context* ctx, int m, int n, int d, int l, const float* Xi, int ldxi,
                                    const float* Xj, int ldxj, const float* yi, const float* yj, const double* Omega,
                                    int ldo, double* Y, int ldy, double gamma);
+
+/* Materialised FP64 RBF block K(m x n) = diag(yi) exp(-gamma D2(Xi, Xj)) diag(yj), column major (ldk >= m):
+ * FP64 norms, an FP64 tensor-core Gram for the cross term, FP64 exp.  The FP64 counterpart of db200_rbf_block
+ * (include/dkernel.cu:132-190).  Xi, Xj point-major float.  Stream-ordered. */
+DB200_API int db200_rbf_block_f64(db200_context* ctx, int m, int n, int d, const float* Xi, int ldxi, const float* Xj,
+                                  int ldxj, const float* yi, const float* yj, double* K, int ldk, double gamma);
 
 /* y = alpha x + beta y + gamma elementwise on n FP64 device values (x may be NULL): the vector updates of
  * include/dbarrier.h:60-73 (Grad = Grad_f + Grad_Phi) and of the D + n I shift of pre_conjgrad. */
@@ -298,10 +340,13 @@ DB200_API int db200_barrier_terms(db200_context* ctx, int n, int k, const double
  * allocating routine.  Requests whose scratch would exceed the array return DB200_ERR_TOO_LARGE (with a message
  * on stderr naming the bytes needed).  The scratch need is about
  *     (m + n) * (4 * roundup(d, 32) + 4) + 2 * n * roundup(l, 16)   bytes   (the n term once when Xi == Xj).
- * The first call on each device resolves the array's device address (cudaGetSymbolAddress, with that device
- * current); make that first call before any stream capture.  All calls share the one array and it keeps the
- * previous call's contents (every byte a call reads is written by that call first); calls that overlap on the
- * GPU -- from two host threads, or on two streams -- race on it and must be serialised by the caller.
+ * Every call resolves the array's device address in the current context (cudaGetSymbolAddress, with the
+ * stream's device current), so the address is never stale after a device reset or in a caller's own context;
+ * the first call on a device also loads the library's device code into that context, so make the first call
+ * before any stream capture begins.  n = 0 writes Y = 0, as db200_rbf_sketch does.  All calls share the one
+ * array and it keeps the previous call's contents (every byte a call reads is written by that call first);
+ * calls that overlap on the GPU -- from two host threads, or on two streams -- race on it and must be serialised
+ * by the caller.
  */
 #define DB200_NOALLOC_SCRATCH_BYTES (32u << 20)
 DB200_API int db200_rbf_sketch_noalloc(void* stream, int m, int n, int d, int l, const float* Xi, int ldxi,
@@ -426,6 +471,12 @@ DB200_API int db200_select_topk(db200_context* ctx, int n, const float* keys, in
  * Z = C R^-1 (n x r FP64), so diag(y) K diag(y) ~ Z Z^T.  nu_out: host, may be NULL.  Synchronous. */
 DB200_API int db200_landmark_factor(db200_context* ctx, int n, int d, const float* X, int ldx, const float* y,
                                     float gamma, int r, const int* idx, double* Z, int ldz, double* nu_out);
+/* db200_landmark_factor with C = diag(y) K(:, L) diag(y_L) in a chosen precision: DB200_MIXED (or
+ * DB200_MIXED_FAST): the tcgen05 tile engine's fp32 kernel block; DB200_FP64: the FP64 kernel block
+ * (db200_rbf_block_f64), the comparator.  Synchronous. */
+DB200_API int db200_landmark_factor_ex(db200_context* ctx, int n, int d, const float* X, int ldx, const float* y,
+                                       float gamma, int r, const int* idx, double* Z, int ldz, double* nu_out,
+                                       int precision);
 
 /* Sampled residual ||Q(:, S) - Z Z(S, :)^T||_F / ||Q(:, S)||_F with Q = diag(y) K diag(y) over s columns S
  * (indices): an estimate of ||Q - Z Z^T||_F / ||Q||_F.  est: host.  Synchronous. */
@@ -441,10 +492,18 @@ typedef struct {
   double ms_features, ms_predict, ms_select, ms_factor, ms_residual, ms_fallback;
 } db200_landmark_report;
 
+/* The landmark selection of db200_svm_solve_landmarks on its own: features (8-NN distance over s_knn reference
+ * points drawn with `seed`) -> MLP log-leverage -> Gumbel keys (`seed`) -> the r largest, written to idx (device,
+ * r ints).  The same seed gives the same landmarks as the solve.  Synchronous. */
+DB200_API int db200_select_landmarks(db200_context* ctx, int n, int d, int r, const float* X, int ldx,
+                                     const db200_mlp* net, unsigned long long seed, int s_knn, int* idx);
+
 /* Learned-landmark SVM solve: features (8-NN distance over s_knn reference points) -> MLP log-leverage ->
  * Gumbel top-r landmarks -> Nystrom factor -> sampled residual estimate (s_res columns); if the estimate exceeds
  * tol the Gaussian pipeline db200_lowrank(l_fb = Omega's columns, q) builds the factor instead; then the barrier
- * (db200_svm_barrier) on the factor.  Z: n x max(r, l_fb) FP64, a: n.  Synchronous. */
+ * (db200_svm_barrier) on the factor.  The landmark columns K(:, L) (n r d work, r / n of one kernel pass) are FP64
+ * (db200_landmark_factor_ex with DB200_FP64) unless params->precision is DB200_MIXED_FAST, which takes the tile
+ * engine's fp32 block.  Z: n x max(r, l_fb) FP64, a: n.  Synchronous. */
 DB200_API int db200_svm_solve_landmarks(db200_context* ctx, int n, int d, int r, const float* X, int ldx,
                                         const float* y, float gamma, double C, const db200_mlp* net,
                                         unsigned long long seed, int s_knn, int s_res, double tol,

@@ -6,6 +6,7 @@ import numpy as np
 import pytest
 
 from oracle import landmarks as LO
+from oracle import oracle as O
 from tests.util import dev, ptr, rel_fro
 
 pytestmark = pytest.mark.gpu
@@ -159,3 +160,30 @@ def test_svm_solve_landmarks_end_to_end(gpu_ctx, tol, expect_fallback):
     assert rep.gap_barrier < 1e-6 and rep.gap_primal_dual < 1e-6  # both relative to |f|
     av = a.cpu().numpy()
     assert np.all(av >= 0) and np.all(av <= w.C)
+
+
+def test_svm_solve_landmarks_matches_oracle_on_same_landmarks(gpu_ctx):
+    """The learned-landmark solve against the FP64 oracle's Nystrom solve on the same landmarks
+    (oracle/landmarks.py: landmark_factor, then the oracle barrier): the landmarks come from
+    db200_select_landmarks with the solve's seed; dual objective within the north star's 1e-6."""
+    import torch
+    from darray_optimizer_b200._lib import Mlp
+    w = _mixture(8192, 14)
+    n, d, r = 8192, 64, 512
+    net = Mlp(gpu_ctx, d + 2, 256, 3, seed=3)
+    dX, dy = dev(w.X), dev(w.y)
+    idx = torch.zeros(r, dtype=torch.int32, device="cuda")
+    gpu_ctx.select_landmarks(n, d, r, ptr(dX), d, net, 91, 2048, ptr(idx))
+    a = torch.zeros(n, dtype=torch.float64, device="cuda")
+    Z = torch.zeros((r, n), dtype=torch.float64, device="cuda")
+    rep, lrep = gpu_ctx.svm_solve_landmarks(n, d, r, ptr(dX), d, ptr(dy), w.gamma, w.C, net, 91, 2048, 256, 1e9,
+                                            0, n, 0, 1, ptr(a), ptr(Z), n)
+    assert lrep.used_fallback == 0
+    L = np.sort(idx.cpu().numpy())
+    assert len(np.unique(L)) == r
+    Zr, _ = LO.landmark_factor(w.X, w.y, w.gamma, L)
+    ref = O.svm_barrier(Zr, w.y, w.C)
+    rel = abs(rep.f - ref.f) / abs(ref.f)
+    print(f"learned landmarks: |f - f_oracle|/|f_oracle| = {rel:.3e}")
+    assert rel <= 1e-6
+    assert rep.gap_primal_dual < 1e-6

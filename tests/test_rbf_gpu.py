@@ -1,10 +1,13 @@
 """Parity of the tcgen05 RBF tile engine (through the C ABI) against the FP64 oracle.
 
 Tolerances (stated here, checked below):
-  * db200_rbf_block: |K_gpu - K_oracle| <= 2e-5 elementwise.  Distances come from split-bf16 products
-    (relative error ~2^-16 of |x||y|), exp2 and norms in fp32.
-  * db200_rbf_sketch: ||Y_gpu - Y_oracle||_F <= 1e-2 ||Y_oracle||_F.  The kernel tile P and Omega enter the
-    sketch product as bf16 (relative rounding 2^-9 each) with fp32 accumulation.
+  * db200_rbf_block: |K_gpu - K_oracle| <= 2e-5 elementwise.  Distances come from split-fp16 products of points
+    scaled by a power of two (22 significant bits per coordinate), exp2 and norms in fp32.
+  * db200_rbf_sketch: ||Y_gpu - Y_oracle||_F <= 2e-3 ||Y_oracle||_F.  The kernel tile P and Omega enter the
+    sketch product as fp16 (relative rounding 2^-12 each) with fp32 accumulation (measured ~3e-4).
+  * db200_rbf_sketch_ex: compensated product (P and Omega each as fp16 hi + lo) <= 6e-5 relative Frobenius (the
+    tensor cores' truncating fp32 accumulation over n points); with the accumulation promoted every 256 points
+    <= 3e-6; P split only <= 4e-4.
 """
 import numpy as np
 import pytest
@@ -106,6 +109,45 @@ def test_rbf_sketch_matches_oracle(gpu_ctx, m, n, d, l):
     assert col <= 6e-3, col
 
 
+@pytest.mark.parametrize("m,n,d,l,seed", [
+    (256, 256, 32, 16, 1),
+    (1000, 1000, 20, 40, 2),
+    (300, 777, 128, 200, 3),
+    (512, 512, 64, 528, 4),     # three compensated panels
+    (4096, 4096, 32, 138, 5),   # the two-Gaussian workload's sketch width
+    (700, 900, 100, 600, 6),
+    (300, 257, 7, 1040, 7),
+])
+def test_rbf_sketch_compensated_matches_oracle(gpu_ctx, m, n, d, l, seed):
+    """The compensated sketch product (fp16 hi + lo for both P and Omega) against the FP64 oracle: 22-bit
+    operands, so the error falls from ~3e-4 (single product) to the fp32 accumulation and exp2 level."""
+    from darray_optimizer_b200 import _lib
+    Xi = _points(m, d, 20 + seed, 0.5)
+    Xj = Xi if m == n else _points(n, d, 40 + seed, 0.5)
+    yi = _labels(m, 5 + seed)
+    yj = yi if m == n else _labels(n, 60 + seed)
+    g = np.random.default_rng(70 + seed)
+    Om = np.asfortranarray(g.standard_normal((n, l)).astype(np.float32))
+    gamma = 1.0 / d
+    Yref = O.sketch(Xi, Xj, yi, yj, Om, gamma)
+    dXi = dev(Xi)
+    dXj = dXi if Xj is Xi else dev(Xj)
+    dyi = dev(yi)
+    dyj = dyi if yj is yi else dev(yj)
+    dOm = dev(Om)
+    errs = {}
+    # compensated: the truncating fp32 accumulation of the tensor cores shrinks long sums by ~2^-25 per step
+    # (measured 1.4e-5 at n = 4096); promoted every 256 points it stays at one chunk's worth
+    for product, tol in ((_lib.SKETCH_COMPENSATED_PROMOTED, 3e-6), (_lib.SKETCH_COMPENSATED, 6e-5),
+                         (_lib.SKETCH_P_SPLIT, 4e-4)):
+        Y = colmajor_empty(m, l, m + 1)
+        gpu_ctx.rbf_sketch_ex(m, n, d, l, ptr(dXi), d, ptr(dXj), d, POINT_MAJOR, ptr(dyi), ptr(dyj), ptr(dOm), n,
+                              ptr(Y), m + 1, gamma, product)
+        gpu_ctx.sync()
+        errs[product] = rel_fro(colmajor_host(Y, m), Yref)
+        assert errs[product] <= tol, (product, errs)
+
+
 def test_rbf_sketch_two_calls_reuse_workspace(gpu_ctx):
     n, d, l = 640, 16, 24
     X = _points(n, d, 21)
@@ -122,9 +164,18 @@ def test_rbf_sketch_two_calls_reuse_workspace(gpu_ctx):
     assert np.array_equal(outs[0], outs[1])  # deterministic: same tiles, same order
 
 
-@pytest.mark.parametrize("m,n,d,l", [(300, 777, 33, 40), (1000, 1000, 128, 138)])
+@pytest.mark.parametrize("m,n,d,l", [
+    (300, 777, 33, 40),      # ragged rows, points and features; one 144-column tile
+    (1000, 1000, 128, 138),  # the two-Gaussian workload's width
+    (1, 5, 3, 1),            # one row, one column (16-column tile), n not a multiple of 8
+    (129, 64, 8, 16),
+    (200, 301, 100, 528),    # two 264-column tiles
+    (64, 1000, 256, 300),    # widest features; 300 = 264 + 36
+    (513, 257, 17, 1040),    # four tiles
+])
 def test_rbf_sketch_f64_matches_oracle(gpu_ctx, m, n, d, l):
-    """The plain FP64 comparator pass agrees with the FP64 oracle to relative 1e-12."""
+    """The plain FP64 comparator pass (one fused launch on the FP64 tensor cores) agrees with the FP64 oracle to
+    relative 1e-12, and every column to 1e-11 of the RMS column norm."""
     import torch
     Xi = _points(m, d, 31, 0.5)
     Xj = Xi if m == n else _points(n, d, 32, 0.5)
@@ -137,7 +188,26 @@ def test_rbf_sketch_f64_matches_oracle(gpu_ctx, m, n, d, l):
     Y = torch.zeros((l, m), dtype=torch.float64, device="cuda")
     gpu_ctx.rbf_sketch_f64(m, n, d, l, ptr(dXi), d, ptr(dXj), d, ptr(dyi), ptr(dyj), ptr(dOm), n, ptr(Y), m, gamma)
     gpu_ctx.sync()
-    assert rel_fro(Y.cpu().numpy().T, Yref) <= 1e-12
+    Yg = Y.cpu().numpy().T
+    assert rel_fro(Yg, Yref) <= 1e-12
+    rms_col = np.linalg.norm(Yref) / np.sqrt(l)
+    assert (np.linalg.norm(Yg - Yref, axis=0) / rms_col).max() <= 1e-11
+
+
+@pytest.mark.parametrize("m,n,d", [(300, 777, 33), (1, 5, 3), (1024, 129, 128)])
+def test_rbf_block_f64_matches_oracle(gpu_ctx, m, n, d):
+    """The materialised FP64 block: relative 1e-13 elementwise against the oracle."""
+    import torch
+    Xi, Xj = _points(m, d, 41, 0.5), _points(n, d, 42, 0.5)
+    yi, yj = _labels(m, 7), _labels(n, 8)
+    gamma = 0.9 / d
+    Kref = O.rbf_block(Xi, Xj, yi, yj, gamma)
+    dXi, dXj, dyi, dyj = dev(Xi), dev(Xj), dev(yi), dev(yj)
+    K = torch.zeros((n, m + 2), dtype=torch.float64, device="cuda")
+    gpu_ctx.rbf_block_f64(m, n, d, ptr(dXi), d, ptr(dXj), d, ptr(dyi), ptr(dyj), ptr(K), m + 2, gamma)
+    gpu_ctx.sync()
+    Kg = K.cpu().numpy()[:, :m].T
+    assert np.max(np.abs(Kg - Kref)) <= 1e-13
 
 
 def test_bounded_wait_expiry_reports_timeout_and_context_survives(gpu_ctx):

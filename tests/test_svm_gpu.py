@@ -2,10 +2,13 @@
 
 * db200_svm_barrier on the oracle's own low-rank factor Z: both run the same FP64 barrier method, so the dual
   objective agrees to relative 1e-9 and both reach the 1e-6 duality-gap stop.
-* db200_lowrank: the factor built from bf16 kernel passes vs the oracle's FP64 factor:
-  ||Z Z^T - Zo Zo^T||_F <= 2e-2 ||Zo Zo^T||_F.
-* db200_svm_solve end to end (config-1 workload): dual objective within 1e-2 of the oracle's, primal-dual gap
-  <= 1e-6, held-out accuracy within 1 percentage point.
+* db200_lowrank: the factor built from tensor-core kernel passes vs the oracle's FP64 factor,
+  ||Z Z^T - Zo Zo^T||_F / ||Zo Zo^T||_F: <= 1e-5 with the compensated sketch product (DB200_MIXED),
+  <= 2e-2 with the single fp16 product (DB200_MIXED_FAST).
+* db200_svm_solve end to end on the two-Gaussian workload (n = 4096, d = 32, l = 138, q = 1, C = 1): dual
+  objective within 1e-6 of the oracle's (DB200_MIXED and DB200_FP64; the fast mixed form, whose single fp16 sketch
+  product moves the sketched subspace, within 1e-4), primal-dual gap <= 1e-6, held-out accuracy within 1
+  percentage point.
 """
 import numpy as np
 import pytest
@@ -117,10 +120,11 @@ def test_barrier_iteration_caps_report_maxiter(gpu_ctx, c1_small):
     assert rep.status == -4 and rep.outer == 2  # DB200_ERR_MAXITER
 
 
-@pytest.mark.parametrize("precision,tol", [(0, 2e-2), (1, 1e-9)])
+@pytest.mark.parametrize("precision,tol", [(0, 1e-5), (2, 2e-2), (1, 1e-9)])
 def test_lowrank_factor_matches_oracle(gpu_ctx, precision, tol):
-    """Mixed: bf16 kernel passes, ||ZZ^T - ZoZo^T|| <= 2e-2.  FP64 comparator: the oracle's own algorithm in FP64,
-    <= 1e-9 (the shifted Cholesky and CholeskyQR2 run in the same order)."""
+    """DB200_MIXED (compensated sketch product): ||ZZ^T - ZoZo^T|| <= 1e-5; DB200_MIXED_FAST (single fp16
+    product): <= 2e-2.  FP64 comparator: the oracle's own algorithm in FP64, <= 1e-9 (the shifted Cholesky and
+    CholeskyQR2 run in the same order)."""
     import torch
     w = datagen.two_gaussians(n=4096, d=32, seed=1)
     Om = w.omega()
@@ -134,12 +138,16 @@ def test_lowrank_factor_matches_oracle(gpu_ctx, precision, tol):
     if precision == 1:  # same FP64 algorithm: compare the factor itself (the identity below cancels at ~1e-8)
         assert np.linalg.norm(Z - lr.Z) <= tol * np.linalg.norm(lr.Z)
     else:
-        assert zzt_rel(Z, lr.Z) <= tol
+        err = zzt_rel(Z, lr.Z)
+        print(f"lowrank precision={precision}: ||ZZ^T - ZoZo^T||/||ZoZo^T|| = {err:.3e}")
+        assert err <= tol
     assert rep.nu > 0
 
 
-@pytest.mark.parametrize("precision", [0, 1])
-def test_svm_solve_end_to_end_matches_oracle(gpu_ctx, precision):
+# dual objective against the oracle's: the north star's 1e-6 for the compensated mixed path and FP64; the fast
+# mixed form's single fp16 sketch product leaves ~2e-5 at this size (4e-4 at n = 131072)
+@pytest.mark.parametrize("precision,ftol", [(0, 1e-6), (1, 1e-8), (2, 1e-4)])
+def test_svm_solve_end_to_end_matches_oracle(gpu_ctx, precision, ftol):
     import torch
     w = datagen.two_gaussians(n=4096, d=32, seed=1)
     test = datagen.two_gaussians(n=2048, d=32, seed=2)
@@ -156,7 +164,9 @@ def test_svm_solve_end_to_end_matches_oracle(gpu_ctx, precision):
     a = da.cpu().numpy()
     assert rep.status == 0
     assert rep.gap_barrier < 1e-6 and rep.gap_primal_dual < 1e-6
-    assert abs(rep.f - ref.f) <= (1e-2 if precision == 0 else 1e-8) * abs(ref.f)
+    rel = abs(rep.f - ref.f) / abs(ref.f)
+    print(f"svm_solve precision={precision}: |f - f_oracle|/|f_oracle| = {rel:.3e}")
+    assert rel <= ftol
     acc_gpu = np.mean(np.sign(O.decision(test.X, w.X, w.y, a, w.gamma)) == test.y)
     acc_ref = np.mean(np.sign(O.decision(test.X, w.X, w.y, ref.a, w.gamma)) == test.y)
     assert abs(acc_gpu - acc_ref) <= 0.01
