@@ -182,6 +182,7 @@ NOALLOC_SCRATCH_BYTES = 32 << 20
 # precisions of the SVM path and sketch products (include/darray_b200.h)
 MIXED, FP64, MIXED_FAST = 0, 1, 2
 SKETCH_SINGLE, SKETCH_P_SPLIT, SKETCH_COMPENSATED, SKETCH_COMPENSATED_PROMOTED = 0, 1, 2, 3
+SKETCH_COMPENSATED_PROMOTED_COARSE = 4
 POINT_MAJOR, FEATURE_MAJOR = 0, 1
 F32, F64 = 0, 1
 

@@ -68,7 +68,7 @@ SketchPlan comp_plan(const SketchPlan& p, int l) {
   SketchPlan c = p;
   c.comp = 2;
   if (!(c.panel <= 256 && c.panel + 128 + 128 * c.g_bufs <= 512)) c = plan_sketch(l, 2);
-  c.promote = 2;  // accumulation promoted every two j tiles, as in db200_lowrank's mixed passes
+  c.promote = 8;  // range-finder passes: accumulation promoted every eight j tiles, as in db200_lowrank
   return c;
 }
 
@@ -180,7 +180,7 @@ int db200_svm_solve_batched(db200_context* ctx, int count, const db200_svm_insta
 
   // ---- device buffers: packed points and test matrices (workspace), per-instance pass outputs (pipeline slot)
   std::vector<SketchPlan> plans((size_t)count);
-  size_t wbytes = 4096, pbytes = 4096 + (size_t)workers * 256;
+  size_t wbytes = 4096, pbytes = 4096 + (size_t)workers * 256;  // + the final pass's instance table, below
   int njobs = 0;  // tile-engine instances: default multi-panel plans split into exact-width panels
   for (int b = 0; b < count; ++b) {
     const db200_svm_instance& I = inst[b];
@@ -192,6 +192,7 @@ int db200_svm_solve_batched(db200_context* ctx, int count, const db200_svm_insta
     const size_t nl = (size_t)I.n * I.l, ll = (size_t)I.l * I.l;
     pbytes += 2 * align_up(nl * 4, 256) + align_up(nl * 8, 256) + 2 * align_up(ll * 8, 256);
   }
+  wbytes += align_up(tile_table_bytes(njobs), 256);
   void* ws = workspace(ctx, wbytes);
   char* base = static_cast<char*>(slot_buffer(ctx, SLOT_PIPE, pbytes + 4096));
   if (!ws || !base) return DB200_ERR_NOMEM;
@@ -244,8 +245,18 @@ int db200_svm_solve_batched(db200_context* ctx, int count, const db200_svm_insta
     else tj.push_back(T);
   }
   const int nj = (int)tj.size();
-  TilePlan tplan;
+  TilePlan tplan, tplan_final;
   if ((st = prepare_rbf_tiles(ctx, RBF_MODE_SKETCH, tj.data(), nj, nullptr, 0, &tplan))) return st;
+  // the final pass (Y = K Q, contracted into the Nystrom core, whose scale the accumulation's truncation would
+  // shrink) promotes every two j tiles, as db200_lowrank's final pass does; its instance table is in the workspace
+  for (TileJob& T : tj)
+    if (T.plan.comp == 2) T.plan.promote = 2;
+  {
+    void* table_final = cw.take<char>(tile_table_bytes(nj));
+    if ((st = prepare_rbf_tiles(ctx, RBF_MODE_SKETCH, tj.data(), nj, table_final, tile_table_bytes(nj),
+                                &tplan_final)))
+      return st;
+  }
 
   // ---- one kernel pass over every instance: pack each test matrix (Omega, or Q from the previous pass), then one
   // persistent launch.  After the first Q pass the sequence is captured once and replayed.
@@ -261,19 +272,22 @@ int db200_svm_solve_batched(db200_context* ctx, int count, const db200_svm_insta
     return launch_rbf_plan(ctx, tp);
   };
   cudaStream_t cs = nullptr;
-  cudaGraphExec_t qpass = nullptr;
+  cudaGraphExec_t graphs[2] = {nullptr, nullptr};  // the range-finder Q pass and the final pass
   cudaEvent_t ev = nullptr;
   auto cleanup = [&]() {
-    if (qpass) cudaGraphExecDestroy(qpass);
+    for (cudaGraphExec_t& g : graphs)
+      if (g) cudaGraphExecDestroy(g);
     if (cs) cudaStreamDestroy(cs);
     if (ev) cudaEventDestroy(ev);
   };
-  auto q_pass = [&]() -> int {
-    if (!use_graph) return enqueue_pass(false, tplan);
-    if (!qpass) {
+  auto q_pass = [&](bool final_pass) -> int {
+    const TilePlan& tp = final_pass ? tplan_final : tplan;
+    if (!use_graph) return enqueue_pass(false, tp);
+    cudaGraphExec_t& gx = graphs[final_pass ? 1 : 0];
+    if (!gx) {
       // capture on a private stream (the context's stream may be the legacy default stream)
-      if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess ||
-          cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess)
+      if (!cs && (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess ||
+                  cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess))
         return fail(ctx, DB200_ERR_CUDA, "svm_solve_batched: stream for graph capture");
       cudaStream_t keep = ctx->stream;
       const bool prof = ctx->profiling;
@@ -285,14 +299,14 @@ int db200_svm_solve_batched(db200_context* ctx, int count, const db200_svm_insta
       if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
         s2 = fail(ctx, DB200_ERR_CUDA, "svm_solve_batched: begin capture");
       } else {
-        s2 = enqueue_pass(false, tplan);
+        s2 = enqueue_pass(false, tp);
         const cudaError_t e = cudaStreamEndCapture(cs, &g);
         if (!s2 && e != cudaSuccess) s2 = cuda_fail(ctx, e, "cudaStreamEndCapture");
       }
       ctx->stream = keep;
       ctx->profiling = prof;
       ctx->launches = launches;
-      if (!s2 && cudaGraphInstantiate(&qpass, g, 0) != cudaSuccess)
+      if (!s2 && cudaGraphInstantiate(&gx, g, 0) != cudaSuccess)
         s2 = fail(ctx, DB200_ERR_CUDA, "svm_solve_batched: graph instantiate");
       if (g) cudaGraphDestroy(g);
       if (s2) return s2;
@@ -300,7 +314,7 @@ int db200_svm_solve_batched(db200_context* ctx, int count, const db200_svm_insta
     // order the replay after the work already queued on the context's stream, and the rest after it
     DB200_CUDA(ctx, cudaEventRecord(ev, ctx->stream));
     DB200_CUDA(ctx, cudaStreamWaitEvent(cs, ev, 0));
-    DB200_CUDA(ctx, cudaGraphLaunch(qpass, cs));
+    DB200_CUDA(ctx, cudaGraphLaunch(gx, cs));
     DB200_CUDA(ctx, cudaEventRecord(ev, cs));
     DB200_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ev, 0));
     count_launch(ctx, count + 1);
@@ -389,14 +403,14 @@ int db200_svm_solve_batched(db200_context* ctx, int count, const db200_svm_insta
   if (!st) st = orth_all();
   for (int it = 0; it < q && !st; ++it) {
     Timer t(ctx->stream);
-    st = q_pass();
+    st = q_pass(false);
     R.kernel_passes += 1;
     if (!st) R.ms_sketch += t.stop();
     if (!st) st = orth_all();
   }
   if (!st) {  // Y = K Q, the pass the Nystrom core contracts
     Timer t(ctx->stream);
-    st = q_pass();
+    st = q_pass(true);
     R.kernel_passes += 1;
     if (!st) R.ms_sketch += t.stop();
   }

@@ -254,8 +254,7 @@ int db200_rbf_sketch_ex(db200_context* ctx, int m, int n, int d, int l, const fl
                         float* Y, int ldy, float gamma, int product) {
   if (!ctx) return DB200_ERR_INVALID;
   if (m < 0 || n < 0 || d < 1 || l < 0) return fail(ctx, DB200_ERR_INVALID, "rbf_sketch: negative size");
-  if (product != DB200_SKETCH_SINGLE && product != DB200_SKETCH_P_SPLIT && product != DB200_SKETCH_COMPENSATED &&
-      product != DB200_SKETCH_COMPENSATED_PROMOTED)
+  if (product < DB200_SKETCH_SINGLE || product > DB200_SKETCH_COMPENSATED_PROMOTED_COARSE)
     return fail(ctx, DB200_ERR_INVALID, "rbf_sketch: unknown sketch product");
   if (m == 0 || l == 0) return DB200_OK;
   if (d > 128) return fail(ctx, DB200_ERR_UNSUPPORTED, "rbf_sketch: d > 128 not supported");
@@ -268,10 +267,11 @@ int db200_rbf_sketch_ex(db200_context* ctx, int m, int n, int d, int l, const fl
   int st = check_points(ctx, m, d, Xi, ldxi, x_layout);
   if (!st) st = check_points(ctx, n, d, Xj, ldxj, x_layout);
   if (st) return st;
-  SketchPlan plan = plan_sketch(l, product == DB200_SKETCH_COMPENSATED_PROMOTED ? 2 : product);
-  // accumulation chunks of two j tiles (256 points): the truncation loss of the tensor cores' fp32 accumulation
-  // stays at ~48 steps x 2^-25 of a value
-  if (product == DB200_SKETCH_COMPENSATED_PROMOTED) plan.promote = 2;
+  const bool promoted = product >= DB200_SKETCH_COMPENSATED_PROMOTED;
+  SketchPlan plan = plan_sketch(l, promoted ? 2 : product);
+  // accumulation chunks of two j tiles (256 points; the truncation loss of the tensor cores' fp32 accumulation
+  // stays at ~48 steps x 2^-25 of a value) or, coarse, of eight (1024 points, ~192 steps)
+  if (promoted) plan.promote = (product == DB200_SKETCH_COMPENSATED_PROMOTED) ? 2 : 8;
   const int npad = point_pad(n);
   const size_t op_halves = packed_sketch_halves(plan, npad);
   PackedPoints pi, pj;

@@ -72,6 +72,8 @@ struct alignas(64) TileInst {
   const float* sj;
   const float* fi;       // the point sets' scales 2^-e of the packed operands (one float each)
   const float* fj;
+  const unsigned* lof_i;  // nonzero when some point of the set has a nonzero lo part (written by the pack)
+  const unsigned* lof_j;
   const float* yi;
   const float* yj;
   float* out;
@@ -170,8 +172,10 @@ __device__ __forceinline__ bool issuer_wait(const Issuer& S, int idx, uint32_t p
   return __all_sync(0xffffffffu, mbar_wait(S.s_bar + 8u * (uint32_t)idx, parity, S.abort_flag));
 }
 
-// Distance MMA of one tile into the next G buffer, for a packed row of 2 * DP elements (split fp16).
-template <int DP>
+// Distance MMA of one tile into the next G buffer, for a packed row of 2 * DP elements (split fp16).  EXACT: both
+// point sets are exact in fp16 after scaling (every lo is zero, e.g. 0/1 features), so only hi.hi is issued; the
+// lo chunks still pass through the Xj ring.
+template <int DP, bool EXACT>
 __device__ __forceinline__ bool issue_mma1(Issuer& S, int g_bufs) {
   constexpr uint32_t idesc_g = idesc_f16(PAIR_M, BN, false);
   constexpr int NKC = (2 * DP) / KC;
@@ -194,8 +198,9 @@ __device__ __forceinline__ bool issue_mma1(Issuer& S, int g_bufs) {
           const int oh = o, ol = DP + o;
           umma_f16_pair(d_tmem, S.dxi + (((oh / KC) * XI_CHUNK + (oh % KC) * 2) >> 4), bdesc, idesc_g,
                         o == 0 ? 0u : 1u);
-          umma_f16_pair(d_tmem, S.dxi + (((ol / KC) * XI_CHUNK + (ol % KC) * 2) >> 4), bdesc, idesc_g, 1u);
-        } else {  // B slice is lo_j: pair with hi_i
+          if (!EXACT)
+            umma_f16_pair(d_tmem, S.dxi + (((ol / KC) * XI_CHUNK + (ol % KC) * 2) >> 4), bdesc, idesc_g, 1u);
+        } else if (!EXACT) {  // B slice is lo_j: pair with hi_i
           const int oh = o - DP;
           umma_f16_pair(d_tmem, S.dxi + (((oh / KC) * XI_CHUNK + (oh % KC) * 2) >> 4), bdesc, idesc_g, 1u);
         }
@@ -258,11 +263,11 @@ __device__ __forceinline__ bool issue_mma2(Issuer& S, const SketchMma& Y, int jt
 // (round to nearest), and the next chunk waits for that drain.  The tensor cores' fp32 accumulation truncates, so
 // a sum over all n points loses ~2^-25 of its value per accumulation step, always toward zero; chunks of T tiles
 // bound that loss by the steps in one chunk.
-template <int MODE, int DP, bool TWO, int COMP>
+template <int MODE, int DP, bool TWO, int COMP, bool EXACT>
 __device__ __forceinline__ bool issue_item(Issuer& S, const SketchMma& Y, int njt, int g_bufs, int promote) {
-  if (!issue_mma1<DP>(S, g_bufs)) return false;
+  if (!issue_mma1<DP, EXACT>(S, g_bufs)) return false;
   for (int jt = 0; jt < njt; ++jt) {
-    if (jt + 1 < njt && !issue_mma1<DP>(S, g_bufs)) return false;
+    if (jt + 1 < njt && !issue_mma1<DP, EXACT>(S, g_bufs)) return false;
     if (MODE == RBF_MODE_SKETCH) {
       const int jc = promote ? jt % promote : jt;  // tile inside the accumulation chunk (0: fresh accumulator)
       if (promote && jc == 0 && jt > 0) {
@@ -280,34 +285,42 @@ __device__ __forceinline__ bool issue_item(Issuer& S, const SketchMma& Y, int nj
   return true;
 }
 
+template <int MODE, bool TWO, int COMP, bool EXACT>
+__device__ __forceinline__ bool issue_item_dpx(Issuer& S, const SketchMma& Y, int nkc, int njt, int g_bufs,
+                                               int promote) {
+  switch (nkc) {
+    case 1: return issue_item<MODE, 32, TWO, COMP, EXACT>(S, Y, njt, g_bufs, promote);
+    case 2: return issue_item<MODE, 64, TWO, COMP, EXACT>(S, Y, njt, g_bufs, promote);
+    case 3: return issue_item<MODE, 96, TWO, COMP, EXACT>(S, Y, njt, g_bufs, promote);
+    default: return issue_item<MODE, 128, TWO, COMP, EXACT>(S, Y, njt, g_bufs, promote);
+  }
+}
+
 template <int MODE, bool TWO, int COMP>
 __device__ __forceinline__ bool issue_item_dp(Issuer& S, const SketchMma& Y, int nkc, int njt, int g_bufs,
-                                              int promote) {
-  switch (nkc) {
-    case 1: return issue_item<MODE, 32, TWO, COMP>(S, Y, njt, g_bufs, promote);
-    case 2: return issue_item<MODE, 64, TWO, COMP>(S, Y, njt, g_bufs, promote);
-    case 3: return issue_item<MODE, 96, TWO, COMP>(S, Y, njt, g_bufs, promote);
-    default: return issue_item<MODE, 128, TWO, COMP>(S, Y, njt, g_bufs, promote);
-  }
+                                              int promote, bool exact) {
+  return exact ? issue_item_dpx<MODE, TWO, COMP, true>(S, Y, nkc, njt, g_bufs, promote)
+               : issue_item_dpx<MODE, TWO, COMP, false>(S, Y, nkc, njt, g_bufs, promote);
 }
 
 // Dispatch of one work item to the loop specialised for its panel split and sketch product (KBLOCK items and
 // compensated panels take one instruction).
 template <int MODE>
 __device__ __forceinline__ bool issue_item_any(Issuer& S, const SketchMma& Y, int nkc, int njt, int g_bufs, bool two,
-                                               int comp, int promote) {
-  if (MODE != RBF_MODE_SKETCH) return issue_item_dp<MODE, false, 0>(S, Y, nkc, njt, g_bufs, 0);
-  if (comp == 2) return issue_item_dp<MODE, false, 2>(S, Y, nkc, njt, g_bufs, promote);
-  if (comp == 1) return issue_item_dp<MODE, false, 1>(S, Y, nkc, njt, g_bufs, promote);
-  return two ? issue_item_dp<MODE, true, 0>(S, Y, nkc, njt, g_bufs, promote)
-             : issue_item_dp<MODE, false, 0>(S, Y, nkc, njt, g_bufs, promote);
+                                               int comp, int promote, bool exact) {
+  if (MODE != RBF_MODE_SKETCH) return issue_item_dpx<MODE, false, 0, false>(S, Y, nkc, njt, g_bufs, 0);
+  if (comp == 2) return issue_item_dp<MODE, false, 2>(S, Y, nkc, njt, g_bufs, promote, exact);
+  if (comp == 1) return issue_item_dp<MODE, false, 1>(S, Y, nkc, njt, g_bufs, promote, exact);
+  return two ? issue_item_dp<MODE, true, 0>(S, Y, nkc, njt, g_bufs, promote, exact)
+             : issue_item_dp<MODE, false, 0>(S, Y, nkc, njt, g_bufs, promote, exact);
 }
 
 // Drain of the sketch accumulator by one epilogue warp: its 32 rows (TMEM lanes from t_lane) x panel/4 columns,
-// 16 columns per TMEM load batch.  accumulate: add into Y with fire-and-forget fp32 reductions (red.global.add,
-// round to nearest, done in L2, so the drain never waits on a global load) instead of storing; every element has
-// one owner thread, whose first chunk stores and later chunks add, in program order.  Kept out of line: its
-// registers would otherwise stay reserved across the epilogue's exp loop.
+// 8 columns per TMEM load batch.  accumulate: add into Y with fp32 reductions (red.global.add, round to nearest,
+// performed in L2) instead of storing.  A reduction does not wait for the old value, so the drain costs no global
+// load latency (a load-add-store drain made the pass 2x slower).  Every element has one owner thread, whose first
+// chunk stores and later chunks add, in program order to the same address.  Kept out of line: its registers
+// would otherwise stay reserved across the epilogue's exp loop.
 __device__ __noinline__ void drain_sketch_chunk(const TileInst* I, int item, uint32_t rank, int row, int qc,
                                                 uint32_t t_lane_base, bool accumulate) {
   const int li = item - I->item_begin;
@@ -318,21 +331,20 @@ __device__ __noinline__ void drain_sketch_chunk(const TileInst* I, int item, uin
   const float y_i = (i < m && I->yi) ? I->yi[i] : 1.0f;
   const int panel = I->panel, l = I->l;
   const int quarter = panel / 4;  // panel is a multiple of 16
-  for (int cc = 0; cc < quarter; cc += 16) {
-    float yv[16];
-    const int nc = min(16, quarter - cc);  // a multiple of 4
+  for (int cc = 0; cc < quarter; cc += 8) {
+    float yv[8];
+    const int nc = min(8, quarter - cc);  // 4 or 8
     const uint32_t ta = t_lane_base + I->tmem_y + qc * quarter + cc;
-#pragma unroll
-    for (int q4 = 0; q4 < 4; ++q4)
-      if (4 * q4 < nc) tmem_ld4(ta + 4 * q4, yv + 4 * q4);
+    tmem_ld4(ta, yv);
+    if (nc > 4) tmem_ld4(ta + 4, yv + 4);
     tmem_wait_ld();
     if (i < m) {
       const int col0 = pn * panel + qc * quarter + cc;
 #pragma unroll
-      for (int e = 0; e < 16; ++e) {
+      for (int e = 0; e < 8; ++e) {
         if (e < nc && col0 + e < l) {
           float* dst = out_i + (size_t)(col0 + e) * ldo;
-          if (accumulate) atomicAdd(dst, y_i * yv[e]);  // result unused: compiles to a reduction
+          if (accumulate) atomicAdd(dst, y_i * yv[e]);  // result unused: a fire-and-forget reduction
           else *dst = y_i * yv[e];
         }
       }
@@ -521,6 +533,8 @@ __global__ void __launch_bounds__(NUM_THREADS, 1) rbf_tile_kernel(const __grid_c
         Y.y2_boff = (uint32_t)((n1 / 2) * 128) >> 4;
         Y.lo_boff = Y.y2_boff;  // compensated panels take one instruction: the lo rows sit where n2's would
         const int comp = I->comp, promote = I->promote;
+        // both point sets exact in fp16 after scaling (no lo part anywhere): hi.hi only
+        const bool exact = (MODE == RBF_MODE_SKETCH) && (*I->lof_i | *I->lof_j) == 0u;
         Y.tmem_p = tmem_base + (uint32_t)I->tmem_p;
         Y.tmem_y = tmem_base + (uint32_t)I->tmem_y;
         Y.tmem_y2 = Y.tmem_y + (uint32_t)n1;
@@ -531,7 +545,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1) rbf_tile_kernel(const __grid_c
           if (!issuer_wait(S, B_Y_EMPTY, (S.ydone - 1) & 1)) { ok = false; break; }
           tc_fence_after();
         }
-        ok = issue_item_any<MODE>(S, Y, nkc, njt, g_bufs, two, comp, promote);
+        ok = issue_item_any<MODE>(S, Y, nkc, njt, g_bufs, two, comp, promote, exact);
         if (!ok) break;
         if (elect_one()) {
           umma_commit_pair(bar(B_XI_EMPTY));
@@ -583,6 +597,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1) rbf_tile_kernel(const __grid_c
       const float y_i = (i < m && I->yi) ? I->yi[i] : 1.0f;
       sjbuf[lane] = sj[qc * EPI_COLS + lane];  // tile 0 of this item
       __syncwarp();
+      bool pending_drain = false, pending_acc = false;
       auto drain = [&](bool accumulate) -> bool {
         if (!__all_sync(0xffffffffu, mbar_wait(bar(B_Y_FULL), ydone & 1, abort_flag))) return false;
         tc_fence_after();
@@ -649,10 +664,20 @@ __global__ void __launch_bounds__(NUM_THREADS, 1) rbf_tile_kernel(const __grid_c
           __syncwarp();
           if (lane == 0) mbar_arrive_remote(lbar(B_P_FULL0 + h));
           ++kp;
-          if (promote && ((jt + 1) % promote == 0 || jt == njt - 1)) {
-            // this tile closed an accumulation chunk: add it into Y (the first chunk stores)
-            if (!drain(jt >= promote)) { ok = false; break; }
-          }
+          // A chunk closed by the previous tile is drained only now, after this tile's P is handed over: the
+          // distance MMA of the next tile (whose G buffer this tile just read) then runs during the drain, and only
+          // the sketch MMA of this tile waits for it.
+          // Up to two drains here (one call site): the chunk closed by the previous tile, then, on the item's last
+          // tile, the chunk this tile closes (nothing follows it to overlap with).  The first chunk of an item
+          // stores, later chunks add.
+          const bool closes = promote && ((jt + 1) % promote == 0 || jt == njt - 1);
+          bool dq[2] = {pending_drain, closes && jt == njt - 1};
+          bool da[2] = {pending_acc, jt >= promote};
+          pending_drain = closes && jt < njt - 1;
+          pending_acc = jt >= promote;
+          for (int dd = 0; dd < 2 && ok; ++dd)
+            if (dq[dd] && !drain(da[dd])) ok = false;
+          if (!ok) break;
         } else {
           if (i < m) {
 #pragma unroll
@@ -713,7 +738,7 @@ __global__ void absmax_points_kernel(const float* __restrict__ X, long long sp, 
 // One warp per point.  Every point of the set is scaled by the same 2^e, e = 14 - ceil(log2 max |x_ik|) (largest
 // |coordinate| in [2^13, 2^14)), and split into fp16 hi = fp16(2^e x), lo = fp16(2^e x - hi).  norms[i] =
 // ||x||^2 (0 on padding rows) and norms[npad + 1] = 2^-e; norms[npad] holds the set's max |x| bits from
-// absmax_points_kernel.  d <= dp <= 128, so each lane holds its (up to 4) coordinates in registers.
+// absmax_points_kernel, and norms[npad + 2] becomes nonzero when some lo part is (zeroed beforehand).  d <= dp <= 128, so each lane holds its (up to 4) coordinates in registers.
 __global__ void pack_points_kernel(const float* __restrict__ X, long long sp, long long sf, int n, int d, int dp,
                                    int npad, __half* __restrict__ Xp, float* __restrict__ norms) {
   const int lane = threadIdx.x & 31;
@@ -727,8 +752,10 @@ __global__ void pack_points_kernel(const float* __restrict__ X, long long sp, lo
   }
   const float sc = ldexpf(1.0f, e);
   if (blockIdx.x == 0 && threadIdx.x == 0) norms[npad + 1] = ldexpf(1.0f, -e);
+  unsigned* lo_flag = reinterpret_cast<unsigned*>(norms + npad + 2);
   for (long long i = (long long)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32; i < npad; i += warps) {
     float acc = 0.f;
+    bool has_lo = false;
     __half* row = Xp + i * (2 * dp);
 #pragma unroll
     for (int t = 0; t < 4; ++t) {
@@ -743,8 +770,10 @@ __global__ void pack_points_kernel(const float* __restrict__ X, long long sp, lo
         // ||x||^2 + ||y||^2 - 2 x.y cancels to ~fp32 round-off for coincident points
         const float h = __half2float(hi), l = __half2float(lo);
         acc = fmaf(h, h, fmaf(2.0f * h, l, acc));
+        if (l != 0.0f) has_lo = true;
       }
     }
+    if (__any_sync(0xffffffffu, has_lo) && lane == 0) atomicOr(lo_flag, 1u);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     if (lane == 0) norms[i] = ldexpf(acc, -2 * e);
@@ -866,7 +895,7 @@ int pack_points(db200_context* ctx, const float* X, int ldx, int layout, int n, 
   const long long sp = (layout == DB200_POINT_MAJOR) ? ldx : 1;
   const long long sf = (layout == DB200_POINT_MAJOR) ? 1 : ldx;
   unsigned* mx = reinterpret_cast<unsigned*>(norms + npad);
-  DB200_CUDA(ctx, cudaMemsetAsync(mx, 0, sizeof(unsigned), ctx->stream));
+  DB200_CUDA(ctx, cudaMemsetAsync(mx, 0, 4 * sizeof(unsigned), ctx->stream));  // max |x|, scale, lo flag
   if (n > 0) {
     long long mblocks = ((long long)n * d + 255) / 256;
     if (mblocks > (long long)ctx->num_sms * 4) mblocks = (long long)ctx->num_sms * 4;
@@ -965,6 +994,8 @@ int prepare_rbf_tiles(db200_context* ctx, int mode, const TileJob* jobs, int cou
     I.sj = pj.norms;
     I.fi = pi.norms + pi.npad + 1;  // the pack writes the set's scale after the norms and the max |x|
     I.fj = pj.norms + pj.npad + 1;
+    I.lof_i = reinterpret_cast<const unsigned*>(pi.norms + pi.npad + 2);  // and whether any lo part is nonzero
+    I.lof_j = reinterpret_cast<const unsigned*>(pj.norms + pj.npad + 2);
     I.yi = J.yi;
     I.yj = J.yj;
     I.out = J.out;

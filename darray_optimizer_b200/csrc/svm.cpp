@@ -578,13 +578,15 @@ int lowrank_impl(db200_context* ctx, int n, int d, int l, int q, const float* X,
   double ms_sketch = 0, ms_orth = 0, ms_core = 0;
   int st;
 
-  // one pass Y = diag(y) K diag(y) Om, into Y32 (mixed) or Y64 (FP64).  Mixed: every pass takes the compensated
-  // sketch product with promoted accumulation (DB200_SKETCH_COMPENSATED_PROMOTED).  Measured at n = 131072, the
-  // dual objective's distance from the FP64 path is 3.1e-6 when only the final pass (whose Y scales the core
-  // C = Q^T K Q) promotes, 4.9e-7 when the first and the final pass do, 2.5e-7 when all three do
-  auto sketch_f32 = [&](const float* Om, int ldom) -> int {
+  // one pass Y = diag(y) K diag(y) Om, into Y32 (mixed) or Y64 (FP64).  Mixed: the compensated sketch product with
+  // promoted accumulation; the range-finder passes (whose subspace, not scale, matters) in 1024-point chunks, the
+  // final pass, whose Y scales the core C = Q^T K Q, in 256-point chunks.  Measured dual-objective distance from
+  // the FP64 path: 5e-7 at n = 4096 (1.6e-6 with coarse chunks in the final pass) and 4e-7 at n = 131072
+  auto sketch_f32 = [&](const float* Om, int ldom, bool final_pass) -> int {
     EventTimer tm(ctx->stream);
-    const int product = precision == DB200_MIXED_FAST ? DB200_SKETCH_SINGLE : DB200_SKETCH_COMPENSATED_PROMOTED;
+    const int product = precision == DB200_MIXED_FAST ? DB200_SKETCH_SINGLE
+                        : final_pass                  ? DB200_SKETCH_COMPENSATED_PROMOTED
+                                                      : DB200_SKETCH_COMPENSATED_PROMOTED_COARSE;
     int s2 = db200_rbf_sketch_ex(ctx, n, n, d, l, X, ldx, X, ldx, DB200_POINT_MAJOR, y, y, Om, ldom, Y32, n, gamma,
                                  product);
     ms_sketch += tm.stop_ms();
@@ -615,14 +617,14 @@ int lowrank_impl(db200_context* ctx, int n, int d, int l, int q, const float* X,
     if ((st = convert<float, double>(ctx, Omega, ldo, Q, n, n, l))) return st;
     if ((st = sketch_f64(Q, n))) return st;
   } else {
-    if ((st = sketch_f32(Omega, ldo))) return st;
+    if ((st = sketch_f32(Omega, ldo, false))) return st;
   }
   if ((st = orth())) return st;
   for (int it = 0; it < q; ++it) {
-    if ((st = fp64 ? sketch_f64(Q, n) : sketch_f32(Qf, n))) return st;
+    if ((st = fp64 ? sketch_f64(Q, n) : sketch_f32(Qf, n, false))) return st;
     if ((st = orth())) return st;
   }
-  if ((st = fp64 ? sketch_f64(Q, n) : sketch_f32(Qf, n))) return st;  // Y = K Q
+  if ((st = fp64 ? sketch_f64(Q, n) : sketch_f32(Qf, n, true))) return st;  // Y = K Q
   EventTimer tcore(ctx->stream);
   double nu = 0;
   st = fp64 ? nystrom_core<double>(ctx, n, l, Q, Y64, Cm, R, d_pair, d_scalar, Z, ldz, &nu)

@@ -116,13 +116,18 @@ DB200_API int db200_rbf_sketch(db200_context* ctx, int m, int n, int d, int l, c
  *   the single product's rounding of P shifts the sketched subspace enough to move the objective by ~4e-4 at
  *   n = 131072; the shrink does not matter there (the subspace is scale free).
  * DB200_SKETCH_COMPENSATED_PROMOTED: the compensated product with the accumulator restarted every 256 points j and
- *   each chunk added into Y in fp32 with round-to-nearest, so the shrink is that of one chunk (~1e-6 relative).
- *   The kernel passes of the mixed SVM path use it: at n = 131072 the dual objective then lies 2.5e-7 from the
- *   FP64 path's (3.1e-6 with only the final pass promoted, whose Y scales the core C = Q^T K Q). */
+ *   each chunk added into Y in fp32 with round-to-nearest (reductions in L2), so the shrink is that of one chunk
+ *   (~1e-6 relative).  ~1.8x the time of DB200_SKETCH_COMPENSATED at l = 528.
+ * DB200_SKETCH_COMPENSATED_PROMOTED_COARSE: the same with chunks of 1024 points (~1.25x).
+ * The mixed SVM path runs its range-finder passes coarse and its final pass (whose Y scales the core
+ * C = Q^T K Q) with 256-point chunks: the dual objective then lies ~5e-7 from the FP64 path's at n = 4096 and
+ * ~4e-7 at n = 131072 (with 1024-point chunks in the final pass too, 1.6e-6 at n = 4096; without promotion,
+ * 6e-6 and 3e-6). */
 #define DB200_SKETCH_SINGLE 0
 #define DB200_SKETCH_P_SPLIT 1
 #define DB200_SKETCH_COMPENSATED 2
 #define DB200_SKETCH_COMPENSATED_PROMOTED 3
+#define DB200_SKETCH_COMPENSATED_PROMOTED_COARSE 4
 
 /* db200_rbf_sketch with a choice of sketch product (DB200_SKETCH_*).  Same arguments and layout otherwise. */
 DB200_API int db200_rbf_sketch_ex(db200_context* ctx, int m, int n, int d, int l, const float* Xi, int ldxi,
@@ -194,8 +199,9 @@ typedef struct db200_barrier_params {
 
 /* Precision of the path.
  * DB200_MIXED: kernel passes on the tensor cores, distances in split fp16 and the compensated sketch product with
- *   promoted fp32 accumulation (DB200_SKETCH_COMPENSATED_PROMOTED), which keeps the dual objective within ~3e-7
- *   of the FP64 path's; the Woodbury capacity matrix
+ *   promoted fp32 accumulation (range finder DB200_SKETCH_COMPENSATED_PROMOTED_COARSE, final pass
+ *   DB200_SKETCH_COMPENSATED_PROMOTED), which keeps the dual objective within ~5e-7 of the FP64 path's; the
+ *   Woodbury capacity matrix
  *   I + Z^T D^-1 Z formed in integers on the int8 tensor cores from 8 signed 7-bit slices of every column (Ozaki
  *   scheme, error ~3e-14 of the column norms; from r = 2048 first 6 slices, ~3e-10, while refinement converges
  *   with them) and factored in FP64 while each Newton step refined

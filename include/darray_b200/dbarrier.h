@@ -103,10 +103,12 @@ LMatrix<T> pre_conjgrad(int rk, int n, int k, LMatrix<T>& Z, LMatrix<T>& M, LMat
 }
 
 // LIBSVM model text with the reference's bias estimate and layout (include/dbarrier.h:395-470).  Host I/O, as
-// in the reference; dX is d x n (point-major).
+// in the reference; dX is d x n (point-major).  With `bias` (the solve's b, db200_svm_report.b of a solve with
+// db200_barrier_params.bias = 1) the model's rho is -b and the reference's estimate from the margin support
+// vectors is not made; without it (NULL, the reference's call) the estimate is written.
 template <typename T>
 void writemodel(const std::string filepath, int n, int d, int k, LMatrix<T>& a, T C, LMatrix<T>& dZ, LMatrix<T> dY,
-                LMatrix<T> dX, T gamma, int minus, int plus) {
+                LMatrix<T> dX, T gamma, int minus, int plus, const double* bias = nullptr) {
   std::vector<int> sv, bsv;
   for (int i = 0; i < n; ++i)
     if (a.data()[i] > 1e-6) {
@@ -114,7 +116,7 @@ void writemodel(const std::string filepath, int n, int d, int k, LMatrix<T>& a, 
       if (a.data()[i] < C - 1e-6) bsv.push_back(i);
     }
   std::printf("#BSV %d, #SV %d\n", (int)bsv.size(), (int)sv.size());
-  const int nb = std::min((int)bsv.size(), 50);
+  const int nb = bias ? 0 : std::min((int)bsv.size(), 50);
   std::vector<double> bs(nb, 0.0);
   double acc = 0.0;
   for (int j = 0; j < nb; ++j) {
@@ -128,10 +130,11 @@ void writemodel(const std::string filepath, int n, int d, int k, LMatrix<T>& a, 
     acc += yj;
     bs[j] = yj;
   }
-  const double b = nb ? acc / nb : 0.0;
+  const double b = bias ? *bias : (nb ? acc / nb : 0.0);
   double sumsq = 0.0;
   for (double v : bs) sumsq += (v - b) * (v - b);
-  std::printf("approx mean b=%.6e std b=%.6e, #samples=%d\n ", b, nb ? std::sqrt(sumsq / nb) : 0.0, nb);
+  if (bias) std::printf("b=%.6e from the solve\n ", b);
+  else std::printf("approx mean b=%.6e std b=%.6e, #samples=%d\n ", b, nb ? std::sqrt(sumsq / nb) : 0.0, nb);
   FILE* fp = std::fopen(filepath.c_str(), "w");
   if (!fp) return;
   std::fprintf(fp, "svm_type c_svc\n");

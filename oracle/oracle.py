@@ -436,26 +436,33 @@ def decision(Xtest, X, y, a, gamma, block=2048) -> np.ndarray:
     return sketch(Xtest, X, None, None, coef, gamma, block)[:, 0]
 
 
-def writemodel(path, a, C, Z, y, X, gamma, minus, plus) -> dict:
-    """LIBSVM model text as written by include/dbarrier.h:395-470 (bias estimate restated from there)."""
+def writemodel(path, a, C, Z, y, X, gamma, minus, plus, bias=None) -> dict:
+    """LIBSVM model text as written by include/dbarrier.h:395-470 (bias estimate restated from there: the first 50
+    margin support vectors, each with y_j - sum_i a_i y_j ||z_i||^2, averaged).  `bias`: a bias b from a solve of
+    the dual with y^T a = 0 (the extension of the barrier that the reference leaves out), written as rho = -b in
+    place of the estimate."""
     n = len(a)
     sv = [i for i in range(n) if a[i] > 1e-6]
     bsv = [i for i in sv if a[i] < C - 1e-6]
-    nb = min(len(bsv), 50)
-    bs = []
-    zz = np.einsum("ij,ij->i", Z, Z)
-    for j in range(nb):
-        jj = bsv[j]
-        yj = float(y[jj])
-        for ii in sv:
-            yj -= a[ii] * y[jj] * zz[ii]
-        bs.append(yj)
-    b = float(np.mean(bs)) if nb else 0.0
+    if bias is None:
+        nb = min(len(bsv), 50)
+        bs = []
+        zz = np.einsum("ij,ij->i", Z, Z)
+        for j in range(nb):
+            jj = bsv[j]
+            yj = float(y[jj])
+            for ii in sv:
+                yj -= a[ii] * y[jj] * zz[ii]
+            bs.append(yj)
+        b = float(np.mean(bs)) if nb else 0.0
+    else:
+        b = float(bias)
     lines = ["svm_type c_svc", "kernel_type rbf", "gamma %.7f" % gamma, "nr_class 2", "total_sv %d" % len(sv),
              "rho %f" % (-b), "label %d %d" % (plus, minus), "nr_sv %d %d" % (len(bsv), len(sv) - len(bsv)), "SV"]
     for j in sv:
-        feats = " ".join("%d:%7f" % (k + 1, X[j, k]) for k in range(X.shape[1]) if X[j, k] != 0)
-        lines.append(("%7f " % (y[j] * a[j])) + feats + " ")
+        # "%7f " per nonzero feature, as the reference prints them (a point without any leaves "alpha ")
+        feats = "".join("%d:%7f " % (k + 1, X[j, k]) for k in range(X.shape[1]) if X[j, k] != 0)
+        lines.append(("%7f " % (y[j] * a[j])) + feats)
     if path is not None:
         with open(path, "w") as fh:
             fh.write("\n".join(lines) + "\n")

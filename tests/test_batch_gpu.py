@@ -115,7 +115,9 @@ def test_batched_solve_matches_single_solves(gpu_ctx, use_graph, workers):
         Z1 = torch.zeros_like(Z)
         a1 = torch.zeros_like(a)
         rep1 = gpu_ctx.svm_solve(n, d, l, 1, ptr(dX), d, ptr(dy), ptr(dOm), n, gamma, C, ptr(a1), ptr(Z1), n)
-        # the kernel passes are the same (Z to 1e-12); the barriers' FP64 capacity Grams add with atomics, whose order
-        # differs between the batched workers and the single solve: f agrees to 1e-7 (the stop is at gap 1e-6)
+        # The same algorithm, not the same bits: the FP64 Grams of CholeskyQR2 and of the barriers' capacity matrix
+        # add their row splits with atomics, in an order that varies from run to run (~1e-16), which the fp32 test
+        # matrices of the next kernel pass can round differently.  Factors agree to the mixed path's precision and
+        # the objectives well inside the 1e-6 stop.
         assert abs(rep1.f - r.f) <= 1e-7 * abs(rep1.f), (k, rep1.f, r.f)
-        assert rel_fro(Z1.cpu().numpy(), Z.cpu().numpy()) <= 1e-12
+        assert rel_fro(Z1.cpu().numpy(), Z.cpu().numpy()) <= 1e-5

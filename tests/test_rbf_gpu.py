@@ -148,6 +148,31 @@ def test_rbf_sketch_compensated_matches_oracle(gpu_ctx, m, n, d, l, seed):
         assert errs[product] <= tol, (product, errs)
 
 
+@pytest.mark.parametrize("perturb", [False, True])
+def test_rbf_sketch_binary_features(gpu_ctx, perturb):
+    """Sparse binary features (x in {0, 1}, Bernoulli(0.11), d = 123, the sparse-binary workload's shape): every
+    point is exact in fp16, so the distance products reduce to hi.hi.  With one perturbed coordinate the set is no
+    longer exact and the full split runs.  Both against the FP64 oracle, single and compensated products."""
+    from darray_optimizer_b200 import _lib
+    n, d, l = 2048, 123, 264
+    g = np.random.default_rng(31)
+    X = (g.random((n, d)) < 0.11).astype(np.float32)
+    if perturb:
+        X[17, 5] = 0.3
+    y = _labels(n, 9)
+    Om = np.asfortranarray(g.standard_normal((n, l)).astype(np.float32))
+    gamma = 0.05
+    Yref = O.sketch(X, X, y, y, Om, gamma)
+    dX, dy, dOm = dev(X), dev(y), dev(Om)
+    for product, tol in ((_lib.SKETCH_SINGLE, 2e-3), (_lib.SKETCH_COMPENSATED_PROMOTED, 3e-6)):
+        Y = colmajor_empty(n, l)
+        gpu_ctx.rbf_sketch_ex(n, n, d, l, ptr(dX), d, ptr(dX), d, POINT_MAJOR, ptr(dy), ptr(dy), ptr(dOm), n, ptr(Y),
+                              n, gamma, product)
+        gpu_ctx.sync()
+        err = rel_fro(colmajor_host(Y, n), Yref)
+        assert err <= tol, (product, perturb, err)
+
+
 def test_rbf_sketch_two_calls_reuse_workspace(gpu_ctx):
     n, d, l = 640, 16, 24
     X = _points(n, d, 21)
