@@ -38,11 +38,17 @@ struct DevBuf {
   T* as() { return static_cast<T*>(p); }
 };
 
-// copy an m x n column-major host block (leading dimension ld) into a packed device buffer
+// copy an m x n column-major host block (leading dimension ld) into a packed device buffer: one copy, strided
+// (cudaMemcpy2DAsync) when ld > m
 template <class T>
 void up(db200_context* c, T* dst, const T* src, int m, int n, int ld) {
-  for (int j = 0; j < n; ++j)
-    check(c, db200_copy_to_device(c, dst + (size_t)j * m, src + (size_t)j * ld, sizeof(T) * m), "copy to device");
+  if (ld == m) {
+    check(c, db200_copy_to_device(c, dst, src, sizeof(T) * (size_t)m * n), "copy to device");
+    return;
+  }
+  if (cudaMemcpy2DAsync(dst, sizeof(T) * (size_t)m, src, sizeof(T) * (size_t)ld, sizeof(T) * (size_t)m, (size_t)n,
+                        cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
+    check(c, DB200_ERR_CUDA, "copy to device");
 }
 template <class T>
 void down(db200_context* c, T* dst, int ld, const T* src, int m, int n) {
@@ -50,8 +56,10 @@ void down(db200_context* c, T* dst, int ld, const T* src, int m, int n) {
     check(c, db200_copy_to_host(c, dst, src, sizeof(T) * (size_t)m * n), "copy to host");
     return;
   }
-  for (int j = 0; j < n; ++j)
-    check(c, db200_copy_to_host(c, dst + (size_t)j * ld, src + (size_t)j * m, sizeof(T) * m), "copy to host");
+  if (cudaMemcpy2DAsync(dst, sizeof(T) * (size_t)ld, src, sizeof(T) * (size_t)m, sizeof(T) * (size_t)m, (size_t)n,
+                        cudaMemcpyDeviceToHost, c->stream) != cudaSuccess)
+    check(c, DB200_ERR_CUDA, "copy to host");
+  check(c, db200_synchronize(c), "copy to host");
 }
 
 }  // namespace

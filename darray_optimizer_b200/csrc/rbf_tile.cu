@@ -315,6 +315,12 @@ __device__ __forceinline__ bool issue_item_any(Issuer& S, const SketchMma& Y, in
              : issue_item_dp<MODE, false, 0>(S, Y, nkc, njt, g_bufs, promote, exact);
 }
 
+// fp32 add into global memory performed in L2 without returning the old value (red, not atom: the warp does not
+// wait for a reply)
+__device__ __forceinline__ void red_add_f32(float* p, float v) {
+  asm volatile("red.global.add.f32 [%0], %1;" ::"l"(p), "f"(v) : "memory");
+}
+
 // Drain of the sketch accumulator by one epilogue warp: its 32 rows (TMEM lanes from t_lane) x panel/4 columns,
 // 8 columns per TMEM load batch.  accumulate: add into Y with fp32 reductions (red.global.add, round to nearest,
 // performed in L2) instead of storing.  A reduction does not wait for the old value, so the drain costs no global
@@ -344,7 +350,7 @@ __device__ __noinline__ void drain_sketch_chunk(const TileInst* I, int item, uin
       for (int e = 0; e < 8; ++e) {
         if (e < nc && col0 + e < l) {
           float* dst = out_i + (size_t)(col0 + e) * ldo;
-          if (accumulate) atomicAdd(dst, y_i * yv[e]);  // result unused: a fire-and-forget reduction
+          if (accumulate) red_add_f32(dst, y_i * yv[e]);
           else *dst = y_i * yv[e];
         }
       }

@@ -21,6 +21,8 @@
 #include <vector>
 
 #include "mpi_one.h"
+#include "fmt_lite.h"
+#include "utils.h"
 
 namespace DArray {
 

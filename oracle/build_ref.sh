@@ -38,3 +38,18 @@ if command -v nvcc > /dev/null && [ -f "$REF/include/dkernel.cu" ]; then
       -Xlinker -Bsymbolic -lcublas -lcusolver
   echo "$HERE/_ref/libdkernel_ref.so"
 fi
+
+# The reference's own test programs tests/test3.cpp .. test7.cpp, unmodified, compiled against this build's
+# one-rank mirror headers (include/darray_b200/) and linked with libdarray_b200.so: the drop-in proof that code
+# written against DArray's headers builds and runs on the product without source changes.  Outputs to
+# oracle/_ref/reftests/ (the binaries find the product library through a relative rpath).
+ROOT="$(cd "$HERE/.." && pwd)"
+if [ -f "$ROOT/darray_optimizer_b200/lib/libdarray_b200.so" ] && [ -f "$REF/tests/test3.cpp" ]; then
+  mkdir -p "$HERE/_ref/reftests"
+  for t in test3 test4 test5 test6 test7; do
+    g++ -O2 -std=c++17 -w -I "$ROOT/include/darray_b200" -I "$ROOT/include" "$REF/tests/$t.cpp" \
+        -o "$HERE/_ref/reftests/$t" -L "$ROOT/darray_optimizer_b200/lib" -ldarray_b200 \
+        -Wl,-rpath,'$ORIGIN/../../../darray_optimizer_b200/lib'
+    echo "$HERE/_ref/reftests/$t"
+  done
+fi
