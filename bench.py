@@ -200,10 +200,75 @@ def run_reference(args):
             "data": "synthetic (seeded Philox)", "config": config(),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    # the reference's own GPU path for the same product, one kernel block at a time (reported, not the metric)
+    try:
+        import torch
+        if torch.cuda.is_available():
+            line["reference_gpu_block"] = kernel_block("reference")
+    except Exception as e:  # a reported leg only: the CPU line above stands
+        line["reference_gpu_block"] = {"unavailable": f"{type(e).__name__}: {e}"[:200]}
     print(json.dumps(line), flush=True)
     from darray_optimizer_b200 import replicas
     replicas.finalize(rep)
     return 0
+
+
+def kernel_block(impl, reps=3, b=8192, d=128, l=528):
+    """One 8192 x 8192 kernel block at the C2 shape (d = 128, l = 528) through the reference's GPU interface:
+    rbf_kernel then tc_gemm (include/dkernel.cu:132-231, include/dkernel.h:13-46's LRA loop body), host buffers in
+    and out, wall time per block (both calls are synchronous).  impl "reference": the reference's own dkernel.cu
+    built for sm_100a (cuBLAS sgemm; oracle/_ref/libdkernel_ref.so, built by oracle/build_ref.sh); impl "dropin":
+    the product library's C++ symbols of the same names and signatures.  The C2 pass is 256 such blocks."""
+    import ctypes
+    fp, ci, cf = ctypes.POINTER(ctypes.c_float), ctypes.c_int, ctypes.c_float
+    if impl == "reference":
+        path = ROOT / "oracle" / "_ref" / "libdkernel_ref.so"
+        if not path.exists():
+            return {"unavailable": "oracle/_ref/libdkernel_ref.so not built (oracle/build_ref.sh needs the reference "
+                                   "sources)"}
+        lib = ctypes.CDLL(str(path))
+        lib.ref_rbf_kernel.argtypes = [ci, ci, ci, fp, fp, fp, fp, fp, ci, cf]
+        lib.ref_tc_gemm.argtypes = [ci, ci, ci, fp, ci, fp, ci, fp, ci, cf]
+        lib.ref_cuda_init()
+        source = "include/dkernel.cu rbf_kernel + tc_gemm, compiled unmodified for sm_100a (cuBLAS sgemm)"
+    else:
+        from darray_optimizer_b200 import _lib
+        lib = _lib.load()
+        o_rbf = getattr(lib, "_Z10rbf_kerneliiiiPfiS_iS_S_S_if")
+        o_rbf.argtypes = [ci, ci, ci, ci, fp, ci, fp, ci, fp, fp, fp, ci, cf]
+        o_gemm = getattr(lib, "_Z7tc_gemmiiiiPfiS_iS_iff")
+        o_gemm.argtypes = [ci, ci, ci, ci, fp, ci, fp, ci, fp, ci, cf, cf]
+        getattr(lib, "_Z9cuda_initv")()
+        source = "darray_optimizer_b200 drop-in rbf_kernel + tc_gemm (same C++ signatures)"
+    g = np.random.default_rng(20261205)
+    X = np.asfortranarray(g.random((b, d), dtype=np.float32))
+    y = np.where(g.random(b) < 0.5, 1.0, -1.0).astype(np.float32)
+    Om = np.asfortranarray(g.standard_normal((b, l)).astype(np.float32))
+    gamma = 0.5 / d
+    K = np.zeros((b, b), np.float32, order="F")
+    Y = np.zeros((b, l), np.float32, order="F")
+
+    def p(a):
+        return a.ctypes.data_as(fp)
+
+    def run():
+        if impl == "reference":
+            lib.ref_rbf_kernel(b, b, d, p(X), p(X), p(y), p(y), p(K), b, gamma)
+            lib.ref_tc_gemm(b, l, b, p(K), b, p(Om), b, p(Y), b, 1.0)
+        else:
+            o_rbf(0, b, b, d, p(X), b, p(X), b, p(y), p(y), p(K), b, gamma)
+            o_gemm(0, b, l, b, p(K), b, p(Om), b, p(Y), b, 1.0, 0.0)
+
+    run()  # warm-up: handles, allocations, module load
+    ts = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        run()
+        ts.append(time.perf_counter() - t0)
+    s = float(statistics.median(ts))
+    fl = 2.0 * b * b * (d + l)
+    return {"source": source, "block": [b, b], "d": d, "l": l, "s_per_block": s, "tflops": fl / s / 1e12,
+            "c2_pass_s": s * (N_POINTS // b) ** 2, "y_checksum": float(np.abs(Y).sum(dtype=np.float64))}
 
 
 # ------------------------------------------------------------------------------------------ our arm
@@ -272,6 +337,10 @@ def run_ours(args):
     if not args.no_batch and rank == 0:
         batch = batch_run(ctx)
     extra = {}
+    if not args.no_e2e and rank == 0:
+        # one 8192 x 8192 block through the drop-in C++ symbols rbf_kernel + tc_gemm (host buffers), the shape
+        # `bench.py --impl reference` times the reference's own GPU code on
+        extra["dropin_block"] = kernel_block("dropin")
     if args.c3 and rank == 0:
         extra["c3"] = c3_run(ctx)
     if args.c5 and rank == 0:
@@ -280,6 +349,8 @@ def run_ours(args):
         extra["libsvm"] = libsvm_run(ctx)
     if args.lu and rank == 0:
         extra["lu"] = lu_run(ctx)
+    if args.potrf and rank == 0:
+        extra["potrf"] = potrf_run(ctx)
     return finish(args, ctx, w, rep, ms_max, kernel_ms, kernel_count, launches, clocks, e2e_val, h2d, d2h, Om,
                   solve, batch, extra, precision)
 
@@ -431,14 +502,104 @@ def c5_run(ctx, n=524288, r=2048, n_test=16384, tol=1e-2):
     acc = float(np.mean(np.sign(dec.cpu().numpy()) == yt))
     del Z, a
     uniform = landmarks.landmark_residual(ctx, w, r, None, 11)
-    return {"workload": f"C5 mixture of 32 rotated anisotropic Gaussians (n={n}, d={d}, gamma=1/d, r={r}, C={w.C})",
-            "solve_s": solve_s, "used_fallback": lrep.used_fallback, "rank": lrep.rank,
-            "residual_est_learned": lrep.residual_est, "residual_est_uniform_landmarks": uniform,
-            "residual_est_fallback": lrep.residual_fallback, "tol": tol,
-            "landmark_ms": {k: getattr(lrep, k) for k in ("ms_features", "ms_predict", "ms_select", "ms_factor",
-                                                         "ms_residual", "ms_fallback")},
-            "f": rep.f, "gap_barrier": rep.gap_barrier, "gap_primal_dual": rep.gap_primal_dual, "newton": rep.newton,
-            "ms_barrier": rep.ms_barrier, "test_accuracy": acc, "n_test": n_test}
+    out = {"workload": f"C5 mixture of 32 rotated anisotropic Gaussians (n={n}, d={d}, gamma=1/d, r={r}, C={w.C})",
+           "solve_s": solve_s, "used_fallback": lrep.used_fallback, "rank": lrep.rank,
+           "residual_est_learned": lrep.residual_est, "residual_est_uniform_landmarks": uniform,
+           "residual_est_fallback": lrep.residual_fallback, "tol": tol,
+           "landmark_ms": {k: getattr(lrep, k) for k in ("ms_features", "ms_predict", "ms_select", "ms_factor",
+                                                        "ms_residual", "ms_fallback")},
+           "f": rep.f, "gap_barrier": rep.gap_barrier, "gap_primal_dual": rep.gap_primal_dual, "newton": rep.newton,
+           "ms_barrier": rep.ms_barrier, "test_accuracy": acc, "n_test": n_test}
+
+    def solve_and_score(fn):
+        Zs = torch.zeros((l_fb, n), dtype=torch.float64, device="cuda")
+        a_s = torch.zeros(n, dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rp = fn(Zs, a_s)
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t0
+        dec = torch.zeros(n_test, dtype=torch.float64, device="cuda")
+        ctx.rbf_sketch_f64(n_test, n, d, 1, dXt.data_ptr(), d, X.data_ptr(), d, 0, y.data_ptr(), a_s.data_ptr(), n,
+                           dec.data_ptr(), n_test, w.gamma)
+        ctx.sync()
+        return {"s": el, "f": rp.f, "gap_primal_dual": rp.gap_primal_dual,
+                "test_accuracy": float(np.mean(np.sign(dec.cpu().numpy()) == yt))}
+
+    # learned landmarks alone (no residual test, no fallback) against the Gaussian-sketch solve alone, same r
+    out["learned_only"] = solve_and_score(lambda Zs, a_s: ctx.svm_solve_landmarks(
+        n, d, r, X.data_ptr(), d, y.data_ptr(), w.gamma, w.C, net, 11, 16384, 512, 1e30, O.data_ptr(), n, l_fb, 1,
+        a_s.data_ptr(), Zs.data_ptr(), n)[0])
+    out["gaussian_only"] = solve_and_score(lambda Zs, a_s: ctx.svm_solve(
+        n, d, l_fb, 1, X.data_ptr(), d, y.data_ptr(), O.data_ptr(), n, w.gamma, w.C, a_s.data_ptr(), Zs.data_ptr(),
+        n))
+    out["learned_vs_gaussian_time"] = out["learned_only"]["s"] / out["gaussian_only"]["s"]
+    out["bounds"] = c5_bounds(ctx, w, X, y, r)
+    return out
+
+
+def c5_bounds(ctx, w, X, y, r, s_res=512, seed=11):
+    """What any rank-r method could reach at C5, from a rank-(2r + 16) Gaussian Nystrom factor Z2 (one power
+    iteration, the single fp16 sketch product): (1) the residual of Z2's best rank-r part (its top r right singular
+    directions), near the truncated eigendecomposition's; (2) the residual of r landmarks chosen from the ridge
+    leverage scores of Z2 (top r, and r drawn in proportion by Gumbel top-r), for lambda with effective dimension
+    r / 2 and r: the landmark choice a perfect leverage model would make.  Residuals as db200_residual_estimate,
+    over the same 512 sampled columns as the learned path's."""
+    import torch
+    from darray_optimizer_b200 import landmarks
+    n, d = w.n, w.d
+    l2 = 2 * r + 16
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(w.seed + 1)
+    O2 = torch.randn((l2, n), dtype=torch.float32, device="cuda", generator=gen)
+    Z2 = torch.zeros((l2, n), dtype=torch.float64, device="cuda")
+    t0 = time.perf_counter()
+    ctx.lowrank(n, d, l2, 1, X.data_ptr(), d, y.data_ptr(), O2.data_ptr(), n, w.gamma, Z2.data_ptr(), n,
+                precision=2)
+    ctx.sync()
+    t_factor = time.perf_counter() - t0
+    del O2
+    g = np.random.default_rng(seed + 17)
+    S = torch.from_numpy(np.sort(g.choice(n, size=min(s_res, n), replace=False)).astype(np.int32)).cuda()
+
+    def residual(Zr, k):
+        return ctx.residual_estimate(n, d, X.data_ptr(), d, y.data_ptr(), w.gamma, k, Zr.data_ptr(), n, S.numel(),
+                                     S.data_ptr())
+
+    out = {"factor_rank": l2, "factor_s": t_factor, "residual_rank_2r_factor": residual(Z2, l2)}
+    # best rank-r part of Z2: Z2 V_r (V_r = top r eigenvectors of Z2^T Z2), rows of the (l2 x n) storage
+    G = Z2 @ Z2.T
+    evals, V = torch.linalg.eigh(G)
+    Vr = V[:, -r:]
+    Zr = (Vr.T @ Z2).contiguous()  # r x n: column major n x r
+    out["residual_best_rank_r"] = residual(Zr, r)
+    del Zr
+    sig2 = evals.cpu().numpy()
+    for frac in (0.5, 1.0):
+        lam = landmarks.lambda_for_deff(sig2, frac * r)
+        lev = torch.empty(n, dtype=torch.float64, device="cuda")
+        ctx.ridge_leverage(n, l2, Z2.data_ptr(), n, lam, lev.data_ptr())
+        key = f"deff_{frac:g}r"
+        res = {}
+        for how in ("top", "sampled"):
+            if how == "top":
+                keys = lev.to(torch.float32)
+            else:
+                logits = torch.log(torch.clamp(lev, min=1e-30)).to(torch.float32)
+                keys = torch.empty(n, dtype=torch.float32, device="cuda")
+                ctx.gumbel_keys(n, logits.data_ptr(), seed, keys.data_ptr())
+            idx = torch.empty(r, dtype=torch.int32, device="cuda")
+            ctx.select_topk(n, keys.data_ptr(), r, idx.data_ptr())
+            Zl = torch.empty((r, n), dtype=torch.float64, device="cuda")
+            ctx.landmark_factor(n, d, X.data_ptr(), d, y.data_ptr(), w.gamma, r, idx.data_ptr(), Zl.data_ptr(), n)
+            res[how] = residual(Zl, r)
+            del Zl
+        out[key] = {"lambda": lam, "residual_top_r": res["top"], "residual_sampled_r": res["sampled"]}
+    out["residual_exact_leverage"] = min(min(v["residual_top_r"], v["residual_sampled_r"])
+                                         for k, v in out.items() if k.startswith("deff_"))
+    del Z2
+    torch.cuda.empty_cache()
+    return out
 
 
 def solve_run(ctx, w, X, y, O, n_test, mixed_only=False):
@@ -733,6 +894,55 @@ def lu_run(ctx, n=8192, steps=3, cpu_n=4096):
     return out
 
 
+def potrf_run(ctx, n=16384, steps=3, cpu_n=4096):
+    """Cholesky leg (perftests/perftest_cholesky.cpp:46-84's workload and check): db200_potrf on the n x n matrix
+    A = min(i + 1, j + 1) = C C^T (C lower triangular of ones) resident in HBM, GFLOP/s = n^3 / 3 / time as the
+    perftest prints it (CUDA events, a fresh copy per step); the factor must be the upper triangle of ones (the
+    perftest checks A[n-1][n-1] = 1 to 1e-5; the FP64 factor of this integer matrix is exact, so the whole factor is
+    compared).  CPU baseline: the reference's own cholesky_factorize<float> (include/lapack_like.h:10-56, built
+    into oracle/_ref at one rank) on cpu_n x cpu_n."""
+    import ctypes
+    import torch
+    i = torch.arange(1, n + 1, device="cuda", dtype=torch.float64)
+    A0 = torch.minimum(i[:, None], i[None, :])  # symmetric: row or column major alike
+    A = torch.empty_like(A0)
+    stream = torch.cuda.current_stream()
+    A.copy_(A0)
+    ctx.potrf(n, A.data_ptr(), n)  # warm-up
+    times = []
+    for _ in range(steps):
+        A.copy_(A0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ctx.potrf(n, A.data_ptr(), n)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    ms = statistics.median(times)
+    # column-major upper factor = lower triangle of the row-major torch view
+    err = float((A - torch.tril(torch.ones_like(A))).abs().max())
+    out = {"workload": f"blocked upper Cholesky, n={n}, A = min(i+1, j+1) FP64 (perftest_cholesky)", "ms": ms,
+           "gflops": n ** 3 / 3.0 / (ms / 1e3) / 1e9, "a_last": float(A[n - 1, n - 1]),
+           "max_abs_err_vs_ones_factor": err}
+    del A, A0
+    torch.cuda.empty_cache()
+    ref_lib = ROOT / "oracle" / "_ref" / "libdarray_ref.so"
+    if ref_lib.exists():
+        lib = ctypes.CDLL(str(ref_lib))
+        fp = ctypes.POINTER(ctypes.c_float)
+        lib.ref_cholesky.argtypes = [fp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        ii = np.arange(1, cpu_n + 1, dtype=np.float32)
+        Ah = np.asfortranarray(np.minimum(ii[:, None], ii[None, :]))
+        t0 = time.perf_counter()
+        lib.ref_cholesky(Ah.ctypes.data_as(fp), cpu_n, 256, 0)
+        cs = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": cpu_n ** 3 / 3.0 / cs / 1e9, "unit": "GFLOP/s", "cores": os.cpu_count(),
+                               "kind": "reference", "a_last": float(Ah[cpu_n - 1, cpu_n - 1]),
+                               "sample": f"cholesky_factorize<float> 'U', n={cpu_n}, bs=256, one rank "
+                                         f"(OpenBLAS threads for its spotrf/strsm/ssyrk), {cs:.2f} s"}
+    return out
+
+
 def summarize(line):
     """The numbers a reader looks for first, gathered at the end of the JSON line (whose tail is what a truncated
     log keeps): the solve times, speed-ups and parities, the compensated and FP64 passes, the batch."""
@@ -765,6 +975,14 @@ def summarize(line):
     if bt:
         out.update({"batch_solves_per_s": bt.get("solves_per_s"), "batch_gap_pd_max": bt.get("gap_primal_dual_max"),
                     "batch_speedup_vs_sequential": bt.get("speedup_vs_sequential")})
+    db = line.get("dropin_block") or {}
+    if db:
+        out["dropin_block_s"] = db.get("s_per_block")
+    for key in ("potrf", "lu"):
+        leg = line.get(key) or {}
+        if leg:
+            out[f"{key}_gflops"] = leg.get("gflops")
+            out[f"{key}_cpu_gflops"] = (leg.get("cpu_baseline") or {}).get("value")
     return out
 
 
@@ -853,6 +1071,9 @@ def main():
                     help="add the LIBSVM input leg (C2 points as text, GPU reader vs the reference's reader)")
     ap.add_argument("--lu", action="store_true",
                     help="add the LU leg (n = 8192 FP32, partial pivoting; the reference's LU as CPU baseline)")
+    ap.add_argument("--potrf", action="store_true",
+                    help="add the Cholesky leg (n = 16384 FP64, perftest_cholesky's matrix; the reference's as CPU "
+                         "baseline)")
     ap.add_argument("--n-test", type=int, default=16384, help="held-out points for the solve leg's accuracy")
     ap.add_argument("--n", type=int, default=N_POINTS, help="points (default: the C2 workload, 131072)")
     ap.add_argument("--detail-out", default=None,

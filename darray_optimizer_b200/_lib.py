@@ -173,11 +173,26 @@ SIGNATURES = {
                                    ctypes.POINTER(_c_int)]),
 }
 
+# all-reduce callback of a row-sharded solve (include/darray_b200.h: db200_allreduce_fn)
+ALLREDUCE_FN = ctypes.CFUNCTYPE(_c_int, _vp, _vp, ctypes.c_longlong, _c_int, _vp)
+
+
+class Collective(ctypes.Structure):
+    _fields_ = [("world", _c_int), ("rank", _c_int), ("allreduce", ALLREDUCE_FN), ("user", _vp)]
+
+
+SIGNATURES.update({
+    "db200_set_collective": (_c_int, [_vp, ctypes.POINTER(Collective)]),
+    "db200_row_shard": (_c_int, [_c_int, _c_int, _c_int, ctypes.POINTER(_c_int), ctypes.POINTER(_c_int)]),
+})
+
 STATUS = {
     0: "DB200_OK", -1: "DB200_ERR_INVALID", -2: "DB200_ERR_CUDA", -3: "DB200_ERR_NOT_SPD",
     -4: "DB200_ERR_MAXITER", -5: "DB200_ERR_INFEASIBLE", -6: "DB200_ERR_TIMEOUT", -7: "DB200_ERR_NOMEM",
     -8: "DB200_ERR_UNSUPPORTED", -9: "DB200_ERR_TOO_LARGE", -10: "DB200_ERR_SINGULAR",
+    -11: "DB200_ERR_COLLECTIVE",
 }
+REDUCE_SUM, REDUCE_MAX, REDUCE_MIN = 0, 1, 2
 NOALLOC_SCRATCH_BYTES = 32 << 20
 # precisions of the SVM path and sketch products (include/darray_b200.h)
 MIXED, FP64, MIXED_FAST = 0, 1, 2
@@ -227,6 +242,14 @@ class Context:
         if st != 0:
             raise DB200Error(st, f"db200_create(device={device}) failed")
         self.h = h
+
+    def set_collective(self, world: int, rank: int, fn=None):
+        """Attach a row-sharding collective (fn: an ALLREDUCE_FN, kept alive here) or detach (world 1)."""
+        self._collective_fn = fn
+        if world <= 1 or fn is None:
+            return self.check(self.lib.db200_set_collective(self.h, None))
+        c = Collective(world, rank, fn, None)
+        return self.check(self.lib.db200_set_collective(self.h, ctypes.byref(c)))
 
     def check(self, st: int):
         if st != 0:

@@ -92,6 +92,16 @@ void* slot_buffer(db200_context* ctx, int slot, size_t bytes) {
   return ctx->slot[slot];
 }
 
+int allreduce(db200_context* ctx, double* buf, long long count, int op) {
+  if (!sharded(ctx) || count <= 0) return DB200_OK;
+  const int st = ctx->coll_fn(ctx->coll_user, buf, count, op, ctx->stream);
+  if (st != 0)
+    return fail(ctx, DB200_ERR_COLLECTIVE, "collective all-reduce of " + std::to_string(count) +
+                                               " values failed on rank " + std::to_string(ctx->coll_rank) +
+                                               " (status " + std::to_string(st) + ")");
+  return DB200_OK;
+}
+
 }  // namespace db200
 
 using namespace db200;
@@ -130,8 +140,9 @@ int db200_create(db200_context** out, int device, void* stream) {
   } else {
     ctx->stream = static_cast<cudaStream_t>(stream);  // NULL: the CUDA default stream
   }
-  if (cudaMalloc(&ctx->d_status, sizeof(int)) != cudaSuccess ||
-      cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream) != cudaSuccess ||
+  // [0] the status word, [1] the arrival counter of the blocked Cholesky's diagonal-block kernel, [2..3] spare
+  if (cudaMalloc(&ctx->d_status, 4 * sizeof(int)) != cudaSuccess ||
+      cudaMemsetAsync(ctx->d_status, 0, 4 * sizeof(int), ctx->stream) != cudaSuccess ||
       cudaMallocHost(&ctx->h_pinned, 4096) != cudaSuccess) {
     db200_destroy(ctx);
     return DB200_ERR_CUDA;
@@ -345,6 +356,32 @@ int db200_lra_host(db200_context* ctx, int n, int d, int k, const float* X, int 
     DB200_CUDA(ctx, cudaMemcpy2DAsync(A, sizeof(float) * lda, dA, sizeof(float) * n, sizeof(float) * n, k,
                                       cudaMemcpyDeviceToHost, ctx->stream));
   return db200_synchronize(ctx);
+}
+
+int db200_set_collective(db200_context* ctx, const db200_collective* c) {
+  if (!ctx) return DB200_ERR_INVALID;
+  if (!c || c->world <= 1) {
+    ctx->coll_world = 1;
+    ctx->coll_rank = 0;
+    ctx->coll_fn = nullptr;
+    ctx->coll_user = nullptr;
+    return DB200_OK;
+  }
+  if (c->rank < 0 || c->rank >= c->world || !c->allreduce)
+    return fail(ctx, DB200_ERR_INVALID, "set_collective: rank outside [0, world) or no all-reduce");
+  ctx->coll_world = c->world;
+  ctx->coll_rank = c->rank;
+  ctx->coll_fn = c->allreduce;
+  ctx->coll_user = c->user;
+  return DB200_OK;
+}
+
+int db200_row_shard(int n, int world, int rank, int* start, int* count) {
+  if (n < 0 || world < 1 || rank < 0 || rank >= world || !start || !count) return DB200_ERR_INVALID;
+  const int base = n / world, extra = n % world;
+  *count = base + (rank < extra ? 1 : 0);
+  *start = rank * base + (rank < extra ? rank : extra);
+  return DB200_OK;
 }
 
 }  // extern "C"

@@ -20,11 +20,6 @@ bool is_n(char c) { return c == 'N' || c == 'n'; }
 bool is_t(char c) { return c == 'T' || c == 't' || c == 'C' || c == 'c'; }
 }  // namespace
 
-namespace db200 {
-int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz, const float* y, double C,
-                     const db200_barrier_params& P, double* a, db200_svm_report* rep);
-}
-
 extern "C" {
 
 db200_context* db200_default_context(void) {

@@ -14,7 +14,8 @@ struct db200_context {
   int num_sms = 148;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
-  int* d_status = nullptr;       // device status word written by kernels whose bounded waits give up
+  int* d_status = nullptr;       // [0] device status word written by kernels whose bounded waits give up,
+                                 // [1] arrival counter of potrf_block_kernel (zero between launches)
   void* ws = nullptr;            // device workspace (packed operands, small factors)
   size_t ws_size = 0;
   void* io = nullptr;            // device staging for the host-pointer entry points
@@ -37,6 +38,10 @@ struct db200_context {
   // Optional per-launch timing of the tcgen05 tile kernels (CUDA events on the launching stream).
   bool profiling = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
+  // Row-sharded solves (db200_set_collective): the host's all-reduce; world 1 = none attached.
+  int coll_world = 1, coll_rank = 0;
+  db200_allreduce_fn coll_fn = nullptr;
+  void* coll_user = nullptr;
 };
 
 namespace db200 {
@@ -152,11 +157,23 @@ int launch_rbf_plan(db200_context* ctx, const TilePlan& plan);
 // ------------------------------------------------------------------ SVM pipeline pieces (svm.cpp)
 // Orthonormalise Y (n x l, FP64) in place by CholeskyQR2 (shifted CholeskyQR3 when the Gram is not positive
 // definite); R (l x l) optional.  tc_gram: Grams on the int8 tensor cores (Ozaki, 8 digits), else FP64 pipes.
-int cholqr2_impl(db200_context* ctx, int n, int l, double* Y, int ldy, double* Rout, int ldr, bool tc_gram);
-// Nystrom core: C = Q^T Yk (Yk = K Q), symmetrised; R^T R = C + nu I (shifted Cholesky); Z = Q R^T.
+// dist: Y holds this rank's rows of a row-sharded matrix and the Grams are all-reduced over the attached collective.
+int cholqr2_impl(db200_context* ctx, int n, int l, double* Y, int ldy, double* Rout, int ldr, bool tc_gram,
+                 bool dist = false);
+// Nystrom core: C = Q^T Yk (Yk = K Q), symmetrised; R^T R = C + nu I (shifted Cholesky); Z = Q R^T.  dist: Q, Yk
+// and Z are this rank's rows and C is all-reduced.
 template <typename TY>
 int nystrom_core(db200_context* ctx, int n, int l, const double* Q, const TY* Yk, double* Cm, double* R, int* d_pair,
-                 double* d_scalar, double* Z, int ldz, double* nu_out);
+                 double* d_scalar, double* Z, int ldz, double* nu_out, bool dist = false);
+// The log-barrier solve of db200_svm_barrier.  dist: Z, y and a are this rank's n rows of a row-sharded problem and
+// every reduction over rows goes through the attached collective.
+int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz, const float* y, double C,
+                     const db200_barrier_params& P, double* a, db200_svm_report* rep, bool dist = false);
+
+// Row-sharded solves: whether a collective of more than one rank is attached, and its all-reduce of `count` FP64
+// values at device address buf (in place, on the context's stream; a no-op when none is attached).
+inline bool sharded(const db200_context* ctx) { return ctx->coll_world > 1 && ctx->coll_fn; }
+int allreduce(db200_context* ctx, double* buf, long long count, int op);
 
 // Launch the fused tile kernel for one problem.  For RBF_MODE_SKETCH, `op` is the packed Omega^T and `out` is Y
 // (m x l, column major, leading dimension ldo); for RBF_MODE_KBLOCK, `out` is the kernel block K (m x n, column

@@ -243,27 +243,38 @@ __global__ void __launch_bounds__(GTHREADS, 1) tall_kernel(int n, int p, int q, 
 
 // One block column of the right-looking blocked upper Cholesky: the kb x kb diagonal block (kb <= 64) is factored
 // in every CTA (redundantly; 64 steps with one barrier each, the block's elements in registers, only a reciprocal
-// of the pivot on the sequential path, the row scaling by 1/sqrt(pivot) done for all rows afterwards), CTA 0 writes
-// R11 back (zeros below its diagonal), and CTA c >= 1 overwrites the 64 panel columns
-// [k0 + kb + 64 (c - 1), +64) with R11^-T A12 by forward substitution (one warp per 8 columns, the solution held
-// two rows per lane and broadcast by shuffles).  On a non-positive or NaN pivot nothing is written,
-// status <- DB200_ERR_NOT_SPD and *bad <- k0 (first failing block).  A block column after a failed one returns
-// at once.  Follows cholesky_factorize (include/lapack_like.h:10-57): potrf of the diagonal block, trsm of the
-// panel, syrk of the trailing matrix (the last is the DMMA gram_kernel launched after this one).
+// of the pivot on the sequential path, the row scaling by 1/sqrt(pivot) done for all rows afterwards), the last CTA
+// to have staged the block writes R11 back (zeros below its diagonal), and CTA c >= 1 overwrites the 64 panel
+// columns [k0 + kb + 64 (c - 1), +64) with R11^-T A12 by forward substitution (one warp per 8 columns, the
+// solution held two rows per lane and broadcast by shuffles).  The write-back waits for nothing: every CTA counts
+// itself in `arrivals` after staging A11, and the CTA that arrives last, when every other CTA has read A11, is
+// the one that overwrites it (and re-arms the counter for the next launch).  On a non-positive or NaN pivot
+// nothing is written, status <- DB200_ERR_NOT_SPD and *bad <- k0 (first failing block).  A block column after a
+// failed one writes nothing.  Follows cholesky_factorize (include/lapack_like.h:10-57): potrf of the diagonal
+// block, trsm of the panel, syrk of the trailing matrix (the DMMA gram_kernel or syrk_update_kernel launched after
+// this one).
 __global__ void __launch_bounds__(256) potrf_block_kernel(double* A, int lda, int k0, int kb, int l, int* status,
-                                                          int* bad) {
-  if (*(volatile int*)status) return;
+                                                          int* bad, int* arrivals) {
   __shared__ double rs[64][65];  // staging, then R11 (row-major: rs[i][j] = R[k0 + i][k0 + j])
   __shared__ double rowk[2][64];
   __shared__ double inv[64];
   __shared__ double dsq[64];
+  __shared__ int writer;
   const int t = threadIdx.x;
   // stage the diagonal block coalesced (column j contiguous in i)
   for (int e = t; e < 64 * 64; e += 256) {
     const int i = e & 63, j = e >> 6;
     rs[i][j] = (i < kb && j < kb && i <= j) ? A[(long long)(k0 + j) * lda + k0 + i] : 0.0;
   }
+  __syncthreads();  // this CTA's reads of A11 are done
+  if (t == 0) {
+    __threadfence();
+    const int before = atomicAdd(arrivals, 1);
+    writer = (before == (int)gridDim.x - 1);
+    if (writer) *arrivals = 0;  // every CTA has arrived: re-armed for the next launch
+  }
   __syncthreads();
+  if (*(volatile int*)status) return;  // an earlier block column failed (checked after counting in)
   // thread t owns column j = t & 63, rows i = rg + 4 q (q = 0..15)
   const int j = t & 63, rg = t >> 6;
   double a[16];
@@ -291,7 +302,7 @@ __global__ void __launch_bounds__(256) potrf_block_kernel(double* A, int lda, in
     if (rg == (k & 3)) rs[k][j] = (j >= k) ? own : 0.0;  // row k as eliminated (pivot at j == k)
   }
   if (failed) {
-    if (blockIdx.x == 0 && t == 0 && atomicCAS(status, 0, DB200_ERR_NOT_SPD) == 0) *bad = k0;
+    if (writer && t == 0 && atomicCAS(status, 0, DB200_ERR_NOT_SPD) == 0) *bad = k0;
     return;
   }
   // R[k][j] = a_kj / sqrt(a_kk), off the sequential path: square roots first, then every row in parallel
@@ -309,13 +320,13 @@ __global__ void __launch_bounds__(256) potrf_block_kernel(double* A, int lda, in
   __syncthreads();
   if (t < kb) rs[t][t] = dsq[t];
   __syncthreads();
-  if (blockIdx.x == 0) {
+  if (writer) {
     for (int e = t; e < kb * 64; e += 256) {
       const int i = e & 63, jj = e >> 6;
       if (i < kb) A[(long long)(k0 + jj) * lda + k0 + i] = (i <= jj) ? rs[i][jj] : 0.0;
     }
-    return;
   }
+  if (blockIdx.x == 0) return;
   // panel: x = R11^-T b for 8 columns per warp; lane holds rows lane and lane + 32
   const int warp = t >> 5, lane = t & 31;
   const int c0 = k0 + kb + (blockIdx.x - 1) * 64 + warp * 8;
@@ -812,19 +823,52 @@ template int gemm_tall<float, float>(db200_context*, int, int, int, const float*
 
 int potrf_upper(db200_context* ctx, double* A, int lda, int l, int* d_status, int* d_bad, int nb) {
   if (nb < 1 || nb > 64) nb = 64;
-  for (int k0 = 0; k0 < l; k0 += nb) {
-    const int kb = (l - k0 < nb) ? l - k0 : nb;
-    const int rest = l - k0 - kb;
-    potrf_block_kernel<<<1 + (rest + 63) / 64, 256, 0, ctx->stream>>>(A, lda, k0, kb, l, d_status, d_bad);
-    count_launch(ctx);
+  // the diagonal-block kernel's arrival counter starts every factorisation at zero
+  DB200_CUDA(ctx, cudaMemsetAsync(ctx->d_status + 1, 0, sizeof(int), ctx->stream));
+  // A trailing matrix of at least one wave of 128 x 128 upper tiles takes its update on the FP64 tensor cores
+  // (gram_kernel, alpha = -1, added in place).  While the matrix beyond the next 4 nb columns is that large, the
+  // factor goes by outer panels of 4 nb columns: each nb-block of the panel is factored (potrf_block_kernel, which
+  // also solves its row to the last column), the panel's own later rows are updated at once (a strip of at most
+  // 3 nb rows), and the trailing matrix takes one rank-4 nb update per panel instead of four rank-nb ones.
+  auto big = [&](int rest) {
+    const int tp = (rest + GT - 1) / GT;
+    return rest > 0 && tp * (tp + 1) / 2 >= ctx->num_sms;
+  };
+  for (int K0 = 0; K0 < l;) {
+    const int rest0 = l - K0;
+    const int KB = big(rest0 - 4 * nb) ? 4 * nb : (rest0 < nb ? rest0 : nb);
+    for (int k0 = K0; k0 < K0 + KB; k0 += nb) {
+      const int kb = (K0 + KB - k0 < nb) ? K0 + KB - k0 : nb;
+      const int rest = l - k0 - kb;
+      potrf_block_kernel<<<1 + (rest + 63) / 64, 256, 0, ctx->stream>>>(A, lda, k0, kb, l, d_status, d_bad,
+                                                                         ctx->d_status + 1);
+      count_launch(ctx);
+      const int pr = K0 + KB - (k0 + kb);  // rows of this panel below the block
+      if (pr > 0) {
+        const double* P = A + (long long)(k0 + kb) * lda + k0;
+        double* C = A + (long long)(k0 + kb) * lda + k0 + kb;
+        gram_kernel<double, double><<<dim3((pr + GT - 1) / GT, (rest + GT - 1) / GT, 1), GTHREADS, 0,
+                                      ctx->stream>>>(kb, pr, rest, P, lda, P, lda, nullptr, -1.0, C, lda, kb, 1, 0);
+        count_launch(ctx);
+      }
+    }
+    const int rest = l - K0 - KB;
     if (rest > 0) {
-      // trailing update A22 -= A12^T A12 (upper triangle only)
-      const int nt = (rest + 31) / 32;
-      syrk_update_kernel<<<nt * (nt + 1) / 2, 256, 0, ctx->stream>>>(A + (long long)(k0 + kb) * lda + k0, lda, kb,
-                                                                     rest, A + (long long)(k0 + kb) * lda + k0 + kb,
-                                                                     lda, d_status);
+      // trailing update A22 -= A12^T A12 (upper triangle only) with the panel's KB rows
+      const double* P = A + (long long)(K0 + KB) * lda + K0;
+      double* C = A + (long long)(K0 + KB) * lda + K0 + KB;
+      if (KB > nb || big(rest)) {
+        const int tp = (rest + GT - 1) / GT;
+        gram_kernel<double, double><<<dim3(tp, tp, 1), GTHREADS, 0, ctx->stream>>>(KB, rest, rest, P, lda, P, lda,
+                                                                                 nullptr, -1.0, C, lda, KB, 1, 0);
+      } else {
+        // the r ~ 500..2000 capacity factors of the barrier: 32 x 32 tiles, so that they spread over the GPU
+        const int nt = (rest + 31) / 32;
+        syrk_update_kernel<<<nt * (nt + 1) / 2, 256, 0, ctx->stream>>>(P, lda, KB, rest, C, lda, d_status);
+      }
       count_launch(ctx);
     }
+    K0 += KB;
   }
   zero_lower_kernel<<<grid_for((long long)l * l, 256, 1024), 256, 0, ctx->stream>>>(A, lda, l);
   count_launch(ctx);

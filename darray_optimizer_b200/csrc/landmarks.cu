@@ -914,6 +914,8 @@ int db200_svm_solve_landmarks(db200_context* ctx, int n, int d, int r, const flo
                               const db200_barrier_params* params, double* a, double* Z, int ldz, db200_svm_report* rep,
                               db200_landmark_report* lrep) {
   if (!ctx) return DB200_ERR_INVALID;
+  if (sharded(ctx))
+    return fail(ctx, DB200_ERR_UNSUPPORTED, "svm_solve_landmarks: not row-sharded (detach the collective first)");
   if (n < 2 || d < 1 || d > 128 || ldx < d || r < 1 || r > n || !X || !y || !net || net->in != d + 2 || s_knn < 9 ||
       s_res < 1 || !a || !Z || ldz < n || (Omega && (ldo < n || l_fb < 1 || l_fb > n)) || q < 0)
     return fail(ctx, DB200_ERR_INVALID, "svm_solve_landmarks: bad arguments (model input must be d + 2)");

@@ -62,10 +62,23 @@ int read_status(db200_context* ctx, int* d_pair, int* st, int* bad) {
   return DB200_OK;
 }
 
+// All-reduce k <= 64 host values over the attached collective through device scratch d_tmp (k doubles).
+int allreduce_host(db200_context* ctx, double* d_tmp, double* vals, int k, int op) {
+  if (!sharded(ctx)) return DB200_OK;
+  std::memcpy(ctx->h_pinned, vals, sizeof(double) * k);
+  DB200_CUDA(ctx, cudaMemcpyAsync(d_tmp, ctx->h_pinned, sizeof(double) * k, cudaMemcpyHostToDevice, ctx->stream));
+  int st = allreduce(ctx, d_tmp, k, op);
+  if (st) return st;
+  DB200_CUDA(ctx, cudaMemcpyAsync(ctx->h_pinned, d_tmp, sizeof(double) * k, cudaMemcpyDeviceToHost, ctx->stream));
+  DB200_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  std::memcpy(vals, ctx->h_pinned, sizeof(double) * k);
+  return DB200_OK;
+}
+
 // One CholeskyQR pass Yout = Yin R^-1 with R = chol(Yin^T Yin + shift I); returns NOT_SPD without touching Yout
 // when the Gram is not positive definite.  W, Rinv: l x l scratch; R (l x l) receives the factor.
 int cholqr_pass(db200_context* ctx, int n, int l, const double* Yin, int ldin, double* Yout, int ldout, double* R,
-                double* Rinv, double shift_rel, int* d_pair, double* d_scalar, bool tc_gram) {
+                double* Rinv, double shift_rel, int* d_pair, double* d_scalar, bool tc_gram, bool dist) {
   // Gram W = Y^T Y (upper triangle).  tc_gram: on the int8 tensor cores, 8 signed 7-bit digits per value, exact
   // integer products, error ~3e-14 of ||y_p|| ||y_q||; otherwise on the FP64 pipes.  The Cholesky stays FP64.
   int st = DB200_OK;
@@ -77,6 +90,8 @@ int cholqr_pass(db200_context* ctx, int n, int l, const double* Yin, int ldin, d
   } else if ((st = gram<double, double>(ctx, n, l, l, Yin, ldin, Yin, ldin, nullptr, 1.0, 0.0, R, l, true))) {
     return st;
   }
+  // row-sharded: the Gram of all rows is the sum of the ranks' Grams (upper triangles; the lower one is never read)
+  if (dist && (st = allreduce(ctx, R, (long long)l * l, DB200_REDUCE_SUM))) return st;
   if (shift_rel > 0.0) {
     // shift = shift_rel * trace(W)
     if ((st = trace(ctx, R, l, l, d_scalar))) return st;
@@ -97,7 +112,8 @@ int cholqr_pass(db200_context* ctx, int n, int l, const double* Yin, int ldin, d
 
 }  // namespace
 
-int cholqr2_impl(db200_context* ctx, int n, int l, double* Y, int ldy, double* Rout, int ldr, bool tc_gram) {
+int cholqr2_impl(db200_context* ctx, int n, int l, double* Y, int ldy, double* Rout, int ldr, bool tc_gram,
+                 bool dist) {
   // slot layout: [pair | scalar | T (n x l) | R1 | R2 | R3 | Rinv | Racc]
   const size_t ll = (size_t)l * l;
   const size_t bytes = 1024 + align_up((size_t)n * l * 8, 256) + 5 * align_up(ll * 8, 256) + 1024;
@@ -112,24 +128,26 @@ int cholqr2_impl(db200_context* ctx, int n, int l, double* Y, int ldy, double* R
   double* R3 = cv.take<double>(ll);
   double* Rinv = cv.take<double>(ll);
   double* Racc = cv.take<double>(ll);
-  int st = cholqr_pass(ctx, n, l, Y, ldy, T, n, R1, Rinv, 0.0, d_pair, d_scalar, tc_gram);
+  int st = cholqr_pass(ctx, n, l, Y, ldy, T, n, R1, Rinv, 0.0, d_pair, d_scalar, tc_gram, dist);
   bool shifted = false;
   if (st == DB200_ERR_NOT_SPD) {
     // shifted CholeskyQR3 (Fukaya, Kannan, Nakatsukasa, Yamamoto, Yanagisawa 2020): first pass with
-    // shift 11 (n l + l (l + 1)) u ||Y||^2, ||Y||_2^2 <= trace(Y^T Y)
+    // shift 11 (n l + l (l + 1)) u ||Y||^2, ||Y||_2^2 <= trace(Y^T Y); n counts the rows of every rank
+    double rows = n;
+    if (dist && (st = allreduce_host(ctx, d_scalar, &rows, 1, DB200_REDUCE_SUM))) return st;
     const double u = 1.1102230246251565e-16;
-    const double rel = 11.0 * ((double)n * l + (double)l * (l + 1)) * u;
-    st = cholqr_pass(ctx, n, l, Y, ldy, T, n, R1, Rinv, rel, d_pair, d_scalar, tc_gram);
+    const double rel = 11.0 * (rows * l + (double)l * (l + 1)) * u;
+    st = cholqr_pass(ctx, n, l, Y, ldy, T, n, R1, Rinv, rel, d_pair, d_scalar, tc_gram, dist);
     shifted = true;
   }
   if (st) return st;
   // second pass T -> Y
-  if ((st = cholqr_pass(ctx, n, l, T, n, Y, ldy, R2, Rinv, 0.0, d_pair, d_scalar, tc_gram))) return st;
+  if ((st = cholqr_pass(ctx, n, l, T, n, Y, ldy, R2, Rinv, 0.0, d_pair, d_scalar, tc_gram, dist))) return st;
   // R = R2 R1 (upper * upper)
   if ((st = gemm_tall<double, double>(ctx, l, l, l, R2, l, R1, l, false, 0.0, Racc, l))) return st;
   if (shifted) {
     // third pass Y -> T, then copy back; R = R3 (R2 R1)
-    if ((st = cholqr_pass(ctx, n, l, Y, ldy, T, n, R3, Rinv, 0.0, d_pair, d_scalar, tc_gram))) return st;
+    if ((st = cholqr_pass(ctx, n, l, Y, ldy, T, n, R3, Rinv, 0.0, d_pair, d_scalar, tc_gram, dist))) return st;
     DB200_CUDA(ctx, cudaMemcpy2DAsync(Y, sizeof(double) * ldy, T, sizeof(double) * n, sizeof(double) * n, l,
                                       cudaMemcpyDeviceToDevice, ctx->stream));
     if ((st = gemm_tall<double, double>(ctx, l, l, l, R3, l, Racc, l, false, 0.0, R1, l))) return st;
@@ -145,12 +163,8 @@ int cholqr2_impl(db200_context* ctx, int n, int l, double* Y, int ldy, double* R
 // ---------------------------------------------------------------------------------------------- barrier
 namespace {
 
-__attribute__((unused)) void set_a0_host(const std::vector<float>& y, double C, double* pval, double* mval) {
-  long plus = 0, minus = 0;
-  for (float v : y) {
-    if (v == 1.0f) ++plus;
-    else ++minus;
-  }
+// Class-balanced start (tests/testsvm.cpp:192-212) from the class counts.
+void set_a0_counts(double plus, double minus, double C, double* pval, double* mval) {
   if (plus > minus) {
     *mval = 0.9 * C;
     *pval = minus > 0 ? *mval * minus / plus : *mval;
@@ -163,7 +177,7 @@ __attribute__((unused)) void set_a0_host(const std::vector<float>& y, double C, 
 }  // namespace
 
 int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz, const float* y, double C,
-                     const db200_barrier_params& P, double* a, db200_svm_report* rep) {
+                     const db200_barrier_params& P, double* a, db200_svm_report* rep, bool dist) {
   if (r > 4096) return fail(ctx, DB200_ERR_UNSUPPORTED, "svm_barrier: r > 4096");
   EventTimer timer(ctx->stream);
   const size_t rr = (size_t)r * r;
@@ -204,22 +218,42 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
   constexpr int kSlices[2] = {6, 8};
   int tc_level = (r >= 2048) ? 0 : 1;  // index into kSlices; 2 = FP64
   bool tc_ok = true;
+  int st0 = DB200_OK;
 
-  // class-balanced start (tests/testsvm.cpp:192-212)
+  // Reductions over rows: at one rank the kernels' own sums; row-sharded, all-reduced over the ranks (the
+  // r-vectors Z^T x, the capacity matrix and the scalar sums, maxima and minima), so that every rank takes the same
+  // decisions.
+  auto reduce = [&](double* buf, long long count, int op) -> int {
+    return dist ? allreduce(ctx, buf, count, op) : DB200_OK;
+  };
+  auto gemv_t = [&](const double* v, const double* scale, double sign, double* out) -> int {
+    int s2 = bar_gemv_t(ctx, n, r, Z, ldz, v, scale, sign, out);
+    return s2 ? s2 : reduce(out, r, DB200_REDUCE_SUM);
+  };
+  // red after bar_grad_hess: [0] sum a, [1] sum logs, [2] max D, [3] min D
+  auto reduce_grad = [&]() -> int {
+    int s2 = reduce(red, 2, DB200_REDUCE_SUM);
+    if (!s2) s2 = reduce(red + 2, 1, DB200_REDUCE_MAX);
+    return s2 ? s2 : reduce(red + 3, 1, DB200_REDUCE_MIN);
+  };
+
+  // class-balanced start (tests/testsvm.cpp:192-212) from the class counts of all rows
   std::vector<float> hy(n);
   DB200_CUDA(ctx, cudaMemcpyAsync(hy.data(), y, sizeof(float) * n, cudaMemcpyDeviceToHost, ctx->stream));
   DB200_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  double counts[2] = {0.0, (double)n};  // [plus, rows]
+  for (int i = 0; i < n; ++i) counts[0] += hy[i] == 1.0f;
+  if (dist && (st0 = allreduce_host(ctx, red, counts, 2, DB200_REDUCE_SUM))) return st0;
+  const double n_all = counts[1];  // rows of every rank
   double pval = 0, mval = 0;
-  set_a0_host(hy, C, &pval, &mval);
+  set_a0_counts(counts[0], n_all - counts[0], C, &pval, &mval);
   {
     std::vector<double> ha(n), hyd(n);
-    long plus = 0;
     for (int i = 0; i < n; ++i) {
       ha[i] = (hy[i] == 1.0f) ? pval : mval;
       hyd[i] = (hy[i] == 1.0f) ? 1.0 : -1.0;
-      plus += hy[i] == 1.0f;
     }
-    if (P.bias && (plus == 0 || plus == n))
+    if (P.bias && (counts[0] == 0 || counts[0] == n_all))
       return fail(ctx, DB200_ERR_INFEASIBLE, "svm_barrier: the bias needs both classes (y^T a = 0)");
     DB200_CUDA(ctx, cudaMemcpyAsync(a, ha.data(), sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
     if (P.bias)
@@ -255,11 +289,12 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
         if ((st = bar_init_red(ctx, red, 2, 1, 1))) return st;
         if ((st = bar_grad_hess(ctx, n, r, Z, ldz, w, a, C, t, g, dinv, red, zw, nullptr))) return st;
       } else {
-        if ((st = bar_gemv_t(ctx, n, r, Z, ldz, a, nullptr, 1.0, w))) return st;
+        if ((st = gemv_t(a, nullptr, 1.0, w))) return st;
         if ((st = bar_init_red(ctx, red, 2, 1, 1))) return st;
         if ((st = bar_grad_hess(ctx, n, r, Z, ldz, w, a, C, t, g, dinv, red, nullptr, zw))) return st;
         zw_ok = true;
       }
+      if ((st = reduce_grad())) return st;
       if ((st = bar_dot(ctx, r, w, w, sc))) return st;
       DB200_CUDA(ctx, cudaMemcpyAsync(red + 8, sc, sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
       if ((st = fetch(red, 9))) return st;
@@ -281,6 +316,7 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
         } else {
           if ((s2 = gram<double, double>(ctx, n, r, r, Z, ldz, Z, ldz, dinv, 1.0, 0.0, M, r, true))) return s2;
         }
+        if ((s2 = reduce(M, (long long)rr, DB200_REDUCE_SUM))) return s2;  // upper triangles summed
         if ((s2 = bar_add_identity(ctx, M, r, r))) return s2;
         // A capacity matrix with a huge dynamic range (late in the barrier D^-1 spans ~18 orders) can sit on the
         // edge of numerical positive definiteness: its last bits (the Gram's rounding and the order of its
@@ -308,7 +344,7 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
       auto solve = [&](const double* rhs, double* out, bool use_tc, bool* converged, bool track_v) -> int {
         int s2;
         *converged = true;
-        if ((s2 = bar_gemv_t(ctx, n, r, Z, ldz, rhs, dinv, -1.0, u))) return s2;
+        if ((s2 = gemv_t(rhs, dinv, -1.0, u))) return s2;
         if ((s2 = trsv_upper(ctx, M, L, r, r, u, true))) return s2;   // R^T z = rhs
         if ((s2 = trsv_upper(ctx, M, L, r, r, u, false))) return s2;  // R u = z
         if ((s2 = bar_init_red(ctx, red, 2, 0, 1))) return s2;
@@ -317,9 +353,10 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
         *converged = false;
         double prev = 0.0;
         for (int it = 0; it <= P.refine_max; ++it) {
-          if ((s2 = bar_gemv_t(ctx, n, r, Z, ldz, out, nullptr, 1.0, v))) return s2;
+          if ((s2 = gemv_t(out, nullptr, 1.0, v))) return s2;
           if ((s2 = bar_init_red(ctx, red + 16, 2, 0, 0))) return s2;
           if ((s2 = bar_residual(ctx, n, r, Z, ldz, v, rhs, dinv, out, res, red + 16, zv))) return s2;
+          if ((s2 = reduce(red + 16, 2, DB200_REDUCE_SUM))) return s2;
           if ((s2 = fetch(red + 16, 2))) return s2;
           const double rn = std::sqrt(h[0]), gn = std::sqrt(h[1]);
           if (rn <= 1e-10 * gn) {
@@ -329,7 +366,7 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
           }
           if (it == P.refine_max || (it > 0 && rn >= 0.5 * prev) || !std::isfinite(rn)) break;
           prev = rn;
-          if ((s2 = bar_gemv_t(ctx, n, r, Z, ldz, res, dinv, -1.0, u))) return s2;
+          if ((s2 = gemv_t(res, dinv, -1.0, u))) return s2;
           if ((s2 = trsv_upper(ctx, M, L, r, r, u, true))) return s2;
           if ((s2 = trsv_upper(ctx, M, L, r, r, u, false))) return s2;
           if ((s2 = bar_init_red(ctx, red + 16, 2, 0, 1))) return s2;
@@ -342,7 +379,7 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
       // out = -H~^-1 rhs: one Woodbury application of the factored capacity matrix, no refinement.
       auto apply = [&](const double* rhs, double* out, double* rd) -> int {
         int s2;
-        if ((s2 = bar_gemv_t(ctx, n, r, Z, ldz, rhs, dinv, -1.0, u))) return s2;
+        if ((s2 = gemv_t(rhs, dinv, -1.0, u))) return s2;
         if ((s2 = trsv_upper(ctx, M, L, r, r, u, true))) return s2;
         if ((s2 = trsv_upper(ctx, M, L, r, r, u, false))) return s2;
         if ((s2 = bar_init_red(ctx, rd, 2, 0, 1))) return s2;
@@ -371,6 +408,7 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
         if ((s2 = apply(yd, sy, red + 16))) return s2;
         if ((s2 = bar_dot(ctx, n, yd, s, sc + 4))) return s2;
         if ((s2 = bar_dot(ctx, n, yd, sy, sc + 5))) return s2;
+        if ((s2 = reduce(sc + 4, 2, DB200_REDUCE_SUM))) return s2;
         if ((s2 = fetch(sc + 4, 2))) return s2;
         const double ysy = h[1];
         if (ysy == 0.0 || !std::isfinite(ysy))
@@ -383,9 +421,10 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
           for (int it = 0; it <= P.refine_max; ++it) {
             DB200_CUDA(ctx, cudaMemcpyAsync(gb, g, sizeof(double) * n, cudaMemcpyDeviceToDevice, ctx->stream));
             if ((s2 = bar_axpy(ctx, n, nu, yd, gb))) return s2;
-            if ((s2 = bar_gemv_t(ctx, n, r, Z, ldz, s, nullptr, 1.0, v))) return s2;
+            if ((s2 = gemv_t(s, nullptr, 1.0, v))) return s2;
             if ((s2 = bar_init_red(ctx, red + 16, 2, 0, 0))) return s2;
             if ((s2 = bar_residual(ctx, n, r, Z, ldz, v, gb, dinv, s, res, red + 16, zv))) return s2;
+            if ((s2 = reduce(red + 16, 2, DB200_REDUCE_SUM))) return s2;
             if ((s2 = fetch(red + 16, 2))) return s2;
             const double rn = std::sqrt(h[0]), gn = std::sqrt(h[1]);
             if (rn <= 1e-10 * gn) {
@@ -398,6 +437,7 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
             if ((s2 = apply(res, delta, red + 16))) return s2;
             if ((s2 = bar_axpy(ctx, n, 1.0, delta, s))) return s2;
             if ((s2 = bar_dot(ctx, n, yd, s, sc + 6))) return s2;
+            if ((s2 = reduce(sc + 6, 1, DB200_REDUCE_SUM))) return s2;
             if ((s2 = fetch(sc + 6, 1))) return s2;
             const double dnu = -h[0] / ysy;
             if ((s2 = bar_axpy(ctx, n, dnu, sy, s))) return s2;
@@ -427,7 +467,9 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
         v_current = false;
         if ((st = newton_dir(false, &conv))) return st;
       }
-      if (!v_current && (st = bar_gemv_t(ctx, n, r, Z, ldz, s, nullptr, 1.0, v))) return st;
+      if (!v_current && (st = gemv_t(s, nullptr, 1.0, v))) return st;
+      // direction statistics of s: [0] g.s, [1] sum s, [2] largest step inside the box
+      if ((st = reduce(red, 2, DB200_REDUCE_SUM)) || (st = reduce(red + 2, 1, DB200_REDUCE_MIN))) return st;
       if ((st = bar_dot(ctx, r, w, v, sc + 1))) return st;
       if ((st = bar_dot(ctx, r, v, v, sc + 2))) return st;
       DB200_CUDA(ctx, cudaMemcpyAsync(red + 8, sc + 1, 2 * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
@@ -446,6 +488,7 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
         for (int k = 0; k < 16; ++k) ht[k] = tau * std::pow(P.beta, k);
         DB200_CUDA(ctx, cudaMemcpyAsync(taus, ht, sizeof(ht), cudaMemcpyHostToDevice, ctx->stream));
         if ((st = bar_linesearch16(ctx, n, a, s, C, taus, ls))) return st;
+        if ((st = reduce(ls, 32, DB200_REDUCE_SUM))) return st;
         if ((st = fetch(ls, 32))) return st;
         for (int k = 0; k < 16; ++k) {
           if (h[16 + k] != 0.0) continue;  // leaves the box
@@ -478,20 +521,24 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
       }
     }
     // f(a) for the barrier stop
-    if ((st = bar_gemv_t(ctx, n, r, Z, ldz, a, nullptr, 1.0, w))) return st;
+    if ((st = gemv_t(a, nullptr, 1.0, w))) return st;
     if ((st = bar_init_red(ctx, red, 2, 1, 1))) return st;
     if ((st = bar_grad_hess(ctx, n, r, Z, ldz, w, a, C, t, g, dinv, red, nullptr, zw))) return st;
+    if ((st = reduce_grad())) return st;
     zw_ok = true;
     if ((st = bar_dot(ctx, r, w, w, sc))) return st;
     DB200_CUDA(ctx, cudaMemcpyAsync(red + 8, sc, sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
     if ((st = fetch(red, 9))) return st;
     suma_now = h[0];
     fa = 0.5 * h[8] - suma_now;
-    if (2.0 * n / t < P.gap_tol * std::fabs(fa)) {
+    if (2.0 * n_all / t < P.gap_tol * std::fabs(fa)) {
       // The barrier bound is met.  Stop once the true primal-dual gap at w = Z^T a is within tolerance too, or
-      // when a further outer step no longer halves it (it is then limited by the inexact Newton solves, not t).
+      // when a further outer step no longer halves it (it is then limited by the conditioning of the Newton
+      // systems at large t, not by t: the plain-FP64 barrier stalls at the same gap, and a 10^6-fold tighter inner
+      // Newton stop does not move it).
       if ((st = bar_dot(ctx, r, w, w, sc))) return st;
       if ((st = bar_hinge(ctx, n, r, Z, ldz, w, sc + 3, P.bias ? yd : nullptr, bias_nu))) return st;
+      if ((st = reduce(sc + 3, 1, DB200_REDUCE_SUM))) return st;
       if ((st = fetch(sc, 4))) return st;
       const double pd = (0.5 * h[0] + C * h[3] + fa) / std::fabs(fa);
       if (pd < P.gap_tol || (prev_pd >= 0 && pd > 0.5 * prev_pd)) break;
@@ -505,6 +552,7 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
   }
   // primal-dual gap at w = Z^T a (w is current), with the bias when the dual carries y^T a = 0
   if ((st = bar_hinge(ctx, n, r, Z, ldz, w, sc + 3, P.bias ? yd : nullptr, bias_nu))) return st;
+  if ((st = reduce(sc + 3, 1, DB200_REDUCE_SUM))) return st;
   if ((st = fetch(sc, 4))) return st;
   const double primal = 0.5 * h[0] + C * h[3];
   if (rep) {
@@ -512,7 +560,7 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
     rep->t = t;
     rep->outer = outer;
     rep->newton = total_newton;
-    rep->gap_barrier = 2.0 * n / t / std::fabs(fa);
+    rep->gap_barrier = 2.0 * n_all / t / std::fabs(fa);
     rep->gap_primal_dual = (primal + fa) / std::fabs(fa);
     rep->status = status;
     rep->refine = refine_total;
@@ -526,10 +574,11 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
 // ---------------------------------------------------------------------------------------------- low rank
 template <typename TY>
 int nystrom_core(db200_context* ctx, int n, int l, const double* Q, const TY* Yk, double* Cm, double* R, int* d_pair,
-                 double* d_scalar, double* Z, int ldz, double* nu_out) {
+                 double* d_scalar, double* Z, int ldz, double* nu_out, bool dist) {
   // C = Q^T (K Q), symmetrised; R^T R = C + nu I with nu = 1e-7 trace(C)/l, x10 until positive definite
   int st = gram<double, TY>(ctx, n, l, l, Q, n, Yk, n, nullptr, 1.0, 0.0, Cm, l, false);
   if (st) return st;
+  if (dist && (st = allreduce(ctx, Cm, (long long)l * l, DB200_REDUCE_SUM))) return st;
   if ((st = symmetrize(ctx, Cm, l, l, 0.0))) return st;
   if ((st = trace(ctx, Cm, l, l, d_scalar))) return st;
   double tr = 0;
@@ -554,81 +603,102 @@ int nystrom_core(db200_context* ctx, int n, int l, const double* Q, const TY* Yk
   return DB200_OK;
 }
 template int nystrom_core<float>(db200_context*, int, int, const double*, const float*, double*, double*, int*,
-                                 double*, double*, int, double*);
+                                 double*, double*, int, double*, bool);
 template int nystrom_core<double>(db200_context*, int, int, const double*, const double*, double*, double*, int*,
-                                  double*, double*, int, double*);
+                                  double*, double*, int, double*, bool);
 
 int lowrank_impl(db200_context* ctx, int n, int d, int l, int q, const float* X, int ldx, const float* y,
-                 const float* Omega, int ldo, float gamma, int precision, double* Z, int ldz, db200_svm_report* rep) {
+                 const float* Omega, int ldo, float gamma, int precision, double* Z, int ldz, db200_svm_report* rep,
+                 bool dist) {
   if (l > n) return fail(ctx, DB200_ERR_INVALID, "lowrank: l > n");
   const bool fp64 = (precision == DB200_FP64);
-  const size_t nl = (size_t)n * l, ll = (size_t)l * l;
-  const size_t bytes = 4096 + 2 * align_up(nl * 4, 256) + 2 * align_up(nl * 8, 256) + 3 * align_up(ll * 8, 256) + 4096;
+  // this rank's rows [s0, s0 + m) of Y, Q and Z (all n rows at one rank)
+  int s0 = 0, m = n;
+  if (dist) {
+    db200_row_shard(n, ctx->coll_world, ctx->coll_rank, &s0, &m);
+    if (m < 1) return fail(ctx, DB200_ERR_INVALID, "lowrank: fewer points than ranks");
+  }
+  const float* Xi = X + (size_t)s0 * ldx;
+  const float* yi = y + s0;
+  const size_t ml = (size_t)m * l, nl = (size_t)n * l, ll = (size_t)l * l;
+  // Qg: all rows of Q (FP64) for the next pass, gathered from the ranks; at one rank Q itself is complete
+  const size_t bytes = 4096 + align_up(ml * 4, 256) + align_up(nl * 4, 256) + 2 * align_up(ml * 8, 256) +
+                       (dist ? align_up(nl * 8, 256) : 0) + 3 * align_up(ll * 8, 256) + 4096;
   char* base = static_cast<char*>(slot_buffer(ctx, SLOT_PIPE, bytes));
   if (!base) return DB200_ERR_NOMEM;
   Carve cv{base};
   int* d_pair = cv.take<int>(4);
   double* d_scalar = cv.take<double>(4);
-  float* Y32 = cv.take<float>(nl);  // mixed: kernel-pass output (fp32 accumulation)
-  float* Qf = cv.take<float>(nl);   // mixed: Q as the next pass's test matrix
-  double* Q = cv.take<double>(nl);
-  double* Y64 = cv.take<double>(nl);  // FP64: kernel-pass output
+  float* Y32 = cv.take<float>(ml);  // mixed: kernel-pass output (fp32 accumulation)
+  float* Qf = cv.take<float>(nl);   // mixed: all rows of Q as the next pass's test matrix
+  double* Q = cv.take<double>(ml);
+  double* Y64 = cv.take<double>(ml);  // FP64: kernel-pass output
+  double* Qg = dist ? cv.take<double>(nl) : Q;
   double* Cm = cv.take<double>(ll);
   double* R = cv.take<double>(ll);
   double ms_sketch = 0, ms_orth = 0, ms_core = 0;
   int st;
 
-  // one pass Y = diag(y) K diag(y) Om, into Y32 (mixed) or Y64 (FP64).  Mixed: the compensated sketch product with
-  // promoted accumulation; the range-finder passes (whose subspace, not scale, matters) in 1024-point chunks, the
-  // final pass, whose Y scales the core C = Q^T K Q, in 256-point chunks.  Measured dual-objective distance from
-  // the FP64 path: 5e-7 at n = 4096 (1.6e-6 with coarse chunks in the final pass) and 4e-7 at n = 131072
+  // one pass Y = diag(y) K diag(y) Om over this rank's rows, into Y32 (mixed) or Y64 (FP64).  Mixed: the compensated
+  // sketch product with promoted accumulation; the range-finder passes (whose subspace, not scale, matters) in
+  // 1024-point chunks, the final pass, whose Y scales the core C = Q^T K Q, in 256-point chunks.  Measured
+  // dual-objective distance from the FP64 path: 5e-7 at n = 4096 (1.6e-6 with coarse chunks in the final pass) and
+  // 4e-7 at n = 131072
   auto sketch_f32 = [&](const float* Om, int ldom, bool final_pass) -> int {
     EventTimer tm(ctx->stream);
     const int product = precision == DB200_MIXED_FAST ? DB200_SKETCH_SINGLE
                         : final_pass                  ? DB200_SKETCH_COMPENSATED_PROMOTED
                                                       : DB200_SKETCH_COMPENSATED_PROMOTED_COARSE;
-    int s2 = db200_rbf_sketch_ex(ctx, n, n, d, l, X, ldx, X, ldx, DB200_POINT_MAJOR, y, y, Om, ldom, Y32, n, gamma,
+    int s2 = db200_rbf_sketch_ex(ctx, m, n, d, l, Xi, ldx, X, ldx, DB200_POINT_MAJOR, yi, y, Om, ldom, Y32, m, gamma,
                                  product);
     ms_sketch += tm.stop_ms();
     return s2;
   };
   auto sketch_f64 = [&](const double* Om, int ldom) -> int {
     EventTimer tm(ctx->stream);
-    int s2 = db200_rbf_sketch_f64(ctx, n, n, d, l, X, ldx, X, ldx, y, y, Om, ldom, Y64, n, gamma);
+    int s2 = db200_rbf_sketch_f64(ctx, m, n, d, l, Xi, ldx, X, ldx, yi, y, Om, ldom, Y64, m, gamma);
     ms_sketch += tm.stop_ms();
     return s2;
   };
   auto orth = [&]() -> int {
     EventTimer tm(ctx->stream);
-    int s2 = fp64 ? DB200_OK : convert<float, double>(ctx, Y32, n, Q, n, n, l);
+    int s2 = fp64 ? DB200_OK : convert<float, double>(ctx, Y32, m, Q, m, m, l);
     if (!s2 && fp64)
-      s2 = (cudaMemcpyAsync(Q, Y64, sizeof(double) * nl, cudaMemcpyDeviceToDevice, ctx->stream) == cudaSuccess)
+      s2 = (cudaMemcpyAsync(Q, Y64, sizeof(double) * ml, cudaMemcpyDeviceToDevice, ctx->stream) == cudaSuccess)
                ? DB200_OK
                : DB200_ERR_CUDA;
     // int8 Grams from n = 65536 (C2: CholeskyQR2 35 -> 28 ms, C3 207 -> 160 ms); below, the slicing's fixed
-    // cost outweighs the FP64 Gram
-    if (!s2) s2 = cholqr2_impl(ctx, n, l, Q, n, nullptr, 0, !fp64 && n >= 65536);
-    if (!s2 && !fp64) s2 = convert<double, float>(ctx, Q, n, Qf, n, n, l);
+    // cost outweighs the FP64 Gram.  Decided on the global n, the same at every rank.
+    if (!s2) s2 = cholqr2_impl(ctx, m, l, Q, m, nullptr, 0, !fp64 && n >= 65536, dist);
+    if (!s2 && dist) {
+      // all rows of Q: each rank's block at its offset in a zero matrix, summed over the ranks
+      if (cudaMemsetAsync(Qg, 0, sizeof(double) * nl, ctx->stream) != cudaSuccess ||
+          cudaMemcpy2DAsync(Qg + s0, sizeof(double) * n, Q, sizeof(double) * m, sizeof(double) * m, l,
+                            cudaMemcpyDeviceToDevice, ctx->stream) != cudaSuccess)
+        s2 = cuda_fail(ctx, cudaGetLastError(), "lowrank: gather Q");
+      if (!s2) s2 = allreduce(ctx, Qg, (long long)nl, DB200_REDUCE_SUM);
+    }
+    if (!s2 && !fp64) s2 = convert<double, float>(ctx, Qg, n, Qf, n, n, l);
     ms_orth += tm.stop_ms();
     return s2;
   };
   if (fp64) {
-    // the FP64 comparator takes Omega in FP64
-    if ((st = convert<float, double>(ctx, Omega, ldo, Q, n, n, l))) return st;
-    if ((st = sketch_f64(Q, n))) return st;
+    // the FP64 comparator takes Omega in FP64 (all rows, in Qg: Q itself at one rank)
+    if ((st = convert<float, double>(ctx, Omega, ldo, Qg, n, n, l))) return st;
+    if ((st = sketch_f64(Qg, n))) return st;
   } else {
     if ((st = sketch_f32(Omega, ldo, false))) return st;
   }
   if ((st = orth())) return st;
   for (int it = 0; it < q; ++it) {
-    if ((st = fp64 ? sketch_f64(Q, n) : sketch_f32(Qf, n, false))) return st;
+    if ((st = fp64 ? sketch_f64(Qg, n) : sketch_f32(Qf, n, false))) return st;
     if ((st = orth())) return st;
   }
-  if ((st = fp64 ? sketch_f64(Q, n) : sketch_f32(Qf, n, true))) return st;  // Y = K Q
+  if ((st = fp64 ? sketch_f64(Qg, n) : sketch_f32(Qf, n, true))) return st;  // Y = K Q (this rank's rows)
   EventTimer tcore(ctx->stream);
   double nu = 0;
-  st = fp64 ? nystrom_core<double>(ctx, n, l, Q, Y64, Cm, R, d_pair, d_scalar, Z, ldz, &nu)
-            : nystrom_core<float>(ctx, n, l, Q, Y32, Cm, R, d_pair, d_scalar, Z, ldz, &nu);
+  st = fp64 ? nystrom_core<double>(ctx, m, l, Q, Y64, Cm, R, d_pair, d_scalar, Z, ldz, &nu, dist)
+            : nystrom_core<float>(ctx, m, l, Q, Y32, Cm, R, d_pair, d_scalar, Z, ldz, &nu, dist);
   if (st) return st;
   ms_core = tcore.stop_ms();
   if (rep) {
@@ -719,7 +789,7 @@ int db200_svm_barrier(db200_context* ctx, int n, int r, const double* Z, int ldz
   db200_barrier_params P;
   if (p) P = *p;
   else db200_barrier_defaults(&P);
-  int st = svm_barrier_impl(ctx, n, r, Z, ldz, y, C, P, a, rep);
+  int st = svm_barrier_impl(ctx, n, r, Z, ldz, y, C, P, a, rep, sharded(ctx));
   if (st && st != DB200_ERR_MAXITER) return st;
   int s2 = db200_synchronize(ctx);
   return s2 ? s2 : st;
@@ -728,10 +798,12 @@ int db200_svm_barrier(db200_context* ctx, int n, int r, const double* Z, int ldz
 int db200_lowrank(db200_context* ctx, int n, int d, int l, int q, const float* X, int ldx, const float* y,
                   const float* Omega, int ldo, float gamma, int precision, double* Z, int ldz, db200_svm_report* rep) {
   if (!ctx) return DB200_ERR_INVALID;
-  if (n < 1 || d < 1 || l < 1 || q < 0 || !X || ldx < d || !y || !Omega || ldo < n || !Z || ldz < n ||
+  int s0 = 0, rows = n;  // rows of Z this rank writes
+  if (sharded(ctx) && n >= 0) db200_row_shard(n, ctx->coll_world, ctx->coll_rank, &s0, &rows);
+  if (n < 1 || d < 1 || l < 1 || q < 0 || !X || ldx < d || !y || !Omega || ldo < n || !Z || ldz < rows ||
       (precision != DB200_MIXED && precision != DB200_FP64 && precision != DB200_MIXED_FAST))
     return fail(ctx, DB200_ERR_INVALID, "lowrank: bad arguments");
-  int st = lowrank_impl(ctx, n, d, l, q, X, ldx, y, Omega, ldo, gamma, precision, Z, ldz, rep);
+  int st = lowrank_impl(ctx, n, d, l, q, X, ldx, y, Omega, ldo, gamma, precision, Z, ldz, rep, sharded(ctx));
   if (st) return st;
   return db200_synchronize(ctx);
 }
@@ -748,7 +820,10 @@ int db200_svm_solve(db200_context* ctx, int n, int d, int l, int q, const float*
   else db200_barrier_defaults(&P);
   int st = db200_lowrank(ctx, n, d, l, q, X, ldx, y, Omega, ldo, gamma, P.precision, Z, ldz, &local);
   if (st) return st;
-  st = db200_svm_barrier(ctx, n, l, Z, ldz, y, C, &P, a, &local);
+  // row-sharded: the barrier runs over this rank's rows of Z, y and a
+  int s0 = 0, rows = n;
+  if (sharded(ctx)) db200_row_shard(n, ctx->coll_world, ctx->coll_rank, &s0, &rows);
+  st = db200_svm_barrier(ctx, rows, l, Z, ldz, y + s0, C, &P, a, &local);
   local.ms_total = total.stop_ms();
   if (rep) *rep = local;
   return st;

@@ -38,6 +38,7 @@ extern "C" {
 #define DB200_ERR_UNSUPPORTED (-8) /* shape outside what the kernels implement */
 #define DB200_ERR_TOO_LARGE (-9)   /* request exceeds the fixed scratch of db200_rbf_sketch_noalloc */
 #define DB200_ERR_SINGULAR (-10)   /* LU met a zero pivot */
+#define DB200_ERR_COLLECTIVE (-11) /* the collective set by db200_set_collective reported a failure */
 
 /* Layout of a point matrix X holding n points of d features. */
 #define DB200_POINT_MAJOR 0   /* x(i,k) = X[k + i*ldx]  (the reference's DMatrix X, d x n column major) */
@@ -256,6 +257,42 @@ DB200_API int db200_lowrank(db200_context* ctx, int n, int d, int l, int q, cons
 DB200_API int db200_svm_solve(db200_context* ctx, int n, int d, int l, int q, const float* X, int ldx,
                               const float* y, const float* Omega, int ldo, float gamma, double C,
                               const db200_barrier_params* p, double* a, double* Z, int ldz, db200_svm_report* rep);
+
+/* ------------------------------------------------------------------------------------------------------
+ * Row-sharded solve over several ranks (one process per GPU), the counterpart of DArray's row-distributed
+ * matrices (include/darray.h:737-1054 replicates and reduces blocks over MPI).  Every rank holds all of X, y
+ * and Omega and owns the rows [start, start + count) of Y = K Omega, of the factor Z and of the dual vector a
+ * (db200_row_shard): the kernel passes need no exchange; CholeskyQR2 and the Nystrom core all-reduce one l x l
+ * Gram each; the power and final passes need all of Q (gathered as a sum over ranks of zero-filled row blocks);
+ * each Newton step all-reduces the r x r capacity matrix, the r-vectors Z^T x and a few scalars.  The library
+ * calls the host-supplied collective for every exchange, so the plumbing (torch.distributed over NCCL, or a
+ * test's in-process loopback) stays outside it.
+ * ------------------------------------------------------------------------------------------------------ */
+#define DB200_REDUCE_SUM 0
+#define DB200_REDUCE_MAX 1
+#define DB200_REDUCE_MIN 2
+/* All-reduce of `count` FP64 values at device address buf in place (op: DB200_REDUCE_*), called with the
+ * context's stream (cudaStream_t), on which buf is ready: the callee orders the reduction after the stream's
+ * work and the stream's later work after the reduction (synchronising is enough), and returns 0 on success.
+ * Every rank calls it with the same count and op in the same order. */
+typedef int (*db200_allreduce_fn)(void* user, double* buf, long long count, int op, void* stream);
+typedef struct db200_collective {
+  int world;                   /* ranks sharing the problem */
+  int rank;                    /* this rank, 0 <= rank < world */
+  db200_allreduce_fn allreduce;
+  void* user;                  /* passed back to allreduce */
+} db200_collective;
+
+/* Attach (c with world > 1) or detach (c == NULL or world == 1) a collective.  While one is attached:
+ *   db200_lowrank and db200_svm_solve take the full X, y and Omega (n points) and write this rank's rows of Z
+ *   (count x l, ldz >= count) and a (count) as db200_row_shard(n, world, rank) gives them;
+ *   db200_svm_barrier takes this rank's rows: n = its row count, Z (n x r), y and a (n); the reports hold the
+ *   global objective and gaps, the same on every rank.
+ * db200_svm_solve_landmarks refuses to run (DB200_ERR_UNSUPPORTED); other entry points ignore it. */
+DB200_API int db200_set_collective(db200_context* ctx, const db200_collective* c);
+
+/* Contiguous balanced row blocks: rank k owns count = n / world (+1 for k < n % world) rows from start. */
+DB200_API int db200_row_shard(int n, int world, int rank, int* start, int* count);
 
 /* ------------------------------------------------------------------------------------------------------
  * Support for the one-rank DArray mirror (the headers under include/darray_b200/) and other host callers.

@@ -67,6 +67,34 @@ def test_potrf_ragged_blocks(gpu_ctx, n, nb):
     assert np.all(np.tril(R, -1) == 0)
 
 
+@pytest.mark.parametrize("n", [4096, 8192])
+def test_potrf_known_answer_large(gpu_ctx, n):
+    # perftest_cholesky's sizes: the min(i+1, j+1) matrix of integers factors exactly in FP64 (every pivot 1),
+    # so the whole factor must be the upper triangle of ones; the trailing updates run on the DMMA tile path here
+    import torch
+    i = torch.arange(1, n + 1, device="cuda", dtype=torch.float64)
+    A = torch.minimum(i[:, None], i[None, :])
+    gpu_ctx.potrf(n, A.data_ptr(), n)
+    gpu_ctx.sync()
+    # column major upper factor = lower triangle of the row-major view
+    assert float((A - torch.tril(torch.ones_like(A))).abs().max()) == 0.0
+    assert float(A[n - 1, n - 1]) == 1.0
+
+
+@pytest.mark.parametrize("n,nb", [(3000, 64), (2500, 48)])
+def test_potrf_large_matches_oracle(gpu_ctx, n, nb):
+    # both trailing-update paths in one factor: 128 x 128 DMMA tiles while the trailing matrix is large, 32 x 32
+    # tiles for the last blocks
+    g = np.random.default_rng(n)
+    B = g.standard_normal((n, n))
+    A = B @ B.T / n + np.eye(n)
+    dA = d64(A)
+    gpu_ctx.potrf(n, dA.data_ptr(), n, nb)
+    R = h64(dA, n)
+    assert rel(R, O.cholesky_upper(A)) < 1e-11
+    assert np.all(np.tril(R, -1) == 0)
+
+
 def test_potrf_test3_factor_and_reference(gpu_ctx):
     A = G["chol_test3_A"].astype(np.float64)
     dA = d64(A)
