@@ -703,7 +703,7 @@ def solve_run(ctx, w, X, y, O, n_test, mixed_only=False):
     return out
 
 
-def batch_run(ctx, count=64, workers=8):
+def batch_run(ctx, count=64, workers=16):
     """Batched form: `count` SVM instances of uneven n, d, gamma and C (darray_optimizer_b200.batched.workload) in
     one db200_svm_solve_batched call -- batched persistent kernel passes replayed from a CUDA graph, tile plans from
     the autotuner, barriers on worker threads -- against the same instances solved one after another."""

@@ -92,6 +92,47 @@ void* slot_buffer(db200_context* ctx, int slot, size_t bytes) {
   return ctx->slot[slot];
 }
 
+int graph_run(db200_context* ctx, const std::vector<long long>& key, const std::function<int()>& body) {
+  if (ctx->graphs_off) return body();
+  for (auto& e : ctx->graphs) {
+    if (e.key != key) continue;
+    DB200_CUDA(ctx, cudaGraphLaunch(e.exec, ctx->stream));
+    ctx->launches += e.launches;
+    return DB200_OK;
+  }
+  if (!ctx->cap_stream && cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    ctx->graphs_off = true;
+    return body();
+  }
+  const long long launches0 = ctx->launches;
+  cudaStream_t saved = ctx->stream;
+  ctx->stream = ctx->cap_stream;
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(ctx->cap_stream, cudaStreamCaptureModeThreadLocal);
+  int st = (e == cudaSuccess) ? body() : DB200_ERR_CUDA;
+  if (e == cudaSuccess) e = cudaStreamEndCapture(ctx->cap_stream, &g);
+  ctx->stream = saved;
+  cudaGraphExec_t x = nullptr;
+  if (e == cudaSuccess && st == DB200_OK && g) e = cudaGraphInstantiate(&x, g, 0);
+  if (g) cudaGraphDestroy(g);
+  const long long captured = ctx->launches - launches0;
+  ctx->launches = launches0;
+  if (e != cudaSuccess || st != DB200_OK || !x) {
+    cudaGetLastError();  // the failed capture's error is not the caller's
+    ctx->graphs_off = true;
+    return body();
+  }
+  if (ctx->graphs.size() >= 64) {
+    cudaGraphExecDestroy(ctx->graphs.front().exec);
+    ctx->graphs.erase(ctx->graphs.begin());
+  }
+  ctx->graphs.push_back({key, x, captured});
+  DB200_CUDA(ctx, cudaGraphLaunch(x, ctx->stream));
+  ctx->launches += captured;
+  return DB200_OK;
+}
+
 int allreduce(db200_context* ctx, double* buf, long long count, int op) {
   if (!sharded(ctx) || count <= 0) return DB200_OK;
   const int st = ctx->coll_fn(ctx->coll_user, buf, count, op, ctx->stream);
@@ -158,6 +199,9 @@ int db200_destroy(db200_context* ctx) {
   for (db200_context* w : ctx->workers) db200_destroy(w);
   ctx->workers.clear();
   prof_clear(ctx);
+  for (auto& e : ctx->graphs) cudaGraphExecDestroy(e.exec);
+  ctx->graphs.clear();
+  if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
   if (ctx->ws) cudaFree(ctx->ws);
   if (ctx->io) cudaFree(ctx->io);
   for (void* p : ctx->slot)

@@ -2,6 +2,7 @@
 #pragma once
 #include <cstddef>
 #include <cstdint>
+#include <functional>
 #include <string>
 #include <utility>
 #include <vector>
@@ -38,6 +39,16 @@ struct db200_context {
   // Optional per-launch timing of the tcgen05 tile kernels (CUDA events on the launching stream).
   bool profiling = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
+  // CUDA graphs of repeated launch sequences (the barrier's capacity-matrix factor), keyed by the pointers and
+  // sizes they were captured with; captured on a private non-blocking stream and replayed on `stream`.
+  struct GraphEntry {
+    std::vector<long long> key;
+    cudaGraphExec_t exec = nullptr;
+    long long launches = 0;  // kernels in the graph (added to `launches` per replay)
+  };
+  cudaStream_t cap_stream = nullptr;
+  std::vector<GraphEntry> graphs;
+  bool graphs_off = false;   // a capture failed once: sequences run eagerly from then on
   // Row-sharded solves (db200_set_collective): the host's all-reduce; world 1 = none attached.
   int coll_world = 1, coll_rank = 0;
   db200_allreduce_fn coll_fn = nullptr;
@@ -173,6 +184,12 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
 // Row-sharded solves: whether a collective of more than one rank is attached, and its all-reduce of `count` FP64
 // values at device address buf (in place, on the context's stream; a no-op when none is attached).
 inline bool sharded(const db200_context* ctx) { return ctx->coll_world > 1 && ctx->coll_fn; }
+
+// Enqueue what `body` launches on ctx->stream through a CUDA graph cached under `key` (the sequence's pointers and
+// sizes): the first call with a key captures body on a private stream and instantiates it, later calls replay
+// it with one launch.  body must only enqueue work on ctx->stream (no host synchronisation or reads).  If a
+// capture fails, the context runs every sequence eagerly from then on.
+int graph_run(db200_context* ctx, const std::vector<long long>& key, const std::function<int()>& body);
 int allreduce(db200_context* ctx, double* buf, long long count, int op);
 
 // Launch the fused tile kernel for one problem.  For RBF_MODE_SKETCH, `op` is the packed Omega^T and `out` is Y

@@ -163,6 +163,45 @@ int cholqr2_impl(db200_context* ctx, int n, int l, double* Y, int ldy, double* R
 // ---------------------------------------------------------------------------------------------- barrier
 namespace {
 
+// The capacity matrix M = I + Z^T D^-1 Z of a Newton step and its first Cholesky attempt, as launches on
+// ctx->stream only (so that the sequence can be captured in a graph): the Gram (int8 tensor cores, `slices`
+// digits, or FP64), then the identity, the unshifted backup L = M, the status pair and potrf.
+struct FactorSeq {
+  const double* Z;
+  int ldz;
+  const double* dinv;
+  double* M;
+  double* L;
+  int* d_pair;
+  int n, r;
+  bool use_tc;
+  int slices;
+  void* scratch;
+};
+
+int factor_gram(db200_context* ctx, const FactorSeq& f) {
+  const size_t rr = (size_t)f.r * f.r;
+  if (f.use_tc) {
+    DB200_CUDA(ctx, cudaMemsetAsync(f.M, 0, sizeof(double) * rr, ctx->stream));
+    return gram_tc_weighted(ctx, f.n, f.r, f.Z, f.ldz, f.dinv, f.M, f.r, f.scratch, f.slices);
+  }
+  return gram<double, double>(ctx, f.n, f.r, f.r, f.Z, f.ldz, f.Z, f.ldz, f.dinv, 1.0, 0.0, f.M, f.r, true);
+}
+
+int factor_tail(db200_context* ctx, const FactorSeq& f) {
+  int st = bar_add_identity(ctx, f.M, f.r, f.r);
+  if (st) return st;
+  DB200_CUDA(ctx, cudaMemcpyAsync(f.L, f.M, sizeof(double) * (size_t)f.r * f.r, cudaMemcpyDeviceToDevice,
+                                  ctx->stream));
+  DB200_CUDA(ctx, cudaMemsetAsync(f.d_pair, 0, 2 * sizeof(int), ctx->stream));
+  return potrf_upper(ctx, f.M, f.r, f.r, f.d_pair, f.d_pair + 1);
+}
+
+int factor_seq(db200_context* ctx, const FactorSeq& f) {
+  int st = factor_gram(ctx, f);
+  return st ? st : factor_tail(ctx, f);
+}
+
 // Class-balanced start (tests/testsvm.cpp:192-212) from the class counts.
 void set_a0_counts(double plus, double minus, double C, double* pval, double* mval) {
   if (plus > minus) {
@@ -236,6 +275,40 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
     if (!s2) s2 = reduce(red + 2, 1, DB200_REDUCE_MAX);
     return s2 ? s2 : reduce(red + 3, 1, DB200_REDUCE_MIN);
   };
+  // A fixed launch sequence of a Newton step (its pointers and scalars are those of this call): at one rank it is
+  // replayed from a CUDA graph, one launch instead of several per step; row-sharded it runs as it is, since its
+  // all-reduces call back into the host.
+  long long c_bits = 0;
+  std::memcpy(&c_bits, &C, sizeof(c_bits));
+  auto seq = [&](long long tag, std::initializer_list<long long> extra, const std::function<int()>& body) -> int {
+    if (dist) return body();
+    std::vector<long long> key = {tag, (long long)Z, ldz, n, r, (long long)base, (long long)a, c_bits};
+    key.insert(key.end(), extra);
+    return graph_run(ctx, key, body);
+  };
+  // out = -H~^-1 rhs by Woodbury on the factored capacity matrix; rd[0..2] <- its direction statistics
+  auto woodbury_body = [&](const double* rhs, double* out, double* rd) -> int {
+    int s2;
+    if ((s2 = gemv_t(rhs, dinv, -1.0, u))) return s2;
+    if ((s2 = trsv_upper(ctx, M, L, r, r, u, true))) return s2;   // R^T z = rhs
+    if ((s2 = trsv_upper(ctx, M, L, r, r, u, false))) return s2;  // R u = z
+    if ((s2 = bar_init_red(ctx, rd, 2, 0, 1))) return s2;
+    return bar_direction(ctx, n, r, Z, ldz, u, rhs, dinv, a, C, out, rd);
+  };
+  auto woodbury = [&](const double* rhs, double* out, double* rd) -> int {
+    return seq(1, {(long long)rhs, (long long)out, (long long)rd},
+               [&]() -> int { return woodbury_body(rhs, out, rd); });
+  };
+  // red[16..17] <- |res|^2, |rhs|^2 of the Newton residual res = rhs + H out, with v = Z^T out and zv = Z v
+  auto residual = [&](const double* rhs, double* out) -> int {
+    return seq(2, {(long long)rhs, (long long)out}, [&]() -> int {
+      int s2;
+      if ((s2 = gemv_t(out, nullptr, 1.0, v))) return s2;
+      if ((s2 = bar_init_red(ctx, red + 16, 2, 0, 0))) return s2;
+      if ((s2 = bar_residual(ctx, n, r, Z, ldz, v, rhs, dinv, out, res, red + 16, zv))) return s2;
+      return reduce(red + 16, 2, DB200_REDUCE_SUM);
+    });
+  };
 
   // class-balanced start (tests/testsvm.cpp:192-212) from the class counts of all rows
   std::vector<float> hy(n);
@@ -294,9 +367,13 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
         if ((st = bar_grad_hess(ctx, n, r, Z, ldz, w, a, C, t, g, dinv, red, nullptr, zw))) return st;
         zw_ok = true;
       }
-      if ((st = reduce_grad())) return st;
-      if ((st = bar_dot(ctx, r, w, w, sc))) return st;
-      DB200_CUDA(ctx, cudaMemcpyAsync(red + 8, sc, sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+      if ((st = seq(5, {}, [&]() -> int {  // the row reductions and w.w into red[0..9) for one readback
+             int s2;
+             if ((s2 = reduce_grad()) || (s2 = bar_dot(ctx, r, w, w, sc))) return s2;
+             DB200_CUDA(ctx, cudaMemcpyAsync(red + 8, sc, sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+             return DB200_OK;
+           })))
+        return st;
       if ((st = fetch(red, 9))) return st;
       const double suma = h[0], sumlog = h[1], dmax = h[2], dmin = h[3], ww = h[8];
       if (dmax / dmin > 1e18) break;  // tests/testsvm.cpp:258-263
@@ -310,30 +387,35 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
       // Capacity matrix M = I + Z^T D^-1 Z and its Cholesky factor (upper in M, its transpose in L).
       auto factor = [&](bool use_tc) -> int {
         int s2;
-        if (use_tc) {
-          DB200_CUDA(ctx, cudaMemsetAsync(M, 0, sizeof(double) * rr, ctx->stream));
-          if ((s2 = gram_tc_weighted(ctx, n, r, Z, ldz, dinv, M, r, tc_scratch, kSlices[tc_level]))) return s2;
-        } else {
-          if ((s2 = gram<double, double>(ctx, n, r, r, Z, ldz, Z, ldz, dinv, 1.0, 0.0, M, r, true))) return s2;
-        }
-        if ((s2 = reduce(M, (long long)rr, DB200_REDUCE_SUM))) return s2;  // upper triangles summed
-        if ((s2 = bar_add_identity(ctx, M, r, r))) return s2;
         // A capacity matrix with a huge dynamic range (late in the barrier D^-1 spans ~18 orders) can sit on the
         // edge of numerical positive definiteness: its last bits (the Gram's rounding and the order of its
         // split-k additions) decide whether the FP64 Cholesky passes.  A relative diagonal shift, x10 from 1e-11 up
         // to 1 until the Cholesky succeeds, keeps it positive definite; the shifted M still gives a descent
-        // direction, which the mixed path's refinement corrects against the exact operator.
-        DB200_CUDA(ctx, cudaMemcpyAsync(L, M, sizeof(double) * rr, cudaMemcpyDeviceToDevice, ctx->stream));
+        // direction, which the mixed path's refinement corrects against the exact operator.  L keeps the
+        // unshifted M for the retries.
+        const FactorSeq fs{Z, ldz, dinv, M, L, d_pair, n, r, use_tc, kSlices[tc_level], tc_scratch};
+        if (!dist) {
+          // Gram, identity, backup, first Cholesky: one graph replay per Newton step (about 17 launches as
+          // separate calls, which the host's launch path serialises when many solves share the GPU)
+          const std::vector<long long> key = {(long long)Z, ldz, (long long)dinv, (long long)M, (long long)L,
+                                              (long long)d_pair, n, r, use_tc ? fs.slices : 0,
+                                              (long long)tc_scratch};
+          if ((s2 = graph_run(ctx, key, [&]() -> int { return factor_seq(ctx, fs); }))) return s2;
+        } else {
+          if ((s2 = factor_gram(ctx, fs))) return s2;
+          if ((s2 = reduce(M, (long long)rr, DB200_REDUCE_SUM))) return s2;  // upper triangles summed
+          if ((s2 = factor_tail(ctx, fs))) return s2;
+        }
         double eps = 1e-11;
-        for (int tries = 0; tries < 12; ++tries) {
-          DB200_CUDA(ctx, cudaMemsetAsync(d_pair, 0, 2 * sizeof(int), ctx->stream));
-          if ((s2 = potrf_upper(ctx, M, r, r, d_pair, d_pair + 1))) return s2;
+        for (int tries = 0;; ++tries) {
           int pst = 0, bad = 0;
           if ((s2 = read_status(ctx, d_pair, &pst, &bad))) return s2;
           if (pst == 0 || tries == 11) break;
           DB200_CUDA(ctx, cudaMemcpyAsync(M, L, sizeof(double) * rr, cudaMemcpyDeviceToDevice, ctx->stream));
           if ((s2 = bar_scale_diag(ctx, M, r, r, 1.0 + eps))) return s2;
           eps *= 10.0;
+          DB200_CUDA(ctx, cudaMemsetAsync(d_pair, 0, 2 * sizeof(int), ctx->stream));
+          if ((s2 = potrf_upper(ctx, M, r, r, d_pair, d_pair + 1))) return s2;
         }
         return transpose64(ctx, M, r, r, r, L, r);
       };
@@ -344,19 +426,12 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
       auto solve = [&](const double* rhs, double* out, bool use_tc, bool* converged, bool track_v) -> int {
         int s2;
         *converged = true;
-        if ((s2 = gemv_t(rhs, dinv, -1.0, u))) return s2;
-        if ((s2 = trsv_upper(ctx, M, L, r, r, u, true))) return s2;   // R^T z = rhs
-        if ((s2 = trsv_upper(ctx, M, L, r, r, u, false))) return s2;  // R u = z
-        if ((s2 = bar_init_red(ctx, red, 2, 0, 1))) return s2;
-        if ((s2 = bar_direction(ctx, n, r, Z, ldz, u, rhs, dinv, a, C, out, red))) return s2;
+        if ((s2 = woodbury(rhs, out, red))) return s2;
         if (!use_tc) return DB200_OK;
         *converged = false;
         double prev = 0.0;
         for (int it = 0; it <= P.refine_max; ++it) {
-          if ((s2 = gemv_t(out, nullptr, 1.0, v))) return s2;
-          if ((s2 = bar_init_red(ctx, red + 16, 2, 0, 0))) return s2;
-          if ((s2 = bar_residual(ctx, n, r, Z, ldz, v, rhs, dinv, out, res, red + 16, zv))) return s2;
-          if ((s2 = reduce(red + 16, 2, DB200_REDUCE_SUM))) return s2;
+          if ((s2 = residual(rhs, out))) return s2;
           if ((s2 = fetch(red + 16, 2))) return s2;
           const double rn = std::sqrt(h[0]), gn = std::sqrt(h[1]);
           if (rn <= 1e-10 * gn) {
@@ -366,25 +441,17 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
           }
           if (it == P.refine_max || (it > 0 && rn >= 0.5 * prev) || !std::isfinite(rn)) break;
           prev = rn;
-          if ((s2 = gemv_t(res, dinv, -1.0, u))) return s2;
-          if ((s2 = trsv_upper(ctx, M, L, r, r, u, true))) return s2;
-          if ((s2 = trsv_upper(ctx, M, L, r, r, u, false))) return s2;
-          if ((s2 = bar_init_red(ctx, red + 16, 2, 0, 1))) return s2;
-          if ((s2 = bar_direction(ctx, n, r, Z, ldz, u, res, dinv, a, C, delta, red + 16))) return s2;
-          if ((s2 = bar_axpy(ctx, n, 1.0, delta, out))) return s2;
+          if ((s2 = seq(3, {(long long)out}, [&]() -> int {  // out += -H~^-1 res
+                 int s3 = woodbury_body(res, delta, red + 16);
+                 return s3 ? s3 : bar_axpy(ctx, n, 1.0, delta, out);
+               })))
+            return s2;
           ++refine_total;
         }
         return DB200_OK;
       };
       // out = -H~^-1 rhs: one Woodbury application of the factored capacity matrix, no refinement.
-      auto apply = [&](const double* rhs, double* out, double* rd) -> int {
-        int s2;
-        if ((s2 = gemv_t(rhs, dinv, -1.0, u))) return s2;
-        if ((s2 = trsv_upper(ctx, M, L, r, r, u, true))) return s2;
-        if ((s2 = trsv_upper(ctx, M, L, r, r, u, false))) return s2;
-        if ((s2 = bar_init_red(ctx, rd, 2, 0, 1))) return s2;
-        return bar_direction(ctx, n, r, Z, ldz, u, rhs, dinv, a, C, out, rd);
-      };
+      auto apply = [&](const double* rhs, double* out, double* rd) -> int { return woodbury(rhs, out, rd); };
       // Newton direction s = -(Z Z^T + D)^-1 g.  Mixed: capacity matrix on the int8 tensor cores (Ozaki slices,
       // ~1e-12 of the column norms) factored in FP64, then refinement; a step whose refinement misses 1e-10 is
       // recomputed with the FP64 capacity matrix.  FP64: the capacity matrix on the FP64 pipes, no refinement.
@@ -467,13 +534,22 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
         v_current = false;
         if ((st = newton_dir(false, &conv))) return st;
       }
-      if (!v_current && (st = gemv_t(s, nullptr, 1.0, v))) return st;
-      // direction statistics of s: [0] g.s, [1] sum s, [2] largest step inside the box
-      if ((st = reduce(red, 2, DB200_REDUCE_SUM)) || (st = reduce(red + 2, 1, DB200_REDUCE_MIN))) return st;
-      if ((st = bar_dot(ctx, r, w, v, sc + 1))) return st;
-      if ((st = bar_dot(ctx, r, v, v, sc + 2))) return st;
-      DB200_CUDA(ctx, cudaMemcpyAsync(red + 8, sc + 1, 2 * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
-      DB200_CUDA(ctx, cudaMemcpyAsync(red + 12, d_pair, 2 * sizeof(int), cudaMemcpyDeviceToDevice, ctx->stream));
+      // v = Z^T s (unless current), the direction statistics of s ([0] g.s, [1] sum s, [2] largest step inside
+      // the box), w.v, v.v and the Cholesky status gathered in red[0..13) for one readback
+      const bool need_v = !v_current;
+      if ((st = seq(4, {need_v ? 1 : 0}, [&]() -> int {
+             int s2;
+             if (need_v && (s2 = gemv_t(s, nullptr, 1.0, v))) return s2;
+             if ((s2 = reduce(red, 2, DB200_REDUCE_SUM)) || (s2 = reduce(red + 2, 1, DB200_REDUCE_MIN))) return s2;
+             if ((s2 = bar_dot(ctx, r, w, v, sc + 1))) return s2;
+             if ((s2 = bar_dot(ctx, r, v, v, sc + 2))) return s2;
+             DB200_CUDA(ctx, cudaMemcpyAsync(red + 8, sc + 1, 2 * sizeof(double), cudaMemcpyDeviceToDevice,
+                                             ctx->stream));
+             DB200_CUDA(ctx, cudaMemcpyAsync(red + 12, d_pair, 2 * sizeof(int), cudaMemcpyDeviceToDevice,
+                                             ctx->stream));
+             return DB200_OK;
+           })))
+        return st;
       if ((st = fetch(red, 13))) return st;
       int pst;
       std::memcpy(&pst, &h[12], sizeof(int));
@@ -486,7 +562,11 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
       for (int round = 0; round < 4 && accepted < 0; ++round) {
         double ht[16];
         for (int k = 0; k < 16; ++k) ht[k] = tau * std::pow(P.beta, k);
-        DB200_CUDA(ctx, cudaMemcpyAsync(taus, ht, sizeof(ht), cudaMemcpyHostToDevice, ctx->stream));
+        // through the pinned staging area (past the readback slots): an asynchronous copy, which the fetch below
+        // completes before the next round writes the slots again
+        double* h_taus = ctx->h_pinned + 256;
+        std::memcpy(h_taus, ht, sizeof(ht));
+        DB200_CUDA(ctx, cudaMemcpyAsync(taus, h_taus, sizeof(ht), cudaMemcpyHostToDevice, ctx->stream));
         if ((st = bar_linesearch16(ctx, n, a, s, C, taus, ls))) return st;
         if ((st = reduce(ls, 32, DB200_REDUCE_SUM))) return st;
         if ((st = fetch(ls, 32))) return st;
