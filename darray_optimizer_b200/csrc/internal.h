@@ -99,12 +99,17 @@ int lu_factorize(db200_context* ctx, int m, int n, int nleft, float* A, long lon
                  int swap_left_panels);
 
 // ------------------------------------------------------------------ RBF tile engine (rbf_tile.cu)
-enum RbfMode { RBF_MODE_SKETCH = 0, RBF_MODE_KBLOCK = 1 };
+// SKETCH: Y = (y_i y_j exp(-gamma d_ij^2)) Omega; KBLOCK: K = y_i y_j exp(-gamma d_ij^2) stored; UPDATE: the distance
+// GEMM alone, out[i, j] += alpha x_i.x_j (TileJob::gamma carries alpha), the split-fp16 product of a rank-d update
+enum RbfMode { RBF_MODE_SKETCH = 0, RBF_MODE_KBLOCK = 1, RBF_MODE_UPDATE = 2 };
 
 struct PackedPoints {
   const void* xp = nullptr;   // fp16 [npad][2*dp]: [hi | lo] split of each point scaled by the set's 2^e
   const float* norms = nullptr;  // fp32: ||x||^2 [npad] (zero on padding rows), then max |x| bits and 2^-e
   int n = 0, npad = 0, dp = 0;
+  // a slice of a packed set (rows from a multiple of 128, npad a multiple of 128): the parent's norms + npad, where
+  // its max |x|, scale and lo flag sit; null for a set of its own
+  const float* tail = nullptr;
 };
 // floats of the norms-and-scale array of a packed set of npad points
 inline size_t packed_norm_floats(int npad) { return (size_t)npad + 64; }

@@ -9,13 +9,18 @@
 //                     panel's remaining columns
 //   lu_laswp_kernel   the panel's row interchanges applied in order to the other columns (one thread per column)
 //   lu_trsm_kernel    U12 = L11^-1 A12 with the unit lower w x w block in shared memory (one thread per column)
-//   lu_update_kernel  A22 -= L21 U12: 64 x 64 output tiles, K = w, FP32 FMA
+//   lu_update_kernel  A22 -= L21 U12: 64 x 64 output tiles, K = w, FP32 FMA (small trailing matrices)
+//   lu_update_tc      the same update on the tcgen05 tile engine (UPDATE mode) once A22 holds a million entries:
+//                     the rows of L21 and the columns of U12 as two point sets, each scaled by a power of two and
+//                     split into fp16 hi + lo (22 significant bits), hi.hi + hi.lo + lo.hi accumulated in fp32,
+//                     A22 read, updated and written once by the epilogue
 // Pivots are recorded 1-based relative to the first row, like LAPACK's ipiv and the reference's.
 #include <cfloat>
 #include <cmath>
 #include <algorithm>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "gridsync.cuh"
 #include "internal.h"
@@ -355,6 +360,62 @@ __global__ void __launch_bounds__(256) lu_update_kernel(float* A, long long lda,
   }
 }
 
+// Workspace bytes of lu_update_tc for a trailing matrix of `rows` x `cols`.
+size_t lu_update_tc_bytes(int rows, int cols) {
+  const size_t per_point = 2 * 32 * 2;  // fp16 hi | lo of 32 features
+  return 4096 + (size_t)point_pad(rows) * per_point + packed_norm_floats(point_pad(rows)) * 4 +
+         (size_t)point_pad(cols) * per_point + packed_norm_floats(point_pad(cols)) * 4;
+}
+
+int lu_update_tc(db200_context* ctx, float* A, long long lda, int m, int n, int k, int w, int r0, int c0, void* ws) {
+  const int rows = m - r0, cols = n - c0, dp = 32;
+  Carve cv{static_cast<char*>(ws)};
+  PackedPoints pl;  // L21: point i = row r0 + i, features A[r0 + i, k .. k + w) (column major: feature-major)
+  pl.n = rows;
+  pl.npad = point_pad(rows);
+  pl.dp = dp;
+  void* xl = cv.take<uint16_t>((size_t)pl.npad * 2 * dp);
+  float* nl = cv.take<float>(packed_norm_floats(pl.npad));
+  int st = pack_points(ctx, A + r0 + (long long)k * lda, (int)lda, DB200_FEATURE_MAJOR, rows, w, dp, pl.npad, xl, nl);
+  if (st) return st;
+  pl.xp = xl;
+  pl.norms = nl;
+  PackedPoints pu;  // U12: point j = column c0 + j, features A[k .. k + w, c0 + j] (point-major)
+  pu.n = cols;
+  pu.npad = point_pad(cols);
+  pu.dp = dp;
+  void* xu = cv.take<uint16_t>((size_t)pu.npad * 2 * dp);
+  float* nu = cv.take<float>(packed_norm_floats(pu.npad));
+  if ((st = pack_points(ctx, A + k + (long long)c0 * lda, (int)lda, DB200_POINT_MAJOR, cols, w, dp, pu.npad, xu, nu)))
+    return st;
+  // column ranges of A22 (slices of the packed U12 sharing its scale), so that a trailing matrix of few 256-row
+  // blocks still fills the 74 CTA pairs
+  const int itiles = pl.npad / 256;
+  int ranges = std::min((148 + itiles - 1) / itiles, (cols + 127) / 128);
+  const int width = round_up((cols + ranges - 1) / ranges, 128);
+  ranges = (cols + width - 1) / width;
+  std::vector<TileJob> jobs((size_t)ranges);
+  for (int q = 0; q < ranges; ++q) {
+    const int j0 = q * width, nc = std::min(width, cols - j0);
+    PackedPoints ps;
+    ps.xp = static_cast<const uint16_t*>(xu) + (size_t)j0 * 2 * dp;
+    ps.norms = nu + j0;
+    ps.n = nc;
+    ps.npad = round_up(nc, 128);  // within the parent's rows: j0 + npad <= roundup(cols, 128) <= pu.npad
+    ps.dp = dp;
+    ps.tail = nu + pu.npad;
+    TileJob& J = jobs[(size_t)q];
+    J.pi = pl;
+    J.pj = ps;
+    J.gamma = -1.0f;  // alpha: A22 -= L21 U12
+    J.out = A + r0 + (long long)(c0 + j0) * lda;
+    J.ldo = lda;
+  }
+  TilePlan T;
+  if ((st = prepare_rbf_tiles(ctx, RBF_MODE_UPDATE, jobs.data(), ranges, nullptr, 0, &T))) return st;
+  return launch_rbf_plan(ctx, T);
+}
+
 }  // namespace
 
 int lu_factorize(db200_context* ctx, int m, int n, int nleft, float* A, long long lda, int* ipiv, int pivot,
@@ -381,6 +442,14 @@ int lu_factorize(db200_context* ctx, int m, int n, int nleft, float* A, long lon
     DB200_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lu_panel_coop_kernel, CP_THREADS,
                                                                   cp_smem));
     if (coop && per_sm > 0) coop_max = std::min(ctx->num_sms * per_sm, 4096);
+  }
+  // the tensor-core trailing update: workspace for the largest (first) trailing matrix, taken before the loop so
+  // that no later step reallocates it
+  constexpr long long TC_MIN_ENTRIES = 1 << 20;
+  void* tc_ws = nullptr;
+  if ((long long)(m - W) * (n - W) >= TC_MIN_ENTRIES) {
+    tc_ws = workspace(ctx, lu_update_tc_bytes(m, n));
+    if (!tc_ws) return DB200_ERR_NOMEM;
   }
   unsigned bar_base = 0;
   for (int k = 0; k < mn; k += W) {
@@ -425,10 +494,17 @@ int lu_factorize(db200_context* ctx, int m, int n, int nleft, float* A, long lon
       DB200_CUDA(ctx, cudaGetLastError());
       ++launches;
       if (k + w < m) {
-        dim3 grid((unsigned)((cols + UT - 1) / UT), (unsigned)((m - (k + w) + UT - 1) / UT));
-        lu_update_kernel<<<grid, 256, 0, ctx->stream>>>(A, lda, m, n, k, w, k + w, k + w);
-        DB200_CUDA(ctx, cudaGetLastError());
-        ++launches;
+        if (tc_ws && (long long)(m - (k + w)) * cols >= TC_MIN_ENTRIES) {
+          count_launch(ctx, launches);
+          launches = 0;
+          const int s2 = lu_update_tc(ctx, A, lda, m, n, k, w, k + w, k + w, tc_ws);
+          if (s2) return s2;
+        } else {
+          dim3 grid((unsigned)((cols + UT - 1) / UT), (unsigned)((m - (k + w) + UT - 1) / UT));
+          lu_update_kernel<<<grid, 256, 0, ctx->stream>>>(A, lda, m, n, k, w, k + w, k + w);
+          DB200_CUDA(ctx, cudaGetLastError());
+          ++launches;
+        }
       }
     }
     count_launch(ctx, launches);

@@ -13,6 +13,8 @@
 //   epi   P   = exp2(min(a_i + b_j + c G, 0)),  a = -gamma*log2(e)*||x||^2,  c = 2*gamma*log2(e) 2^-(e_I+e_J)
 //   MMA2  Y  += P . Omega~_j   (SKETCH mode; P is written to tensor memory as the fp16 A operand, Omega~ is fp16)
 //         or  K[i, j] = y_i y_j P   stored as fp32 (KBLOCK mode)
+//         or  out[i, j] += alpha 2^-(e_I+e_J) G, no exp (UPDATE mode: the split-fp16 product of a rank-d update, e.g.
+//             the trailing update of a blocked LU, with x_i the rows of L21 and x_j the columns of U12)
 // so the kernel matrix is never written to HBM in SKETCH mode.  Algorithm restated from
 // include/dkernel.cu:102-129 (vecnorm, rbf) and :151-178 / :194-231 (distance GEMM, rbf, sketch GEMM).
 //
@@ -634,14 +636,16 @@ __global__ void __launch_bounds__(NUM_THREADS, 1) rbf_tile_kernel(const __grid_c
         if (lane == 0) mbar_arrive_remote(lbar(B_G_EMPTY0 + b));
 
         const int j0 = jt * BN + qc * EPI_COLS;
-        const float4* sj4 = reinterpret_cast<const float4*>(sjbuf + (jt & 1) * EPI_COLS);
+        if (MODE != RBF_MODE_UPDATE) {
+          const float4* sj4 = reinterpret_cast<const float4*>(sjbuf + (jt & 1) * EPI_COLS);
 #pragma unroll
-        for (int c = 0; c < EPI_COLS / 4; ++c) {
-          const float4 s4 = sj4[c];
-          v[4 * c + 0] = fast_exp2(fminf(fmaf(c_dot, v[4 * c + 0], fmaf(c_row, s4.x, a_i)), 0.0f));
-          v[4 * c + 1] = fast_exp2(fminf(fmaf(c_dot, v[4 * c + 1], fmaf(c_row, s4.y, a_i)), 0.0f));
-          v[4 * c + 2] = fast_exp2(fminf(fmaf(c_dot, v[4 * c + 2], fmaf(c_row, s4.z, a_i)), 0.0f));
-          v[4 * c + 3] = fast_exp2(fminf(fmaf(c_dot, v[4 * c + 3], fmaf(c_row, s4.w, a_i)), 0.0f));
+          for (int c = 0; c < EPI_COLS / 4; ++c) {
+            const float4 s4 = sj4[c];
+            v[4 * c + 0] = fast_exp2(fminf(fmaf(c_dot, v[4 * c + 0], fmaf(c_row, s4.x, a_i)), 0.0f));
+            v[4 * c + 1] = fast_exp2(fminf(fmaf(c_dot, v[4 * c + 1], fmaf(c_row, s4.y, a_i)), 0.0f));
+            v[4 * c + 2] = fast_exp2(fminf(fmaf(c_dot, v[4 * c + 2], fmaf(c_row, s4.z, a_i)), 0.0f));
+            v[4 * c + 3] = fast_exp2(fminf(fmaf(c_dot, v[4 * c + 3], fmaf(c_row, s4.w, a_i)), 0.0f));
+          }
         }
 
         sjbuf[((jt + 1) & 1) * EPI_COLS + lane] = sj_next;
@@ -684,6 +688,25 @@ __global__ void __launch_bounds__(NUM_THREADS, 1) rbf_tile_kernel(const __grid_c
           for (int dd = 0; dd < 2 && ok; ++dd)
             if (dq[dd] && !drain(da[dd])) ok = false;
           if (!ok) break;
+        } else if (MODE == RBF_MODE_UPDATE) {
+          // each (i, j) has one owner thread: a plain read-modify-write, 8 columns at a time with every load
+          // issued before the first store (the stores could alias the loads, so interleaved they would serialise)
+          if (i < m) {
+#pragma unroll
+            for (int hh = 0; hh < EPI_COLS; hh += 8) {
+              float o[8];
+#pragma unroll
+              for (int c = 0; c < 8; ++c) {
+                const int j = j0 + hh + c;
+                o[c] = (j < n_cols) ? out_i[(size_t)j * ldo] : 0.0f;
+              }
+#pragma unroll
+              for (int c = 0; c < 8; ++c) {
+                const int j = j0 + hh + c;
+                if (j < n_cols) out_i[(size_t)j * ldo] = fmaf(c_dot, v[hh + c], o[c]);
+              }
+            }
+          }
         } else {
           if (i < m) {
 #pragma unroll
@@ -995,13 +1018,17 @@ int prepare_rbf_tiles(db200_context* ctx, int mode, const TileJob* jobs, int cou
     I.l = J.l;
     I.nkc = kp / KC;
     I.c_row = -J.gamma * LOG2E;
-    I.c_dot = 2.0f * J.gamma * LOG2E;
+    I.c_dot = (mode == RBF_MODE_UPDATE) ? J.gamma : 2.0f * J.gamma * LOG2E;  // UPDATE: gamma carries alpha
     I.si = pi.norms;
     I.sj = pj.norms;
-    I.fi = pi.norms + pi.npad + 1;  // the pack writes the set's scale after the norms and the max |x|
-    I.fj = pj.norms + pj.npad + 1;
-    I.lof_i = reinterpret_cast<const unsigned*>(pi.norms + pi.npad + 2);  // and whether any lo part is nonzero
-    I.lof_j = reinterpret_cast<const unsigned*>(pj.norms + pj.npad + 2);
+    // the pack writes the set's max |x|, its scale and whether any lo part is nonzero after the norms (a slice of a
+    // packed set reads its parent's)
+    const float* tail_i = pi.tail ? pi.tail : pi.norms + pi.npad;
+    const float* tail_j = pj.tail ? pj.tail : pj.norms + pj.npad;
+    I.fi = tail_i + 1;
+    I.fj = tail_j + 1;
+    I.lof_i = reinterpret_cast<const unsigned*>(tail_i + 2);
+    I.lof_j = reinterpret_cast<const unsigned*>(tail_j + 2);
     I.yi = J.yi;
     I.yj = J.yj;
     I.out = J.out;
@@ -1030,8 +1057,9 @@ int prepare_rbf_tiles(db200_context* ctx, int mode, const TileJob* jobs, int cou
   T.smem = make_layout(nkc_max, panel_max, T.nsx, T.nso, om_mult).total + 1024;
   {
     const int max_clusters = ctx->num_sms / 2;
-    cudaError_t e = (mode == RBF_MODE_SKETCH) ? plan_clusters<RBF_MODE_SKETCH>(T.smem, max_clusters, items, &T.clusters)
-                                              : plan_clusters<RBF_MODE_KBLOCK>(T.smem, max_clusters, items, &T.clusters);
+    cudaError_t e = (mode == RBF_MODE_SKETCH)   ? plan_clusters<RBF_MODE_SKETCH>(T.smem, max_clusters, items, &T.clusters)
+                    : (mode == RBF_MODE_UPDATE) ? plan_clusters<RBF_MODE_UPDATE>(T.smem, max_clusters, items, &T.clusters)
+                                                : plan_clusters<RBF_MODE_KBLOCK>(T.smem, max_clusters, items, &T.clusters);
     DB200_CUDA(ctx, e);
   }
   const size_t bytes = tile_table_bytes(count);
@@ -1072,8 +1100,9 @@ int launch_rbf_plan(db200_context* ctx, const TilePlan& T) {
   a.status = ctx->d_status;
   cudaEvent_t e0 = nullptr;
   prof_begin(ctx, &e0);
-  cudaError_t err = (T.mode == RBF_MODE_SKETCH) ? launch_kernel<RBF_MODE_SKETCH>(a, T.smem, T.clusters, ctx->stream)
-                                                : launch_kernel<RBF_MODE_KBLOCK>(a, T.smem, T.clusters, ctx->stream);
+  cudaError_t err = (T.mode == RBF_MODE_SKETCH)   ? launch_kernel<RBF_MODE_SKETCH>(a, T.smem, T.clusters, ctx->stream)
+                    : (T.mode == RBF_MODE_UPDATE) ? launch_kernel<RBF_MODE_UPDATE>(a, T.smem, T.clusters, ctx->stream)
+                                                  : launch_kernel<RBF_MODE_KBLOCK>(a, T.smem, T.clusters, ctx->stream);
   DB200_CUDA(ctx, err);
   prof_end(ctx, e0);
   count_launch(ctx);
