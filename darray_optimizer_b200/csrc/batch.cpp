@@ -333,6 +333,24 @@ int db200_svm_solve_batched(db200_context* ctx, int count, const db200_svm_insta
       ctx->workers.push_back(w);
     }
   }
+  // Every worker's CholeskyQR2 and barrier buffers sized for the largest instance now: grown on demand, they would
+  // be reallocated whenever a worker met a larger instance than before, and each cudaFree / cudaMalloc stalls the
+  // whole device, i.e. every other worker (orthonormalisation 130 ms in one call, 770 ms in another).
+  {
+    size_t la = 0, bar = 0;
+    const bool mixed = (P.precision != DB200_FP64);
+    for (int b = 0; b < count; ++b) {
+      la = std::max(la, cholqr2_slot_bytes(inst[b].n, inst[b].l));
+      bar = std::max(bar, barrier_slot_bytes(inst[b].n, inst[b].l, mixed));
+    }
+    for (int k = 0; k < workers; ++k) {
+      db200_context* w = (workers == 1) ? ctx : ctx->workers[(size_t)k];
+      if (!slot_buffer(w, SLOT_LA, la) || !slot_buffer(w, SLOT_BAR, bar)) {
+        cleanup();
+        return fail(ctx, DB200_ERR_NOMEM, "svm_solve_batched: worker buffers");
+      }
+    }
+  }
   // largest instances first (LPT): the per-instance work grows with n l^2
   std::vector<int> order((size_t)count);
   for (int b = 0; b < count; ++b) order[(size_t)b] = b;

@@ -186,6 +186,11 @@ int nystrom_core(db200_context* ctx, int n, int l, const double* Q, const TY* Yk
 int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz, const float* y, double C,
                      const db200_barrier_params& P, double* a, db200_svm_report* rep, bool dist = false);
 
+// Bytes of the context buffers cholqr2_impl (SLOT_LA) and svm_barrier_impl (SLOT_BAR, mixed: with the int8 Gram's
+// scratch) take for n rows and l (r) columns; callers that run many problems on one context can size them up front.
+size_t cholqr2_slot_bytes(int n, int l);
+size_t barrier_slot_bytes(int n, int r, bool mixed);
+
 // Row-sharded solves: whether a collective of more than one rank is attached, and its all-reduce of `count` FP64
 // values at device address buf (in place, on the context's stream; a no-op when none is attached).
 inline bool sharded(const db200_context* ctx) { return ctx->coll_world > 1 && ctx->coll_fn; }

@@ -826,17 +826,19 @@ int potrf_upper(db200_context* ctx, double* A, int lda, int l, int* d_status, in
   // the diagonal-block kernel's arrival counter starts every factorisation at zero
   DB200_CUDA(ctx, cudaMemsetAsync(ctx->d_status + 1, 0, sizeof(int), ctx->stream));
   // A trailing matrix of at least one wave of 128 x 128 upper tiles takes its update on the FP64 tensor cores
-  // (gram_kernel, alpha = -1, added in place).  While the matrix beyond the next 4 nb columns is that large, the
-  // factor goes by outer panels of 4 nb columns: each nb-block of the panel is factored (potrf_block_kernel, which
+  // (gram_kernel, alpha = -1, added in place).  While the matrix beyond the next 8 nb columns is that large, the
+  // factor goes by outer panels of 8 nb columns: each nb-block of the panel is factored (potrf_block_kernel, which
   // also solves its row to the last column), the panel's own later rows are updated at once (a strip of at most
-  // 3 nb rows), and the trailing matrix takes one rank-4 nb update per panel instead of four rank-nb ones.
+  // 7 nb rows), and the trailing matrix takes one rank-8 nb update per panel instead of eight rank-nb ones
+  // (measured at n = 16384 / 32768 with nb = 64: rank-64 updates 225 ms / -, rank-256 120 / 856 ms, rank-512
+  // 105 / 755 ms).
   auto big = [&](int rest) {
     const int tp = (rest + GT - 1) / GT;
     return rest > 0 && tp * (tp + 1) / 2 >= ctx->num_sms;
   };
   for (int K0 = 0; K0 < l;) {
     const int rest0 = l - K0;
-    const int KB = big(rest0 - 4 * nb) ? 4 * nb : (rest0 < nb ? rest0 : nb);
+    const int KB = big(rest0 - 8 * nb) ? 8 * nb : (rest0 < nb ? rest0 : nb);
     for (int k0 = K0; k0 < K0 + KB; k0 += nb) {
       const int kb = (K0 + KB - k0 < nb) ? K0 + KB - k0 : nb;
       const int rest = l - k0 - kb;

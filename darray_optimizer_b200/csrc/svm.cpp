@@ -112,12 +112,16 @@ int cholqr_pass(db200_context* ctx, int n, int l, const double* Yin, int ldin, d
 
 }  // namespace
 
-int cholqr2_impl(db200_context* ctx, int n, int l, double* Y, int ldy, double* Rout, int ldr, bool tc_gram,
-                 bool dist) {
+size_t cholqr2_slot_bytes(int n, int l) {
   // slot layout: [pair | scalar | T (n x l) | R1 | R2 | R3 | Rinv | Racc]
   const size_t ll = (size_t)l * l;
-  const size_t bytes = 1024 + align_up((size_t)n * l * 8, 256) + 5 * align_up(ll * 8, 256) + 1024;
-  char* base = static_cast<char*>(slot_buffer(ctx, SLOT_LA, bytes));
+  return 1024 + align_up((size_t)n * l * 8, 256) + 5 * align_up(ll * 8, 256) + 1024;
+}
+
+int cholqr2_impl(db200_context* ctx, int n, int l, double* Y, int ldy, double* Rout, int ldr, bool tc_gram,
+                 bool dist) {
+  const size_t ll = (size_t)l * l;
+  char* base = static_cast<char*>(slot_buffer(ctx, SLOT_LA, cholqr2_slot_bytes(n, l)));
   if (!base) return DB200_ERR_NOMEM;
   Carve cv{base};
   int* d_pair = cv.take<int>(4);
@@ -215,6 +219,13 @@ void set_a0_counts(double plus, double minus, double C, double* pval, double* mv
 
 }  // namespace
 
+size_t barrier_slot_bytes(int n, int r, bool mixed) {
+  const size_t rr = (size_t)r * r;
+  const size_t tc_bytes = mixed ? gram_tc_scratch_bytes(n, r) : 0;
+  return 4096 + 10 * align_up((size_t)n * 8, 256) + 6 * align_up((size_t)r * 8, 256) + 2 * align_up(rr * 8, 256) +
+         align_up(tc_bytes, 256) + 4096;
+}
+
 int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz, const float* y, double C,
                      const db200_barrier_params& P, double* a, db200_svm_report* rep, bool dist) {
   if (r > 4096) return fail(ctx, DB200_ERR_UNSUPPORTED, "svm_barrier: r > 4096");
@@ -222,9 +233,7 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
   const size_t rr = (size_t)r * r;
   const bool mixed = (P.precision != DB200_FP64);
   const size_t tc_bytes = mixed ? gram_tc_scratch_bytes(n, r) : 0;
-  const size_t bytes = 4096 + 10 * align_up((size_t)n * 8, 256) + 6 * align_up((size_t)r * 8, 256) +
-                       2 * align_up(rr * 8, 256) + align_up(tc_bytes, 256) + 4096;
-  char* base = static_cast<char*>(slot_buffer(ctx, SLOT_BAR, bytes));
+  char* base = static_cast<char*>(slot_buffer(ctx, SLOT_BAR, barrier_slot_bytes(n, r, mixed)));
   if (!base) return DB200_ERR_NOMEM;
   Carve cv{base};
   double* red = cv.take<double>(64);
