@@ -8,6 +8,8 @@ Tolerances (stated here, checked below):
   * db200_rbf_sketch_ex: compensated product (P and Omega each as fp16 hi + lo) <= 6e-5 relative Frobenius (the
     tensor cores' truncating fp32 accumulation over n points); with the accumulation promoted every 256 points
     <= 3e-6; P split only <= 4e-4.
+  * at the full C2 size (n = 131072, d = 128, l = 528) on 64 sampled rows against the FP64 oracle: the single
+    product <= 6e-4 (measured 3.0e-4), the promoted compensated product <= 3e-6 (measured 1.3e-6).
 """
 import numpy as np
 import pytest
@@ -280,3 +282,26 @@ def test_lra_host_matches_oracle(gpu_ctx, pinned, pad):
     A = Ah.numpy()
     assert rel_fro(A[:, :n].T, ref) <= 2e-3
     assert np.all(A[:, n:] == 7.0)
+
+
+@pytest.mark.parametrize("product,tol", [(0, 6e-4), (3, 3e-6)])  # DB200_SKETCH_SINGLE, _COMPENSATED_PROMOTED
+def test_rbf_sketch_full_size_sampled_rows(gpu_ctx, product, tol):
+    """The C2 workload at full size (n = 131072, d = 128, l = 528, gamma = 0.5/d, uniform [0,1)^128 points with
+    hyperplane labels): the GPU pass over all rows, 64 seeded rows of it against the FP64 oracle's rows."""
+    import torch
+    from darray_optimizer_b200 import datagen
+    w = datagen.uniform_hyperplane()
+    Om = w.omega()
+    n, d, l = w.n, w.d, w.l
+    assert (n, d, l) == (131072, 128, 528)
+    dX, dy, dO = dev(w.X), dev(w.y), dev(Om)
+    Y = torch.zeros((l, n), dtype=torch.float32, device="cuda")
+    gpu_ctx.rbf_sketch_ex(n, n, d, l, ptr(dX), d, ptr(dX), d, POINT_MAJOR, ptr(dy), ptr(dy), ptr(dO), n, ptr(Y), n,
+                          w.gamma, product)
+    gpu_ctx.sync()
+    rows = np.sort(np.random.default_rng(64).choice(n, 64, replace=False))
+    Yg = Y[:, torch.from_numpy(rows).cuda()].cpu().numpy().T  # 64 x l
+    ref = O.sketch(w.X[rows], w.X, w.y[rows], w.y, Om, w.gamma)
+    err = rel_fro(Yg, ref)
+    print(f"C2 full size, product {product}: sampled-row error vs FP64 {err:.3e}")
+    assert err <= tol
