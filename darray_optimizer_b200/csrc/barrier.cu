@@ -286,6 +286,18 @@ __global__ void init_red_kernel(double* red, int nsum, int nmax, int nmin) {
   else if (i < nsum + nmax + nmin) red[i] = DBL_MAX;
 }
 
+// taus[k] = t0 beta^k (k < 16), t0 = min(1, 0.99 * *step_max), by repeated multiplication (the host forms the
+// same values the same way)
+__global__ void steps16_kernel(const double* step_max, double beta, double* taus) {
+  if (threadIdx.x != 0) return;
+  const double m = 0.99 * *step_max;
+  double t = (m < 1.0) ? m : 1.0;  // as std::min(1.0, m): 1 when m is NaN
+  for (int k = 0; k < 16; ++k) {
+    taus[k] = t;
+    t *= beta;
+  }
+}
+
 __global__ void dot_kernel(int r, const double* x, const double* y, double* out) {
   double s = 0.0;
   for (int k = threadIdx.x; k < r; k += blockDim.x) s += x[k] * y[k];
@@ -420,6 +432,13 @@ int bar_add_identity(db200_context* ctx, double* M, int ldm, int r) {
 
 int bar_scale_diag(db200_context* ctx, double* M, int ldm, int r, double factor) {
   scale_diag_kernel<<<(r + 255) / 256, 256, 0, ctx->stream>>>(M, ldm, r, factor);
+  DB200_CUDA(ctx, cudaGetLastError());
+  count_launch(ctx);
+  return DB200_OK;
+}
+
+int bar_steps16(db200_context* ctx, const double* step_max, double beta, double* taus) {
+  steps16_kernel<<<1, 32, 0, ctx->stream>>>(step_max, beta, taus);
   DB200_CUDA(ctx, cudaGetLastError());
   count_launch(ctx);
   return DB200_OK;

@@ -47,5 +47,7 @@ int bar_hinge(db200_context* ctx, int n, int r, const double* Z, long long ld, c
 int bar_add_identity(db200_context* ctx, double* M, int ldm, int r);
 int bar_scale_diag(db200_context* ctx, double* M, int ldm, int r, double factor);
 int bar_dot(db200_context* ctx, int r, const double* x, const double* y, double* out);
+// taus[k] = min(1, 0.99 * *step_max) beta^k for k < 16 (the line search's first candidates, formed on the device)
+int bar_steps16(db200_context* ctx, const double* step_max, double beta, double* taus);
 
 }  // namespace db200

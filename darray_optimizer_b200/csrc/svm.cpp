@@ -287,11 +287,12 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
   // A fixed launch sequence of a Newton step (its pointers and scalars are those of this call): at one rank it is
   // replayed from a CUDA graph, one launch instead of several per step; row-sharded it runs as it is, since its
   // all-reduces call back into the host.
-  long long c_bits = 0;
+  long long c_bits = 0, beta_bits = 0;
   std::memcpy(&c_bits, &C, sizeof(c_bits));
+  std::memcpy(&beta_bits, &P.beta, sizeof(beta_bits));
   auto seq = [&](long long tag, std::initializer_list<long long> extra, const std::function<int()>& body) -> int {
     if (dist) return body();
-    std::vector<long long> key = {tag, (long long)Z, ldz, n, r, (long long)base, (long long)a, c_bits};
+    std::vector<long long> key = {tag, (long long)Z, ldz, n, r, (long long)base, (long long)a, c_bits, beta_bits};
     key.insert(key.end(), extra);
     return graph_run(ctx, key, body);
   };
@@ -361,6 +362,26 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
   // check) updates w += tau v and zw += tau zv, which saves the two passes over Z that recompute them; the
   // outer step's stop test recomputes both from a.
   bool zw_ok = false;
+  // Capacity matrix M = I + Z^T D^-1 Z of the current D and its first Cholesky attempt (status in d_pair), enqueued
+  // only: the caller reads the status.
+  auto factor_launch = [&](bool use_tc) -> int {
+    const FactorSeq fs{Z, ldz, dinv, M, L, d_pair, n, r, use_tc, kSlices[tc_level], tc_scratch};
+    int s2;
+    if (!dist) {
+      // Gram, identity, backup, first Cholesky: one graph replay per Newton step (about 17 launches as separate
+      // calls, which the host's launch path serialises when many solves share the GPU)
+      const std::vector<long long> key = {(long long)Z, ldz, (long long)dinv, (long long)M, (long long)L,
+                                          (long long)d_pair, n, r, use_tc ? fs.slices : 0, (long long)tc_scratch};
+      return graph_run(ctx, key, [&]() -> int { return factor_seq(ctx, fs); });
+    }
+    if ((s2 = factor_gram(ctx, fs))) return s2;
+    if ((s2 = reduce(M, (long long)rr, DB200_REDUCE_SUM))) return s2;  // upper triangles summed
+    return factor_tail(ctx, fs);
+  };
+  // The first direction attempt of a Newton step factors its capacity matrix before the gradient statistics are
+  // read back, so that one readback returns both: pre_status holds that factorisation's status for factor().
+  bool prefactored = false, pre_tc = false;
+  int pre_status = 0;
   for (outer = 1; outer <= P.max_outer; ++outer) {
     int ni = 0;
     while (true) {
@@ -376,16 +397,23 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
         if ((st = bar_grad_hess(ctx, n, r, Z, ldz, w, a, C, t, g, dinv, red, nullptr, zw))) return st;
         zw_ok = true;
       }
-      if ((st = seq(5, {}, [&]() -> int {  // the row reductions and w.w into red[0..9) for one readback
+      pre_tc = mixed && tc_ok;
+      if ((st = factor_launch(pre_tc))) return st;
+      // the row reductions, w.w and the Cholesky status into red[0..13) for one readback
+      if ((st = seq(5, {}, [&]() -> int {
              int s2;
              if ((s2 = reduce_grad()) || (s2 = bar_dot(ctx, r, w, w, sc))) return s2;
              DB200_CUDA(ctx, cudaMemcpyAsync(red + 8, sc, sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+             DB200_CUDA(ctx, cudaMemcpyAsync(red + 12, d_pair, 2 * sizeof(int), cudaMemcpyDeviceToDevice,
+                                             ctx->stream));
              return DB200_OK;
            })))
         return st;
-      if ((st = fetch(red, 9))) return st;
+      if ((st = fetch(red, 13))) return st;
       const double suma = h[0], sumlog = h[1], dmax = h[2], dmin = h[3], ww = h[8];
-      if (dmax / dmin > 1e18) break;  // tests/testsvm.cpp:258-263
+      std::memcpy(&pre_status, &h[12], sizeof(int));
+      prefactored = true;
+      if (dmax / dmin > 1e18) break;  // tests/testsvm.cpp:258-263 (the factorisation above goes unused)
       const double lastg = 0.5 * ww - suma - sumlog / t;
       // Newton direction s = -(Z Z^T + D)^-1 g by Woodbury.  Mixed: capacity matrix M = I + Z^T D^-1 Z on the
       // int8 tensor cores (Ozaki slices, ~1e-12 of the column norms) factored in FP64, then iterative refinement
@@ -402,23 +430,17 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
         // to 1 until the Cholesky succeeds, keeps it positive definite; the shifted M still gives a descent
         // direction, which the mixed path's refinement corrects against the exact operator.  L keeps the
         // unshifted M for the retries.
-        const FactorSeq fs{Z, ldz, dinv, M, L, d_pair, n, r, use_tc, kSlices[tc_level], tc_scratch};
-        if (!dist) {
-          // Gram, identity, backup, first Cholesky: one graph replay per Newton step (about 17 launches as
-          // separate calls, which the host's launch path serialises when many solves share the GPU)
-          const std::vector<long long> key = {(long long)Z, ldz, (long long)dinv, (long long)M, (long long)L,
-                                              (long long)d_pair, n, r, use_tc ? fs.slices : 0,
-                                              (long long)tc_scratch};
-          if ((s2 = graph_run(ctx, key, [&]() -> int { return factor_seq(ctx, fs); }))) return s2;
+        int pst = 0, bad = 0;
+        if (prefactored && use_tc == pre_tc) {
+          pst = pre_status;  // factored before the gradient readback
         } else {
-          if ((s2 = factor_gram(ctx, fs))) return s2;
-          if ((s2 = reduce(M, (long long)rr, DB200_REDUCE_SUM))) return s2;  // upper triangles summed
-          if ((s2 = factor_tail(ctx, fs))) return s2;
+          if ((s2 = factor_launch(use_tc))) return s2;
+          if ((s2 = read_status(ctx, d_pair, &pst, &bad))) return s2;
         }
+        prefactored = false;
         double eps = 1e-11;
         for (int tries = 0;; ++tries) {
-          int pst = 0, bad = 0;
-          if ((s2 = read_status(ctx, d_pair, &pst, &bad))) return s2;
+          if (tries > 0 && (s2 = read_status(ctx, d_pair, &pst, &bad))) return s2;
           if (pst == 0 || tries == 11) break;
           DB200_CUDA(ctx, cudaMemcpyAsync(M, L, sizeof(double) * rr, cudaMemcpyDeviceToDevice, ctx->stream));
           if ((s2 = bar_scale_diag(ctx, M, r, r, 1.0 + eps))) return s2;
@@ -544,7 +566,9 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
         if ((st = newton_dir(false, &conv))) return st;
       }
       // v = Z^T s (unless current), the direction statistics of s ([0] g.s, [1] sum s, [2] largest step inside
-      // the box), w.v, v.v and the Cholesky status gathered in red[0..13) for one readback
+      // the box), w.v, v.v and the Cholesky status in red[0..13), and the line search's first 16 candidates,
+      // tau_k = min(1, 0.99 step_max) beta^k formed on the device from red[2], their barrier sums in red[32..64):
+      // one readback
       const bool need_v = !v_current;
       if ((st = seq(4, {need_v ? 1 : 0}, [&]() -> int {
              int s2;
@@ -556,40 +580,52 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
                                              ctx->stream));
              DB200_CUDA(ctx, cudaMemcpyAsync(red + 12, d_pair, 2 * sizeof(int), cudaMemcpyDeviceToDevice,
                                              ctx->stream));
+             if ((s2 = bar_steps16(ctx, red + 2, P.beta, taus))) return s2;
+             if ((s2 = bar_linesearch16(ctx, n, a, s, C, taus, ls))) return s2;
+             if ((s2 = reduce(ls, 32, DB200_REDUCE_SUM))) return s2;
+             DB200_CUDA(ctx, cudaMemcpyAsync(red + 32, ls, 32 * sizeof(double), cudaMemcpyDeviceToDevice,
+                                             ctx->stream));
              return DB200_OK;
            })))
         return st;
-      if ((st = fetch(red, 13))) return st;
+      if ((st = fetch(red, 64))) return st;
       int pst;
       std::memcpy(&pst, &h[12], sizeof(int));
       if (pst) return fail(ctx, DB200_ERR_NOT_SPD, "svm_barrier: Woodbury capacity matrix not positive definite");
       const double gs = h[0], sums = h[1], tmax = h[2], wv = h[8], vv = h[9];
       const double lam2 = -gs;
-      // backtracking line search inside the box, 16 candidates per device pass
+      // backtracking line search inside the box, 16 candidates per device pass; the first pass ran above with the
+      // same candidates (formed by the same multiplications as here)
       double tau = std::min(1.0, 0.99 * tmax);
       double accepted = -1.0, newg = lastg;
       for (int round = 0; round < 4 && accepted < 0; ++round) {
         double ht[16];
-        for (int k = 0; k < 16; ++k) ht[k] = tau * std::pow(P.beta, k);
-        // through the pinned staging area (past the readback slots): an asynchronous copy, which the fetch below
-        // completes before the next round writes the slots again
-        double* h_taus = ctx->h_pinned + 256;
-        std::memcpy(h_taus, ht, sizeof(ht));
-        DB200_CUDA(ctx, cudaMemcpyAsync(taus, h_taus, sizeof(ht), cudaMemcpyHostToDevice, ctx->stream));
-        if ((st = bar_linesearch16(ctx, n, a, s, C, taus, ls))) return st;
-        if ((st = reduce(ls, 32, DB200_REDUCE_SUM))) return st;
-        if ((st = fetch(ls, 32))) return st;
         for (int k = 0; k < 16; ++k) {
-          if (h[16 + k] != 0.0) continue;  // leaves the box
+          ht[k] = tau;
+          tau *= P.beta;
+        }
+        const double* hl = h + 32;  // round 0: read back with the step statistics
+        if (round > 0) {
+          // through the pinned staging area (past the readback slots): an asynchronous copy, which the fetch
+          // below completes before the next round writes the slots again
+          double* h_taus = ctx->h_pinned + 256;
+          std::memcpy(h_taus, ht, sizeof(ht));
+          DB200_CUDA(ctx, cudaMemcpyAsync(taus, h_taus, sizeof(ht), cudaMemcpyHostToDevice, ctx->stream));
+          if ((st = bar_linesearch16(ctx, n, a, s, C, taus, ls))) return st;
+          if ((st = reduce(ls, 32, DB200_REDUCE_SUM))) return st;
+          if ((st = fetch(ls, 32))) return st;
+          hl = h;
+        }
+        for (int k = 0; k < 16; ++k) {
+          if (hl[16 + k] != 0.0) continue;  // leaves the box
           const double tk = ht[k];
-          const double fk = 0.5 * (ww + 2.0 * tk * wv + tk * tk * vv) - (suma + tk * sums) - h[k] / t;
+          const double fk = 0.5 * (ww + 2.0 * tk * wv + tk * tk * vv) - (suma + tk * sums) - hl[k] / t;
           if (fk <= lastg + P.alpha * tk * gs) {
             accepted = tk;
             newg = fk;
             break;
           }
         }
-        tau = ht[15] * P.beta;
       }
       if (accepted < 0) accepted = 0.0;  // no decrease found: stop this Newton loop below
       if (accepted > 0) {
