@@ -275,31 +275,42 @@ __global__ void __launch_bounds__(256) potrf_block_kernel(double* A, int lda, in
   }
   __syncthreads();
   if (*(volatile int*)status) return;  // an earlier block column failed (checked after counting in)
-  // thread t owns column j = t & 63, rows i = rg + 4 q (q = 0..15)
+  // Thread t owns column j = t & 63 and the rows rg + 4 q.  The 64 steps run as 16 groups of 4 (a rolled loop, so
+  // that the kernel's code stays small: fully unrolled it missed the instruction cache most of the time when it ran
+  // between other kernels); the owners of the group's rows 4 kk .. 4 kk + 3 hold them in a[0], and after each
+  // group every thread shifts its column down by one row slot (a[q] holds row rg + 4 (q + kk)), so that no register
+  // is indexed at run time.
   const int j = t & 63, rg = t >> 6;
   double a[16];
 #pragma unroll
   for (int q = 0; q < 16; ++q) a[q] = rs[rg + 4 * q][j];
   bool failed = false;
+#pragma unroll 1
+  for (int kk = 0; 4 * kk < kb && !failed; ++kk) {
 #pragma unroll
-  for (int k = 0; k < 64; ++k) {
-    if (k >= kb) break;
-    const double own = a[k >> 2];  // this thread's element of row k (used by the row's owners only)
-    if (rg == (k & 3)) rowk[k & 1][j] = own;
-    __syncthreads();  // row k published; also orders the staging reads before the first rs write below
-    const double piv = rowk[k & 1][k];
-    if (!(piv > 0.0)) {  // the same value in every thread: a uniform exit
-      failed = true;
-      break;
-    }
-    const double u = 1.0 / piv;
-    const double ckj = rowk[k & 1][j] * u;
+    for (int kr = 0; kr < 4; ++kr) {
+      const int k = 4 * kk + kr;
+      if (k >= kb) break;
+      const double own = a[0];  // row k's element of column j for its owners (rg == kr)
+      if (rg == kr) rowk[k & 1][j] = own;
+      __syncthreads();  // row k published; also orders the staging reads before the first rs write below
+      const double piv = rowk[k & 1][k];
+      if (!(piv > 0.0)) {  // the same value in every thread: a uniform exit
+        failed = true;
+        break;
+      }
+      const double u = 1.0 / piv;
+      const double ckj = rowk[k & 1][j] * u;
 #pragma unroll
-    for (int q = 0; q < 16; ++q) {
-      const int i = rg + 4 * q;
-      if (i > k) a[q] -= rowk[k & 1][i] * ckj;  // i > j entries are never read back
+      for (int q = 0; q < 16; ++q) {
+        const int i = rg + 4 * (q + kk);
+        if (i > k && i < 64) a[q] -= rowk[k & 1][i] * ckj;  // i > j entries are never read back
+      }
+      if (rg == kr) rs[k][j] = (j >= k) ? own : 0.0;  // row k as eliminated (pivot at j == k)
     }
-    if (rg == (k & 3)) rs[k][j] = (j >= k) ? own : 0.0;  // row k as eliminated (pivot at j == k)
+#pragma unroll
+    for (int q = 0; q < 15; ++q) a[q] = a[q + 1];
+    a[15] = 0.0;
   }
   if (failed) {
     if (writer && t == 0 && atomicCAS(status, 0, DB200_ERR_NOT_SPD) == 0) *bad = k0;
@@ -338,16 +349,30 @@ __global__ void __launch_bounds__(256) potrf_block_kernel(double* A, int lda, in
     v[cc][0] = (ok && lane < kb) ? col[lane] : 0.0;
     v[cc][1] = (ok && lane + 32 < kb) ? col[lane + 32] : 0.0;
   }
-#pragma unroll
-  for (int i = 0; i < 64; ++i) {
+  // rows 0..31 of the solution (held in v[.][0]), then rows 32..63 (v[.][1]): two rolled loops, each with constant
+  // register indices
+#pragma unroll 4
+  for (int i = 0; i < 32; ++i) {
     if (i >= kb) break;
     const double ri = inv[i];
     const double r0 = rs[i][lane], r1 = rs[i][lane + 32];  // R[i][row] for this lane's two rows
 #pragma unroll
     for (int cc = 0; cc < 8; ++cc) {
-      const double x = __shfl_sync(0xffffffffu, v[cc][i >> 5], i & 31) * ri;
-      if (lane == (i & 31)) v[cc][i >> 5] = x;
-      if (i < 32 && lane > i) v[cc][0] -= r0 * x;
+      const double x = __shfl_sync(0xffffffffu, v[cc][0], i) * ri;
+      if (lane == i) v[cc][0] = x;
+      if (lane > i) v[cc][0] -= r0 * x;
+      v[cc][1] -= r1 * x;  // lane + 32 > i for every lane
+    }
+  }
+#pragma unroll 4
+  for (int i = 32; i < 64; ++i) {
+    if (i >= kb) break;
+    const double ri = inv[i];
+    const double r1 = rs[i][lane + 32];
+#pragma unroll
+    for (int cc = 0; cc < 8; ++cc) {
+      const double x = __shfl_sync(0xffffffffu, v[cc][1], i - 32) * ri;
+      if (lane == i - 32) v[cc][1] = x;
       if (lane + 32 > i) v[cc][1] -= r1 * x;
     }
   }
