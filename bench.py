@@ -382,20 +382,25 @@ def precision_legs(ctx, w, X, y, O, Y, steps=3):
     per = kms / steps  # the pass is one launch (every panel in one work list)
     out["compensated_promoted"] = {"ms_per_pass": per, "tflops": F / (per / 1e3) / 1e12,
                                    "err_vs_fp64": sampled_sketch_error(ctx, w, X, y, O64, Yc, rows)}
-    dmma, dfma = ctx.probe_fp64_peak()
+    # two plain-FP64 passes (the faster reported), then the FP64 peak probe: the probe's seconds of full-power
+    # DMMA would leave the clocks of a pass right after it lowered
     Y64 = torch.zeros((l, n), dtype=torch.float64, device="cuda")
     s = torch.cuda.current_stream()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(s)
-    ctx.rbf_sketch_f64(n, n, d, l, X.data_ptr(), d, X.data_ptr(), d, y.data_ptr(), y.data_ptr(), O64.data_ptr(), n,
-                       Y64.data_ptr(), n, w.gamma)
-    e1.record(s)
-    ctx.sync()
-    torch.cuda.synchronize()
-    ms64 = e0.elapsed_time(e1)
+    passes = []
+    for _ in range(2):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        ctx.rbf_sketch_f64(n, n, d, l, X.data_ptr(), d, X.data_ptr(), d, y.data_ptr(), y.data_ptr(), O64.data_ptr(),
+                           n, Y64.data_ptr(), n, w.gamma)
+        e1.record(s)
+        ctx.sync()
+        torch.cuda.synchronize()
+        passes.append(e0.elapsed_time(e1))
+    ms64 = min(passes)
+    dmma, dfma = ctx.probe_fp64_peak()
     tf64 = F / (ms64 / 1e3) / 1e12
-    out["fp64_pass"] = {"ms": ms64, "tflops": tf64, "dmma_peak_tflops": dmma, "dfma_peak_tflops": dfma,
-                        "frac_of_dmma_peak": tf64 / dmma,
+    out["fp64_pass"] = {"ms": ms64, "ms_both": passes, "tflops": tf64, "dmma_peak_tflops": dmma,
+                        "dfma_peak_tflops": dfma, "frac_of_dmma_peak": tf64 / dmma,
                         "kernel": "rbf_sketch_f64_kernel (fused FP64 DMMA distances + exp + sketch, K never stored)"}
     del Y64, O64, Yc
     return out

@@ -158,6 +158,7 @@ struct TileJob {
 struct TilePlan {
   int mode = 0, count = 0, n_items = 0, nsx = 0, nso = 0, nkc_max = 0, panel_max = 0, om_mult = 1;
   int clusters = 0;  // persistent grid: CTA pairs resident at once (at most one per item)
+  bool lean = false; // SKETCH with the single product and no promotion in every instance: the lean kernel
   size_t smem = 0;
   const void* table = nullptr;
   alignas(64) unsigned char tm1[4 * 128];  // instance 0's tensor maps (kernel parameters of one-instance launches)

@@ -365,7 +365,10 @@ __device__ __noinline__ void drain_sketch_chunk(const TileInst* I, int item, uin
 // CTA's own 128 rows, B (Xj, Omega~) is split by rows between the two CTAs, the accumulators (G, Y) sit in each
 // CTA's tensor memory for its own rows.  Each CTA loads its own operand halves with TMA and the completion is
 // counted on the leader's barrier.  All rings and barrier phases run on across work items and instances.
-template <int MODE>
+// LEAN (SKETCH launches whose every instance takes the single product without promotion): the compensated
+// product's residual split and the promoted accumulation's chunk drains are compiled out of the epilogue, whose
+// arithmetic sits on the critical path of the single-product pass (2.5 ms of 33 ms at C2 in the general form).
+template <int MODE, bool LEAN>
 __global__ void __launch_bounds__(NUM_THREADS, 1) rbf_tile_kernel(const __grid_constant__ LaunchArgs args) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -540,7 +543,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1) rbf_tile_kernel(const __grid_c
         Y.idesc_y2 = idesc_f16(PAIR_M, two ? n2 : 16, false);
         Y.y2_boff = (uint32_t)((n1 / 2) * 128) >> 4;
         Y.lo_boff = Y.y2_boff;  // compensated panels take one instruction: the lo rows sit where n2's would
-        const int comp = I->comp, promote = I->promote;
+        const int comp = LEAN ? 0 : I->comp, promote = LEAN ? 0 : I->promote;
         // both point sets exact in fp16 after scaling (no lo part anywhere): hi.hi only
         const bool exact = (MODE == RBF_MODE_SKETCH) && (*I->lof_i | *I->lof_j) == 0u;
         Y.tmem_p = tmem_base + (uint32_t)I->tmem_p;
@@ -590,8 +593,8 @@ __global__ void __launch_bounds__(NUM_THREADS, 1) rbf_tile_kernel(const __grid_c
       const int li = item - I->item_begin;
       const int it = li % I->n_itiles, pn = li / I->n_itiles;
       const int njt = I->n_jtiles, g_bufs = I->g_bufs, m = I->m;
-      const bool p_lo = (I->comp >= 1);
-      const int promote = (MODE == RBF_MODE_SKETCH) ? I->promote : 0;
+      const bool p_lo = !LEAN && (I->comp >= 1);
+      const int promote = (MODE == RBF_MODE_SKETCH && !LEAN) ? I->promote : 0;
       const float c_row = I->c_row;
       const float* sj = I->sj;
       const uint32_t t_p = tmem_base + t_lane + (uint32_t)I->tmem_p + (uint32_t)(qc * (EPI_COLS / 2));
@@ -658,8 +661,10 @@ __global__ void __launch_bounds__(NUM_THREADS, 1) rbf_tile_kernel(const __grid_c
           for (int c = 0; c < EPI_COLS / 2; ++c) {
             const __half2 hh = __floats2half2_rn(v[2 * c], v[2 * c + 1]);
             pk[c] = *reinterpret_cast<const uint32_t*>(&hh);
-            const float2 hf = __half22float2(hh);
-            pl[c] = pack_f16x2(v[2 * c] - hf.x, v[2 * c + 1] - hf.y);
+            if (!LEAN) {
+              const float2 hf = __half22float2(hh);
+              pl[c] = pack_f16x2(v[2 * c] - hf.x, v[2 * c + 1] - hf.y);
+            }
           }
           if (!__all_sync(0xffffffffu, mbar_wait(bar(B_P_EMPTY0 + h), (kp & 1) ^ 1, abort_flag))) {
             ok = false;
@@ -874,9 +879,9 @@ cudaLaunchConfig_t launch_config(cudaLaunchAttribute* attr, int clusters, size_t
 
 // Persistent grid size: as many CTA pairs as can be resident at once, no more than there are items.  Not
 // stream-ordered (so launches can be captured in a CUDA graph afterwards).
-template <int MODE>
+template <int MODE, bool LEAN>
 cudaError_t plan_clusters(size_t smem, int max_clusters, int n_items, int* clusters) {
-  auto k = rbf_tile_kernel<MODE>;
+  auto k = rbf_tile_kernel<MODE, LEAN>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   cudaLaunchAttribute attr[1];
@@ -891,11 +896,11 @@ cudaError_t plan_clusters(size_t smem, int max_clusters, int n_items, int* clust
   return cudaSuccess;
 }
 
-template <int MODE>
+template <int MODE, bool LEAN>
 cudaError_t launch_kernel(const LaunchArgs& a, size_t smem, int clusters, cudaStream_t st) {
   cudaLaunchAttribute attr[1];
   cudaLaunchConfig_t cfg = launch_config(attr, clusters, smem, st);
-  return cudaLaunchKernelEx(&cfg, rbf_tile_kernel<MODE>, a);
+  return cudaLaunchKernelEx(&cfg, rbf_tile_kernel<MODE, LEAN>, a);
 }
 
 }  // namespace
@@ -1045,6 +1050,8 @@ int prepare_rbf_tiles(db200_context* ctx, int mode, const TileJob* jobs, int cou
   T.nkc_max = nkc_max;
   T.panel_max = panel_max;
   T.nso = (mode == RBF_MODE_SKETCH) ? MAX_NSO : 0;
+  T.lean = (mode == RBF_MODE_SKETCH);
+  for (int b = 0; b < count; ++b) T.lean = T.lean && host[(size_t)b].comp == 0 && host[(size_t)b].promote == 0;
   T.om_mult = om_mult;
   {  // the Xj ring takes whatever shared memory is left
     const SmemLayout L0 = make_layout(nkc_max, panel_max, 0, T.nso, om_mult);
@@ -1057,9 +1064,12 @@ int prepare_rbf_tiles(db200_context* ctx, int mode, const TileJob* jobs, int cou
   T.smem = make_layout(nkc_max, panel_max, T.nsx, T.nso, om_mult).total + 1024;
   {
     const int max_clusters = ctx->num_sms / 2;
-    cudaError_t e = (mode == RBF_MODE_SKETCH)   ? plan_clusters<RBF_MODE_SKETCH>(T.smem, max_clusters, items, &T.clusters)
-                    : (mode == RBF_MODE_UPDATE) ? plan_clusters<RBF_MODE_UPDATE>(T.smem, max_clusters, items, &T.clusters)
-                                                : plan_clusters<RBF_MODE_KBLOCK>(T.smem, max_clusters, items, &T.clusters);
+    cudaError_t e =
+        (mode == RBF_MODE_SKETCH)
+            ? (T.lean ? plan_clusters<RBF_MODE_SKETCH, true>(T.smem, max_clusters, items, &T.clusters)
+                      : plan_clusters<RBF_MODE_SKETCH, false>(T.smem, max_clusters, items, &T.clusters))
+        : (mode == RBF_MODE_UPDATE) ? plan_clusters<RBF_MODE_UPDATE, false>(T.smem, max_clusters, items, &T.clusters)
+                                    : plan_clusters<RBF_MODE_KBLOCK, false>(T.smem, max_clusters, items, &T.clusters);
     DB200_CUDA(ctx, e);
   }
   const size_t bytes = tile_table_bytes(count);
@@ -1100,9 +1110,12 @@ int launch_rbf_plan(db200_context* ctx, const TilePlan& T) {
   a.status = ctx->d_status;
   cudaEvent_t e0 = nullptr;
   prof_begin(ctx, &e0);
-  cudaError_t err = (T.mode == RBF_MODE_SKETCH)   ? launch_kernel<RBF_MODE_SKETCH>(a, T.smem, T.clusters, ctx->stream)
-                    : (T.mode == RBF_MODE_UPDATE) ? launch_kernel<RBF_MODE_UPDATE>(a, T.smem, T.clusters, ctx->stream)
-                                                  : launch_kernel<RBF_MODE_KBLOCK>(a, T.smem, T.clusters, ctx->stream);
+  cudaError_t err =
+      (T.mode == RBF_MODE_SKETCH)
+          ? (T.lean ? launch_kernel<RBF_MODE_SKETCH, true>(a, T.smem, T.clusters, ctx->stream)
+                    : launch_kernel<RBF_MODE_SKETCH, false>(a, T.smem, T.clusters, ctx->stream))
+      : (T.mode == RBF_MODE_UPDATE) ? launch_kernel<RBF_MODE_UPDATE, false>(a, T.smem, T.clusters, ctx->stream)
+                                    : launch_kernel<RBF_MODE_KBLOCK, false>(a, T.smem, T.clusters, ctx->stream);
   DB200_CUDA(ctx, err);
   prof_end(ctx, e0);
   count_launch(ctx);
