@@ -598,16 +598,16 @@ int svm_barrier_impl(db200_context* ctx, int n, int r, const double* Z, int ldz,
       // same candidates (formed by the same multiplications as here)
       double tau = std::min(1.0, 0.99 * tmax);
       double accepted = -1.0, newg = lastg;
-      for (int round = 0; round < 4 && accepted < 0; ++round) {
+      for (int sweep = 0; sweep < 4 && accepted < 0; ++sweep) {
         double ht[16];
         for (int k = 0; k < 16; ++k) {
           ht[k] = tau;
           tau *= P.beta;
         }
-        const double* hl = h + 32;  // round 0: read back with the step statistics
-        if (round > 0) {
+        const double* hl = h + 32;  // the first pass: read back with the step statistics
+        if (sweep > 0) {
           // through the pinned staging area (past the readback slots): an asynchronous copy, which the fetch
-          // below completes before the next round writes the slots again
+          // below completes before the next sweep writes the slots again
           double* h_taus = ctx->h_pinned + 256;
           std::memcpy(h_taus, ht, sizeof(ht));
           DB200_CUDA(ctx, cudaMemcpyAsync(taus, h_taus, sizeof(ht), cudaMemcpyHostToDevice, ctx->stream));
