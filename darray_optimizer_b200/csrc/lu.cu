@@ -24,6 +24,7 @@
 
 #include "gridsync.cuh"
 #include "internal.h"
+#include "ptx.cuh"
 
 namespace db200 {
 
@@ -274,6 +275,159 @@ __global__ void __launch_bounds__(CP_THREADS) lu_panel_coop_kernel(float* A, lon
   }
 }
 
+// ------------------------------------------------------------------ cluster panel
+// The same column steps over the G <= 8 CTAs of one thread-block cluster (the grid is that one cluster): each CTA
+// holds its slice in shared memory and keeps its candidate record and, when it owns row j, row j in its own shared
+// memory (two slots by column parity, as above); one cluster barrier per column replaces the grid barrier, and the
+// other CTAs' records are read through distributed shared memory.  The pivot rule and the arithmetic are those of
+// lu_panel_coop_kernel, so both give the same factors.
+constexpr int CL_MAX = 16;        // cluster size limit (above 8 when the GPU allows non-portable clusters)
+constexpr int CL_THREADS = 1024;  // a thread per row of a 1024-row slice: the column step's latency chain is short
+
+__device__ __forceinline__ float ld_cluster_f32(uint32_t cluster_addr) {
+  float v;
+  asm volatile("ld.shared::cluster.f32 %0, [%1];" : "=f"(v) : "r"(cluster_addr) : "memory");
+  return v;
+}
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__global__ void __launch_bounds__(CL_THREADS) lu_panel_cluster_kernel(float* A, long long lda, int m, int k, int w,
+                                                                      int R, int* ipiv, int pivot, int* singular) {
+  extern __shared__ float tile[];  // [W][R]: tile[c * R + i] = A[r0 + i, k + c]
+  __shared__ float s_cand[2][CAND];  // this CTA's candidate record per column parity
+  __shared__ float s_rowj[2][W];     // row j, in the CTA that owns it
+  __shared__ float urow[W];
+  __shared__ float red_v[CL_THREADS / 32];
+  __shared__ int red_i[CL_THREADS / 32];
+  __shared__ int s_win;
+  const int tid = threadIdx.x, lane = tid % 32, wid = tid / 32;
+  const int G = gridDim.x, b = blockIdx.x;  // one cluster: the block index is the rank in the cluster
+  const int r0 = k + b * R;
+  const int rows = max(0, min(R, m - r0));
+  for (int e = tid; e < w * R; e += CL_THREADS) {
+    const int c = e / R, i = e % R;
+    tile[c * R + i] = i < rows ? A[(r0 + i) + (long long)(k + c) * lda] : 0.0f;
+  }
+  __syncthreads();
+  for (int jj = 0; jj < w; ++jj) {
+    const int j = k + jj, par = jj & 1;
+    // local candidate: the largest |a| of column jj among own rows >= j, the smallest row on ties
+    float bv = -1.0f;
+    int bi = m;
+    for (int i = tid; i < rows; i += CL_THREADS) {
+      const int r = r0 + i;
+      const float v = fabsf(tile[jj * R + i]);
+      if (r >= j && v > bv) {
+        bv = v;
+        bi = r;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ov > bv || (ov == bv && oi < bi)) {
+        bv = ov;
+        bi = oi;
+      }
+    }
+    if (lane == 0) {
+      red_v[wid] = bv;
+      red_i[wid] = bi;
+    }
+    __syncthreads();
+    if (wid == 0) {  // the 32 warp candidates, reduced by one warp (lower warps hold lower rows: ties keep the row)
+      bv = red_v[lane];
+      bi = red_i[lane];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const float ov = __shfl_xor_sync(0xffffffffu, bv, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ov > bv || (ov == bv && oi < bi)) {
+          bv = ov;
+          bi = oi;
+        }
+      }
+      if (lane == 0) {
+        s_cand[par][0] = bv;
+        s_cand[par][1] = __int_as_float(bi);
+        s_win = bi;
+      }
+    }
+    __syncthreads();
+    const int lbi = s_win;
+    if (tid < w) s_cand[par][2 + tid] = (lbi < m) ? tile[tid * R + (lbi - r0)] : 0.0f;
+    if (j >= r0 && j < r0 + rows && tid < w) s_rowj[par][tid] = tile[tid * R + (j - r0)];
+    cluster_sync_all();  // every record of this column published
+    // the same pivot in every CTA: the largest candidate, the smallest row on ties (one warp reads the G records)
+    if (wid == 0) {
+      float gv = -1.0f;
+      int gb = -1, gi = m;
+      for (int q = lane; q < G; q += 32) {
+        const uint32_t cq = mapa_shared(smem_addr(&s_cand[par][0]), (uint32_t)q);
+        const float v = ld_cluster_f32(cq);
+        const int r = __float_as_int(ld_cluster_f32(cq + 4));
+        if (v > gv || (v == gv && r < gi)) {
+          gv = v;
+          gi = r;
+          gb = q;
+        }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const float ov = __shfl_xor_sync(0xffffffffu, gv, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, gi, o);
+        const int ob = __shfl_xor_sync(0xffffffffu, gb, o);
+        if (ov > gv || (ov == gv && oi < gi)) {
+          gv = ov;
+          gi = oi;
+          gb = ob;
+        }
+      }
+      if (lane == 0) {
+        s_win = pivot ? gb : -1;
+        if (b == 0) ipiv[j] = (pivot && gi < m) ? gi + 1 : j + 1;
+        red_i[0] = (pivot && gi < m) ? gi : j;
+      }
+    }
+    __syncthreads();
+    const int p = red_i[0], wb = s_win;
+    const uint32_t owner_j = (uint32_t)((j - k) / R);
+    float old_j = 0.0f;  // row j's value in column tid, from its owner
+    if (tid < w) {
+      old_j = ld_cluster_f32(mapa_shared(smem_addr(&s_rowj[par][tid]), owner_j));
+      urow[tid] = (wb >= 0 && p != j) ? ld_cluster_f32(mapa_shared(smem_addr(&s_cand[par][2 + tid]), (uint32_t)wb))
+                                      : old_j;
+    }
+    __syncthreads();
+    if (p != j && tid < w) {
+      if (p >= r0 && p < r0 + rows) tile[tid * R + (p - r0)] = old_j;      // old row j to row p
+      if (j >= r0 && j < r0 + rows) tile[tid * R + (j - r0)] = urow[tid];  // pivot row to row j
+    }
+    __syncthreads();
+    const float d = urow[jj];
+    if (d == 0.0f) {  // the same in every CTA: all of them go on to the next column's cluster barrier
+      if (b == 0 && tid == 0) atomicCAS(singular, 0, j + 1);
+      continue;
+    }
+    const float inv = 1.0f / d;
+    for (int i = tid; i < rows; i += CL_THREADS) {
+      if (r0 + i <= j) continue;
+      const float l = tile[jj * R + i] * inv;
+      tile[jj * R + i] = l;
+      for (int c = jj + 1; c < w; ++c) tile[c * R + i] = fmaf(-l, urow[c], tile[c * R + i]);
+    }
+    __syncthreads();
+  }
+  cluster_sync_all();  // no CTA leaves while another may still read its records
+  for (int e = tid; e < w * R; e += CL_THREADS) {
+    const int c = e / R, i = e % R;
+    if (i < rows) A[(r0 + i) + (long long)(k + c) * lda] = tile[c * R + i];
+  }
+}
+
 // Row interchanges ipiv[k .. k+w) (1-based, relative to row 0) applied in order to columns [c0, c1) and
 // [c2, c3).
 __global__ void lu_laswp_kernel(float* A, long long lda, int k, int w, const int* ipiv, int c0, int c1, int c2,
@@ -443,6 +597,37 @@ int lu_factorize(db200_context* ctx, int m, int n, int nleft, float* A, long lon
                                                                   cp_smem));
     if (coop && per_sm > 0) coop_max = std::min(ctx->num_sms * per_sm, 4096);
   }
+  // the cluster panel: the largest cluster (16, else the portable 8) of CTAs with full slices that fits
+  int cl_max = 0;
+  {
+    DB200_CUDA(ctx, cudaFuncSetAttribute(lu_panel_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)cp_smem));
+    const bool wide = cudaFuncSetAttribute(lu_panel_cluster_kernel,
+                                           cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess;
+    cudaGetLastError();
+    for (int size : {CL_MAX, 8}) {
+      if (size > 8 && !wide) continue;
+      cudaLaunchConfig_t cfg = {};
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = (unsigned)size;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.gridDim = dim3((unsigned)size);
+      cfg.blockDim = dim3(CL_THREADS);
+      cfg.dynamicSmemBytes = cp_smem;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      int clusters = 0;
+      const bool fits = cudaOccupancyMaxActiveClusters(&clusters, lu_panel_cluster_kernel, &cfg) == cudaSuccess &&
+                        clusters >= 1;
+      cudaGetLastError();
+      if (fits) {
+        cl_max = size;
+        break;
+      }
+    }
+  }
   // the tensor-core trailing update: workspace for the largest (first) trailing matrix, taken before the loop so
   // that no later step reallocates it
   constexpr long long TC_MIN_ENTRIES = 1 << 20;
@@ -458,7 +643,25 @@ int lu_factorize(db200_context* ctx, int m, int n, int nleft, float* A, long lon
     // CTAs of at least 64 rows each, at most one slice of CP_MAX_ROWS per CTA
     int G = std::min(coop_max, (rows + 63) / 64);
     const int R = G > 0 ? (rows + G - 1) / G : 0;
-    if (G > 0 && R <= CP_MAX_ROWS) {
+    // cluster panel: up to cl_max CTAs of at least 256 rows (at least 1024 beyond 8 CTAs)
+    int Gc = std::min(8, std::max(1, (rows + 255) / 256));
+    if (rows > 8 * 1024) Gc = std::min(cl_max, (rows + 1023) / 1024);
+    const int Rc = (rows + Gc - 1) / Gc;
+    if (cl_max > 0 && Gc <= cl_max && Rc <= CP_MAX_ROWS) {
+      cudaLaunchConfig_t cfg = {};
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = (unsigned)Gc;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.gridDim = dim3((unsigned)Gc);
+      cfg.blockDim = dim3(CL_THREADS);
+      cfg.dynamicSmemBytes = (size_t)Rc * W * sizeof(float);
+      cfg.stream = ctx->stream;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      DB200_CUDA(ctx, cudaLaunchKernelEx(&cfg, lu_panel_cluster_kernel, A, lda, m, k, w, Rc, ipiv, pivot, singular));
+    } else if (G > 0 && R <= CP_MAX_ROWS) {
       if (bar_base > 0x40000000u) {  // keep the monotone barrier target far from wrapping
         DB200_CUDA(ctx, cudaMemsetAsync(bar, 0, sizeof(unsigned), ctx->stream));
         bar_base = 0;
