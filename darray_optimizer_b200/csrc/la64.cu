@@ -5,6 +5,7 @@
 // the panel, syrk on the trailing matrix), include/blas_like.h:63-127 (matrix_multiply T,N; triangular_solve
 // L,U,T,N) and include/cblas_like.h:40-69, in FP64 on the GPU.  All matrices are column major.
 #include <cstdio>
+#include <type_traits>
 
 #include "internal.h"
 #include "la64.h"
@@ -141,6 +142,153 @@ __global__ void __launch_bounds__(GTHREADS, 1) gram_kernel(int n, int p, int q, 
       }
     }
   }
+}
+
+// The same Gram for FP64 operands with 16-byte-aligned columns (base and leading dimensions), as a cp.async
+// pipeline: 16-row stages of A's and B's 128 columns land column-major in shared memory (padded so that the
+// fragment loads of a warp spread over the banks), GP_STAGES deep, while the 8 warps run the DMMA tiles of the
+// stage before; a stage's rows past the split's end or columns past p / q are zero-filled by the copy.  The weights
+// scale A's fragments.  Same tiles, accumulators and epilogue as gram_kernel.
+constexpr int GP_KS = 16;                   // rows per stage
+constexpr int GP_KPAD = GP_KS + 4;          // doubles per staged column (= 4 mod 16: conflict-free fragment loads)
+constexpr int GP_STAGES = 4;
+constexpr int GP_STAGE_DOUBLES = 2 * GT * GP_KPAD;  // A and B
+constexpr size_t GP_SMEM = (size_t)GP_STAGES * GP_STAGE_DOUBLES * sizeof(double);
+
+__device__ __forceinline__ void gp_cp16(double* smem, const double* gmem, int valid_doubles) {
+  const uint32_t sa = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+  const int bytes = valid_doubles <= 0 ? 0 : (valid_doubles >= 2 ? 16 : 8);  // the rest zero-filled
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(sa), "l"(gmem), "r"(bytes) : "memory");
+}
+
+__global__ void __launch_bounds__(GTHREADS, 1) gram_pipe_kernel(int n, int p, int q, const double* __restrict__ A,
+                                                               long long lda, const double* __restrict__ B,
+                                                               long long ldb, const double* __restrict__ w,
+                                                               double alpha, double* C, int ldc, int rows_per_split,
+                                                               int upper_only, int atomic) {
+  const int bi = blockIdx.x, bj = blockIdx.y;
+  if (upper_only && bi > bj) return;
+  extern __shared__ __align__(16) double gsm[];
+  const int i0 = bi * GT, j0 = bj * GT;
+  const int r0 = blockIdx.z * rows_per_split;
+  const int r1 = min(n, r0 + rows_per_split);
+  const int lane = threadIdx.x % 32, warp = threadIdx.x / 32;
+  const int wm = warp / 2, wn = warp % 2;  // warp tile: rows 32 wm .. +31, columns 64 wn .. +63
+  const int fr = lane / 4, fk = lane % 4;
+  const int nst = (r1 > r0) ? (r1 - r0 + GP_KS - 1) / GP_KS : 0;
+  // stage s: rows r0 + 16 s .. + 15; each thread copies 4 chunks of A and 4 of B (16 B = 2 rows of one column)
+  auto issue = [&](int st) {
+    double* sA = gsm + (size_t)(st % GP_STAGES) * GP_STAGE_DOUBLES;
+    double* sB = sA + GT * GP_KPAD;
+    const int kbase = r0 + st * GP_KS;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int e = threadIdx.x + GTHREADS * u;  // 0 .. 1023: column e / 8, row pair e % 8
+      const int c = e >> 3, kp = (e & 7) * 2;
+      const int k = kbase + kp;
+      const int valid = (k < r1) ? min(2, r1 - k) : 0;
+      const int ia = i0 + c, jb = j0 + c;
+      gp_cp16(sA + c * GP_KPAD + kp, (ia < p && valid) ? A + (long long)ia * lda + k : A, ia < p ? valid : 0);
+      gp_cp16(sB + c * GP_KPAD + kp, (jb < q && valid) ? B + (long long)jb * ldb + k : B, jb < q ? valid : 0);
+    }
+  };
+  double acc[2][8][4];
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int b = 0; b < 8; ++b)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) acc[a][b][e] = 0.0;
+#pragma unroll
+  for (int st = 0; st < GP_STAGES - 1; ++st) {
+    if (st < nst) issue(st);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  }
+  for (int st = 0; st < nst; ++st) {
+    asm volatile("cp.async.wait_group %0;" ::"n"(GP_STAGES - 2) : "memory");
+    __syncthreads();  // stage st visible to all; stage st - 1's buffer is free for the copy below
+    if (st + GP_STAGES - 1 < nst) issue(st + GP_STAGES - 1);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    const double* sA = gsm + (size_t)(st % GP_STAGES) * GP_STAGE_DOUBLES;
+    const double* sB = sA + GT * GP_KPAD;
+    const int kbase = r0 + st * GP_KS;
+#pragma unroll
+    for (int kk = 0; kk < GP_KS; kk += 8) {
+      double wa = 1.0, wb = 1.0;
+      if (w) {
+        const int ka = kbase + kk + fk, kb = ka + 4;
+        wa = ka < r1 ? __ldg(w + ka) : 0.0;
+        wb = kb < r1 ? __ldg(w + kb) : 0.0;
+      }
+      double af[2][4], bf[8][2];
+#pragma unroll
+      for (int a = 0; a < 2; ++a) {
+        const int r = 32 * wm + 16 * a + fr;
+        af[a][0] = wa * sA[r * GP_KPAD + kk + fk];
+        af[a][1] = wa * sA[(r + 8) * GP_KPAD + kk + fk];
+        af[a][2] = wb * sA[r * GP_KPAD + kk + fk + 4];
+        af[a][3] = wb * sA[(r + 8) * GP_KPAD + kk + fk + 4];
+      }
+#pragma unroll
+      for (int b = 0; b < 8; ++b) {
+        const int c = 64 * wn + 8 * b + fr;
+        bf[b][0] = sB[c * GP_KPAD + kk + fk];
+        bf[b][1] = sB[c * GP_KPAD + kk + fk + 4];
+      }
+#pragma unroll
+      for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 8; ++b) dmma16(acc[a][b], af[a], bf[b]);
+    }
+  }
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+#pragma unroll
+  for (int a = 0; a < 2; ++a) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int i = i0 + 32 * wm + 16 * a + 8 * h + fr;
+      if (i >= p) continue;
+#pragma unroll
+      for (int b = 0; b < 8; ++b) {
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int j = j0 + 64 * wn + 8 * b + 2 * fk + e;
+          if (j >= q) continue;
+          if (upper_only && i > j) continue;
+          double* dst = C + (long long)j * ldc + i;
+          const double v = alpha * acc[a][b][2 * h + e];
+          if (atomic)
+            atomicAdd(dst, v);
+          else
+            *dst += v;
+        }
+      }
+    }
+  }
+}
+
+// Whether gram_pipe_kernel can stage A and B (16-byte copies: aligned bases, even leading dimensions).
+inline bool gram_pipe_ok(const double* A, long long lda, const double* B, long long ldb) {
+  return (reinterpret_cast<uintptr_t>(A) % 16 == 0) && (reinterpret_cast<uintptr_t>(B) % 16 == 0) && lda % 2 == 0 &&
+         ldb % 2 == 0;
+}
+
+// Launch of the FP64 Gram tiles (pipelined when the operands allow it), grid (tp, tq, splits).
+int launch_gram64(db200_context* ctx, dim3 grid, int n, int p, int q, const double* A, long long lda, const double* B,
+                  long long ldb, const double* w, double alpha, double* C, int ldc, int rows, bool upper_only,
+                  bool atomic) {
+  if (gram_pipe_ok(A, lda, B, ldb)) {
+    DB200_CUDA(ctx, cudaFuncSetAttribute(gram_pipe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)GP_SMEM));
+    gram_pipe_kernel<<<grid, GTHREADS, GP_SMEM, ctx->stream>>>(n, p, q, A, lda, B, ldb, w, alpha, C, ldc, rows,
+                                                               upper_only ? 1 : 0, atomic ? 1 : 0);
+  } else {
+    gram_kernel<double, double><<<grid, GTHREADS, 0, ctx->stream>>>(n, p, q, A, lda, B, ldb, w, alpha, C, ldc, rows,
+                                                                    upper_only ? 1 : 0, atomic ? 1 : 0);
+  }
+  DB200_CUDA(ctx, cudaGetLastError());
+  count_launch(ctx);
+  return DB200_OK;
 }
 
 // C[n x q] = alpha * A[n x p] * op(B) + beta * C (op(B) = B, p x q, or B^T with B q x p when transB) on the FP64
@@ -810,6 +958,8 @@ int gram(db200_context* ctx, int n, int p, int q, const TA* A, long long lda, co
   splits = (n + rows - 1) / rows;
   if (splits > 65535) return fail(ctx, DB200_ERR_UNSUPPORTED, "gram: too many row splits");
   dim3 grid(tp, tq, splits);
+  if constexpr (std::is_same<TA, double>::value && std::is_same<TBt, double>::value)
+    return launch_gram64(ctx, grid, n, p, q, A, lda, B, ldb, w, alpha, C, ldc, rows, upper_only, splits > 1);
   gram_kernel<TA, TBt><<<grid, GTHREADS, 0, ctx->stream>>>(n, p, q, A, lda, B, ldb, w, alpha, C, ldc, rows,
                                                      upper_only ? 1 : 0, splits > 1 ? 1 : 0);
   DB200_CUDA(ctx, cudaGetLastError());
@@ -874,9 +1024,9 @@ int potrf_upper(db200_context* ctx, double* A, int lda, int l, int* d_status, in
       if (pr > 0) {
         const double* P = A + (long long)(k0 + kb) * lda + k0;
         double* C = A + (long long)(k0 + kb) * lda + k0 + kb;
-        gram_kernel<double, double><<<dim3((pr + GT - 1) / GT, (rest + GT - 1) / GT, 1), GTHREADS, 0,
-                                      ctx->stream>>>(kb, pr, rest, P, lda, P, lda, nullptr, -1.0, C, lda, kb, 1, 0);
-        count_launch(ctx);
+        const int s2 = launch_gram64(ctx, dim3((pr + GT - 1) / GT, (rest + GT - 1) / GT, 1), kb, pr, rest, P, lda, P,
+                                     lda, nullptr, -1.0, C, lda, kb, true, false);
+        if (s2) return s2;
       }
     }
     const int rest = l - K0 - KB;
@@ -886,14 +1036,15 @@ int potrf_upper(db200_context* ctx, double* A, int lda, int l, int* d_status, in
       double* C = A + (long long)(K0 + KB) * lda + K0 + KB;
       if (KB > nb || big(rest)) {
         const int tp = (rest + GT - 1) / GT;
-        gram_kernel<double, double><<<dim3(tp, tp, 1), GTHREADS, 0, ctx->stream>>>(KB, rest, rest, P, lda, P, lda,
-                                                                                 nullptr, -1.0, C, lda, KB, 1, 0);
+        const int s2 = launch_gram64(ctx, dim3(tp, tp, 1), KB, rest, rest, P, lda, P, lda, nullptr, -1.0, C, lda, KB,
+                                     true, false);
+        if (s2) return s2;
       } else {
         // the r ~ 500..2000 capacity factors of the barrier: 32 x 32 tiles, so that they spread over the GPU
         const int nt = (rest + 31) / 32;
         syrk_update_kernel<<<nt * (nt + 1) / 2, 256, 0, ctx->stream>>>(P, lda, KB, rest, C, lda, d_status);
+        count_launch(ctx);
       }
-      count_launch(ctx);
     }
     K0 += KB;
   }
