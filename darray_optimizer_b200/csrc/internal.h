@@ -100,8 +100,11 @@ int lu_factorize(db200_context* ctx, int m, int n, int nleft, float* A, long lon
 
 // ------------------------------------------------------------------ RBF tile engine (rbf_tile.cu)
 // SKETCH: Y = (y_i y_j exp(-gamma d_ij^2)) Omega; KBLOCK: K = y_i y_j exp(-gamma d_ij^2) stored; UPDATE: the distance
-// GEMM alone, out[i, j] += alpha x_i.x_j (TileJob::gamma carries alpha), the split-fp16 product of a rank-d update
-enum RbfMode { RBF_MODE_SKETCH = 0, RBF_MODE_KBLOCK = 1, RBF_MODE_UPDATE = 2 };
+// GEMM alone, out[i, j] += alpha x_i.x_j (TileJob::gamma carries alpha), the split-fp16 product of a rank-d update;
+// KNN: the 8 smallest squared distances d_ij^2 of each point i over the points j of each quarter of the tile columns,
+// sorted, in out[32 i + 8 quarter + t] (TileJob::gamma = 1; TileJob::yj carries the points' indices as int, and j
+// with index i is skipped)
+enum RbfMode { RBF_MODE_SKETCH = 0, RBF_MODE_KBLOCK = 1, RBF_MODE_UPDATE = 2, RBF_MODE_KNN = 3 };
 
 struct PackedPoints {
   const void* xp = nullptr;   // fp16 [npad][2*dp]: [hi | lo] split of each point scaled by the set's 2^e

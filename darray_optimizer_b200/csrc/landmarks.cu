@@ -99,6 +99,42 @@ __global__ void __launch_bounds__(KNN_THREADS) knn_kernel(int n, int d, const fl
   }
 }
 
+// Rows ref[j] of X (point-major) gathered into R (s x d, point-major with leading dimension d).
+__global__ void gather_rows_kernel(const float* __restrict__ X, int ldx, const int* __restrict__ ref, int s, int d,
+                                   float* __restrict__ R) {
+  const long long total = (long long)s * d;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+    const int j = (int)(e / d), c = (int)(e % d);
+    R[e] = X[(long long)ref[j] * ldx + c];
+  }
+}
+
+// out[i] = sqrt of the k-th smallest of the 32 candidates part[32 i ..] (four sorted quarters of 8).
+__global__ void knn_merge_kernel(int n, const float* __restrict__ part, int k, float* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float best[8];
+#pragma unroll
+  for (int t = 0; t < 8; ++t) best[t] = INFINITY;
+  const float* p = part + (size_t)i * 32;
+#pragma unroll 4
+  for (int c = 0; c < 32; ++c) {
+    float x = p[c];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      const float lo = fminf(best[t], x), hi = fmaxf(best[t], x);
+      best[t] = lo;
+      x = hi;
+    }
+  }
+  float v = best[0];
+#pragma unroll
+  for (int t = 0; t < 8; ++t)
+    if (t == k - 1) v = best[t];
+  out[i] = sqrtf(fmaxf(v, 0.0f));
+}
+
+
 // F[i, :] = [x_i (d), ||x_i||, knn_i], row major n x (d + 2); one warp per point.
 __global__ void features_kernel(int n, int d, const float* __restrict__ X, int ldx, const float* __restrict__ knn,
                                 float* __restrict__ F) {
@@ -461,6 +497,53 @@ struct LandTimer {
 
 // ------------------------------------------------------------------ internal entry points (shared with C ABI)
 int knn_distance(db200_context* ctx, int n, int d, const float* X, int ldx, int s, const int* ref, int k, float* out) {
+  if (k <= 8 && d <= 128) {
+    // On the tensor cores: squared distances |x_i|^2 + |x_j|^2 - 2 x_i.x_j from the tile engine's split-fp16
+    // distance GEMM (22 significant bits per coordinate), each row's 8 smallest per column quarter kept in
+    // registers (RBF_MODE_KNN), then the quarters merged.  The reference points are gathered and packed as the
+    // second point set; their indices skip each point's own distance.
+    const int dp = feature_pad(d), npad = point_pad(n), spad = point_pad(s);
+    const size_t bytes = 4096 + (size_t)s * d * 4 + (size_t)npad * 2 * dp * 2 + packed_norm_floats(npad) * 4 +
+                         (size_t)spad * 2 * dp * 2 + packed_norm_floats(spad) * 4 + (size_t)n * 32 * 4 + 8 * 256;
+    char* ws = static_cast<char*>(workspace(ctx, bytes));
+    if (!ws) return DB200_ERR_NOMEM;
+    Carve cv{ws};
+    float* R = cv.take<float>((size_t)s * d);
+    void* xq = cv.take<uint16_t>((size_t)npad * 2 * dp);
+    float* nq = cv.take<float>(packed_norm_floats(npad));
+    void* xr = cv.take<uint16_t>((size_t)spad * 2 * dp);
+    float* nr = cv.take<float>(packed_norm_floats(spad));
+    float* part = cv.take<float>((size_t)n * 32);
+    gather_rows_kernel<<<blocks_for((long long)s * d, 256, 65535LL * 8), 256, 0, ctx->stream>>>(X, ldx, ref, s, d, R);
+    DB200_CUDA(ctx, cudaGetLastError());
+    count_launch(ctx);
+    int st = pack_points(ctx, X, ldx, DB200_POINT_MAJOR, n, d, dp, npad, xq, nq);
+    if (!st) st = pack_points(ctx, R, d, DB200_POINT_MAJOR, s, d, dp, spad, xr, nr);
+    if (st) return st;
+    TileJob J;
+    J.pi.xp = xq;
+    J.pi.norms = nq;
+    J.pi.n = n;
+    J.pi.npad = npad;
+    J.pi.dp = dp;
+    J.pj.xp = xr;
+    J.pj.norms = nr;
+    J.pj.n = s;
+    J.pj.npad = spad;
+    J.pj.dp = dp;
+    J.yj = reinterpret_cast<const float*>(ref);  // the reference points' indices (RBF_MODE_KNN)
+    J.gamma = 1.0f;
+    J.out = part;
+    J.ldo = 32;
+    TilePlan T;
+    if ((st = prepare_rbf_tiles(ctx, RBF_MODE_KNN, &J, 1, nullptr, 0, &T))) return st;
+    if ((st = launch_rbf_plan(ctx, T))) return st;
+    knn_merge_kernel<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(n, part, k, out);
+    DB200_CUDA(ctx, cudaGetLastError());
+    count_launch(ctx);
+    return DB200_OK;
+  }
+  // k > 8: one thread per query on the FP32 pipes
   const unsigned grid = (unsigned)((n + KNN_THREADS - 1) / KNN_THREADS);
   if (d <= 32)
     knn_kernel<32><<<grid, KNN_THREADS, 0, ctx->stream>>>(n, d, X, ldx, s, ref, k, out);

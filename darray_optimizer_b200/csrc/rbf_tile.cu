@@ -15,6 +15,8 @@
 //         or  K[i, j] = y_i y_j P   stored as fp32 (KBLOCK mode)
 //         or  out[i, j] += alpha 2^-(e_I+e_J) G, no exp (UPDATE mode: the split-fp16 product of a rank-d update, e.g.
 //             the trailing update of a blocked LU, with x_i the rows of L21 and x_j the columns of U12)
+//         or  the 8 smallest d_ij^2 = |x_i|^2 + |x_j|^2 - 2 x.y of each row per column quarter, kept sorted in registers
+//             across the j tiles (KNN mode: k-nearest-neighbour distances; a second kernel merges the quarters)
 // so the kernel matrix is never written to HBM in SKETCH mode.  Algorithm restated from
 // include/dkernel.cu:102-129 (vecnorm, rbf) and :151-178 / :194-231 (distance GEMM, rbf, sketch GEMM).
 //
@@ -608,6 +610,9 @@ __global__ void __launch_bounds__(NUM_THREADS, 1) rbf_tile_kernel(const __grid_c
       const float y_i = (i < m && I->yi) ? I->yi[i] : 1.0f;
       sjbuf[lane] = sj[qc * EPI_COLS + lane];  // tile 0 of this item
       __syncwarp();
+      float best[8];  // KNN: this row's 8 smallest squared distances in this column quarter, ascending
+#pragma unroll
+      for (int t = 0; t < 8; ++t) best[t] = INFINITY;
       bool pending_drain = false, pending_acc = false;
       auto drain = [&](bool accumulate) -> bool {
         if (!__all_sync(0xffffffffu, mbar_wait(bar(B_Y_FULL), ydone & 1, abort_flag))) return false;
@@ -639,7 +644,28 @@ __global__ void __launch_bounds__(NUM_THREADS, 1) rbf_tile_kernel(const __grid_c
         if (lane == 0) mbar_arrive_remote(lbar(B_G_EMPTY0 + b));
 
         const int j0 = jt * BN + qc * EPI_COLS;
-        if (MODE != RBF_MODE_UPDATE) {
+        if (MODE == RBF_MODE_KNN) {
+          // d^2 = |x_i|^2 + |x_j|^2 - 2 x.y (x.y = c_dot G), inserted into the sorted list; padding columns and the
+          // point itself skipped
+          const float* sjt = sjbuf + (jt & 1) * EPI_COLS;
+          const int* idx_j = reinterpret_cast<const int*>(yj_all);
+          const float s_i = I->si[i];
+#pragma unroll
+          for (int c = 0; c < EPI_COLS; ++c) {
+            const int j = j0 + c;
+            const float d2 = fmaf(-2.0f * c_dot, v[c], s_i + sjt[c]);
+            if (j < n_cols && d2 < best[7] && __ldg(idx_j + j) != i) {
+              float x = d2;
+#pragma unroll
+              for (int t = 0; t < 8; ++t) {  // insertion: x moves down while it is smaller
+                const float lo = fminf(best[t], x), hi = fmaxf(best[t], x);
+                best[t] = lo;
+                x = hi;
+              }
+            }
+          }
+        }
+        if (MODE != RBF_MODE_UPDATE && MODE != RBF_MODE_KNN) {
           const float4* sj4 = reinterpret_cast<const float4*>(sjbuf + (jt & 1) * EPI_COLS);
 #pragma unroll
           for (int c = 0; c < EPI_COLS / 4; ++c) {
@@ -693,6 +719,8 @@ __global__ void __launch_bounds__(NUM_THREADS, 1) rbf_tile_kernel(const __grid_c
           for (int dd = 0; dd < 2 && ok; ++dd)
             if (dq[dd] && !drain(da[dd])) ok = false;
           if (!ok) break;
+        } else if (MODE == RBF_MODE_KNN) {
+          // (the list was updated above)
         } else if (MODE == RBF_MODE_UPDATE) {
           // each (i, j) has one owner thread: a plain read-modify-write, 8 columns at a time with every load
           // issued before the first store (the stores could alias the loads, so interleaved they would serialise)
@@ -726,6 +754,11 @@ __global__ void __launch_bounds__(NUM_THREADS, 1) rbf_tile_kernel(const __grid_c
         }
       }
       if (!ok) break;
+      if (MODE == RBF_MODE_KNN && i < m) {
+        float* o = I->out + (size_t)i * 32 + qc * 8;
+#pragma unroll
+        for (int t = 0; t < 8; ++t) o[t] = best[t];
+      }
       if (MODE == RBF_MODE_SKETCH && !promote) {
         if (!drain(false)) { ok = false; break; }
       }
@@ -1023,7 +1056,8 @@ int prepare_rbf_tiles(db200_context* ctx, int mode, const TileJob* jobs, int cou
     I.l = J.l;
     I.nkc = kp / KC;
     I.c_row = -J.gamma * LOG2E;
-    I.c_dot = (mode == RBF_MODE_UPDATE) ? J.gamma : 2.0f * J.gamma * LOG2E;  // UPDATE: gamma carries alpha
+    // UPDATE: gamma carries alpha; KNN: 1
+    I.c_dot = (mode == RBF_MODE_UPDATE || mode == RBF_MODE_KNN) ? J.gamma : 2.0f * J.gamma * LOG2E;
     I.si = pi.norms;
     I.sj = pj.norms;
     // the pack writes the set's max |x|, its scale and whether any lo part is nonzero after the norms (a slice of a
@@ -1069,6 +1103,7 @@ int prepare_rbf_tiles(db200_context* ctx, int mode, const TileJob* jobs, int cou
             ? (T.lean ? plan_clusters<RBF_MODE_SKETCH, true>(T.smem, max_clusters, items, &T.clusters)
                       : plan_clusters<RBF_MODE_SKETCH, false>(T.smem, max_clusters, items, &T.clusters))
         : (mode == RBF_MODE_UPDATE) ? plan_clusters<RBF_MODE_UPDATE, false>(T.smem, max_clusters, items, &T.clusters)
+        : (mode == RBF_MODE_KNN)    ? plan_clusters<RBF_MODE_KNN, false>(T.smem, max_clusters, items, &T.clusters)
                                     : plan_clusters<RBF_MODE_KBLOCK, false>(T.smem, max_clusters, items, &T.clusters);
     DB200_CUDA(ctx, e);
   }
@@ -1115,6 +1150,7 @@ int launch_rbf_plan(db200_context* ctx, const TilePlan& T) {
           ? (T.lean ? launch_kernel<RBF_MODE_SKETCH, true>(a, T.smem, T.clusters, ctx->stream)
                     : launch_kernel<RBF_MODE_SKETCH, false>(a, T.smem, T.clusters, ctx->stream))
       : (T.mode == RBF_MODE_UPDATE) ? launch_kernel<RBF_MODE_UPDATE, false>(a, T.smem, T.clusters, ctx->stream)
+      : (T.mode == RBF_MODE_KNN)    ? launch_kernel<RBF_MODE_KNN, false>(a, T.smem, T.clusters, ctx->stream)
                                     : launch_kernel<RBF_MODE_KBLOCK, false>(a, T.smem, T.clusters, ctx->stream);
   DB200_CUDA(ctx, err);
   prof_end(ctx, e0);
