@@ -5,6 +5,7 @@
 #include <string>
 
 #include "internal.h"
+#include "la64.h"
 
 namespace db200 {
 
@@ -188,6 +189,7 @@ int db200_create(db200_context** out, int device, void* stream) {
     db200_destroy(ctx);
     return DB200_ERR_CUDA;
   }
+  db200::potrf_cluster_init(ctx);
   *out = ctx;
   return DB200_OK;
 }

@@ -51,6 +51,8 @@ struct db200_context {
   bool graphs_off = false;   // a capture failed once: sequences run eagerly from then on
   // Row-sharded solves (db200_set_collective): the host's all-reduce; world 1 = none attached.
   int coll_world = 1, coll_rank = 0;
+  // Largest thread-block cluster of the one-launch Cholesky (potrf_cluster.cu) this device holds; 0: none.
+  int potrf_nc_max = 0;
   db200_allreduce_fn coll_fn = nullptr;
   void* coll_user = nullptr;
 };

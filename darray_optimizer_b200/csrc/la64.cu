@@ -998,6 +998,12 @@ template int gemm_tall<float, float>(db200_context*, int, int, int, const float*
 
 int potrf_upper(db200_context* ctx, double* A, int lda, int l, int* d_status, int* d_bad, int nb) {
   if (nb < 1 || nb > 64) nb = 64;
+  // up to l = 544 (the barrier's capacity matrices, the CholeskyQR2 and Nystrom Grams) the whole factor is one
+  // launch on a thread-block cluster; an explicit smaller block size keeps the multi-kernel path
+  if (nb == 64) {
+    const int s = potrf_cluster(ctx, A, lda, l, d_status, d_bad);
+    if (s != DB200_ERR_UNSUPPORTED) return s;
+  }
   // the diagonal-block kernel's arrival counter starts every factorisation at zero
   DB200_CUDA(ctx, cudaMemsetAsync(ctx->d_status + 1, 0, sizeof(int), ctx->stream));
   // A trailing matrix of at least one wave of 128 x 128 upper tiles takes its update on the FP64 tensor cores

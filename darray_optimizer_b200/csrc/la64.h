@@ -20,6 +20,14 @@ int gemm_tall(db200_context* ctx, int n, int p, int q, const TA* A, long long ld
 // Restates cholesky_factorize(A, 'U', n, 0, bs) of include/lapack_like.h:10-56.
 int potrf_upper(db200_context* ctx, double* A, int lda, int l, int* d_status, int* d_bad, int nb = 64);
 
+// The same factor in one launch on a thread-block cluster for 1 <= l <= 544 (potrf_cluster.cu); returns
+// DB200_ERR_UNSUPPORTED, launching nothing, where no cluster configuration holds the matrix.  potrf_cluster_init
+// probes the device's largest cluster once (outside any stream capture); potrf_cluster_size gives the cluster size
+// used for l (0: none).
+void potrf_cluster_init(db200_context* ctx);
+int potrf_cluster_size(const db200_context* ctx, int l);
+int potrf_cluster(db200_context* ctx, double* A, int lda, int l, int* d_status, int* d_bad);
+
 // X = R^-1 for upper triangular R.
 int trinv_upper(db200_context* ctx, const double* R, int ldr, int l, double* X, int ldx);
 

@@ -252,6 +252,22 @@ __device__ __forceinline__ void mbar_arrive_expect_tx_remote(uint32_t cluster_ad
 __device__ __forceinline__ void st_shared_remote_u32(uint32_t cluster_addr, uint32_t v) {
   asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(cluster_addr), "r"(v) : "memory");
 }
+__device__ __forceinline__ uint32_t cluster_nctarank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ double ld_shared_remote_f64(uint32_t cluster_addr) {
+  double v;
+  asm volatile("ld.shared::cluster.f64 %0, [%1];" : "=d"(v) : "r"(cluster_addr) : "memory");
+  return v;
+}
+// 16-byte load from a 16-byte aligned location in the shared memory of a CTA of the cluster
+__device__ __forceinline__ double2 ld_shared_remote_v2f64(uint32_t cluster_addr) {
+  double2 v;
+  asm volatile("ld.shared::cluster.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "r"(cluster_addr) : "memory");
+  return v;
+}
 // Wait with cluster-scope acquire: for barriers that the other CTA of the pair arrives on.
 __device__ __forceinline__ bool mbar_try_wait_cluster(uint32_t bar, uint32_t parity) {
   uint32_t ok;

@@ -95,6 +95,76 @@ def test_potrf_large_matches_oracle(gpu_ctx, n, nb):
     assert np.all(np.tril(R, -1) == 0)
 
 
+@pytest.mark.parametrize("n", [1, 2, 31, 32, 33, 64, 65, 100, 138, 272, 300, 511, 513, 528, 544])
+def test_potrf_cluster_matches_oracle(gpu_ctx, n):
+    # up to n = 544 the default block size takes the one-launch cluster factor (one kernel, no lower-triangle pass)
+    import torch
+    g = np.random.default_rng(1000 + n)
+    B = g.standard_normal((n, n))
+    A = B @ B.T / n + np.eye(n)
+    lda = n + 7
+    dA = torch.zeros((n, lda), dtype=torch.float64, device="cuda")
+    dA[:, :n] = torch.from_numpy(np.ascontiguousarray(A.T)).cuda()
+    dA[:, n:] = 5.0  # rows beyond n stay untouched
+    low = torch.tril(torch.ones((n, n), dtype=torch.bool, device="cuda"), -1)  # rows i > j of column j
+    dA[:, :n][low.T] = float("nan")  # the strictly lower triangle is never read
+    l0 = gpu_ctx.launches()
+    gpu_ctx.potrf(n, dA.data_ptr(), lda)
+    assert gpu_ctx.launches() - l0 == 1
+    R = h64(dA, n)
+    assert rel(R, O.cholesky_upper(A)) < 1e-11
+    assert np.all(np.tril(R, -1) == 0)
+    assert bool((dA[:, n:] == 5.0).all())
+
+
+@pytest.mark.parametrize("n", [96, 528])
+def test_potrf_cluster_agrees_with_blocked_path(gpu_ctx, n):
+    g = np.random.default_rng(n)
+    B = g.standard_normal((n, n))
+    A = B @ B.T / n + 0.1 * np.eye(n)
+    d1, d2 = d64(A), d64(A)
+    gpu_ctx.potrf(n, d1.data_ptr(), n)       # one cluster launch
+    gpu_ctx.potrf(n, d2.data_ptr(), n, 32)   # the multi-kernel path
+    R1, R2 = h64(d1, n), h64(d2, n)
+    assert rel(R1, R2) < 1e-12
+
+
+@pytest.mark.parametrize("n", [300, 544])
+def test_potrf_cluster_known_answer_min_matrix(gpu_ctx, n):
+    # min(i+1, j+1) factors exactly (every pivot 1): the factor must be the upper triangle of ones, bit for bit
+    import torch
+    i = torch.arange(1, n + 1, device="cuda", dtype=torch.float64)
+    A = torch.minimum(i[:, None], i[None, :])
+    gpu_ctx.potrf(n, A.data_ptr(), n)
+    gpu_ctx.sync()
+    assert float((A - torch.tril(torch.ones_like(A))).abs().max()) == 0.0
+
+
+@pytest.mark.parametrize("n,bad", [(300, 0), (300, 31), (300, 32), (300, 150), (300, 299), (544, 520), (5, 4)])
+def test_potrf_cluster_not_spd_reports_block(gpu_ctx, n, bad):
+    A = np.eye(n)
+    A[bad, bad] = -1.0
+    dA = d64(A)
+    with pytest.raises(DB200Error) as ei:
+        gpu_ctx.potrf(n, dA.data_ptr(), n)
+    assert ei.value.status == -3  # DB200_ERR_NOT_SPD
+    assert f"starting at row {bad // 32 * 32}" in str(ei.value)
+    # the context stays usable: an SPD factor right after
+    A2 = np.eye(n) * 4.0
+    d2 = d64(A2)
+    gpu_ctx.potrf(n, d2.data_ptr(), n)
+    assert np.allclose(h64(d2, n), 2.0 * np.eye(n))
+
+
+def test_potrf_cluster_nan_pivot_reports_error(gpu_ctx):
+    A = np.eye(200)
+    A[77, 77] = np.nan
+    dA = d64(A)
+    with pytest.raises(DB200Error) as ei:
+        gpu_ctx.potrf(200, dA.data_ptr(), 200)
+    assert ei.value.status == -3
+
+
 def test_potrf_test3_factor_and_reference(gpu_ctx):
     A = G["chol_test3_A"].astype(np.float64)
     dA = d64(A)
