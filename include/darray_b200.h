@@ -161,7 +161,9 @@ DB200_API int db200_lra_host(db200_context* ctx, int n, int d, int k, const floa
  * ------------------------------------------------------------------------------------------------------ */
 
 /* In-place upper Cholesky A = R^T R of the n x n matrix A (only the upper triangle is read; the strictly lower
- * part is zeroed), blocked right-looking with block size nb (<= 64; 0 = 64).  A non-positive pivot returns
+ * part is zeroed), blocked right-looking with block size nb (<= 64; 0 = 64).  With nb = 64 and n <= 544 the whole
+ * factor is one kernel on a thread-block cluster, in 32-column steps (the failing block named below is then the
+ * 32-row block).  A non-positive pivot returns
  * DB200_ERR_NOT_SPD (db200_last_error names the failing block).  Replaces cholesky_factorize(A, 'U', n, 0, bs)
  * and cholesky_factorize_recursive (include/lapack_like.h:10-90), in FP64.  Synchronous. */
 DB200_API int db200_potrf(db200_context* ctx, int n, double* A, int lda, int nb);
