@@ -165,7 +165,7 @@ def test_svm_solve_landmarks_end_to_end(gpu_ctx, tol, expect_fallback):
 def test_svm_solve_landmarks_matches_oracle_on_same_landmarks(gpu_ctx):
     """The learned-landmark solve against the FP64 oracle's Nystrom solve on the same landmarks
     (oracle/landmarks.py: landmark_factor, then the oracle barrier): the landmarks come from
-    db200_select_landmarks with the solve's seed; dual objective within the north star's 1e-6."""
+    db200_select_landmarks with the solve's seed; dual objective within 1e-6 relative, the SVM parity target."""
     import torch
     from darray_optimizer_b200._lib import Mlp
     w = _mixture(8192, 14)

@@ -144,7 +144,7 @@ def test_lowrank_factor_matches_oracle(gpu_ctx, precision, tol):
     assert rep.nu > 0
 
 
-# dual objective against the oracle's: the north star's 1e-6 for the compensated mixed path and FP64; the fast
+# dual objective against the oracle's: 1e-6 relative (the SVM parity target) for the compensated mixed path and FP64; the fast
 # mixed form's single fp16 sketch product leaves ~2e-5 at this size (4e-4 at n = 131072)
 @pytest.mark.parametrize("precision,ftol", [(0, 1e-6), (1, 1e-8), (2, 1e-4)])
 def test_svm_solve_end_to_end_matches_oracle(gpu_ctx, precision, ftol):
